@@ -1,0 +1,198 @@
+/*
+ * x2 — C ABI of the B200 path-sample engine (libx2.so).
+ *
+ * The reference has no C ABI for this path: it sits behind two C++ interfaces, the per-sample
+ * `integrate<Backend>(const mixed::Config&, U32 pixel, U32 index, Backend&, Radiance&)`
+ * (xpu2/interactive/async_integrator.h:3047) and the per-lane `GpuLane`
+ * (xpu2/interactive/async_gpu.h:82, begin/launch/poll/downloadFilm/sums/counts at :1372-1707).
+ * Every entry point below names the reference interface it replaces.
+ *
+ * Conventions: plain C, status codes are int (X2_OK = 0). Handles are owned by the library; the caller
+ * owns every array it passes. No callbacks. One context is used from one host thread. Calls are
+ * asynchronous on the context's CUDA stream except where a comment says they wait; waits are bounded.
+ */
+#ifndef X2_H
+#define X2_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes. The reference reports failures as cpu::need -> std::runtime_error on the host and as
+ * SampleStatus::Error / DeviceState::errors on the device (async_gpu_abi.h:45); here they are codes. */
+enum {
+    X2_OK = 0,
+    X2_EINVAL = 1,    /* a bad argument: null pointer, size out of range, config the engine does not admit */
+    X2_ECUDA = 2,     /* a CUDA runtime error (x2_last_error has the text) */
+    X2_ENOMEM = 3,    /* a device or host allocation failed */
+    X2_ETIMEOUT = 4,  /* a bounded wait gave up */
+    X2_EAUDIT = 5,    /* the per-pixel sample-count audit failed (async_render.h:1036-1039) */
+    X2_ENODEV = 6,    /* no CUDA device */
+    X2_EDEVICE = 7    /* the device reported errors (sample errors, a traversal stack overflow) */
+};
+
+/* Per-sample outcome, SampleStatus in async_integrator.h:35 (same values). */
+enum { X2_DONE = 0, X2_MISS = 1, X2_ERROR = 2, X2_SKIP = 3, X2_DEFER = 4 };
+
+/* sample::Identity (sample_stream.h:42): 32-bit pixel, 64-bit sample index, stream (frame seed) and branch. */
+typedef struct x2_identity {
+    uint32_t pixel;
+    uint32_t pad;
+    uint64_t index, stream, branch;
+} x2_identity;
+
+/* The unit of work, async::Chunk (async_integrator.h:3057-3063): one 8x8 tile and a sample range. 16 bytes. */
+typedef struct x2_chunk {
+    uint32_t tile, first, count, cell;
+} x2_chunk;
+
+/* Pixel filters, surface::Filter (surface_core.h:24). */
+enum { X2_FILTER_BOX = 0 };
+
+/* Materials admitted: the UsdPreviewSurface subset (shade_material.h:338-383) with useSpecularWorkflow = 1.
+ * LAMBERT: diffuseColor = diffuse, specularColor black -> one Lambert lobe (shade_builder.h:689-697).
+ * GGX: the Schlick specular path (MatModoUsdSpecular; shade_builder.h:541-556): one GGX lobe whose Fresnel is
+ * Schlick with F0 = specular, plus a Lambert lobe under it only when diffuse is not black (not admitted: keep it
+ * black). emission is emissiveColor (addEmission). */
+enum { X2_MAT_LAMBERT = 0, X2_MAT_GGX = 1 };
+typedef struct x2_material {
+    uint32_t kind;
+    float diffuse[3];
+    float specular[3];
+    float emission[3];
+    float roughness;
+} x2_material;
+
+/* Lights admitted: lights::Light (light_core.h:59-117) of type Env (constant, whole sphere or hemisphere, no
+ * image) and Rect (no image, no spread, no clear radius). Linear parts are rows, as the reference stores them. */
+enum { X2_LIGHT_ENV = 0, X2_LIGHT_RECT = 1 };
+enum { X2_SIDE_REGULAR = 0, X2_SIDE_REVERSE = 1, X2_SIDE_TWO = 2 };
+typedef struct x2_light {
+    uint32_t type, sidedness, visible_in_camera, hemispherical;
+    float radiance[3];
+    float position[3], direction[3];  /* local origin; local +Z (the lit side of a one-sided rect), unit */
+    float local2render[3][3];         /* rows, with scale */
+    float render2local[3][3];         /* its inverse (rows) */
+    float render2local_rot[3][3];     /* rotation only (rows) */
+    float scale, inv_area, plane_offset, half_width, half_height;
+    uint32_t visibility_mask;         /* rdl2 VisibilityType bits of the lobes that see it (0xfc: all) */
+} x2_light;
+
+/* surface::Camera's perspective subset (surface_core.h:93-115): row-vector matrices, clip planes. */
+typedef struct x2_camera {
+    float raster_to_camera[4][4];
+    float camera_to_render[4][4];
+    float near_clip, far_clip;
+} x2_camera;
+
+/* A scene: triangles grouped by mesh (geom), meshes contiguous in triangle order; each mesh one material.
+ * Vertices are fp32 (3 a vertex), triangles 3 vertex indices each. mesh_first has mesh_count + 1 entries. */
+typedef struct x2_scene_desc {
+    uint32_t vertex_count, triangle_count, mesh_count, material_count, light_count, pad;
+    const float* vertices;
+    const uint32_t* triangles;
+    const uint32_t* mesh_first;
+    const uint32_t* mesh_material;
+    const x2_material* materials;
+    const x2_light* lights;
+    x2_camera camera;
+} x2_scene_desc;
+
+/* mixed::Config (gpu_jobs.h:10-44), the fields this engine reads, field for field with the same defaults
+ * (x2_config_defaults). Policy 15 and the shadow-reuse mask are what mixed::config (cpu_jobs.h:8-27) sets for
+ * the path tracer. */
+typedef struct x2_config {
+    uint32_t width, height, seed, spp, sampling;
+    uint32_t filter;
+    float filter_width;
+    uint32_t light_count, bsdf_samples, light_samples, max_depth, max_diffuse_depth, clamp_depth;
+    float rr_threshold, clamp_value;
+    uint32_t max_glossy_depth, max_mirror_depth, max_hair_depth, max_presence_depth, shadow_terminator_fix;
+    float roughness_clamping, transparency_threshold;
+    uint32_t visible_lights;
+    float presence_threshold, presence_quality;
+    uint32_t shadow_reuse;
+    uint32_t reserved[8];
+} x2_config;
+
+/* Ray counters, the reference's XPU2_PROFILE ray counts (async_gpu_abi.h:16-20): hit rays (trace), shadow rays
+ * of light samples (NEE) and of BSDF samples, and the bounces that stood for a shadow ray (held). */
+typedef struct x2_counters {
+    uint64_t trace, shadow_nee, shadow_bsdf, held, samples, errors, stack_overflows, pad;
+} x2_counters;
+
+/* A finished launch, GpuLane's Completion (async_gpu.h:65-71). */
+typedef struct x2_completion {
+    uint64_t launch;      /* its sequence number */
+    uint64_t samples;     /* samples finished (Done or Skip) */
+    uint64_t errors;      /* samples that ended in Error */
+    float milliseconds;   /* device time of the launch (CUDA events on the context's stream) */
+    uint32_t pad;
+} x2_completion;
+
+typedef struct x2_ctx x2_ctx;
+typedef struct x2_scene x2_scene;
+
+/* ---- library ---- */
+const char* x2_version(void);
+const char* x2_last_error(void);        /* text of the last failure on this thread */
+void x2_config_defaults(x2_config* c);  /* mixed::Config's defaults (gpu_jobs.h:11-44) plus the path tracer's */
+
+/* ---- context: replaces GpuLane's construction (async_gpu.h:82) ---- */
+int x2_open(int device, x2_ctx** out);
+int x2_close(x2_ctx* ctx);
+int x2_synchronize(x2_ctx* ctx, int timeout_ms);  /* waits (bounded) for the context's stream */
+
+/* ---- sampler test API: sample::samplingWord (sample_stream.h:127-144) for n identities/dimensions ---- */
+int x2_sample_words(x2_ctx* ctx, const x2_identity* ids, const uint32_t* dims, uint64_t n, uint32_t policy,
+                    uint32_t* out);                      /* host arrays; waits */
+int x2_sample_words_device(x2_ctx* ctx, const x2_identity* d_ids, const uint32_t* d_dims, uint64_t n,
+                           uint32_t policy, uint32_t* d_out);  /* device arrays; asynchronous */
+
+/* ---- scene: replaces the plan upload of GpuLane (cpu::Plan -> device records) ---- */
+int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* desc, x2_scene** out);  /* builds the BVH on the device */
+int x2_scene_free(x2_scene* scene);
+int x2_config_set(x2_scene* scene, const x2_config* config);  /* mixed::config(plan) */
+int x2_scene_info(x2_scene* scene, uint64_t* bvh_nodes, uint64_t* bvh_bytes, uint64_t* triangle_bytes,
+                  float* build_ms);
+
+/* ---- per-sample API: integrate() (async_integrator.h:3047) for n (pixel, index) pairs ----
+ * pairs: 2n uint32 (pixel, index); rgba: 4n doubles (Radiance rgb + alpha); status: n SampleStatus. */
+int x2_integrate(x2_scene* scene, const uint32_t* pairs, uint64_t n, double* rgba, uint32_t* status); /* waits */
+int x2_integrate_device(x2_scene* scene, const uint32_t* d_pairs, uint64_t n, double* d_rgba, uint32_t* d_status);
+
+/* ---- traversal API: Backend::trace / Backend::visible (async_cpu.h:669-720, :944-967; async_gpu_device.h:298-355,
+ * 521-533) for n rays, 8 floats each (origin xyz, direction xyz, near, far): the closest hit's scene triangle
+ * (~0u: none) and t, and whether anything occludes [near, far]. ---- */
+int x2_trace_rays(x2_scene* scene, const float* rays, uint64_t n, uint32_t* tri, float* t, uint32_t* occluded); /* waits */
+int x2_trace_rays_device(x2_scene* scene, const float* d_rays, uint64_t n, uint32_t* d_tri, float* d_t, uint32_t* d_occluded);
+
+/* ---- lane API: GpuLane::begin/launch/poll/downloadFilm/sums/counts (async_gpu.h:1372-1707) ---- */
+int x2_frame_begin(x2_scene* scene, uint32_t samples_per_chunk);          /* begin(): clears the film */
+int x2_launch(x2_scene* scene, const x2_chunk* chunks, uint32_t count);   /* launch(): host chunks */
+int x2_poll(x2_scene* scene, x2_completion* out);  /* poll(): 1 and *out when a launch finished, 0 if none */
+int x2_wait(x2_scene* scene, int timeout_ms, x2_completion* out);  /* waits for every launch in flight */
+int x2_render_frame(x2_scene* scene, uint32_t first, uint32_t count);  /* every tile, samples [first, first+count) */
+int x2_film_download(x2_scene* scene, double* sums, double* odd, uint32_t* counts);  /* downloadFilm(); waits */
+int x2_film_device(x2_scene* scene, double** d_sums, double** d_odd, uint32_t** d_counts);
+int x2_audit(x2_scene* scene, const uint32_t* expected, int64_t* bad_pixel);  /* async_render.h:992-1048 */
+int x2_counters_read(x2_scene* scene, x2_counters* out);  /* waits */
+int x2_counters_reset(x2_scene* scene);
+/* Counting mode (no reference counterpart; the algorithmic-bytes count of the roofline): launches made while it is
+ * on count BVH node visits and triangle tests per ray. It slows them: never time a counting launch. */
+int x2_count_traversal(x2_scene* scene, int on);
+int x2_traversal_counts(x2_scene* scene, uint64_t* rays, uint64_t* nodes, uint64_t* triangles);  /* waits; resets */
+
+/* ---- host-side synthetic scenes (test and bench inputs, not the hot path) ----
+ * config_id 0: the closed box with two boxes and a rect light; 1: heightfield + icospheres with 16 rect lights
+ * and an environment; 100 + k: a config-1 variant scaled down by k (fewer tiles and spheres) for tests.
+ * The descriptor and its arrays are owned by the library until x2_scene_desc_free. */
+int x2_scene_generate(uint32_t config_id, uint64_t seed, x2_scene_desc** out, x2_config* config);
+void x2_scene_desc_free(x2_scene_desc* desc);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* X2_H */

@@ -1,0 +1,625 @@
+// ORACLE — test infrastructure only. Never linked into, called by or shipped with the product path.
+//
+// The reference's own CPU integrator, `integratePaths<Backend>` (xpu2/interactive/async_integrator.h:1986-3042),
+// compiled UNMODIFIED from the reference's headers (oracle/Makefile) and driven by OracleBackend, which this
+// file writes following the reference's CpuBackend (xpu2/interactive/async_cpu.h:586-1163): a hit is
+// reconstructed by the reference's resume::geometryHit (resume_core.h:17-45), shaded by the reference's
+// hitState + shadeMaterial (shade_material.h:121, :787), lit by the reference's lights::sample/eval/intersect
+// (light_core.h:988-1025). The only part not from the reference is traversal: the reference delegates it to
+// Embree (async_cpu.h:669-720, :944-967), which is absent here, so this file supplies a binary BVH whose
+// triangle test (Woop et al. 2013, watertight, fp32, no contraction) and tie break (nearest t, then lowest
+// triangle) are the same arithmetic the device traversal uses: both devices then choose the same primitive.
+// The film and the chunk loop follow renderChunk (async_cpu.h:1584-1667) and the audit async_render.h:992-1048.
+#define XPU2_PATHS_ONLY 1
+#include "async_integrator.h"
+
+#include "../include/x2.h"
+
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <thread>
+#include <vector>
+
+namespace xi = xpu2::interactive;
+using xi::sample::U32;
+using xi::sample::U64;
+using xi::surface::V3;
+
+namespace {
+
+// ---- traversal (the Embree stand-in) ----
+struct Node {
+    float lo[3], hi[3];
+    U32 first, count;  // leaf: triangles [first, first+count) of order; inner: left child = first, right = first+1
+};
+
+struct Bvh {
+    std::vector<Node> nodes;
+    std::vector<U32> order;
+};
+
+struct TriTest {  // Woop, Benthin, Wald 2013: the ray's shear, once a ray
+    int kx, ky, kz;
+    float Sx, Sy, Sz;
+};
+inline TriTest shear(V3 d) {
+    const float ax = std::fabs(d.x), ay = std::fabs(d.y), az = std::fabs(d.z);
+    TriTest s;
+    s.kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    s.kx = s.kz == 2 ? 0 : s.kz + 1;
+    s.ky = s.kx == 2 ? 0 : s.kx + 1;
+    const float dz = (&d.x)[s.kz];
+    if (dz < 0.0f) std::swap(s.kx, s.ky);
+    s.Sx = (&d.x)[s.kx] / dz;
+    s.Sy = (&d.x)[s.ky] / dz;
+    s.Sz = 1.0f / dz;
+    return s;
+}
+// The hit distance t of the ray against triangle (a, b, c), or false. Same operations as the device test.
+inline bool triHit(const TriTest& s, V3 o, V3 a, V3 b, V3 c, float tmin, float tmax, float& tOut) {
+    const float A[3] = {a.x - o.x, a.y - o.y, a.z - o.z}, B[3] = {b.x - o.x, b.y - o.y, b.z - o.z},
+                C[3] = {c.x - o.x, c.y - o.y, c.z - o.z};
+    const float Ax = A[s.kx] - s.Sx * A[s.kz], Ay = A[s.ky] - s.Sy * A[s.kz];
+    const float Bx = B[s.kx] - s.Sx * B[s.kz], By = B[s.ky] - s.Sy * B[s.kz];
+    const float Cx = C[s.kx] - s.Sx * C[s.kz], Cy = C[s.ky] - s.Sy * C[s.kz];
+    float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
+        V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+        W = float(double(Bx) * double(Ay) - double(By) * double(Ax));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = U + V + W;
+    if (det == 0.0f) return false;
+    const float Az = s.Sz * A[s.kz], Bz = s.Sz * B[s.kz], Cz = s.Sz * C[s.kz];
+    const float T = U * Az + V * Bz + W * Cz;
+    const float t = T / det;
+    if (!(t >= tmin && t <= tmax)) return false;
+    tOut = t;
+    return true;
+}
+
+struct Scene {
+    std::vector<V3> vertices;
+    std::vector<U32> tris;       // 3 a triangle
+    std::vector<U32> triGeom;    // mesh of each triangle
+    std::vector<U32> meshFirst;  // mesh_count + 1
+    std::vector<xi::lights::Light> lights;
+    std::vector<xi::shade::MaterialRecord> records;  // one a mesh
+    std::vector<float> pool;
+    xi::mixed::Config config{};
+    Bvh bvh;
+    V3 vertex(U32 i) const { return vertices[i]; }
+};
+
+void buildBvh(Scene& s) {
+    const U32 n = U32(s.tris.size() / 3);
+    std::vector<float> cen(size_t(n) * 3);
+    std::vector<float> blo(size_t(n) * 3), bhi(size_t(n) * 3);
+    for (U32 t = 0; t < n; ++t) {
+        const V3 a = s.vertex(s.tris[3 * t]), b = s.vertex(s.tris[3 * t + 1]), c = s.vertex(s.tris[3 * t + 2]);
+        const float lo[3] = {std::min({a.x, b.x, c.x}), std::min({a.y, b.y, c.y}), std::min({a.z, b.z, c.z})};
+        const float hi[3] = {std::max({a.x, b.x, c.x}), std::max({a.y, b.y, c.y}), std::max({a.z, b.z, c.z})};
+        for (int k = 0; k < 3; ++k) {
+            blo[3 * t + k] = lo[k];
+            bhi[3 * t + k] = hi[k];
+            cen[3 * t + k] = 0.5f * (lo[k] + hi[k]);
+        }
+    }
+    s.bvh.order.resize(n);
+    for (U32 i = 0; i < n; ++i) s.bvh.order[i] = i;
+    s.bvh.nodes.clear();
+    s.bvh.nodes.reserve(size_t(n) * 2 / 2 + 16);
+    struct Item { U32 node, first, count; };
+    std::vector<Item> work;
+    s.bvh.nodes.push_back(Node{});
+    work.push_back({0, 0, n});
+    while (!work.empty()) {
+        const Item it = work.back();
+        work.pop_back();
+        Node nd{};
+        float clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+        for (int k = 0; k < 3; ++k) { nd.lo[k] = INFINITY; nd.hi[k] = -INFINITY; }
+        for (U32 i = it.first; i < it.first + it.count; ++i) {
+            const U32 t = s.bvh.order[i];
+            for (int k = 0; k < 3; ++k) {
+                nd.lo[k] = std::min(nd.lo[k], blo[3 * t + k]);
+                nd.hi[k] = std::max(nd.hi[k], bhi[3 * t + k]);
+                clo[k] = std::min(clo[k], cen[3 * t + k]);
+                chi[k] = std::max(chi[k], cen[3 * t + k]);
+            }
+        }
+        if (it.count <= 4) {
+            nd.first = it.first;
+            nd.count = it.count;
+            s.bvh.nodes[it.node] = nd;
+            continue;
+        }
+        int axis = 0;
+        for (int k = 1; k < 3; ++k)
+            if (chi[k] - clo[k] > chi[axis] - clo[axis]) axis = k;
+        const U32 mid = it.first + it.count / 2;
+        std::nth_element(s.bvh.order.begin() + it.first, s.bvh.order.begin() + mid, s.bvh.order.begin() + it.first + it.count,
+                         [&](U32 x, U32 y) { return cen[3 * x + axis] < cen[3 * y + axis] || (cen[3 * x + axis] == cen[3 * y + axis] && x < y); });
+        const U32 left = U32(s.bvh.nodes.size());
+        s.bvh.nodes.push_back(Node{});
+        s.bvh.nodes.push_back(Node{});
+        nd.first = left;
+        nd.count = 0;
+        s.bvh.nodes[it.node] = nd;
+        work.push_back({left, it.first, mid - it.first});
+        work.push_back({left + 1, mid, it.first + it.count - mid});
+    }
+}
+
+inline bool boxHit(const Node& nd, V3 o, V3 inv, float tmin, float tmax) {
+    float t0 = tmin, t1 = tmax;
+    const float oo[3] = {o.x, o.y, o.z}, ii[3] = {inv.x, inv.y, inv.z};
+    for (int k = 0; k < 3; ++k) {
+        float a = (nd.lo[k] - oo[k]) * ii[k], b = (nd.hi[k] - oo[k]) * ii[k];
+        if (a > b) std::swap(a, b);
+        a -= std::fabs(a) * 4e-7f;  // widened by 2 gamma(3) each way: the slab test stays conservative
+        b += std::fabs(b) * 4e-7f;
+        t0 = a > t0 ? a : t0;  // NaN (0 * inf) keeps the bound
+        t1 = b < t1 ? b : t1;
+    }
+    return t0 <= t1;
+}
+
+// Closest hit on [tmin, tmax]: the nearest t, then the lowest triangle index. Returns ~0u on a miss.
+U32 closest(const Scene& s, V3 o, V3 d, float tmin, float tmax, float& tBest) {
+    const TriTest sh = shear(d);
+    const V3 inv{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    U32 best = ~0u;
+    tBest = tmax;
+    U32 stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+        const Node& nd = s.bvh.nodes[stack[--sp]];
+        if (!boxHit(nd, o, inv, tmin, tBest)) continue;
+        if (nd.count) {
+            for (U32 i = nd.first; i < nd.first + nd.count; ++i) {
+                const U32 t = s.bvh.order[i];
+                float th;
+                if (!triHit(sh, o, s.vertex(s.tris[3 * t]), s.vertex(s.tris[3 * t + 1]), s.vertex(s.tris[3 * t + 2]), tmin, tBest, th)) continue;
+                if (th < tBest || (th == tBest && t < best)) {
+                    tBest = th;
+                    best = t;
+                }
+            }
+        } else {
+            stack[sp++] = nd.first;
+            stack[sp++] = nd.first + 1;
+        }
+    }
+    return best;
+}
+bool occluded(const Scene& s, V3 o, V3 d, float tmin, float tmax) {
+    const TriTest sh = shear(d);
+    const V3 inv{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    U32 stack[128];
+    int sp = 0;
+    stack[sp++] = 0;
+    while (sp) {
+        const Node& nd = s.bvh.nodes[stack[--sp]];
+        if (!boxHit(nd, o, inv, tmin, tmax)) continue;
+        if (nd.count) {
+            for (U32 i = nd.first; i < nd.first + nd.count; ++i) {
+                const U32 t = s.bvh.order[i];
+                float th;
+                if (triHit(sh, o, s.vertex(s.tris[3 * t]), s.vertex(s.tris[3 * t + 1]), s.vertex(s.tris[3 * t + 2]), tmin, tmax, th)) return true;
+            }
+        } else {
+            stack[sp++] = nd.first;
+            stack[sp++] = nd.first + 1;
+        }
+    }
+    return false;
+}
+
+// ---- the Backend concept (async_integrator.h:52-57), after CpuBackend ----
+struct NoTextures {  // shadeMaterial's texture source: no maps are admitted, so nothing is ever looked up
+    unsigned lookup(unsigned, xi::tex::Binding, const xi::tex::Footprint&, V3&) const { return xi::tex::Invalid; }
+};
+
+struct Counts {
+    uint64_t trace = 0, nee = 0, bsdf = 0, held = 0;
+};
+
+struct OracleBackend {
+    const Scene& s;
+    Counts* counts;
+    struct Scratch {
+        xi::shade::Bsdf bsdf;
+        xi::async::paths::Pending pending[xi::async::paths::MaxPending];
+    };
+    static Scratch& scratch() {
+        static thread_local std::unique_ptr<Scratch> p;
+        if (!p) p = std::make_unique<Scratch>();
+        return *p;
+    }
+    // Members the reference integrator reads directly (subsurface exits' light set, the sample's time, the
+    // shadow ray's receiver): unused by the admitted scenes, kept at CpuBackend's initial values.
+    U32 exitLightSet = ~0u, shadowLight = ~0u, shadowReceiver = ~0u;
+    float time = 0.0f;
+    void setTime(float t) { time = t; }
+    xi::resume::Hit trace(const xi::surface::Ray& ray) const {
+        ++counts->trace;
+        xi::resume::Hit out;
+        float t;
+        const U32 tri = closest(s, ray.origin, ray.direction, ray.nearT, ray.farT, t);
+        if (tri == ~0u) return out;
+        out.geom = s.triGeom[tri];
+        out.prim = tri - s.meshFirst[out.geom];
+        out.t = t;
+        if (!xi::resume::geometryHit(out, ray, s.vertex(s.tris[3 * tri]), s.vertex(s.tris[3 * tri + 1]), s.vertex(s.tris[3 * tri + 2])))
+            out.normal = {};
+        return out;
+    }
+    bool visible(V3 o, V3 d) const { return visible(o, d, INFINITY); }
+    bool visible(V3 o, V3 d, float distance) const { return visible(o, d, 0.0f, distance); }
+    bool visible(V3 o, V3 d, float near, float distance) const { return !occluded(s, o, d, near, distance); }
+    void countRay(U32 kind) const {
+        if (kind == xi::async::paths::RayCountNee) ++counts->nee;
+        else if (kind == xi::async::paths::RayCountBsdf) ++counts->bsdf;
+        else ++counts->held;
+    }
+    bool deferred() const { return false; }
+    bool textureMissed() const { return false; }
+    xi::shade::Bsdf& bsdf() const { return scratch().bsdf; }
+    xi::async::paths::Pending* pending() const { return scratch().pending; }
+    const xi::lights::Light& light(U32 i) const { return s.lights[i]; }
+    U32 lightSet(U32) const { return 0; }
+    bool inSet(U32, U32 i) const { return i < s.lights.size(); }
+    bool inLobeSet(U32 set, U32) const { return set == ~0u; }
+    const xi::lights::TreeNode* treeNodes() const { return nullptr; }
+    int treeRoot(U32) const { return -1; }
+    void shadowFor(U32, U32) {}
+    bool castsShadow(U32, bool) const { return true; }
+    const xi::volume::Shader* volumes() const { return nullptr; }
+    xi::volume::Grids volumeGrids() const { return xi::volume::Grids{}; }
+    U32 volumeCrossings(V3, V3, float, xi::volume::Crossing*, U32, U32) const { return 0; }
+    xi::volume::Regions emissiveRegions() const { return xi::volume::Regions{nullptr, 0, nullptr}; }
+    const xi::aov::Tables& aovs() const {
+        static const xi::aov::Tables none{};
+        return none;
+    }
+    int geomLabel(U32) const { return -1; }
+    const float* walkSequences() const { return nullptr; }
+    const xi::lights::Filter* filters() const { return nullptr; }
+    const xi::lights::FilterList* filterList(U32, U32) const { return nullptr; }
+    float filterVdb(U32, U32, V3) const { return 1.0f; }
+    V3 filterMap(U32, U32, float, float) const { return V3{1, 1, 1}; }
+    U32 materialId(U32 geom) const { return geom < s.records.size() ? s.records[geom].offset : ~0u; }
+    xi::resume::Hit traceMaterial(xi::surface::Ray ray, U32 material) const {
+        for (int k = 0; k < 64; ++k) {
+            const xi::resume::Hit h = trace(ray);
+            if (h.geom == ~0u || materialId(h.geom) == material) return h;
+            ray.nearT = h.t + fmaxf(1e-6f, h.t * 1e-6f);
+            if (!(ray.nearT < ray.farT)) break;
+        }
+        return xi::resume::Hit{};
+    }
+    bool stateOf(const xi::resume::Hit& h, const xi::surface::Ray& ray, xi::shade::State& st) const {
+        const U32 tri = s.meshFirst[h.geom] + h.prim;
+        const U32 ia = s.tris[3 * tri], ib = s.tris[3 * tri + 1], ic = s.tris[3 * tri + 2];
+        xi::shade::MeshAttributes attributes;  // no normals, no uvs: the geometric normal and the default st
+        if (!xi::shade::hitState(attributes, h.prim, ia, ib, ic, s.vertex(ia), s.vertex(ib), s.vertex(ic), h.u, h.v, h.point,
+                                 ray.direction, st))
+            return false;
+        st.geom = h.geom;
+        return true;
+    }
+    bool surfaceState(const xi::resume::Hit& h, const xi::surface::Ray& ray, xi::shade::State& st) const { return stateOf(h, ray, st); }
+    unsigned presenceAt(const xi::resume::Hit&, const xi::surface::Ray&, float& presence) const {
+        presence = 1.0f;
+        return xi::tex::Ready;
+    }
+    unsigned shade(const xi::resume::Hit& h, const xi::surface::Ray& ray, xi::shade::State& st, xi::shade::Bsdf& bsdf, float& presence) const {
+        if (!stateOf(h, ray, st)) return xi::tex::Invalid;
+        if (h.geom >= s.records.size()) return xi::tex::Invalid;
+        const NoTextures textures;
+        return xi::shade::shadeMaterial(s.records[h.geom], s.pool.data(), st, textures, bsdf, presence, nullptr, nullptr);
+    }
+};
+
+xi::lights::Light toLight(const x2_light& x, U32 index) {
+    xi::lights::Light l;
+    std::memset(&l, 0, sizeof(l));
+    l.type = x.type == X2_LIGHT_ENV ? xi::lights::Env : xi::lights::Rect;
+    l.sidedness = x.sidedness;
+    l.index = index;
+    l.radiance = V3{x.radiance[0], x.radiance[1], x.radiance[2]};
+    l.position = V3{x.position[0], x.position[1], x.position[2]};
+    l.direction = V3{x.direction[0], x.direction[1], x.direction[2]};
+    for (int i = 0; i < 3; ++i) {
+        l.local2Render[i] = V3{x.local2render[i][0], x.local2render[i][1], x.local2render[i][2]};
+        l.render2Local[i] = V3{x.render2local[i][0], x.render2local[i][1], x.render2local[i][2]};
+        l.render2LocalRot[i] = V3{x.render2local_rot[i][0], x.render2local_rot[i][1], x.render2local_rot[i][2]};
+    }
+    l.scale = x.scale;
+    l.invArea = x.inv_area;
+    l.planeOffset = x.plane_offset;
+    l.halfWidth = x.half_width;
+    l.halfHeight = x.half_height;
+    l.image = nullptr;
+    l.visibleInCamera = x.visible_in_camera;
+    l.hemispherical = x.hemispherical;
+    l.fallback = V3{1, 1, 1};
+    l.spread = 1.0f;
+    l.mesh = nullptr;
+    l.lpeLabel = -1;
+    l.ref = nullptr;
+    l.visibilityMask = x.visibility_mask;
+    return l;
+}
+
+xi::mixed::Config toConfig(const x2_config& x, const x2_camera& cam) {
+    xi::mixed::Config c{};
+    std::memset(c.camera.rasterToCamera.m, 0, sizeof(c.camera.rasterToCamera.m));
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) {
+            c.camera.rasterToCamera.m[i][j] = cam.raster_to_camera[i][j];
+            c.camera.cameraToRender.m[i][j] = cam.camera_to_render[i][j];
+        }
+    c.camera.nearClip = cam.near_clip;
+    c.camera.farClip = cam.far_clip;
+    c.camera.type = xi::surface::CameraPerspective;
+    c.sky = V3{0, 0, 0};
+    c.width = x.width;
+    c.height = x.height;
+    c.seed = x.seed;
+    c.meshes = 0;
+    c.filter = xi::surface::Filter(x.filter);
+    c.filterWidth = x.filter_width;
+    c.spp = x.spp;
+    c.sampling = x.sampling;
+    c.paths = 1;
+    c.lightCount = x.light_count;
+    c.bsdfSamples = x.bsdf_samples;
+    c.lightSamples = x.light_samples;
+    c.maxDepth = x.max_depth;
+    c.maxDiffuseDepth = x.max_diffuse_depth;
+    c.clampDepth = x.clamp_depth;
+    c.rrThreshold = x.rr_threshold;
+    c.clampValue = x.clamp_value;
+    c.maxGlossyDepth = x.max_glossy_depth;
+    c.maxMirrorDepth = x.max_mirror_depth;
+    c.maxHairDepth = x.max_hair_depth;
+    c.maxPresenceDepth = x.max_presence_depth;
+    c.shadowTerminatorFix = x.shadow_terminator_fix;
+    c.roughnessClamping = x.roughness_clamping;
+    c.transparencyThreshold = x.transparency_threshold;
+    c.visibleLights = x.visible_lights;
+    c.presenceThreshold = x.presence_threshold;
+    c.presenceQuality = x.presence_quality;
+    c.shadowReuse = x.shadow_reuse;
+    return c;
+}
+
+struct Handle {
+    Scene scene;
+    Counts counts;
+};
+
+}  // namespace
+
+extern "C" {
+
+// The scene and config as the engine takes them (x2.h), built into the reference's records.
+void* x2ref_open(const x2_scene_desc* d, const x2_config* cfg) {
+    if (!d || !cfg) return nullptr;
+    auto* h = new Handle();
+    Scene& s = h->scene;
+    s.vertices.resize(d->vertex_count);
+    for (U32 i = 0; i < d->vertex_count; ++i) s.vertices[i] = V3{d->vertices[3 * i], d->vertices[3 * i + 1], d->vertices[3 * i + 2]};
+    s.tris.assign(d->triangles, d->triangles + size_t(d->triangle_count) * 3);
+    s.meshFirst.assign(d->mesh_first, d->mesh_first + d->mesh_count + 1);
+    s.triGeom.resize(d->triangle_count);
+    for (U32 m = 0; m < d->mesh_count; ++m)
+        for (U32 t = d->mesh_first[m]; t < d->mesh_first[m + 1]; ++t) s.triGeom[t] = m;
+    // One UsdPreviewSurface record a mesh (its material's parameters in the pool).
+    for (U32 m = 0; m < d->mesh_count; ++m) {
+        const x2_material& x = d->materials[d->mesh_material[m]];
+        xi::shade::UsdPreviewSurfaceParams p{};
+        p.diffuseColor = V3{x.diffuse[0], x.diffuse[1], x.diffuse[2]};
+        p.emissiveColor = V3{x.emission[0], x.emission[1], x.emission[2]};
+        p.specularColor = V3{x.specular[0], x.specular[1], x.specular[2]};
+        p.useSpecularWorkflow = 1.0f;
+        p.metallic = 0.0f;
+        p.roughness = x.roughness;
+        p.clearcoat = 0.0f;
+        p.clearcoatRoughness = 0.01f;
+        p.opacity = 1.0f;
+        p.opacityThreshold = 0.0f;
+        p.ior = 1.5f;
+        p.normal = V3{0, 0, 1};
+        xi::shade::MaterialRecord r;
+        r.kind = xi::shade::MatUsdPreviewSurface;
+        r.flags = x.kind == X2_MAT_GGX ? U32(xi::shade::MatModoUsdSpecular) : 0u;
+        r.offset = U32(s.pool.size());
+        r.count = xi::shade::UsdPreviewSurfaceFloats;
+        const float* f = reinterpret_cast<const float*>(&p);
+        s.pool.insert(s.pool.end(), f, f + xi::shade::UsdPreviewSurfaceFloats);
+        s.records.push_back(r);
+    }
+    for (U32 i = 0; i < d->light_count; ++i) s.lights.push_back(toLight(d->lights[i], i));
+    s.config = toConfig(*cfg, d->camera);
+    buildBvh(s);
+    return h;
+}
+
+void x2ref_close(void* p) { delete static_cast<Handle*>(p); }
+
+// integrate() for n (pixel, index) pairs on `threads` host threads.
+int x2ref_integrate(void* p, const uint32_t* pairs, uint64_t n, double* rgba, uint32_t* status, int threads) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h || (!pairs && n)) return X2_EINVAL;
+    std::atomic<uint64_t> next{0};
+    std::vector<Counts> per(std::max(threads, 1));
+    auto work = [&](int w) {
+        OracleBackend backend{h->scene, &per[w]};
+        for (;;) {
+            const uint64_t i = next.fetch_add(1);
+            if (i >= n) break;
+            xi::async::Radiance r;
+            const auto st = xi::async::integratePaths(h->scene.config, pairs[2 * i], pairs[2 * i + 1], backend, r);
+            rgba[4 * i] = r.rgb[0];
+            rgba[4 * i + 1] = r.rgb[1];
+            rgba[4 * i + 2] = r.rgb[2];
+            rgba[4 * i + 3] = r.alpha;
+            status[i] = U32(st);
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < threads; ++w) pool.emplace_back(work, w);
+    work(0);
+    for (auto& t : pool) t.join();
+    for (const auto& c : per) {
+        h->counts.trace += c.trace;
+        h->counts.nee += c.nee;
+        h->counts.bsdf += c.bsdf;
+        h->counts.held += c.held;
+    }
+    return X2_OK;
+}
+
+// renderChunk (async_cpu.h:1584-1667): workers claim 8x8 tiles and render their samples [first, first+count)
+// into an FP64 film: sums (4 a pixel), odd-index sums and counts. Ray counts in rays[4] (trace, nee, bsdf, held).
+int x2ref_render(void* p, uint32_t first, uint32_t count, int threads, double* sums, double* odd, uint32_t* counts, uint64_t* rays) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h) return X2_EINVAL;
+    const auto& c = h->scene.config;
+    const U32 tilesX = (c.width + 7) / 8, tilesY = (c.height + 7) / 8, tiles = tilesX * tilesY;
+    std::atomic<U32> next{0};
+    std::vector<Counts> per(std::max(threads, 1));
+    std::atomic<uint64_t> errors{0};
+    auto work = [&](int w) {
+        OracleBackend backend{h->scene, &per[w]};
+        for (;;) {
+            const U32 tile = next.fetch_add(1);
+            if (tile >= tiles) break;
+            for (U32 s = 0; s < count; ++s)
+                for (U32 pos = 0; pos < 64; ++pos) {
+                    const U32 pixel = xi::async::tilePixel(tile, pos, c.width, c.height);
+                    if (pixel == ~0u) continue;
+                    const U32 index = first + s;
+                    xi::async::Radiance r;
+                    const auto st = xi::async::integratePaths(c, pixel, index, backend, r);
+                    if (st == xi::async::SampleStatus::Done) {
+                        // Each tile is one worker's: no two threads share a pixel.
+                        for (int k = 0; k < 3; ++k) sums[4 * size_t(pixel) + k] += r.rgb[k];
+                        sums[4 * size_t(pixel) + 3] += r.alpha;
+                        if (odd && (index & 1)) {
+                            for (int k = 0; k < 3; ++k) odd[4 * size_t(pixel) + k] += r.rgb[k];
+                            odd[4 * size_t(pixel) + 3] += r.alpha;
+                        }
+                        ++counts[pixel];
+                    } else if (st == xi::async::SampleStatus::Skip) {
+                        ++counts[pixel];
+                    } else {
+                        ++errors;
+                    }
+                }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < threads; ++w) pool.emplace_back(work, w);
+    work(0);
+    for (auto& t : pool) t.join();
+    Counts total;
+    for (const auto& k : per) {
+        total.trace += k.trace;
+        total.nee += k.nee;
+        total.bsdf += k.bsdf;
+        total.held += k.held;
+    }
+    if (rays) {
+        rays[0] = total.trace;
+        rays[1] = total.nee;
+        rays[2] = total.bsdf;
+        rays[3] = total.held;
+    }
+    return errors ? X2_EDEVICE : X2_OK;
+}
+
+// renderChunk over a list of tiles only (a bounded sample of a frame for the CPU baseline): each tile's 64 pixels
+// times samples [first, first+count); returns the samples rendered in *samples and ray counts in rays[4].
+int x2ref_render_tiles(void* p, const uint32_t* tiles, uint32_t ntiles, uint32_t first, uint32_t count, int threads, uint64_t* samples,
+                       uint64_t* rays) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h || !tiles) return X2_EINVAL;
+    const auto& c = h->scene.config;
+    std::atomic<U32> next{0};
+    std::atomic<uint64_t> done{0}, errors{0};
+    std::vector<Counts> per(std::max(threads, 1));
+    auto work = [&](int w) {
+        OracleBackend backend{h->scene, &per[w]};
+        for (;;) {
+            const U32 k = next.fetch_add(1);
+            if (k >= ntiles) break;
+            for (U32 s = 0; s < count; ++s)
+                for (U32 pos = 0; pos < 64; ++pos) {
+                    const U32 pixel = xi::async::tilePixel(tiles[k], pos, c.width, c.height);
+                    if (pixel == ~0u) continue;
+                    xi::async::Radiance r;
+                    const auto st = xi::async::integratePaths(c, pixel, first + s, backend, r);
+                    if (st == xi::async::SampleStatus::Done) ++done;
+                    else ++errors;
+                }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < threads; ++w) pool.emplace_back(work, w);
+    work(0);
+    for (auto& t : pool) t.join();
+    Counts total;
+    for (const auto& k : per) {
+        total.trace += k.trace;
+        total.nee += k.nee;
+        total.bsdf += k.bsdf;
+        total.held += k.held;
+    }
+    if (samples) *samples = done;
+    if (rays) {
+        rays[0] = total.trace;
+        rays[1] = total.nee;
+        rays[2] = total.bsdf;
+        rays[3] = total.held;
+    }
+    return errors ? X2_EDEVICE : X2_OK;
+}
+
+// Traversal parity: closest hit (triangle, t) or ~0u, and occlusion, for n rays (origin, direction, near, far).
+int x2ref_trace(void* p, const float* rays, uint64_t n, uint32_t* tri, float* t, uint32_t* occl) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h) return X2_EINVAL;
+    for (uint64_t i = 0; i < n; ++i) {
+        const float* r = rays + 8 * i;
+        const V3 o{r[0], r[1], r[2]}, d{r[3], r[4], r[5]};
+        float th;
+        tri[i] = closest(h->scene, o, d, r[6], r[7], th);
+        t[i] = tri[i] == ~0u ? 0.0f : th;
+        occl[i] = occluded(h->scene, o, d, r[6], r[7]) ? 1u : 0u;
+    }
+    return X2_OK;
+}
+
+// sample::samplingWord (sample_stream.h:127-144), the reference's own.
+int x2ref_sample_words(const x2_identity* ids, const uint32_t* dims, uint64_t n, uint32_t policy, uint32_t* out) {
+    for (uint64_t i = 0; i < n; ++i) {
+        const xi::sample::Identity id{ids[i].pixel, ids[i].index, ids[i].stream, ids[i].branch};
+        out[i] = xi::sample::samplingWord(id, dims[i], policy);
+    }
+    return X2_OK;
+}
+
+// paths::childBranch (async_integrator.h:281-287), the reference's own.
+uint64_t x2ref_child_branch(uint64_t parent, uint32_t a, uint32_t b) { return xi::async::paths::childBranch(parent, a, b); }
+
+}  // extern "C"

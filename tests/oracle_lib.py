@@ -1,0 +1,154 @@
+"""Loaders for the oracle (test infrastructure only): the plain-C sampler restatement (oracle/liboracle_sampler.so)
+and the reference integrator compiled from the reference's own sources (oracle/_ref/libx2ref.so).
+"""
+import ctypes as C
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "xpu2-foundation_b200"))
+import x2  # noqa: E402
+
+SAMPLER = os.path.join(ROOT, "oracle", "liboracle_sampler.so")
+REFERENCE = os.path.join(ROOT, "oracle", "_ref", "libx2ref.so")
+
+
+def sampler():
+    lib = C.CDLL(SAMPLER)
+    u32, u64, vp = C.c_uint32, C.c_uint64, C.c_void_p
+    lib.oracle_sampling_words.argtypes = [vp, vp, u64, u32, vp]
+    lib.oracle_philox.argtypes = [vp, vp, u64, vp]
+    lib.oracle_sobol.argtypes = [u32, u32]
+    lib.oracle_sobol.restype = u32
+    lib.oracle_direction.argtypes = [u32, u32]
+    lib.oracle_direction.restype = u32
+    lib.oracle_child_branch.argtypes = [u64, u32, u32]
+    lib.oracle_child_branch.restype = u64
+    lib.oracle_unit.argtypes = [u32]
+    lib.oracle_unit.restype = C.c_float
+    lib.oracle_word.argtypes = [u32, u64, u64, u64, u32]
+    lib.oracle_word.restype = u32
+    return lib
+
+
+def sampling_words(lib, ids, dims, policy):
+    ids = np.ascontiguousarray(ids, dtype=x2.IDENTITY_DTYPE)
+    dims = np.ascontiguousarray(dims, dtype=np.uint32)
+    out = np.empty(len(dims), np.uint32)
+    lib.oracle_sampling_words(ids.ctypes.data, dims.ctypes.data, len(dims), policy, out.ctypes.data)
+    return out
+
+
+def have_reference():
+    return os.path.exists(REFERENCE)
+
+
+class Reference:
+    """The reference's integratePaths (async_integrator.h:1986) over a scene, on host threads."""
+
+    def __init__(self, synthetic, config=None):
+        self.lib = lib = C.CDLL(REFERENCE)
+        vp, u32, u64, i32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
+        lib.x2ref_open.argtypes = [C.POINTER(x2.SceneDesc), C.POINTER(x2.Config)]
+        lib.x2ref_open.restype = vp
+        lib.x2ref_close.argtypes = [vp]
+        lib.x2ref_integrate.argtypes = [vp, vp, u64, vp, vp, i32]
+        lib.x2ref_integrate.restype = i32
+        lib.x2ref_render.argtypes = [vp, u32, u32, i32, vp, vp, vp, vp]
+        lib.x2ref_render.restype = i32
+        lib.x2ref_render_tiles.argtypes = [vp, vp, u32, u32, u32, i32, vp, vp]
+        lib.x2ref_render_tiles.restype = i32
+        lib.x2ref_trace.argtypes = [vp, vp, u64, vp, vp, vp]
+        lib.x2ref_trace.restype = i32
+        lib.x2ref_sample_words.argtypes = [vp, vp, u64, u32, vp]
+        lib.x2ref_sample_words.restype = i32
+        lib.x2ref_child_branch.argtypes = [u64, u32, u32]
+        lib.x2ref_child_branch.restype = u64
+        cfg = synthetic.config if config is None else config
+        self.config = cfg
+        self.h = lib.x2ref_open(synthetic.desc_ptr, C.byref(cfg))
+        if not self.h:
+            raise RuntimeError("x2ref_open failed")
+
+    def close(self):
+        if self.h:
+            self.lib.x2ref_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def integrate(self, pixels, indices, threads=None):
+        pairs = np.ascontiguousarray(np.stack([np.asarray(pixels, np.uint32), np.asarray(indices, np.uint32)], 1))
+        n = len(pairs)
+        rgba = np.empty((n, 4), np.float64)
+        status = np.empty(n, np.uint32)
+        rc = self.lib.x2ref_integrate(self.h, pairs.ctypes.data, n, rgba.ctypes.data, status.ctypes.data, threads or os.cpu_count())
+        assert rc == 0
+        return rgba, status
+
+    def render(self, first, count, threads=None):
+        p = self.config.width * self.config.height
+        sums = np.zeros((p, 4))
+        odd = np.zeros((p, 4))
+        counts = np.zeros(p, np.uint32)
+        rays = np.zeros(4, np.uint64)
+        rc = self.lib.x2ref_render(self.h, first, count, threads or os.cpu_count(), sums.ctypes.data, odd.ctypes.data, counts.ctypes.data,
+                                   rays.ctypes.data)
+        return rc, sums, odd, counts, rays
+
+    def render_tiles(self, tiles, first, count, threads=None):
+        """A bounded sample of a frame: the given tiles' pixels x samples [first, first+count). Returns (rc,
+        samples rendered, ray counts [trace, nee, bsdf, held])."""
+        tiles = np.ascontiguousarray(tiles, np.uint32)
+        samples = np.zeros(1, np.uint64)
+        rays = np.zeros(4, np.uint64)
+        rc = self.lib.x2ref_render_tiles(self.h, tiles.ctypes.data, len(tiles), first, count, threads or os.cpu_count(), samples.ctypes.data,
+                                         rays.ctypes.data)
+        return rc, int(samples[0]), rays
+
+    def trace(self, rays):
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = len(rays)
+        tri = np.empty(n, np.uint32)
+        t = np.empty(n, np.float32)
+        occ = np.empty(n, np.uint32)
+        self.lib.x2ref_trace(self.h, rays.ctypes.data, n, tri.ctypes.data, t.ctypes.data, occ.ctypes.data)
+        return tri, t, occ
+
+
+def reference_sampling_words(ids, dims, policy):
+    lib = C.CDLL(REFERENCE)
+    lib.x2ref_sample_words.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_uint32, C.c_void_p]
+    ids = np.ascontiguousarray(ids, dtype=x2.IDENTITY_DTYPE)
+    dims = np.ascontiguousarray(dims, dtype=np.uint32)
+    out = np.empty(len(dims), np.uint32)
+    lib.x2ref_sample_words(ids.ctypes.data, dims.ctypes.data, len(dims), policy, out.ctypes.data)
+    return out
+
+
+def random_identities(n, seed):
+    """Seeded identities exercising every field: 32-bit pixels, 64-bit indices (high bits too), streams, branches."""
+    r = np.random.default_rng(seed)
+    ids = np.zeros(n, x2.IDENTITY_DTYPE)
+    ids["pixel"] = r.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    idx = r.integers(0, 2**63, n, dtype=np.uint64)
+    small = r.random(n) < 0.5
+    idx[small] = r.integers(0, 4096, small.sum(), dtype=np.uint64)
+    ids["index"] = idx
+    ids["stream"] = r.integers(0, 2**63, n, dtype=np.uint64)
+    ids["branch"] = r.integers(0, 2**63, n, dtype=np.uint64)
+    return ids
+
+
+def sample_pairs(config, n, seed):
+    """n seeded (pixel, index) samples of a frame."""
+    r = np.random.default_rng(seed)
+    pixels = r.integers(0, config.width * config.height, n).astype(np.uint32)
+    indices = r.integers(0, config.spp, n).astype(np.uint32)
+    return pixels, indices

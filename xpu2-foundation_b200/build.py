@@ -1,0 +1,62 @@
+"""Builds libx2.so in-tree for sm_100a (nvcc), next to the Python layer in x2/.
+
+The CUDA sources are compiled without floating-point contraction (-fmad=false): the path arithmetic is
+written to round exactly as the reference's CPU lane (-ffp-contract=off) does, and the parity tests rely on it.
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT = os.path.join(HERE, "x2", "libx2.so")
+BUILD = os.path.join(HERE, "_build")
+CU = ["api.cu", "render.cu", "bvh_build.cu"]
+CPP = ["scene_gen.cpp"]
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+         "-Xptxas", "-warn-spills"]
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(r.stdout + r.stderr)
+        raise RuntimeError("build failed: " + " ".join(cmd))
+    return r.stdout + r.stderr
+
+
+def _stale(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def build(verbose=False, force=False):
+    os.makedirs(BUILD, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    headers.append(os.path.join(HERE, "..", "include", "x2.h"))
+    objs = []
+    for f in CU:
+        src = os.path.join(CSRC, f)
+        obj = os.path.join(BUILD, f + ".o")
+        if force or _stale(obj, [src] + headers):
+            log = _run([NVCC] + ARCH + FLAGS + ["-rdc=false", "-c", src, "-o", obj] + (["-Xptxas", "-v"] if verbose else []))
+            if verbose:
+                sys.stdout.write(log)
+        objs.append(obj)
+    for f in CPP:
+        src = os.path.join(CSRC, f)
+        obj = os.path.join(BUILD, f + ".o")
+        if force or _stale(obj, [src] + headers):
+            _run(["g++", "-std=c++17", "-O2", "-fPIC", "-c", src, "-o", obj])
+        objs.append(obj)
+    if force or _stale(OUT, objs):
+        _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", OUT] + objs + ["-lcudart_static"])
+    return OUT
+
+
+if __name__ == "__main__":
+    print(build(verbose="-v" in sys.argv, force="-f" in sys.argv))

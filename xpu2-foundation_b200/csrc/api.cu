@@ -1,0 +1,814 @@
+// The C ABI (include/x2.h): context, scene upload and BVH build, the per-sample API and the lane API
+// (GpuLane's begin/launch/poll/downloadFilm, async_gpu.h:1372-1707). One CUDA stream a context; every device
+// wait is bounded (x2_wait, x2_synchronize poll events with a timeout instead of blocking).
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/x2.h"
+#include "engine.h"
+#include "render.h"
+
+namespace x2 {
+
+namespace {
+thread_local std::string g_error;
+}
+
+void setError(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_error = buf;
+}
+
+namespace {
+
+// Sobol direction numbers: dimension 0 van der Corput, 1..16 by the Bratley-Fox recurrence from Joe and Kuo's
+// primitive polynomials (degree s, coefficients a, initial m) for their dimensions 2..17.
+void sobolDirections(uint32_t out[17][32]) {
+    static const uint32_t s[16] = {1, 2, 3, 3, 4, 4, 5, 5, 5, 5, 5, 5, 6, 6, 6, 6};
+    static const uint32_t a[16] = {0, 1, 1, 2, 1, 4, 2, 4, 7, 11, 13, 14, 1, 13, 16, 19};
+    static const uint32_t m0[16][6] = {{1}, {1, 3}, {1, 3, 1}, {1, 1, 1}, {1, 1, 3, 3}, {1, 3, 5, 13}, {1, 1, 5, 5, 17},
+                                       {1, 1, 5, 5, 5}, {1, 1, 7, 11, 19}, {1, 1, 5, 1, 1}, {1, 1, 1, 3, 11}, {1, 3, 5, 5, 31},
+                                       {1, 3, 3, 9, 7, 49}, {1, 1, 1, 15, 21, 21}, {1, 3, 1, 13, 27, 49}, {1, 1, 1, 15, 7, 5}};
+    for (int i = 0; i < 32; ++i) out[0][i] = 1u << (31 - i);
+    for (int d = 0; d < 16; ++d) {
+        uint64_t m[32];
+        for (uint32_t i = 0; i < s[d]; ++i) m[i] = m0[d][i];
+        for (uint32_t i = s[d]; i < 32; ++i) {
+            uint64_t v = m[i - s[d]] ^ (m[i - s[d]] << s[d]);
+            for (uint32_t k = 1; k < s[d]; ++k)
+                if ((a[d] >> (s[d] - 1 - k)) & 1u) v ^= m[i - k] << k;
+            m[i] = v;
+        }
+        for (int i = 0; i < 32; ++i) out[d + 1][i] = uint32_t(m[i] << (31 - i));
+    }
+}
+
+#define CUDA_OR(expr, code)                                                                         \
+    do {                                                                                            \
+        cudaError_t e_ = (expr);                                                                    \
+        if (e_ != cudaSuccess) {                                                                    \
+            setError("%s:%d %s: %s", __FILE__, __LINE__, #expr, cudaGetErrorString(e_));            \
+            return code;                                                                            \
+        }                                                                                           \
+    } while (0)
+
+// Waits for an event with a deadline (no unbounded cudaEventSynchronize).
+int waitEvent(cudaEvent_t e, int timeoutMs) {
+    const auto until = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeoutMs < 0 ? 0 : timeoutMs);
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(e);
+        if (q == cudaSuccess) return X2_OK;
+        if (q != cudaErrorNotReady) {
+            setError("device error while waiting: %s", cudaGetErrorString(q));
+            return X2_ECUDA;
+        }
+        if (std::chrono::steady_clock::now() >= until) {
+            setError("wait timed out after %d ms", timeoutMs);
+            return X2_ETIMEOUT;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+constexpr int kSlots = 2;  // launches in flight, as GpuLane keeps (async_gpu.h:1425)
+
+struct Slot {
+    bool busy = false;
+    uint64_t seq = 0;
+    x2_chunk* chunks = nullptr;  // device
+    uint32_t chunkCap = 0;
+    unsigned long long* claimed = nullptr;
+    Counters* counters = nullptr;      // device
+    Counters* hostCounters = nullptr;  // pinned
+    cudaEvent_t begin = nullptr, end = nullptr, done = nullptr;  // done: the counters have reached the host
+};
+
+}  // namespace
+}  // namespace x2
+
+using namespace x2;
+
+struct x2_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int smCount = 0;
+    int renderBlocksPerSm = 0;
+};
+
+struct x2_scene {
+    x2_ctx* ctx = nullptr;
+    DeviceBvh bvh;
+    uint32_t* triMesh = nullptr;
+    uint32_t* meshFirst = nullptr;
+    uint32_t* meshMaterial = nullptr;
+    MaterialRec* materials = nullptr;
+    x2_light* lights = nullptr;
+    uint32_t* overflow = nullptr;
+    uint32_t lightCount = 0, triangleCount = 0;
+    x2_camera camera{};
+    x2_config config{};
+    bool configured = false;
+    float buildMs = 0.0f;
+    // film
+    double* sums = nullptr;
+    double* odd = nullptr;
+    uint32_t* counts = nullptr;
+    uint32_t filmPixels = 0, samplesPerChunk = 0;
+    bool adaptive = false;
+    // launches
+    Slot slots[kSlots];
+    uint64_t nextSeq = 1;
+    x2_chunk* staging = nullptr;  // pinned
+    uint32_t stagingCap = 0;
+    Counters total{};
+    // the per-sample API's scratch (device pairs/outputs for host callers)
+    Slot integrateSlot;
+    unsigned long long* auditWord = nullptr;
+    TraversalStats* stats = nullptr;  // device
+    bool counting = false;
+};
+
+namespace {
+
+SceneView viewOf(const x2_scene* s) {
+    SceneView v;
+    v.bvh = Bvh8{s->bvh.nodes, s->bvh.tris, s->bvh.nodeCount, s->bvh.triCount};
+    v.triMesh = s->triMesh;
+    v.meshFirst = s->meshFirst;
+    v.meshMaterial = s->meshMaterial;
+    v.materials = s->materials;
+    v.lights = s->lights;
+    v.camera = s->camera;
+    v.config = s->config;
+    v.overflow = s->overflow;
+    v.stats = s->counting ? s->stats : nullptr;
+    return v;
+}
+
+int ensureSlot(Slot& sl, uint32_t chunks) {
+    if (!sl.begin) {
+        CUDA_OR(cudaEventCreate(&sl.begin), X2_ECUDA);
+        CUDA_OR(cudaEventCreate(&sl.end), X2_ECUDA);
+        CUDA_OR(cudaEventCreateWithFlags(&sl.done, cudaEventDisableTiming), X2_ECUDA);
+        CUDA_OR(cudaMalloc(&sl.claimed, sizeof(unsigned long long)), X2_ENOMEM);
+        CUDA_OR(cudaMalloc(&sl.counters, sizeof(Counters)), X2_ENOMEM);
+        CUDA_OR(cudaMallocHost(&sl.hostCounters, sizeof(Counters)), X2_ENOMEM);
+        std::memset(sl.hostCounters, 0, sizeof(Counters));
+    }
+    if (chunks > sl.chunkCap) {
+        if (sl.chunks) cudaFree(sl.chunks);
+        sl.chunks = nullptr;
+        const uint32_t cap = chunks < 1024 ? 1024 : chunks;
+        CUDA_OR(cudaMalloc(&sl.chunks, sizeof(x2_chunk) * cap), X2_ENOMEM);
+        sl.chunkCap = cap;
+    }
+    return X2_OK;
+}
+void freeSlot(Slot& sl) {
+    if (sl.begin) cudaEventDestroy(sl.begin);
+    if (sl.end) cudaEventDestroy(sl.end);
+    if (sl.done) cudaEventDestroy(sl.done);
+    if (sl.claimed) cudaFree(sl.claimed);
+    if (sl.counters) cudaFree(sl.counters);
+    if (sl.hostCounters) cudaFreeHost(sl.hostCounters);
+    if (sl.chunks) cudaFree(sl.chunks);
+    sl = Slot{};
+}
+void accumulate(Counters& t, const Counters& c) {
+    t.trace += c.trace;
+    t.nee += c.nee;
+    t.bsdf += c.bsdf;
+    t.held += c.held;
+    t.samples += c.samples;
+    t.errors += c.errors;
+}
+
+int checkDevice(x2_ctx* ctx) {
+    if (!ctx) {
+        setError("null context");
+        return X2_EINVAL;
+    }
+    CUDA_OR(cudaSetDevice(ctx->device), X2_ECUDA);
+    return X2_OK;
+}
+
+// Collects a finished slot (its end event has fired).
+void retire(x2_scene* s, Slot& sl, x2_completion* out) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, sl.begin, sl.end);
+    accumulate(s->total, *sl.hostCounters);
+    if (out) {
+        out->launch = sl.seq;
+        out->samples = sl.hostCounters->samples;
+        out->errors = sl.hostCounters->errors;
+        out->milliseconds = ms;
+        out->pad = 0;
+    }
+    sl.busy = false;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* x2_version(void) { return "x2-b200 0.1 (sm_100a)"; }
+const char* x2_last_error(void) { return g_error.c_str(); }
+
+int x2_open(int device, x2_ctx** out) {
+    if (!out) return X2_EINVAL;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+        setError("no CUDA device");
+        return X2_ENODEV;
+    }
+    if (device < 0 || device >= count) {
+        setError("device %d out of range (%d devices)", device, count);
+        return X2_EINVAL;
+    }
+    CUDA_OR(cudaSetDevice(device), X2_ECUDA);
+    auto* ctx = new x2_ctx();
+    ctx->device = device;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        setError("stream creation failed");
+        delete ctx;
+        return X2_ECUDA;
+    }
+    uint32_t dirs[17][32];
+    sobolDirections(dirs);
+    if (uploadSobol(dirs) != cudaSuccess) {
+        setError("sobol table upload failed");
+        cudaStreamDestroy(ctx->stream);
+        delete ctx;
+        return X2_ECUDA;
+    }
+    cudaDeviceGetAttribute(&ctx->smCount, cudaDevAttrMultiProcessorCount, device);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&ctx->renderBlocksPerSm, renderChunks, kRenderBlock, 0);
+    if (ctx->renderBlocksPerSm < 1) ctx->renderBlocksPerSm = 1;
+    *out = ctx;
+    return X2_OK;
+}
+
+int x2_close(x2_ctx* ctx) {
+    if (!ctx) return X2_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return X2_OK;
+}
+
+int x2_synchronize(x2_ctx* ctx, int timeoutMs) {
+    if (int rc = checkDevice(ctx)) return rc;
+    cudaEvent_t e;
+    CUDA_OR(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), X2_ECUDA);
+    cudaEventRecord(e, ctx->stream);
+    const int rc = waitEvent(e, timeoutMs);
+    cudaEventDestroy(e);
+    return rc;
+}
+
+int x2_sample_words_device(x2_ctx* ctx, const x2_identity* ids, const uint32_t* dims, uint64_t n, uint32_t policy, uint32_t* out) {
+    if (int rc = checkDevice(ctx)) return rc;
+    if (!n) return X2_OK;
+    if (!ids || !dims || !out) {
+        setError("null array");
+        return X2_EINVAL;
+    }
+    const int blocks = ctx->smCount * 8;
+    sampleWords<<<blocks, 256, 0, ctx->stream>>>(ids, dims, n, policy, out);
+    CUDA_OR(cudaGetLastError(), X2_ECUDA);
+    return X2_OK;
+}
+
+int x2_sample_words(x2_ctx* ctx, const x2_identity* ids, const uint32_t* dims, uint64_t n, uint32_t policy, uint32_t* out) {
+    if (int rc = checkDevice(ctx)) return rc;
+    if (!n) return X2_OK;
+    if (!ids || !dims || !out) {
+        setError("null array");
+        return X2_EINVAL;
+    }
+    x2_identity* dIds = nullptr;
+    uint32_t *dDims = nullptr, *dOut = nullptr;
+    CUDA_OR(cudaMallocAsync(&dIds, sizeof(x2_identity) * n, ctx->stream), X2_ENOMEM);
+    CUDA_OR(cudaMallocAsync(&dDims, sizeof(uint32_t) * n, ctx->stream), X2_ENOMEM);
+    CUDA_OR(cudaMallocAsync(&dOut, sizeof(uint32_t) * n, ctx->stream), X2_ENOMEM);
+    cudaMemcpyAsync(dIds, ids, sizeof(x2_identity) * n, cudaMemcpyHostToDevice, ctx->stream);
+    cudaMemcpyAsync(dDims, dims, sizeof(uint32_t) * n, cudaMemcpyHostToDevice, ctx->stream);
+    int rc = x2_sample_words_device(ctx, dIds, dDims, n, policy, dOut);
+    if (rc == X2_OK) cudaMemcpyAsync(out, dOut, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, ctx->stream);
+    cudaFreeAsync(dIds, ctx->stream);
+    cudaFreeAsync(dDims, ctx->stream);
+    cudaFreeAsync(dOut, ctx->stream);
+    const int w = x2_synchronize(ctx, 600000);
+    return rc ? rc : w;
+}
+
+int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
+    if (int rc = checkDevice(ctx)) return rc;
+    if (!d || !out || !d->vertices || !d->triangles || !d->mesh_first || !d->mesh_material || !d->materials ||
+        (d->light_count && !d->lights) || d->triangle_count == 0 || d->mesh_count == 0) {
+        setError("incomplete scene description");
+        return X2_EINVAL;
+    }
+    // Admission (as the reference's plan admission rejects what its port does not carry).
+    for (uint32_t i = 0; i < d->material_count; ++i) {
+        const x2_material& m = d->materials[i];
+        if (m.kind != X2_MAT_LAMBERT && m.kind != X2_MAT_GGX) {
+            setError("material %u: unknown kind %u", i, m.kind);
+            return X2_EINVAL;
+        }
+        if (m.kind == X2_MAT_GGX) {
+            const bool specBlack = m.specular[0] <= 1e-6f && m.specular[1] <= 1e-6f && m.specular[2] <= 1e-6f;
+            const bool diffBlack = m.diffuse[0] <= 1e-6f && m.diffuse[1] <= 1e-6f && m.diffuse[2] <= 1e-6f;
+            if (!specBlack && !diffBlack) {
+                setError("material %u: a GGX lobe over a diffuse base is not admitted", i);
+                return X2_EINVAL;
+            }
+            if (!specBlack && !(m.roughness > 1e-6f)) {
+                setError("material %u: a mirror (roughness 0) is not admitted", i);
+                return X2_EINVAL;
+            }
+        }
+    }
+    for (uint32_t i = 0; i < d->light_count; ++i) {
+        const x2_light& l = d->lights[i];
+        if ((l.type != X2_LIGHT_ENV && l.type != X2_LIGHT_RECT) || l.sidedness > X2_SIDE_TWO) {
+            setError("light %u: type %u / sidedness %u not admitted", i, l.type, l.sidedness);
+            return X2_EINVAL;
+        }
+    }
+    if (d->mesh_first[0] != 0 || d->mesh_first[d->mesh_count] != d->triangle_count) {
+        setError("mesh ranges do not cover the triangles");
+        return X2_EINVAL;
+    }
+    std::vector<uint32_t> triMesh(d->triangle_count);
+    for (uint32_t m = 0; m < d->mesh_count; ++m) {
+        if (d->mesh_first[m + 1] < d->mesh_first[m] || d->mesh_material[m] >= d->material_count) {
+            setError("mesh %u: bad range or material", m);
+            return X2_EINVAL;
+        }
+        for (uint32_t t = d->mesh_first[m]; t < d->mesh_first[m + 1]; ++t) triMesh[t] = m;
+    }
+    for (uint64_t i = 0; i < uint64_t(d->triangle_count) * 3; ++i)
+        if (d->triangles[i] >= d->vertex_count) {
+            setError("triangle %llu: vertex index out of range", (unsigned long long)(i / 3));
+            return X2_EINVAL;
+        }
+    auto* s = new x2_scene();
+    s->ctx = ctx;
+    s->camera = d->camera;
+    s->lightCount = d->light_count;
+    s->triangleCount = d->triangle_count;
+    cudaStream_t st = ctx->stream;
+    float* dVerts = nullptr;
+    uint32_t* dTris = nullptr;
+    std::vector<MaterialRec> mats(d->material_count);
+    for (uint32_t i = 0; i < d->material_count; ++i) {
+        const x2_material& m = d->materials[i];
+        mats[i].kind = m.kind;
+        for (int k = 0; k < 3; ++k) {
+            mats[i].diffuse[k] = m.diffuse[k];
+            mats[i].specular[k] = m.specular[k];
+            mats[i].emission[k] = m.emission[k];
+        }
+        mats[i].roughness = m.roughness;
+    }
+    cudaEvent_t b0, b1;
+    cudaEventCreate(&b0);
+    cudaEventCreate(&b1);
+    auto fail = [&](int code) {
+        cudaFree(dVerts);
+        cudaFree(dTris);
+        x2_scene_free(s);
+        cudaEventDestroy(b0);
+        cudaEventDestroy(b1);
+        return code;
+    };
+    if (cudaMalloc(&dVerts, sizeof(float) * 3 * size_t(d->vertex_count)) != cudaSuccess ||
+        cudaMalloc(&dTris, sizeof(uint32_t) * 3 * size_t(d->triangle_count)) != cudaSuccess ||
+        cudaMalloc(&s->triMesh, sizeof(uint32_t) * d->triangle_count) != cudaSuccess ||
+        cudaMalloc(&s->meshFirst, sizeof(uint32_t) * (d->mesh_count + 1)) != cudaSuccess ||
+        cudaMalloc(&s->meshMaterial, sizeof(uint32_t) * d->mesh_count) != cudaSuccess ||
+        cudaMalloc(&s->materials, sizeof(MaterialRec) * (d->material_count ? d->material_count : 1)) != cudaSuccess ||
+        cudaMalloc(&s->lights, sizeof(x2_light) * (d->light_count ? d->light_count : 1)) != cudaSuccess ||
+        cudaMalloc(&s->overflow, sizeof(uint32_t)) != cudaSuccess || cudaMalloc(&s->auditWord, sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&s->stats, sizeof(TraversalStats)) != cudaSuccess) {
+        setError("device allocation failed for the scene");
+        return fail(X2_ENOMEM);
+    }
+    cudaMemcpyAsync(dVerts, d->vertices, sizeof(float) * 3 * size_t(d->vertex_count), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(dTris, d->triangles, sizeof(uint32_t) * 3 * size_t(d->triangle_count), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s->triMesh, triMesh.data(), sizeof(uint32_t) * d->triangle_count, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s->meshFirst, d->mesh_first, sizeof(uint32_t) * (d->mesh_count + 1), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s->meshMaterial, d->mesh_material, sizeof(uint32_t) * d->mesh_count, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(s->materials, mats.data(), sizeof(MaterialRec) * d->material_count, cudaMemcpyHostToDevice, st);
+    if (d->light_count) cudaMemcpyAsync(s->lights, d->lights, sizeof(x2_light) * d->light_count, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(s->overflow, 0, sizeof(uint32_t), st);
+    cudaMemsetAsync(s->stats, 0, sizeof(TraversalStats), st);
+    cudaEventRecord(b0, st);
+    if (buildBvh(dVerts, dTris, d->triangle_count, st, &s->bvh) != 0) return fail(X2_ECUDA);
+    cudaEventRecord(b1, st);
+    if (cudaStreamSynchronize(st) != cudaSuccess) {
+        setError("scene upload failed: %s", cudaGetErrorString(cudaGetLastError()));
+        return fail(X2_ECUDA);
+    }
+    cudaEventElapsedTime(&s->buildMs, b0, b1);
+    cudaEventDestroy(b0);
+    cudaEventDestroy(b1);
+    cudaFree(dVerts);
+    cudaFree(dTris);
+    *out = s;
+    return X2_OK;
+}
+
+int x2_scene_free(x2_scene* s) {
+    if (!s) return X2_OK;
+    if (s->ctx) cudaSetDevice(s->ctx->device);
+    if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
+    cudaFree(s->bvh.nodes);
+    cudaFree(s->bvh.tris);
+    cudaFree(s->triMesh);
+    cudaFree(s->meshFirst);
+    cudaFree(s->meshMaterial);
+    cudaFree(s->materials);
+    cudaFree(s->lights);
+    cudaFree(s->overflow);
+    cudaFree(s->auditWord);
+    cudaFree(s->stats);
+    cudaFree(s->sums);
+    cudaFree(s->odd);
+    cudaFree(s->counts);
+    for (auto& sl : s->slots) freeSlot(sl);
+    freeSlot(s->integrateSlot);
+    if (s->staging) cudaFreeHost(s->staging);
+    delete s;
+    return X2_OK;
+}
+
+int x2_config_set(x2_scene* s, const x2_config* c) {
+    if (!s || !c) return X2_EINVAL;
+    if (c->width == 0 || c->height == 0 || uint64_t(c->width) * c->height > 0xffffffffull) {
+        setError("bad image size %ux%u", c->width, c->height);
+        return X2_EINVAL;
+    }
+    if (c->filter != X2_FILTER_BOX) {
+        setError("filter %u not admitted (box only)", c->filter);
+        return X2_EINVAL;
+    }
+    if (c->light_count != s->lightCount) {
+        setError("config light_count %u differs from the scene's %u lights", c->light_count, s->lightCount);
+        return X2_EINVAL;
+    }
+    if (c->bsdf_samples == 0 || c->bsdf_samples > 64 || c->light_samples == 0 || c->light_samples > 64) {
+        setError("bsdf/light samples out of [1, 64]");
+        return X2_EINVAL;
+    }
+    s->config = *c;
+    s->configured = true;
+    return X2_OK;
+}
+
+int x2_scene_info(x2_scene* s, uint64_t* nodes, uint64_t* bvhBytes, uint64_t* triBytes, float* buildMs) {
+    if (!s) return X2_EINVAL;
+    if (nodes) *nodes = s->bvh.nodeCount;
+    if (bvhBytes) *bvhBytes = uint64_t(s->bvh.nodeCount) * sizeof(Node8);
+    if (triBytes) *triBytes = uint64_t(s->bvh.triCount) * sizeof(TriRec);
+    if (buildMs) *buildMs = s->buildMs;
+    return X2_OK;
+}
+
+int x2_integrate_device(x2_scene* s, const uint32_t* pairs, uint64_t n, double* rgba, uint32_t* status) {
+    if (!s || !s->configured) {
+        setError("scene not configured");
+        return X2_EINVAL;
+    }
+    if (int rc = checkDevice(s->ctx)) return rc;
+    if (!n) return X2_OK;
+    if (int rc = ensureSlot(s->integrateSlot, 1)) return rc;
+    Slot& sl = s->integrateSlot;
+    cudaStream_t st = s->ctx->stream;
+    cudaMemsetAsync(sl.counters, 0, sizeof(Counters), st);
+    const int blocks = s->ctx->smCount * s->ctx->renderBlocksPerSm;
+    integratePairs<<<blocks, kRenderBlock, 0, st>>>(viewOf(s), pairs, n, rgba, status, sl.counters);
+    CUDA_OR(cudaGetLastError(), X2_ECUDA);
+    cudaMemcpyAsync(sl.hostCounters, sl.counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+    cudaEventRecord(sl.done, st);
+    sl.busy = true;
+    return X2_OK;
+}
+
+int x2_integrate(x2_scene* s, const uint32_t* pairs, uint64_t n, double* rgba, uint32_t* status) {
+    if (!s || !s->configured) {
+        setError("scene not configured");
+        return X2_EINVAL;
+    }
+    if (int rc = checkDevice(s->ctx)) return rc;
+    if (!n) return X2_OK;
+    if (!pairs || !rgba || !status) {
+        setError("null array");
+        return X2_EINVAL;
+    }
+    cudaStream_t st = s->ctx->stream;
+    uint32_t *dPairs = nullptr, *dStatus = nullptr;
+    double* dRgba = nullptr;
+    CUDA_OR(cudaMallocAsync(&dPairs, sizeof(uint32_t) * 2 * n, st), X2_ENOMEM);
+    CUDA_OR(cudaMallocAsync(&dRgba, sizeof(double) * 4 * n, st), X2_ENOMEM);
+    CUDA_OR(cudaMallocAsync(&dStatus, sizeof(uint32_t) * n, st), X2_ENOMEM);
+    cudaMemcpyAsync(dPairs, pairs, sizeof(uint32_t) * 2 * n, cudaMemcpyHostToDevice, st);
+    int rc = x2_integrate_device(s, dPairs, n, dRgba, dStatus);
+    if (rc == X2_OK) {
+        cudaMemcpyAsync(rgba, dRgba, sizeof(double) * 4 * n, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(status, dStatus, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st);
+    }
+    cudaFreeAsync(dPairs, st);
+    cudaFreeAsync(dRgba, st);
+    cudaFreeAsync(dStatus, st);
+    const int w = x2_synchronize(s->ctx, 600000);
+    if (rc == X2_OK && w == X2_OK && s->integrateSlot.busy) {
+        accumulate(s->total, *s->integrateSlot.hostCounters);
+        s->integrateSlot.busy = false;
+    }
+    return rc ? rc : w;
+}
+
+int x2_trace_rays_device(x2_scene* s, const float* rays, uint64_t n, uint32_t* tri, float* t, uint32_t* occluded) {
+    if (!s) return X2_EINVAL;
+    if (int rc = checkDevice(s->ctx)) return rc;
+    if (!n) return X2_OK;
+    if (!rays) {
+        setError("null rays");
+        return X2_EINVAL;
+    }
+    traceRays<<<s->ctx->smCount * 8, 128, 0, s->ctx->stream>>>(viewOf(s), rays, n, tri, t, occluded);
+    CUDA_OR(cudaGetLastError(), X2_ECUDA);
+    return X2_OK;
+}
+
+int x2_trace_rays(x2_scene* s, const float* rays, uint64_t n, uint32_t* tri, float* t, uint32_t* occluded) {
+    if (!s) return X2_EINVAL;
+    if (int rc = checkDevice(s->ctx)) return rc;
+    if (!n) return X2_OK;
+    if (!rays || !tri || !t || !occluded) {
+        setError("null array");
+        return X2_EINVAL;
+    }
+    cudaStream_t st = s->ctx->stream;
+    float *dRays = nullptr, *dT = nullptr;
+    uint32_t *dTri = nullptr, *dOcc = nullptr;
+    CUDA_OR(cudaMallocAsync(&dRays, sizeof(float) * 8 * n, st), X2_ENOMEM);
+    CUDA_OR(cudaMallocAsync(&dT, sizeof(float) * n, st), X2_ENOMEM);
+    CUDA_OR(cudaMallocAsync(&dTri, sizeof(uint32_t) * n, st), X2_ENOMEM);
+    CUDA_OR(cudaMallocAsync(&dOcc, sizeof(uint32_t) * n, st), X2_ENOMEM);
+    cudaMemcpyAsync(dRays, rays, sizeof(float) * 8 * n, cudaMemcpyHostToDevice, st);
+    const int rc = x2_trace_rays_device(s, dRays, n, dTri, dT, dOcc);
+    if (rc == X2_OK) {
+        cudaMemcpyAsync(tri, dTri, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(t, dT, sizeof(float) * n, cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(occluded, dOcc, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, st);
+    }
+    cudaFreeAsync(dRays, st);
+    cudaFreeAsync(dT, st);
+    cudaFreeAsync(dTri, st);
+    cudaFreeAsync(dOcc, st);
+    const int w = x2_synchronize(s->ctx, 600000);
+    return rc ? rc : w;
+}
+
+int x2_frame_begin(x2_scene* s, uint32_t samplesPerChunk) {
+    if (!s || !s->configured || samplesPerChunk == 0) {
+        setError("scene not configured or zero samples a chunk");
+        return X2_EINVAL;
+    }
+    if (int rc = checkDevice(s->ctx)) return rc;
+    // No launch of the previous frame may still write the film.
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    const uint32_t pixels = s->config.width * s->config.height;
+    cudaStream_t st = s->ctx->stream;
+    if (pixels != s->filmPixels) {
+        cudaFree(s->sums);
+        cudaFree(s->odd);
+        cudaFree(s->counts);
+        s->sums = s->odd = nullptr;
+        s->counts = nullptr;
+        CUDA_OR(cudaMalloc(&s->sums, sizeof(double) * 4 * size_t(pixels)), X2_ENOMEM);
+        CUDA_OR(cudaMalloc(&s->odd, sizeof(double) * 4 * size_t(pixels)), X2_ENOMEM);
+        CUDA_OR(cudaMalloc(&s->counts, sizeof(uint32_t) * size_t(pixels)), X2_ENOMEM);
+        s->filmPixels = pixels;
+    }
+    cudaMemsetAsync(s->sums, 0, sizeof(double) * 4 * size_t(pixels), st);
+    cudaMemsetAsync(s->odd, 0, sizeof(double) * 4 * size_t(pixels), st);
+    cudaMemsetAsync(s->counts, 0, sizeof(uint32_t) * size_t(pixels), st);
+    cudaMemsetAsync(s->overflow, 0, sizeof(uint32_t), st);
+    s->samplesPerChunk = samplesPerChunk;
+    CUDA_OR(cudaGetLastError(), X2_ECUDA);
+    return X2_OK;
+}
+
+int x2_launch(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
+    if (!s || !s->configured || !s->filmPixels || !s->samplesPerChunk) {
+        setError("x2_frame_begin first");
+        return X2_EINVAL;
+    }
+    if (int rc = checkDevice(s->ctx)) return rc;
+    if (!count) return X2_OK;
+    if (!chunks) return X2_EINVAL;
+    const uint32_t tiles = ((s->config.width + 7) / 8) * ((s->config.height + 7) / 8);
+    for (uint32_t i = 0; i < count; ++i)
+        if (chunks[i].tile >= tiles || chunks[i].count > s->samplesPerChunk) {
+            setError("chunk %u: tile %u of %u or count %u over %u samples a chunk", i, chunks[i].tile, tiles, chunks[i].count,
+                     s->samplesPerChunk);
+            return X2_EINVAL;
+        }
+    // A free slot: at most two launches in flight; wait (bounded) for the older one otherwise.
+    Slot* sl = nullptr;
+    for (auto& c : s->slots)
+        if (!c.busy) sl = &c;
+    if (!sl) {
+        Slot* oldest = &s->slots[0];
+        for (auto& c : s->slots)
+            if (c.seq < oldest->seq) oldest = &c;
+        if (int rc = waitEvent(oldest->done, 600000)) return rc;
+        retire(s, *oldest, nullptr);
+        sl = oldest;
+    }
+    if (int rc = ensureSlot(*sl, count)) return rc;
+    cudaStream_t st = s->ctx->stream;
+    CUDA_OR(cudaMemcpyAsync(sl->chunks, chunks, sizeof(x2_chunk) * count, cudaMemcpyHostToDevice, st), X2_ECUDA);
+    cudaMemsetAsync(sl->claimed, 0, sizeof(unsigned long long), st);
+    cudaMemsetAsync(sl->counters, 0, sizeof(Counters), st);
+    RenderArgs a;
+    a.scene = viewOf(s);
+    a.chunks = sl->chunks;
+    a.samplesPerChunk = s->samplesPerChunk;
+    a.itemCount = (unsigned long long)count * 64ull * s->samplesPerChunk;
+    a.claimed = sl->claimed;
+    a.sums = s->sums;
+    a.odd = s->adaptive ? s->odd : nullptr;
+    a.counts = s->counts;
+    a.counters = sl->counters;
+    const int blocks = s->ctx->smCount * s->ctx->renderBlocksPerSm;
+    cudaEventRecord(sl->begin, st);
+    renderChunks<<<blocks, kRenderBlock, 0, st>>>(a);
+    CUDA_OR(cudaGetLastError(), X2_ECUDA);
+    cudaEventRecord(sl->end, st);
+    cudaMemcpyAsync(sl->hostCounters, sl->counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+    cudaEventRecord(sl->done, st);
+    sl->busy = true;
+    sl->seq = s->nextSeq++;
+    return X2_OK;
+}
+
+int x2_poll(x2_scene* s, x2_completion* out) {
+    if (!s) return X2_EINVAL;
+    Slot* oldest = nullptr;
+    for (auto& c : s->slots)
+        if (c.busy && (!oldest || c.seq < oldest->seq)) oldest = &c;
+    if (!oldest) return 0;
+    const cudaError_t q = cudaEventQuery(oldest->done);
+    if (q == cudaErrorNotReady) return 0;
+    if (q != cudaSuccess) {
+        setError("launch failed: %s", cudaGetErrorString(q));
+        return -X2_ECUDA;
+    }
+    retire(s, *oldest, out);
+    return 1;
+}
+
+int x2_wait(x2_scene* s, int timeoutMs, x2_completion* out) {
+    if (!s) return X2_EINVAL;
+    if (out) std::memset(out, 0, sizeof(*out));
+    if (int rc = x2_synchronize(s->ctx, timeoutMs)) return rc;
+    for (;;) {
+        x2_completion c;
+        const int r = x2_poll(s, &c);
+        if (r < 0) return -r;
+        if (r == 0) break;
+        if (out) {
+            out->launch = c.launch;
+            out->samples += c.samples;
+            out->errors += c.errors;
+            out->milliseconds += c.milliseconds;
+        }
+    }
+    return X2_OK;
+}
+
+int x2_render_frame(x2_scene* s, uint32_t first, uint32_t count) {
+    if (!s || !s->configured) return X2_EINVAL;
+    if (!s->filmPixels || s->samplesPerChunk < count) {
+        setError("x2_frame_begin with at least %u samples a chunk first", count);
+        return X2_EINVAL;
+    }
+    const uint32_t tiles = ((s->config.width + 7) / 8) * ((s->config.height + 7) / 8);
+    // Staging must not be rewritten while an earlier launch's copy may still read it: wait for the stream.
+    if (int rc = x2_synchronize(s->ctx, 600000)) return rc;
+    if (tiles > s->stagingCap) {
+        if (s->staging) cudaFreeHost(s->staging);
+        s->staging = nullptr;
+        CUDA_OR(cudaMallocHost(&s->staging, sizeof(x2_chunk) * tiles), X2_ENOMEM);
+        s->stagingCap = tiles;
+    }
+    for (uint32_t t = 0; t < tiles; ++t) s->staging[t] = x2_chunk{t, first, count, 0};
+    return x2_launch(s, s->staging, tiles);
+}
+
+int x2_film_device(x2_scene* s, double** sums, double** odd, uint32_t** counts) {
+    if (!s || !s->filmPixels) return X2_EINVAL;
+    if (sums) *sums = s->sums;
+    if (odd) *odd = s->odd;
+    if (counts) *counts = s->counts;
+    return X2_OK;
+}
+
+int x2_film_download(x2_scene* s, double* sums, double* odd, uint32_t* counts) {
+    if (!s || !s->filmPixels) {
+        setError("no film");
+        return X2_EINVAL;
+    }
+    if (int rc = checkDevice(s->ctx)) return rc;
+    cudaStream_t st = s->ctx->stream;
+    const size_t p = s->filmPixels;
+    if (sums) cudaMemcpyAsync(sums, s->sums, sizeof(double) * 4 * p, cudaMemcpyDeviceToHost, st);
+    if (odd) cudaMemcpyAsync(odd, s->odd, sizeof(double) * 4 * p, cudaMemcpyDeviceToHost, st);
+    if (counts) cudaMemcpyAsync(counts, s->counts, sizeof(uint32_t) * p, cudaMemcpyDeviceToHost, st);
+    return x2_wait(s, 600000, nullptr);
+}
+
+int x2_audit(x2_scene* s, const uint32_t* expected, int64_t* badPixel) {
+    if (!s || !s->filmPixels) return X2_EINVAL;
+    if (int rc = checkDevice(s->ctx)) return rc;
+    cudaStream_t st = s->ctx->stream;
+    const unsigned long long none = ~0ull;
+    uint32_t* dExpected = nullptr;
+    if (expected) {
+        CUDA_OR(cudaMallocAsync(&dExpected, sizeof(uint32_t) * s->filmPixels, st), X2_ENOMEM);
+        cudaMemcpyAsync(dExpected, expected, sizeof(uint32_t) * s->filmPixels, cudaMemcpyHostToDevice, st);
+    }
+    cudaMemcpyAsync(s->auditWord, &none, sizeof(none), cudaMemcpyHostToDevice, st);
+    auditCounts<<<(s->filmPixels + 255) / 256, 256, 0, st>>>(s->counts, dExpected, s->config.spp, s->filmPixels, s->auditWord);
+    unsigned long long first = ~0ull;
+    cudaMemcpyAsync(&first, s->auditWord, sizeof(first), cudaMemcpyDeviceToHost, st);
+    if (dExpected) cudaFreeAsync(dExpected, st);
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    if (badPixel) *badPixel = first == ~0ull ? -1 : int64_t(first);
+    if (first != ~0ull) {
+        setError("Sample audit failure at pixel %llu", first);
+        return X2_EAUDIT;
+    }
+    return X2_OK;
+}
+
+int x2_counters_read(x2_scene* s, x2_counters* out) {
+    if (!s || !out) return X2_EINVAL;
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    uint32_t overflow = 0;
+    cudaMemcpy(&overflow, s->overflow, sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    out->trace = s->total.trace;
+    out->shadow_nee = s->total.nee;
+    out->shadow_bsdf = s->total.bsdf;
+    out->held = s->total.held;
+    out->samples = s->total.samples;
+    out->errors = s->total.errors;
+    out->stack_overflows = overflow;
+    out->pad = 0;
+    return X2_OK;
+}
+
+int x2_count_traversal(x2_scene* s, int on) {
+    if (!s) return X2_EINVAL;
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    s->counting = on != 0;
+    return X2_OK;
+}
+
+int x2_traversal_counts(x2_scene* s, uint64_t* rays, uint64_t* nodes, uint64_t* triangles) {
+    if (!s) return X2_EINVAL;
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    TraversalStats h{};
+    CUDA_OR(cudaMemcpy(&h, s->stats, sizeof(h), cudaMemcpyDeviceToHost), X2_ECUDA);
+    CUDA_OR(cudaMemset(s->stats, 0, sizeof(h)), X2_ECUDA);
+    if (rays) *rays = h.rays;
+    if (nodes) *nodes = h.nodes;
+    if (triangles) *triangles = h.tris;
+    return X2_OK;
+}
+
+int x2_counters_reset(x2_scene* s) {
+    if (!s) return X2_EINVAL;
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    s->total = Counters{};
+    return X2_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,254 @@
+// Closest-hit and any-hit traversal of the compressed 8-wide BVH (bvh.cuh) for one ray a thread.
+//
+// A node is five 16-byte read-only loads. Its eight children are tested with one FMA a slab (Ylitie et al. 2017:
+// the ray is expressed in the node's quantised frame once, t = q * (2^e / d) + (p - o) / d), widened by 2^-20 of
+// the distance each way so the quantised boxes stay conservative. Hit children enter a 32-bit mask: internal
+// children on bits 24..31 in near-to-far order for the ray's octant (the build places each child in the slot of
+// the octant it lies toward), leaf triangles on bits 0..23. The stack holds (child base, mask | imask) pairs and
+// lives in registers/local memory; an overflow is counted, never silent.
+//
+// The triangle test is Woop, Benthin and Wald's watertight test in fp32 without contraction (the library is built
+// with -fmad=false): the same operations, in the same order, as the oracle's, so both pick the same triangle. Ties
+// go to the nearest t, then the lowest scene triangle index (the reference's triangle::nearer rule, triangle_hit.h:26).
+#pragma once
+#include "bvh.cuh"
+
+#include <cfloat>
+
+namespace x2 {
+
+constexpr int kStack = 32;
+
+struct RayQ {
+    float ox, oy, oz, dx, dy, dz;
+    float ix, iy, iz;  // inverse direction for the box test (components below 1e-18 clamped)
+    uint32_t oct7;     // XOR pattern that orders a node's slots near to far
+    int kx, ky, kz;    // the shear's axes
+    float Sx, Sy, Sz;
+};
+
+__device__ __forceinline__ float pick3(float x, float y, float z, int k) { return k == 0 ? x : (k == 1 ? y : z); }
+
+__device__ __forceinline__ RayQ makeRay(float ox, float oy, float oz, float dx, float dy, float dz) {
+    RayQ r;
+    r.ox = ox;
+    r.oy = oy;
+    r.oz = oz;
+    r.dx = dx;
+    r.dy = dy;
+    r.dz = dz;
+    const float tiny = 1e-18f;
+    r.ix = 1.0f / (fabsf(dx) > tiny ? dx : copysignf(tiny, dx));
+    r.iy = 1.0f / (fabsf(dy) > tiny ? dy : copysignf(tiny, dy));
+    r.iz = 1.0f / (fabsf(dz) > tiny ? dz : copysignf(tiny, dz));
+    const uint32_t oct = (signbit(dx) ? 1u : 0u) | (signbit(dy) ? 2u : 0u) | (signbit(dz) ? 4u : 0u);
+    r.oct7 = ~oct & 7u;
+    const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+    int kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    int kx = kz == 2 ? 0 : kz + 1;
+    int ky = kx == 2 ? 0 : kx + 1;
+    const float dzz = pick3(dx, dy, dz, kz);
+    if (dzz < 0.0f) {
+        const int t = kx;
+        kx = ky;
+        ky = t;
+    }
+    r.kx = kx;
+    r.ky = ky;
+    r.kz = kz;
+    r.Sx = pick3(dx, dy, dz, kx) / dzz;
+    r.Sy = pick3(dx, dy, dz, ky) / dzz;
+    r.Sz = 1.0f / dzz;
+    return r;
+}
+
+// Watertight ray/triangle test; the operations match the oracle's triHit exactly.
+__device__ __forceinline__ bool triTest(const RayQ& r, const float4& a, const float4& b, const float4& c, float tmin, float tmax, float& tOut) {
+    const float Akx = pick3(a.x, a.y, a.z, r.kx) - pick3(r.ox, r.oy, r.oz, r.kx);
+    const float Aky = pick3(a.x, a.y, a.z, r.ky) - pick3(r.ox, r.oy, r.oz, r.ky);
+    const float Akz = pick3(a.x, a.y, a.z, r.kz) - pick3(r.ox, r.oy, r.oz, r.kz);
+    const float Bkx = pick3(b.x, b.y, b.z, r.kx) - pick3(r.ox, r.oy, r.oz, r.kx);
+    const float Bky = pick3(b.x, b.y, b.z, r.ky) - pick3(r.ox, r.oy, r.oz, r.ky);
+    const float Bkz = pick3(b.x, b.y, b.z, r.kz) - pick3(r.ox, r.oy, r.oz, r.kz);
+    const float Ckx = pick3(c.x, c.y, c.z, r.kx) - pick3(r.ox, r.oy, r.oz, r.kx);
+    const float Cky = pick3(c.x, c.y, c.z, r.ky) - pick3(r.ox, r.oy, r.oz, r.ky);
+    const float Ckz = pick3(c.x, c.y, c.z, r.kz) - pick3(r.ox, r.oy, r.oz, r.kz);
+    const float Ax = Akx - r.Sx * Akz, Ay = Aky - r.Sy * Akz;
+    const float Bx = Bkx - r.Sx * Bkz, By = Bky - r.Sy * Bkz;
+    const float Cx = Ckx - r.Sx * Ckz, Cy = Cky - r.Sy * Ckz;
+    float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+    if (U == 0.0f || V == 0.0f || W == 0.0f) {
+        U = float(double(Cx) * double(By) - double(Cy) * double(Bx));
+        V = float(double(Ax) * double(Cy) - double(Ay) * double(Cx));
+        W = float(double(Bx) * double(Ay) - double(By) * double(Ax));
+    }
+    if ((U < 0.0f || V < 0.0f || W < 0.0f) && (U > 0.0f || V > 0.0f || W > 0.0f)) return false;
+    const float det = U + V + W;
+    if (det == 0.0f) return false;
+    const float Az = r.Sz * Akz, Bz = r.Sz * Bkz, Cz = r.Sz * Ckz;
+    const float T = U * Az + V * Bz + W * Cz;
+    const float t = T / det;
+    if (!(t >= tmin && t <= tmax)) return false;
+    tOut = t;
+    return true;
+}
+
+__device__ __forceinline__ uint32_t byteOf(uint32_t lo, uint32_t hi, int s) {
+    return ((s < 4 ? lo : hi) >> (8 * (s & 3))) & 0xffu;
+}
+
+// One node: the hit mask (bits 24..31 internal children in traversal order, 0..23 leaf triangles), its child and
+// triangle bases and its internal-child mask.
+__device__ __forceinline__ uint32_t visitNode(const Node8* __restrict__ nodes, uint32_t index, const RayQ& r, float tmin, float tmax,
+                                              uint32_t& childBase, uint32_t& triBase, uint32_t& imask) {
+    const uint4* p = reinterpret_cast<const uint4*>(nodes + index);
+    const uint4 n0 = __ldg(p), n1 = __ldg(p + 1), n2 = __ldg(p + 2), n3 = __ldg(p + 3), n4 = __ldg(p + 4);
+    const float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
+    const uint32_t ex = n0.w & 0xffu, ey = (n0.w >> 8) & 0xffu, ez = (n0.w >> 16) & 0xffu;
+    imask = n0.w >> 24;
+    childBase = n1.x;
+    triBase = n1.y;
+    const float sx = __uint_as_float(ex << 23) * r.ix, sy = __uint_as_float(ey << 23) * r.iy, sz = __uint_as_float(ez << 23) * r.iz;
+    const float ax = (px - r.ox) * r.ix, ay = (py - r.oy) * r.iy, az = (pz - r.oz) * r.iz;
+    const bool fx = r.ix >= 0.0f, fy = r.iy >= 0.0f, fz = r.iz >= 0.0f;
+    uint32_t hits = 0;
+#pragma unroll
+    for (int s = 0; s < 8; ++s) {
+        const uint32_t meta = byteOf(n1.z, n1.w, s);
+        const float qlx = float(byteOf(n2.x, n2.y, s)), qly = float(byteOf(n2.z, n2.w, s)), qlz = float(byteOf(n3.x, n3.y, s));
+        const float qhx = float(byteOf(n3.z, n3.w, s)), qhy = float(byteOf(n4.x, n4.y, s)), qhz = float(byteOf(n4.z, n4.w, s));
+        const float nx = __fmaf_rn(fx ? qlx : qhx, sx, ax), fxx = __fmaf_rn(fx ? qhx : qlx, sx, ax);
+        const float ny = __fmaf_rn(fy ? qly : qhy, sy, ay), fyy = __fmaf_rn(fy ? qhy : qly, sy, ay);
+        const float nz = __fmaf_rn(fz ? qlz : qhz, sz, az), fzz = __fmaf_rn(fz ? qhz : qlz, sz, az);
+        float entry = fmaxf(nx, fmaxf(ny, nz)), exit = fminf(fxx, fminf(fyy, fzz));
+        entry = __fsub_rn(entry, fabsf(entry) * 0x1p-20f);
+        exit = __fadd_rn(exit, fabsf(exit) * 0x1p-20f);
+        entry = fmaxf(entry, tmin);
+        exit = fminf(exit, tmax);
+        if (meta && entry <= exit) {
+            const uint32_t internal = (imask >> s) & 1u;
+            hits |= (meta >> 5) << ((meta & 31u) ^ (internal ? r.oct7 : 0u));
+        }
+    }
+    return hits;
+}
+
+// Traversal work of a counting run (node visits and triangle tests), for the roofline's algorithmic bytes. The
+// timed kernels are instantiated without it.
+struct TraversalStats {
+    unsigned long long rays, nodes, tris;
+};
+
+// Closest hit on [tmin, tmax]: the scene triangle index (~0u: none), its t and its position in leaf order.
+template <bool kStats>
+static __device__ __noinline__ uint32_t traceClosest(const Bvh8 bvh, const RayQ& r, float tmin, float tmax, float& tHit, uint32_t* leafOut,
+                                                     uint32_t* overflow, TraversalStats* stats) {
+    uint2 stack[kStack];
+    int sp = 0;
+    uint32_t best = ~0u, bestLeaf = 0, nodes = 0, tris = 0;
+    float tBest = tmax;
+    uint32_t gBase = 0, gBits = 0x80000000u, gImask = 1u << (7u ^ r.oct7);
+    for (;;) {
+        while (gBits & 0xff000000u) {
+            const uint32_t b = __ffs(gBits >> 24) - 1;
+            gBits &= ~(1u << (24 + b));
+            const uint32_t slot = b ^ r.oct7;
+            const uint32_t child = gBase + __popc(gImask & ((1u << slot) - 1u));
+            if (gBits & 0xff000000u) {
+                if (sp < kStack) stack[sp++] = make_uint2(gBase, gBits | (gImask << 16));
+                else atomicAdd(overflow, 1u);
+            }
+            uint32_t childBase, triBase, imask;
+            const uint32_t hits = visitNode(bvh.nodes, child, r, tmin, tBest, childBase, triBase, imask);
+            if (kStats) ++nodes;
+            uint32_t tBits = hits & 0x00ffffffu;
+            while (tBits) {
+                const uint32_t k = __ffs(tBits) - 1;
+                tBits &= tBits - 1;
+                const float4* tp = reinterpret_cast<const float4*>(bvh.tris + triBase + k);
+                const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+                if (kStats) ++tris;
+                float t;
+                if (triTest(r, v0, v1, v2, tmin, tBest, t)) {
+                    const uint32_t id = __float_as_uint(v0.w);
+                    if (t < tBest || (t == tBest && id < best)) {
+                        tBest = t;
+                        best = id;
+                        bestLeaf = triBase + k;
+                    }
+                }
+            }
+            gBase = childBase;
+            gBits = hits & 0xff000000u;
+            gImask = imask;
+        }
+        if (sp == 0) break;
+        const uint2 e = stack[--sp];
+        gBase = e.x;
+        gBits = e.y & 0xff000000u;
+        gImask = (e.y >> 16) & 0xffu;
+    }
+    if (kStats) {
+        atomicAdd(&stats->rays, 1ull);
+        atomicAdd(&stats->nodes, (unsigned long long)nodes);
+        atomicAdd(&stats->tris, (unsigned long long)tris);
+    }
+    tHit = tBest;
+    *leafOut = bestLeaf;
+    return best;
+}
+
+// Any hit on [tmin, tmax].
+template <bool kStats>
+static __device__ __noinline__ bool traceAny(const Bvh8 bvh, const RayQ& r, float tmin, float tmax, uint32_t* overflow, TraversalStats* stats) {
+    uint2 stack[kStack];
+    int sp = 0;
+    uint32_t nodes = 0, tris = 0;
+    bool hit = false;
+    uint32_t gBase = 0, gBits = 0x80000000u, gImask = 1u << (7u ^ r.oct7);
+    for (;;) {
+        while (gBits & 0xff000000u) {
+            const uint32_t b = __ffs(gBits >> 24) - 1;
+            gBits &= ~(1u << (24 + b));
+            const uint32_t slot = b ^ r.oct7;
+            const uint32_t child = gBase + __popc(gImask & ((1u << slot) - 1u));
+            if (gBits & 0xff000000u) {
+                if (sp < kStack) stack[sp++] = make_uint2(gBase, gBits | (gImask << 16));
+                else atomicAdd(overflow, 1u);
+            }
+            uint32_t childBase, triBase, imask;
+            const uint32_t hits = visitNode(bvh.nodes, child, r, tmin, tmax, childBase, triBase, imask);
+            if (kStats) ++nodes;
+            uint32_t tBits = hits & 0x00ffffffu;
+            while (tBits) {
+                const uint32_t k = __ffs(tBits) - 1;
+                tBits &= tBits - 1;
+                const float4* tp = reinterpret_cast<const float4*>(bvh.tris + triBase + k);
+                const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+                if (kStats) ++tris;
+                float t;
+                if (triTest(r, v0, v1, v2, tmin, tmax, t)) {
+                    hit = true;
+                    goto done;
+                }
+            }
+            gBase = childBase;
+            gBits = hits & 0xff000000u;
+            gImask = imask;
+        }
+        if (sp == 0) break;
+        const uint2 e = stack[--sp];
+        gBase = e.x;
+        gBits = e.y & 0xff000000u;
+        gImask = (e.y >> 16) & 0xffu;
+    }
+done:
+    if (kStats) {
+        atomicAdd(&stats->rays, 1ull);
+        atomicAdd(&stats->nodes, (unsigned long long)nodes);
+        atomicAdd(&stats->tris, (unsigned long long)tris);
+    }
+    return hit;
+}
+
+}  // namespace x2

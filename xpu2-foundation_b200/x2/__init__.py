@@ -1,0 +1,346 @@
+"""x2 — Python layer over the B200 path-sample engine's C ABI (libx2.so, include/x2.h).
+
+Mirrors the reference's two interfaces for the path: the per-sample `integrate(config, pixel, index, backend, out)`
+(xpu2/interactive/async_integrator.h:3047) as `Scene.integrate`, and the GPU lane
+(xpu2/interactive/async_gpu.h:1372-1707: begin / launch / poll / downloadFilm / sums / counts) as
+`Scene.frame_begin / launch / poll / wait / film / audit`. Errors raise `X2Error` with the library's message, as
+the reference's `cpu::need` raises `std::runtime_error`.
+
+There is no CPU fallback: without the built library or a CUDA device every call raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY = os.path.join(_HERE, "libx2.so")
+
+OK, EINVAL, ECUDA, ENOMEM, ETIMEOUT, EAUDIT, ENODEV, EDEVICE = range(8)
+DONE, MISS, ERROR, SKIP, DEFER = range(5)
+MAT_LAMBERT, MAT_GGX = 0, 1
+LIGHT_ENV, LIGHT_RECT = 0, 1
+
+
+class X2Error(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"x2 error {code}: {message}")
+        self.code = code
+
+
+class Identity(C.Structure):
+    _fields_ = [("pixel", C.c_uint32), ("pad", C.c_uint32), ("index", C.c_uint64), ("stream", C.c_uint64), ("branch", C.c_uint64)]
+
+
+class Chunk(C.Structure):
+    _fields_ = [("tile", C.c_uint32), ("first", C.c_uint32), ("count", C.c_uint32), ("cell", C.c_uint32)]
+
+
+class Material(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("diffuse", C.c_float * 3), ("specular", C.c_float * 3), ("emission", C.c_float * 3),
+                ("roughness", C.c_float)]
+
+
+class Light(C.Structure):
+    _fields_ = [("type", C.c_uint32), ("sidedness", C.c_uint32), ("visible_in_camera", C.c_uint32), ("hemispherical", C.c_uint32),
+                ("radiance", C.c_float * 3), ("position", C.c_float * 3), ("direction", C.c_float * 3),
+                ("local2render", (C.c_float * 3) * 3), ("render2local", (C.c_float * 3) * 3), ("render2local_rot", (C.c_float * 3) * 3),
+                ("scale", C.c_float), ("inv_area", C.c_float), ("plane_offset", C.c_float), ("half_width", C.c_float),
+                ("half_height", C.c_float), ("visibility_mask", C.c_uint32)]
+
+
+class Camera(C.Structure):
+    _fields_ = [("raster_to_camera", (C.c_float * 4) * 4), ("camera_to_render", (C.c_float * 4) * 4), ("near_clip", C.c_float),
+                ("far_clip", C.c_float)]
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("vertex_count", C.c_uint32), ("triangle_count", C.c_uint32), ("mesh_count", C.c_uint32), ("material_count", C.c_uint32),
+                ("light_count", C.c_uint32), ("pad", C.c_uint32), ("vertices", C.POINTER(C.c_float)), ("triangles", C.POINTER(C.c_uint32)),
+                ("mesh_first", C.POINTER(C.c_uint32)), ("mesh_material", C.POINTER(C.c_uint32)), ("materials", C.POINTER(Material)),
+                ("lights", C.POINTER(Light)), ("camera", Camera)]
+
+
+_U = C.c_uint32
+_F = C.c_float
+
+
+class Config(C.Structure):
+    """mixed::Config's fields this engine reads (gpu_jobs.h:10-44), with its defaults (x2_config_defaults)."""
+    _fields_ = [("width", _U), ("height", _U), ("seed", _U), ("spp", _U), ("sampling", _U), ("filter", _U), ("filter_width", _F),
+                ("light_count", _U), ("bsdf_samples", _U), ("light_samples", _U), ("max_depth", _U), ("max_diffuse_depth", _U),
+                ("clamp_depth", _U), ("rr_threshold", _F), ("clamp_value", _F), ("max_glossy_depth", _U), ("max_mirror_depth", _U),
+                ("max_hair_depth", _U), ("max_presence_depth", _U), ("shadow_terminator_fix", _U), ("roughness_clamping", _F),
+                ("transparency_threshold", _F), ("visible_lights", _U), ("presence_threshold", _F), ("presence_quality", _F),
+                ("shadow_reuse", _U), ("reserved", _U * 8)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class Counters(C.Structure):
+    _fields_ = [("trace", C.c_uint64), ("shadow_nee", C.c_uint64), ("shadow_bsdf", C.c_uint64), ("held", C.c_uint64),
+                ("samples", C.c_uint64), ("errors", C.c_uint64), ("stack_overflows", C.c_uint64), ("pad", C.c_uint64)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "pad"}
+
+
+class Completion(C.Structure):
+    _fields_ = [("launch", C.c_uint64), ("samples", C.c_uint64), ("errors", C.c_uint64), ("milliseconds", C.c_float), ("pad", C.c_uint32)]
+
+
+_lib = None
+
+
+def library():
+    """The loaded libx2.so (ctypes), its signatures declared. Raises when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIBRARY):
+        raise X2Error(ENODEV, f"{LIBRARY} is not built (run xpu2-foundation_b200/build.py)")
+    lib = C.CDLL(LIBRARY)
+    vp, u32, u64, i32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
+    sig = {
+        "x2_version": ([], C.c_char_p), "x2_last_error": ([], C.c_char_p), "x2_config_defaults": ([C.POINTER(Config)], None),
+        "x2_open": ([i32, C.POINTER(vp)], i32), "x2_close": ([vp], i32), "x2_synchronize": ([vp, i32], i32),
+        "x2_sample_words": ([vp, vp, vp, u64, u32, vp], i32), "x2_sample_words_device": ([vp, vp, vp, u64, u32, vp], i32),
+        "x2_scene_load": ([vp, C.POINTER(SceneDesc), C.POINTER(vp)], i32), "x2_scene_free": ([vp], i32),
+        "x2_config_set": ([vp, C.POINTER(Config)], i32),
+        "x2_scene_info": ([vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), C.POINTER(C.c_float)], i32),
+        "x2_integrate": ([vp, vp, u64, vp, vp], i32), "x2_integrate_device": ([vp, vp, u64, vp, vp], i32),
+        "x2_trace_rays": ([vp, vp, u64, vp, vp, vp], i32), "x2_trace_rays_device": ([vp, vp, u64, vp, vp, vp], i32),
+        "x2_frame_begin": ([vp, u32], i32), "x2_launch": ([vp, vp, u32], i32), "x2_poll": ([vp, C.POINTER(Completion)], i32),
+        "x2_wait": ([vp, i32, C.POINTER(Completion)], i32), "x2_render_frame": ([vp, u32, u32], i32),
+        "x2_film_download": ([vp, vp, vp, vp], i32), "x2_film_device": ([vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)], i32),
+        "x2_audit": ([vp, vp, C.POINTER(C.c_int64)], i32), "x2_counters_read": ([vp, C.POINTER(Counters)], i32),
+        "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
+        "x2_traversal_counts": ([vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
+        "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
+    }
+    for name, (args, res) in sig.items():
+        f = getattr(lib, name)
+        f.argtypes = args
+        f.restype = res
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != OK:
+        raise X2Error(rc, library().x2_last_error().decode())
+
+
+def _ptr(a):
+    return C.c_void_p(a.ctypes.data) if a is not None else C.c_void_p(0)
+
+
+def config_defaults():
+    c = Config()
+    library().x2_config_defaults(C.byref(c))
+    return c
+
+
+class Context:
+    """One CUDA device and stream (GpuLane's own, async_gpu.h:82)."""
+
+    def __init__(self, device=0):
+        self._h = C.c_void_p()
+        _check(library().x2_open(device, C.byref(self._h)))
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self):
+        if self._h:
+            library().x2_close(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self, timeout_ms=600000):
+        _check(library().x2_synchronize(self._h, timeout_ms))
+
+    def sample_words(self, ids, dims, policy):
+        """sample::samplingWord for structured `ids` (IDENTITY_DTYPE) and uint32 `dims` (host arrays)."""
+        ids = np.ascontiguousarray(ids, dtype=IDENTITY_DTYPE)
+        dims = np.ascontiguousarray(dims, dtype=np.uint32)
+        out = np.empty(len(dims), np.uint32)
+        _check(library().x2_sample_words(self._h, _ptr(ids), _ptr(dims), len(dims), policy, _ptr(out)))
+        return out
+
+
+IDENTITY_DTYPE = np.dtype([("pixel", "<u4"), ("pad", "<u4"), ("index", "<u8"), ("stream", "<u8"), ("branch", "<u8")])
+
+
+class SyntheticScene:
+    """A seeded synthetic scene made by the library's host generator (x2_scene_generate): its descriptor (owned
+    by the library until freed) and the config that goes with it."""
+
+    def __init__(self, config_id, seed=None):
+        self._desc = C.POINTER(SceneDesc)()
+        self.config = Config()
+        self.config_id = config_id
+        self.seed = (config_id % 100) + 1 if seed is None else seed
+        _check(library().x2_scene_generate(config_id, self.seed, C.byref(self._desc), C.byref(self.config)))
+
+    @property
+    def desc(self):
+        return self._desc.contents
+
+    @property
+    def desc_ptr(self):
+        return self._desc
+
+    def arrays(self):
+        d = self.desc
+        return {
+            "vertices": np.ctypeslib.as_array(d.vertices, (d.vertex_count * 3,)).copy(),
+            "triangles": np.ctypeslib.as_array(d.triangles, (d.triangle_count * 3,)).copy(),
+            "mesh_first": np.ctypeslib.as_array(d.mesh_first, (d.mesh_count + 1,)).copy(),
+            "mesh_material": np.ctypeslib.as_array(d.mesh_material, (d.mesh_count,)).copy(),
+        }
+
+    def free(self):
+        if self._desc:
+            library().x2_scene_desc_free(self._desc)
+            self._desc = C.POINTER(SceneDesc)()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Scene:
+    """A scene on the device with its BVH (built on the device at load) and its config."""
+
+    def __init__(self, ctx, desc, config):
+        self.ctx = ctx
+        self._h = C.c_void_p()
+        _check(library().x2_scene_load(ctx.handle, C.byref(desc) if isinstance(desc, SceneDesc) else desc, C.byref(self._h)))
+        self.set_config(config)
+
+    def set_config(self, config):
+        _check(library().x2_config_set(self._h, C.byref(config)))
+        self.config = config
+
+    @property
+    def handle(self):
+        return self._h
+
+    def info(self):
+        n, b, t, ms = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_float()
+        _check(library().x2_scene_info(self._h, C.byref(n), C.byref(b), C.byref(t), C.byref(ms)))
+        return {"bvh_nodes": n.value, "bvh_bytes": b.value, "triangle_bytes": t.value, "build_ms": ms.value}
+
+    def free(self):
+        if self._h:
+            library().x2_scene_free(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    # -- per sample: integrate() --
+    def integrate(self, pixels, indices):
+        """Radiance (rgb + alpha, float64) and SampleStatus of each (pixel, index) sample."""
+        pixels = np.asarray(pixels, np.uint32)
+        indices = np.asarray(indices, np.uint32)
+        pairs = np.ascontiguousarray(np.stack([pixels, indices], axis=1).astype(np.uint32))
+        n = len(pixels)
+        rgba = np.empty((n, 4), np.float64)
+        status = np.empty(n, np.uint32)
+        _check(library().x2_integrate(self._h, _ptr(pairs), n, _ptr(rgba), _ptr(status)))
+        return rgba, status
+
+    # -- traversal: Backend::trace / visible --
+    def trace_rays(self, rays):
+        """Closest hit (scene triangle, ~0 for none), its t, and occlusion of [near, far] for (n, 8) float32 rays."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        n = len(rays)
+        tri = np.empty(n, np.uint32)
+        t = np.empty(n, np.float32)
+        occ = np.empty(n, np.uint32)
+        _check(library().x2_trace_rays(self._h, _ptr(rays), n, _ptr(tri), _ptr(t), _ptr(occ)))
+        return tri, t, occ
+
+    # -- lane API --
+    def frame_begin(self, samples_per_chunk):
+        _check(library().x2_frame_begin(self._h, samples_per_chunk))
+
+    def launch(self, chunks):
+        chunks = np.ascontiguousarray(chunks, dtype=CHUNK_DTYPE)
+        _check(library().x2_launch(self._h, _ptr(chunks), len(chunks)))
+
+    def render_frame(self, first, count):
+        _check(library().x2_render_frame(self._h, first, count))
+
+    def poll(self):
+        c = Completion()
+        r = library().x2_poll(self._h, C.byref(c))
+        if r < 0:
+            _check(-r)
+        return c if r == 1 else None
+
+    def wait(self, timeout_ms=600000):
+        c = Completion()
+        _check(library().x2_wait(self._h, timeout_ms, C.byref(c)))
+        return c
+
+    def film(self, odd=False):
+        p = self.config.width * self.config.height
+        sums = np.empty((p, 4), np.float64)
+        counts = np.empty(p, np.uint32)
+        o = np.empty((p, 4), np.float64) if odd else None
+        _check(library().x2_film_download(self._h, _ptr(sums), _ptr(o), _ptr(counts)))
+        return (sums, o, counts) if odd else (sums, counts)
+
+    def audit(self, expected=None):
+        """The per-pixel sample-count audit (async_render.h:1010-1040); raises X2Error(EAUDIT) on a mismatch."""
+        bad = C.c_int64()
+        e = None if expected is None else np.ascontiguousarray(expected, np.uint32)
+        _check(library().x2_audit(self._h, _ptr(e), C.byref(bad)))
+
+    def counters(self):
+        c = Counters()
+        _check(library().x2_counters_read(self._h, C.byref(c)))
+        return c.as_dict()
+
+    def reset_counters(self):
+        _check(library().x2_counters_reset(self._h))
+
+    def count_traversal(self, on):
+        """Counting mode: following launches count node visits and triangle tests (never time them)."""
+        _check(library().x2_count_traversal(self._h, 1 if on else 0))
+
+    def traversal_counts(self):
+        r, n, t = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        _check(library().x2_traversal_counts(self._h, C.byref(r), C.byref(n), C.byref(t)))
+        return {"rays": r.value, "nodes": n.value, "triangles": t.value}
+
+
+CHUNK_DTYPE = np.dtype([("tile", "<u4"), ("first", "<u4"), ("count", "<u4"), ("cell", "<u4")])
+
+
+def image(sums, counts, width, height):
+    """The film's pixel values: (sum over samples) / count, rgba, as the reference's merge does."""
+    c = np.maximum(counts, 1).astype(np.float64)[:, None]
+    return (sums / c).reshape(height, width, 4)
