@@ -1,9 +1,11 @@
-"""Benchmark of the path-sample hot path on B200: Msamples/s and Mrays/s of the plain megakernel on the 12.3M-triangle
-scene (config 1: 1920x1080, 64 spp, 16 rect lights + environment, depth 12).
+"""Benchmark of the path-sample hot path on B200: Msamples/s and Mrays/s on the 12.3M-triangle scene (config 1:
+1920x1080, 64 spp, 16 rect lights + environment, depth 12), wavefront form against the plain megakernel.
 
-A step renders one whole frame (132,710,400 samples) through the lane API. `value` is device time of the render
-launches (CUDA events on the library's stream, inputs resident in HBM, max over ranks); `e2e` is the same metric
-through the public API with host buffers: chunk upload, render, film download and the sample-count audit every step.
+A step renders one whole frame (132,710,400 samples) through the lane API in the wavefront form. `value` is the
+device time of those launches (CUDA events on the library's stream around the whole launch, film reduction
+included; inputs resident in HBM; max over ranks). The plain megakernel renders the same frame (the same samples, so
+the same image and RMSE) and is reported beside it. `e2e` is the headline through the public API with host buffers:
+chunk upload, render, film download and the sample-count audit every step.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
@@ -28,9 +30,12 @@ sys.path.insert(0, os.path.join(ROOT, "xpu2-foundation_b200"))
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 WORKLOAD = "config 1: heightfield 64x64 tiles x 16x16 quads + 2000 level-4 icospheres (12,337,152 triangles), " \
-           "16 rect lights + env 0.2, 1920x1080, 64 spp, max depth 12, plain megakernel"
+           "16 rect lights + env 0.2, 1920x1080, 64 spp, max depth 12"
 METRIC = "Msamples/s (config 1, 1 frame = 1920x1080x64 samples a step)"
 NODE_BYTES, TRI_BYTES, FILM_BYTES = 80, 48, 36
+# Per ray record bytes the traversal kernels read and write besides the BVH: extend reads a 32-byte ray and writes
+# an 8-byte hit; shadow reads a 32-byte record and writes a 1-byte flag.
+EXTEND_RAY_BYTES, SHADOW_RAY_BYTES = 40, 33
 
 
 def peaks():
@@ -75,12 +80,13 @@ class Clocks:
         except Exception:
             self.proc.kill()
         self.thread.join(timeout=2)
-        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        rows = [r for r in self.rows if len(r) >= 9]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows if len(r) >= 9 for i in range(4) if r[5 + i].lower() == "active"})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
-                "samples": len(self.rows)}
+                "samples": len(rows)}
 
 
 def dist_setup(n):
@@ -114,9 +120,9 @@ def barrier(dist, local):
         torch.cuda.synchronize(local)
 
 
-def cpu_baseline(synthetic, budget_s=15.0, impl_line=False):
+def cpu_baseline(synthetic, budget_s=15.0):
     """The reference's CPU integrator (compiled from its sources) on all host cores, on a bounded sample of the frame:
-    every k-th 8x8 tile at the frame's full spp, k chosen so the run takes about budget_s."""
+    seeded random 8x8 tiles at the frame's full spp, as many as take about budget_s."""
     import oracle_lib
 
     if not oracle_lib.have_reference():
@@ -126,22 +132,21 @@ def cpu_baseline(synthetic, budget_s=15.0, impl_line=False):
     t0 = time.perf_counter()
     ref = oracle_lib.Reference(synthetic)
     build_s = time.perf_counter() - t0
-    tiles_x, tiles_y = (cfg.width + 7) // 8, (cfg.height + 7) // 8
-    tiles = tiles_x * tiles_y
-    probe = np.arange(0, tiles, max(1, tiles // (2 * threads)), dtype=np.uint32)[: 2 * threads]
+    tiles = ((cfg.width + 7) // 8) * ((cfg.height + 7) // 8)
+    order = np.random.default_rng(17).permutation(tiles).astype(np.uint32)
+    probe = order[:threads]
     t0 = time.perf_counter()
-    ref.render_tiles(probe, 0, 4, threads)
-    per_tile = (time.perf_counter() - t0) / len(probe) * (cfg.spp / 4.0)
-    want = max(threads, int(budget_s / max(per_tile, 1e-6) * threads))
-    step = max(1, tiles // want)
-    sample = np.arange(0, tiles, step, dtype=np.uint32)
+    ref.render_tiles(probe, 0, cfg.spp, threads)
+    per_batch = time.perf_counter() - t0  # one tile a thread at full spp
+    batches = max(1, int(budget_s / max(per_batch, 1e-3)))
+    sample = order[threads: threads + min(tiles - threads, batches * threads)]
     t0 = time.perf_counter()
     rc, samples, rays = ref.render_tiles(sample, 0, cfg.spp, threads)
     dt = time.perf_counter() - t0
     ref.close()
     value = samples / dt / 1e6
     return {"value": value, "unit": "Msamples/s", "cores": threads, "kind": "reference",
-            "sample": f"{len(sample)} of {tiles} 8x8 tiles (every {step}th) x {cfg.spp} spp = {samples} samples of the same frame; "
+            "sample": f"{len(sample)} of {tiles} seeded-random 8x8 tiles x {cfg.spp} spp = {samples} samples of the same frame; "
                       f"reference integratePaths compiled from source (-O2 -ffp-contract=off), {threads} std::threads; "
                       f"CPU BVH build {build_s:.1f}s excluded",
             "mrays_per_s": float(rays[0] + rays[1] + rays[2]) / dt / 1e6, "seconds": dt, "rc": rc}, None
@@ -158,8 +163,9 @@ def run_reference(args):
     s = x2.SyntheticScene(1)
     cfg = s.config
     vals, base = [], None
+    per_step = max(2.0, 90.0 / max(1, args.warmup + args.steps))
     for k in range(args.warmup + args.steps):
-        base, why = cpu_baseline(s, budget_s=max(2.0, 60.0 / max(1, args.warmup + args.steps)))
+        base, why = cpu_baseline(s, budget_s=per_step)
         if base is None:
             print(json.dumps({"impl": "reference", "unavailable": why}))
             return
@@ -179,13 +185,21 @@ def run_reference(args):
 
 
 def traffic_from_profile():
-    """The dominant kernel's DRAM bytes per launch from the committed ncu summary, when there is one."""
-    p = os.path.join(ROOT, "profiles", "render_config1_traffic.json")
+    """DRAM bytes per launch of the dominant kernel from the committed ncu summary, when there is one."""
     try:
-        with open(p) as f:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
             return json.load(f)
     except Exception:
-        return None
+        return {}
+
+
+def frame(scene, cfg, first, wavefront):
+    scene.frame_begin(cfg.spp)
+    if wavefront:
+        scene.render_frame_wavefront(first, cfg.spp)
+    else:
+        scene.render_frame(first, cfg.spp)
+    return scene.wait()
 
 
 def run(args):
@@ -203,39 +217,45 @@ def run(args):
     first = rank * cfg.spp  # each rank its own sample indices: distinct samples of the same pixels
     tiles = ((cfg.width + 7) // 8) * ((cfg.height + 7) // 8)
 
-    # Counting run (untimed): node visits and triangle tests of one frame, for the algorithmic bytes.
+    # Untimed: node visits and triangle tests of one frame (counting mode), and the wavefront's per-kernel times.
     scene.count_traversal(True)
-    scene.frame_begin(cfg.spp)
-    scene.render_frame(first, cfg.spp)
-    scene.wait()
+    frame(scene, cfg, first, True)
     tc = scene.traversal_counts()
     scene.count_traversal(False)
+    scene.wavefront_timing(True)
+    frame(scene, cfg, first, True)
+    kms = scene.wavefront_timing(False)
     scene.reset_counters()
 
-    # Device-timed steps: inputs resident, one render launch a step (the film cleared between, not timed).
+    # Device-timed wavefront frames.
     for _ in range(args.warmup):
-        scene.frame_begin(cfg.spp)
-        scene.render_frame(first, cfg.spp)
-        scene.wait()
+        frame(scene, cfg, first, True)
     scene.reset_counters()
     clocks = Clocks(local)
     barrier(dist, local)
     clocks.start()
     ms = []
     for _ in range(args.steps):
-        scene.frame_begin(cfg.spp)
-        scene.render_frame(first, cfg.spp)
-        c = scene.wait()
-        ms.append(c.milliseconds)
+        ms.append(frame(scene, cfg, first, True).milliseconds)
     barrier(dist, local)
     clk = clocks.stop()
     counters = scene.counters()
+    winfo = scene.wavefront_info()
     scene.audit()
     total_ms = max_over_ranks(dist, float(sum(ms)), local)
     ms_per_step = total_ms / args.steps
     value = world * samples_per_frame * args.steps / (total_ms / 1e3) / 1e6
     rays = counters["trace"] + counters["shadow_nee"] + counters["shadow_bsdf"]
-    mrays = world * rays / (sum(ms) / 1e3) / 1e6
+    mrays = world * rays / (total_ms / 1e3) / 1e6
+
+    # The plain megakernel on the same frame (the same samples: same image, same RMSE).
+    plain = None
+    if not args.skip_plain:
+        frame(scene, cfg, first, False)
+        pms = [frame(scene, cfg, first, False).milliseconds for _ in range(args.plain_steps)]
+        pmax = max_over_ranks(dist, float(sum(pms)), local) / len(pms)
+        plain = {"value": world * samples_per_frame / (pmax / 1e3) / 1e6, "unit": "Msamples/s", "ms_per_step": pmax,
+                 "steps": len(pms), "warmup": 1, "mrays_per_s": world * rays / args.steps / (pmax / 1e3) / 1e6}
 
     # End to end through the public API: chunks up, render, film down, audit, every step.
     film_bytes = cfg.width * cfg.height * (4 * 8 + 4)
@@ -244,7 +264,7 @@ def run(args):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         scene.frame_begin(cfg.spp)
-        scene.render_frame(first, cfg.spp)
+        scene.render_frame_wavefront(first, cfg.spp)
         sums, counts = scene.film()
         scene.audit()
     e2e_s = max_over_ranks(dist, time.perf_counter() - t0, local)
@@ -255,39 +275,49 @@ def run(args):
         import torch
 
         ts = torch.from_numpy(sums).cuda(local)
-        tc_ = torch.from_numpy(counts.astype(np.int64)).cuda(local)
+        tcnt = torch.from_numpy(counts.astype(np.int64)).cuda(local)
         dist.reduce(ts, 0)
-        dist.reduce(tc_, 0)
-        if rank == 0 and not bool((tc_ == world * cfg.spp).all()):
+        dist.reduce(tcnt, 0)
+        if rank == 0 and not bool((tcnt == world * cfg.spp).all()):
             raise RuntimeError("merged sample-count audit failed")
 
+    # Roofline of the dominant wavefront kernel: its algorithmic bytes (BVH nodes and triangles its rays visit, and
+    # its ray records) over its time in the per-kernel timed frame.
     hbm, peak_kind = peaks()
-    alg_bytes = tc["nodes"] * NODE_BYTES + tc["triangles"] * TRI_BYTES + samples_per_frame * FILM_BYTES
-    achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
-    prof = traffic_from_profile()
+    per_kernel = {
+        "extend": (tc["closest"]["nodes"] * NODE_BYTES + tc["closest"]["triangles"] * TRI_BYTES + tc["closest"]["rays"] * EXTEND_RAY_BYTES,
+                   kms["extend"]),
+        "shadow": (tc["any"]["nodes"] * NODE_BYTES + tc["any"]["triangles"] * TRI_BYTES + tc["any"]["rays"] * SHADOW_RAY_BYTES, kms["shadow"]),
+    }
+    dominant = max(kms, key=lambda k: kms[k])
+    dom = dominant if dominant in per_kernel else max(per_kernel, key=lambda k: per_kernel[k][1])
+    alg_bytes, dom_ms = per_kernel[dom]
+    launches_per_frame = winfo["iterations"]
+    achieved = alg_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    prof = traffic_from_profile().get(dom, {})
     if rank == 0:
         base, why = cpu_baseline(s) if world == 1 else (None, "rank 0 at N=1 only")
         line = {
             "metric": METRIC, "value": value, "unit": "Msamples/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator, config 1; no dataset)",
-            "config": {"workload": WORKLOAD, "triangles": s.desc.triangle_count, "samples_per_step": samples_per_frame * world,
+            "config": {"workload": WORKLOAD + ", wavefront form", "triangles": s.desc.triangle_count, "samples_per_step": samples_per_frame * world,
                        "l2": "inputs larger than L2 (BVH %.0f MB + triangles %.0f MB > 126 MB)" % (info["bvh_bytes"] / 1e6, info["triangle_bytes"] / 1e6),
-                       "bvh_build_ms": info["build_ms"], "scene_load_s": load_s, "parallelism": f"{world} GPU(s), replicated scene, "
-                       "distinct sample indices a rank"},
+                       "bvh_build_ms": info["build_ms"], "scene_load_s": load_s, "paths_in_flight": winfo["paths"],
+                       "parallelism": f"{world} GPU(s), replicated scene, distinct sample indices a rank"},
             "mrays_per_s": mrays,
-            "rays_per_sample": {"trace": counters["trace"] / (samples_per_frame * args.steps),
-                                "shadow_nee": counters["shadow_nee"] / (samples_per_frame * args.steps),
-                                "shadow_bsdf": counters["shadow_bsdf"] / (samples_per_frame * args.steps),
-                                "held": counters["held"] / (samples_per_frame * args.steps)},
+            "rays_per_sample": {k: counters[c] / (samples_per_frame * args.steps)
+                                for k, c in (("trace", "trace"), ("shadow_nee", "shadow_nee"), ("shadow_bsdf", "shadow_bsdf"), ("held", "held"))},
+            "plain_megakernel": plain,
+            "wavefront_over_plain": (value / plain["value"]) if plain else None,
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": chunk_bytes, "d2h_bytes_per_step": film_bytes},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                         "traffic": (prof or {}).get("dram_bytes_per_launch"), "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": alg_bytes,
-                         "per_launch": {"rays": tc["rays"], "node_visits": tc["nodes"], "triangle_tests": tc["triangles"],
-                                        "node_bytes": NODE_BYTES, "triangle_bytes": TRI_BYTES, "film_bytes_per_sample": FILM_BYTES}},
+            "roofline": {"bound": "hbm", "kernel": "wf" + dom.capitalize(), "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "traffic": prof.get("dram_bytes_per_launch"), "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_frame": alg_bytes, "kernel_ms_per_frame": dom_ms,
+                         "kernel_ms_by_kind": kms, "traversal": tc,
+                         "bytes": {"node": NODE_BYTES, "triangle": TRI_BYTES, "extend_ray": EXTEND_RAY_BYTES, "shadow_ray": SHADOW_RAY_BYTES}},
             "cpu_baseline": base if base else {"value": None, "unavailable": why},
-            "clocks": clk, "gpu_launches": args.steps,
+            "clocks": clk, "gpu_launches": launches_per_frame * 5 * args.steps,
             "errors": counters["errors"], "stack_overflows": counters["stack_overflows"],
         }
         print(json.dumps(line))
@@ -303,9 +333,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="x2", choices=["x2", "reference"])
+    ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--skip-plain", action="store_true")
     args = ap.parse_args()
-    if args.warmup < 3:
-        args.warmup = 3
+    args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference(args)
     else:

@@ -175,6 +175,19 @@ int x2_launch(x2_scene* scene, const x2_chunk* chunks, uint32_t count);   /* lau
 int x2_poll(x2_scene* scene, x2_completion* out);  /* poll(): 1 and *out when a launch finished, 0 if none */
 int x2_wait(x2_scene* scene, int timeout_ms, x2_completion* out);  /* waits for every launch in flight */
 int x2_render_frame(x2_scene* scene, uint32_t first, uint32_t count);  /* every tile, samples [first, first+count) */
+/* The wavefront form of a launch (no counterpart in the reference, whose wavefront was ruled out,
+ * xi/INDEXER.md:161-181): the same samples as x2_launch, by compacted extend / shade / shadow kernels with path
+ * regeneration, replayed as a CUDA graph; the same film. One BSDF sample a lobe (bsdf_samples = 1). Paths in flight:
+ * x2_wavefront_reserve (default 2^20). x2_items_download reads the last wavefront launch's per-item radiance and
+ * status (item = chunk * 64 * samples_per_chunk + position * samples_per_chunk + sample). */
+int x2_wavefront_reserve(x2_scene* scene, uint32_t paths);
+int x2_launch_wavefront(x2_scene* scene, const x2_chunk* chunks, uint32_t count);
+int x2_render_frame_wavefront(x2_scene* scene, uint32_t first, uint32_t count);
+int x2_items_download(x2_scene* scene, float* rgba, uint8_t* status, uint64_t n);  /* waits */
+int x2_wavefront_info(x2_scene* scene, uint32_t* paths, uint32_t* records, uint32_t* iterations);
+/* Per-kernel timing of wavefront launches (a diagnostic: no graph, a host sync an iteration). on: 1 on, 0 off, -1
+ * unchanged; ms (5 floats, or null): the last timed launch's logic, extend, shade, shadow and film-reduce times. */
+int x2_wavefront_timing(x2_scene* scene, int on, float* ms);
 int x2_film_download(x2_scene* scene, double* sums, double* odd, uint32_t* counts);  /* downloadFilm(); waits */
 int x2_film_device(x2_scene* scene, double** d_sums, double** d_odd, uint32_t** d_counts);
 int x2_audit(x2_scene* scene, const uint32_t* expected, int64_t* bad_pixel);  /* async_render.h:992-1048 */
@@ -183,7 +196,8 @@ int x2_counters_reset(x2_scene* scene);
 /* Counting mode (no reference counterpart; the algorithmic-bytes count of the roofline): launches made while it is
  * on count BVH node visits and triangle tests per ray. It slows them: never time a counting launch. */
 int x2_count_traversal(x2_scene* scene, int on);
-int x2_traversal_counts(x2_scene* scene, uint64_t* rays, uint64_t* nodes, uint64_t* triangles);  /* waits; resets */
+/* Each output is two counts: [0] closest-hit rays, [1] any-hit (shadow) rays. Waits; resets the counts. */
+int x2_traversal_counts(x2_scene* scene, uint64_t* rays, uint64_t* nodes, uint64_t* triangles);
 
 /* ---- host-side synthetic scenes (test and bench inputs, not the hot path) ----
  * config_id 0: the closed box with two boxes and a rect light; 1: heightfield + icospheres with 16 rect lights

@@ -170,10 +170,22 @@ inline bool boxHit(const Node& nd, V3 o, V3 inv, float tmin, float tmax) {
     return t0 <= t1;
 }
 
+// The triangle test's t is a convex combination of the vertices' sheared depths, rounded: its absolute error is a
+// few ulps of the distance to the vertices. Boxes are tested against [tmin - eps, tmax + eps], eps = 2^-18 times
+// the origin's distance to the far corner of the scene's bounds, so no box holding an accepted hit is culled.
+inline float rayTolerance(const Scene& s, V3 o) {
+    const Node& root = s.bvh.nodes[0];
+    const float x = std::max(std::fabs(root.lo[0] - o.x), std::fabs(root.hi[0] - o.x));
+    const float y = std::max(std::fabs(root.lo[1] - o.y), std::fabs(root.hi[1] - o.y));
+    const float z = std::max(std::fabs(root.lo[2] - o.z), std::fabs(root.hi[2] - o.z));
+    return (x + y + z) * 0x1p-18f;
+}
+
 // Closest hit on [tmin, tmax]: the nearest t, then the lowest triangle index. Returns ~0u on a miss.
 U32 closest(const Scene& s, V3 o, V3 d, float tmin, float tmax, float& tBest) {
     const TriTest sh = shear(d);
     const V3 inv{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    const float eps = rayTolerance(s, o);
     U32 best = ~0u;
     tBest = tmax;
     U32 stack[128];
@@ -181,7 +193,7 @@ U32 closest(const Scene& s, V3 o, V3 d, float tmin, float tmax, float& tBest) {
     stack[sp++] = 0;
     while (sp) {
         const Node& nd = s.bvh.nodes[stack[--sp]];
-        if (!boxHit(nd, o, inv, tmin, tBest)) continue;
+        if (!boxHit(nd, o, inv, tmin - eps, tBest + eps)) continue;
         if (nd.count) {
             for (U32 i = nd.first; i < nd.first + nd.count; ++i) {
                 const U32 t = s.bvh.order[i];
@@ -202,12 +214,13 @@ U32 closest(const Scene& s, V3 o, V3 d, float tmin, float tmax, float& tBest) {
 bool occluded(const Scene& s, V3 o, V3 d, float tmin, float tmax) {
     const TriTest sh = shear(d);
     const V3 inv{1.0f / d.x, 1.0f / d.y, 1.0f / d.z};
+    const float eps = rayTolerance(s, o);
     U32 stack[128];
     int sp = 0;
     stack[sp++] = 0;
     while (sp) {
         const Node& nd = s.bvh.nodes[stack[--sp]];
-        if (!boxHit(nd, o, inv, tmin, tmax)) continue;
+        if (!boxHit(nd, o, inv, tmin - eps, tmax + eps)) continue;
         if (nd.count) {
             for (U32 i = nd.first; i < nd.first + nd.count; ++i) {
                 const U32 t = s.bvh.order[i];
@@ -606,6 +619,35 @@ int x2ref_trace(void* p, const float* rays, uint64_t n, uint32_t* tri, float* t,
         tri[i] = closest(h->scene, o, d, r[6], r[7], th);
         t[i] = tri[i] == ~0u ? 0.0f : th;
         occl[i] = occluded(h->scene, o, d, r[6], r[7]) ? 1u : 0u;
+    }
+    return X2_OK;
+}
+
+// The same queries by testing every triangle (no BVH): the arbiter when two traversals disagree.
+int x2ref_trace_brute(void* p, const float* rays, uint64_t n, uint32_t* tri, float* t, uint32_t* occl) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h) return X2_EINVAL;
+    const Scene& s = h->scene;
+    const U32 nt = U32(s.tris.size() / 3);
+    for (uint64_t i = 0; i < n; ++i) {
+        const float* r = rays + 8 * i;
+        const V3 o{r[0], r[1], r[2]}, d{r[3], r[4], r[5]};
+        const TriTest sh = shear(d);
+        U32 best = ~0u;
+        float tBest = r[7];
+        bool any = false;
+        for (U32 k = 0; k < nt; ++k) {
+            float th;
+            const V3 a = s.vertex(s.tris[3 * k]), b = s.vertex(s.tris[3 * k + 1]), c = s.vertex(s.tris[3 * k + 2]);
+            if (triHit(sh, o, a, b, c, r[6], r[7], th)) any = true;
+            if (triHit(sh, o, a, b, c, r[6], tBest, th) && (th < tBest || (th == tBest && k < best))) {
+                tBest = th;
+                best = k;
+            }
+        }
+        tri[i] = best;
+        t[i] = best == ~0u ? 0.0f : tBest;
+        occl[i] = any ? 1u : 0u;
     }
     return X2_OK;
 }

@@ -112,13 +112,16 @@ class Reference:
                                          rays.ctypes.data)
         return rc, int(samples[0]), rays
 
-    def trace(self, rays):
+    def trace(self, rays, brute=False):
+        """Closest hit (triangle, t) and occlusion through the oracle's BVH, or by testing every triangle."""
         rays = np.ascontiguousarray(rays, np.float32)
         n = len(rays)
         tri = np.empty(n, np.uint32)
         t = np.empty(n, np.float32)
         occ = np.empty(n, np.uint32)
-        self.lib.x2ref_trace(self.h, rays.ctypes.data, n, tri.ctypes.data, t.ctypes.data, occ.ctypes.data)
+        f = self.lib.x2ref_trace_brute if brute else self.lib.x2ref_trace
+        f.argtypes = [C.c_void_p] * 2 + [C.c_uint64] + [C.c_void_p] * 3
+        f(self.h, rays.ctypes.data, n, tri.ctypes.data, t.ctypes.data, occ.ctypes.data)
         return tri, t, occ
 
 

@@ -89,10 +89,26 @@ def test_traversal_matches_oracle(which, box, field):
     tri, t, occ = scene.trace_rays(rays)
     ref = oracle_lib.Reference(s)
     rtri, rt, rocc = ref.trace(rays)
-    assert np.array_equal(tri, rtri)
+    bad = np.flatnonzero((tri != rtri) | (occ != rocc))
+    if len(bad):
+        btri, bt, bocc = ref.trace(rays[bad[:50]], brute=True)
+        rows = [f"ray {i} {rays[i].tolist()}: device ({tri[i]}, {t[i]!r}, {occ[i]}) oracle ({rtri[i]}, {rt[i]!r}, {rocc[i]}) "
+                f"brute ({b}, {bb!r}, {o})" for i, b, bb, o in zip(bad[:5], btri, bt, bocc)]
+        pytest.fail(f"{len(bad)} of {len(rays)} rays differ:\n" + "\n".join(rows))
     assert np.array_equal(t[tri != 0xFFFFFFFF], rt[rtri != 0xFFFFFFFF])
-    assert np.array_equal(occ, rocc)
     assert scene.counters()["stack_overflows"] == 0
+
+
+@needs_reference
+def test_oracle_traversal_matches_brute_force(box):
+    """The oracle's own BVH against testing every triangle (the box scene's 34)."""
+    s, _ = box
+    rays = np.concatenate([random_rays(s.desc, 20000, 3), random_rays(s.desc, 20000, 4, shadow=True)])
+    ref = oracle_lib.Reference(s)
+    a = ref.trace(rays)
+    b = ref.trace(rays, brute=True)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
 
 
 # ---- per-sample radiance ----

@@ -14,6 +14,7 @@
 #include "../../include/x2.h"
 #include "engine.h"
 #include "render.h"
+#include "wavefront.h"
 
 namespace x2 {
 
@@ -137,13 +138,28 @@ struct x2_scene {
     unsigned long long* auditWord = nullptr;
     TraversalStats* stats = nullptr;  // device
     bool counting = false;
+    float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};  // the vertices' bounds
+    // wavefront
+    WaveState wave{};
+    uint32_t wavePaths = 0, waveRecords = 0, reservePaths = 0;
+    uint32_t* extendQ = nullptr;
+    uint32_t* shadowQ = nullptr;
+    uint32_t* waveCounters = nullptr;  // extend count, last extend count, shadow count
+    uint32_t* hostLast = nullptr;      // pinned
+    unsigned long long* claimed = nullptr;
+    float4* out = nullptr;
+    uint8_t* outStatus = nullptr;
+    uint64_t outCap = 0, lastItems = 0;
+    uint32_t waveIterations = 0;       // of the last wavefront launch
+    bool waveTiming = false;           // time each kernel kind (no graph)
+    float waveMs[5] = {0, 0, 0, 0, 0}; // logic, extend, shade, shadow, film reduce
 };
 
 namespace {
 
 SceneView viewOf(const x2_scene* s) {
     SceneView v;
-    v.bvh = Bvh8{s->bvh.nodes, s->bvh.tris, s->bvh.nodeCount, s->bvh.triCount};
+    v.bvh = Bvh8{s->bvh.nodes, s->bvh.tris, s->bvh.nodeCount, s->bvh.triCount, {s->lo[0], s->lo[1], s->lo[2]}, {s->hi[0], s->hi[1], s->hi[2]}};
     v.triMesh = s->triMesh;
     v.meshFirst = s->meshFirst;
     v.meshMaterial = s->meshMaterial;
@@ -218,6 +234,60 @@ void retire(x2_scene* s, Slot& sl, x2_completion* out) {
     sl.busy = false;
 }
 
+void freeWave(x2_scene* s) {
+    WaveState& w = s->wave;
+    void* ptrs[] = {w.ray0, w.ray1, w.T, w.held, w.meta, w.branch, w.rad, w.hit, w.state, w.item, w.ncount, w.sray0, w.sray1, w.scontrib, w.svis};
+    for (void* p : ptrs) cudaFree(p);
+    w = WaveState{};
+    cudaFree(s->extendQ);
+    cudaFree(s->shadowQ);
+    s->extendQ = s->shadowQ = nullptr;
+    s->wavePaths = s->waveRecords = 0;
+}
+
+// Path slots for `paths` paths with `records` shadow records each.
+int ensureWave(x2_scene* s, uint32_t paths, uint32_t records) {
+    if (s->wavePaths == paths && s->waveRecords == records) return X2_OK;
+    freeWave(s);
+    WaveState& w = s->wave;
+    const size_t P = paths, R = size_t(paths) * records;
+    bool ok = cudaMalloc(&w.ray0, sizeof(float4) * P) == cudaSuccess && cudaMalloc(&w.ray1, sizeof(float4) * P) == cudaSuccess &&
+              cudaMalloc(&w.T, sizeof(float4) * P) == cudaSuccess && cudaMalloc(&w.held, sizeof(float4) * P) == cudaSuccess &&
+              cudaMalloc(&w.meta, sizeof(uint4) * P) == cudaSuccess && cudaMalloc(&w.branch, sizeof(uint2) * P) == cudaSuccess &&
+              cudaMalloc(&w.rad, sizeof(float4) * P) == cudaSuccess && cudaMalloc(&w.hit, sizeof(uint2) * P) == cudaSuccess &&
+              cudaMalloc(&w.state, sizeof(uint32_t) * P) == cudaSuccess && cudaMalloc(&w.item, sizeof(uint32_t) * P) == cudaSuccess &&
+              cudaMalloc(&w.ncount, sizeof(uint32_t) * P) == cudaSuccess && cudaMalloc(&w.sray0, sizeof(float4) * R) == cudaSuccess &&
+              cudaMalloc(&w.sray1, sizeof(float4) * R) == cudaSuccess && cudaMalloc(&w.scontrib, sizeof(float4) * R) == cudaSuccess &&
+              cudaMalloc(&w.svis, R) == cudaSuccess && cudaMalloc(&s->extendQ, sizeof(uint32_t) * P) == cudaSuccess &&
+              cudaMalloc(&s->shadowQ, sizeof(uint32_t) * R) == cudaSuccess;
+    if (ok && !s->waveCounters) ok = cudaMalloc(&s->waveCounters, sizeof(uint32_t) * 4) == cudaSuccess;
+    if (ok && !s->claimed) ok = cudaMalloc(&s->claimed, sizeof(unsigned long long)) == cudaSuccess;
+    if (ok && !s->hostLast) ok = cudaMallocHost(&s->hostLast, sizeof(uint32_t) * 4) == cudaSuccess;
+    if (!ok) {
+        freeWave(s);
+        setError("device allocation failed for %u wavefront paths", paths);
+        return X2_ENOMEM;
+    }
+    s->wavePaths = paths;
+    s->waveRecords = records;
+    return X2_OK;
+}
+
+int ensureItems(x2_scene* s, uint64_t items) {
+    if (items <= s->outCap) return X2_OK;
+    cudaFree(s->out);
+    cudaFree(s->outStatus);
+    s->out = nullptr;
+    s->outStatus = nullptr;
+    s->outCap = 0;
+    if (cudaMalloc(&s->out, sizeof(float4) * items) != cudaSuccess || cudaMalloc(&s->outStatus, items) != cudaSuccess) {
+        setError("device allocation failed for %llu item outputs", (unsigned long long)items);
+        return X2_ENOMEM;
+    }
+    s->outCap = items;
+    return X2_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -246,7 +316,7 @@ int x2_open(int device, x2_ctx** out) {
     }
     uint32_t dirs[17][32];
     sobolDirections(dirs);
-    if (uploadSobol(dirs) != cudaSuccess) {
+    if (uploadSobol(dirs) != cudaSuccess || uploadSobolWavefront(dirs) != cudaSuccess) {
         setError("sobol table upload failed");
         cudaStreamDestroy(ctx->stream);
         delete ctx;
@@ -368,6 +438,16 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
     auto* s = new x2_scene();
     s->ctx = ctx;
     s->camera = d->camera;
+    for (int k = 0; k < 3; ++k) {
+        s->lo[k] = 3.402823466e38f;
+        s->hi[k] = -3.402823466e38f;
+    }
+    for (uint64_t i = 0; i < uint64_t(d->triangle_count) * 3; ++i)
+        for (int k = 0; k < 3; ++k) {
+            const float v = d->vertices[3 * size_t(d->triangles[i]) + k];
+            s->lo[k] = v < s->lo[k] ? v : s->lo[k];
+            s->hi[k] = v > s->hi[k] ? v : s->hi[k];
+        }
     s->lightCount = d->light_count;
     s->triangleCount = d->triangle_count;
     cudaStream_t st = ctx->stream;
@@ -403,7 +483,7 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
         cudaMalloc(&s->materials, sizeof(MaterialRec) * (d->material_count ? d->material_count : 1)) != cudaSuccess ||
         cudaMalloc(&s->lights, sizeof(x2_light) * (d->light_count ? d->light_count : 1)) != cudaSuccess ||
         cudaMalloc(&s->overflow, sizeof(uint32_t)) != cudaSuccess || cudaMalloc(&s->auditWord, sizeof(unsigned long long)) != cudaSuccess ||
-        cudaMalloc(&s->stats, sizeof(TraversalStats)) != cudaSuccess) {
+        cudaMalloc(&s->stats, 2 * sizeof(TraversalStats)) != cudaSuccess) {
         setError("device allocation failed for the scene");
         return fail(X2_ENOMEM);
     }
@@ -415,7 +495,7 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
     cudaMemcpyAsync(s->materials, mats.data(), sizeof(MaterialRec) * d->material_count, cudaMemcpyHostToDevice, st);
     if (d->light_count) cudaMemcpyAsync(s->lights, d->lights, sizeof(x2_light) * d->light_count, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(s->overflow, 0, sizeof(uint32_t), st);
-    cudaMemsetAsync(s->stats, 0, sizeof(TraversalStats), st);
+    cudaMemsetAsync(s->stats, 0, 2 * sizeof(TraversalStats), st);
     cudaEventRecord(b0, st);
     if (buildBvh(dVerts, dTris, d->triangle_count, st, &s->bvh) != 0) return fail(X2_ECUDA);
     cudaEventRecord(b1, st);
@@ -446,6 +526,14 @@ int x2_scene_free(x2_scene* s) {
     cudaFree(s->overflow);
     cudaFree(s->auditWord);
     cudaFree(s->stats);
+    freeWave(s);
+    cudaFree(s->out);
+    cudaFree(s->outStatus);
+    cudaFree(s->extendQ);
+    cudaFree(s->shadowQ);
+    cudaFree(s->waveCounters);
+    cudaFree(s->claimed);
+    if (s->hostLast) cudaFreeHost(s->hostLast);
     cudaFree(s->sums);
     cudaFree(s->odd);
     cudaFree(s->counts);
@@ -723,6 +811,231 @@ int x2_render_frame(x2_scene* s, uint32_t first, uint32_t count) {
     return x2_launch(s, s->staging, tiles);
 }
 
+int x2_wavefront_reserve(x2_scene* s, uint32_t paths) {
+    if (!s) return X2_EINVAL;
+    s->reservePaths = paths;
+    return X2_OK;
+}
+
+int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
+    if (!s || !s->configured || !s->filmPixels || !s->samplesPerChunk) {
+        setError("x2_frame_begin first");
+        return X2_EINVAL;
+    }
+    if (s->config.bsdf_samples != 1) {
+        setError("the wavefront form takes one BSDF sample a lobe (bsdf_samples = 1)");
+        return X2_EINVAL;
+    }
+    if (int rc = checkDevice(s->ctx)) return rc;
+    if (!count) return X2_OK;
+    if (!chunks) return X2_EINVAL;
+    const uint32_t tiles = ((s->config.width + 7) / 8) * ((s->config.height + 7) / 8);
+    for (uint32_t i = 0; i < count; ++i)
+        if (chunks[i].tile >= tiles || chunks[i].count > s->samplesPerChunk) {
+            setError("chunk %u: tile %u of %u or count %u over %u samples a chunk", i, chunks[i].tile, tiles, chunks[i].count,
+                     s->samplesPerChunk);
+            return X2_EINVAL;
+        }
+    // Every earlier launch has finished: the wavefront's host loop waits on the stream anyway.
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    Slot& sl = s->slots[0];
+    if (int rc = ensureSlot(sl, count)) return rc;
+    const unsigned long long items = (unsigned long long)count * 64ull * s->samplesPerChunk;
+    if (items > 0xffffffffull) {
+        setError("%llu work items in one wavefront launch (at most 2^32 - 1)", items);
+        return X2_EINVAL;
+    }
+    uint32_t paths = s->reservePaths ? s->reservePaths : (1u << 20);
+    if (paths > items) paths = uint32_t(items < 1024 ? 1024 : items);
+    const uint32_t records = s->config.light_count * s->config.light_samples + 1;
+    if (int rc = ensureWave(s, paths, records)) return rc;
+    if (int rc = ensureItems(s, items)) return rc;
+    cudaStream_t st = s->ctx->stream;
+    CUDA_OR(cudaMemcpyAsync(sl.chunks, chunks, sizeof(x2_chunk) * count, cudaMemcpyHostToDevice, st), X2_ECUDA);
+    cudaMemsetAsync(s->wave.state, 0, sizeof(uint32_t) * paths, st);
+    cudaMemsetAsync(s->wave.ncount, 0, sizeof(uint32_t) * paths, st);
+    cudaMemsetAsync(s->claimed, 0, sizeof(unsigned long long), st);
+    cudaMemsetAsync(s->waveCounters, 0, sizeof(uint32_t) * 4, st);
+    cudaMemsetAsync(sl.counters, 0, sizeof(Counters), st);
+    cudaMemsetAsync(s->outStatus, X2_SKIP, items, st);
+    WaveArgs a;
+    a.scene = viewOf(s);
+    a.w = s->wave;
+    a.paths = paths;
+    a.recordsPerPath = records;
+    a.chunks = sl.chunks;
+    a.itemCount = items;
+    a.samplesPerChunk = s->samplesPerChunk;
+    a.claimed = s->claimed;
+    a.extendQ = s->extendQ;
+    a.extendCount = s->waveCounters;
+    a.lastExtend = s->waveCounters + 1;
+    a.shadowQ = s->shadowQ;
+    a.shadowCount = s->waveCounters + 2;
+    a.out = s->out;
+    a.outStatus = s->outStatus;
+    a.counters = sl.counters;
+    const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
+    const int gridWork = s->ctx->smCount * 16;
+    const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
+    if (s->waveTiming) {
+        // Diagnostic form: no graph; events around every kernel, the iteration's times added once it is done.
+        cudaEvent_t ev[6];
+        for (auto& e : ev) cudaEventCreate(&e);
+        for (float& m : s->waveMs) m = 0.0f;
+        cudaEventRecord(sl.begin, st);
+        uint32_t iterations = 0;
+        int rc = X2_OK;
+        for (;;) {
+            wfResetQueues<<<1, 32, 0, st>>>(a);
+            cudaEventRecord(ev[0], st);
+            wfLogic<<<gridLogic, kWaveBlock, 0, st>>>(a);
+            cudaEventRecord(ev[1], st);
+            wfExtend<<<gridWork, kWaveBlock, 0, st>>>(a);
+            cudaEventRecord(ev[2], st);
+            wfShade<<<gridWork, kWaveBlock, 0, st>>>(a);
+            cudaEventRecord(ev[3], st);
+            wfShadow<<<gridWork, kWaveBlock, 0, st>>>(a);
+            cudaEventRecord(ev[4], st);
+            wfResetQueues<<<1, 32, 0, st>>>(a);
+            cudaMemcpyAsync(s->hostLast, s->waveCounters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            if ((rc = x2_synchronize(s->ctx, 600000)) != X2_OK) break;
+            for (int k = 0; k < 4; ++k) {
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+                s->waveMs[k] += ms;
+            }
+            ++iterations;
+            if (s->hostLast[0] == 0) break;
+            if (iterations > maxIter) {
+                setError("wavefront did not drain after %u iterations", iterations);
+                rc = X2_EDEVICE;
+                break;
+            }
+        }
+        if (rc == X2_OK) {
+            cudaEventRecord(ev[0], st);
+            wfFilmReduce<<<int((64ull * count + 255) / 256), 256, 0, st>>>(a, count, s->sums, s->adaptive ? s->odd : nullptr, s->counts);
+            cudaEventRecord(ev[5], st);
+            cudaEventRecord(sl.end, st);
+            cudaMemcpyAsync(sl.hostCounters, sl.counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+            cudaEventRecord(sl.done, st);
+            rc = x2_synchronize(s->ctx, 600000);
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, ev[0], ev[5]);
+            s->waveMs[4] = ms;
+        }
+        for (auto& e : ev) cudaEventDestroy(e);
+        if (rc) return rc;
+        sl.busy = true;
+        sl.seq = s->nextSeq++;
+        s->lastItems = items;
+        s->waveIterations = iterations;
+        return X2_OK;
+    }
+    // One graph of kIter iterations, replayed until no path is left to trace.
+    constexpr int kIter = 8;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    CUDA_OR(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), X2_ECUDA);
+    for (int it = 0; it < kIter; ++it) {
+        wfResetQueues<<<1, 32, 0, st>>>(a);
+        wfLogic<<<gridLogic, kWaveBlock, 0, st>>>(a);
+        wfExtend<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wfShade<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wfShadow<<<gridWork, kWaveBlock, 0, st>>>(a);
+    }
+    wfResetQueues<<<1, 32, 0, st>>>(a);  // the last iteration's extend count, for the host
+    CUDA_OR(cudaStreamEndCapture(st, &graph), X2_ECUDA);
+    if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+        cudaGraphDestroy(graph);
+        setError("graph instantiation failed");
+        return X2_ECUDA;
+    }
+    cudaEventRecord(sl.begin, st);
+    uint32_t iterations = 0;
+    int rc = X2_OK;
+    for (;;) {
+        if (cudaGraphLaunch(exec, st) != cudaSuccess) {
+            setError("graph launch failed");
+            rc = X2_ECUDA;
+            break;
+        }
+        iterations += kIter;
+        cudaMemcpyAsync(s->hostLast, s->waveCounters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if ((rc = x2_synchronize(s->ctx, 600000)) != X2_OK) break;
+        if (s->hostLast[0] == 0) break;
+        if (iterations > maxIter) {
+            setError("wavefront did not drain after %u iterations", iterations);
+            rc = X2_EDEVICE;
+            break;
+        }
+    }
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (rc) return rc;
+    wfFilmReduce<<<int((64ull * count + 255) / 256), 256, 0, st>>>(a, count, s->sums, s->adaptive ? s->odd : nullptr, s->counts);
+    CUDA_OR(cudaGetLastError(), X2_ECUDA);
+    cudaEventRecord(sl.end, st);
+    // The extend kernels counted the traced rays; the launch's counters go to the host as x2_launch's do.
+    cudaMemcpyAsync(sl.hostCounters, sl.counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+    cudaEventRecord(sl.done, st);
+    sl.busy = true;
+    sl.seq = s->nextSeq++;
+    s->lastItems = items;
+    s->waveIterations = iterations;
+    return X2_OK;
+}
+
+int x2_render_frame_wavefront(x2_scene* s, uint32_t first, uint32_t count) {
+    if (!s || !s->configured) return X2_EINVAL;
+    if (!s->filmPixels || s->samplesPerChunk < count) {
+        setError("x2_frame_begin with at least %u samples a chunk first", count);
+        return X2_EINVAL;
+    }
+    const uint32_t tiles = ((s->config.width + 7) / 8) * ((s->config.height + 7) / 8);
+    if (int rc = x2_synchronize(s->ctx, 600000)) return rc;
+    if (tiles > s->stagingCap) {
+        if (s->staging) cudaFreeHost(s->staging);
+        s->staging = nullptr;
+        CUDA_OR(cudaMallocHost(&s->staging, sizeof(x2_chunk) * tiles), X2_ENOMEM);
+        s->stagingCap = tiles;
+    }
+    for (uint32_t t = 0; t < tiles; ++t) s->staging[t] = x2_chunk{t, first, count, 0};
+    return x2_launch_wavefront(s, s->staging, tiles);
+}
+
+int x2_items_download(x2_scene* s, float* rgba, uint8_t* status, uint64_t n) {
+    if (!s || !s->out) {
+        setError("no wavefront launch yet");
+        return X2_EINVAL;
+    }
+    if (n > s->lastItems) {
+        setError("%llu items asked, the last launch had %llu", (unsigned long long)n, (unsigned long long)s->lastItems);
+        return X2_EINVAL;
+    }
+    cudaStream_t st = s->ctx->stream;
+    if (rgba) cudaMemcpyAsync(rgba, s->out, sizeof(float4) * n, cudaMemcpyDeviceToHost, st);
+    if (status) cudaMemcpyAsync(status, s->outStatus, n, cudaMemcpyDeviceToHost, st);
+    return x2_wait(s, 600000, nullptr);
+}
+
+int x2_wavefront_timing(x2_scene* s, int on, float* ms) {
+    if (!s) return X2_EINVAL;
+    if (ms)
+        for (int k = 0; k < 5; ++k) ms[k] = s->waveMs[k];
+    if (on >= 0) s->waveTiming = on != 0;
+    return X2_OK;
+}
+
+int x2_wavefront_info(x2_scene* s, uint32_t* paths, uint32_t* records, uint32_t* iterations) {
+    if (!s) return X2_EINVAL;
+    if (paths) *paths = s->wavePaths;
+    if (records) *records = s->waveRecords;
+    if (iterations) *iterations = s->waveIterations;
+    return X2_OK;
+}
+
 int x2_film_device(x2_scene* s, double** sums, double** odd, uint32_t** counts) {
     if (!s || !s->filmPixels) return X2_EINVAL;
     if (sums) *sums = s->sums;
@@ -795,12 +1108,14 @@ int x2_count_traversal(x2_scene* s, int on) {
 int x2_traversal_counts(x2_scene* s, uint64_t* rays, uint64_t* nodes, uint64_t* triangles) {
     if (!s) return X2_EINVAL;
     if (int rc = x2_wait(s, 600000, nullptr)) return rc;
-    TraversalStats h{};
-    CUDA_OR(cudaMemcpy(&h, s->stats, sizeof(h), cudaMemcpyDeviceToHost), X2_ECUDA);
+    TraversalStats h[2]{};
+    CUDA_OR(cudaMemcpy(h, s->stats, sizeof(h), cudaMemcpyDeviceToHost), X2_ECUDA);
     CUDA_OR(cudaMemset(s->stats, 0, sizeof(h)), X2_ECUDA);
-    if (rays) *rays = h.rays;
-    if (nodes) *nodes = h.nodes;
-    if (triangles) *triangles = h.tris;
+    for (int k = 0; k < 2; ++k) {
+        if (rays) rays[k] = h[k].rays;
+        if (nodes) nodes[k] = h[k].nodes;
+        if (triangles) triangles[k] = h[k].tris;
+    }
     return X2_OK;
 }
 

@@ -34,6 +34,7 @@ struct Bvh8 {
     const Node8* nodes;
     const TriRec* tris;
     uint32_t nodeCount, triCount;
+    float lo[3], hi[3];  // the scene's bounds, for each ray's distance tolerance (traverse.cuh, makeRay)
 };
 
 }  // namespace x2

@@ -169,7 +169,7 @@ __global__ void traceRays(SceneView s, const float* __restrict__ rays, unsigned 
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const float* r = rays + 8 * i;
-        const RayQ q = makeRay(r[0], r[1], r[2], r[3], r[4], r[5]);
+        const RayQ q = makeRay(s.bvh, r[0], r[1], r[2], r[3], r[4], r[5]);
         float th;
         uint32_t leaf;
         const uint32_t id = traceClosest<false>(s.bvh, q, r[6], r[7], th, &leaf, s.overflow, nullptr);

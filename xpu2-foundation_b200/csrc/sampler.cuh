@@ -14,8 +14,8 @@ namespace x2 {
 typedef uint32_t U32;
 typedef uint64_t U64;
 
-// One copy a translation unit (whole-program compilation); the kernels live in render.cu, whose copy
-// uploadSobol (render.cu) fills.
+// One copy a translation unit (whole-program compilation): every unit with sampling kernels (render.cu,
+// wavefront.cu) exports an upload function that x2_open calls for its copy.
 static __constant__ U32 c_sobol[17][32];
 
 struct Identity {

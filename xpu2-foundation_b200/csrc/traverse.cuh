@@ -25,12 +25,23 @@ struct RayQ {
     uint32_t oct7;     // XOR pattern that orders a node's slots near to far
     int kx, ky, kz;    // the shear's axes
     float Sx, Sy, Sz;
+    // The triangle test's t carries an absolute error of a few ulps of the distance to the vertices (its sheared
+    // products cancel), which a near hit can make large relative to t: boxes are tested against [tmin - eps,
+    // tmax + eps], eps = 2^-18 times the ray origin's distance to the farthest corner of the scene's bounds.
+    float eps;
 };
 
 __device__ __forceinline__ float pick3(float x, float y, float z, int k) { return k == 0 ? x : (k == 1 ? y : z); }
 
-__device__ __forceinline__ RayQ makeRay(float ox, float oy, float oz, float dx, float dy, float dz) {
+__device__ __forceinline__ float rayTolerance(const Bvh8& b, float ox, float oy, float oz) {
+    const float x = fmaxf(fabsf(b.lo[0] - ox), fabsf(b.hi[0] - ox)), y = fmaxf(fabsf(b.lo[1] - oy), fabsf(b.hi[1] - oy)),
+                z = fmaxf(fabsf(b.lo[2] - oz), fabsf(b.hi[2] - oz));
+    return (x + y + z) * 0x1p-18f;
+}
+
+__device__ __forceinline__ RayQ makeRay(const Bvh8& bvh, float ox, float oy, float oz, float dx, float dy, float dz) {
     RayQ r;
+    r.eps = rayTolerance(bvh, ox, oy, oz);
     r.ox = ox;
     r.oy = oy;
     r.oz = oz;
@@ -110,6 +121,11 @@ __device__ __forceinline__ uint32_t visitNode(const Node8* __restrict__ nodes, u
     triBase = n1.y;
     const float sx = __uint_as_float(ex << 23) * r.ix, sy = __uint_as_float(ey << 23) * r.iy, sz = __uint_as_float(ez << 23) * r.iz;
     const float ax = (px - r.ox) * r.ix, ay = (py - r.oy) * r.iy, az = (pz - r.oz) * r.iz;
+    // The slab distances q * s + a carry an absolute error of a few ulps of their terms (not of their result, which
+    // can be much smaller): widen by (|a| + 255 |s|) * 2^-21 each way, folded into the constant term.
+    const float wx = (fabsf(ax) + 255.0f * fabsf(sx)) * 0x1p-21f, wy = (fabsf(ay) + 255.0f * fabsf(sy)) * 0x1p-21f,
+                wz = (fabsf(az) + 255.0f * fabsf(sz)) * 0x1p-21f;
+    const float axn = ax - wx, axf = ax + wx, ayn = ay - wy, ayf = ay + wy, azn = az - wz, azf = az + wz;
     const bool fx = r.ix >= 0.0f, fy = r.iy >= 0.0f, fz = r.iz >= 0.0f;
     uint32_t hits = 0;
 #pragma unroll
@@ -117,9 +133,9 @@ __device__ __forceinline__ uint32_t visitNode(const Node8* __restrict__ nodes, u
         const uint32_t meta = byteOf(n1.z, n1.w, s);
         const float qlx = float(byteOf(n2.x, n2.y, s)), qly = float(byteOf(n2.z, n2.w, s)), qlz = float(byteOf(n3.x, n3.y, s));
         const float qhx = float(byteOf(n3.z, n3.w, s)), qhy = float(byteOf(n4.x, n4.y, s)), qhz = float(byteOf(n4.z, n4.w, s));
-        const float nx = __fmaf_rn(fx ? qlx : qhx, sx, ax), fxx = __fmaf_rn(fx ? qhx : qlx, sx, ax);
-        const float ny = __fmaf_rn(fy ? qly : qhy, sy, ay), fyy = __fmaf_rn(fy ? qhy : qly, sy, ay);
-        const float nz = __fmaf_rn(fz ? qlz : qhz, sz, az), fzz = __fmaf_rn(fz ? qhz : qlz, sz, az);
+        const float nx = __fmaf_rn(fx ? qlx : qhx, sx, axn), fxx = __fmaf_rn(fx ? qhx : qlx, sx, axf);
+        const float ny = __fmaf_rn(fy ? qly : qhy, sy, ayn), fyy = __fmaf_rn(fy ? qhy : qly, sy, ayf);
+        const float nz = __fmaf_rn(fz ? qlz : qhz, sz, azn), fzz = __fmaf_rn(fz ? qhz : qlz, sz, azf);
         float entry = fmaxf(nx, fmaxf(ny, nz)), exit = fminf(fxx, fminf(fyy, fzz));
         entry = __fsub_rn(entry, fabsf(entry) * 0x1p-20f);
         exit = __fadd_rn(exit, fabsf(exit) * 0x1p-20f);
@@ -159,7 +175,7 @@ static __device__ __noinline__ uint32_t traceClosest(const Bvh8 bvh, const RayQ&
                 else atomicAdd(overflow, 1u);
             }
             uint32_t childBase, triBase, imask;
-            const uint32_t hits = visitNode(bvh.nodes, child, r, tmin, tBest, childBase, triBase, imask);
+            const uint32_t hits = visitNode(bvh.nodes, child, r, tmin - r.eps, tBest + r.eps, childBase, triBase, imask);
             if (kStats) ++nodes;
             uint32_t tBits = hits & 0x00ffffffu;
             while (tBits) {
@@ -217,7 +233,7 @@ static __device__ __noinline__ bool traceAny(const Bvh8 bvh, const RayQ& r, floa
                 else atomicAdd(overflow, 1u);
             }
             uint32_t childBase, triBase, imask;
-            const uint32_t hits = visitNode(bvh.nodes, child, r, tmin, tmax, childBase, triBase, imask);
+            const uint32_t hits = visitNode(bvh.nodes, child, r, tmin - r.eps, tmax + r.eps, childBase, triBase, imask);
             if (kStats) ++nodes;
             uint32_t tBits = hits & 0x00ffffffu;
             while (tBits) {

@@ -1,0 +1,365 @@
+// The wavefront form of the path tracer: the same samples as the plain megakernel, split into small kernels that each
+// run one kind of work over compacted queues, with path regeneration.
+//
+// Path state lives in HBM, structure of arrays, one slot a path in flight (P slots). One iteration:
+//   logic   each slot: add the previous vertex's unoccluded shadow-ray contributions in the reference's order
+//           (light samples in light order, then the BSDF sample's), write a finished sample to the per-item output,
+//           claim a new sample for an empty slot (regeneration: a camera ray), and append every slot with a ray to
+//           trace to the extend queue (warp-aggregated atomics);
+//   extend  closest hit of every queued ray (traverse.cuh);
+//   shade   each queued path's vertex (integrator.cuh shadeVertex): its shadow rays go to fixed per-path record slots
+//           and, by one warp-aggregated reservation a warp, to the shadow queue; its child becomes the slot's ray;
+//   shadow  any hit of every queued shadow ray, a visibility flag each.
+// Iterations are captured once as a CUDA graph and replayed until every item is done. The per-item output (rgb,
+// alpha, status) is then summed into the film in sample order by filmReduce, so the film does not depend on the
+// order paths finish in.
+#include "integrator.cuh"
+#include "wavefront.h"
+
+namespace x2 {
+
+enum : uint32_t { kEmpty = 0, kTrace = 1, kDone = 2, kError = 3 };
+
+// This translation unit's copy of the Sobol direction table (sampler.cuh): filled at x2_open like render.cu's.
+cudaError_t uploadSobolWavefront(const uint32_t directions[17][32]) {
+    return cudaMemcpyToSymbol(c_sobol, directions, sizeof(uint32_t) * 17 * 32);
+}
+
+namespace {
+
+__device__ __forceinline__ uint32_t tilePixelW(uint32_t tile, uint32_t position, uint32_t width, uint32_t height) {
+    const uint32_t tilesX = (width + 7) / 8;
+    const uint32_t x = (tile % tilesX) * 8 + position % 8;
+    const uint32_t y = (tile / tilesX) * 8 + position / 8;
+    return x < width && y < height ? y * width + x : ~0u;
+}
+
+// Warp-aggregated append: each lane with `want` items gets a contiguous range; one atomic a warp. Every lane of the
+// warp must call it (the callers' loops keep their warps whole).
+__device__ __forceinline__ uint32_t warpReserve(uint32_t* counter, uint32_t want) {
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t incl = want;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+        const uint32_t v = __shfl_up_sync(full, incl, off);
+        if (lane >= uint32_t(off)) incl += v;
+    }
+    const uint32_t total = __shfl_sync(full, incl, 31);
+    uint32_t base = 0;
+    if (lane == 31 && total) base = atomicAdd(counter, total);
+    base = __shfl_sync(full, base, 31);
+    return base + incl - want;
+}
+
+__device__ __forceinline__ void warpAddCounters(Counters* dst, unsigned long long trace, unsigned long long nee, unsigned long long bsdf,
+                                                unsigned long long held, unsigned long long samples, unsigned long long errors) {
+    const unsigned full = 0xffffffffu;
+#pragma unroll
+    for (int off = 16; off; off >>= 1) {
+        trace += __shfl_down_sync(full, trace, off);
+        nee += __shfl_down_sync(full, nee, off);
+        bsdf += __shfl_down_sync(full, bsdf, off);
+        held += __shfl_down_sync(full, held, off);
+        samples += __shfl_down_sync(full, samples, off);
+        errors += __shfl_down_sync(full, errors, off);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (trace) atomicAdd(&dst->trace, trace);
+        if (nee) atomicAdd(&dst->nee, nee);
+        if (bsdf) atomicAdd(&dst->bsdf, bsdf);
+        if (held) atomicAdd(&dst->held, held);
+        if (samples) atomicAdd(&dst->samples, samples);
+        if (errors) atomicAdd(&dst->errors, errors);
+    }
+}
+
+__device__ __forceinline__ uint32_t packDepths(const Pending& p) {
+    return (p.depth & 0xffu) | ((p.nonMirror & 0xffu) << 8) | ((p.diffuse & 0xffu) << 16) | ((p.glossy & 0xffu) << 24);
+}
+
+__device__ __forceinline__ void loadPending(const WaveState& w, uint32_t p, Pending& pv) {
+    const float4 r0 = w.ray0[p], r1 = w.ray1[p], T = w.T[p], h = w.held[p];
+    const uint4 m = w.meta[p];
+    pv.origin = V3{r0.x, r0.y, r0.z};
+    pv.nearT = r0.w;
+    pv.dir = V3{r1.x, r1.y, r1.z};
+    pv.farT = r1.w;
+    pv.T = V3{T.x, T.y, T.z};
+    pv.heldFar = T.w;
+    pv.held = V3{h.x, h.y, h.z};
+    pv.heldLight = __float_as_uint(h.w);
+    pv.depth = m.z & 0xffu;
+    pv.nonMirror = (m.z >> 8) & 0xffu;
+    pv.diffuse = (m.z >> 16) & 0xffu;
+    pv.glossy = m.z >> 24;
+    pv.mirror = m.w & 0xffu;
+    pv.lobeType = (m.w >> 8) & 0xffu;
+    const uint2 b = w.branch[p];
+    pv.branch = (U64(b.y) << 32) | b.x;
+}
+
+__device__ __forceinline__ void storePending(const WaveState& w, uint32_t p, const Pending& c, uint32_t pixel, uint32_t index) {
+    w.ray0[p] = make_float4(c.origin.x, c.origin.y, c.origin.z, c.nearT);
+    w.ray1[p] = make_float4(c.dir.x, c.dir.y, c.dir.z, c.farT);
+    w.T[p] = make_float4(c.T.x, c.T.y, c.T.z, c.heldFar);
+    w.held[p] = make_float4(c.held.x, c.held.y, c.held.z, __uint_as_float(c.heldLight));
+    w.meta[p] = make_uint4(pixel, index, packDepths(c), (c.mirror & 0xffu) | ((c.lobeType & 0xffu) << 8));
+    w.branch[p] = make_uint2(uint32_t(c.branch), uint32_t(c.branch >> 32));
+}
+
+}  // namespace
+
+// ---- logic ----
+__global__ void __launch_bounds__(kWaveBlock) wfLogic(WaveArgs a) {
+    const WaveState& w = a.w;
+    const uint32_t width = a.scene.config.width, height = a.scene.config.height;
+    const unsigned long long perChunk = 64ull * a.samplesPerChunk;
+    unsigned long long samples = 0, errors = 0;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < a.paths; base += gridDim.x * blockDim.x) {
+        const uint32_t p = base + threadIdx.x;
+        uint32_t st = p < a.paths ? w.state[p] : kTrace + 100;  // out of range: no work, no claim
+        if (p < a.paths) {
+            // The previous vertex's shadow rays, in the order they were made.
+            const uint32_t n = w.ncount[p];
+            if (n) {
+                float4 rad = w.rad[p];
+                const size_t first = size_t(p) * a.recordsPerPath;
+                for (uint32_t k = 0; k < n; ++k)
+                    if (w.svis[first + k]) {
+                        const float4 c = w.scontrib[first + k];
+                        rad.x = rad.x + c.x;
+                        rad.y = rad.y + c.y;
+                        rad.z = rad.z + c.z;
+                    }
+                w.rad[p] = rad;
+                w.ncount[p] = 0;
+            }
+            if (st == kDone || st == kError) {
+                const unsigned long long item = w.item[p];
+                a.out[item] = st == kDone ? w.rad[p] : make_float4(0, 0, 0, 0);
+                a.outStatus[item] = st == kDone ? uint8_t(X2_DONE) : uint8_t(X2_ERROR);
+                if (st == kDone) ++samples;
+                else ++errors;
+                st = kEmpty;
+                w.state[p] = kEmpty;
+            }
+        }
+        // Regeneration: every empty slot of the warp claims one item, one atomic a warp, in item order.
+        const bool wants = st == kEmpty;
+        const unsigned full = 0xffffffffu;
+        const unsigned want = __ballot_sync(full, wants);
+        unsigned long long first = 0;
+        if (want) {
+            if ((threadIdx.x & 31u) == 0) first = atomicAdd(a.claimed, (unsigned long long)__popc(want));
+            first = __shfl_sync(full, first, 0);
+        }
+        if (wants) {
+            const unsigned long long item = first + __popc(want & ((1u << (threadIdx.x & 31u)) - 1u));
+            if (item < a.itemCount) {
+                const unsigned long long chunkIndex = item / perChunk;
+                const uint32_t offset = uint32_t(item - chunkIndex * perChunk);
+                const uint32_t position = offset / a.samplesPerChunk, s = offset % a.samplesPerChunk;
+                const x2_chunk chunk = a.chunks[chunkIndex];
+                const uint32_t pixel = s < chunk.count ? tilePixelW(chunk.tile, position, width, height) : ~0u;
+                if (pixel == ~0u) {
+                    a.outStatus[item] = uint8_t(X2_SKIP);  // not a sample of this launch
+                } else {
+                    const uint32_t index = chunk.first + s;
+                    CameraRay camera;
+                    if (!cameraRay(a.scene, pixel, index, camera)) {
+                        a.out[item] = make_float4(0, 0, 0, 0);
+                        a.outStatus[item] = uint8_t(X2_ERROR);
+                        ++errors;
+                    } else {
+                        Pending p0;
+                        cameraPending(camera, p0);
+                        storePending(w, p, p0, pixel, index);
+                        w.rad[p] = make_float4(0, 0, 0, 0);
+                        w.item[p] = uint32_t(item);
+                        w.state[p] = kTrace;
+                        st = kTrace;
+                    }
+                }
+            }
+        }
+        // The extend queue: every slot with a ray to trace.
+        const bool trace = st == kTrace;
+        const uint32_t at = warpReserve(a.extendCount, trace ? 1u : 0u);
+        if (trace) a.extendQ[at] = p;
+    }
+    warpAddCounters(a.counters, 0, 0, 0, 0, samples, errors);
+}
+
+// ---- extend: closest hits ----
+__global__ void __launch_bounds__(kWaveBlock) wfExtend(WaveArgs a) {
+    const WaveState& w = a.w;
+    const uint32_t n = *a.extendCount;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t p = a.extendQ[i];
+        const float4 r0 = w.ray0[p], r1 = w.ray1[p];
+        const RayQ r = makeRay(a.scene.bvh, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
+        float t;
+        uint32_t leaf;
+        const uint32_t tri = a.scene.stats ? traceClosest<true>(a.scene.bvh, r, r0.w, r1.w, t, &leaf, a.scene.overflow, a.scene.stats)
+                                           : traceClosest<false>(a.scene.bvh, r, r0.w, r1.w, t, &leaf, a.scene.overflow, nullptr);
+        w.hit[p] = make_uint2(tri == ~0u ? ~0u : leaf, __float_as_uint(t));
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters->trace, (unsigned long long)n);
+}
+
+// ---- shade ----
+struct WaveSink {
+    const WaveState& w;
+    uint32_t p, n, recordsPerPath;
+    bool pushed;
+    Pending child;
+    unsigned long long nNee, nBsdf, nHeld;
+    __device__ void shadow(const ShadowReq& q, bool isBsdf) {
+        const size_t k = size_t(p) * recordsPerPath + n++;
+        w.sray0[k] = make_float4(q.origin.x, q.origin.y, q.origin.z, q.near);
+        w.sray1[k] = make_float4(q.dir.x, q.dir.y, q.dir.z, q.far);
+        w.scontrib[k] = make_float4(q.contribution.x, q.contribution.y, q.contribution.z, 0.0f);
+        if (isBsdf) ++nBsdf;
+        else ++nNee;
+    }
+    __device__ void held() { ++nHeld; }
+    __device__ uint32_t top(uint32_t t) const { return t; }
+    __device__ void push(const Pending& c) {
+        child = c;
+        pushed = true;
+    }
+};
+
+__global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) {
+    const WaveState& w = a.w;
+    const SceneView& s = a.scene;
+    const uint32_t n = *a.extendCount;
+    unsigned long long nee = 0, bsdf = 0, held = 0;
+    // Every lane of a warp runs the same rounds: the shadow queue's reservation is a warp-wide scan.
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t records = 0, p = 0;
+        if (i < n) {
+            p = a.extendQ[i];
+            Pending pv;
+            loadPending(w, p, pv);
+            const uint4 m = w.meta[p];
+            const uint32_t pixel = m.x, index = m.y;
+            const Identity root{pixel, U64(index), U64(s.config.seed), 0};
+            const uint2 hr = w.hit[p];
+            Hit hit;
+            hit.geom = ~0u;
+            hit.prim = 0;
+            hit.t = hit.u = hit.v = 0;
+            hit.normal = hit.origin = hit.below = hit.point = V3{0, 0, 0};
+            V3 va{0, 0, 0}, vb{0, 0, 0}, vc{0, 0, 0};
+            if (hr.x != ~0u) {
+                const float4* tp = reinterpret_cast<const float4*>(s.bvh.tris + hr.x);
+                const float4 A = __ldg(tp), B = __ldg(tp + 1), Cc = __ldg(tp + 2);
+                va = V3{A.x, A.y, A.z};
+                vb = V3{B.x, B.y, B.z};
+                vc = V3{Cc.x, Cc.y, Cc.z};
+                const uint32_t tri = __float_as_uint(A.w);
+                hit.geom = __ldg(s.triMesh + tri);
+                hit.prim = tri - __ldg(s.meshFirst + hit.geom);
+                hit.t = __uint_as_float(hr.y);
+                if (!geometryHit(hit, pv.origin, pv.dir, va, vb, vc)) hit.normal = V3{0, 0, 0};
+            }
+            float4 rad4 = w.rad[p];
+            V3 radiance{rad4.x, rad4.y, rad4.z};
+            float alpha = rad4.w;
+            // The camera's position (a pinhole: every camera ray's origin).
+            const V3 cameraPosition = add(mvector(s.camera.camera_to_render, V3{0, 0, 0}),
+                                          V3{s.camera.camera_to_render[3][0], s.camera.camera_to_render[3][1], s.camera.camera_to_render[3][2]});
+            afterTrace(s, root, pv, hit, cameraPosition, radiance, alpha);
+            uint32_t next = kDone;
+            if (hit.geom != ~0u) {
+                WaveSink sink{w, p, 0, a.recordsPerPath, false, Pending{}, 0, 0, 0};
+                if (!shadeVertex(s, root, pixel, index, pv, hit, va, vb, vc, 0u, radiance, alpha, sink)) {
+                    next = kError;
+                } else {
+                    records = sink.n;
+                    if (sink.pushed) {
+                        storePending(w, p, sink.child, pixel, index);
+                        next = kTrace;
+                    }
+                }
+                nee += sink.nNee;
+                bsdf += sink.nBsdf;
+                held += sink.nHeld;
+            }
+            w.rad[p] = make_float4(radiance.x, radiance.y, radiance.z, alpha);
+            w.ncount[p] = records;
+            w.state[p] = next;
+            const size_t first = size_t(p) * a.recordsPerPath;
+            for (uint32_t k = 0; k < records; ++k) w.svis[first + k] = 0;
+        }
+        const uint32_t at = warpReserve(a.shadowCount, records);
+        for (uint32_t k = 0; k < records; ++k) a.shadowQ[at + k] = p * a.recordsPerPath + k;
+    }
+    warpAddCounters(a.counters, 0, nee, bsdf, held, 0, 0);
+}
+
+// ---- shadow: any hits ----
+__global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) {
+    const WaveState& w = a.w;
+    const uint32_t n = *a.shadowCount;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k = a.shadowQ[i];
+        const float4 r0 = w.sray0[k], r1 = w.sray1[k];
+        const RayQ r = makeRay(a.scene.bvh, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
+        const bool hit = a.scene.stats ? traceAny<true>(a.scene.bvh, r, r0.w, r1.w, a.scene.overflow, a.scene.stats + 1)
+                                       : traceAny<false>(a.scene.bvh, r, r0.w, r1.w, a.scene.overflow, nullptr);
+        w.svis[k] = hit ? 0 : 1;
+    }
+}
+
+// Queue counters for the next iteration: the extend and shadow counts start at zero; the previous counts are kept
+// for the host (the graph's last extend count tells whether paths remain).
+__global__ void wfResetQueues(WaveArgs a) {
+    if (threadIdx.x == 0) {
+        *a.lastExtend = *a.extendCount;
+        *a.extendCount = 0;
+        *a.shadowCount = 0;
+    }
+}
+
+// The film: each (chunk, position)'s samples summed in sample order, then added to the pixel (async_gpu.cu:320-364's
+// sums and counts, without the per-sample atomics).
+__global__ void wfFilmReduce(WaveArgs a, uint32_t chunkCount, double* sums, double* odd, uint32_t* counts) {
+    const uint32_t width = a.scene.config.width, height = a.scene.config.height;
+    const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 64ull * chunkCount) return;
+    const uint32_t chunkIndex = uint32_t(i / 64), position = uint32_t(i % 64);
+    const x2_chunk chunk = a.chunks[chunkIndex];
+    const uint32_t pixel = tilePixelW(chunk.tile, position, width, height);
+    if (pixel == ~0u) return;
+    double v[4] = {0, 0, 0, 0}, o[4] = {0, 0, 0, 0};
+    uint32_t n = 0;
+    const unsigned long long first = (unsigned long long)chunkIndex * 64ull * a.samplesPerChunk + (unsigned long long)position * a.samplesPerChunk;
+    for (uint32_t s = 0; s < chunk.count; ++s) {
+        if (a.outStatus[first + s] != X2_DONE) continue;
+        const float4 r = a.out[first + s];
+        v[0] += double(r.x);
+        v[1] += double(r.y);
+        v[2] += double(r.z);
+        v[3] += double(r.w);
+        if (odd && ((chunk.first + s) & 1u)) {
+            o[0] += double(r.x);
+            o[1] += double(r.y);
+            o[2] += double(r.z);
+            o[3] += double(r.w);
+        }
+        ++n;
+    }
+    if (!n) return;
+    for (int k = 0; k < 4; ++k) atomicAdd(sums + 4ull * pixel + k, v[k]);
+    if (odd)
+        for (int k = 0; k < 4; ++k)
+            if (o[k] != 0.0) atomicAdd(odd + 4ull * pixel + k, o[k]);
+    atomicAdd(counts + pixel, n);
+}
+
+}  // namespace x2

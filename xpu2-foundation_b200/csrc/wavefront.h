@@ -1,0 +1,56 @@
+// The wavefront form's state and kernels (internal to libx2).
+#pragma once
+#include "integrator.cuh"
+
+namespace x2 {
+
+constexpr int kWaveBlock = 128;
+
+// Path slots (structure of arrays, `paths` slots) and shadow-ray records (recordsPerPath a slot).
+struct WaveState {
+    float4* ray0;      // origin, near
+    float4* ray1;      // direction, far
+    float4* T;         // throughput, held light's shadow end
+    float4* held;      // held light's contribution, held light index (bits)
+    uint4* meta;       // pixel, sample index, packed depths, mirror depth | lobe type << 8
+    uint2* branch;     // the vertex's branch address (lo, hi)
+    float4* rad;       // radiance so far, alpha
+    uint2* hit;        // the extend kernel's closest hit: leaf-order triangle (~0u: none), t bits
+    uint32_t* state;   // empty / trace / done / error
+    uint32_t* item;    // the slot's work item
+    uint32_t* ncount;  // shadow records the last vertex made
+    float4* sray0;     // records: origin, near
+    float4* sray1;     // direction, far
+    float4* scontrib;  // contribution when unoccluded
+    uint8_t* svis;     // 1: nothing occludes [near, far]
+};
+
+struct WaveArgs {
+    SceneView scene;
+    WaveState w;
+    uint32_t paths, recordsPerPath;
+    const x2_chunk* chunks;
+    unsigned long long itemCount;
+    uint32_t samplesPerChunk;
+    unsigned long long* claimed;
+    uint32_t* extendQ;
+    uint32_t* extendCount;
+    uint32_t* lastExtend;
+    uint32_t* shadowQ;
+    uint32_t* shadowCount;
+    float4* out;          // per item: rgb, alpha
+    uint8_t* outStatus;   // per item: SampleStatus (Skip for items that are not samples)
+    Counters* counters;
+};
+
+// Fills wavefront.cu's copy of the Sobol direction table (every translation unit with sampling kernels has one).
+cudaError_t uploadSobolWavefront(const uint32_t directions[17][32]);
+
+__global__ void wfLogic(WaveArgs a);
+__global__ void wfExtend(WaveArgs a);
+__global__ void wfShade(WaveArgs a);
+__global__ void wfShadow(WaveArgs a);
+__global__ void wfResetQueues(WaveArgs a);
+__global__ void wfFilmReduce(WaveArgs a, uint32_t chunkCount, double* sums, double* odd, uint32_t* counts);
+
+}  // namespace x2

@@ -10,6 +10,7 @@ There is no CPU fallback: without the built library or a CUDA device every call 
 """
 import ctypes as C
 import os
+import weakref
 
 import numpy as np
 
@@ -115,8 +116,12 @@ def library():
         "x2_wait": ([vp, i32, C.POINTER(Completion)], i32), "x2_render_frame": ([vp, u32, u32], i32),
         "x2_film_download": ([vp, vp, vp, vp], i32), "x2_film_device": ([vp, C.POINTER(vp), C.POINTER(vp), C.POINTER(vp)], i32),
         "x2_audit": ([vp, vp, C.POINTER(C.c_int64)], i32), "x2_counters_read": ([vp, C.POINTER(Counters)], i32),
+        "x2_wavefront_reserve": ([vp, u32], i32), "x2_launch_wavefront": ([vp, vp, u32], i32),
+        "x2_render_frame_wavefront": ([vp, u32, u32], i32), "x2_items_download": ([vp, vp, vp, u64], i32),
+        "x2_wavefront_info": ([vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)], i32),
+        "x2_wavefront_timing": ([vp, i32, vp], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
-        "x2_traversal_counts": ([vp, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64)], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
+        "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
     }
     for name, (args, res) in sig.items():
@@ -149,13 +154,17 @@ class Context:
         self._h = C.c_void_p()
         _check(library().x2_open(device, C.byref(self._h)))
         self.device = device
+        self._scenes = weakref.WeakSet()
 
     @property
     def handle(self):
         return self._h
 
     def close(self):
+        """Frees the context's scenes first: a scene never outlives the context it was loaded on."""
         if self._h:
+            for s in list(self._scenes):
+                s.free()
             library().x2_close(self._h)
             self._h = C.c_void_p()
 
@@ -233,6 +242,7 @@ class Scene:
         self.ctx = ctx
         self._h = C.c_void_p()
         _check(library().x2_scene_load(ctx.handle, C.byref(desc) if isinstance(desc, SceneDesc) else desc, C.byref(self._h)))
+        ctx._scenes.add(self)
         self.set_config(config)
 
     def set_config(self, config):
@@ -293,6 +303,35 @@ class Scene:
     def render_frame(self, first, count):
         _check(library().x2_render_frame(self._h, first, count))
 
+    # -- wavefront form --
+    def wavefront_reserve(self, paths):
+        _check(library().x2_wavefront_reserve(self._h, paths))
+
+    def launch_wavefront(self, chunks):
+        chunks = np.ascontiguousarray(chunks, dtype=CHUNK_DTYPE)
+        _check(library().x2_launch_wavefront(self._h, _ptr(chunks), len(chunks)))
+
+    def render_frame_wavefront(self, first, count):
+        _check(library().x2_render_frame_wavefront(self._h, first, count))
+
+    def items(self, n):
+        """The last wavefront launch's per-item radiance (n x 4 float32) and SampleStatus."""
+        rgba = np.empty((n, 4), np.float32)
+        status = np.empty(n, np.uint8)
+        _check(library().x2_items_download(self._h, _ptr(rgba), _ptr(status), n))
+        return rgba, status
+
+    def wavefront_timing(self, on=None):
+        """Switch per-kernel timing (diagnostic) and return the last timed launch's milliseconds by kernel."""
+        ms = np.zeros(5, np.float32)
+        _check(library().x2_wavefront_timing(self._h, -1 if on is None else int(bool(on)), _ptr(ms)))
+        return dict(zip(("logic", "extend", "shade", "shadow", "film"), ms.tolist()))
+
+    def wavefront_info(self):
+        p, r, i = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        _check(library().x2_wavefront_info(self._h, C.byref(p), C.byref(r), C.byref(i)))
+        return {"paths": p.value, "records_per_path": r.value, "iterations": i.value}
+
     def poll(self):
         c = Completion()
         r = library().x2_poll(self._h, C.byref(c))
@@ -332,9 +371,10 @@ class Scene:
         _check(library().x2_count_traversal(self._h, 1 if on else 0))
 
     def traversal_counts(self):
-        r, n, t = C.c_uint64(), C.c_uint64(), C.c_uint64()
-        _check(library().x2_traversal_counts(self._h, C.byref(r), C.byref(n), C.byref(t)))
-        return {"rays": r.value, "nodes": n.value, "triangles": t.value}
+        """Node visits and triangle tests of the launches made in counting mode, by ray kind."""
+        r, n, t = (C.c_uint64 * 2)(), (C.c_uint64 * 2)(), (C.c_uint64 * 2)()
+        _check(library().x2_traversal_counts(self._h, r, n, t))
+        return {kind: {"rays": r[k], "nodes": n[k], "triangles": t[k]} for k, kind in enumerate(("closest", "any"))}
 
 
 CHUNK_DTYPE = np.dtype([("tile", "<u4"), ("first", "<u4"), ("count", "<u4"), ("cell", "<u4")])
