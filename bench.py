@@ -327,6 +327,37 @@ def run(args):
         dist.destroy_process_group()
 
 
+def probe(args):
+    """One bounded launch for profilers (ncu): `--probe-tiles` evenly spaced tiles of config 1 at 64 spp, in one form;
+    the wavefront form without its graph (`--probe-timed`) so each kernel launch is visible on its own."""
+    import x2
+
+    ctx = x2.Context(0)
+    s = x2.SyntheticScene(1)
+    cfg = s.config
+    scene = x2.Scene(ctx, s.desc, cfg)
+    tiles = ((cfg.width + 7) // 8) * ((cfg.height + 7) // 8)
+    sel = np.linspace(0, tiles - 1, args.probe_tiles).astype(np.uint32)
+    chunks = np.zeros(len(sel), x2.CHUNK_DTYPE)
+    chunks["tile"], chunks["first"], chunks["count"] = sel, 0, cfg.spp
+    n = len(sel) * 64 * cfg.spp
+    scene.frame_begin(cfg.spp)
+    if args.probe == "plain":
+        scene.launch(chunks)
+    else:
+        scene.wavefront_timing(args.probe_timed)
+        scene.launch_wavefront(chunks)
+    c = scene.wait()
+    out = {"probe": args.probe, "tiles": len(sel), "samples": n, "ms": c.milliseconds, "msamples_per_s": n / c.milliseconds / 1e3,
+           "errors": c.errors}
+    if args.probe == "wavefront":
+        out["kernel_ms"] = scene.wavefront_timing(None)
+        out["wavefront"] = scene.wavefront_info()
+    print(json.dumps(out))
+    scene.free()
+    ctx.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -335,9 +366,14 @@ def main():
     ap.add_argument("--impl", default="x2", choices=["x2", "reference"])
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--skip-plain", action="store_true")
+    ap.add_argument("--probe", choices=["plain", "wavefront"], help="one bounded launch for a profiler, then exit")
+    ap.add_argument("--probe-tiles", type=int, default=592)
+    ap.add_argument("--probe-timed", action="store_true", help="wavefront probe without its graph (per-kernel launches)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
-    if args.impl == "reference":
+    if args.probe:
+        probe(args)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run(args)
