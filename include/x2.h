@@ -188,6 +188,16 @@ int x2_wavefront_info(x2_scene* scene, uint32_t* paths, uint32_t* records, uint3
 /* Per-kernel timing of wavefront launches (a diagnostic: no graph, a host sync an iteration). on: 1 on, 0 off, -1
  * unchanged; ms (5 floats, or null): the last timed launch's logic, extend, shade, shadow and film-reduce times. */
 int x2_wavefront_timing(x2_scene* scene, int on, float* ms);
+/* A wavefront launch that allocates nothing. No counterpart in the reference. For callers that cannot call
+ * cudaMalloc: a process whose device memory another allocator already holds, or a path where cudaMalloc's implicit
+ * device synchronisation is not allowed. Its scratch is one file-scope device array of at most 36 MiB that every GPU
+ * loading the library holds until exit; the caller passes the chunks (device memory) and the film it adds to
+ * (device: 4 doubles and one count a pixel; zero them first). Limits: at most 2^20 work items a call
+ * (count x 64 x samples_per_chunk), light_count x light_samples <= 32, bsdf_samples = 1; beyond them X2_EINVAL.
+ * The first call on a device looks up the array's address: make it before any stream capture. Calls share the
+ * array: calls that overlap on the GPU race. Waits for the launch; *samples_done (or null) gets the samples rendered. */
+int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chunks, uint32_t count, uint32_t samples_per_chunk,
+                               double* d_sums, uint32_t* d_counts, uint64_t* samples_done);
 int x2_film_download(x2_scene* scene, double* sums, double* odd, uint32_t* counts);  /* downloadFilm(); waits */
 int x2_film_device(x2_scene* scene, double** d_sums, double** d_odd, uint32_t** d_counts);
 int x2_audit(x2_scene* scene, const uint32_t* expected, int64_t* bad_pixel);  /* async_render.h:992-1048 */

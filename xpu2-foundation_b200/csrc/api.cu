@@ -290,6 +290,22 @@ int ensureItems(x2_scene* s, uint64_t items) {
 
 }  // namespace
 
+namespace x2 {
+// The scene's device view, stream and device for entry points in other translation units (noalloc.cu).
+int sceneView(x2_scene* s, SceneView* view, cudaStream_t* stream, int* device, int* smCount) {
+    if (!s || !s->configured) {
+        setError("scene not configured");
+        return X2_EINVAL;
+    }
+    if (int rc = checkDevice(s->ctx)) return rc;
+    *view = viewOf(s);
+    *stream = s->ctx->stream;
+    *device = s->ctx->device;
+    *smCount = s->ctx->smCount;
+    return X2_OK;
+}
+}  // namespace x2
+
 extern "C" {
 
 const char* x2_version(void) { return "x2-b200 0.1 (sm_100a)"; }

@@ -1,0 +1,192 @@
+// x2_launch_wavefront_static: the wavefront launch for callers that cannot allocate device memory.
+//
+// Some callers cannot call cudaMalloc: a process whose device memory is already reserved by another allocator (a
+// framework's caching allocator holding the GPU), or code on a latency-bound path where cudaMalloc's implicit device
+// synchronisation is not allowed. This entry point runs the same wavefront kernels as x2_launch_wavefront with all
+// of their scratch — path slots, shadow-ray records, queues, per-item outputs, counters — in one file-scope array
+// of kScratchBytes that every GPU which loads the library holds until the process exits. It allocates nothing: no
+// cudaMalloc/cudaFree, no events, no graph; the caller passes the chunks and the film (device pointers).
+//
+// Limits (calls beyond them return X2_EINVAL): at most kMaxItems work items a call (chunks x 64 x samples a chunk),
+// at most kMaxRecords - 1 light samples a vertex (light_count x light_samples), one BSDF sample (bsdf_samples = 1),
+// kPaths paths in flight.
+//
+// Set-up: the first call on a device looks up the array's device address (cudaGetSymbolAddress, with that device
+// current) and keeps it; make that first call before any stream capture. Every call shares the array and keeps the
+// last call's contents; each call clears what must start at zero. Calls that overlap on the GPU (two host threads,
+// two streams, two contexts on one device) race on the array and must not be made.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <mutex>
+#include <thread>
+
+#include "../../include/x2.h"
+#include "engine.h"
+#include "wavefront.h"
+
+namespace x2 {
+
+namespace {
+
+constexpr uint32_t kPaths = 8192, kMaxRecords = 33, kMaxItems = 1u << 20;
+
+constexpr size_t align256(size_t n) { return (n + 255) & ~size_t(255); }
+// The array's parts, in order.
+constexpr size_t kRay0 = 0, kRay1 = kRay0 + align256(16ull * kPaths), kT = kRay1 + align256(16ull * kPaths),
+                 kHeld = kT + align256(16ull * kPaths), kMeta = kHeld + align256(16ull * kPaths), kBranch = kMeta + align256(16ull * kPaths),
+                 kRad = kBranch + align256(8ull * kPaths), kHit = kRad + align256(16ull * kPaths), kState = kHit + align256(8ull * kPaths),
+                 kItem = kState + align256(4ull * kPaths), kNcount = kItem + align256(4ull * kPaths),
+                 kSray0 = kNcount + align256(4ull * kPaths), kSray1 = kSray0 + align256(16ull * kPaths * kMaxRecords),
+                 kScontrib = kSray1 + align256(16ull * kPaths * kMaxRecords), kSvis = kScontrib + align256(16ull * kPaths * kMaxRecords),
+                 kExtendQ = kSvis + align256(1ull * kPaths * kMaxRecords), kShadowQ = kExtendQ + align256(4ull * kPaths),
+                 kOut = kShadowQ + align256(4ull * kPaths * kMaxRecords), kOutStatus = kOut + align256(16ull * kMaxItems),
+                 kQueueCounters = kOutStatus + align256(1ull * kMaxItems), kClaimed = kQueueCounters + align256(16),
+                 kCounters = kClaimed + align256(8), kScratchBytes = kCounters + align256(sizeof(Counters));
+static_assert(kScratchBytes <= 36ull << 20, "the static scratch stays modest (36 MiB)");
+
+static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
+
+std::mutex g_mutex;
+void* g_address[64] = {};  // the array's device address, by device
+
+int waitStream(cudaStream_t st, int timeoutMs) {
+    const auto until = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeoutMs);
+    for (;;) {
+        const cudaError_t q = cudaStreamQuery(st);
+        if (q == cudaSuccess) return X2_OK;
+        if (q != cudaErrorNotReady) {
+            setError("device error: %s", cudaGetErrorString(q));
+            return X2_ECUDA;
+        }
+        if (std::chrono::steady_clock::now() >= until) {
+            setError("wait timed out after %d ms", timeoutMs);
+            return X2_ETIMEOUT;
+        }
+        std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+}  // namespace
+
+// Internal: the scene's device view and stream (api.cu).
+int sceneView(x2_scene* scene, SceneView* view, cudaStream_t* stream, int* device, int* smCount);
+
+}  // namespace x2
+
+using namespace x2;
+
+extern "C" int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chunks, uint32_t count, uint32_t samples_per_chunk,
+                                          double* d_sums, uint32_t* d_counts, uint64_t* samples_done) {
+    SceneView view;
+    cudaStream_t st;
+    int device = 0, smCount = 0;
+    if (int rc = sceneView(scene, &view, &st, &device, &smCount)) return rc;
+    const x2_config& c = view.config;
+    if (!d_chunks || !d_sums || !d_counts || samples_per_chunk == 0) {
+        setError("null chunks or film, or zero samples a chunk");
+        return X2_EINVAL;
+    }
+    const unsigned long long items = (unsigned long long)count * 64ull * samples_per_chunk;
+    if (items > kMaxItems) {
+        setError("%llu work items in one call; the static scratch holds at most %u", items, kMaxItems);
+        return X2_EINVAL;
+    }
+    const uint32_t records = c.light_count * c.light_samples + 1;
+    if (records > kMaxRecords || c.bsdf_samples != 1) {
+        setError("at most %u light samples a vertex and one BSDF sample (%u lights x %u samples, %u BSDF samples)", kMaxRecords - 1,
+                 c.light_count, c.light_samples, c.bsdf_samples);
+        return X2_EINVAL;
+    }
+    if (!count) return X2_OK;
+    unsigned char* base = nullptr;
+    {
+        std::lock_guard<std::mutex> lock(g_mutex);
+        if (device < 0 || device >= 64) {
+            setError("device %d out of range", device);
+            return X2_EINVAL;
+        }
+        if (!g_address[device]) {
+            void* p = nullptr;
+            const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+            if (e != cudaSuccess || !p) {
+                setError("cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
+                return X2_ECUDA;
+            }
+            g_address[device] = p;
+        }
+        base = static_cast<unsigned char*>(g_address[device]);
+    }
+    WaveArgs a;
+    a.scene = view;
+    a.w.ray0 = reinterpret_cast<float4*>(base + kRay0);
+    a.w.ray1 = reinterpret_cast<float4*>(base + kRay1);
+    a.w.T = reinterpret_cast<float4*>(base + kT);
+    a.w.held = reinterpret_cast<float4*>(base + kHeld);
+    a.w.meta = reinterpret_cast<uint4*>(base + kMeta);
+    a.w.branch = reinterpret_cast<uint2*>(base + kBranch);
+    a.w.rad = reinterpret_cast<float4*>(base + kRad);
+    a.w.hit = reinterpret_cast<uint2*>(base + kHit);
+    a.w.state = reinterpret_cast<uint32_t*>(base + kState);
+    a.w.item = reinterpret_cast<uint32_t*>(base + kItem);
+    a.w.ncount = reinterpret_cast<uint32_t*>(base + kNcount);
+    a.w.sray0 = reinterpret_cast<float4*>(base + kSray0);
+    a.w.sray1 = reinterpret_cast<float4*>(base + kSray1);
+    a.w.scontrib = reinterpret_cast<float4*>(base + kScontrib);
+    a.w.svis = base + kSvis;
+    a.paths = kPaths;
+    a.recordsPerPath = records;
+    a.chunks = d_chunks;
+    a.itemCount = items;
+    a.samplesPerChunk = samples_per_chunk;
+    a.claimed = reinterpret_cast<unsigned long long*>(base + kClaimed);
+    a.extendQ = reinterpret_cast<uint32_t*>(base + kExtendQ);
+    uint32_t* queues = reinterpret_cast<uint32_t*>(base + kQueueCounters);
+    a.extendCount = queues;
+    a.lastExtend = queues + 1;
+    a.shadowQ = reinterpret_cast<uint32_t*>(base + kShadowQ);
+    a.shadowCount = queues + 2;
+    a.out = reinterpret_cast<float4*>(base + kOut);
+    a.outStatus = base + kOutStatus;
+    a.counters = reinterpret_cast<Counters*>(base + kCounters);
+    // What must start at zero; the rest is written before it is read.
+    cudaMemsetAsync(a.w.state, 0, 4ull * kPaths, st);
+    cudaMemsetAsync(a.w.ncount, 0, 4ull * kPaths, st);
+    cudaMemsetAsync(queues, 0, 16, st);
+    cudaMemsetAsync(a.claimed, 0, 8, st);
+    cudaMemsetAsync(a.counters, 0, sizeof(Counters), st);
+    cudaMemsetAsync(a.outStatus, X2_SKIP, items, st);
+    const int gridLogic = int((kPaths + kWaveBlock - 1) / kWaveBlock);
+    const int gridWork = smCount * 16;
+    const uint64_t maxIter = items * (uint64_t(c.max_depth) + 2) / kPaths + uint64_t(c.max_depth) + 64;
+    uint32_t last = 1;
+    for (uint64_t it = 0; last; ++it) {
+        if (it > maxIter) {
+            setError("wavefront did not drain after %llu iterations", (unsigned long long)it);
+            return X2_EDEVICE;
+        }
+        wfResetQueues<<<1, 32, 0, st>>>(a);
+        wfLogic<<<gridLogic, kWaveBlock, 0, st>>>(a);
+        wfExtend<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wfShade<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wfShadow<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wfResetQueues<<<1, 32, 0, st>>>(a);
+        const cudaError_t e = cudaMemcpyAsync(&last, queues + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if (e != cudaSuccess) {
+            setError("launch failed: %s", cudaGetErrorString(e));
+            return X2_ECUDA;
+        }
+        if (int rc = waitStream(st, 600000)) return rc;
+    }
+    wfFilmReduce<<<int((64ull * count + 255) / 256), 256, 0, st>>>(a, count, d_sums, nullptr, d_counts);
+    Counters h{};
+    cudaMemcpyAsync(&h, a.counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+    if (int rc = waitStream(st, 600000)) return rc;
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        setError("launch failed: %s", cudaGetErrorString(e));
+        return X2_ECUDA;
+    }
+    if (samples_done) *samples_done = h.samples;
+    return h.errors ? X2_EDEVICE : X2_OK;
+}

@@ -120,6 +120,7 @@ def library():
         "x2_render_frame_wavefront": ([vp, u32, u32], i32), "x2_items_download": ([vp, vp, vp, u64], i32),
         "x2_wavefront_info": ([vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)], i32),
         "x2_wavefront_timing": ([vp, i32, vp], i32),
+        "x2_launch_wavefront_static": ([vp, vp, u32, u32, vp, vp, C.POINTER(u64)], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
@@ -320,6 +321,14 @@ class Scene:
         status = np.empty(n, np.uint8)
         _check(library().x2_items_download(self._h, _ptr(rgba), _ptr(status), n))
         return rgba, status
+
+    def launch_wavefront_static(self, d_chunks, count, samples_per_chunk, d_sums, d_counts):
+        """The wavefront launch that allocates nothing (x2_launch_wavefront_static): device pointers (ints) to the
+        chunks and to the film it adds to; waits; returns the samples rendered."""
+        done = C.c_uint64()
+        _check(library().x2_launch_wavefront_static(self._h, C.c_void_p(d_chunks), count, samples_per_chunk, C.c_void_p(d_sums),
+                                                    C.c_void_p(d_counts), C.byref(done)))
+        return done.value
 
     def wavefront_timing(self, on=None):
         """Switch per-kernel timing (diagnostic) and return the last timed launch's milliseconds by kernel."""
