@@ -272,14 +272,9 @@ def run(args):
 
     # Multi-GPU: the lanes' films summed over NCCL at frame end, then the audit of the merged counts.
     if dist is not None:
-        import torch
+        from x2 import lanes
 
-        ts = torch.from_numpy(sums).cuda(local)
-        tcnt = torch.from_numpy(counts.astype(np.int64)).cuda(local)
-        dist.reduce(ts, 0)
-        dist.reduce(tcnt, 0)
-        if rank == 0 and not bool((tcnt == world * cfg.spp).all()):
-            raise RuntimeError("merged sample-count audit failed")
+        lanes.merge_and_audit(sums, counts, world * cfg.spp, device="cuda:%d" % local)
 
     # Roofline of the dominant wavefront kernel: its algorithmic bytes (BVH nodes and triangles its rays visit, and
     # its ray records) over its time in the per-kernel timed frame.
@@ -353,6 +348,8 @@ def probe(args):
     if args.probe == "wavefront":
         out["kernel_ms"] = scene.wavefront_timing(None)
         out["wavefront"] = scene.wavefront_info()
+        if args.probe_timed:
+            out["queues"] = scene.wavefront_queues().tolist()  # per iteration: rays extended, shadow rays
     print(json.dumps(out))
     scene.free()
     ctx.close()

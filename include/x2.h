@@ -188,6 +188,15 @@ int x2_wavefront_info(x2_scene* scene, uint32_t* paths, uint32_t* records, uint3
 /* Per-kernel timing of wavefront launches (a diagnostic: no graph, a host sync an iteration). on: 1 on, 0 off, -1
  * unchanged; ms (5 floats, or null): the last timed launch's logic, extend, shade, shadow and film-reduce times. */
 int x2_wavefront_timing(x2_scene* scene, int on, float* ms);
+/* Wavefront launch shape (no reference counterpart; the autotuner's knobs): refill = 1..32 idle lanes of a
+ * traversal warp that make it fetch the next rays of its queue (0: one ray a thread, no fetch); blocks_per_sm = the
+ * traversal and shade grids' blocks a SM (1..32); trace_blocks / shade_blocks = the occupancy variant of the traversal
+ * and shade kernels, blocks a SM their registers must allow (traversal 0, 10 or 12; shade 0, 3 or 4; 0: the compiler's
+ * choice). Defaults: refill 8, blocks_per_sm 16, trace_blocks 0, shade_blocks 4. */
+int x2_wavefront_tune(x2_scene* scene, uint32_t refill, uint32_t blocks_per_sm, uint32_t trace_blocks, uint32_t shade_blocks);
+/* The last timed wavefront launch's queue sizes: for each iteration, rays extended then shadow rays (2 a
+ * iteration, at most max values). */
+int x2_wavefront_queues(x2_scene* scene, uint32_t* sizes, uint32_t max);
 /* A wavefront launch that allocates nothing. No counterpart in the reference. For callers that cannot call
  * cudaMalloc: a process whose device memory another allocator already holds, or a path where cudaMalloc's implicit
  * device synchronisation is not allowed. Its scratch is one file-scope device array of at most 36 MiB that every GPU

@@ -83,6 +83,8 @@ int waitEvent(cudaEvent_t e, int timeoutMs) {
 }
 
 constexpr int kSlots = 2;  // launches in flight, as GpuLane keeps (async_gpu.h:1425)
+constexpr uint32_t kQueueLog = 4096;
+constexpr int kWaveCounters = 8;  // extend count, last extend count, shadow count, extend fetch, shadow fetch
 
 struct Slot {
     bool busy = false;
@@ -144,7 +146,10 @@ struct x2_scene {
     uint32_t wavePaths = 0, waveRecords = 0, reservePaths = 0;
     uint32_t* extendQ = nullptr;
     uint32_t* shadowQ = nullptr;
-    uint32_t* waveCounters = nullptr;  // extend count, last extend count, shadow count
+    uint32_t* waveCounters = nullptr;  // kWaveCounters words
+    uint32_t refill = kDefaultRefill;  // idle lanes that make a traversal warp fetch rays (0: one ray a thread)
+    uint32_t blocksPerSm = kDefaultBlocksPerSm;  // traversal and shade grids: blocks a SM
+    uint32_t traceBlocks = kDefaultTraceBlocks, shadeBlocks = kDefaultShadeBlocks;  // occupancy variants
     uint32_t* hostLast = nullptr;      // pinned
     unsigned long long* claimed = nullptr;
     float4* out = nullptr;
@@ -153,6 +158,7 @@ struct x2_scene {
     uint32_t waveIterations = 0;       // of the last wavefront launch
     bool waveTiming = false;           // time each kernel kind (no graph)
     float waveMs[5] = {0, 0, 0, 0, 0}; // logic, extend, shade, shadow, film reduce
+    uint32_t queueLog[2 * 4096] = {};  // timed launches: each iteration's extend and shadow queue sizes
 };
 
 namespace {
@@ -260,7 +266,7 @@ int ensureWave(x2_scene* s, uint32_t paths, uint32_t records) {
               cudaMalloc(&w.sray1, sizeof(float4) * R) == cudaSuccess && cudaMalloc(&w.scontrib, sizeof(float4) * R) == cudaSuccess &&
               cudaMalloc(&w.svis, R) == cudaSuccess && cudaMalloc(&s->extendQ, sizeof(uint32_t) * P) == cudaSuccess &&
               cudaMalloc(&s->shadowQ, sizeof(uint32_t) * R) == cudaSuccess;
-    if (ok && !s->waveCounters) ok = cudaMalloc(&s->waveCounters, sizeof(uint32_t) * 4) == cudaSuccess;
+    if (ok && !s->waveCounters) ok = cudaMalloc(&s->waveCounters, sizeof(uint32_t) * kWaveCounters) == cudaSuccess;
     if (ok && !s->claimed) ok = cudaMalloc(&s->claimed, sizeof(unsigned long long)) == cudaSuccess;
     if (ok && !s->hostLast) ok = cudaMallocHost(&s->hostLast, sizeof(uint32_t) * 4) == cudaSuccess;
     if (!ok) {
@@ -833,6 +839,18 @@ int x2_wavefront_reserve(x2_scene* s, uint32_t paths) {
     return X2_OK;
 }
 
+int x2_wavefront_tune(x2_scene* s, uint32_t refill, uint32_t blocks_per_sm, uint32_t trace_blocks, uint32_t shade_blocks) {
+    if (!s || refill > 32 || blocks_per_sm < 1 || blocks_per_sm > 32 || trace_blocks > 32 || shade_blocks > 32) {
+        setError("refill is 0..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32");
+        return X2_EINVAL;
+    }
+    s->refill = refill;
+    s->blocksPerSm = blocks_per_sm;
+    s->traceBlocks = trace_blocks;
+    s->shadeBlocks = shade_blocks;
+    return X2_OK;
+}
+
 int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     if (!s || !s->configured || !s->filmPixels || !s->samplesPerChunk) {
         setError("x2_frame_begin first");
@@ -871,7 +889,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     cudaMemsetAsync(s->wave.state, 0, sizeof(uint32_t) * paths, st);
     cudaMemsetAsync(s->wave.ncount, 0, sizeof(uint32_t) * paths, st);
     cudaMemsetAsync(s->claimed, 0, sizeof(unsigned long long), st);
-    cudaMemsetAsync(s->waveCounters, 0, sizeof(uint32_t) * 4, st);
+    cudaMemsetAsync(s->waveCounters, 0, sizeof(uint32_t) * kWaveCounters, st);
     cudaMemsetAsync(sl.counters, 0, sizeof(Counters), st);
     cudaMemsetAsync(s->outStatus, X2_SKIP, items, st);
     WaveArgs a;
@@ -888,11 +906,15 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     a.lastExtend = s->waveCounters + 1;
     a.shadowQ = s->shadowQ;
     a.shadowCount = s->waveCounters + 2;
+    a.extendNext = s->waveCounters + 3;
+    a.shadowNext = s->waveCounters + 4;
+    a.refill = s->refill;
     a.out = s->out;
     a.outStatus = s->outStatus;
     a.counters = sl.counters;
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
-    const int gridWork = s->ctx->smCount * 16;
+    const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
+    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks);
     const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     if (s->waveTiming) {
         // Diagnostic form: no graph; events around every kernel, the iteration's times added once it is done.
@@ -907,19 +929,23 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
             cudaEventRecord(ev[0], st);
             wfLogic<<<gridLogic, kWaveBlock, 0, st>>>(a);
             cudaEventRecord(ev[1], st);
-            wfExtend<<<gridWork, kWaveBlock, 0, st>>>(a);
+            wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
             cudaEventRecord(ev[2], st);
-            wfShade<<<gridWork, kWaveBlock, 0, st>>>(a);
+            wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
             cudaEventRecord(ev[3], st);
-            wfShadow<<<gridWork, kWaveBlock, 0, st>>>(a);
+            wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
             cudaEventRecord(ev[4], st);
+            cudaMemcpyAsync(s->hostLast, s->waveCounters, 4 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
             wfResetQueues<<<1, 32, 0, st>>>(a);
-            cudaMemcpyAsync(s->hostLast, s->waveCounters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
             if ((rc = x2_synchronize(s->ctx, 600000)) != X2_OK) break;
             for (int k = 0; k < 4; ++k) {
                 float ms = 0.0f;
                 cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
                 s->waveMs[k] += ms;
+            }
+            if (iterations < kQueueLog) {
+                s->queueLog[2 * iterations] = s->hostLast[0];      // rays extended
+                s->queueLog[2 * iterations + 1] = s->hostLast[2];  // shadow rays
             }
             ++iterations;
             if (s->hostLast[0] == 0) break;
@@ -957,9 +983,9 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     for (int it = 0; it < kIter; ++it) {
         wfResetQueues<<<1, 32, 0, st>>>(a);
         wfLogic<<<gridLogic, kWaveBlock, 0, st>>>(a);
-        wfExtend<<<gridWork, kWaveBlock, 0, st>>>(a);
-        wfShade<<<gridWork, kWaveBlock, 0, st>>>(a);
-        wfShadow<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
     }
     wfResetQueues<<<1, 32, 0, st>>>(a);  // the last iteration's extend count, for the host
     CUDA_OR(cudaStreamEndCapture(st, &graph), X2_ECUDA);
@@ -1041,6 +1067,13 @@ int x2_wavefront_timing(x2_scene* s, int on, float* ms) {
     if (ms)
         for (int k = 0; k < 5; ++k) ms[k] = s->waveMs[k];
     if (on >= 0) s->waveTiming = on != 0;
+    return X2_OK;
+}
+
+int x2_wavefront_queues(x2_scene* s, uint32_t* sizes, uint32_t max) {
+    if (!s || !sizes) return X2_EINVAL;
+    const uint32_t n = s->waveIterations < kQueueLog ? s->waveIterations : kQueueLog;
+    for (uint32_t i = 0; i < 2 * n && i < max; ++i) sizes[i] = s->queueLog[i];
     return X2_OK;
 }
 

@@ -41,7 +41,7 @@ constexpr size_t kRay0 = 0, kRay1 = kRay0 + align256(16ull * kPaths), kT = kRay1
                  kScontrib = kSray1 + align256(16ull * kPaths * kMaxRecords), kSvis = kScontrib + align256(16ull * kPaths * kMaxRecords),
                  kExtendQ = kSvis + align256(1ull * kPaths * kMaxRecords), kShadowQ = kExtendQ + align256(4ull * kPaths),
                  kOut = kShadowQ + align256(4ull * kPaths * kMaxRecords), kOutStatus = kOut + align256(16ull * kMaxItems),
-                 kQueueCounters = kOutStatus + align256(1ull * kMaxItems), kClaimed = kQueueCounters + align256(16),
+                 kQueueCounters = kOutStatus + align256(1ull * kMaxItems), kClaimed = kQueueCounters + align256(32),
                  kCounters = kClaimed + align256(8), kScratchBytes = kCounters + align256(sizeof(Counters));
 static_assert(kScratchBytes <= 36ull << 20, "the static scratch stays modest (36 MiB)");
 
@@ -146,18 +146,22 @@ extern "C" int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chu
     a.lastExtend = queues + 1;
     a.shadowQ = reinterpret_cast<uint32_t*>(base + kShadowQ);
     a.shadowCount = queues + 2;
+    a.extendNext = queues + 3;
+    a.shadowNext = queues + 4;
+    a.refill = kDefaultRefill;
     a.out = reinterpret_cast<float4*>(base + kOut);
     a.outStatus = base + kOutStatus;
     a.counters = reinterpret_cast<Counters*>(base + kCounters);
     // What must start at zero; the rest is written before it is read.
     cudaMemsetAsync(a.w.state, 0, 4ull * kPaths, st);
     cudaMemsetAsync(a.w.ncount, 0, 4ull * kPaths, st);
-    cudaMemsetAsync(queues, 0, 16, st);
+    cudaMemsetAsync(queues, 0, 32, st);
     cudaMemsetAsync(a.claimed, 0, 8, st);
     cudaMemsetAsync(a.counters, 0, sizeof(Counters), st);
     cudaMemsetAsync(a.outStatus, X2_SKIP, items, st);
     const int gridLogic = int((kPaths + kWaveBlock - 1) / kWaveBlock);
-    const int gridWork = smCount * 16;
+    const int gridWork = smCount * int(kDefaultBlocksPerSm);
+    const WaveKernels wk = waveKernels(kDefaultTraceBlocks, kDefaultShadeBlocks);
     const uint64_t maxIter = items * (uint64_t(c.max_depth) + 2) / kPaths + uint64_t(c.max_depth) + 64;
     uint32_t last = 1;
     for (uint64_t it = 0; last; ++it) {
@@ -167,9 +171,9 @@ extern "C" int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chu
         }
         wfResetQueues<<<1, 32, 0, st>>>(a);
         wfLogic<<<gridLogic, kWaveBlock, 0, st>>>(a);
-        wfExtend<<<gridWork, kWaveBlock, 0, st>>>(a);
-        wfShade<<<gridWork, kWaveBlock, 0, st>>>(a);
-        wfShadow<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
         wfResetQueues<<<1, 32, 0, st>>>(a);
         const cudaError_t e = cudaMemcpyAsync(&last, queues + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         if (e != cudaSuccess) {

@@ -104,12 +104,18 @@ __device__ __forceinline__ bool triTest(const RayQ& r, const float4& a, const fl
     return true;
 }
 
-__device__ __forceinline__ uint32_t byteOf(uint32_t lo, uint32_t hi, int s) {
-    return ((s < 4 ? lo : hi) >> (8 * (s & 3))) & 0xffu;
+// Byte j of w as an exact float: 0x4B0000bb is 2^23 + bb, less 2^23 (a byte permute and an add, no conversion).
+__device__ __forceinline__ float qbyte(uint32_t w, int j) {
+    return __fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | uint32_t(j))), 8388608.0f);
 }
 
 // One node: the hit mask (bits 24..31 internal children in traversal order, 0..23 leaf triangles), its child and
 // triangle bases and its internal-child mask.
+//
+// Conservative by construction: the quantised child boxes contain the exact ones (the build rounds outward), and the
+// computed slab distance q * s + a = q * 2^e * (1/d) + (p - o) * (1/d) differs from the exact one by at most four
+// roundings of its terms (1/d, p - o, the product, the FMA), under 2^-22 (|a| + 255 |s|); every slab is widened by
+// 2^-21 (|a| + 255 |s|) each way, folded into the constant term.
 __device__ __forceinline__ uint32_t visitNode(const Node8* __restrict__ nodes, uint32_t index, const RayQ& r, float tmin, float tmax,
                                               uint32_t& childBase, uint32_t& triBase, uint32_t& imask) {
     const uint4* p = reinterpret_cast<const uint4*>(nodes + index);
@@ -121,30 +127,28 @@ __device__ __forceinline__ uint32_t visitNode(const Node8* __restrict__ nodes, u
     triBase = n1.y;
     const float sx = __uint_as_float(ex << 23) * r.ix, sy = __uint_as_float(ey << 23) * r.iy, sz = __uint_as_float(ez << 23) * r.iz;
     const float ax = (px - r.ox) * r.ix, ay = (py - r.oy) * r.iy, az = (pz - r.oz) * r.iz;
-    // The slab distances q * s + a carry an absolute error of a few ulps of their terms (not of their result, which
-    // can be much smaller): widen by (|a| + 255 |s|) * 2^-21 each way, folded into the constant term.
     const float wx = (fabsf(ax) + 255.0f * fabsf(sx)) * 0x1p-21f, wy = (fabsf(ay) + 255.0f * fabsf(sy)) * 0x1p-21f,
                 wz = (fabsf(az) + 255.0f * fabsf(sz)) * 0x1p-21f;
     const float axn = ax - wx, axf = ax + wx, ayn = ay - wy, ayf = ay + wy, azn = az - wz, azf = az + wz;
+    // The near and far planes' quantised words for the ray's direction signs, chosen once a node.
     const bool fx = r.ix >= 0.0f, fy = r.iy >= 0.0f, fz = r.iz >= 0.0f;
+    const uint32_t nx0 = fx ? n2.x : n3.z, nx1 = fx ? n2.y : n3.w, fx0 = fx ? n3.z : n2.x, fx1 = fx ? n3.w : n2.y;
+    const uint32_t ny0 = fy ? n2.z : n4.x, ny1 = fy ? n2.w : n4.y, fy0 = fy ? n4.x : n2.z, fy1 = fy ? n4.y : n2.w;
+    const uint32_t nz0 = fz ? n3.x : n4.z, nz1 = fz ? n3.y : n4.w, fz0 = fz ? n4.z : n3.x, fz1 = fz ? n4.w : n3.y;
+    // Child metadata with internal slots' bit positions (24 + slot: bits 3 and 4 both set, which no triangle offset
+    // has) permuted to the ray's near-to-far order; an empty slot's byte is 0 and sets nothing.
+    const uint32_t m0 = n1.z ^ ((((n1.z & (n1.z << 1)) & 0x10101010u) >> 4) * r.oct7);
+    const uint32_t m1 = n1.w ^ ((((n1.w & (n1.w << 1)) & 0x10101010u) >> 4) * r.oct7);
     uint32_t hits = 0;
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
-        const uint32_t meta = byteOf(n1.z, n1.w, s);
-        const float qlx = float(byteOf(n2.x, n2.y, s)), qly = float(byteOf(n2.z, n2.w, s)), qlz = float(byteOf(n3.x, n3.y, s));
-        const float qhx = float(byteOf(n3.z, n3.w, s)), qhy = float(byteOf(n4.x, n4.y, s)), qhz = float(byteOf(n4.z, n4.w, s));
-        const float nx = __fmaf_rn(fx ? qlx : qhx, sx, axn), fxx = __fmaf_rn(fx ? qhx : qlx, sx, axf);
-        const float ny = __fmaf_rn(fy ? qly : qhy, sy, ayn), fyy = __fmaf_rn(fy ? qhy : qly, sy, ayf);
-        const float nz = __fmaf_rn(fz ? qlz : qhz, sz, azn), fzz = __fmaf_rn(fz ? qhz : qlz, sz, azf);
-        float entry = fmaxf(nx, fmaxf(ny, nz)), exit = fminf(fxx, fminf(fyy, fzz));
-        entry = __fsub_rn(entry, fabsf(entry) * 0x1p-20f);
-        exit = __fadd_rn(exit, fabsf(exit) * 0x1p-20f);
-        entry = fmaxf(entry, tmin);
-        exit = fminf(exit, tmax);
-        if (meta && entry <= exit) {
-            const uint32_t internal = (imask >> s) & 1u;
-            hits |= (meta >> 5) << ((meta & 31u) ^ (internal ? r.oct7 : 0u));
-        }
+        const int j = s & 3;
+        const float nx = __fmaf_rn(qbyte(s < 4 ? nx0 : nx1, j), sx, axn), fxx = __fmaf_rn(qbyte(s < 4 ? fx0 : fx1, j), sx, axf);
+        const float ny = __fmaf_rn(qbyte(s < 4 ? ny0 : ny1, j), sy, ayn), fyy = __fmaf_rn(qbyte(s < 4 ? fy0 : fy1, j), sy, ayf);
+        const float nz = __fmaf_rn(qbyte(s < 4 ? nz0 : nz1, j), sz, azn), fzz = __fmaf_rn(qbyte(s < 4 ? fz0 : fz1, j), sz, azf);
+        const float entry = fmaxf(fmaxf(nx, fmaxf(ny, nz)), tmin), exit = fminf(fminf(fxx, fminf(fyy, fzz)), tmax);
+        const uint32_t meta = ((s < 4 ? m0 : m1) >> (8 * j)) & 0xffu;
+        if (entry <= exit) hits |= (meta >> 5) << (meta & 31u);
     }
     return hits;
 }
@@ -212,6 +216,78 @@ static __device__ __noinline__ uint32_t traceClosest(const Bvh8 bvh, const RayQ&
     tHit = tBest;
     *leafOut = bestLeaf;
     return best;
+}
+
+// A ray traced one node a step, for kernels that keep every lane of a warp busy by handing a lane whose ray is done
+// the next ray of the queue (persistent threads with dynamic ray fetch; Aila and Laine 2009). The steps visit the
+// same nodes and test the same triangles, in the same order, as traceClosest / traceAny, so the results are the same.
+struct Walk {
+    uint2 stack[kStack];
+    int sp;
+    uint32_t base, bits, imask;  // the node group being visited: its child base, hit mask, internal-child mask
+    float tmin, tmax;            // closest hit: tmax is the nearest hit so far
+    uint32_t best, bestLeaf;     // closest hit: scene triangle (~0u none) and leaf-order index; any hit: 1 if occluded
+    uint32_t nodes, tris;        // counting mode
+};
+
+template <bool kAny>
+__device__ __forceinline__ void walkStart(Walk& w, const RayQ& r, float tmin, float tmax) {
+    w.sp = 0;
+    w.base = 0;
+    w.bits = 0x80000000u;
+    w.imask = 1u << (7u ^ r.oct7);
+    w.tmin = tmin;
+    w.tmax = tmax;
+    w.best = kAny ? 0u : ~0u;
+    w.bestLeaf = 0;
+}
+
+// One node visit and its triangle tests; true once the ray is done.
+template <bool kAny>
+__device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk& w, uint32_t* overflow) {
+    if (!(w.bits & 0xff000000u)) {
+        if (w.sp == 0) return true;
+        const uint2 e = w.stack[--w.sp];
+        w.base = e.x;
+        w.bits = e.y & 0xff000000u;
+        w.imask = (e.y >> 16) & 0xffu;
+    }
+    const uint32_t b = __ffs(w.bits >> 24) - 1;
+    w.bits &= ~(1u << (24 + b));
+    const uint32_t slot = b ^ r.oct7;
+    const uint32_t child = w.base + __popc(w.imask & ((1u << slot) - 1u));
+    if (w.bits & 0xff000000u) {
+        if (w.sp < kStack) w.stack[w.sp++] = make_uint2(w.base, w.bits | (w.imask << 16));
+        else atomicAdd(overflow, 1u);
+    }
+    uint32_t childBase, triBase, imask;
+    const uint32_t hits = visitNode(bvh.nodes, child, r, w.tmin - r.eps, w.tmax + r.eps, childBase, triBase, imask);
+    ++w.nodes;
+    uint32_t tBits = hits & 0x00ffffffu;
+    while (tBits) {
+        const uint32_t k = __ffs(tBits) - 1;
+        tBits &= tBits - 1;
+        const float4* tp = reinterpret_cast<const float4*>(bvh.tris + triBase + k);
+        const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+        ++w.tris;
+        float t;
+        if (triTest(r, v0, v1, v2, w.tmin, w.tmax, t)) {
+            if (kAny) {
+                w.best = 1;
+                return true;
+            }
+            const uint32_t id = __float_as_uint(v0.w);
+            if (t < w.tmax || (t == w.tmax && id < w.best)) {
+                w.tmax = t;
+                w.best = id;
+                w.bestLeaf = triBase + k;
+            }
+        }
+    }
+    w.base = childBase;
+    w.bits = hits & 0xff000000u;
+    w.imask = imask;
+    return !(w.bits & 0xff000000u) && w.sp == 0;
 }
 
 // Any hit on [tmin, tmax].

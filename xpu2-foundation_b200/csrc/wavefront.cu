@@ -192,9 +192,64 @@ __global__ void __launch_bounds__(kWaveBlock) wfLogic(WaveArgs a) {
 }
 
 // ---- extend: closest hits ----
-__global__ void __launch_bounds__(kWaveBlock) wfExtend(WaveArgs a) {
+// Persistent traversal over a queue: each lane walks its ray a node a step; a warp fetches the next rays of the queue
+// (one atomic a warp) for its idle lanes once `refill` of them are idle, so lanes whose rays end early are not left
+// waiting for the warp's longest ray. kAny: shadow records (visibility out), else extend rays (closest hit out).
+template <bool kAny, bool kStats>
+__device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, const uint32_t* __restrict__ queue, uint32_t* next) {
+    const WaveState& w = a.w;
+    const Bvh8 bvh = a.scene.bvh;
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    Walk walk;
+    walk.nodes = walk.tris = 0;
+    RayQ r;
+    uint32_t k = 0, rays = 0;
+    bool live = false, drained = false;
+    for (;;) {
+        const uint32_t idle = __ballot_sync(full, !live);
+        if (!drained && __popc(idle) >= a.refill) {
+            const uint32_t leader = __ffs(idle) - 1, want = __popc(idle);
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(next, want);
+            base = __shfl_sync(full, base, leader);
+            drained = base + want >= n;
+            if (!live) {
+                const uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
+                if (i < n) {
+                    k = queue[i];
+                    const float4 r0 = kAny ? w.sray0[k] : w.ray0[k], r1 = kAny ? w.sray1[k] : w.ray1[k];
+                    r = makeRay(bvh, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
+                    walkStart<kAny>(walk, r, r0.w, r1.w);
+                    live = true;
+                    ++rays;
+                }
+            }
+        }
+        if (!__any_sync(full, live)) break;
+        if (live && walkStep<kAny>(bvh, r, walk, a.scene.overflow)) {
+            if (kAny) w.svis[k] = walk.best ? 0 : 1;
+            else w.hit[k] = make_uint2(walk.best == ~0u ? ~0u : walk.bestLeaf, __float_as_uint(walk.tmax));
+            live = false;
+        }
+    }
+    if (kStats) {
+        TraversalStats* st = a.scene.stats + (kAny ? 1 : 0);
+        atomicAdd(&st->rays, (unsigned long long)rays);
+        atomicAdd(&st->nodes, (unsigned long long)walk.nodes);
+        atomicAdd(&st->tris, (unsigned long long)walk.tris);
+    }
+}
+
+__device__ __forceinline__ void extendBody(const WaveArgs& a) {
     const WaveState& w = a.w;
     const uint32_t n = *a.extendCount;
+    if (a.refill) {
+        if (a.scene.stats) persistentTrace<false, true>(a, n, a.extendQ, a.extendNext);
+        else persistentTrace<false, false>(a, n, a.extendQ, a.extendNext);
+        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters->trace, (unsigned long long)n);
+        return;
+    }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t p = a.extendQ[i];
         const float4 r0 = w.ray0[p], r1 = w.ray1[p];
@@ -231,7 +286,7 @@ struct WaveSink {
     }
 };
 
-__global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) {
+__device__ __forceinline__ void shadeBody(const WaveArgs& a) {
     const WaveState& w = a.w;
     const SceneView& s = a.scene;
     const uint32_t n = *a.extendCount;
@@ -303,9 +358,14 @@ __global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) {
 }
 
 // ---- shadow: any hits ----
-__global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) {
+__device__ __forceinline__ void shadowBody(const WaveArgs& a) {
     const WaveState& w = a.w;
     const uint32_t n = *a.shadowCount;
+    if (a.refill) {
+        if (a.scene.stats) persistentTrace<true, true>(a, n, a.shadowQ, a.shadowNext);
+        else persistentTrace<true, false>(a, n, a.shadowQ, a.shadowNext);
+        return;
+    }
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t k = a.shadowQ[i];
         const float4 r0 = w.sray0[k], r1 = w.sray1[k];
@@ -316,6 +376,32 @@ __global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) {
     }
 }
 
+// The kernels, each in a few occupancy variants (blocks of kWaveBlock threads a SM that the register allocation must
+// allow), chosen at launch (x2_wavefront_tune).
+__global__ void __launch_bounds__(kWaveBlock) wfExtend(WaveArgs a) { extendBody(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) { shadeBody(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) { shadowBody(a); }
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfExtendOcc(WaveArgs a) {
+    extendBody(a);
+}
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadeOcc(WaveArgs a) {
+    shadeBody(a);
+}
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadowOcc(WaveArgs a) {
+    shadowBody(a);
+}
+
+WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks) {
+    WaveKernels k;
+    k.extend = traceBlocks >= 12 ? wfExtendOcc<12> : traceBlocks >= 10 ? wfExtendOcc<10> : wfExtend;
+    k.shadow = traceBlocks >= 12 ? wfShadowOcc<12> : traceBlocks >= 10 ? wfShadowOcc<10> : wfShadow;
+    k.shade = shadeBlocks >= 4 ? wfShadeOcc<4> : shadeBlocks >= 3 ? wfShadeOcc<3> : wfShade;
+    return k;
+}
+
 // Queue counters for the next iteration: the extend and shadow counts start at zero; the previous counts are kept
 // for the host (the graph's last extend count tells whether paths remain).
 __global__ void wfResetQueues(WaveArgs a) {
@@ -323,6 +409,8 @@ __global__ void wfResetQueues(WaveArgs a) {
         *a.lastExtend = *a.extendCount;
         *a.extendCount = 0;
         *a.shadowCount = 0;
+        *a.extendNext = 0;
+        *a.shadowNext = 0;
     }
 }
 

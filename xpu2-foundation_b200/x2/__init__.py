@@ -119,7 +119,8 @@ def library():
         "x2_wavefront_reserve": ([vp, u32], i32), "x2_launch_wavefront": ([vp, vp, u32], i32),
         "x2_render_frame_wavefront": ([vp, u32, u32], i32), "x2_items_download": ([vp, vp, vp, u64], i32),
         "x2_wavefront_info": ([vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)], i32),
-        "x2_wavefront_timing": ([vp, i32, vp], i32),
+        "x2_wavefront_timing": ([vp, i32, vp], i32), "x2_wavefront_queues": ([vp, vp, u32], i32),
+        "x2_wavefront_tune": ([vp, u32, u32, u32, u32], i32),
         "x2_launch_wavefront_static": ([vp, vp, u32, u32, vp, vp, C.POINTER(u64)], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
@@ -335,6 +336,18 @@ class Scene:
         ms = np.zeros(5, np.float32)
         _check(library().x2_wavefront_timing(self._h, -1 if on is None else int(bool(on)), _ptr(ms)))
         return dict(zip(("logic", "extend", "shade", "shadow", "film"), ms.tolist()))
+
+    def wavefront_tune(self, refill=8, blocks_per_sm=16, trace_blocks=0, shade_blocks=4):
+        """Launch shape of the wavefront kernels: idle lanes that make a traversal warp fetch rays (0: one ray a
+        thread), grid blocks a SM, and the traversal and shade kernels' occupancy variants (blocks a SM)."""
+        _check(library().x2_wavefront_tune(self._h, refill, blocks_per_sm, trace_blocks, shade_blocks))
+
+    def wavefront_queues(self):
+        """The last timed launch's per-iteration queue sizes as an (iterations, 2) array: rays extended, shadow rays."""
+        n = self.wavefront_info()["iterations"]
+        sizes = np.zeros(2 * min(n, 4096), np.uint32)
+        _check(library().x2_wavefront_queues(self._h, _ptr(sizes), sizes.size))
+        return sizes.reshape(-1, 2)
 
     def wavefront_info(self):
         p, r, i = C.c_uint32(), C.c_uint32(), C.c_uint32()
