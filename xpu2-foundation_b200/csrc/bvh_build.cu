@@ -155,6 +155,160 @@ __device__ __forceinline__ float area(const Aabb& b) {
     return x * y + y * z + z * x;
 }
 
+__device__ __forceinline__ bool isLeafNode(uint32_t b, uint32_t n) { return b >= n - 1; }
+
+__device__ __forceinline__ Aabb loadBox(const Aabb* box, uint32_t i) {
+    const float* p = reinterpret_cast<const float*>(box + i);
+    Aabb b;
+    for (int k = 0; k < 3; ++k) {
+        b.lo[k] = __ldcg(p + k);
+        b.hi[k] = __ldcg(p + 3 + k);
+    }
+    return b;
+}
+
+__device__ __forceinline__ void grow(Aabb& a, const Aabb& b) {
+    for (int k = 0; k < 3; ++k) {
+        a.lo[k] = fminf(a.lo[k], b.lo[k]);
+        a.hi[k] = fmaxf(a.hi[k], b.hi[k]);
+    }
+}
+
+// Treelet restructuring (Karras and Aila 2013, "Fast Parallel Construction of High-Quality Bounding Volume
+// Hierarchies"): bottom up, as refit, each internal node of at least kTreelet triangles is the root of a treelet of
+// kTreelet subtrees (grown by opening the largest-area subtree), rearranged into the binary tree over them of least
+// surface-area cost (Ci per internal node's area, Ct per triangle's leaf area), found by dynamic programming over the
+// 2^kTreelet - 1 subsets. The treelet keeps its root and reuses its internal nodes; subtrees below it are final.
+// Reads of nodes other threads wrote go through L2 (__ldcg), after the arrival counter that orders them.
+constexpr int kTreelet = 7;
+constexpr float kCi = 1.2f, kCt = 1.0f;
+constexpr int kRestructurePasses = 2;
+
+__device__ void optimiseTreelet(uint32_t root, uint32_t n, uint32_t* left, uint32_t* right, uint32_t* parent, Aabb* box, uint32_t* count,
+                                float* cost) {
+    uint32_t L[kTreelet], I[kTreelet - 1];
+    float La[kTreelet];
+    int nl = 2, ni = 1;
+    I[0] = root;
+    L[0] = __ldcg(left + root);
+    L[1] = __ldcg(right + root);
+    La[0] = area(loadBox(box, L[0]));
+    La[1] = area(loadBox(box, L[1]));
+    while (nl < kTreelet) {
+        int j = -1;
+        float best = -1.0f;
+        for (int i = 0; i < nl; ++i)
+            if (!isLeafNode(L[i], n) && La[i] > best) {
+                best = La[i];
+                j = i;
+            }
+        if (j < 0) break;
+        const uint32_t x = L[j];
+        I[ni++] = x;
+        L[j] = __ldcg(left + x);
+        L[nl] = __ldcg(right + x);
+        La[j] = area(loadBox(box, L[j]));
+        La[nl] = area(loadBox(box, L[nl]));
+        ++nl;
+    }
+    Aabb lb[kTreelet];
+    float lc[kTreelet];
+    uint32_t lcount[kTreelet];
+    for (int i = 0; i < nl; ++i) {
+        lb[i] = loadBox(box, L[i]);
+        lc[i] = __ldcg(cost + L[i]);
+        lcount[i] = __ldcg(count + L[i]);
+    }
+    const uint32_t all = (1u << nl) - 1u;
+    float c[1 << kTreelet], sa[1 << kTreelet];
+    uint8_t part[1 << kTreelet];
+    for (uint32_t S = 1; S <= all; ++S) {
+        Aabb b = lb[__ffs(S) - 1];
+        for (uint32_t m = S & (S - 1); m; m &= m - 1) grow(b, lb[__ffs(m) - 1]);
+        sa[S] = area(b);
+        if (!(S & (S - 1))) {
+            c[S] = lc[__ffs(S) - 1];
+            part[S] = 0;
+            continue;
+        }
+        const uint32_t lowest = S & (0u - S);
+        float best = FLT_MAX;
+        uint32_t bp = lowest;
+        for (uint32_t P = (S - 1) & S; P; P = (P - 1) & S) {
+            if (!(P & lowest)) continue;
+            const float v = c[P] + c[S ^ P];
+            if (v < best) {
+                best = v;
+                bp = P;
+            }
+        }
+        c[S] = kCi * sa[S] + best;
+        part[S] = uint8_t(bp);
+    }
+    // Rebuild top down: each subset of two or more subtrees takes the next internal node of the treelet.
+    uint32_t stackS[kTreelet], stackN[kTreelet];
+    int sp = 0, next = 1;
+    stackS[sp] = all;
+    stackN[sp++] = root;
+    while (sp) {
+        --sp;
+        const uint32_t S = stackS[sp], nd = stackN[sp];
+        const uint32_t P = part[S], Q = S ^ P;
+        uint32_t child[2];
+        const uint32_t sub[2] = {P, Q};
+        for (int h = 0; h < 2; ++h) {
+            if (!(sub[h] & (sub[h] - 1))) {
+                child[h] = L[__ffs(sub[h]) - 1];
+            } else {
+                child[h] = I[next++];
+                stackS[sp] = sub[h];
+                stackN[sp++] = child[h];
+            }
+            parent[child[h]] = nd;
+        }
+        left[nd] = child[0];
+        right[nd] = child[1];
+        Aabb b = lb[__ffs(S) - 1];
+        uint32_t cnt = 0;
+        for (uint32_t m = S; m; m &= m - 1) {
+            grow(b, lb[__ffs(m) - 1]);
+            cnt += lcount[__ffs(m) - 1];
+        }
+        box[nd] = b;
+        count[nd] = cnt;
+        cost[nd] = c[S];
+    }
+}
+
+__global__ void restructure(uint32_t n, uint32_t* left, uint32_t* right, uint32_t* parent, Aabb* box, uint32_t* count, float* cost,
+                            unsigned* flags) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    uint32_t node = n - 1 + k;
+    cost[node] = kCt * area(box[node]);
+    if (n == 1) return;
+    __threadfence();
+    node = __ldcg(parent + node);
+    for (;;) {
+        if (atomicAdd(&flags[node], 1u) == 0u) return;  // the first arrival leaves the node to the second
+        __threadfence();
+        const uint32_t l = __ldcg(left + node), r = __ldcg(right + node);
+        const uint32_t cnt = __ldcg(count + l) + __ldcg(count + r);
+        if (cnt >= uint32_t(kTreelet)) {
+            optimiseTreelet(node, n, left, right, parent, box, count, cost);
+        } else {
+            Aabb b = loadBox(box, l);
+            grow(b, loadBox(box, r));
+            box[node] = b;
+            count[node] = cnt;
+            cost[node] = kCi * area(b) + __ldcg(cost + l) + __ldcg(cost + r);
+        }
+        __threadfence();
+        if (node == 0) return;
+        node = __ldcg(parent + node);
+    }
+}
+
 struct CollapseArgs {
     uint32_t n;
     const uint32_t* left;
@@ -175,10 +329,21 @@ struct CollapseArgs {
     uint32_t* overflow;
 };
 
-__device__ __forceinline__ bool isLeafNode(uint32_t b, uint32_t n) { return b >= n - 1; }
 
 // One wide node from binary node `b`: open the largest-area internal node until eight children; binary subtrees of
 // at most three triangles become leaves; order the slots by direction octant; quantise the child boxes.
+__global__ void countLeafTriangles(const TriRec* __restrict__ tris, uint32_t n, unsigned* seen) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t id = __float_as_uint(tris[i].v0.w);
+    if (id < n) atomicAdd(seen + id, 1u);
+}
+
+__global__ void checkLeafTriangles(const unsigned* __restrict__ seen, uint32_t n, uint32_t* bad) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && seen[i] != 1u) atomicAdd(bad, 1u);
+}
+
 __global__ void collapse(CollapseArgs a) {
     const uint32_t q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= a.queueInCount) return;
@@ -193,14 +358,19 @@ __global__ void collapse(CollapseArgs a) {
         c[nc++] = a.right[item.x];
     }
     while (nc < 8) {
+        // Subtrees of more than three triangles first (each would otherwise become a node of its own); then the small
+        // ones, whose triangles stay in this node either way but get tighter boxes.
         int best = -1;
         float bestArea = -1.0f;
+        bool bestBig = false;
         for (int i = 0; i < nc; ++i) {
             if (isLeafNode(c[i], n)) continue;
+            const bool big = a.count[c[i]] > 3;
             const float s = area(a.box[c[i]]);
-            if (s > bestArea) {
+            if ((big && !bestBig) || (big == bestBig && s > bestArea)) {
                 bestArea = s;
                 best = i;
+                bestBig = big;
             }
         }
         if (best < 0) break;
@@ -366,6 +536,7 @@ int buildBvh(const float* dVertices, const uint32_t* dTriangles, uint32_t n, cud
     Aabb *triBox = nullptr, *box = nullptr;
     uint64_t *keys = nullptr, *keysSorted = nullptr;
     uint32_t *values = nullptr, *order = nullptr, *left = nullptr, *right = nullptr, *parent = nullptr, *count = nullptr;
+    float* cost = nullptr;
     unsigned *flags = nullptr, *sceneBox = nullptr, *counters = nullptr;
     uint2 *qa = nullptr, *qb = nullptr;
     void* temp = nullptr;
@@ -389,6 +560,7 @@ int buildBvh(const float* dVertices, const uint32_t* dTriangles, uint32_t n, cud
     CK(cudaMallocAsync(&right, sizeof(uint32_t) * n, stream));
     CK(cudaMallocAsync(&parent, sizeof(uint32_t) * bn, stream));
     CK(cudaMallocAsync(&count, sizeof(uint32_t) * bn, stream));
+    CK(cudaMallocAsync(&cost, sizeof(float) * bn, stream));
     CK(cudaMallocAsync(&flags, sizeof(unsigned) * n, stream));
     CK(cudaMallocAsync(&sceneBox, sizeof(unsigned) * 6, stream));
     CK(cudaMallocAsync(&counters, sizeof(uint32_t) * 4, stream));
@@ -408,6 +580,11 @@ int buildBvh(const float* dVertices, const uint32_t* dTriangles, uint32_t n, cud
     if (n > 1) karras<<<int((n - 1 + kBlock - 1) / kBlock), kBlock, 0, stream>>>(keysSorted, n, left, right, parent);
     refit<<<grid, kBlock, 0, stream>>>(n, order, triBox, left, right, parent, box, count, flags);
     CK(cudaGetLastError());
+    for (int pass = 0; pass < kRestructurePasses && n >= uint32_t(kTreelet); ++pass) {
+        CK(cudaMemsetAsync(flags, 0, sizeof(unsigned) * n, stream));
+        restructure<<<grid, kBlock, 0, stream>>>(n, left, right, parent, box, count, cost, flags);
+        CK(cudaGetLastError());
+    }
     // Wide node 0 is the root; counters: [0] wide nodes, [1] triangles placed, [2] next queue size, [3] overflow.
     host[0] = 1;
     CK(cudaMemcpyAsync(counters, host, sizeof(uint32_t), cudaMemcpyHostToDevice, stream));
@@ -449,6 +626,17 @@ int buildBvh(const float* dVertices, const uint32_t* dTriangles, uint32_t n, cud
         setError("BVH collapse placed %u of %u triangles (%u overflows)", host[1], n, host[3]);
         goto fail;
     }
+    // Every scene triangle in exactly one leaf (the restructured hierarchy is a tree over all of them).
+    CK(cudaMemsetAsync(flags, 0, sizeof(unsigned) * n, stream));
+    CK(cudaMemsetAsync(counters + 3, 0, sizeof(uint32_t), stream));
+    countLeafTriangles<<<grid, kBlock, 0, stream>>>(tris, n, flags);
+    checkLeafTriangles<<<grid, kBlock, 0, stream>>>(flags, n, counters + 3);
+    CK(cudaMemcpyAsync(host + 3, counters + 3, sizeof(uint32_t), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
+    if (host[3] != 0) {
+        setError("BVH build: %u triangles not in exactly one leaf", host[3]);
+        goto fail;
+    }
     out->nodes = nodes;
     out->tris = tris;
     out->nodeCount = host[0];
@@ -467,6 +655,7 @@ fail:
     cudaFreeAsync(right, stream);
     cudaFreeAsync(parent, stream);
     cudaFreeAsync(count, stream);
+    cudaFreeAsync(cost, stream);
     cudaFreeAsync(flags, stream);
     cudaFreeAsync(sceneBox, stream);
     cudaFreeAsync(counters, stream);
