@@ -188,12 +188,20 @@ int x2_wavefront_info(x2_scene* scene, uint32_t* paths, uint32_t* records, uint3
 /* Per-kernel timing of wavefront launches (a diagnostic: no graph, a host sync an iteration). on: 1 on, 0 off, -1
  * unchanged; ms (5 floats, or null): the last timed launch's logic, extend, shade, shadow and film-reduce times. */
 int x2_wavefront_timing(x2_scene* scene, int on, float* ms);
-/* Wavefront launch shape (no reference counterpart; the autotuner's knobs): refill = 1..32 idle lanes of a
- * traversal warp that make it fetch the next rays of its queue (0: one ray a thread, no fetch); blocks_per_sm = the
- * traversal and shade grids' blocks a SM (1..32); trace_blocks / shade_blocks = the occupancy variant of the traversal
- * and shade kernels, blocks a SM their registers must allow (traversal 0, 10 or 12; shade 0, 3 or 4; 0: the compiler's
- * choice). Defaults: refill 8, blocks_per_sm 16, trace_blocks 0, shade_blocks 4. */
-int x2_wavefront_tune(x2_scene* scene, uint32_t refill, uint32_t blocks_per_sm, uint32_t trace_blocks, uint32_t shade_blocks);
+/* Wavefront launch shape (no reference counterpart; the autotuner's knobs). The results do not depend on it. */
+typedef struct x2_wavefront_shape {
+    uint32_t paths;          /* path slots in flight (0: 2^20, fewer when the launch has fewer items) */
+    uint32_t refill;         /* 1..32 idle lanes that make a traversal warp fetch the next rays of its queue (0: one
+                                ray a thread, no fetch) */
+    uint32_t blocks_per_sm;  /* traversal and shade grids: blocks a SM, 1..32 */
+    uint32_t trace_blocks;   /* traversal kernels' occupancy variant: blocks a SM their registers allow (0, 9, 10;
+                                0: the compiler's choice) */
+    uint32_t shade_blocks;   /* shade kernel's occupancy variant (0, 3, 4) */
+    uint32_t tri_limit;      /* triangle tests a lane makes a traversal step, the rest on the next steps (1..32) */
+    uint32_t reserved[2];
+} x2_wavefront_shape;
+void x2_wavefront_shape_defaults(x2_wavefront_shape* shape);
+int x2_wavefront_tune(x2_scene* scene, const x2_wavefront_shape* shape);
 /* The last timed wavefront launch's queue sizes: for each iteration, rays extended then shadow rays (2 a
  * iteration, at most max values). */
 int x2_wavefront_queues(x2_scene* scene, uint32_t* sizes, uint32_t max);

@@ -150,6 +150,7 @@ struct x2_scene {
     uint32_t refill = kDefaultRefill;  // idle lanes that make a traversal warp fetch rays (0: one ray a thread)
     uint32_t blocksPerSm = kDefaultBlocksPerSm;  // traversal and shade grids: blocks a SM
     uint32_t traceBlocks = kDefaultTraceBlocks, shadeBlocks = kDefaultShadeBlocks;  // occupancy variants
+    uint32_t triLimit = kDefaultTriLimit;  // triangle tests a traversal step
     uint32_t* hostLast = nullptr;      // pinned
     unsigned long long* claimed = nullptr;
     float4* out = nullptr;
@@ -839,15 +840,28 @@ int x2_wavefront_reserve(x2_scene* s, uint32_t paths) {
     return X2_OK;
 }
 
-int x2_wavefront_tune(x2_scene* s, uint32_t refill, uint32_t blocks_per_sm, uint32_t trace_blocks, uint32_t shade_blocks) {
-    if (!s || refill > 32 || blocks_per_sm < 1 || blocks_per_sm > 32 || trace_blocks > 32 || shade_blocks > 32) {
-        setError("refill is 0..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32");
+void x2_wavefront_shape_defaults(x2_wavefront_shape* shape) {
+    if (!shape) return;
+    *shape = x2_wavefront_shape{};
+    shape->refill = kDefaultRefill;
+    shape->blocks_per_sm = kDefaultBlocksPerSm;
+    shape->trace_blocks = kDefaultTraceBlocks;
+    shape->shade_blocks = kDefaultShadeBlocks;
+    shape->tri_limit = kDefaultTriLimit;
+}
+
+int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
+    if (!s || !shape || shape->refill > 32 || shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 || shape->trace_blocks > 32 ||
+        shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32) {
+        setError("refill is 0..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32");
         return X2_EINVAL;
     }
-    s->refill = refill;
-    s->blocksPerSm = blocks_per_sm;
-    s->traceBlocks = trace_blocks;
-    s->shadeBlocks = shade_blocks;
+    s->reservePaths = shape->paths;
+    s->refill = shape->refill;
+    s->blocksPerSm = shape->blocks_per_sm;
+    s->traceBlocks = shape->trace_blocks;
+    s->shadeBlocks = shape->shade_blocks;
+    s->triLimit = shape->tri_limit;
     return X2_OK;
 }
 
@@ -909,6 +923,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     a.extendNext = s->waveCounters + 3;
     a.shadowNext = s->waveCounters + 4;
     a.refill = s->refill;
+    a.triLimit = s->triLimit;
     a.out = s->out;
     a.outStatus = s->outStatus;
     a.counters = sl.counters;

@@ -149,6 +149,7 @@ extern "C" int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chu
     a.extendNext = queues + 3;
     a.shadowNext = queues + 4;
     a.refill = kDefaultRefill;
+    a.triLimit = kDefaultTriLimit;
     a.out = reinterpret_cast<float4*>(base + kOut);
     a.outStatus = base + kOutStatus;
     a.counters = reinterpret_cast<Counters*>(base + kCounters);

@@ -1,8 +1,8 @@
 // Closest-hit and any-hit traversal of the compressed 8-wide BVH (bvh.cuh) for one ray a thread.
 //
 // A node is five 16-byte read-only loads. Its eight children are tested with one FMA a slab (Ylitie et al. 2017:
-// the ray is expressed in the node's quantised frame once, t = q * (2^e / d) + (p - o) / d), widened by 2^-20 of
-// the distance each way so the quantised boxes stay conservative. Hit children enter a 32-bit mask: internal
+// the ray is expressed in the node's quantised frame once, t = q * (2^e / d) + (p - o) / d), widened by a bound on
+// its rounding so the quantised boxes stay conservative (visitNode). Hit children enter a 32-bit mask: internal
 // children on bits 24..31 in near-to-far order for the ray's octant (the build places each child in the slot of
 // the octant it lies toward), leaf triangles on bits 0..23. The stack holds (child base, mask | imask) pairs and
 // lives in registers/local memory; an overflow is counted, never silent.
@@ -25,6 +25,7 @@ struct RayQ {
     uint32_t oct7;     // XOR pattern that orders a node's slots near to far
     int kx, ky, kz;    // the shear's axes
     float Sx, Sy, Sz;
+    float okx, oky, okz;  // the origin's components along kx, ky, kz
     // The triangle test's t carries an absolute error of a few ulps of the distance to the vertices (its sheared
     // products cancel), which a near hit can make large relative to t: boxes are tested against [tmin - eps,
     // tmax + eps], eps = 2^-18 times the ray origin's distance to the farthest corner of the scene's bounds.
@@ -70,20 +71,23 @@ __device__ __forceinline__ RayQ makeRay(const Bvh8& bvh, float ox, float oy, flo
     r.Sx = pick3(dx, dy, dz, kx) / dzz;
     r.Sy = pick3(dx, dy, dz, ky) / dzz;
     r.Sz = 1.0f / dzz;
+    r.okx = pick3(ox, oy, oz, kx);
+    r.oky = pick3(ox, oy, oz, ky);
+    r.okz = pick3(ox, oy, oz, kz);
     return r;
 }
 
 // Watertight ray/triangle test; the operations match the oracle's triHit exactly.
 __device__ __forceinline__ bool triTest(const RayQ& r, const float4& a, const float4& b, const float4& c, float tmin, float tmax, float& tOut) {
-    const float Akx = pick3(a.x, a.y, a.z, r.kx) - pick3(r.ox, r.oy, r.oz, r.kx);
-    const float Aky = pick3(a.x, a.y, a.z, r.ky) - pick3(r.ox, r.oy, r.oz, r.ky);
-    const float Akz = pick3(a.x, a.y, a.z, r.kz) - pick3(r.ox, r.oy, r.oz, r.kz);
-    const float Bkx = pick3(b.x, b.y, b.z, r.kx) - pick3(r.ox, r.oy, r.oz, r.kx);
-    const float Bky = pick3(b.x, b.y, b.z, r.ky) - pick3(r.ox, r.oy, r.oz, r.ky);
-    const float Bkz = pick3(b.x, b.y, b.z, r.kz) - pick3(r.ox, r.oy, r.oz, r.kz);
-    const float Ckx = pick3(c.x, c.y, c.z, r.kx) - pick3(r.ox, r.oy, r.oz, r.kx);
-    const float Cky = pick3(c.x, c.y, c.z, r.ky) - pick3(r.ox, r.oy, r.oz, r.ky);
-    const float Ckz = pick3(c.x, c.y, c.z, r.kz) - pick3(r.ox, r.oy, r.oz, r.kz);
+    const float Akx = pick3(a.x, a.y, a.z, r.kx) - r.okx;
+    const float Aky = pick3(a.x, a.y, a.z, r.ky) - r.oky;
+    const float Akz = pick3(a.x, a.y, a.z, r.kz) - r.okz;
+    const float Bkx = pick3(b.x, b.y, b.z, r.kx) - r.okx;
+    const float Bky = pick3(b.x, b.y, b.z, r.ky) - r.oky;
+    const float Bkz = pick3(b.x, b.y, b.z, r.kz) - r.okz;
+    const float Ckx = pick3(c.x, c.y, c.z, r.kx) - r.okx;
+    const float Cky = pick3(c.x, c.y, c.z, r.ky) - r.oky;
+    const float Ckz = pick3(c.x, c.y, c.z, r.kz) - r.okz;
     const float Ax = Akx - r.Sx * Akz, Ay = Aky - r.Sy * Akz;
     const float Bx = Bkx - r.Sx * Bkz, By = Bky - r.Sy * Bkz;
     const float Cx = Ckx - r.Sx * Ckz, Cy = Cky - r.Sy * Ckz;
@@ -102,6 +106,18 @@ __device__ __forceinline__ bool triTest(const RayQ& r, const float4& a, const fl
     if (!(t >= tmin && t <= tmax)) return false;
     tOut = t;
     return true;
+}
+
+// Three-input max / min (one instruction on sm_100; same NaN rule as fmaxf / fminf).
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+    float r;
+    asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
 }
 
 // Byte j of w as an exact float: 0x4B0000bb is 2^23 + bb, less 2^23 (a byte permute and an add, no conversion).
@@ -146,7 +162,7 @@ __device__ __forceinline__ uint32_t visitNode(const Node8* __restrict__ nodes, u
         const float nx = __fmaf_rn(qbyte(s < 4 ? nx0 : nx1, j), sx, axn), fxx = __fmaf_rn(qbyte(s < 4 ? fx0 : fx1, j), sx, axf);
         const float ny = __fmaf_rn(qbyte(s < 4 ? ny0 : ny1, j), sy, ayn), fyy = __fmaf_rn(qbyte(s < 4 ? fy0 : fy1, j), sy, ayf);
         const float nz = __fmaf_rn(qbyte(s < 4 ? nz0 : nz1, j), sz, azn), fzz = __fmaf_rn(qbyte(s < 4 ? fz0 : fz1, j), sz, azf);
-        const float entry = fmaxf(fmaxf(nx, fmaxf(ny, nz)), tmin), exit = fminf(fminf(fxx, fminf(fyy, fzz)), tmax);
+        const float entry = max3f(nx, ny, fmaxf(nz, tmin)), exit = min3f(fxx, fyy, fminf(fzz, tmax));
         const uint32_t meta = ((s < 4 ? m0 : m1) >> (8 * j)) & 0xffu;
         if (entry <= exit) hits |= (meta >> 5) << (meta & 31u);
     }
@@ -225,6 +241,7 @@ struct Walk {
     uint2 stack[kStack];
     int sp;
     uint32_t base, bits, imask;  // the node group being visited: its child base, hit mask, internal-child mask
+    uint32_t tbase, tbits;       // triangles of the last node still to test: first leaf-order index, mask
     float tmin, tmax;            // closest hit: tmax is the nearest hit so far
     uint32_t best, bestLeaf;     // closest hit: scene triangle (~0u none) and leaf-order index; any hit: 1 if occluded
     uint32_t nodes, tris;        // counting mode
@@ -236,38 +253,47 @@ __device__ __forceinline__ void walkStart(Walk& w, const RayQ& r, float tmin, fl
     w.base = 0;
     w.bits = 0x80000000u;
     w.imask = 1u << (7u ^ r.oct7);
+    w.tbase = 0;
+    w.tbits = 0;
     w.tmin = tmin;
     w.tmax = tmax;
     w.best = kAny ? 0u : ~0u;
     w.bestLeaf = 0;
 }
 
-// One node visit and its triangle tests; true once the ray is done.
+// One step: a node visit (when no triangles are pending) and then at most `triLimit` triangle tests, the rest left
+// for the next steps, so that a lane with a full leaf does not hold its warp for all of them at once. The tests run
+// in the same order whatever the limit. True once the ray is done.
 template <bool kAny>
-__device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk& w, uint32_t* overflow) {
-    if (!(w.bits & 0xff000000u)) {
-        if (w.sp == 0) return true;
-        const uint2 e = w.stack[--w.sp];
-        w.base = e.x;
-        w.bits = e.y & 0xff000000u;
-        w.imask = (e.y >> 16) & 0xffu;
+__device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk& w, uint32_t* overflow, uint32_t triLimit) {
+    if (!w.tbits) {
+        if (!(w.bits & 0xff000000u)) {
+            if (w.sp == 0) return true;
+            const uint2 e = w.stack[--w.sp];
+            w.base = e.x;
+            w.bits = e.y & 0xff000000u;
+            w.imask = (e.y >> 16) & 0xffu;
+        }
+        const uint32_t b = __ffs(w.bits >> 24) - 1;
+        w.bits &= ~(1u << (24 + b));
+        const uint32_t slot = b ^ r.oct7;
+        const uint32_t child = w.base + __popc(w.imask & ((1u << slot) - 1u));
+        if (w.bits & 0xff000000u) {
+            if (w.sp < kStack) w.stack[w.sp++] = make_uint2(w.base, w.bits | (w.imask << 16));
+            else atomicAdd(overflow, 1u);
+        }
+        uint32_t childBase, imask;
+        const uint32_t hits = visitNode(bvh.nodes, child, r, w.tmin - r.eps, w.tmax + r.eps, childBase, w.tbase, imask);
+        ++w.nodes;
+        w.tbits = hits & 0x00ffffffu;
+        w.base = childBase;
+        w.bits = hits & 0xff000000u;
+        w.imask = imask;
     }
-    const uint32_t b = __ffs(w.bits >> 24) - 1;
-    w.bits &= ~(1u << (24 + b));
-    const uint32_t slot = b ^ r.oct7;
-    const uint32_t child = w.base + __popc(w.imask & ((1u << slot) - 1u));
-    if (w.bits & 0xff000000u) {
-        if (w.sp < kStack) w.stack[w.sp++] = make_uint2(w.base, w.bits | (w.imask << 16));
-        else atomicAdd(overflow, 1u);
-    }
-    uint32_t childBase, triBase, imask;
-    const uint32_t hits = visitNode(bvh.nodes, child, r, w.tmin - r.eps, w.tmax + r.eps, childBase, triBase, imask);
-    ++w.nodes;
-    uint32_t tBits = hits & 0x00ffffffu;
-    while (tBits) {
-        const uint32_t k = __ffs(tBits) - 1;
-        tBits &= tBits - 1;
-        const float4* tp = reinterpret_cast<const float4*>(bvh.tris + triBase + k);
+    for (uint32_t n = 0; w.tbits && n < triLimit; ++n) {
+        const uint32_t k = __ffs(w.tbits) - 1;
+        w.tbits &= w.tbits - 1;
+        const float4* tp = reinterpret_cast<const float4*>(bvh.tris + w.tbase + k);
         const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
         ++w.tris;
         float t;
@@ -280,14 +306,11 @@ __device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk& w
             if (t < w.tmax || (t == w.tmax && id < w.best)) {
                 w.tmax = t;
                 w.best = id;
-                w.bestLeaf = triBase + k;
+                w.bestLeaf = w.tbase + k;
             }
         }
     }
-    w.base = childBase;
-    w.bits = hits & 0xff000000u;
-    w.imask = imask;
-    return !(w.bits & 0xff000000u) && w.sp == 0;
+    return !w.tbits && !(w.bits & 0xff000000u) && w.sp == 0;
 }
 
 // Any hit on [tmin, tmax].

@@ -227,7 +227,7 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
             }
         }
         if (!__any_sync(full, live)) break;
-        if (live && walkStep<kAny>(bvh, r, walk, a.scene.overflow)) {
+        if (live && walkStep<kAny>(bvh, r, walk, a.scene.overflow, a.triLimit)) {
             if (kAny) w.svis[k] = walk.best ? 0 : 1;
             else w.hit[k] = make_uint2(walk.best == ~0u ? ~0u : walk.bestLeaf, __float_as_uint(walk.tmax));
             live = false;
@@ -396,8 +396,8 @@ __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadowOcc(WaveArgs a
 
 WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks) {
     WaveKernels k;
-    k.extend = traceBlocks >= 12 ? wfExtendOcc<12> : traceBlocks >= 10 ? wfExtendOcc<10> : wfExtend;
-    k.shadow = traceBlocks >= 12 ? wfShadowOcc<12> : traceBlocks >= 10 ? wfShadowOcc<10> : wfShadow;
+    k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : wfExtend;
+    k.shadow = traceBlocks >= 10 ? wfShadowOcc<10> : traceBlocks >= 9 ? wfShadowOcc<9> : wfShadow;
     k.shade = shadeBlocks >= 4 ? wfShadeOcc<4> : shadeBlocks >= 3 ? wfShadeOcc<3> : wfShade;
     return k;
 }

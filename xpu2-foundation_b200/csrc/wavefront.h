@@ -6,7 +6,8 @@ namespace x2 {
 
 constexpr int kWaveBlock = 128;
 // Launch-shape defaults (x2_wavefront_tune changes them a scene).
-constexpr uint32_t kDefaultRefill = 8, kDefaultBlocksPerSm = 16, kDefaultTraceBlocks = 0, kDefaultShadeBlocks = 4;
+constexpr uint32_t kDefaultRefill = 8, kDefaultBlocksPerSm = 16, kDefaultTraceBlocks = 0, kDefaultShadeBlocks = 4,
+                   kDefaultTriLimit = 1;
 
 // Path slots (structure of arrays, `paths` slots) and shadow-ray records (recordsPerPath a slot).
 struct WaveState {
@@ -43,6 +44,7 @@ struct WaveArgs {
     uint32_t* extendNext;  // the extend and shadow kernels' fetch counters over their queues
     uint32_t* shadowNext;
     uint32_t refill;       // a warp fetches new rays once this many of its lanes are idle (0: one ray a thread)
+    uint32_t triLimit;     // triangle tests a lane makes a traversal step
     float4* out;          // per item: rgb, alpha
     uint8_t* outStatus;   // per item: SampleStatus (Skip for items that are not samples)
     Counters* counters;
@@ -52,7 +54,7 @@ struct WaveArgs {
 cudaError_t uploadSobolWavefront(const uint32_t directions[17][32]);
 
 __global__ void wfLogic(WaveArgs a);
-// The extend, shade and shadow kernels for an occupancy: at least `traceBlocks` / `shadeBlocks` blocks a SM (12, 10
+// The extend, shade and shadow kernels for an occupancy: at least `traceBlocks` / `shadeBlocks` blocks a SM (10, 9
 // or 0 for the traversals; 4, 3 or 0 for shade; 0 leaves the register allocation to the compiler).
 struct WaveKernels {
     void (*extend)(WaveArgs);

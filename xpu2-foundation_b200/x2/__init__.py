@@ -87,6 +87,20 @@ class Counters(C.Structure):
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "pad"}
 
 
+class WavefrontShape(C.Structure):
+    FIELDS = ("paths", "refill", "blocks_per_sm", "trace_blocks", "shade_blocks", "tri_limit")
+    _fields_ = [(f, C.c_uint32) for f in FIELDS] + [("reserved", C.c_uint32 * 2)]
+
+    def as_dict(self):
+        return {k: int(getattr(self, k)) for k in self.FIELDS}
+
+
+def wavefront_shape_defaults():
+    s = WavefrontShape()
+    library().x2_wavefront_shape_defaults(C.byref(s))
+    return s
+
+
 class Completion(C.Structure):
     _fields_ = [("launch", C.c_uint64), ("samples", C.c_uint64), ("errors", C.c_uint64), ("milliseconds", C.c_float), ("pad", C.c_uint32)]
 
@@ -120,7 +134,7 @@ def library():
         "x2_render_frame_wavefront": ([vp, u32, u32], i32), "x2_items_download": ([vp, vp, vp, u64], i32),
         "x2_wavefront_info": ([vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)], i32),
         "x2_wavefront_timing": ([vp, i32, vp], i32), "x2_wavefront_queues": ([vp, vp, u32], i32),
-        "x2_wavefront_tune": ([vp, u32, u32, u32, u32], i32),
+        "x2_wavefront_tune": ([vp, C.POINTER(WavefrontShape)], i32), "x2_wavefront_shape_defaults": ([C.POINTER(WavefrontShape)], None),
         "x2_launch_wavefront_static": ([vp, vp, u32, u32, vp, vp, C.POINTER(u64)], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
@@ -337,10 +351,16 @@ class Scene:
         _check(library().x2_wavefront_timing(self._h, -1 if on is None else int(bool(on)), _ptr(ms)))
         return dict(zip(("logic", "extend", "shade", "shadow", "film"), ms.tolist()))
 
-    def wavefront_tune(self, refill=8, blocks_per_sm=16, trace_blocks=0, shade_blocks=4):
-        """Launch shape of the wavefront kernels: idle lanes that make a traversal warp fetch rays (0: one ray a
-        thread), grid blocks a SM, and the traversal and shade kernels' occupancy variants (blocks a SM)."""
-        _check(library().x2_wavefront_tune(self._h, refill, blocks_per_sm, trace_blocks, shade_blocks))
+    def wavefront_tune(self, **shape):
+        """Launch shape of the wavefront kernels (x2_wavefront_shape fields by name; the others keep their defaults).
+        Returns the shape set, as a dict."""
+        s = wavefront_shape_defaults()
+        for k, v in shape.items():
+            if k not in WavefrontShape.FIELDS:
+                raise ValueError("no wavefront shape field %r" % k)
+            setattr(s, k, int(v))
+        _check(library().x2_wavefront_tune(self._h, C.byref(s)))
+        return s.as_dict()
 
     def wavefront_queues(self):
         """The last timed launch's per-iteration queue sizes as an (iterations, 2) array: rays extended, shadow rays."""
