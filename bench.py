@@ -289,7 +289,11 @@ def run(args):
     alg_bytes, dom_ms = per_kernel[dom]
     launches_per_frame = winfo["iterations"]
     achieved = alg_bytes / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    # DRAM traffic a launch: the ncu capture's DRAM bytes a ray (profiles/traffic.json) times this frame's rays of
+    # that kind a launch; compare with the algorithmic bytes a launch.
     prof = traffic_from_profile().get(dom, {})
+    dom_rays = tc["any" if dom == "shadow" else "closest"]["rays"]
+    traffic = prof["dram_bytes_per_ray"] * dom_rays / launches_per_frame if "dram_bytes_per_ray" in prof and launches_per_frame else None
     if rank == 0:
         base, why = cpu_baseline(s) if world == 1 else (None, "rank 0 at N=1 only")
         line = {
@@ -307,7 +311,9 @@ def run(args):
             "wavefront_over_plain": (value / plain["value"]) if plain else None,
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": chunk_bytes, "d2h_bytes_per_step": film_bytes},
             "roofline": {"bound": "hbm", "kernel": "wf" + dom.capitalize(), "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": prof.get("dram_bytes_per_launch"), "peak_kind": peak_kind,
+                         "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes / launches_per_frame if launches_per_frame else None,
+                         "traffic_source": prof.get("source"),
                          "algorithmic_bytes_per_frame": alg_bytes, "kernel_ms_per_frame": dom_ms,
                          "kernel_ms_by_kind": kms, "traversal": tc,
                          "bytes": {"node": NODE_BYTES, "triangle": TRI_BYTES, "extend_ray": EXTEND_RAY_BYTES, "shadow_ray": SHADOW_RAY_BYTES}},
