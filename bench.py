@@ -328,11 +328,44 @@ def run(args):
         dist.destroy_process_group()
 
 
+def probe_batch(args):
+    """Config 2: its 48 requests (config-1-style scenes of 0.1M..2M triangles, 128^2..1024^2, 4..256 spp, depth 4..32,
+    frame seed 1 + r) rendered in one batched wavefront launch, `--probe-tiles` of them (all by default), after one
+    untimed warm-up batch; every film audited. Prints the aggregate Msamples/s."""
+    import x2
+
+    ctx = x2.Context(0)
+    count = min(48, args.probe_tiles) if args.probe_tiles else 48
+    t0 = time.perf_counter()
+    scenes, triangles = [], 0
+    for r in range(count):
+        s = x2.SyntheticScene(200 + r)
+        scenes.append((s.config, x2.Scene(ctx, s.desc, s.config)))
+        triangles += s.desc.triangle_count
+        s.free()
+    load_s = time.perf_counter() - t0
+    requests = [(sc, 0, cfg.spp) for cfg, sc in scenes]
+    samples = sum(cfg.width * cfg.height * cfg.spp for cfg, _ in scenes)
+    ctx.render_batch(requests)
+    runs = [ctx.render_batch(requests) for _ in range(max(1, args.steps))]
+    for _, sc in scenes:
+        sc.audit()
+    ms = statistics.median(c.milliseconds for c in runs)
+    print(json.dumps({"probe": "batch", "requests": count, "samples": samples, "triangles": triangles, "ms": ms,
+                      "msamples_per_s": samples / ms / 1e3, "errors": int(sum(c.errors for c in runs)), "load_s": load_s,
+                      "shape": x2.wavefront_shape_defaults().as_dict()}))
+    for _, sc in scenes:
+        sc.free()
+    ctx.close()
+
+
 def probe(args):
     """One bounded launch for profilers (ncu): `--probe-tiles` evenly spaced tiles of config 1 at 64 spp, in one form;
     the wavefront form without its graph (`--probe-timed`) so each kernel launch is visible on its own."""
     import x2
 
+    if args.probe == "batch":
+        return probe_batch(args)
     ctx = x2.Context(0)
     s = x2.SyntheticScene(1)
     cfg = s.config
@@ -369,7 +402,7 @@ def main():
     ap.add_argument("--impl", default="x2", choices=["x2", "reference"])
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--skip-plain", action="store_true")
-    ap.add_argument("--probe", choices=["plain", "wavefront"], help="one bounded launch for a profiler, then exit")
+    ap.add_argument("--probe", choices=["plain", "wavefront", "batch"], help="one bounded launch for a profiler, then exit")
     ap.add_argument("--probe-tiles", type=int, default=592)
     ap.add_argument("--probe-timed", action="store_true", help="wavefront probe without its graph (per-kernel launches)")
     args = ap.parse_args()

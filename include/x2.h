@@ -191,17 +191,30 @@ int x2_wavefront_timing(x2_scene* scene, int on, float* ms);
 /* Wavefront launch shape (no reference counterpart; the autotuner's knobs). The results do not depend on it. */
 typedef struct x2_wavefront_shape {
     uint32_t paths;          /* path slots in flight (0: 2^20, fewer when the launch has fewer items) */
-    uint32_t refill;         /* 1..32 idle lanes that make a traversal warp fetch the next rays of its queue (0: one
-                                ray a thread, no fetch) */
+    uint32_t refill;         /* 1..32 idle lanes that make a traversal warp fetch the next rays of its queue */
     uint32_t blocks_per_sm;  /* traversal and shade grids: blocks a SM, 1..32 */
     uint32_t trace_blocks;   /* traversal kernels' occupancy variant: blocks a SM their registers allow (0, 9, 10;
                                 0: the compiler's choice) */
     uint32_t shade_blocks;   /* shade kernel's occupancy variant (0, 3, 4) */
     uint32_t tri_limit;      /* triangle tests a lane makes a traversal step, the rest on the next steps (1..32) */
-    uint32_t reserved[2];
+    uint32_t batch_window;   /* x2_render_batch: work items a window (0: 2^27; at least one chunk a window) */
+    uint32_t reserved[1];
 } x2_wavefront_shape;
 void x2_wavefront_shape_defaults(x2_wavefront_shape* shape);
 int x2_wavefront_tune(x2_scene* scene, const x2_wavefront_shape* shape);
+/* Batched renders (no reference counterpart; the reference renders one plan a lane): a request is one scene's frame,
+ * samples [first, first + count) of every pixel, at the scene's own config (resolution, depth, lights, frame seed). */
+typedef struct x2_request {
+    x2_scene* scene;
+    uint32_t first, count;  /* count 1..2^21 */
+} x2_request;
+/* Renders n requests (1..65535; distinct scenes of ctx, each configured with bsdf_samples = 1) in one wavefront
+ * launch: path slots shared by all requests and regenerated across them, each path in its own scene; the first
+ * request's scene holds the path state and its launch shape (x2_wavefront_tune) applies. Each scene's film is reset
+ * first (as x2_frame_begin(scene, count)) and then holds exactly the film x2_launch_wavefront gives for all its
+ * tiles; x2_film_download / x2_audit read it. Waits. out (or null): samples and errors of the whole batch, its device
+ * milliseconds; the ray counters go to the first scene's x2_counters. */
+int x2_render_batch(x2_ctx* ctx, const x2_request* requests, uint32_t n, x2_completion* out);
 /* The last timed wavefront launch's queue sizes: for each iteration, rays extended then shadow rays (2 a
  * iteration, at most max values). */
 int x2_wavefront_queues(x2_scene* scene, uint32_t* sizes, uint32_t max);
@@ -228,7 +241,9 @@ int x2_traversal_counts(x2_scene* scene, uint64_t* rays, uint64_t* nodes, uint64
 
 /* ---- host-side synthetic scenes (test and bench inputs, not the hot path) ----
  * config_id 0: the closed box with two boxes and a rect light; 1: heightfield + icospheres with 16 rect lights
- * and an environment; 100 + k: a config-1 variant scaled down by k (fewer tiles and spheres) for tests.
+ * and an environment; 100 + k: a config-1 variant scaled down by k (fewer tiles and spheres) for tests;
+ * 200 + r (r < 48): batched request r (config-1-style, 0.1M..2M triangles, 128^2..1024^2, 4..256 spp, depth 4..32,
+ * frame seed 1 + r); 300 + r: the same request shrunk (triangles / 64, resolution and spp / 8).
  * The descriptor and its arrays are owned by the library until x2_scene_desc_free. */
 int x2_scene_generate(uint32_t config_id, uint64_t seed, x2_scene_desc** out, x2_config* config);
 void x2_scene_desc_free(x2_scene_desc* desc);

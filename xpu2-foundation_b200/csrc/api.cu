@@ -3,6 +3,7 @@
 // wait is bounded (x2_wait, x2_synchronize poll events with a timeout instead of blocking).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -151,6 +152,7 @@ struct x2_scene {
     uint32_t blocksPerSm = kDefaultBlocksPerSm;  // traversal and shade grids: blocks a SM
     uint32_t traceBlocks = kDefaultTraceBlocks, shadeBlocks = kDefaultShadeBlocks;  // occupancy variants
     uint32_t triLimit = kDefaultTriLimit;  // triangle tests a traversal step
+    uint32_t batchWindow = 0;              // x2_render_batch: items a window (0: the default)
     uint32_t* hostLast = nullptr;      // pinned
     unsigned long long* claimed = nullptr;
     float4* out = nullptr;
@@ -851,9 +853,9 @@ void x2_wavefront_shape_defaults(x2_wavefront_shape* shape) {
 }
 
 int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
-    if (!s || !shape || shape->refill > 32 || shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 || shape->trace_blocks > 32 ||
-        shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32) {
-        setError("refill is 0..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32");
+    if (!s || !shape || shape->refill < 1 || shape->refill > 32 || shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 ||
+        shape->trace_blocks > 32 || shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32) {
+        setError("refill is 1..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32");
         return X2_EINVAL;
     }
     s->reservePaths = shape->paths;
@@ -862,6 +864,7 @@ int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     s->traceBlocks = shape->trace_blocks;
     s->shadeBlocks = shape->shade_blocks;
     s->triLimit = shape->tri_limit;
+    s->batchWindow = shape->batch_window;
     return X2_OK;
 }
 
@@ -927,6 +930,10 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     a.out = s->out;
     a.outStatus = s->outStatus;
     a.counters = sl.counters;
+    a.scenes = nullptr;
+    a.chunkRequest = nullptr;
+    a.chunkItems = nullptr;
+    a.chunkCount = count;
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
     const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks);
@@ -942,7 +949,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
         for (;;) {
             wfResetQueues<<<1, 32, 0, st>>>(a);
             cudaEventRecord(ev[0], st);
-            wfLogic<<<gridLogic, kWaveBlock, 0, st>>>(a);
+            wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
             cudaEventRecord(ev[1], st);
             wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
             cudaEventRecord(ev[2], st);
@@ -997,7 +1004,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     CUDA_OR(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), X2_ECUDA);
     for (int it = 0; it < kIter; ++it) {
         wfResetQueues<<<1, 32, 0, st>>>(a);
-        wfLogic<<<gridLogic, kWaveBlock, 0, st>>>(a);
+        wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
         wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
         wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
         wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
@@ -1075,6 +1082,226 @@ int x2_items_download(x2_scene* s, float* rgba, uint8_t* status, uint64_t n) {
     if (rgba) cudaMemcpyAsync(rgba, s->out, sizeof(float4) * n, cudaMemcpyDeviceToHost, st);
     if (status) cudaMemcpyAsync(status, s->outStatus, n, cudaMemcpyDeviceToHost, st);
     return x2_wait(s, 600000, nullptr);
+}
+
+// Many renders in one wavefront launch: the requests' chunks (every tile of each frame, its sample range) are one work
+// list; path slots regenerate across requests, each path shading and tracing in its own request's scene. The work list
+// runs in windows of at most kBatchWindow items (the per-item outputs' size); each window's samples are summed into
+// their films in sample order, as a single launch's are, so each film equals the one x2_launch_wavefront gives.
+int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completion* out) {
+    if (!ctx || !req || n == 0 || n > 65535 || !req[0].scene) {
+        setError("a batch takes 1..65535 requests");
+        return X2_EINVAL;
+    }
+    const uint64_t kBatchWindow = req[0].scene->batchWindow ? req[0].scene->batchWindow : (1ull << 27);
+    if (int rc = checkDevice(ctx)) return rc;
+    uint32_t records = 1, maxDepth = 0;
+    for (uint32_t r = 0; r < n; ++r) {
+        x2_scene* s = req[r].scene;
+        if (!s || s->ctx != ctx || !s->configured || req[r].count == 0 || req[r].count > (1u << 21)) {
+            setError("batch request %u: no configured scene of this context, or a sample count outside 1..2^21", r);
+            return X2_EINVAL;
+        }
+        if (s->config.bsdf_samples != 1) {
+            setError("batch request %u: the wavefront form takes one BSDF sample a lobe (bsdf_samples = 1)", r);
+            return X2_EINVAL;
+        }
+        for (uint32_t q = 0; q < r; ++q)
+            if (req[q].scene == s) {
+                setError("batch requests %u and %u render the same scene (one film a scene)", q, r);
+                return X2_EINVAL;
+            }
+        records = std::max(records, s->config.light_count * s->config.light_samples + 1);
+        maxDepth = std::max(maxDepth, s->config.max_depth);
+    }
+    for (uint32_t r = 0; r < n; ++r)
+        if (int rc = x2_frame_begin(req[r].scene, req[r].count)) return rc;
+    // Host tables: each request's scene and film, each chunk's request.
+    std::vector<SceneView> views(n);
+    std::vector<BatchFilm> films(n);
+    std::vector<x2_chunk> chunks;
+    std::vector<uint32_t> chunkReq;
+    for (uint32_t r = 0; r < n; ++r) {
+        x2_scene* s = req[r].scene;
+        views[r] = viewOf(s);
+        views[r].stats = nullptr;
+        films[r] = BatchFilm{s->sums, s->adaptive ? s->odd : nullptr, s->counts};
+        const uint32_t tiles = ((s->config.width + 7) / 8) * ((s->config.height + 7) / 8);
+        for (uint32_t t = 0; t < tiles; ++t) {
+            chunks.push_back(x2_chunk{t, req[r].first, req[r].count, 0});
+            chunkReq.push_back(r);
+        }
+    }
+    const uint32_t chunkTotal = uint32_t(chunks.size());
+    // Windows of whole chunks.
+    std::vector<uint32_t> windowStart{0};
+    uint64_t windowMax = 0;
+    {
+        uint64_t acc = 0;
+        for (uint32_t c = 0; c < chunkTotal; ++c) {
+            const uint64_t items = 64ull * chunks[c].count;
+            if (acc && acc + items > kBatchWindow) {
+                windowStart.push_back(c);
+                windowMax = std::max(windowMax, acc);
+                acc = 0;
+            }
+            acc += items;
+        }
+        windowMax = std::max(windowMax, acc);
+        windowStart.push_back(chunkTotal);
+    }
+    x2_scene* s0 = req[0].scene;
+    cudaStream_t st = ctx->stream;
+    uint32_t paths = s0->reservePaths ? s0->reservePaths : (1u << 20);
+    if (uint64_t(paths) > windowMax) paths = uint32_t(windowMax);
+    if (int rc = ensureWave(s0, paths, records)) return rc;
+    if (int rc = ensureItems(s0, windowMax)) return rc;
+    SceneView* dViews = nullptr;
+    BatchFilm* dFilms = nullptr;
+    x2_chunk* dChunks = nullptr;
+    uint32_t* dChunkReq = nullptr;
+    unsigned long long* dChunkItems = nullptr;
+    Counters* dCounters = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    Counters hc{};
+    int rc = X2_OK;
+    const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
+    const int gridWork = ctx->smCount * int(s0->blocksPerSm);
+    const WaveKernels wk = waveKernelsBatch();
+    std::vector<unsigned long long> items;
+    uint32_t iterations = 0;
+    if (cudaMalloc(&dViews, sizeof(SceneView) * n) != cudaSuccess || cudaMalloc(&dFilms, sizeof(BatchFilm) * n) != cudaSuccess ||
+        cudaMalloc(&dChunks, sizeof(x2_chunk) * chunkTotal) != cudaSuccess || cudaMalloc(&dChunkReq, sizeof(uint32_t) * chunkTotal) != cudaSuccess ||
+        cudaMalloc(&dChunkItems, sizeof(unsigned long long) * (chunkTotal + 1)) != cudaSuccess ||
+        cudaMalloc(&dCounters, sizeof(Counters)) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+        setError("device allocation failed for a batch of %u requests", n);
+        rc = X2_ENOMEM;
+    }
+    if (!rc) {
+        cudaMemcpyAsync(dViews, views.data(), sizeof(SceneView) * n, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(dFilms, films.data(), sizeof(BatchFilm) * n, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(dChunks, chunks.data(), sizeof(x2_chunk) * chunkTotal, cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(dChunkReq, chunkReq.data(), sizeof(uint32_t) * chunkTotal, cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(dCounters, 0, sizeof(Counters), st);
+        cudaEventRecord(e0, st);
+    }
+    for (size_t wi = 0; !rc && wi + 1 < windowStart.size(); ++wi) {
+        const uint32_t c0 = windowStart[wi], c1 = windowStart[wi + 1];
+        items.assign(c1 - c0 + 1, 0ull);
+        for (uint32_t c = c0; c < c1; ++c) items[c - c0 + 1] = items[c - c0] + 64ull * chunks[c].count;
+        const uint64_t windowItems = items.back();
+        // The host table is read by the copy before the next window rewrites it.
+        cudaMemcpyAsync(dChunkItems, items.data(), sizeof(unsigned long long) * items.size(), cudaMemcpyHostToDevice, st);
+        cudaMemsetAsync(s0->wave.state, 0, sizeof(uint32_t) * paths, st);
+        cudaMemsetAsync(s0->wave.ncount, 0, sizeof(uint32_t) * paths, st);
+        cudaMemsetAsync(s0->claimed, 0, sizeof(unsigned long long), st);
+        cudaMemsetAsync(s0->waveCounters, 0, sizeof(uint32_t) * kWaveCounters, st);
+        cudaMemsetAsync(s0->outStatus, X2_SKIP, windowItems, st);
+        WaveArgs a{};
+        a.scene = views[0];
+        a.w = s0->wave;
+        a.paths = paths;
+        a.recordsPerPath = records;
+        a.chunks = dChunks + c0;
+        a.itemCount = windowItems;
+        a.samplesPerChunk = 0;
+        a.claimed = s0->claimed;
+        a.extendQ = s0->extendQ;
+        a.extendCount = s0->waveCounters;
+        a.lastExtend = s0->waveCounters + 1;
+        a.shadowQ = s0->shadowQ;
+        a.shadowCount = s0->waveCounters + 2;
+        a.extendNext = s0->waveCounters + 3;
+        a.shadowNext = s0->waveCounters + 4;
+        a.refill = s0->refill;
+        a.triLimit = s0->triLimit;
+        a.out = s0->out;
+        a.outStatus = s0->outStatus;
+        a.counters = dCounters;
+        a.scenes = dViews;
+        a.chunkRequest = dChunkReq + c0;
+        a.chunkItems = dChunkItems;
+        a.chunkCount = c1 - c0;
+        const uint64_t maxIter = windowItems * (uint64_t(maxDepth) + 2) / paths + uint64_t(maxDepth) + 64;
+        constexpr int kIter = 8;
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            setError("stream capture failed");
+            rc = X2_ECUDA;
+            break;
+        }
+        for (int it = 0; it < kIter; ++it) {
+            wfResetQueues<<<1, 32, 0, st>>>(a);
+            wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
+            wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
+            wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
+            wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
+        }
+        wfResetQueues<<<1, 32, 0, st>>>(a);
+        if (cudaStreamEndCapture(st, &graph) != cudaSuccess || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+            if (graph) cudaGraphDestroy(graph);
+            setError("batch graph capture failed");
+            rc = X2_ECUDA;
+            break;
+        }
+        for (uint64_t it = 0;;) {
+            if (cudaGraphLaunch(exec, st) != cudaSuccess) {
+                setError("graph launch failed");
+                rc = X2_ECUDA;
+                break;
+            }
+            it += kIter;
+            iterations += kIter;
+            cudaMemcpyAsync(s0->hostLast, s0->waveCounters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+            if ((rc = x2_synchronize(ctx, 600000)) != X2_OK) break;
+            if (s0->hostLast[0] == 0) break;
+            if (it > maxIter) {
+                setError("batch window did not drain after %llu iterations", (unsigned long long)it);
+                rc = X2_EDEVICE;
+                break;
+            }
+        }
+        cudaGraphExecDestroy(exec);
+        cudaGraphDestroy(graph);
+        if (rc) break;
+        wfFilmReduceBatch<<<int((64ull * (c1 - c0) + 255) / 256), 256, 0, st>>>(a, dFilms);
+        if (cudaGetLastError() != cudaSuccess) {
+            setError("batch film reduction failed to launch");
+            rc = X2_ECUDA;
+        }
+    }
+    if (!rc) {
+        cudaEventRecord(e1, st);
+        cudaMemcpyAsync(&hc, dCounters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+        rc = x2_synchronize(ctx, 600000);
+    }
+    float ms = 0.0f;
+    if (!rc) cudaEventElapsedTime(&ms, e0, e1);
+    if (out) {
+        out->launch = 0;
+        out->samples = hc.samples;
+        out->errors = hc.errors;
+        out->milliseconds = ms;
+        out->pad = 0;
+    }
+    if (!rc) {
+        for (uint32_t r = 0; r < n; ++r) req[r].scene->waveIterations = iterations;
+        accumulate(s0->total, hc);
+    }
+    cudaFree(dViews);
+    cudaFree(dFilms);
+    cudaFree(dChunks);
+    cudaFree(dChunkReq);
+    cudaFree(dChunkItems);
+    cudaFree(dCounters);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (!rc && hc.errors) {
+        setError("%llu samples of the batch ended in error", (unsigned long long)hc.errors);
+        return X2_EDEVICE;
+    }
+    return rc;
 }
 
 int x2_wavefront_timing(x2_scene* s, int on, float* ms) {

@@ -153,6 +153,10 @@ extern "C" int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chu
     a.out = reinterpret_cast<float4*>(base + kOut);
     a.outStatus = base + kOutStatus;
     a.counters = reinterpret_cast<Counters*>(base + kCounters);
+    a.scenes = nullptr;
+    a.chunkRequest = nullptr;
+    a.chunkItems = nullptr;
+    a.chunkCount = count;
     // What must start at zero; the rest is written before it is read.
     cudaMemsetAsync(a.w.state, 0, 4ull * kPaths, st);
     cudaMemsetAsync(a.w.ncount, 0, 4ull * kPaths, st);
@@ -171,7 +175,7 @@ extern "C" int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chu
             return X2_EDEVICE;
         }
         wfResetQueues<<<1, 32, 0, st>>>(a);
-        wfLogic<<<gridLogic, kWaveBlock, 0, st>>>(a);
+        wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
         wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
         wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
         wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);

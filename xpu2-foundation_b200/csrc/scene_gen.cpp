@@ -12,6 +12,7 @@
 // down by k for tests. Random numbers: xoshiro256** seeded by splitmix64.
 #include "../../include/x2.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -373,6 +374,25 @@ Holder* makeField(uint64_t seed, int tilesPerSide, int spheres, int icoLevel, ui
     return h;
 }
 
+// Batched requests (one frame a request, each its own scene and frame seed): request r draws a triangle count
+// log-uniform in [0.1M, 2M] (half heightfield tiles of 16x16 quads, half level-4 icospheres), a square resolution among
+// 128, 256, 512 and 1024, log-uniform 4..256 spp and a uniform 4..32 depth; its frame seed is 1 + r. `shrink` > 1
+// divides the triangle count by shrink^2 and the resolution and spp by shrink (the parity tests' small copies).
+Holder* makeRequest(uint32_t r, uint64_t seed, uint32_t shrink, x2_config* cfg) {
+    Rng g(seed ^ (0x51ed270b27a4f1c3ull * (uint64_t(r) + 1)));
+    const double tris = std::exp(std::log(1e5) + g.uniform() * (std::log(2e6) - std::log(1e5))) / (double(shrink) * shrink);
+    const uint32_t res = 128u << uint32_t(g.next() % 4);
+    const double sppReal = std::exp(std::log(4.0) + g.uniform() * (std::log(256.0) - std::log(4.0)));
+    const uint32_t depth = 4u + uint32_t(g.next() % 29u);
+    const int tiles = std::max(1, int(std::lround(std::sqrt(tris / 2.0 / 512.0))));
+    const int spheres = std::max(1, int(std::lround(tris / 2.0 / 5120.0)));
+    const uint32_t side = std::max(8u, res / shrink);
+    const uint32_t spp = std::max(1u, uint32_t(std::lround(sppReal / double(shrink))));
+    Holder* h = makeField(seed + r, tiles, spheres, 4, side, side, spp, depth, cfg);
+    cfg->seed = 1u + r;
+    return h;
+}
+
 }  // namespace
 
 extern "C" void x2_config_defaults(x2_config* c) {
@@ -403,6 +423,10 @@ extern "C" int x2_scene_generate(uint32_t config_id, uint64_t seed, x2_scene_des
             h = makeField(seed, 64, 2000, 4, 1920, 1080, 64, 12, config);
         } else if (config_id == 11) {
             h = makeField(seed, 32, 2000, 2, 1920, 1080, 64, 12, config);
+        } else if (config_id >= 200 && config_id < 248) {
+            h = makeRequest(config_id - 200, seed, 1, config);
+        } else if (config_id >= 300 && config_id < 348) {
+            h = makeRequest(config_id - 300, seed, 8, config);
         } else if (config_id > 100 && config_id <= 164) {
             const int k = int(config_id - 100);
             const int tiles = 64 / k > 0 ? 64 / k : 1, spheres = 2000 / (k * k) > 0 ? 2000 / (k * k) : 1;

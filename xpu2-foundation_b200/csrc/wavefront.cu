@@ -99,22 +99,52 @@ __device__ __forceinline__ void loadPending(const WaveState& w, uint32_t p, Pend
     pv.branch = (U64(b.y) << 32) | b.x;
 }
 
-__device__ __forceinline__ void storePending(const WaveState& w, uint32_t p, const Pending& c, uint32_t pixel, uint32_t index) {
+// meta.w: mirror depth (bits 0..7), lobe type (8..15), the path's request in a batch (16..31).
+__device__ __forceinline__ void storePending(const WaveState& w, uint32_t p, const Pending& c, uint32_t pixel, uint32_t index,
+                                             uint32_t request = 0) {
     w.ray0[p] = make_float4(c.origin.x, c.origin.y, c.origin.z, c.nearT);
     w.ray1[p] = make_float4(c.dir.x, c.dir.y, c.dir.z, c.farT);
     w.T[p] = make_float4(c.T.x, c.T.y, c.T.z, c.heldFar);
     w.held[p] = make_float4(c.held.x, c.held.y, c.held.z, __uint_as_float(c.heldLight));
-    w.meta[p] = make_uint4(pixel, index, packDepths(c), (c.mirror & 0xffu) | ((c.lobeType & 0xffu) << 8));
+    w.meta[p] = make_uint4(pixel, index, packDepths(c), (c.mirror & 0xffu) | ((c.lobeType & 0xffu) << 8) | (request << 16));
     w.branch[p] = make_uint2(uint32_t(c.branch), uint32_t(c.branch >> 32));
 }
 
 }  // namespace
 
+// The request a path slot's sample belongs to (batches; 0 otherwise) and that request's scene.
+__device__ __forceinline__ uint32_t requestOf(const WaveState& w, uint32_t p) { return w.meta[p].w >> 16; }
+template <bool kBatch>
+__device__ __forceinline__ const SceneView& sceneOf(const WaveArgs& a, uint32_t request) {
+    return kBatch ? a.scenes[request] : a.scene;
+}
+
+// A work item's chunk. One launch: chunks of 64 x samplesPerChunk items. A batch: chunks of 64 x count items each
+// (each request its own samples a pixel), found by binary search of the chunks' first items.
+template <bool kBatch>
+__device__ __forceinline__ uint32_t chunkOfItem(const WaveArgs& a, unsigned long long item, unsigned long long& first, uint32_t& perPixel) {
+    if (!kBatch) {
+        const unsigned long long perChunk = 64ull * a.samplesPerChunk;
+        const uint32_t c = uint32_t(item / perChunk);
+        first = c * perChunk;
+        perPixel = a.samplesPerChunk;
+        return c;
+    }
+    uint32_t lo = 0, hi = a.chunkCount;  // chunkItems[lo] <= item < chunkItems[hi]
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (a.chunkItems[mid] <= item) lo = mid;
+        else hi = mid;
+    }
+    first = a.chunkItems[lo];
+    perPixel = uint32_t((a.chunkItems[lo + 1] - first) / 64ull);
+    return lo;
+}
+
 // ---- logic ----
-__global__ void __launch_bounds__(kWaveBlock) wfLogic(WaveArgs a) {
+template <bool kBatch>
+__device__ __forceinline__ void logicBody(const WaveArgs& a) {
     const WaveState& w = a.w;
-    const uint32_t width = a.scene.config.width, height = a.scene.config.height;
-    const unsigned long long perChunk = 64ull * a.samplesPerChunk;
     unsigned long long samples = 0, errors = 0;
     for (uint32_t base = blockIdx.x * blockDim.x; base < a.paths; base += gridDim.x * blockDim.x) {
         const uint32_t p = base + threadIdx.x;
@@ -157,24 +187,28 @@ __global__ void __launch_bounds__(kWaveBlock) wfLogic(WaveArgs a) {
         if (wants) {
             const unsigned long long item = first + __popc(want & ((1u << (threadIdx.x & 31u)) - 1u));
             if (item < a.itemCount) {
-                const unsigned long long chunkIndex = item / perChunk;
-                const uint32_t offset = uint32_t(item - chunkIndex * perChunk);
-                const uint32_t position = offset / a.samplesPerChunk, s = offset % a.samplesPerChunk;
+                unsigned long long chunkFirst;
+                uint32_t perPixel;
+                const uint32_t chunkIndex = chunkOfItem<kBatch>(a, item, chunkFirst, perPixel);
+                const uint32_t offset = uint32_t(item - chunkFirst);
+                const uint32_t position = offset / perPixel, s = offset % perPixel;
                 const x2_chunk chunk = a.chunks[chunkIndex];
-                const uint32_t pixel = s < chunk.count ? tilePixelW(chunk.tile, position, width, height) : ~0u;
+                const uint32_t request = kBatch ? a.chunkRequest[chunkIndex] : 0u;
+                const SceneView& sv = sceneOf<kBatch>(a, request);
+                const uint32_t pixel = s < chunk.count ? tilePixelW(chunk.tile, position, sv.config.width, sv.config.height) : ~0u;
                 if (pixel == ~0u) {
                     a.outStatus[item] = uint8_t(X2_SKIP);  // not a sample of this launch
                 } else {
                     const uint32_t index = chunk.first + s;
                     CameraRay camera;
-                    if (!cameraRay(a.scene, pixel, index, camera)) {
+                    if (!cameraRay(sv, pixel, index, camera)) {
                         a.out[item] = make_float4(0, 0, 0, 0);
                         a.outStatus[item] = uint8_t(X2_ERROR);
                         ++errors;
                     } else {
                         Pending p0;
                         cameraPending(camera, p0);
-                        storePending(w, p, p0, pixel, index);
+                        storePending(w, p, p0, pixel, index, request);
                         w.rad[p] = make_float4(0, 0, 0, 0);
                         w.item[p] = uint32_t(item);
                         w.state[p] = kTrace;
@@ -191,14 +225,18 @@ __global__ void __launch_bounds__(kWaveBlock) wfLogic(WaveArgs a) {
     warpAddCounters(a.counters, 0, 0, 0, 0, samples, errors);
 }
 
+__global__ void __launch_bounds__(kWaveBlock) wfLogic(WaveArgs a) { logicBody<false>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfLogicBatch(WaveArgs a) { logicBody<true>(a); }
+
 // ---- extend: closest hits ----
 // Persistent traversal over a queue: each lane walks its ray a node a step; a warp fetches the next rays of the queue
 // (one atomic a warp) for its idle lanes once `refill` of them are idle, so lanes whose rays end early are not left
 // waiting for the warp's longest ray. kAny: shadow records (visibility out), else extend rays (closest hit out).
-template <bool kAny, bool kStats>
+template <bool kAny, bool kStats, bool kBatch>
 __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, const uint32_t* __restrict__ queue, uint32_t* next) {
     const WaveState& w = a.w;
-    const Bvh8 bvh = a.scene.bvh;
+    Bvh8 bvh = a.scene.bvh;  // a batch: the lane's ray's scene, set at each fetch
+    uint32_t* overflow = a.scene.overflow;
     const unsigned full = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u;
     Walk walk;
@@ -218,6 +256,11 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
                 const uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
                 if (i < n) {
                     k = queue[i];
+                    if (kBatch) {
+                        const SceneView& sv = a.scenes[requestOf(w, kAny ? k / a.recordsPerPath : k)];
+                        bvh = sv.bvh;
+                        overflow = sv.overflow;
+                    }
                     const float4 r0 = kAny ? w.sray0[k] : w.ray0[k], r1 = kAny ? w.sray1[k] : w.ray1[k];
                     r = makeRay(bvh, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
                     walkStart<kAny>(walk, r, r0.w, r1.w);
@@ -227,7 +270,7 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
             }
         }
         if (!__any_sync(full, live)) break;
-        if (live && walkStep<kAny>(bvh, r, walk, a.scene.overflow, a.triLimit)) {
+        if (live && walkStep<kAny>(bvh, r, walk, overflow, a.triLimit)) {
             if (kAny) w.svis[k] = walk.best ? 0 : 1;
             else w.hit[k] = make_uint2(walk.best == ~0u ? ~0u : walk.bestLeaf, __float_as_uint(walk.tmax));
             live = false;
@@ -241,25 +284,11 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
     }
 }
 
+template <bool kBatch>
 __device__ __forceinline__ void extendBody(const WaveArgs& a) {
-    const WaveState& w = a.w;
     const uint32_t n = *a.extendCount;
-    if (a.refill) {
-        if (a.scene.stats) persistentTrace<false, true>(a, n, a.extendQ, a.extendNext);
-        else persistentTrace<false, false>(a, n, a.extendQ, a.extendNext);
-        if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters->trace, (unsigned long long)n);
-        return;
-    }
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t p = a.extendQ[i];
-        const float4 r0 = w.ray0[p], r1 = w.ray1[p];
-        const RayQ r = makeRay(a.scene.bvh, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
-        float t;
-        uint32_t leaf;
-        const uint32_t tri = a.scene.stats ? traceClosest<true>(a.scene.bvh, r, r0.w, r1.w, t, &leaf, a.scene.overflow, a.scene.stats)
-                                           : traceClosest<false>(a.scene.bvh, r, r0.w, r1.w, t, &leaf, a.scene.overflow, nullptr);
-        w.hit[p] = make_uint2(tri == ~0u ? ~0u : leaf, __float_as_uint(t));
-    }
+    if (!kBatch && a.scene.stats) persistentTrace<false, true, false>(a, n, a.extendQ, a.extendNext);
+    else persistentTrace<false, false, kBatch>(a, n, a.extendQ, a.extendNext);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters->trace, (unsigned long long)n);
 }
 
@@ -286,9 +315,9 @@ struct WaveSink {
     }
 };
 
+template <bool kBatch>
 __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
     const WaveState& w = a.w;
-    const SceneView& s = a.scene;
     const uint32_t n = *a.extendCount;
     unsigned long long nee = 0, bsdf = 0, held = 0;
     // Every lane of a warp runs the same rounds: the shadow queue's reservation is a warp-wide scan.
@@ -301,7 +330,8 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
             Pending pv;
             loadPending(w, p, pv);
             const uint4 m = w.meta[p];
-            const uint32_t pixel = m.x, index = m.y;
+            const uint32_t pixel = m.x, index = m.y, request = m.w >> 16;
+            const SceneView& s = sceneOf<kBatch>(a, request);
             const Identity root{pixel, U64(index), U64(s.config.seed), 0};
             const uint2 hr = w.hit[p];
             Hit hit;
@@ -337,7 +367,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
                 } else {
                     records = sink.n;
                     if (sink.pushed) {
-                        storePending(w, p, sink.child, pixel, index);
+                        storePending(w, p, sink.child, pixel, index, request);
                         next = kTrace;
                     }
                 }
@@ -358,47 +388,48 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
 }
 
 // ---- shadow: any hits ----
+template <bool kBatch>
 __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
-    const WaveState& w = a.w;
     const uint32_t n = *a.shadowCount;
-    if (a.refill) {
-        if (a.scene.stats) persistentTrace<true, true>(a, n, a.shadowQ, a.shadowNext);
-        else persistentTrace<true, false>(a, n, a.shadowQ, a.shadowNext);
-        return;
-    }
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint32_t k = a.shadowQ[i];
-        const float4 r0 = w.sray0[k], r1 = w.sray1[k];
-        const RayQ r = makeRay(a.scene.bvh, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
-        const bool hit = a.scene.stats ? traceAny<true>(a.scene.bvh, r, r0.w, r1.w, a.scene.overflow, a.scene.stats + 1)
-                                       : traceAny<false>(a.scene.bvh, r, r0.w, r1.w, a.scene.overflow, nullptr);
-        w.svis[k] = hit ? 0 : 1;
-    }
+    if (!kBatch && a.scene.stats) persistentTrace<true, true, false>(a, n, a.shadowQ, a.shadowNext);
+    else persistentTrace<true, false, kBatch>(a, n, a.shadowQ, a.shadowNext);
 }
 
 // The kernels, each in a few occupancy variants (blocks of kWaveBlock threads a SM that the register allocation must
-// allow), chosen at launch (x2_wavefront_tune).
-__global__ void __launch_bounds__(kWaveBlock) wfExtend(WaveArgs a) { extendBody(a); }
-__global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) { shadeBody(a); }
-__global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) { shadowBody(a); }
+// allow), chosen at launch (x2_wavefront_tune); batches in the compiler's allocation.
+__global__ void __launch_bounds__(kWaveBlock) wfExtend(WaveArgs a) { extendBody<false>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) { shadeBody<false>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) { shadowBody<false>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfExtendBatch(WaveArgs a) { extendBody<true>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShadowBatch(WaveArgs a) { shadowBody<true>(a); }
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfExtendOcc(WaveArgs a) {
-    extendBody(a);
+    extendBody<false>(a);
 }
-template <int kMinBlocks>
+template <int kMinBlocks, bool kBatch>
 __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadeOcc(WaveArgs a) {
-    shadeBody(a);
+    shadeBody<kBatch>(a);
 }
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadowOcc(WaveArgs a) {
-    shadowBody(a);
+    shadowBody<false>(a);
 }
 
 WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks) {
     WaveKernels k;
+    k.logic = wfLogic;
     k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : wfExtend;
     k.shadow = traceBlocks >= 10 ? wfShadowOcc<10> : traceBlocks >= 9 ? wfShadowOcc<9> : wfShadow;
-    k.shade = shadeBlocks >= 4 ? wfShadeOcc<4> : shadeBlocks >= 3 ? wfShadeOcc<3> : wfShade;
+    k.shade = shadeBlocks >= 4 ? wfShadeOcc<4, false> : shadeBlocks >= 3 ? wfShadeOcc<3, false> : wfShade;
+    return k;
+}
+
+WaveKernels waveKernelsBatch() {
+    WaveKernels k;
+    k.logic = wfLogicBatch;
+    k.extend = wfExtendBatch;
+    k.shadow = wfShadowBatch;
+    k.shade = wfShadeOcc<4, true>;
     return k;
 }
 
@@ -448,6 +479,44 @@ __global__ void wfFilmReduce(WaveArgs a, uint32_t chunkCount, double* sums, doub
         for (int k = 0; k < 4; ++k)
             if (o[k] != 0.0) atomicAdd(odd + 4ull * pixel + k, o[k]);
     atomicAdd(counts + pixel, n);
+}
+
+// A batch's films: each chunk's samples (64 x its count items from chunkItems[c]) into its request's film.
+__global__ void wfFilmReduceBatch(WaveArgs a, const BatchFilm* __restrict__ films) {
+    const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 64ull * a.chunkCount) return;
+    const uint32_t chunkIndex = uint32_t(i / 64), position = uint32_t(i % 64);
+    const x2_chunk chunk = a.chunks[chunkIndex];
+    const uint32_t request = a.chunkRequest[chunkIndex];
+    const SceneView& sv = a.scenes[request];
+    const uint32_t pixel = tilePixelW(chunk.tile, position, sv.config.width, sv.config.height);
+    if (pixel == ~0u) return;
+    const BatchFilm f = films[request];
+    const unsigned long long begin = a.chunkItems[chunkIndex], perPixel = (a.chunkItems[chunkIndex + 1] - begin) / 64ull;
+    const unsigned long long first = begin + position * perPixel;
+    double v[4] = {0, 0, 0, 0}, o[4] = {0, 0, 0, 0};
+    uint32_t n = 0;
+    for (uint32_t s = 0; s < chunk.count; ++s) {
+        if (a.outStatus[first + s] != X2_DONE) continue;
+        const float4 r = a.out[first + s];
+        v[0] += double(r.x);
+        v[1] += double(r.y);
+        v[2] += double(r.z);
+        v[3] += double(r.w);
+        if (f.odd && ((chunk.first + s) & 1u)) {
+            o[0] += double(r.x);
+            o[1] += double(r.y);
+            o[2] += double(r.z);
+            o[3] += double(r.w);
+        }
+        ++n;
+    }
+    if (!n) return;
+    for (int k = 0; k < 4; ++k) atomicAdd(f.sums + 4ull * pixel + k, v[k]);
+    if (f.odd)
+        for (int k = 0; k < 4; ++k)
+            if (o[k] != 0.0) atomicAdd(f.odd + 4ull * pixel + k, o[k]);
+    atomicAdd(f.counts + pixel, n);
 }
 
 }  // namespace x2

@@ -43,26 +43,42 @@ struct WaveArgs {
     uint32_t* shadowCount;
     uint32_t* extendNext;  // the extend and shadow kernels' fetch counters over their queues
     uint32_t* shadowNext;
-    uint32_t refill;       // a warp fetches new rays once this many of its lanes are idle (0: one ray a thread)
+    uint32_t refill;       // a warp fetches new rays once this many of its lanes are idle (1..32)
     uint32_t triLimit;     // triangle tests a lane makes a traversal step
     float4* out;          // per item: rgb, alpha
     uint8_t* outStatus;   // per item: SampleStatus (Skip for items that are not samples)
     Counters* counters;
+    // Batches (many renders in one launch): each request's scene, each chunk's request and first item (chunkCount + 1
+    // entries, the last the item count), the chunk count. Unused by single launches.
+    const SceneView* scenes;
+    const uint32_t* chunkRequest;
+    const unsigned long long* chunkItems;
+    uint32_t chunkCount;
+};
+
+// A batch request's film (device).
+struct BatchFilm {
+    double* sums;
+    double* odd;  // null: not kept
+    uint32_t* counts;
 };
 
 // Fills wavefront.cu's copy of the Sobol direction table (every translation unit with sampling kernels has one).
 cudaError_t uploadSobolWavefront(const uint32_t directions[17][32]);
 
-__global__ void wfLogic(WaveArgs a);
-// The extend, shade and shadow kernels for an occupancy: at least `traceBlocks` / `shadeBlocks` blocks a SM (10, 9
-// or 0 for the traversals; 4, 3 or 0 for shade; 0 leaves the register allocation to the compiler).
+// The logic, extend, shade and shadow kernels for an occupancy: at least `traceBlocks` / `shadeBlocks` blocks a SM
+// (10, 9 or 0 for the traversals; 4, 3 or 0 for shade; 0 leaves the register allocation to the compiler); and the
+// batch forms, which take each path's scene from WaveArgs::scenes.
 struct WaveKernels {
+    void (*logic)(WaveArgs);
     void (*extend)(WaveArgs);
     void (*shade)(WaveArgs);
     void (*shadow)(WaveArgs);
 };
 WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks);
+WaveKernels waveKernelsBatch();
 __global__ void wfResetQueues(WaveArgs a);
 __global__ void wfFilmReduce(WaveArgs a, uint32_t chunkCount, double* sums, double* odd, uint32_t* counts);
+__global__ void wfFilmReduceBatch(WaveArgs a, const BatchFilm* films);
 
 }  // namespace x2

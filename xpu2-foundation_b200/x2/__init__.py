@@ -87,9 +87,13 @@ class Counters(C.Structure):
         return {k: int(getattr(self, k)) for k, _ in self._fields_ if k != "pad"}
 
 
+class Request(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("first", C.c_uint32), ("count", C.c_uint32)]
+
+
 class WavefrontShape(C.Structure):
-    FIELDS = ("paths", "refill", "blocks_per_sm", "trace_blocks", "shade_blocks", "tri_limit")
-    _fields_ = [(f, C.c_uint32) for f in FIELDS] + [("reserved", C.c_uint32 * 2)]
+    FIELDS = ("paths", "refill", "blocks_per_sm", "trace_blocks", "shade_blocks", "tri_limit", "batch_window")
+    _fields_ = [(f, C.c_uint32) for f in FIELDS] + [("reserved", C.c_uint32 * 1)]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k in self.FIELDS}
@@ -136,6 +140,7 @@ def library():
         "x2_wavefront_timing": ([vp, i32, vp], i32), "x2_wavefront_queues": ([vp, vp, u32], i32),
         "x2_wavefront_tune": ([vp, C.POINTER(WavefrontShape)], i32), "x2_wavefront_shape_defaults": ([C.POINTER(WavefrontShape)], None),
         "x2_launch_wavefront_static": ([vp, vp, u32, u32, vp, vp, C.POINTER(u64)], i32),
+        "x2_render_batch": ([vp, C.POINTER(Request), u32, C.POINTER(Completion)], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
@@ -199,6 +204,18 @@ class Context:
     def synchronize(self, timeout_ms=600000):
         _check(library().x2_synchronize(self._h, timeout_ms))
 
+    def render_batch(self, requests):
+        """Many frames in one wavefront launch (x2_render_batch): requests are (Scene, first, count); each scene's
+        film then holds its frame. Returns the batch's Completion (samples, errors, device milliseconds)."""
+        arr = (Request * len(requests))()
+        for i, (scene, first, count) in enumerate(requests):
+            arr[i].scene = scene.handle.value
+            arr[i].first = first
+            arr[i].count = count
+        c = Completion()
+        _check(library().x2_render_batch(self._h, arr, len(requests), C.byref(c)))
+        return c
+
     def sample_words(self, ids, dims, policy):
         """sample::samplingWord for structured `ids` (IDENTITY_DTYPE) and uint32 `dims` (host arrays)."""
         ids = np.ascontiguousarray(ids, dtype=IDENTITY_DTYPE)
@@ -219,7 +236,9 @@ class SyntheticScene:
         self._desc = C.POINTER(SceneDesc)()
         self.config = Config()
         self.config_id = config_id
-        self.seed = (config_id % 100) + 1 if seed is None else seed
+        if seed is None:  # a config's generator seed is its index + 1; batched requests (200+, 300+) are config 2's
+            seed = 3 if 200 <= config_id < 400 else (config_id % 100) + 1
+        self.seed = seed
         _check(library().x2_scene_generate(config_id, self.seed, C.byref(self._desc), C.byref(self.config)))
 
     @property
