@@ -202,6 +202,11 @@ typedef struct x2_wavefront_shape {
 } x2_wavefront_shape;
 void x2_wavefront_shape_defaults(x2_wavefront_shape* shape);
 int x2_wavefront_tune(x2_scene* scene, const x2_wavefront_shape* shape);
+/* The autotuner: times wavefront launches of `tiles` evenly spaced tiles (0: all) at `spp` samples, one knob at a time
+ * (paths, refill, tri_limit, shade_blocks, trace_blocks, blocks_per_sm, best of two launches a candidate), sets the
+ * fastest shape and returns it (best, best_ms may be null). Renders into the scene's film, which it leaves reset (as
+ * x2_frame_begin(scene, spp)). Waits. */
+int x2_wavefront_autotune(x2_scene* scene, uint32_t tiles, uint32_t spp, x2_wavefront_shape* best, float* best_ms);
 /* Batched renders (no reference counterpart; the reference renders one plan a lane): a request is one scene's frame,
  * samples [first, first + count) of every pixel, at the scene's own config (resolution, depth, lights, frame seed). */
 typedef struct x2_request {

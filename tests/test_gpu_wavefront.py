@@ -95,3 +95,23 @@ def test_wavefront_rejects_many_bsdf_samples(ctx):
     with pytest.raises(x2.X2Error) as e:
         scene.render_frame_wavefront(0, 1)
     assert e.value.code == x2.EINVAL
+
+
+def test_autotuned_shape_renders_the_same_film(ctx):
+    s = x2.SyntheticScene(108)
+    cfg = s.config
+    cfg.spp = 4
+    scene = x2.Scene(ctx, s.desc, cfg)
+    scene.frame_begin(4)
+    scene.render_frame_wavefront(0, 4)
+    scene.wait()
+    want, wc = scene.film()
+    shape, ms = scene.wavefront_autotune(tiles=64, spp=4)
+    assert ms > 0 and 1 <= shape["refill"] <= 32 and 1 <= shape["tri_limit"] <= 32
+    scene.frame_begin(4)
+    scene.render_frame_wavefront(0, 4)
+    scene.wait()
+    scene.audit()
+    got, gc = scene.film()
+    assert np.array_equal(gc, wc)
+    assert np.array_equal(got, want)

@@ -1084,6 +1084,73 @@ int x2_items_download(x2_scene* s, float* rgba, uint8_t* status, uint64_t n) {
     return x2_wait(s, 600000, nullptr);
 }
 
+// The launch-shape autotuner: coordinate descent over the shape's knobs (paths in flight, refill, triangle tests a step,
+// traversal and shade occupancy variants), each candidate timed as a wavefront launch of `tiles` evenly spaced tiles
+// at `spp` samples (best of two launches), keeping a knob's best value before the next knob. The results of a launch
+// do not depend on its shape, so any choice renders the same film. Leaves the best shape set and the film reset.
+int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefront_shape* best, float* bestMs) {
+    if (!s || !s->configured || spp == 0) {
+        setError("autotune: scene not configured or zero spp");
+        return X2_EINVAL;
+    }
+    const uint32_t all = ((s->config.width + 7) / 8) * ((s->config.height + 7) / 8);
+    if (tiles == 0 || tiles > all) tiles = all;
+    std::vector<x2_chunk> chunks(tiles);
+    for (uint32_t i = 0; i < tiles; ++i) chunks[i] = x2_chunk{uint32_t(uint64_t(i) * all / tiles), 0, spp, 0};
+    x2_wavefront_shape cur;
+    x2_wavefront_shape_defaults(&cur);
+    cur.paths = s->reservePaths;
+    cur.batch_window = s->batchWindow;
+    auto timeShape = [&](const x2_wavefront_shape& sh, float& ms) -> int {
+        if (int rc = x2_wavefront_tune(s, &sh)) return rc;
+        ms = 3.4e38f;
+        for (int k = 0; k < 2; ++k) {
+            if (int rc = x2_frame_begin(s, spp)) return rc;
+            if (int rc = x2_launch_wavefront(s, chunks.data(), tiles)) return rc;
+            x2_completion c{};
+            if (int rc = x2_wait(s, 600000, &c)) return rc;
+            ms = std::min(ms, c.milliseconds);
+        }
+        return X2_OK;
+    };
+    float curMs = 0.0f;
+    if (int rc = timeShape(cur, curMs)) return rc;
+    const uint64_t items = uint64_t(tiles) * 64ull * spp;
+    std::vector<uint32_t> pathOptions;
+    for (uint32_t p = 1u << 18; p <= (1u << 21); p <<= 1)
+        if (p <= items) pathOptions.push_back(p);
+    struct Knob {
+        uint32_t x2_wavefront_shape::*field;
+        std::vector<uint32_t> values;
+    };
+    const Knob knobs[] = {{&x2_wavefront_shape::paths, pathOptions},
+                          {&x2_wavefront_shape::refill, {4, 8, 16}},
+                          {&x2_wavefront_shape::tri_limit, {1, 2, 4}},
+                          {&x2_wavefront_shape::shade_blocks, {0, 3, 4}},
+                          {&x2_wavefront_shape::trace_blocks, {0, 9}},
+                          {&x2_wavefront_shape::blocks_per_sm, {8, 16, 32}}};
+    for (const Knob& k : knobs) {
+        x2_wavefront_shape keep = cur;
+        for (uint32_t v : k.values) {
+            if (cur.*k.field == v) continue;
+            x2_wavefront_shape trial = cur;
+            trial.*k.field = v;
+            float ms = 0.0f;
+            if (int rc = timeShape(trial, ms)) return rc;
+            if (ms < curMs) {
+                curMs = ms;
+                keep = trial;
+            }
+        }
+        cur = keep;
+    }
+    if (int rc = x2_wavefront_tune(s, &cur)) return rc;
+    if (int rc = x2_frame_begin(s, spp)) return rc;
+    if (best) *best = cur;
+    if (bestMs) *bestMs = curMs;
+    return X2_OK;
+}
+
 // Many renders in one wavefront launch: the requests' chunks (every tile of each frame, its sample range) are one work
 // list; path slots regenerate across requests, each path shading and tracing in its own request's scene. The work list
 // runs in windows of at most kBatchWindow items (the per-item outputs' size); each window's samples are summed into

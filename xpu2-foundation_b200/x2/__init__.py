@@ -141,6 +141,7 @@ def library():
         "x2_wavefront_tune": ([vp, C.POINTER(WavefrontShape)], i32), "x2_wavefront_shape_defaults": ([C.POINTER(WavefrontShape)], None),
         "x2_launch_wavefront_static": ([vp, vp, u32, u32, vp, vp, C.POINTER(u64)], i32),
         "x2_render_batch": ([vp, C.POINTER(Request), u32, C.POINTER(Completion)], i32),
+        "x2_wavefront_autotune": ([vp, u32, u32, C.POINTER(WavefrontShape), C.POINTER(C.c_float)], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
@@ -380,6 +381,14 @@ class Scene:
             setattr(s, k, int(v))
         _check(library().x2_wavefront_tune(self._h, C.byref(s)))
         return s.as_dict()
+
+    def wavefront_autotune(self, tiles=0, spp=None):
+        """Time the wavefront launch shapes on `tiles` evenly spaced tiles (0: all) at `spp` samples (default: the
+        config's), set the fastest and return (shape dict, its milliseconds). Leaves the film reset."""
+        best = WavefrontShape()
+        ms = C.c_float()
+        _check(library().x2_wavefront_autotune(self._h, tiles, spp or self.config.spp, C.byref(best), C.byref(ms)))
+        return best.as_dict(), ms.value
 
     def wavefront_queues(self):
         """The last timed launch's per-iteration queue sizes as an (iterations, 2) array: rays extended, shadow rays."""
