@@ -66,8 +66,10 @@ typedef struct x2_material {
 } x2_material;
 
 /* Lights admitted: lights::Light (light_core.h:59-117) of type Env (constant, whole sphere or hemisphere, no
- * image) and Rect (no image, no spread, no clear radius). Linear parts are rows, as the reference stores them. */
-enum { X2_LIGHT_ENV = 0, X2_LIGHT_RECT = 1 };
+ * image), Rect (no image, no spread, no clear radius) and Distant (no image: a cone of half-angle acos(cos_theta_max)
+ * about -direction, sampled uniformly; inv_area = 1 / (2 pi versine_theta_max)). Linear parts are rows, as the
+ * reference stores them. */
+enum { X2_LIGHT_ENV = 0, X2_LIGHT_RECT = 1, X2_LIGHT_DISTANT = 4 };
 enum { X2_SIDE_REGULAR = 0, X2_SIDE_REVERSE = 1, X2_SIDE_TWO = 2 };
 typedef struct x2_light {
     uint32_t type, sidedness, visible_in_camera, hemispherical;
@@ -78,7 +80,34 @@ typedef struct x2_light {
     float render2local_rot[3][3];     /* rotation only (rows) */
     float scale, inv_area, plane_offset, half_width, half_height;
     uint32_t visibility_mask;         /* rdl2 VisibilityType bits of the lobes that see it (0xfc: all) */
+    float cos_theta_max, versine_theta_max;  /* Distant: the cone's half-angle cosine, 1 - that */
 } x2_light;
+
+/* Participating media: volume::Shader (volume_core.h:64-111) of kind VDB (a VdbVolume) whose density (and, when it
+ * glows, emission) are dense grids, bound to an axis-aligned box (its closed mesh: two triangles a face, outward
+ * normals; rays cross it at entry and exit as the reference's volume crossings do, async_cpu.h:1089-1149).
+ * Extinction = gain x density (interpolation: 0 point, 1 box/trilinear, 2 quadratic; shadows read the nearest voxel),
+ * albedo = color_mult, emission = incandescence x the emission grid's nearest voxel, Henyey-Greenstein g. */
+typedef struct x2_volume {
+    float bound_lo[3], bound_hi[3];
+    uint32_t density_grid, emission_grid;  /* grid indices (emission: ~0u none) */
+    uint32_t interpolation;
+    float feature_size;                    /* the march's step unit: the cube root of a voxel's volume */
+    float world_to_grid[12];               /* rows of an affine map (x, y, z, translation), render -> grid space */
+    float gain[3], color_mult[3], incandescence[3];
+    float g;
+    uint32_t light_set;                    /* lights that light it: bit i light i (~0u all) */
+    float surface_opacity_threshold;
+} x2_volume;
+
+/* A dense grid of float (channels 1) or float3 (channels 3) voxels: dims from index lo, x fastest; zero outside.
+ * world_to_index: OpenVDB's linear world-to-index map, a row-vector 4x4 in doubles (volume_grid.h:33-47). */
+typedef struct x2_grid {
+    uint32_t channels;
+    int32_t lo[3], dims[3];
+    double world_to_index[16];
+    const float* values;
+} x2_grid;
 
 /* surface::Camera's perspective subset (surface_core.h:93-115): row-vector matrices, clip planes. */
 typedef struct x2_camera {
@@ -98,6 +127,9 @@ typedef struct x2_scene_desc {
     const x2_material* materials;
     const x2_light* lights;
     x2_camera camera;
+    uint32_t volume_count, grid_count;  /* volume_count <= 32 */
+    const x2_volume* volumes;
+    const x2_grid* grids;
 } x2_scene_desc;
 
 /* mixed::Config (gpu_jobs.h:10-44), the fields this engine reads, field for field with the same defaults
@@ -114,6 +146,10 @@ typedef struct x2_config {
     uint32_t visible_lights;
     float presence_threshold, presence_quality;
     uint32_t shadow_reuse;
+    /* Volumes (gpu_jobs.h:18-28): how many (the scene's), MoonRay's volume scene variables. */
+    uint32_t volume_count, max_volume_depth, volume_illumination_samples, volume_overlap_mode;
+    float volume_transmittance_threshold, volume_attenuation_factor, volume_contribution_factor, volume_phase_attenuation_factor;
+    float inv_volume_quality, inv_volume_shadow_quality;
     uint32_t reserved[8];
 } x2_config;
 
@@ -213,7 +249,7 @@ typedef struct x2_request {
     x2_scene* scene;
     uint32_t first, count;  /* count 1..2^21 */
 } x2_request;
-/* Renders n requests (1..65535; distinct scenes of ctx, each configured with bsdf_samples = 1) in one wavefront
+/* Renders n requests (1..256; distinct scenes of ctx, each configured with bsdf_samples = 1) in one wavefront
  * launch: path slots shared by all requests and regenerated across them, each path in its own scene; the first
  * request's scene holds the path state and its launch shape (x2_wavefront_tune) applies. Each scene's film is reset
  * first (as x2_frame_begin(scene, count)) and then holds exactly the film x2_launch_wavefront gives for all its

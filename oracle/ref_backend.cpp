@@ -94,7 +94,19 @@ struct Scene {
     xi::mixed::Config config{};
     Bvh bvh;
     V3 vertex(U32 i) const { return vertices[i]; }
+    // Volumes: their shaders, their bounds as closed meshes (twelve triangles a box, outward), their dense grids.
+    std::vector<xi::volume::Shader> volumes;
+    std::vector<V3> volumeTris;  // 3 vertices a triangle, 12 triangles a volume
+    std::vector<std::vector<float>> gridValues;
+    std::vector<nanovdb::FloatGrid> floatGrids;
+    std::vector<nanovdb::Vec3fGrid> vecGrids;
+    std::vector<xi::volume::Grid> grids;
 };
+
+// A box's 12 triangles by corner (corner i: hi on x for bit 0, y for bit 1, z for bit 2), each counter-clockwise seen
+// from outside, so cross(b - a, c - a) points out. The engine's device code uses the same table.
+const int kBoxTriangles[12][3] = {{0, 4, 6}, {0, 6, 2}, {1, 3, 7}, {1, 7, 5}, {0, 1, 5}, {0, 5, 4},
+                                  {2, 6, 7}, {2, 7, 3}, {0, 2, 3}, {0, 3, 1}, {4, 5, 7}, {4, 7, 6}};
 
 void buildBvh(Scene& s) {
     const U32 n = U32(s.tris.size() / 3);
@@ -294,9 +306,45 @@ struct OracleBackend {
     int treeRoot(U32) const { return -1; }
     void shadowFor(U32, U32) {}
     bool castsShadow(U32, bool) const { return true; }
-    const xi::volume::Shader* volumes() const { return nullptr; }
-    xi::volume::Grids volumeGrids() const { return xi::volume::Grids{}; }
-    U32 volumeCrossings(V3, V3, float, xi::volume::Crossing*, U32, U32) const { return 0; }
+    const xi::volume::Shader* volumes() const { return s.volumes.empty() ? nullptr : s.volumes.data(); }
+    xi::volume::Grids volumeGrids() const {
+        xi::volume::Grids g;
+        g.grids = s.grids.empty() ? nullptr : s.grids.data();
+        g.count = U32(s.grids.size());
+        g.maps = nullptr;
+        g.time = time;
+        return g;
+    }
+    // The ray's crossings of the volumes' bounds from tnear on, as the reference's CPU backend collects them
+    // (async_cpu.h:1089-1149): the nearest crossing from t, entering where the ray runs against the outward normal,
+    // then on from just past it; a repeat of the same crossing at the same t dropped. Every ray type sees volumes.
+    U32 volumeCrossings(V3 o, V3 d, float tnear, xi::volume::Crossing* x, U32 max, U32) const {
+        if (s.volumes.empty()) return 0;
+        const TriTest sh = shear(d);
+        const U32 tris = U32(s.volumeTris.size() / 3);
+        U32 n = 0;
+        float t = tnear;
+        for (U32 k = 0; k < 4 * max && n < max; ++k) {
+            float best = INFINITY;
+            U32 hitTri = ~0u;
+            for (U32 i = 0; i < tris; ++i) {
+                float th;
+                if (triHit(sh, o, s.volumeTris[3 * i], s.volumeTris[3 * i + 1], s.volumeTris[3 * i + 2], t, INFINITY, th) && th < best) {
+                    best = th;
+                    hitTri = i;
+                }
+            }
+            if (hitTri == ~0u) break;
+            const V3 a = s.volumeTris[3 * hitTri], b = s.volumeTris[3 * hitTri + 1], c = s.volumeTris[3 * hitTri + 2];
+            const V3 e1{b.x - a.x, b.y - a.y, b.z - a.z}, e2{c.x - a.x, c.y - a.y, c.z - a.z};
+            const V3 ng{e1.y * e2.z - e1.z * e2.y, e1.z * e2.x - e1.x * e2.z, e1.x * e2.y - e1.y * e2.x};
+            const U32 v = hitTri / 12;
+            const U32 flags = d.x * ng.x + d.y * ng.y + d.z * ng.z < 0.0f ? xi::volume::Entry : xi::volume::Exit;
+            if (!(n > 0 && x[n - 1].t == best && x[n - 1].volume == v && x[n - 1].flags == flags)) x[n++] = xi::volume::Crossing{best, v, flags};
+            t = best + std::fmax(1e-6f, best * 1e-6f);
+        }
+        return n;
+    }
     xi::volume::Regions emissiveRegions() const { return xi::volume::Regions{nullptr, 0, nullptr}; }
     const xi::aov::Tables& aovs() const {
         static const xi::aov::Tables none{};
@@ -344,7 +392,9 @@ struct OracleBackend {
 xi::lights::Light toLight(const x2_light& x, U32 index) {
     xi::lights::Light l;
     std::memset(&l, 0, sizeof(l));
-    l.type = x.type == X2_LIGHT_ENV ? xi::lights::Env : xi::lights::Rect;
+    l.type = x.type == X2_LIGHT_ENV ? xi::lights::Env : x.type == X2_LIGHT_DISTANT ? xi::lights::Distant : xi::lights::Rect;
+    l.cosThetaMax = x.cos_theta_max;
+    l.versineThetaMax = x.versine_theta_max;
     l.sidedness = x.sidedness;
     l.index = index;
     l.radiance = V3{x.radiance[0], x.radiance[1], x.radiance[2]};
@@ -412,6 +462,16 @@ xi::mixed::Config toConfig(const x2_config& x, const x2_camera& cam) {
     c.presenceThreshold = x.presence_threshold;
     c.presenceQuality = x.presence_quality;
     c.shadowReuse = x.shadow_reuse;
+    c.volumeCount = x.volume_count;
+    c.maxVolumeDepth = x.max_volume_depth;
+    c.volumeIlluminationSamples = x.volume_illumination_samples;
+    c.volumeOverlapMode = x.volume_overlap_mode;
+    c.volumeTransmittanceThreshold = x.volume_transmittance_threshold;
+    c.volumeAttenuationFactor = x.volume_attenuation_factor;
+    c.volumeContributionFactor = x.volume_contribution_factor;
+    c.volumePhaseAttenuationFactor = x.volume_phase_attenuation_factor;
+    c.invVolumeQuality = x.inv_volume_quality;
+    c.invVolumeShadowQuality = x.inv_volume_shadow_quality;
     return c;
 }
 
@@ -463,6 +523,60 @@ void* x2ref_open(const x2_scene_desc* d, const x2_config* cfg) {
     }
     for (U32 i = 0; i < d->light_count; ++i) s.lights.push_back(toLight(d->lights[i], i));
     s.config = toConfig(*cfg, d->camera);
+    // Grids (dense, as the NanoVDB stand-in holds them) and the VdbVolume shaders over them.
+    s.gridValues.resize(d->grid_count);
+    s.floatGrids.resize(d->grid_count);
+    s.vecGrids.resize(d->grid_count);
+    s.grids.resize(d->grid_count);
+    for (U32 g = 0; g < d->grid_count; ++g) {
+        const x2_grid& xg = d->grids[g];
+        const size_t voxels = size_t(xg.dims[0]) * xg.dims[1] * xg.dims[2];
+        s.gridValues[g].assign(xg.values, xg.values + voxels * xg.channels);
+        xi::volume::Grid& vg = s.grids[g];
+        for (int i = 0; i < 16; ++i) vg.worldToIndex[i] = xg.world_to_index[i];
+        vg.vec3 = xg.channels == 3 ? 1u : 0u;
+        if (xg.channels == 3) {
+            nanovdb::Vec3fGrid& ng = s.vecGrids[g];
+            ng.values = reinterpret_cast<const nanovdb::Vec3f*>(s.gridValues[g].data());
+            ng.background = nanovdb::Vec3f{{0, 0, 0}};
+            for (int a = 0; a < 3; ++a) ng.lo[a] = xg.lo[a], ng.dims[a] = xg.dims[a];
+            vg.data = &ng;
+        } else {
+            nanovdb::FloatGrid& ng = s.floatGrids[g];
+            ng.values = s.gridValues[g].data();
+            ng.background = 0.0f;
+            for (int a = 0; a < 3; ++a) ng.lo[a] = xg.lo[a], ng.dims[a] = xg.dims[a];
+            vg.data = &ng;
+        }
+    }
+    for (U32 v = 0; v < d->volume_count; ++v) {
+        const x2_volume& xv = d->volumes[v];
+        xi::volume::Shader sh;
+        std::memset(&sh, 0, sizeof(sh));
+        sh.kind = xi::volume::KindVdb;
+        sh.g = xv.g;
+        sh.flags = 0;
+        sh.lightSet = xv.light_set;
+        sh.densityGrid = xv.density_grid;
+        sh.emissionGrid = xv.emission_grid;
+        sh.interpolation = xv.interpolation;
+        sh.featureSize = xv.feature_size;
+        for (int i = 0; i < 12; ++i) sh.worldToGrid[i] = xv.world_to_grid[i];
+        sh.gain = V3{xv.gain[0], xv.gain[1], xv.gain[2]};
+        sh.colorMult = V3{xv.color_mult[0], xv.color_mult[1], xv.color_mult[2]};
+        sh.incandescence = V3{xv.incandescence[0], xv.incandescence[1], xv.incandescence[2]};
+        sh.visibility = ~0u;
+        sh.lpeLabel = -1;
+        sh.bakedGrid = xi::volume::NoGrid;
+        sh.velocityGrid = xi::volume::NoGrid;
+        sh.surfaceOpacityThreshold = xv.surface_opacity_threshold;
+        s.volumes.push_back(sh);
+        V3 corner[8];
+        for (int i = 0; i < 8; ++i)
+            corner[i] = V3{(i & 1) ? xv.bound_hi[0] : xv.bound_lo[0], (i & 2) ? xv.bound_hi[1] : xv.bound_lo[1], (i & 4) ? xv.bound_hi[2] : xv.bound_lo[2]};
+        for (const auto& t : kBoxTriangles)
+            for (int k = 0; k < 3; ++k) s.volumeTris.push_back(corner[t[k]]);
+    }
     buildBvh(s);
     return h;
 }

@@ -128,7 +128,7 @@ def test_config1_triangle_count():
 
 
 @pytest.mark.skipif(not oracle_lib.have_reference(), reason="oracle/_ref not built")
-@pytest.mark.parametrize("cid", [0, 108])
+@pytest.mark.parametrize("cid", [0, 108, 33])
 def test_oracle_radiance_golden(cid):
     """The live reference build reproduces the committed golden radiance bit for bit (same build flags)."""
     g = np.load(os.path.join(GOLDEN, f"radiance_c{cid}.npz"))

@@ -120,6 +120,12 @@ struct x2_scene {
     x2_light* lights = nullptr;
     uint32_t* overflow = nullptr;
     uint32_t lightCount = 0, triangleCount = 0;
+    // volumes (device): records, bounds' triangles, grids and their values
+    VolumeRec* volumes = nullptr;
+    float* volumeTris = nullptr;
+    GridRec* grids = nullptr;
+    std::vector<float*> gridValues;
+    uint32_t volumeCount = 0, gridCount = 0;
     x2_camera camera{};
     x2_config config{};
     bool configured = false;
@@ -178,6 +184,10 @@ SceneView viewOf(const x2_scene* s) {
     v.config = s->config;
     v.overflow = s->overflow;
     v.stats = s->counting ? s->stats : nullptr;
+    v.volumes = s->volumes;
+    v.grids = s->grids;
+    v.volumeTris = s->volumeTris;
+    v.gridCount = s->gridCount;
     return v;
 }
 
@@ -438,10 +448,36 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
     }
     for (uint32_t i = 0; i < d->light_count; ++i) {
         const x2_light& l = d->lights[i];
-        if ((l.type != X2_LIGHT_ENV && l.type != X2_LIGHT_RECT) || l.sidedness > X2_SIDE_TWO) {
+        if ((l.type != X2_LIGHT_ENV && l.type != X2_LIGHT_RECT && l.type != X2_LIGHT_DISTANT) || l.sidedness > X2_SIDE_TWO) {
             setError("light %u: type %u / sidedness %u not admitted", i, l.type, l.sidedness);
             return X2_EINVAL;
         }
+    }
+    if (d->volume_count > kDeviceVolumes || (d->volume_count && !d->volumes) || (d->grid_count && !d->grids)) {
+        setError("at most %u volumes, with their records and grids", kDeviceVolumes);
+        return X2_EINVAL;
+    }
+    for (uint32_t g = 0; g < d->grid_count; ++g) {
+        const x2_grid& x = d->grids[g];
+        if ((x.channels != 1 && x.channels != 3) || x.dims[0] <= 0 || x.dims[1] <= 0 || x.dims[2] <= 0 || !x.values) {
+            setError("grid %u: 1 or 3 channels, positive dims, values", g);
+            return X2_EINVAL;
+        }
+    }
+    for (uint32_t v = 0; v < d->volume_count; ++v) {
+        const x2_volume& x = d->volumes[v];
+        if (x.density_grid >= d->grid_count || d->grids[x.density_grid].channels != 1 ||
+            (x.emission_grid != kNoGrid && (x.emission_grid >= d->grid_count || d->grids[x.emission_grid].channels != 3)) ||
+            x.interpolation > kInterpQuadratic || !(x.feature_size > 0.0f) || x.light_set != ~0u) {
+            setError("volume %u: density grid (1 channel), emission grid (3 channels or none), interpolation 0..2, feature size > 0, "
+                     "all lights (light sets not admitted)", v);
+            return X2_EINVAL;
+        }
+        for (int k = 0; k < 3; ++k)
+            if (!(x.bound_lo[k] < x.bound_hi[k])) {
+                setError("volume %u: empty bounds", v);
+                return X2_EINVAL;
+            }
     }
     if (d->mesh_first[0] != 0 || d->mesh_first[d->mesh_count] != d->triangle_count) {
         setError("mesh ranges do not cover the triangles");
@@ -521,6 +557,61 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
     if (d->light_count) cudaMemcpyAsync(s->lights, d->lights, sizeof(x2_light) * d->light_count, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(s->overflow, 0, sizeof(uint32_t), st);
     cudaMemsetAsync(s->stats, 0, 2 * sizeof(TraversalStats), st);
+    // Volumes: their records, their bounds' twelve triangles each (the oracle's table), their grids' values.
+    s->volumeCount = d->volume_count;
+    s->gridCount = d->grid_count;
+    if (d->volume_count) {
+        static const int kBox[12][3] = {{0, 4, 6}, {0, 6, 2}, {1, 3, 7}, {1, 7, 5}, {0, 1, 5}, {0, 5, 4},
+                                        {2, 6, 7}, {2, 7, 3}, {0, 2, 3}, {0, 3, 1}, {4, 5, 7}, {4, 7, 6}};
+        std::vector<VolumeRec> recs(d->volume_count);
+        std::vector<float> tris;
+        for (uint32_t v = 0; v < d->volume_count; ++v) {
+            const x2_volume& x = d->volumes[v];
+            VolumeRec& r = recs[v];
+            for (int i = 0; i < 12; ++i) r.worldToGrid[i] = x.world_to_grid[i];
+            r.gain = V3{x.gain[0], x.gain[1], x.gain[2]};
+            r.colorMult = V3{x.color_mult[0], x.color_mult[1], x.color_mult[2]};
+            r.incandescence = V3{x.incandescence[0], x.incandescence[1], x.incandescence[2]};
+            r.g = x.g;
+            r.featureSize = x.feature_size;
+            r.surfaceThreshold = x.surface_opacity_threshold;
+            r.densityGrid = x.density_grid;
+            r.emissionGrid = x.emission_grid;
+            r.interpolation = x.interpolation;
+            for (const auto& t : kBox)
+                for (int k = 0; k < 3; ++k)
+                    for (int a = 0; a < 3; ++a) tris.push_back((t[k] >> a) & 1 ? x.bound_hi[a] : x.bound_lo[a]);
+        }
+        std::vector<GridRec> grids(d->grid_count);
+        s->gridValues.assign(d->grid_count, nullptr);
+        bool ok = cudaMalloc(&s->volumes, sizeof(VolumeRec) * d->volume_count) == cudaSuccess &&
+                  cudaMalloc(&s->volumeTris, sizeof(float) * tris.size()) == cudaSuccess &&
+                  cudaMalloc(&s->grids, sizeof(GridRec) * (d->grid_count ? d->grid_count : 1)) == cudaSuccess;
+        for (uint32_t g = 0; ok && g < d->grid_count; ++g) {
+            const x2_grid& x = d->grids[g];
+            const size_t n = size_t(x.dims[0]) * x.dims[1] * x.dims[2] * x.channels;
+            ok = cudaMalloc(&s->gridValues[g], sizeof(float) * n) == cudaSuccess;
+            if (!ok) break;
+            cudaMemcpyAsync(s->gridValues[g], x.values, sizeof(float) * n, cudaMemcpyHostToDevice, st);
+            GridRec& r = grids[g];
+            for (int i = 0; i < 16; ++i) r.worldToIndex[i] = x.world_to_index[i];
+            r.values = s->gridValues[g];
+            for (int a = 0; a < 3; ++a) r.lo[a] = x.lo[a], r.dims[a] = x.dims[a];
+            r.channels = x.channels;
+        }
+        if (!ok) {
+            setError("device allocation failed for the volumes");
+            return fail(X2_ENOMEM);
+        }
+        cudaMemcpyAsync(s->volumes, recs.data(), sizeof(VolumeRec) * recs.size(), cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(s->volumeTris, tris.data(), sizeof(float) * tris.size(), cudaMemcpyHostToDevice, st);
+        if (d->grid_count) cudaMemcpyAsync(s->grids, grids.data(), sizeof(GridRec) * grids.size(), cudaMemcpyHostToDevice, st);
+        // The copies read host vectors that go out of scope here.
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            setError("volume upload failed");
+            return fail(X2_ECUDA);
+        }
+    }
     cudaEventRecord(b0, st);
     if (buildBvh(dVerts, dTris, d->triangle_count, st, &s->bvh) != 0) return fail(X2_ECUDA);
     cudaEventRecord(b1, st);
@@ -551,6 +642,10 @@ int x2_scene_free(x2_scene* s) {
     cudaFree(s->overflow);
     cudaFree(s->auditWord);
     cudaFree(s->stats);
+    cudaFree(s->volumes);
+    cudaFree(s->volumeTris);
+    cudaFree(s->grids);
+    for (float* g : s->gridValues) cudaFree(g);
     freeWave(s);
     cudaFree(s->out);
     cudaFree(s->outStatus);
@@ -585,6 +680,15 @@ int x2_config_set(x2_scene* s, const x2_config* c) {
     }
     if (c->bsdf_samples == 0 || c->bsdf_samples > 64 || c->light_samples == 0 || c->light_samples > 64) {
         setError("bsdf/light samples out of [1, 64]");
+        return X2_EINVAL;
+    }
+    if (c->volume_count != s->volumeCount) {
+        setError("config volume_count %u differs from the scene's %u volumes", c->volume_count, s->volumeCount);
+        return X2_EINVAL;
+    }
+    if (c->volume_count && (c->max_volume_depth > 1 || c->volume_overlap_mode > kOverlapRnd || c->max_depth > 120)) {
+        setError("volumes: max_volume_depth 0 or 1 (the multiple-scattering approximation is not built), overlap mode 0..2, "
+                 "max_depth <= 120");
         return X2_EINVAL;
     }
     s->config = *c;
@@ -1156,8 +1260,8 @@ int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefron
 // runs in windows of at most kBatchWindow items (the per-item outputs' size); each window's samples are summed into
 // their films in sample order, as a single launch's are, so each film equals the one x2_launch_wavefront gives.
 int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completion* out) {
-    if (!ctx || !req || n == 0 || n > 65535 || !req[0].scene) {
-        setError("a batch takes 1..65535 requests");
+    if (!ctx || !req || n == 0 || n > 256 || !req[0].scene) {
+        setError("a batch takes 1..256 requests");
         return X2_EINVAL;
     }
     const uint64_t kBatchWindow = req[0].scene->batchWindow ? req[0].scene->batchWindow : (1ull << 27);

@@ -18,6 +18,7 @@ struct Pending {
     V3 origin, dir, T;
     U64 branch;
     uint32_t depth, nonMirror, diffuse, glossy, mirror, lobeType;
+    uint32_t volumeDepth;  // the volume scattering it has been through, every bounce counting one
     float nearT, farT;
     uint32_t heldLight;
     float heldFar;
@@ -29,6 +30,12 @@ struct SampleOut {
     uint32_t status;
     uint32_t trace, nee, bsdf, held;
 };
+
+}  // namespace x2
+
+#include "volume.cuh"
+
+namespace x2 {
 
 // paths::roulette (async_integrator.h:141-149).
 __device__ __forceinline__ bool roulette(float lum, float threshold, float u, float& scale) {
@@ -47,7 +54,7 @@ __device__ __forceinline__ V3 visibleLights(const SceneView& s, const Identity& 
         for (uint32_t j = 0; j < c.light_count; ++j) {
             const x2_light& L = s.lights[j];
             LightHit lh;
-            const uint32_t vp = L.type == X2_LIGHT_ENV ? 2u : 0u;
+            const uint32_t vp = L.type == X2_LIGHT_ENV ? 2u : L.type == X2_LIGHT_DISTANT ? 1u : 0u;
             if (L.visible_in_camera && vp == pass && lightIntersect(L, origin, dir, maxDistance, lh)) ++hits;
         }
     if (!hits) return V3{0, 0, 0};
@@ -88,6 +95,7 @@ __device__ __forceinline__ void cameraPending(const CameraRay& camera, Pending& 
     p0.T = V3{1, 1, 1};
     p0.branch = 0;
     p0.depth = p0.nonMirror = p0.diffuse = p0.glossy = p0.mirror = p0.lobeType = 0;
+    p0.volumeDepth = 0;
     p0.nearT = camera.nearT;  // a camera ray is traced on the camera's clip range
     p0.farT = camera.farT;
     p0.heldLight = ~0u;
@@ -98,14 +106,22 @@ __device__ __forceinline__ void cameraPending(const CameraRay& camera, Pending& 
 // After a ray is traced, before its hit is shaded: the light its BSDF sample held is settled (bounce-ray reuse:
 // reached unless the ray met something short of the shadow ray's end; lightShadowKept is 0 without a clear radius),
 // then, on a camera ray, the lights the camera sees (async_integrator.h:2095-2106, :2172-2185).
-__device__ __forceinline__ void afterTrace(const SceneView& s, const Identity& root, const Pending& pv, const Hit& hit, V3 cameraPosition,
+// With volumes, the volumes the ray passes on its way (async_integrator.h:2107-2118): their light, the throughput
+// through them (pv's T and volume depth change) and, for a camera ray that hits nothing, their opacity as its alpha.
+__device__ __forceinline__ void afterTrace(const SceneView& s, const Identity& root, Pending& pv, const Hit& hit, V3 cameraPosition,
                                            V3& radiance, float& alpha) {
     if (pv.heldLight != ~0u) {
         const float kept = hit.geom != ~0u && hit.t < pv.heldFar ? 0.0f : 1.0f;
         if (kept > 0.0f) radiance = add(radiance, kept < 1.0f ? mul(pv.held, kept) : pv.held);
     }
-    // No volumes: a camera ray that hits nothing adds no alpha (1 - (1+1+1)/3), a hit adds one (below).
-    if (hit.geom == ~0u && pv.depth == 0) alpha += 1.0f * (1.0f - (1.0f + 1.0f + 1.0f) / 3.0f);
+    V3 volumeAlphaT{1, 1, 1};
+    if (s.config.volume_count) {
+        const V3 volumeLight = volumeRadiance(s, root, pv, pv.origin, pv.dir, pv.nearT, hit.geom == ~0u ? pv.farT : hit.t, volumeAlphaT);
+        radiance = add(radiance, volumeLight);
+    }
+    // A camera ray that hits nothing: the volumes' opacity (none without volumes: 1 - (1+1+1)/3); a hit adds one (its
+    // holdouts' minimum transmittance is zero with no holdouts; shadeVertex).
+    if (hit.geom == ~0u && pv.depth == 0) alpha += 1.0f * (1.0f - (volumeAlphaT.x + volumeAlphaT.y + volumeAlphaT.z) / 3.0f);
     if (pv.depth == 0 && s.config.visible_lights) {
         const bool missed = hit.geom == ~0u;
         const V3 Lv = mulv(pv.T, visibleLights(s, root, missed ? pv.origin : cameraPosition, pv.dir, missed ? 3.4028234663852886e+38f : hit.t));
@@ -220,6 +236,14 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
             q.dir = wi;
             q.near = fmaxf(0.0f, 0.0f);
             q.far = fmaxf((lh.distance - 0.0f) * kHitEpsilonEnd, 2.0f * q.near);
+            if (c.volume_count) {
+                // The volumes on the shadow ray's way (transmittance(), async_integrator.h:2722-2731); it matters only
+                // when nothing occludes the ray, and its stream is its own, so it is taken here.
+                Identity tid = lid;
+                tid.branch = childBranch(lightAddress, si, 0xfffb);
+                Stream vs(tid, pv.depth, 0);
+                t = mulv(t, volumeTransmittance(s, vs, q.origin, wi, q.near, q.far, 1.0f, int(pv.depth) + 1));
+            }
             q.contribution = t;
             sink.shadow(q, false);
         }
@@ -295,7 +319,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
             shadowNear = fmaxf(shadowNear, 0.0f);
             shadowFar = fmaxf((lightDistance - 0.0f) * kHitEpsilonEnd, 2.0f * shadowNear);
             held = bounces && thinning >= 1.0f && topNow + kPendingReserve < kMaxPending && lobeMask && (c.shadow_reuse & lobeMask) == lobeMask &&
-                   shadowNear == start;
+                   !c.volume_count && shadowNear == start;
             if (held) {
                 sink.held();
             } else {
@@ -305,6 +329,12 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
                 q.near = shadowNear;
                 q.far = shadowFar;
                 q.contribution = direct;
+                if (c.volume_count) {
+                    Identity tid = bid;
+                    tid.branch = childBranch(sampleBranch, 0xfffb, 0);
+                    Stream vs(tid, pv.depth, 0);
+                    q.contribution = mulv(direct, volumeTransmittance(s, vs, origin, wi, shadowNear, shadowFar, 1.0f, int(pv.depth) + 1));
+                }
                 sink.shadow(q, true);
             }
         }
@@ -339,6 +369,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
         child.farT = kFltMax;
         child.nearT = start;
         child.lobeType = lobe.type;
+        child.volumeDepth = pv.volumeDepth + 1;
         child.heldLight = held ? lightIndex : ~0u;
         child.heldFar = held ? shadowFar : 0.0f;
         child.held = held ? directBefore : V3{0, 0, 0};
@@ -384,7 +415,7 @@ static __device__ __noinline__ void integrate(const SceneView& s, uint32_t pixel
     float alpha = 0.0f;
     PlainSink sink{s, radiance, stack, top, out};
     while (top) {
-        const Pending pv = stack[--top];
+        Pending pv = stack[--top];
         V3 va, vb, vc;
         const Hit hit = trace(s, pv.origin, pv.dir, pv.nearT, pv.farT, va, vb, vc);
         ++out.trace;

@@ -103,6 +103,7 @@ struct Stream {
     Identity id;
     U32 dimension, group;
     Words w;
+    Stream() = default;
     __device__ Stream(const Identity& i, U32 bounce, U32 offset)
         : id(i), dimension(CameraDimensions + bounce * DimensionsPerBounce + offset), group(~0u) {}
     __device__ float next() {

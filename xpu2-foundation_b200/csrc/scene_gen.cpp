@@ -63,6 +63,9 @@ struct Holder {
     std::vector<uint32_t> triangles, meshFirst, meshMaterial;
     std::vector<x2_material> materials;
     std::vector<x2_light> lights;
+    std::vector<x2_volume> volumes;
+    std::vector<x2_grid> grids;
+    std::vector<std::vector<float>> gridValues;
 
     uint32_t vertex(V p) {
         vertices.push_back(p.x);
@@ -89,8 +92,8 @@ struct Holder {
         tri(i, j, k);
         tri(i, k, l);
     }
-    void finish() {
-        meshFirst.push_back(triangleCount());
+    void finish() {  // again after more lights or volumes: the descriptor refreshed, the meshes closed once
+        if (meshFirst.size() == meshMaterial.size()) meshFirst.push_back(triangleCount());
         std::memset(&desc, 0, sizeof(desc));
         desc.vertex_count = uint32_t(vertices.size() / 3);
         desc.triangle_count = triangleCount();
@@ -103,6 +106,11 @@ struct Holder {
         desc.mesh_material = meshMaterial.data();
         desc.materials = materials.data();
         desc.lights = lights.data();
+        for (size_t g = 0; g < grids.size(); ++g) grids[g].values = gridValues[g].data();
+        desc.volume_count = uint32_t(volumes.size());
+        desc.grid_count = uint32_t(grids.size());
+        desc.volumes = volumes.data();
+        desc.grids = grids.data();
     }
 };
 
@@ -374,6 +382,175 @@ Holder* makeField(uint64_t seed, int tilesPerSide, int spheres, int icoLevel, ui
     return h;
 }
 
+// fp16 rounding (round to nearest, ties to even) of a finite float in half's range: the density grid is stored at
+// half precision, as the scene gives it, and read back as the floats it rounds to.
+float roundHalf(float f) {
+    if (f == 0.0f) return f;
+    int e;
+    std::frexp(f, &e);                      // f = m 2^e, 0.5 <= |m| < 1
+    const int bits = e - 1 >= -14 ? 10 : 10 - (-14 - (e - 1));  // mantissa bits kept (subnormals keep fewer)
+    const float q = std::ldexp(1.0f, (e - 1) - bits);
+    return float(std::nearbyint(double(f) / double(q)) * double(q));
+}
+
+// Value noise in 3D with a smooth interpolant, summed over octaves.
+float hash3(int x, int y, int z, uint32_t seed) {
+    uint32_t h = uint32_t(x) * 0x8da6b343u ^ uint32_t(y) * 0x68e31da4u ^ uint32_t(z) * 0xd8163841u ^ seed * 0xcb1ab31fu;
+    h ^= h >> 13;
+    h *= 0x5bd1e995u;
+    h ^= h >> 15;
+    return float(h & 0xffffff) * (1.0f / 16777216.0f) * 2.0f - 1.0f;
+}
+float noise3(float x, float y, float z, uint32_t seed) {
+    const int ix = int(std::floor(x)), iy = int(std::floor(y)), iz = int(std::floor(z));
+    const float fx = x - float(ix), fy = y - float(iy), fz = z - float(iz);
+    const float sx = fx * fx * (3 - 2 * fx), sy = fy * fy * (3 - 2 * fy), sz = fz * fz * (3 - 2 * fz);
+    float v[2][2];
+    for (int j = 0; j < 2; ++j)
+        for (int k = 0; k < 2; ++k) {
+            const float a = hash3(ix, iy + j, iz + k, seed), b = hash3(ix + 1, iy + j, iz + k, seed);
+            v[j][k] = a + (b - a) * sx;
+        }
+    const float y0 = v[0][0] + (v[1][0] - v[0][0]) * sy, y1 = v[0][1] + (v[1][1] - v[0][1]) * sy;
+    return y0 + (y1 - y0) * sz;
+}
+float fbm3(float x, float y, float z, int octaves, uint32_t seed) {
+    float sum = 0, amp = 0.5f, freq = 1;
+    for (int o = 0; o < octaves; ++o) {
+        sum += amp * noise3(x * freq, y * freq, z * freq, seed + uint32_t(o));
+        amp *= 0.5f;
+        freq *= 2.0f;
+    }
+    return sum;
+}
+
+// A blackbody's colour at kelvin, normalised to unit maximum (Tanner Helland's fit to the CIE blackbody locus).
+V blackbody(float kelvin) {
+    const double t = kelvin / 100.0;
+    double r, g, b;
+    if (t <= 66.0) {
+        r = 255.0;
+        g = 99.4708025861 * std::log(t) - 161.1195681661;
+    } else {
+        r = 329.698727446 * std::pow(t - 60.0, -0.1332047592);
+        g = 288.1221695283 * std::pow(t - 60.0, -0.0755148492);
+    }
+    if (t >= 66.0) b = 255.0;
+    else if (t <= 19.0) b = 0.0;
+    else b = 138.5177312231 * std::log(t - 10.0) - 305.0447927307;
+    auto c = [](double v) { return float(std::min(255.0, std::max(0.0, v)) / 255.0); };
+    return {c(r), c(g), c(b)};
+}
+
+// A Distant light of radiance v from direction `toward` (the way its light travels), angular diameter 0.53 degrees.
+x2_light distantLight(V toward, float v) {
+    x2_light l{};
+    l.type = X2_LIGHT_DISTANT;
+    l.radiance[0] = l.radiance[1] = l.radiance[2] = v;
+    const V d = normalized(toward);
+    const V a = std::fabs(d.x) < 0.9f ? V{1, 0, 0} : V{0, 1, 0};
+    const V u = normalized(cross(a, d)), w = cross(d, u);
+    const V rowsOf[3] = {u, w, d};
+    for (int i = 0; i < 3; ++i) {
+        const float r[3] = {rowsOf[i].x, rowsOf[i].y, rowsOf[i].z};
+        for (int j = 0; j < 3; ++j) l.local2render[i][j] = l.render2local_rot[j][i] = l.render2local[j][i] = r[j];
+    }
+    l.direction[0] = d.x;
+    l.direction[1] = d.y;
+    l.direction[2] = d.z;
+    l.scale = 1.0f;
+    const double half = 0.5 * 0.53 * 3.14159265358979323846 / 180.0;
+    l.cos_theta_max = float(std::cos(half));
+    l.versine_theta_max = float(1.0 - std::cos(half));
+    l.inv_area = float(1.0 / (2.0 * 3.14159265358979323846 * (1.0 - std::cos(half))));
+    l.visibility_mask = 0xfcu;
+    return l;
+}
+
+// The participating medium (config 3): an n^3 grid over the cube [-0.9, 0.9]^3 inside the config-0 box, density from
+// seeded 5-octave 3D fBm, its lowest 40% empty, scaled to [0, 8] per unit length and stored at half precision; a
+// temperature channel on the hottest 10% of voxels (1000-3000 K, half precision) glowing with its blackbody colour; a
+// VdbVolume (trilinear density, HG g = 0.6, albedo 0.9); the box's rect light and a sun (Distant, radiance 5).
+Holder* makeVolumeBox(uint64_t seed, int n, uint32_t width, uint32_t height, uint32_t spp, uint32_t depth, x2_config* cfg) {
+    x2_config boxCfg;
+    Holder* h = makeBox(&boxCfg);
+    const float lo = -0.9f, extent = 1.8f, voxel = extent / float(n);
+    const size_t cells = size_t(n) * n * n;
+    std::vector<float> raw(cells), heat(cells);
+    for (int k = 0; k < n; ++k)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                const float x = (float(i) + 0.5f) / float(n) * 4.0f, y = (float(j) + 0.5f) / float(n) * 4.0f, z = (float(k) + 0.5f) / float(n) * 4.0f;
+                const size_t c = (size_t(k) * n + j) * n + i;
+                raw[c] = fbm3(x, y, z, 5, uint32_t(seed));
+                heat[c] = fbm3(x + 17.0f, y + 5.0f, z + 11.0f, 3, uint32_t(seed) + 101u);
+            }
+    std::vector<float> sorted = raw;
+    std::nth_element(sorted.begin(), sorted.begin() + long(cells * 2 / 5), sorted.end());
+    const float threshold = sorted[cells * 2 / 5];
+    float top = threshold;
+    for (float v : raw) top = std::max(top, v);
+    std::vector<float> hs = heat;
+    std::nth_element(hs.begin(), hs.begin() + long(cells * 9 / 10), hs.end());
+    const float hot = hs[cells * 9 / 10];
+    float hottest = hot;
+    for (float v : heat) hottest = std::max(hottest, v);
+    std::vector<float> density(cells), emission(3 * cells, 0.0f);
+    for (size_t c = 0; c < cells; ++c) {
+        density[c] = raw[c] > threshold ? roundHalf(8.0f * (raw[c] - threshold) / (top - threshold)) : 0.0f;
+        if (heat[c] > hot && density[c] > 0.0f) {
+            const float kelvin = roundHalf(1000.0f + 2000.0f * (heat[c] - hot) / std::max(hottest - hot, 1e-6f));
+            const V rgb = blackbody(kelvin);
+            const float power = 4.0f * (kelvin / 3000.0f) * (kelvin / 3000.0f) * (kelvin / 3000.0f) * (kelvin / 3000.0f);
+            emission[3 * c] = rgb.x * power;
+            emission[3 * c + 1] = rgb.y * power;
+            emission[3 * c + 2] = rgb.z * power;
+        }
+    }
+    auto grid = [&](uint32_t channels, std::vector<float>&& values) {
+        x2_grid g{};
+        g.channels = channels;
+        g.lo[0] = g.lo[1] = g.lo[2] = 0;
+        g.dims[0] = g.dims[1] = g.dims[2] = n;
+        for (int i = 0; i < 16; ++i) g.world_to_index[i] = 0.0;
+        for (int a = 0; a < 3; ++a) {
+            g.world_to_index[a * 4 + a] = 1.0 / double(voxel);
+            g.world_to_index[12 + a] = -double(lo) / double(voxel) - 0.5;
+        }
+        g.world_to_index[15] = 1.0;
+        h->grids.push_back(g);
+        h->gridValues.push_back(std::move(values));
+        return uint32_t(h->grids.size() - 1);
+    };
+    x2_volume v{};
+    for (int a = 0; a < 3; ++a) {
+        v.bound_lo[a] = lo;
+        v.bound_hi[a] = lo + extent;
+    }
+    v.density_grid = grid(1, std::move(density));
+    v.emission_grid = grid(3, std::move(emission));
+    v.interpolation = 1;
+    v.feature_size = voxel;
+    for (int i = 0; i < 12; ++i) v.world_to_grid[i] = 0.0f;
+    v.world_to_grid[0] = v.world_to_grid[5] = v.world_to_grid[10] = 1.0f;
+    for (int a = 0; a < 3; ++a) {
+        v.gain[a] = 1.0f;
+        v.color_mult[a] = 0.9f;
+        v.incandescence[a] = 1.0f;
+    }
+    v.g = 0.6f;
+    v.light_set = ~0u;
+    v.surface_opacity_threshold = 0.5f;
+    h->volumes.push_back(v);
+    h->lights.push_back(distantLight({0.25f, -0.45f, -1.0f}, 5.0f));
+    const x2_camera cam = pinhole({0, 0, 3.5f}, {0, 0, 0}, 40.0f, width, height);
+    fillConfig(cfg, width, height, spp, depth, uint32_t(h->lights.size()), uint32_t(h->lights.size()));
+    cfg->volume_count = 1;
+    h->finish();
+    h->desc.camera = cam;
+    return h;
+}
+
 // Batched requests (one frame a request, each its own scene and frame seed): request r draws a triangle count
 // log-uniform in [0.1M, 2M] (half heightfield tiles of 16x16 quads, half level-4 icospheres), a square resolution among
 // 128, 256, 512 and 1024, log-uniform 4..256 spp and a uniform 4..32 depth; its frame seed is 1 + r. `shrink` > 1
@@ -411,6 +588,15 @@ extern "C" void x2_config_defaults(x2_config* c) {
     c->presence_threshold = 0.999f;
     c->presence_quality = 0.75f;
     c->shadow_reuse = 0xfcu;
+    c->max_volume_depth = 1;
+    c->volume_illumination_samples = 4;
+    c->volume_overlap_mode = 0;
+    c->volume_transmittance_threshold = 0.005f;
+    c->volume_attenuation_factor = 0.65f;
+    c->volume_contribution_factor = 0.65f;
+    c->volume_phase_attenuation_factor = 0.5f;
+    c->inv_volume_quality = 2.0f;
+    c->inv_volume_shadow_quality = 1.0f;
 }
 
 extern "C" int x2_scene_generate(uint32_t config_id, uint64_t seed, x2_scene_desc** out, x2_config* config) {
@@ -423,6 +609,10 @@ extern "C" int x2_scene_generate(uint32_t config_id, uint64_t seed, x2_scene_des
             h = makeField(seed, 64, 2000, 4, 1920, 1080, 64, 12, config);
         } else if (config_id == 11) {
             h = makeField(seed, 32, 2000, 2, 1920, 1080, 64, 12, config);
+        } else if (config_id == 3) {
+            h = makeVolumeBox(seed, 256, 512, 512, 256, 64, config);
+        } else if (config_id == 33) {
+            h = makeVolumeBox(seed, 32, 64, 64, 4, 8, config);
         } else if (config_id >= 200 && config_id < 248) {
             h = makeRequest(config_id - 200, seed, 1, config);
         } else if (config_id >= 300 && config_id < 348) {

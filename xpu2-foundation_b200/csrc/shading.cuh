@@ -53,6 +53,7 @@ constexpr float kEpsilon = 1e-6f, kPi = 3.14159265358979323846f, kTwoPi = 6.2831
 constexpr float kOneOverPi = 0.318309886183790671538f;
 constexpr float kInfiniteDistance = 3.4028234663852886e+38f - 1e32f;
 constexpr float kEnvDistance = kInfiniteDistance * 0.9f;
+constexpr float kDistantDistance = kInfiniteDistance * 0.8f;
 constexpr float kHitEpsilonEnd = 1.0f - 1e-3f;
 constexpr float kFltMax = 3.402823466e+38f;
 
@@ -81,7 +82,25 @@ struct MaterialRec {
 struct Counters {
     unsigned long long trace, nee, bsdf, held, samples, errors, overflow, pad;
 };
+// A volume on the device (x2_volume; volume::Shader's VdbVolume fields, volume_core.h:64-111) and a dense grid.
+struct VolumeRec {
+    float worldToGrid[12];
+    V3 gain, colorMult, incandescence;
+    float g, featureSize, surfaceThreshold;
+    uint32_t densityGrid, emissionGrid, interpolation;
+};
+struct GridRec {
+    double worldToIndex[16];
+    const float* values;
+    int lo[3], dims[3];
+    uint32_t channels;
+};
+
 struct SceneView {
+    const VolumeRec* volumes;       // volume_count of them (config.volume_count), their bounds' triangles (12 a volume,
+    const GridRec* grids;           // 9 floats each) and the grids they read
+    const float* volumeTris;
+    uint32_t gridCount;
     Bvh8 bvh;
     const uint32_t* triMesh;        // scene triangle -> mesh
     const uint32_t* meshFirst;      // mesh -> first triangle
@@ -481,6 +500,19 @@ __device__ __forceinline__ bool lightSample(const x2_light& l, V3 p, const V3* n
         h.distance = kEnvDistance;
         return true;
     }
+    if (l.type == X2_LIGHT_DISTANT) {
+        // A cone about the light's direction, uniform in solid angle (light_core.h:502-522 without an image).
+        const float versine = fmaxf(r[0] * l.versine_theta_max, 0.0f);
+        const float cosTheta = 1.0f - versine;
+        float s, c;
+        sincosPoly(r[1] * kTwoPi, s, c);
+        const float sinTheta = sqrtf(fmaxf(0.0f, versine * (2.0f - versine)));
+        wi = rowsMul(l.local2render, mul(V3{sinTheta * c, sinTheta * s, cosTheta}, -1));
+        if (n && dot(*n, wi) < kEpsilon) return false;
+        h.N = mul(wi, -1);
+        h.distance = kDistantDistance;
+        return true;
+    }
     const float distance = planeDistance(l, p);
     if (l.sidedness != X2_SIDE_TWO && distance < kEpsilon) return false;
     const V3 local{(0.5f - r[0]) * (2 * l.half_width), (0.5f - r[1]) * (2 * l.half_height), 0.0f};
@@ -499,7 +531,7 @@ __device__ __forceinline__ float areaToSolidAngleScale(V3 wi, V3 lightNormal, fl
 // lights::eval (light_core.h:740-786).
 __device__ __forceinline__ V3 lightEval(const x2_light& l, V3 wi, const LightHit& h, float& pdf) {
     const V3 radiance{l.radiance[0] * 1.0f, l.radiance[1] * 1.0f, l.radiance[2] * 1.0f};
-    if (l.type == X2_LIGHT_ENV) {
+    if (l.type == X2_LIGHT_ENV || l.type == X2_LIGHT_DISTANT) {
         pdf = l.inv_area;
         return radiance;
     }
@@ -516,6 +548,12 @@ __device__ __forceinline__ bool lightIntersect(const x2_light& l, V3 p, V3 wi, f
         h.distance = kEnvDistance;
         return true;
     }
+    if (l.type == X2_LIGHT_DISTANT) {
+        if (dot(wi, ldir(l)) > -l.cos_theta_max || kDistantDistance > maxDistance) return false;
+        h.N = mul(wi, -1);
+        h.distance = kDistantDistance;
+        return true;
+    }
     const V3 localWi = rowsMul(l.render2local_rot, wi), localP = rowsMul(l.render2local, sub(p, lpos(l)));
     if ((localP.z < 0.0f) == (localWi.z < 0.0f)) return false;
     if (localP.z < 0.0f ? l.sidedness == X2_SIDE_REGULAR : l.sidedness == X2_SIDE_REVERSE) return false;
@@ -530,6 +568,10 @@ __device__ __forceinline__ bool lightIntersect(const x2_light& l, V3 p, V3 wi, f
 // lights::canIlluminate (light_core.h:1025-1069) with no subsurface radius.
 __device__ __forceinline__ bool canIlluminate(const x2_light& l, V3 p, const V3* n) {
     if (l.type == X2_LIGHT_ENV) return true;
+    if (l.type == X2_LIGHT_DISTANT) {
+        const float cullThreshold = -cosf(fminf(acosf(fminf(fmaxf(l.cos_theta_max, -1.0f), 1.0f)) + 0.5f * kPi, kPi));
+        return !(n && dot(*n, ldir(l)) > cullThreshold);
+    }
     const float threshold = kEpsilon - 0.0f;
     if (l.sidedness != X2_SIDE_TWO && planeDistance(l, p) < threshold) return false;
     if (!n) return true;

@@ -95,25 +95,27 @@ __device__ __forceinline__ void loadPending(const WaveState& w, uint32_t p, Pend
     pv.glossy = m.z >> 24;
     pv.mirror = m.w & 0xffu;
     pv.lobeType = (m.w >> 8) & 0xffu;
+    pv.volumeDepth = (m.w >> 16) & 0xffu;
     const uint2 b = w.branch[p];
     pv.branch = (U64(b.y) << 32) | b.x;
 }
 
-// meta.w: mirror depth (bits 0..7), lobe type (8..15), the path's request in a batch (16..31).
+// meta.w: mirror depth (bits 0..7), lobe type (8..15), volume depth (16..23), the path's request in a batch (24..31).
 __device__ __forceinline__ void storePending(const WaveState& w, uint32_t p, const Pending& c, uint32_t pixel, uint32_t index,
                                              uint32_t request = 0) {
     w.ray0[p] = make_float4(c.origin.x, c.origin.y, c.origin.z, c.nearT);
     w.ray1[p] = make_float4(c.dir.x, c.dir.y, c.dir.z, c.farT);
     w.T[p] = make_float4(c.T.x, c.T.y, c.T.z, c.heldFar);
     w.held[p] = make_float4(c.held.x, c.held.y, c.held.z, __uint_as_float(c.heldLight));
-    w.meta[p] = make_uint4(pixel, index, packDepths(c), (c.mirror & 0xffu) | ((c.lobeType & 0xffu) << 8) | (request << 16));
+    w.meta[p] = make_uint4(pixel, index, packDepths(c),
+                           (c.mirror & 0xffu) | ((c.lobeType & 0xffu) << 8) | ((c.volumeDepth & 0xffu) << 16) | (request << 24));
     w.branch[p] = make_uint2(uint32_t(c.branch), uint32_t(c.branch >> 32));
 }
 
 }  // namespace
 
 // The request a path slot's sample belongs to (batches; 0 otherwise) and that request's scene.
-__device__ __forceinline__ uint32_t requestOf(const WaveState& w, uint32_t p) { return w.meta[p].w >> 16; }
+__device__ __forceinline__ uint32_t requestOf(const WaveState& w, uint32_t p) { return w.meta[p].w >> 24; }
 template <bool kBatch>
 __device__ __forceinline__ const SceneView& sceneOf(const WaveArgs& a, uint32_t request) {
     return kBatch ? a.scenes[request] : a.scene;
@@ -330,7 +332,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
             Pending pv;
             loadPending(w, p, pv);
             const uint4 m = w.meta[p];
-            const uint32_t pixel = m.x, index = m.y, request = m.w >> 16;
+            const uint32_t pixel = m.x, index = m.y, request = m.w >> 24;
             const SceneView& s = sceneOf<kBatch>(a, request);
             const Identity root{pixel, U64(index), U64(s.config.seed), 0};
             const uint2 hr = w.hit[p];

@@ -47,7 +47,20 @@ class Light(C.Structure):
                 ("radiance", C.c_float * 3), ("position", C.c_float * 3), ("direction", C.c_float * 3),
                 ("local2render", (C.c_float * 3) * 3), ("render2local", (C.c_float * 3) * 3), ("render2local_rot", (C.c_float * 3) * 3),
                 ("scale", C.c_float), ("inv_area", C.c_float), ("plane_offset", C.c_float), ("half_width", C.c_float),
-                ("half_height", C.c_float), ("visibility_mask", C.c_uint32)]
+                ("half_height", C.c_float), ("visibility_mask", C.c_uint32), ("cos_theta_max", C.c_float),
+                ("versine_theta_max", C.c_float)]
+
+
+class Volume(C.Structure):
+    _fields_ = [("bound_lo", C.c_float * 3), ("bound_hi", C.c_float * 3), ("density_grid", C.c_uint32), ("emission_grid", C.c_uint32),
+                ("interpolation", C.c_uint32), ("feature_size", C.c_float), ("world_to_grid", C.c_float * 12), ("gain", C.c_float * 3),
+                ("color_mult", C.c_float * 3), ("incandescence", C.c_float * 3), ("g", C.c_float), ("light_set", C.c_uint32),
+                ("surface_opacity_threshold", C.c_float)]
+
+
+class Grid(C.Structure):
+    _fields_ = [("channels", C.c_uint32), ("lo", C.c_int32 * 3), ("dims", C.c_int32 * 3), ("world_to_index", C.c_double * 16),
+                ("values", C.POINTER(C.c_float))]
 
 
 class Camera(C.Structure):
@@ -59,7 +72,8 @@ class SceneDesc(C.Structure):
     _fields_ = [("vertex_count", C.c_uint32), ("triangle_count", C.c_uint32), ("mesh_count", C.c_uint32), ("material_count", C.c_uint32),
                 ("light_count", C.c_uint32), ("pad", C.c_uint32), ("vertices", C.POINTER(C.c_float)), ("triangles", C.POINTER(C.c_uint32)),
                 ("mesh_first", C.POINTER(C.c_uint32)), ("mesh_material", C.POINTER(C.c_uint32)), ("materials", C.POINTER(Material)),
-                ("lights", C.POINTER(Light)), ("camera", Camera)]
+                ("lights", C.POINTER(Light)), ("camera", Camera), ("volume_count", C.c_uint32), ("grid_count", C.c_uint32),
+                ("volumes", C.POINTER(Volume)), ("grids", C.POINTER(Grid))]
 
 
 _U = C.c_uint32
@@ -73,7 +87,10 @@ class Config(C.Structure):
                 ("clamp_depth", _U), ("rr_threshold", _F), ("clamp_value", _F), ("max_glossy_depth", _U), ("max_mirror_depth", _U),
                 ("max_hair_depth", _U), ("max_presence_depth", _U), ("shadow_terminator_fix", _U), ("roughness_clamping", _F),
                 ("transparency_threshold", _F), ("visible_lights", _U), ("presence_threshold", _F), ("presence_quality", _F),
-                ("shadow_reuse", _U), ("reserved", _U * 8)]
+                ("shadow_reuse", _U), ("volume_count", _U), ("max_volume_depth", _U), ("volume_illumination_samples", _U),
+                ("volume_overlap_mode", _U), ("volume_transmittance_threshold", _F), ("volume_attenuation_factor", _F),
+                ("volume_contribution_factor", _F), ("volume_phase_attenuation_factor", _F), ("inv_volume_quality", _F),
+                ("inv_volume_shadow_quality", _F), ("reserved", _U * 8)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
