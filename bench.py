@@ -359,6 +359,38 @@ def probe_batch(args):
     ctx.close()
 
 
+def probe_volume(args):
+    """Config 3 (the participating medium: a 256^3 grid in the closed box, a rect light and a sun; 512x512, 256 spp,
+    depth 64): `--probe-tiles` evenly spaced 8x8 tiles (all 4096 by default when the flag is left at its 592 default
+    is not wanted, pass 4096) at full spp in the wavefront form, then the plain megakernel on the same tiles; the
+    films compared and audited. Prints Msamples/s of each form."""
+    import x2
+
+    ctx = x2.Context(0)
+    s = x2.SyntheticScene(3)
+    cfg = s.config
+    scene = x2.Scene(ctx, s.desc, cfg)
+    tiles = ((cfg.width + 7) // 8) * ((cfg.height + 7) // 8)
+    sel = np.linspace(0, tiles - 1, min(tiles, args.probe_tiles)).astype(np.uint32)
+    chunks = np.zeros(len(sel), x2.CHUNK_DTYPE)
+    chunks["tile"], chunks["first"], chunks["count"] = sel, 0, cfg.spp
+    n = len(sel) * 64 * cfg.spp
+    out = {"probe": "volume", "tiles": len(sel), "samples": n, "grid": "256^3", "spp": cfg.spp}
+    films = {}
+    for form in ("wavefront", "plain"):
+        scene.frame_begin(cfg.spp)
+        (scene.launch_wavefront if form == "wavefront" else scene.launch)(chunks)
+        c = scene.wait()
+        films[form] = scene.film()
+        out[form] = {"ms": c.milliseconds, "msamples_per_s": n / c.milliseconds / 1e3, "errors": c.errors}
+    out["films_close"] = bool(np.allclose(films["wavefront"][0], films["plain"][0], rtol=1e-9, atol=1e-9) and
+                              np.array_equal(films["wavefront"][1], films["plain"][1]))
+    out["counters"] = scene.counters()
+    print(json.dumps(out))
+    scene.free()
+    ctx.close()
+
+
 def probe(args):
     """One bounded launch for profilers (ncu): `--probe-tiles` evenly spaced tiles of config 1 at 64 spp, in one form;
     the wavefront form without its graph (`--probe-timed`) so each kernel launch is visible on its own."""
@@ -366,6 +398,8 @@ def probe(args):
 
     if args.probe == "batch":
         return probe_batch(args)
+    if args.probe == "volume":
+        return probe_volume(args)
     ctx = x2.Context(0)
     s = x2.SyntheticScene(1)
     cfg = s.config
@@ -402,7 +436,7 @@ def main():
     ap.add_argument("--impl", default="x2", choices=["x2", "reference"])
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--skip-plain", action="store_true")
-    ap.add_argument("--probe", choices=["plain", "wavefront", "batch"], help="one bounded launch for a profiler, then exit")
+    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume"], help="one bounded launch for a profiler, then exit")
     ap.add_argument("--probe-tiles", type=int, default=592)
     ap.add_argument("--probe-timed", action="store_true", help="wavefront probe without its graph (per-kernel launches)")
     args = ap.parse_args()
