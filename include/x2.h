@@ -256,6 +256,17 @@ typedef struct x2_request {
  * tiles; x2_film_download / x2_audit read it. Waits. out (or null): samples and errors of the whole batch, its device
  * milliseconds; the ray counters go to the first scene's x2_counters. */
 int x2_render_batch(x2_ctx* ctx, const x2_request* requests, uint32_t n, x2_completion* out);
+/* ---- differentiation (no reference counterpart; config 4) ----
+ * The differentiable parameters, set in place: each material's diffuse colour (a Lambert lobe's albedo; 3 floats a
+ * material) and each light's radiance (3 floats a light); host arrays, null leaves a set as it is. Waits. */
+int x2_scene_set_params(x2_scene* scene, const float* albedo, const float* radiance);
+/* The adjoint of samples [first, first + count) of every pixel (the film's mean image): given dL/dimage (device, 3
+ * floats a pixel), adds dL/dalbedo (device, 3 doubles a material) and dL/dradiance (device, 3 doubles a light). Each
+ * sample's path is replayed from its identity (nothing of a primal pass is stored) and each contribution credited to
+ * the light it reached and the Lambert vertices it passed, the sampling decisions held fixed. Requires no volumes,
+ * max_depth < 128, bsdf_samples = 1. Waits. */
+int x2_adjoint(x2_scene* scene, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad,
+               double* d_radiance_grad);
 /* The last timed wavefront launch's queue sizes: for each iteration, rays extended then shadow rays (2 a
  * iteration, at most max values). */
 int x2_wavefront_queues(x2_scene* scene, uint32_t* sizes, uint32_t max);

@@ -14,6 +14,7 @@
 
 #include "../../include/x2.h"
 #include "engine.h"
+#include "adjoint.h"
 #include "render.h"
 #include "wavefront.h"
 
@@ -119,7 +120,7 @@ struct x2_scene {
     MaterialRec* materials = nullptr;
     x2_light* lights = nullptr;
     uint32_t* overflow = nullptr;
-    uint32_t lightCount = 0, triangleCount = 0;
+    uint32_t lightCount = 0, triangleCount = 0, materialCount = 0;
     // volumes (device): records, bounds' triangles, grids and their values
     VolumeRec* volumes = nullptr;
     float* volumeTris = nullptr;
@@ -310,6 +311,11 @@ int ensureItems(x2_scene* s, uint64_t items) {
 }  // namespace
 
 namespace x2 {
+__global__ void addInto(double* dst, const double* src, uint32_t n) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] += src[i];
+}
+
 // The scene's device view, stream and device for entry points in other translation units (noalloc.cu).
 int sceneView(x2_scene* s, SceneView* view, cudaStream_t* stream, int* device, int* smCount) {
     if (!s || !s->configured) {
@@ -351,7 +357,7 @@ int x2_open(int device, x2_ctx** out) {
     }
     uint32_t dirs[17][32];
     sobolDirections(dirs);
-    if (uploadSobol(dirs) != cudaSuccess || uploadSobolWavefront(dirs) != cudaSuccess) {
+    if (uploadSobol(dirs) != cudaSuccess || uploadSobolWavefront(dirs) != cudaSuccess || uploadSobolAdjoint(dirs) != cudaSuccess) {
         setError("sobol table upload failed");
         cudaStreamDestroy(ctx->stream);
         delete ctx;
@@ -511,6 +517,7 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
         }
     s->lightCount = d->light_count;
     s->triangleCount = d->triangle_count;
+    s->materialCount = d->material_count;
     cudaStream_t st = ctx->stream;
     float* dVerts = nullptr;
     uint32_t* dTris = nullptr;
@@ -1186,6 +1193,85 @@ int x2_items_download(x2_scene* s, float* rgba, uint8_t* status, uint64_t n) {
     if (rgba) cudaMemcpyAsync(rgba, s->out, sizeof(float4) * n, cudaMemcpyDeviceToHost, st);
     if (status) cudaMemcpyAsync(status, s->outStatus, n, cudaMemcpyDeviceToHost, st);
     return x2_wait(s, 600000, nullptr);
+}
+
+// The differentiable parameters: each material's diffuse colour (its Lambert albedo) and each light's radiance, set in
+// place on the device (the BVH and everything else stay). Host arrays, 3 floats each; null leaves a set as it is.
+int x2_scene_set_params(x2_scene* s, const float* albedo, const float* radiance) {
+    if (!s) return X2_EINVAL;
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    cudaStream_t st = s->ctx->stream;
+    if (albedo) {
+        std::vector<MaterialRec> mats(s->materialCount);
+        CUDA_OR(cudaMemcpyAsync(mats.data(), s->materials, sizeof(MaterialRec) * mats.size(), cudaMemcpyDeviceToHost, st), X2_ECUDA);
+        CUDA_OR(cudaStreamSynchronize(st), X2_ECUDA);
+        for (uint32_t m = 0; m < s->materialCount; ++m)
+            for (int k = 0; k < 3; ++k) mats[m].diffuse[k] = albedo[3 * m + k];
+        CUDA_OR(cudaMemcpyAsync(s->materials, mats.data(), sizeof(MaterialRec) * mats.size(), cudaMemcpyHostToDevice, st), X2_ECUDA);
+        CUDA_OR(cudaStreamSynchronize(st), X2_ECUDA);
+    }
+    if (radiance && s->lightCount) {
+        std::vector<x2_light> lights(s->lightCount);
+        CUDA_OR(cudaMemcpyAsync(lights.data(), s->lights, sizeof(x2_light) * lights.size(), cudaMemcpyDeviceToHost, st), X2_ECUDA);
+        CUDA_OR(cudaStreamSynchronize(st), X2_ECUDA);
+        for (uint32_t l = 0; l < s->lightCount; ++l)
+            for (int k = 0; k < 3; ++k) lights[l].radiance[k] = radiance[3 * l + k];
+        CUDA_OR(cudaMemcpyAsync(s->lights, lights.data(), sizeof(x2_light) * lights.size(), cudaMemcpyHostToDevice, st), X2_ECUDA);
+        CUDA_OR(cudaStreamSynchronize(st), X2_ECUDA);
+    }
+    return X2_OK;
+}
+
+// The adjoint of a frame's samples [first, first + count) of every pixel: gradients of a loss with respect to each
+// material's albedo and each light's radiance, given the loss's derivative with respect to the image (device, 3
+// floats a pixel, the image being the film's mean). Device outputs (FP64), added to.
+int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad, double* d_radiance_grad) {
+    if (!s || !s->configured || !d_dloss_dimage || !d_albedo_grad || !d_radiance_grad || count == 0) {
+        setError("x2_adjoint: configured scene, device arrays and a sample count");
+        return X2_EINVAL;
+    }
+    if (s->config.volume_count || s->config.max_depth >= 128 || s->config.bsdf_samples != 1) {
+        setError("x2_adjoint: no volumes, max_depth < 128, bsdf_samples = 1");
+        return X2_EINVAL;
+    }
+    const uint32_t params = 3 * (s->materialCount + s->lightCount);
+    if (size_t(params) * sizeof(float) > 96 * 1024) {
+        setError("x2_adjoint: at most %u materials and lights", 96 * 1024 / 12);
+        return X2_EINVAL;
+    }
+    if (int rc = checkDevice(s->ctx)) return rc;
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    cudaStream_t st = s->ctx->stream;
+    const uint32_t tiles = ((s->config.width + 7) / 8) * ((s->config.height + 7) / 8);
+    std::vector<x2_chunk> chunks(tiles);
+    for (uint32_t t = 0; t < tiles; ++t) chunks[t] = x2_chunk{t, first, count, 0};
+    x2_chunk* d = nullptr;
+    double* grads = nullptr;
+    CUDA_OR(cudaMalloc(&d, sizeof(x2_chunk) * tiles), X2_ENOMEM);
+    if (cudaMalloc(&grads, sizeof(double) * params) != cudaSuccess) {
+        cudaFree(d);
+        setError("x2_adjoint: allocation failed");
+        return X2_ENOMEM;
+    }
+    cudaMemcpyAsync(d, chunks.data(), sizeof(x2_chunk) * tiles, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(grads, 0, sizeof(double) * params, st);
+    const size_t shared = sizeof(float) * params;
+    if (shared > 48 * 1024) cudaFuncSetAttribute(adjointKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shared));
+    SceneView v = viewOf(s);
+    v.stats = nullptr;
+    adjointKernel<<<s->ctx->smCount * 8, 128, shared, st>>>(v, d, tiles, count, d_dloss_dimage, grads, s->materialCount, s->lightCount);
+    int rc = cudaGetLastError() == cudaSuccess ? X2_OK : X2_ECUDA;
+    if (!rc) {
+        // Added to the caller's arrays: albedo then radiance.
+        addInto<<<(params + 255) / 256, 256, 0, st>>>(d_albedo_grad, grads, 3 * s->materialCount);
+        addInto<<<(params + 255) / 256, 256, 0, st>>>(d_radiance_grad, grads + 3 * s->materialCount, 3 * s->lightCount);
+        rc = x2_synchronize(s->ctx, 600000);
+    } else {
+        setError("x2_adjoint: launch failed");
+    }
+    cudaFree(d);
+    cudaFree(grads);
+    return rc;
 }
 
 // The launch-shape autotuner: coordinate descent over the shape's knobs (paths in flight, refill, triangle tests a step,

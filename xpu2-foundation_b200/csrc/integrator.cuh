@@ -78,6 +78,35 @@ __device__ __forceinline__ V3 visibleLights(const SceneView& s, const Identity& 
     return V3{0, 0, 0};
 }
 
+// The light visibleLights picks for the same ray (~0u: none): the adjoint credits that light.
+__device__ __forceinline__ uint32_t visibleLightIndex(const SceneView& s, const Identity& root, V3 origin, V3 dir, float maxDistance) {
+    const x2_config& c = s.config;
+    uint32_t hits = 0;
+    for (uint32_t pass = 0; pass < 3; ++pass)
+        for (uint32_t j = 0; j < c.light_count; ++j) {
+            const x2_light& L = s.lights[j];
+            LightHit lh;
+            const uint32_t vp = L.type == X2_LIGHT_ENV ? 2u : L.type == X2_LIGHT_DISTANT ? 1u : 0u;
+            if (L.visible_in_camera && vp == pass && lightIntersect(L, origin, dir, maxDistance, lh)) ++hits;
+        }
+    if (!hits) return ~0u;
+    Identity id = root;
+    id.branch = childBranch(0x5649534c49474854ull, 0, 0);
+    Stream st(id, 0, 0);
+    const float choice = st.next();
+    const uint32_t chosen = uint32_t(choice * float(hits)) < hits ? uint32_t(choice * float(hits)) : hits - 1;
+    uint32_t seen = 0;
+    for (uint32_t pass = 0; pass < 3; ++pass)
+        for (uint32_t j = 0; j < c.light_count; ++j) {
+            const x2_light& L = s.lights[j];
+            LightHit lh;
+            const uint32_t vp = L.type == X2_LIGHT_ENV ? 2u : L.type == X2_LIGHT_DISTANT ? 1u : 0u;
+            if (!L.visible_in_camera || vp != pass || !lightIntersect(L, origin, dir, maxDistance, lh)) continue;
+            if (seen++ == chosen) return j;
+        }
+    return ~0u;
+}
+
 // The camera ray of sample (pixel, index) as integratePaths makes it (async_integrator.h:1994-2026).
 __device__ __forceinline__ bool cameraRay(const SceneView& s, uint32_t pixel, uint32_t index, CameraRay& camera) {
     const x2_config& c = s.config;
@@ -134,6 +163,7 @@ struct ShadowReq {
     V3 origin, dir;
     float near, far;
     V3 contribution;
+    uint32_t light;  // the light it reaches
 };
 
 // One hit (async_integrator.h:2222-3031 for the admitted materials): shading state, emission, a light sample of
@@ -148,7 +178,9 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
     State st;
     if (!hitState(va, vb, vc, hit.u, hit.v, hit.point, pv.dir, st)) return false;
     Bsdf bsdf;
-    shadeMaterial(s.materials[__ldg(s.meshMaterial + hit.geom)], st, bsdf);
+    const uint32_t material = __ldg(s.meshMaterial + hit.geom);
+    shadeMaterial(s.materials[material], st, bsdf);
+    sink.vertex(material, bsdf);
     if (pv.depth == 0) alpha += 1.0f * (1.0f - (0.0f + 0.0f + 0.0f) / 3.0f);
     radiance = add(radiance, mulv(pv.T, bsdf.emission));
     if (bsdf.count == 0) return true;
@@ -245,6 +277,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
                 t = mulv(t, volumeTransmittance(s, vs, q.origin, wi, q.near, q.far, 1.0f, int(pv.depth) + 1));
             }
             q.contribution = t;
+            q.light = i;
             sink.shadow(q, false);
         }
     }
@@ -329,6 +362,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
                 q.near = shadowNear;
                 q.far = shadowFar;
                 q.contribution = direct;
+                q.light = lightIndex;
                 if (c.volume_count) {
                     Identity tid = bid;
                     tid.branch = childBranch(sampleBranch, 0xfffb, 0);
@@ -391,6 +425,7 @@ struct PlainSink {
         if (visible(s, q.origin, q.dir, q.near, q.far)) radiance = add(radiance, q.contribution);
     }
     __device__ void held() { ++out.held; }
+    __device__ void vertex(uint32_t, const Bsdf&) {}
     __device__ uint32_t top(uint32_t) const { return size; }
     __device__ void push(const Pending& p) { stack[size++] = p; }
 };

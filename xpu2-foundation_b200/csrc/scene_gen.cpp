@@ -551,6 +551,20 @@ Holder* makeVolumeBox(uint64_t seed, int n, uint32_t width, uint32_t height, uin
     return h;
 }
 
+// The differentiable scene (config 4): config 1's construction reduced to about 250k triangles (16x16 heightfield
+// tiles, 23 level-4 icospheres) with its meshes sharing a pool of 64 materials (mesh m takes material m mod 64), so
+// each material's parameters are shared by many surfaces; 512x512.
+Holder* makeAdjointField(uint64_t seed, int tiles, int spheres, uint32_t width, uint32_t height, uint32_t spp, uint32_t depth, x2_config* cfg) {
+    Holder* h = makeField(seed, tiles, spheres, 4, width, height, spp, depth, cfg);
+    const uint32_t pool = std::min<uint32_t>(64u, uint32_t(h->materials.size()));
+    h->materials.resize(pool);
+    for (size_t m = 0; m < h->meshMaterial.size(); ++m) h->meshMaterial[m] = uint32_t(m % pool);
+    const x2_camera cam = h->desc.camera;
+    h->finish();
+    h->desc.camera = cam;
+    return h;
+}
+
 // Batched requests (one frame a request, each its own scene and frame seed): request r draws a triangle count
 // log-uniform in [0.1M, 2M] (half heightfield tiles of 16x16 quads, half level-4 icospheres), a square resolution among
 // 128, 256, 512 and 1024, log-uniform 4..256 spp and a uniform 4..32 depth; its frame seed is 1 + r. `shrink` > 1
@@ -609,6 +623,10 @@ extern "C" int x2_scene_generate(uint32_t config_id, uint64_t seed, x2_scene_des
             h = makeField(seed, 64, 2000, 4, 1920, 1080, 64, 12, config);
         } else if (config_id == 11) {
             h = makeField(seed, 32, 2000, 2, 1920, 1080, 64, 12, config);
+        } else if (config_id == 4) {
+            h = makeAdjointField(seed, 16, 23, 512, 512, 32, 12, config);
+        } else if (config_id == 44) {
+            h = makeAdjointField(seed, 4, 3, 64, 64, 4, 6, config);
         } else if (config_id == 3) {
             h = makeVolumeBox(seed, 256, 512, 512, 256, 64, config);
         } else if (config_id == 33) {

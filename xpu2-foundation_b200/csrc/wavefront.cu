@@ -310,6 +310,7 @@ struct WaveSink {
         else ++nNee;
     }
     __device__ void held() { ++nHeld; }
+    __device__ void vertex(uint32_t, const Bsdf&) {}
     __device__ uint32_t top(uint32_t t) const { return t; }
     __device__ void push(const Pending& c) {
         child = c;
