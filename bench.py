@@ -391,6 +391,48 @@ def probe_volume(args):
     ctx.close()
 
 
+def probe_adjoint(args):
+    """Config 4 (248,832 triangles, 64 materials, 512x512): the primal frame at 32 spp (wavefront and plain) and the
+    adjoint of an L2 image loss at 16 spp (x2_adjoint, samples 32..47), each timed with CUDA events after a warm-up;
+    Msamples/s of each and the adjoint's throughput over the primal's."""
+    import torch
+    import x2
+
+    ctx = x2.Context(0)
+    s = x2.SyntheticScene(4)
+    cfg = s.config
+    scene = x2.Scene(ctx, s.desc, cfg)
+    pixels = cfg.width * cfg.height
+    out = {"probe": "adjoint", "triangles": s.desc.triangle_count, "materials": s.desc.material_count, "primal_spp": 32,
+           "adjoint_spp": 16}
+    for form in ("wavefront", "plain"):
+        for k in range(2):
+            scene.frame_begin(32)
+            (scene.render_frame_wavefront if form == "wavefront" else scene.render_frame)(0, 32)
+            c = scene.wait()
+        out[form] = {"ms": c.milliseconds, "msamples_per_s": pixels * 32 / c.milliseconds / 1e3}
+    sums, counts = scene.film()
+    image = sums[:, :3] / counts[:, None]
+    dev = torch.device("cuda", 0)
+    dl = torch.from_numpy((2.0 * (image - 0.5 * image)).astype(np.float32)).to(dev)
+    ga = torch.zeros((s.desc.material_count, 3), dtype=torch.float64, device=dev)
+    gr = torch.zeros((s.desc.light_count, 3), dtype=torch.float64, device=dev)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    scene.adjoint(32, 16, dl.data_ptr(), ga.data_ptr(), gr.data_ptr())
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    scene.adjoint(32, 16, dl.data_ptr(), ga.data_ptr(), gr.data_ptr())
+    adj_s = time.perf_counter() - t0  # x2_adjoint waits for its launch: host time brackets it
+    out["adjoint"] = {"ms": adj_s * 1e3, "msamples_per_s": pixels * 16 / adj_s / 1e6,
+                      "grad_norms": [float(ga.norm()), float(gr.norm())]}
+    out["adjoint_over_primal"] = out["adjoint"]["msamples_per_s"] / out["wavefront"]["msamples_per_s"]
+    out["adjoint_over_plain"] = out["adjoint"]["msamples_per_s"] / out["plain"]["msamples_per_s"]
+    del start, end
+    print(json.dumps(out))
+    scene.free()
+    ctx.close()
+
+
 def probe(args):
     """One bounded launch for profilers (ncu): `--probe-tiles` evenly spaced tiles of config 1 at 64 spp, in one form;
     the wavefront form without its graph (`--probe-timed`) so each kernel launch is visible on its own."""
@@ -400,6 +442,8 @@ def probe(args):
         return probe_batch(args)
     if args.probe == "volume":
         return probe_volume(args)
+    if args.probe == "adjoint":
+        return probe_adjoint(args)
     ctx = x2.Context(0)
     s = x2.SyntheticScene(1)
     cfg = s.config
@@ -436,7 +480,7 @@ def main():
     ap.add_argument("--impl", default="x2", choices=["x2", "reference"])
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--skip-plain", action="store_true")
-    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume"], help="one bounded launch for a profiler, then exit")
+    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint"], help="one bounded launch for a profiler, then exit")
     ap.add_argument("--probe-tiles", type=int, default=592)
     ap.add_argument("--probe-timed", action="store_true", help="wavefront probe without its graph (per-kernel launches)")
     args = ap.parse_args()

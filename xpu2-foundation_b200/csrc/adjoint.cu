@@ -8,7 +8,8 @@
 // the sampling decisions (directions, light choices, Russian roulette) are held fixed. So d(contribution)/d(param) =
 // contribution / param for every channel where the parameter is not zero, and the replay credits each contribution,
 // weighted by the loss's derivative for its pixel (dL/dI / samples a pixel), to the light it reached and to every Lambert
-// vertex on its way. Credits are FP32 atomics into per-block partials in shared memory, reduced once a block into the
+// vertex on its way (each vertex credited once at the path's end with what the path gathered after it). Credits are FP32
+// sums in the thread and atomics into per-block partials in shared memory, reduced once a block into the
 // FP64 gradients.
 #include "integrator.cuh"
 #include "adjoint.h"
@@ -31,39 +32,50 @@ __device__ __forceinline__ uint32_t tilePixelA(uint32_t tile, uint32_t position,
     return x < width && y < height ? y * width + x : ~0u;
 }
 
-// The block's partial gradients: albedo (3 a material) then radiance (3 a light), in shared memory.
+constexpr uint32_t kLightSlots = 32;  // lights whose credits a thread keeps to itself (more: straight to shared memory)
+
+// A thread's credits. Lights: each contribution, weighted by the loss's derivative for its pixel, over its light's
+// radiance, summed in the thread's own array over all its samples, then into the block's partials once. Albedos: a
+// Lambert vertex's lobe scales everything its path gathers after the vertex (its own light samples and BSDF sample,
+// and all that later vertices add through its throughput), so at the path's end each Lambert vertex k is credited
+// once with (radiance at the end - radiance before k's lobe acted) / its albedo (path replay's suffix sums).
 struct Credits {
-    float* partial;
-    uint32_t materials;
+    float* partial;  // the block's: 3 a material's albedo, then 3 a light's radiance
+    uint32_t materials, lights;
     const SceneView& s;
     V3 delta;  // dL/dI of the sample's pixel over its samples
-    // The Lambert vertices on the current path, by depth: material (~0u: not a Lambert vertex) and albedo.
+    float* lightSum;  // the thread's light credits (kLightSlots x 3)
+    // The path's vertices by depth: Lambert material (~0u: none) and albedo, and the radiance before its lobe acted.
     uint32_t* material;
     V3* albedo;
+    V3* before;
+    uint32_t vertices;
 
-    __device__ void credit(V3 c, uint32_t upTo, uint32_t light) {
-        const V3 w{delta.x * c.x, delta.y * c.y, delta.z * c.z};
-        if (w.x == 0.0f && w.y == 0.0f && w.z == 0.0f) return;
-        if (light != ~0u) {
-            const x2_light& L = s.lights[light];
-            float* g = partial + 3 * (materials + light);
-            if (L.radiance[0] != 0.0f) atomicAdd(g, w.x / L.radiance[0]);
-            if (L.radiance[1] != 0.0f) atomicAdd(g + 1, w.y / L.radiance[1]);
-            if (L.radiance[2] != 0.0f) atomicAdd(g + 2, w.z / L.radiance[2]);
+    __device__ void light(V3 c, uint32_t j) {
+        if (j == ~0u) return;
+        const x2_light& L = s.lights[j];
+        const float w[3] = {delta.x * c.x, delta.y * c.y, delta.z * c.z};
+        for (int k = 0; k < 3; ++k) {
+            if (L.radiance[k] == 0.0f || w[k] == 0.0f) continue;
+            const float v = w[k] / L.radiance[k];
+            if (j < kLightSlots) lightSum[3 * j + k] += v;
+            else atomicAdd(partial + 3 * (materials + j) + k, v);
         }
-        for (uint32_t k = 0; k < upTo; ++k) {
+    }
+    __device__ void albedos(V3 total) {
+        for (uint32_t k = 0; k < vertices; ++k) {
             if (material[k] == ~0u) continue;
-            float* g = partial + 3 * material[k];
+            const V3 after = sub(total, before[k]);
             const V3 a = albedo[k];
-            if (a.x != 0.0f) atomicAdd(g, w.x / a.x);
-            if (a.y != 0.0f) atomicAdd(g + 1, w.y / a.y);
-            if (a.z != 0.0f) atomicAdd(g + 2, w.z / a.z);
+            float* g = partial + 3 * material[k];
+            if (a.x != 0.0f && after.x != 0.0f) atomicAdd(g, delta.x * after.x / a.x);
+            if (a.y != 0.0f && after.y != 0.0f) atomicAdd(g + 1, delta.y * after.y / a.y);
+            if (a.z != 0.0f && after.z != 0.0f) atomicAdd(g + 2, delta.z * after.z / a.z);
         }
     }
 };
 
-// The replay's sink: shadow rays traced at once as the plain megakernel's; each unoccluded one credited to its light
-// and to the path's Lambert vertices up to and with the current one.
+// The replay's sink: shadow rays traced at once as the plain megakernel's; each unoccluded one credited to its light.
 struct AdjointSink {
     const SceneView& s;
     Credits& cr;
@@ -75,11 +87,13 @@ struct AdjointSink {
         const bool lambert = b.count && b.lobe.kind == 0;
         cr.material[depth] = lambert ? material : ~0u;
         cr.albedo[depth] = lambert ? b.lobe.albedo : V3{0, 0, 0};
+        cr.before[depth] = radiance;
+        cr.vertices = depth + 1;
     }
     __device__ void shadow(const ShadowReq& q, bool) {
         if (!visible(s, q.origin, q.dir, q.near, q.far)) return;
         radiance = add(radiance, q.contribution);
-        cr.credit(q.contribution, depth + 1, q.light);
+        cr.light(q.contribution, q.light);
     }
     __device__ void held() {}
     __device__ uint32_t top(uint32_t) const { return size; }
@@ -87,7 +101,8 @@ struct AdjointSink {
 };
 
 // One sample's replay (the plain megakernel's loop, integrator.cuh's integrate, with the credits).
-__device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, uint32_t index, V3 delta, float* partial, uint32_t materials) {
+__device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, uint32_t index, V3 delta, float* partial, uint32_t materials,
+                                           uint32_t lights, float* lightSum) {
     CameraRay camera;
     if (!cameraRay(s, pixel, index, camera)) return;
     const Identity root{pixel, U64(index), U64(s.config.seed), 0};
@@ -98,33 +113,28 @@ __device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, u
     V3 radiance{0, 0, 0};
     float alpha = 0.0f;
     uint32_t material[kMaxPathVertices];
-    V3 albedo[kMaxPathVertices];
-    Credits cr{partial, materials, s, delta, material, albedo};
+    V3 albedo[kMaxPathVertices], before[kMaxPathVertices];
+    Credits cr{partial, materials, lights, s, delta, lightSum, material, albedo, before, 0};
     while (top) {
         Pending pv = stack[--top];
         if (pv.depth >= kMaxPathVertices) continue;
         V3 va, vb, vc;
         const Hit hit = trace(s, pv.origin, pv.dir, pv.nearT, pv.farT, va, vb, vc);
-        // The held light (bounce-ray reuse): the parent's BSDF sample reached it, so it passed the parent too.
-        if (pv.heldLight != ~0u && !(hit.geom != ~0u && hit.t < pv.heldFar)) cr.credit(pv.held, pv.depth, pv.heldLight);
-        const V3 before = radiance;
+        // The held light (bounce-ray reuse): reached unless the ray met something short of it.
+        if (pv.heldLight != ~0u && !(hit.geom != ~0u && hit.t < pv.heldFar)) cr.light(pv.held, pv.heldLight);
+        const V3 prior = radiance;
         afterTrace(s, root, pv, hit, cameraPosition, radiance, alpha);
-        // What afterTrace added besides the held light: the light a camera ray sees (no vertex before it).
+        // The light a camera ray sees (afterTrace added it).
         if (pv.depth == 0 && s.config.visible_lights) {
-            const V3 added = sub(radiance, before);
             const bool missed = hit.geom == ~0u;
-            const uint32_t j = visibleLightIndex(s, root, missed ? pv.origin : cameraPosition, pv.dir, missed ? 3.4028234663852886e+38f : hit.t);
-            if (j != ~0u) cr.credit(added, 0, j);
+            cr.light(sub(radiance, prior),
+                     visibleLightIndex(s, root, missed ? pv.origin : cameraPosition, pv.dir, missed ? 3.4028234663852886e+38f : hit.t));
         }
         if (hit.geom == ~0u) continue;
-        // The hit's emission (shadeVertex adds it first): through the vertices before it.
         AdjointSink sink{s, cr, radiance, stack, top, pv.depth};
-        const uint32_t m = __ldg(s.meshMaterial + hit.geom);
-        const MaterialRec& mr = s.materials[m];
-        const V3 emission{mr.emission[0], mr.emission[1], mr.emission[2]};
         if (!shadeVertex(s, root, pixel, index, pv, hit, va, vb, vc, top, radiance, alpha, sink)) return;
-        if (!isBlack(emission)) cr.credit(mulv(pv.T, emission), pv.depth, ~0u);
     }
+    cr.albedos(radiance);
 }
 
 }  // namespace
@@ -135,10 +145,17 @@ __global__ void __launch_bounds__(128) adjointKernel(SceneView s, const x2_chunk
     extern __shared__ float partial[];
     const uint32_t params = 3 * (materials + lights);
     for (uint32_t i = threadIdx.x; i < params; i += blockDim.x) partial[i] = 0.0f;
+    float lightSum[3 * kLightSlots];
+    for (uint32_t i = 0; i < 3 * kLightSlots; ++i) lightSum[i] = 0.0f;
     __syncthreads();
     const unsigned long long items = 64ull * chunkCount * count;
-    for (unsigned long long item = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; item < items;
-         item += (unsigned long long)gridDim.x * blockDim.x) {
+    // Rounds a warp takes together (one item a lane, the warp reconverged between rounds), so its lanes replay
+    // neighbouring samples of one pixel side by side instead of drifting apart through their own item sequences.
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < items; base += stride) {
+        const unsigned long long item = base + (threadIdx.x & 31u);
+        __syncwarp();
+        if (item >= items) continue;
         const uint32_t chunk = uint32_t(item / (64ull * count));
         const uint32_t offset = uint32_t(item - (unsigned long long)chunk * 64ull * count);
         const uint32_t position = offset / count, sample = offset % count;
@@ -149,8 +166,11 @@ __global__ void __launch_bounds__(128) adjointKernel(SceneView s, const x2_chunk
         const float inv = 1.0f / float(ch.count);
         const V3 delta{dLossdImage[3ull * pixel] * inv, dLossdImage[3ull * pixel + 1] * inv, dLossdImage[3ull * pixel + 2] * inv};
         if (delta.x == 0.0f && delta.y == 0.0f && delta.z == 0.0f) continue;
-        adjointSample(s, pixel, ch.first + sample, delta, partial, materials);
+        adjointSample(s, pixel, ch.first + sample, delta, partial, materials, lights, lightSum);
     }
+    for (uint32_t j = 0; j < lights && j < kLightSlots; ++j)
+        for (int k = 0; k < 3; ++k)
+            if (lightSum[3 * j + k] != 0.0f) atomicAdd(partial + 3 * (materials + j) + k, lightSum[3 * j + k]);
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < params; i += blockDim.x)
         if (partial[i] != 0.0f) atomicAdd(gradients + i, double(partial[i]));

@@ -180,9 +180,9 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
     Bsdf bsdf;
     const uint32_t material = __ldg(s.meshMaterial + hit.geom);
     shadeMaterial(s.materials[material], st, bsdf);
-    sink.vertex(material, bsdf);
     if (pv.depth == 0) alpha += 1.0f * (1.0f - (0.0f + 0.0f + 0.0f) / 3.0f);
     radiance = add(radiance, mulv(pv.T, bsdf.emission));
+    sink.vertex(material, bsdf);  // the vertex, its emission added: what comes after passes its lobe
     if (bsdf.count == 0) return true;
 
     uint32_t indirectFlags = 0;
