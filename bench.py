@@ -193,6 +193,12 @@ def traffic_from_profile():
         return {}
 
 
+def apply_shape(scene, spec):
+    """x2_wavefront_tune with the fields named in `spec` ("k=v,k=v"), the others at their defaults."""
+    if spec:
+        scene.wavefront_tune(**{k: int(v) for k, v in (kv.split("=") for kv in spec.split(","))})
+
+
 def frame(scene, cfg, first, wavefront):
     scene.frame_begin(cfg.spp)
     if wavefront:
@@ -211,6 +217,7 @@ def run(args):
     cfg = s.config
     t0 = time.perf_counter()
     scene = x2.Scene(ctx, s.desc, cfg)
+    apply_shape(scene, args.shape)
     info = scene.info()
     load_s = time.perf_counter() - t0
     samples_per_frame = cfg.width * cfg.height * cfg.spp
@@ -301,6 +308,7 @@ def run(args):
             "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded generator, config 1; no dataset)",
             "config": {"workload": WORKLOAD + ", wavefront form", "triangles": s.desc.triangle_count, "samples_per_step": samples_per_frame * world,
+                       "wavefront_shape": args.shape or "library defaults",
                        "l2": "inputs larger than L2 (BVH %.0f MB + triangles %.0f MB > 126 MB)" % (info["bvh_bytes"] / 1e6, info["triangle_bytes"] / 1e6),
                        "bvh_build_ms": info["build_ms"], "scene_load_s": load_s, "paths_in_flight": winfo["paths"],
                        "parallelism": f"{world} GPU(s), replicated scene, distinct sample indices a rank"},
@@ -417,19 +425,32 @@ def probe_adjoint(args):
     dl = torch.from_numpy((2.0 * (image - 0.5 * image)).astype(np.float32)).to(dev)
     ga = torch.zeros((s.desc.material_count, 3), dtype=torch.float64, device=dev)
     gr = torch.zeros((s.desc.light_count, 3), dtype=torch.float64, device=dev)
+    gg = torch.zeros(s.desc.material_count, dtype=torch.float64, device=dev)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    scene.adjoint(32, 16, dl.data_ptr(), ga.data_ptr(), gr.data_ptr())
+    scene.adjoint(32, 16, dl.data_ptr(), ga.data_ptr(), gr.data_ptr(), gg.data_ptr())
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    scene.adjoint(32, 16, dl.data_ptr(), ga.data_ptr(), gr.data_ptr())
+    scene.adjoint(32, 16, dl.data_ptr(), ga.data_ptr(), gr.data_ptr(), gg.data_ptr())
     adj_s = time.perf_counter() - t0  # x2_adjoint waits for its launch: host time brackets it
     out["adjoint"] = {"ms": adj_s * 1e3, "msamples_per_s": pixels * 16 / adj_s / 1e6,
-                      "grad_norms": [float(ga.norm()), float(gr.norm())]}
+                      "grad_norms": {"albedo": float(ga.norm()), "radiance": float(gr.norm()), "roughness": float(gg.norm())}}
     out["adjoint_over_primal"] = out["adjoint"]["msamples_per_s"] / out["wavefront"]["msamples_per_s"]
     out["adjoint_over_plain"] = out["adjoint"]["msamples_per_s"] / out["plain"]["msamples_per_s"]
     del start, end
     print(json.dumps(out))
     scene.free()
+    ctx.close()
+
+
+def probe_rmse(args):
+    """Image RMSE of both forms against the reference's converged renders (16,384 spp, FP64 film) of seeded tiles of
+    every configuration with a fixture (tests/golden/rmse_c*.npz); one JSON line a fixture."""
+    import rmse_lib
+    import x2
+
+    ctx = x2.Context(0)
+    for path in rmse_lib.fixtures():
+        print(json.dumps(dict(probe="rmse", **rmse_lib.measure(ctx, path))), flush=True)
     ctx.close()
 
 
@@ -444,10 +465,13 @@ def probe(args):
         return probe_volume(args)
     if args.probe == "adjoint":
         return probe_adjoint(args)
+    if args.probe == "rmse":
+        return probe_rmse(args)
     ctx = x2.Context(0)
     s = x2.SyntheticScene(1)
     cfg = s.config
     scene = x2.Scene(ctx, s.desc, cfg)
+    apply_shape(scene, args.shape)
     tiles = ((cfg.width + 7) // 8) * ((cfg.height + 7) // 8)
     sel = np.linspace(0, tiles - 1, args.probe_tiles).astype(np.uint32)
     chunks = np.zeros(len(sel), x2.CHUNK_DTYPE)
@@ -461,7 +485,7 @@ def probe(args):
         scene.launch_wavefront(chunks)
     c = scene.wait()
     out = {"probe": args.probe, "tiles": len(sel), "samples": n, "ms": c.milliseconds, "msamples_per_s": n / c.milliseconds / 1e3,
-           "errors": c.errors}
+           "errors": c.errors, "shape": args.shape}
     if args.probe == "wavefront":
         out["kernel_ms"] = scene.wavefront_timing(None)
         out["wavefront"] = scene.wavefront_info()
@@ -480,9 +504,10 @@ def main():
     ap.add_argument("--impl", default="x2", choices=["x2", "reference"])
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--skip-plain", action="store_true")
-    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint"], help="one bounded launch for a profiler, then exit")
+    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint", "rmse"], help="one bounded launch for a profiler, then exit")
     ap.add_argument("--probe-tiles", type=int, default=592)
     ap.add_argument("--probe-timed", action="store_true", help="wavefront probe without its graph (per-kernel launches)")
+    ap.add_argument("--shape", default="", help="wavefront launch shape fields, e.g. lobe_queues=0,refill=8 (default: the library's)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.probe:

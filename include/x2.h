@@ -234,7 +234,9 @@ typedef struct x2_wavefront_shape {
     uint32_t shade_blocks;   /* shade kernel's occupancy variant (0, 3, 4) */
     uint32_t tri_limit;      /* triangle tests a lane makes a traversal step, the rest on the next steps (1..32) */
     uint32_t batch_window;   /* x2_render_batch: work items a window (0: 2^27; at least one chunk a window) */
-    uint32_t reserved[1];
+    uint32_t lobe_queues;    /* 1: shade takes the extended paths from per-lobe queues (GGX, Lambert, then none or
+                                missed), sorted after extend, so a warp runs one lobe's code; 0: in the extend queue's
+                                order */
 } x2_wavefront_shape;
 void x2_wavefront_shape_defaults(x2_wavefront_shape* shape);
 int x2_wavefront_tune(x2_scene* scene, const x2_wavefront_shape* shape);
@@ -258,15 +260,17 @@ typedef struct x2_request {
 int x2_render_batch(x2_ctx* ctx, const x2_request* requests, uint32_t n, x2_completion* out);
 /* ---- differentiation (no reference counterpart; config 4) ----
  * The differentiable parameters, set in place: each material's diffuse colour (a Lambert lobe's albedo; 3 floats a
- * material) and each light's radiance (3 floats a light); host arrays, null leaves a set as it is. Waits. */
-int x2_scene_set_params(x2_scene* scene, const float* albedo, const float* radiance);
+ * material), each material's roughness (a GGX lobe's; 1 float a material) and each light's radiance (3 floats a
+ * light); host arrays, null leaves a set as it is. Waits. */
+int x2_scene_set_params(x2_scene* scene, const float* albedo, const float* roughness, const float* radiance);
 /* The adjoint of samples [first, first + count) of every pixel (the film's mean image): given dL/dimage (device, 3
- * floats a pixel), adds dL/dalbedo (device, 3 doubles a material) and dL/dradiance (device, 3 doubles a light). Each
- * sample's path is replayed from its identity (nothing of a primal pass is stored) and each contribution credited to
- * the light it reached and the Lambert vertices it passed, the sampling decisions held fixed. Requires no volumes,
- * max_depth < 128, bsdf_samples = 1. Waits. */
+ * floats a pixel), adds dL/dalbedo (device, 3 doubles a material), dL/droughness (device, 1 double a material; null:
+ * not wanted) and dL/dradiance (device, 3 doubles a light). Each sample's path is replayed from its identity (nothing
+ * of a primal pass is stored) and each contribution credited to the light it reached and the Lambert and GGX vertices
+ * it passed, the sampling decisions (directions, pdfs, MIS weights, roulette) held fixed. Requires no volumes,
+ * max_depth < 128, bsdf_samples = 1, 4 x materials + 3 x lights <= 24576. Waits. */
 int x2_adjoint(x2_scene* scene, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad,
-               double* d_radiance_grad);
+               double* d_roughness_grad, double* d_radiance_grad);
 /* The last timed wavefront launch's queue sizes: for each iteration, rays extended then shadow rays (2 a
  * iteration, at most max values). */
 int x2_wavefront_queues(x2_scene* scene, uint32_t* sizes, uint32_t max);

@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -475,9 +476,12 @@ xi::mixed::Config toConfig(const x2_config& x, const x2_camera& cam) {
     return c;
 }
 
+#include "adjoint64.h"
+
 struct Handle {
     Scene scene;
     Counts counts;
+    adj64::Scene64 x;  // the engine's own records, for the FP64 adjoint
 };
 
 }  // namespace
@@ -523,6 +527,11 @@ void* x2ref_open(const x2_scene_desc* d, const x2_config* cfg) {
     }
     for (U32 i = 0; i < d->light_count; ++i) s.lights.push_back(toLight(d->lights[i], i));
     s.config = toConfig(*cfg, d->camera);
+    h->x.materials.assign(d->materials, d->materials + d->material_count);
+    h->x.meshMaterial.assign(d->mesh_material, d->mesh_material + d->mesh_count);
+    h->x.lights.assign(d->lights, d->lights + d->light_count);
+    h->x.camera = d->camera;
+    h->x.config = *cfg;
     // Grids (dense, as the NanoVDB stand-in holds them) and the VdbVolume shaders over them.
     s.gridValues.resize(d->grid_count);
     s.floatGrids.resize(d->grid_count);
@@ -720,6 +729,123 @@ int x2ref_render_tiles(void* p, const uint32_t* tiles, uint32_t ntiles, uint32_t
         rays[3] = total.held;
     }
     return errors ? X2_EDEVICE : X2_OK;
+}
+
+// renderChunk over a list of tiles with their film: tile k's position pos (pixel tilePixel(tiles[k], pos)) sums its
+// samples [first, first+count) in FP64 into sums[4 (64 k + pos) ...] (rgb, alpha) and counts them in counts[64 k +
+// pos]; positions past the frame's edge stay zero. Each tile is one worker's, so no two threads share a sum.
+int x2ref_render_tiles_film(void* p, const uint32_t* tiles, uint32_t ntiles, uint32_t first, uint32_t count, int threads, double* sums,
+                            uint32_t* counts) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h || !tiles || !sums || !counts) return X2_EINVAL;
+    const auto& c = h->scene.config;
+    std::atomic<U32> next{0};
+    std::atomic<uint64_t> errors{0};
+    std::vector<Counts> per(std::max(threads, 1));
+    auto work = [&](int w) {
+        OracleBackend backend{h->scene, &per[w]};
+        for (;;) {
+            const U32 k = next.fetch_add(1);
+            if (k >= ntiles) break;
+            for (U32 s = 0; s < count; ++s)
+                for (U32 pos = 0; pos < 64; ++pos) {
+                    const U32 pixel = xi::async::tilePixel(tiles[k], pos, c.width, c.height);
+                    if (pixel == ~0u) continue;
+                    xi::async::Radiance r;
+                    const auto st = xi::async::integratePaths(c, pixel, first + s, backend, r);
+                    double* sum = sums + 4 * (64 * size_t(k) + pos);
+                    if (st == xi::async::SampleStatus::Done) {
+                        for (int j = 0; j < 3; ++j) sum[j] += r.rgb[j];
+                        sum[3] += r.alpha;
+                        ++counts[64 * size_t(k) + pos];
+                    } else if (st == xi::async::SampleStatus::Skip) {
+                        ++counts[64 * size_t(k) + pos];
+                    } else {
+                        ++errors;
+                    }
+                }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < threads; ++w) pool.emplace_back(work, w);
+    work(0);
+    for (auto& t : pool) t.join();
+    return errors ? X2_EDEVICE : X2_OK;
+}
+
+// The FP64 adjoint (adjoint64.h) of samples [first, first + count) of every pixel: given dL/dimage (3 floats a pixel,
+// the image being the mean of those samples), the gradients with respect to each material's albedo (3 a material),
+// roughness (1 a material) and each light's radiance (3 a light), summed in double; `image` (3 doubles a pixel, or
+// null) gets each pixel's radiance summed over the samples in double; `mass` (or null) each gradient's sum of credit
+// magnitudes, in the gradients' order (albedo, roughness, radiance). Requires no volumes and bsdf_samples = 1.
+// Parameters as set with x2ref_set_params (or the scene's own).
+int x2ref_adjoint64(void* p, uint32_t first, uint32_t count, const float* dldi, int threads, double* albedo, double* roughness,
+                    double* radiance, double* image, double* mass) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h || !dldi || !albedo || !roughness || !radiance || count == 0) return X2_EINVAL;
+    const auto& c = h->x.config;
+    if (c.volume_count || c.bsdf_samples != 1 || c.max_depth >= 128) return X2_EINVAL;
+    const U32 pixels = c.width * c.height, M = U32(h->x.materials.size()), L = U32(h->x.lights.size());
+    threads = std::max(threads, 1);
+    std::vector<adj64::Grads> per(threads);
+    std::atomic<U32> next{0};
+    auto work = [&](int w) {
+        adj64::Grads& g = per[w];
+        g.albedo.assign(3 * M, 0.0);
+        g.roughness.assign(M, 0.0);
+        g.radiance.assign(3 * L, 0.0);
+        g.albedoMass.assign(3 * M, 0.0);
+        g.roughnessMass.assign(M, 0.0);
+        g.radianceMass.assign(3 * L, 0.0);
+        for (;;) {
+            const U32 px = next.fetch_add(1);
+            if (px >= pixels) break;
+            const adj64::D3 delta{double(dldi[3 * size_t(px)]) / count, double(dldi[3 * size_t(px) + 1]) / count, double(dldi[3 * size_t(px) + 2]) / count};
+            adj64::Tracer t{h->scene, h->x, g, delta};
+            adj64::D3 sum{0, 0, 0};
+            for (U32 k = 0; k < count; ++k) sum = sum + t.sample(px, first + k);
+            if (image) {
+                image[3 * size_t(px)] = sum.x;
+                image[3 * size_t(px) + 1] = sum.y;
+                image[3 * size_t(px) + 2] = sum.z;
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (int w = 1; w < threads; ++w) pool.emplace_back(work, w);
+    work(0);
+    for (auto& t : pool) t.join();
+    for (U32 i = 0; i < 3 * M; ++i) albedo[i] = 0;
+    for (U32 i = 0; i < M; ++i) roughness[i] = 0;
+    for (U32 i = 0; i < 3 * L; ++i) radiance[i] = 0;
+    if (mass)
+        for (U32 i = 0; i < 4 * M + 3 * L; ++i) mass[i] = 0;
+    for (const auto& g : per) {
+        for (U32 i = 0; i < 3 * M; ++i) albedo[i] += g.albedo[i];
+        for (U32 i = 0; i < M; ++i) roughness[i] += g.roughness[i];
+        for (U32 i = 0; i < 3 * L; ++i) radiance[i] += g.radiance[i];
+        if (!mass) continue;
+        for (U32 i = 0; i < 3 * M; ++i) mass[i] += g.albedoMass[i];
+        for (U32 i = 0; i < M; ++i) mass[3 * M + i] += g.roughnessMass[i];
+        for (U32 i = 0; i < 3 * L; ++i) mass[4 * M + i] += g.radianceMass[i];
+    }
+    return X2_OK;
+}
+
+// The FP64 adjoint's parameters, as x2_scene_set_params sets the engine's (null leaves a set as it is). The reference
+// integrator's records are left as they are: after this, only x2ref_adjoint64 sees the new values.
+int x2ref_set_params(void* p, const float* albedo, const float* roughness, const float* radiance) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h) return X2_EINVAL;
+    for (size_t m = 0; m < h->x.materials.size(); ++m) {
+        if (albedo)
+            for (int k = 0; k < 3; ++k) h->x.materials[m].diffuse[k] = albedo[3 * m + k];
+        if (roughness) h->x.materials[m].roughness = roughness[m];
+    }
+    if (radiance)
+        for (size_t j = 0; j < h->x.lights.size(); ++j)
+            for (int k = 0; k < 3; ++k) h->x.lights[j].radiance[k] = radiance[3 * j + k];
+    return X2_OK;
 }
 
 // Traversal parity: closest hit (triangle, t) or ~0u, and occlusion, for n rays (origin, direction, near, far).

@@ -68,6 +68,7 @@ class Reference:
         lib.x2ref_child_branch.restype = u64
         cfg = synthetic.config if config is None else config
         self.config = cfg
+        self._desc_counts = (synthetic.desc.material_count, synthetic.desc.light_count)
         self.h = lib.x2ref_open(synthetic.desc_ptr, C.byref(cfg))
         if not self.h:
             raise RuntimeError("x2ref_open failed")
@@ -112,6 +113,18 @@ class Reference:
                                          rays.ctypes.data)
         return rc, int(samples[0]), rays
 
+    def render_tiles_film(self, tiles, first, count, threads=None):
+        """The given tiles' film: (rc, sums [tiles, 64, 4] FP64, counts [tiles, 64]); tile k's position pos is pixel
+        tilePixel(tiles[k], pos) (row-major 8x8 within the tile)."""
+        tiles = np.ascontiguousarray(tiles, np.uint32)
+        sums = np.zeros((len(tiles), 64, 4))
+        counts = np.zeros((len(tiles), 64), np.uint32)
+        f = self.lib.x2ref_render_tiles_film
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int, C.c_void_p, C.c_void_p]
+        f.restype = C.c_int
+        rc = f(self.h, tiles.ctypes.data, len(tiles), first, count, threads or os.cpu_count(), sums.ctypes.data, counts.ctypes.data)
+        return rc, sums, counts
+
     def trace(self, rays, brute=False):
         """Closest hit (triangle, t) and occlusion through the oracle's BVH, or by testing every triangle."""
         rays = np.ascontiguousarray(rays, np.float32)
@@ -155,3 +168,34 @@ def sample_pairs(config, n, seed):
     pixels = r.integers(0, config.width * config.height, n).astype(np.uint32)
     indices = r.integers(0, config.spp, n).astype(np.uint32)
     return pixels, indices
+
+
+def adjoint64(ref, first, count, dldi, threads=None, params=None, masses=False):
+    """The FP64 CPU adjoint (oracle/adjoint64.h) of samples [first, first + count) of every pixel, given dL/dimage
+    (pixels x 3): (albedo grads [materials, 3], roughness grads [materials], radiance grads [lights, 3], image sums
+    [pixels, 3]), all FP64, and with `masses` the gradients' credit masses (sums of credit magnitudes) in the same
+    shapes. `params` = (albedo, roughness, radiance) arrays (None entries kept) set first."""
+    lib = ref.lib
+    vp = C.c_void_p
+    lib.x2ref_adjoint64.argtypes = [vp, C.c_uint32, C.c_uint32, vp, C.c_int, vp, vp, vp, vp, vp]
+    lib.x2ref_adjoint64.restype = C.c_int
+    lib.x2ref_set_params.argtypes = [vp, vp, vp, vp]
+    lib.x2ref_set_params.restype = C.c_int
+    if params is not None:
+        arrs = [None if a is None else np.ascontiguousarray(a, np.float32) for a in params]
+        ptrs = [None if a is None else a.ctypes.data for a in arrs]
+        assert lib.x2ref_set_params(ref.h, *ptrs) == 0
+    d = ref._desc_counts
+    dldi = np.ascontiguousarray(dldi, np.float32)
+    ga = np.zeros((d[0], 3))
+    gg = np.zeros(d[0])
+    gr = np.zeros((d[1], 3))
+    img = np.zeros((ref.config.width * ref.config.height, 3))
+    mass = np.zeros(4 * d[0] + 3 * d[1])
+    rc = lib.x2ref_adjoint64(ref.h, first, count, dldi.ctypes.data, threads or os.cpu_count(), ga.ctypes.data, gg.ctypes.data,
+                             gr.ctypes.data, img.ctypes.data, mass.ctypes.data)
+    assert rc == 0, rc
+    if masses:
+        M = d[0]
+        return ga, gg, gr, img, (mass[:3 * M].reshape(M, 3), mass[3 * M:4 * M], mass[4 * M:].reshape(-1, 3))
+    return ga, gg, gr, img

@@ -148,3 +148,65 @@ def test_library_exports_every_declared_symbol():
     for n in sorted(names):
         assert hasattr(lib, n), n
     assert lib.x2_version().startswith(b"x2-b200")
+
+
+@pytest.fixture(scope="module")
+def adjoint_scene():
+    if not oracle_lib.have_reference():
+        pytest.skip("oracle/_ref not built")
+    s = x2.SyntheticScene(44)
+    ref = oracle_lib.Reference(s)
+    yield s, ref
+    ref.close()
+
+
+def test_fp64_adjoint_primal_matches_reference(adjoint_scene):
+    """The FP64 CPU adjoint's own primal (oracle/adjoint64.h, the estimator restated in double) against the reference
+    integrator compiled from source on the same samples: pixel sums within 1e-4 relative on almost every pixel (a
+    shadow ray that grazes an edge can go the other way once its direction is computed in double), and the image
+    mean within 1e-5."""
+    s, ref = adjoint_scene
+    cfg = s.config
+    w = np.zeros((cfg.width * cfg.height, 3), np.float32)
+    _, _, _, img = oracle_lib.adjoint64(ref, 0, cfg.spp, w + 1.0)
+    rc, sums, _, counts, _ = ref.render(0, cfg.spp)
+    assert rc == 0 and (counts == cfg.spp).all()
+    want = sums[:, :3]
+    ok = (np.abs(img - want) <= 1e-4 * np.abs(want) + 1e-6).all(1)
+    assert ok.mean() >= 0.97
+    assert abs(img.mean() - want.mean()) <= 1e-5 * want.mean()
+
+
+def test_fp64_adjoint_against_finite_differences(adjoint_scene):
+    """The FP64 adjoint's albedo and radiance gradients against central differences of its own FP64 primal with
+    common random numbers (both parameters enter linearly, the sampling decisions barely move): within 0.5%."""
+    s, ref = adjoint_scene
+    cfg = s.config
+    d = s.desc
+    albedo = np.array([list(d.materials[m].diffuse) for m in range(d.material_count)], np.float64)
+    radiance = np.array([list(d.lights[i].radiance) for i in range(d.light_count)], np.float64)
+    kinds = np.array([d.materials[m].kind for m in range(d.material_count)])
+    w = np.random.default_rng(11).random((cfg.width * cfg.height, 3)).astype(np.float32)
+    ga, gg, gr, _ = oracle_lib.adjoint64(ref, 0, cfg.spp, w, params=(albedo, None, radiance))
+    assert np.all(ga[kinds != x2.MAT_LAMBERT] == 0) and np.all(gg[kinds != x2.MAT_GGX] == 0)
+
+    def loss(a, r):
+        _, _, _, img = oracle_lib.adjoint64(ref, 0, cfg.spp, w, params=(a, None, r))
+        return float((img / cfg.spp * w).sum())
+
+    lam = np.flatnonzero(kinds == x2.MAT_LAMBERT)
+    for m in lam[np.argsort(-np.abs(ga[lam, 1]))][:3]:
+        h = 1e-4 * albedo[m, 1]
+        up, down = albedo.copy(), albedo.copy()
+        up[m, 1] += h
+        down[m, 1] -= h
+        fd = (loss(up, radiance) - loss(down, radiance)) / (2 * h)
+        assert abs(fd - ga[m, 1]) <= 5e-3 * abs(ga[m, 1]), (m, fd, ga[m, 1])
+    for i in np.argsort(-np.abs(gr[:, 0]))[:3]:
+        h = 1e-4 * radiance[i, 0]
+        up, down = radiance.copy(), radiance.copy()
+        up[i, 0] += h
+        down[i, 0] -= h
+        fd = (loss(albedo, up) - loss(albedo, down)) / (2 * h)
+        assert abs(fd - gr[i, 0]) <= 5e-3 * abs(gr[i, 0]), (i, fd, gr[i, 0])
+    oracle_lib.adjoint64(ref, 0, cfg.spp, w, params=(albedo, None, radiance))

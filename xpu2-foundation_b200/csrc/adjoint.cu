@@ -1,16 +1,25 @@
-// The adjoint of the path tracer: gradients of an image loss with respect to each Lambert material's albedo and each
-// light's radiance, by replaying each sample's path from its identity (path replay: nothing of the primal pass is
-// stored; Vicini, Speierer and Jakob 2021).
+// The adjoint of the path tracer: gradients of an image loss with respect to each Lambert material's albedo, each GGX
+// material's roughness and each light's radiance, by replaying each sample's path from its identity (path replay:
+// nothing of the primal pass is stored; Vicini, Speierer and Jakob 2021).
 //
-// Both parameters enter a sample's radiance multiplicatively: a contribution that reaches light i carries its radiance
-// channel by channel, and one that passed Lambert vertices carries each vertex's albedo once per vertex (the BSDF
-// weight of a cosine-sampled Lambert lobe is its albedo; its light-sample value is albedo / pi times the cosine), while
-// the sampling decisions (directions, light choices, Russian roulette) are held fixed. So d(contribution)/d(param) =
-// contribution / param for every channel where the parameter is not zero, and the replay credits each contribution,
-// weighted by the loss's derivative for its pixel (dL/dI / samples a pixel), to the light it reached and to every Lambert
-// vertex on its way (each vertex credited once at the path's end with what the path gathered after it). Credits are FP32
-// sums in the thread and atomics into per-block partials in shared memory, reduced once a block into the
-// FP64 gradients.
+// The sampling decisions (directions, light choices, Russian roulette and its scale, MIS weights, pdfs) are held fixed
+// at their values for the current parameters: the estimator differentiates only the values a contribution carries.
+// Its expectation is the derivative of the image's expectation (each sampling density, held fixed, still integrates
+// the differentiated integrand; each decision's weight keeps its expectation), so it is unbiased, and finite
+// differences with common random numbers converge to it.
+//
+// - Light radiance and Lambert albedo enter a contribution multiplicatively: a contribution that reaches light i
+//   carries its radiance channel by channel, and one that passed Lambert vertices carries each vertex's albedo once a
+//   vertex (the BSDF weight of a cosine-sampled Lambert lobe is its albedo; its light-sample value is albedo / pi
+//   times the cosine). So d(contribution)/d(param) = contribution / param channel by channel.
+// - GGX roughness enters through the lobe's value f(wo, wi) = F G1(wo) G1(wi) D(m) / cos(wo) at the directions the
+//   vertex used: d(contribution)/dr = contribution * dlog f/dr at the light sample's direction for that light
+//   sample, and at the BSDF sample's direction for everything the path gathered after the BSDF sample (its light hit
+//   and all later vertices).
+//
+// Each vertex's credit is taken once at the path's end from suffix sums (the radiance gathered after the vertex acted),
+// weighted by the loss's derivative for its pixel (dL/dI / samples a pixel). Credits are FP32 sums in the thread and
+// atomics into per-block partials in shared memory, reduced once a block into the FP64 gradients.
 #include "integrator.cuh"
 #include "adjoint.h"
 
@@ -19,6 +28,42 @@ namespace x2 {
 // This translation unit's copy of the Sobol direction table (sampler.cuh).
 cudaError_t uploadSobolAdjoint(const uint32_t directions[17][32]) {
     return cudaMemcpyToSymbol(c_sobol, directions, sizeof(uint32_t) * 17 * 32);
+}
+
+// d log f / d(material roughness) of the GGX lobe l (shading.cuh evalGGX) at directions wo, wi; 0 where f is 0 or
+// the roughness is clamped. With a = the lobe roughness max(0.001, r^2) (r the material's roughness, saturated),
+// T = tan^2 of the half vector's angle and t = tan^2 of a direction's angle:
+//   log D  = log(a^2) - 2 log(a^2 + T) + const         -> 2/a - 4a/(a^2 + T)
+//   log G1 = log 2 - log(1 + S), S = sqrt(1 + a^2 t)   -> -a t / (S (1 + S))
+// and da/dr = 2r where r^2 > 0.001 (0 < r < 1). The Schlick Fresnel does not depend on the roughness.
+// Near a mirror (a of 1e-3..1e-2) the two terms of dlog D are hundreds each and a path's credits cancel over samples to
+// a gradient thousands of times smaller, so T must be exact to far better than float's 1 - cos^2 gives: the tangents
+// are taken from |x cross n|^2 / (x . n)^2, in double (a few dozen FP64 operations a vertex).
+__device__ __forceinline__ float ggxLogDerivative(const Lobe& l, float materialRoughness, V3 wo, V3 wi) {
+    const double r = materialRoughness;
+    if (!(r > 0.0 && r < 1.0) || materialRoughness * materialRoughness <= 0.001f) return 0.0f;
+    const double nx = l.frame.z.x, ny = l.frame.z.y, nz = l.frame.z.z;
+    const double ox = wo.x, oy = wo.y, oz = wo.z, ix = wi.x, iy = wi.y, iz = wi.z;
+    const double cosNO = ox * nx + oy * ny + oz * nz, cosNI = ix * nx + iy * ny + iz * nz;
+    if (cosNO <= 0.0 || cosNI <= 0.0) return 0.0f;
+    double mx = ox + ix, my = oy + iy, mz = oz + iz;
+    const double lm = sqrt(mx * mx + my * my + mz * mz);
+    if (!(lm > 0.001)) return 0.0f;
+    mx /= lm;
+    my /= lm;
+    mz /= lm;
+    const double cosThetaM = mx * nx + my * ny + mz * nz;
+    if (cosThetaM <= 0.0 || mx * ix + my * iy + mz * iz <= 0.0) return 0.0f;
+    auto sin2 = [&](double x, double y, double z) {
+        const double cx = y * nz - z * ny, cy = z * nx - x * nz, cz = x * ny - y * nx;
+        return cx * cx + cy * cy + cz * cz;
+    };
+    const double a = l.roughness, a2 = a * a;
+    const double T = sin2(mx, my, mz) / (cosThetaM * cosThetaM);
+    const double to = sin2(ox, oy, oz) / (cosNO * cosNO), ti = sin2(ix, iy, iz) / (cosNI * cosNI);
+    const double so = sqrt(1.0 + a2 * to), si = sqrt(1.0 + a2 * ti);
+    const double dlogf = 2.0 / a - 4.0 * a / (a2 + T) - a * to / (so * (1.0 + so)) - a * ti / (si * (1.0 + si));
+    return float(dlogf * 2.0 * r);
 }
 
 namespace {
@@ -33,22 +78,33 @@ __device__ __forceinline__ uint32_t tilePixelA(uint32_t tile, uint32_t position,
 }
 
 constexpr uint32_t kLightSlots = 32;  // lights whose credits a thread keeps to itself (more: straight to shared memory)
+constexpr uint32_t kGgxVertex = 0x80000000u;  // a vertex record's material index with this bit: a GGX vertex
+
+// Where a block's partial gradients sit in its shared memory: albedo (3 a material), roughness (1 a material),
+// radiance (3 a light).
+struct Layout {
+    uint32_t materials, lights;
+    __device__ uint32_t albedo(uint32_t m) const { return 3 * m; }
+    __device__ uint32_t roughness(uint32_t m) const { return 3 * materials + m; }
+    __device__ uint32_t radiance(uint32_t j) const { return 4 * materials + 3 * j; }
+};
 
 // A thread's credits. Lights: each contribution, weighted by the loss's derivative for its pixel, over its light's
-// radiance, summed in the thread's own array over all its samples, then into the block's partials once. Albedos: a
-// Lambert vertex's lobe scales everything its path gathers after the vertex (its own light samples and BSDF sample,
-// and all that later vertices add through its throughput), so at the path's end each Lambert vertex k is credited
-// once with (radiance at the end - radiance before k's lobe acted) / its albedo (path replay's suffix sums).
+// radiance, summed in the thread's own array over all its samples, then into the block's partials once. Materials: a
+// vertex's lobe scales everything its path gathers after the vertex acted, so at the path's end each vertex k is
+// credited once with (radiance at the end - radiance before k acted) * scale[k]: scale = 1 / albedo channel by channel
+// for a Lambert vertex (which acts from its light samples on), dlog f/dr at the BSDF sample's direction for a GGX
+// vertex (which acts from its BSDF sample on; its light samples are credited one by one as they land).
 struct Credits {
-    float* partial;  // the block's: 3 a material's albedo, then 3 a light's radiance
-    uint32_t materials, lights;
+    float* partial;
+    Layout at;
     const SceneView& s;
     V3 delta;  // dL/dI of the sample's pixel over its samples
     float* lightSum;  // the thread's light credits (kLightSlots x 3)
-    // The path's vertices by depth: Lambert material (~0u: none) and albedo, and the radiance before its lobe acted.
+    // The path's vertices by depth: material (~0u: none; kGgxVertex set: GGX), the radiance before it acted, the scale.
     uint32_t* material;
-    V3* albedo;
     V3* before;
+    V3* scale;
     uint32_t vertices;
 
     __device__ void light(V3 c, uint32_t j) {
@@ -59,23 +115,32 @@ struct Credits {
             if (L.radiance[k] == 0.0f || w[k] == 0.0f) continue;
             const float v = w[k] / L.radiance[k];
             if (j < kLightSlots) lightSum[3 * j + k] += v;
-            else atomicAdd(partial + 3 * (materials + j) + k, v);
+            else atomicAdd(partial + at.radiance(j) + k, v);
         }
     }
-    __device__ void albedos(V3 total) {
+    __device__ void roughness(uint32_t m, V3 c, float g) {
+        const float v = (delta.x * c.x + delta.y * c.y + delta.z * c.z) * g;
+        if (v != 0.0f && finitef(v)) atomicAdd(partial + at.roughness(m), v);
+    }
+    __device__ void vertexCredits(V3 total) {
         for (uint32_t k = 0; k < vertices; ++k) {
             if (material[k] == ~0u) continue;
             const V3 after = sub(total, before[k]);
-            const V3 a = albedo[k];
-            float* g = partial + 3 * material[k];
-            if (a.x != 0.0f && after.x != 0.0f) atomicAdd(g, delta.x * after.x / a.x);
-            if (a.y != 0.0f && after.y != 0.0f) atomicAdd(g + 1, delta.y * after.y / a.y);
-            if (a.z != 0.0f && after.z != 0.0f) atomicAdd(g + 2, delta.z * after.z / a.z);
+            const V3 f = scale[k];
+            if (material[k] & kGgxVertex) {
+                roughness(material[k] & ~kGgxVertex, after, f.x);
+                continue;
+            }
+            float* g = partial + at.albedo(material[k]);
+            if (f.x != 0.0f && after.x != 0.0f) atomicAdd(g, delta.x * after.x * f.x);
+            if (f.y != 0.0f && after.y != 0.0f) atomicAdd(g + 1, delta.y * after.y * f.y);
+            if (f.z != 0.0f && after.z != 0.0f) atomicAdd(g + 2, delta.z * after.z * f.z);
         }
     }
 };
 
-// The replay's sink: shadow rays traced at once as the plain megakernel's; each unoccluded one credited to its light.
+// The replay's sink: shadow rays traced at once as the plain megakernel's; each unoccluded one credited to its light
+// (and, at a GGX vertex, a light sample to its roughness).
 struct AdjointSink {
     const SceneView& s;
     Credits& cr;
@@ -83,26 +148,60 @@ struct AdjointSink {
     Pending* stack;
     uint32_t& size;
     uint32_t depth;  // the current vertex's depth
-    __device__ void vertex(uint32_t material, const Bsdf& b) {
+    Lobe lobe;       // the current vertex's lobe, when it is GGX
+    V3 wo;
+    uint32_t material;
+    float materialRoughness;
+    bool ggx, sampled;
+
+    __device__ void vertex(uint32_t m, const Bsdf& b, V3 out) {
         const bool lambert = b.count && b.lobe.kind == 0;
-        cr.material[depth] = lambert ? material : ~0u;
-        cr.albedo[depth] = lambert ? b.lobe.albedo : V3{0, 0, 0};
+        ggx = b.count && b.lobe.kind == 1;
+        sampled = false;
         cr.before[depth] = radiance;
         cr.vertices = depth + 1;
+        if (lambert) {
+            const V3 a = b.lobe.albedo;
+            cr.material[depth] = m;
+            cr.scale[depth] = V3{a.x != 0.0f ? 1.0f / a.x : 0.0f, a.y != 0.0f ? 1.0f / a.y : 0.0f, a.z != 0.0f ? 1.0f / a.z : 0.0f};
+        } else if (ggx) {
+            cr.material[depth] = m | kGgxVertex;
+            cr.scale[depth] = V3{0, 0, 0};  // until the BSDF sample is taken
+            lobe = b.lobe;
+            wo = out;
+            material = m;
+            materialRoughness = s.materials[m].roughness;
+        } else {
+            cr.material[depth] = ~0u;
+        }
     }
-    __device__ void shadow(const ShadowReq& q, bool) {
+    // The BSDF sample's direction, the first time the vertex hands on something that came through it.
+    __device__ void bsdfDirection(V3 wi) {
+        if (!ggx || sampled) return;
+        sampled = true;
+        cr.scale[depth] = V3{ggxLogDerivative(lobe, materialRoughness, wo, wi), 0, 0};
+    }
+    __device__ void shadow(const ShadowReq& q, bool bsdf) {
+        if (bsdf) bsdfDirection(q.dir);
         if (!visible(s, q.origin, q.dir, q.near, q.far)) return;
         radiance = add(radiance, q.contribution);
         cr.light(q.contribution, q.light);
+        if (ggx && !bsdf) {
+            cr.roughness(material, q.contribution, ggxLogDerivative(lobe, materialRoughness, wo, q.dir));
+            cr.before[depth] = radiance;  // a GGX vertex's suffix starts after its light samples
+        }
     }
     __device__ void held() {}
     __device__ uint32_t top(uint32_t) const { return size; }
-    __device__ void push(const Pending& p) { stack[size++] = p; }
+    __device__ void push(const Pending& p) {
+        bsdfDirection(p.dir);
+        stack[size++] = p;
+    }
 };
 
 // One sample's replay (the plain megakernel's loop, integrator.cuh's integrate, with the credits).
-__device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, uint32_t index, V3 delta, float* partial, uint32_t materials,
-                                           uint32_t lights, float* lightSum) {
+__device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, uint32_t index, V3 delta, float* partial, Layout at,
+                                           float* lightSum) {
     CameraRay camera;
     if (!cameraRay(s, pixel, index, camera)) return;
     const Identity root{pixel, U64(index), U64(s.config.seed), 0};
@@ -113,8 +212,8 @@ __device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, u
     V3 radiance{0, 0, 0};
     float alpha = 0.0f;
     uint32_t material[kMaxPathVertices];
-    V3 albedo[kMaxPathVertices], before[kMaxPathVertices];
-    Credits cr{partial, materials, lights, s, delta, lightSum, material, albedo, before, 0};
+    V3 before[kMaxPathVertices], scale[kMaxPathVertices];
+    Credits cr{partial, at, s, delta, lightSum, material, before, scale, 0};
     while (top) {
         Pending pv = stack[--top];
         if (pv.depth >= kMaxPathVertices) continue;
@@ -123,7 +222,7 @@ __device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, u
         // The held light (bounce-ray reuse): reached unless the ray met something short of it.
         if (pv.heldLight != ~0u && !(hit.geom != ~0u && hit.t < pv.heldFar)) cr.light(pv.held, pv.heldLight);
         const V3 prior = radiance;
-        afterTrace(s, root, pv, hit, cameraPosition, radiance, alpha);
+        afterTrace<false>(s, root, pv, hit, cameraPosition, radiance, alpha);
         // The light a camera ray sees (afterTrace added it).
         if (pv.depth == 0 && s.config.visible_lights) {
             const bool missed = hit.geom == ~0u;
@@ -132,9 +231,9 @@ __device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, u
         }
         if (hit.geom == ~0u) continue;
         AdjointSink sink{s, cr, radiance, stack, top, pv.depth};
-        if (!shadeVertex(s, root, pixel, index, pv, hit, va, vb, vc, top, radiance, alpha, sink)) return;
+        if (!shadeVertex<false>(s, root, pixel, index, pv, hit, va, vb, vc, top, radiance, alpha, sink)) return;
     }
-    cr.albedos(radiance);
+    cr.vertexCredits(radiance);
 }
 
 }  // namespace
@@ -143,7 +242,8 @@ __device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, u
 __global__ void __launch_bounds__(128) adjointKernel(SceneView s, const x2_chunk* chunks, uint32_t chunkCount, uint32_t count,
                                                      const float* dLossdImage, double* gradients, uint32_t materials, uint32_t lights) {
     extern __shared__ float partial[];
-    const uint32_t params = 3 * (materials + lights);
+    const Layout at{materials, lights};
+    const uint32_t params = 4 * materials + 3 * lights;
     for (uint32_t i = threadIdx.x; i < params; i += blockDim.x) partial[i] = 0.0f;
     float lightSum[3 * kLightSlots];
     for (uint32_t i = 0; i < 3 * kLightSlots; ++i) lightSum[i] = 0.0f;
@@ -166,11 +266,11 @@ __global__ void __launch_bounds__(128) adjointKernel(SceneView s, const x2_chunk
         const float inv = 1.0f / float(ch.count);
         const V3 delta{dLossdImage[3ull * pixel] * inv, dLossdImage[3ull * pixel + 1] * inv, dLossdImage[3ull * pixel + 2] * inv};
         if (delta.x == 0.0f && delta.y == 0.0f && delta.z == 0.0f) continue;
-        adjointSample(s, pixel, ch.first + sample, delta, partial, materials, lights, lightSum);
+        adjointSample(s, pixel, ch.first + sample, delta, partial, at, lightSum);
     }
     for (uint32_t j = 0; j < lights && j < kLightSlots; ++j)
         for (int k = 0; k < 3; ++k)
-            if (lightSum[3 * j + k] != 0.0f) atomicAdd(partial + 3 * (materials + j) + k, lightSum[3 * j + k]);
+            if (lightSum[3 * j + k] != 0.0f) atomicAdd(partial + at.radiance(j) + k, lightSum[3 * j + k]);
     __syncthreads();
     for (uint32_t i = threadIdx.x; i < params; i += blockDim.x)
         if (partial[i] != 0.0f) atomicAdd(gradients + i, double(partial[i]));

@@ -7,9 +7,9 @@ namespace x2 {
 // Fills adjoint.cu's copy of the Sobol direction table (every translation unit with sampling kernels has one).
 cudaError_t uploadSobolAdjoint(const uint32_t directions[17][32]);
 
-// Each sample of the chunks (64 x count items a chunk) replayed, its contributions credited: gradients (FP64, 3 a
-// material's albedo, then 3 a light's radiance) += dL/dI of its pixel / samples a pixel x d(radiance)/d(parameter).
-// Dynamic shared memory: 3 x (materials + lights) floats.
+// Each sample of the chunks (64 x count items a chunk) replayed, its contributions credited: gradients (FP64: 3 a
+// material's albedo, then 1 a material's roughness, then 3 a light's radiance) += dL/dI of its pixel / samples a pixel
+// x d(radiance)/d(parameter). Dynamic shared memory: 4 x materials + 3 x lights floats.
 __global__ void adjointKernel(SceneView s, const x2_chunk* chunks, uint32_t chunkCount, uint32_t count, const float* dLossdImage,
                               double* gradients, uint32_t materials, uint32_t lights);
 

@@ -159,6 +159,8 @@ struct x2_scene {
     uint32_t blocksPerSm = kDefaultBlocksPerSm;  // traversal and shade grids: blocks a SM
     uint32_t traceBlocks = kDefaultTraceBlocks, shadeBlocks = kDefaultShadeBlocks;  // occupancy variants
     uint32_t triLimit = kDefaultTriLimit;  // triangle tests a traversal step
+    uint32_t lobeQueues = 1;               // shade from per-lobe queues (wfSortShade)
+    uint32_t* shadeQ = nullptr;            // the per-lobe queues: 3 x wavePaths entries
     uint32_t batchWindow = 0;              // x2_render_batch: items a window (0: the default)
     uint32_t* hostLast = nullptr;      // pinned
     unsigned long long* claimed = nullptr;
@@ -261,7 +263,8 @@ void freeWave(x2_scene* s) {
     w = WaveState{};
     cudaFree(s->extendQ);
     cudaFree(s->shadowQ);
-    s->extendQ = s->shadowQ = nullptr;
+    cudaFree(s->shadeQ);
+    s->extendQ = s->shadowQ = s->shadeQ = nullptr;
     s->wavePaths = s->waveRecords = 0;
 }
 
@@ -279,7 +282,7 @@ int ensureWave(x2_scene* s, uint32_t paths, uint32_t records) {
               cudaMalloc(&w.ncount, sizeof(uint32_t) * P) == cudaSuccess && cudaMalloc(&w.sray0, sizeof(float4) * R) == cudaSuccess &&
               cudaMalloc(&w.sray1, sizeof(float4) * R) == cudaSuccess && cudaMalloc(&w.scontrib, sizeof(float4) * R) == cudaSuccess &&
               cudaMalloc(&w.svis, R) == cudaSuccess && cudaMalloc(&s->extendQ, sizeof(uint32_t) * P) == cudaSuccess &&
-              cudaMalloc(&s->shadowQ, sizeof(uint32_t) * R) == cudaSuccess;
+              cudaMalloc(&s->shadowQ, sizeof(uint32_t) * R) == cudaSuccess && cudaMalloc(&s->shadeQ, sizeof(uint32_t) * 3 * P) == cudaSuccess;
     if (ok && !s->waveCounters) ok = cudaMalloc(&s->waveCounters, sizeof(uint32_t) * kWaveCounters) == cudaSuccess;
     if (ok && !s->claimed) ok = cudaMalloc(&s->claimed, sizeof(unsigned long long)) == cudaSuccess;
     if (ok && !s->hostLast) ok = cudaMallocHost(&s->hostLast, sizeof(uint32_t) * 4) == cudaSuccess;
@@ -724,7 +727,7 @@ int x2_integrate_device(x2_scene* s, const uint32_t* pairs, uint64_t n, double* 
     cudaStream_t st = s->ctx->stream;
     cudaMemsetAsync(sl.counters, 0, sizeof(Counters), st);
     const int blocks = s->ctx->smCount * s->ctx->renderBlocksPerSm;
-    integratePairs<<<blocks, kRenderBlock, 0, st>>>(viewOf(s), pairs, n, rgba, status, sl.counters);
+    (s->volumeCount ? integratePairsVolumes : integratePairs)<<<blocks, kRenderBlock, 0, st>>>(viewOf(s), pairs, n, rgba, status, sl.counters);
     CUDA_OR(cudaGetLastError(), X2_ECUDA);
     cudaMemcpyAsync(sl.hostCounters, sl.counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
     cudaEventRecord(sl.done, st);
@@ -883,7 +886,7 @@ int x2_launch(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     a.counters = sl->counters;
     const int blocks = s->ctx->smCount * s->ctx->renderBlocksPerSm;
     cudaEventRecord(sl->begin, st);
-    renderChunks<<<blocks, kRenderBlock, 0, st>>>(a);
+    (s->volumeCount ? renderChunksVolumes : renderChunks)<<<blocks, kRenderBlock, 0, st>>>(a);
     CUDA_OR(cudaGetLastError(), X2_ECUDA);
     cudaEventRecord(sl->end, st);
     cudaMemcpyAsync(sl->hostCounters, sl->counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
@@ -961,12 +964,13 @@ void x2_wavefront_shape_defaults(x2_wavefront_shape* shape) {
     shape->trace_blocks = kDefaultTraceBlocks;
     shape->shade_blocks = kDefaultShadeBlocks;
     shape->tri_limit = kDefaultTriLimit;
+    shape->lobe_queues = 1;
 }
 
 int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     if (!s || !shape || shape->refill < 1 || shape->refill > 32 || shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 ||
-        shape->trace_blocks > 32 || shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32) {
-        setError("refill is 1..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32");
+        shape->trace_blocks > 32 || shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32 || shape->lobe_queues > 1) {
+        setError("refill is 1..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32, lobe_queues 0 or 1");
         return X2_EINVAL;
     }
     s->reservePaths = shape->paths;
@@ -976,6 +980,7 @@ int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     s->shadeBlocks = shape->shade_blocks;
     s->triLimit = shape->tri_limit;
     s->batchWindow = shape->batch_window;
+    s->lobeQueues = shape->lobe_queues;
     return X2_OK;
 }
 
@@ -1036,6 +1041,8 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     a.shadowCount = s->waveCounters + 2;
     a.extendNext = s->waveCounters + 3;
     a.shadowNext = s->waveCounters + 4;
+    a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
+    a.shadeCount = s->waveCounters + 5;
     a.refill = s->refill;
     a.triLimit = s->triLimit;
     a.out = s->out;
@@ -1047,7 +1054,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     a.chunkCount = count;
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
-    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks);
+    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0);
     const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     if (s->waveTiming) {
         // Diagnostic form: no graph; events around every kernel, the iteration's times added once it is done.
@@ -1064,6 +1071,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
             cudaEventRecord(ev[1], st);
             wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
             cudaEventRecord(ev[2], st);
+            if (a.shadeQ) wfSortShade<<<gridWork, kWaveBlock, 0, st>>>(a);
             wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
             cudaEventRecord(ev[3], st);
             wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
@@ -1117,6 +1125,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
         wfResetQueues<<<1, 32, 0, st>>>(a);
         wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
         wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
+        if (a.shadeQ) wfSortShade<<<gridWork, kWaveBlock, 0, st>>>(a);
         wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
         wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
     }
@@ -1197,16 +1206,19 @@ int x2_items_download(x2_scene* s, float* rgba, uint8_t* status, uint64_t n) {
 
 // The differentiable parameters: each material's diffuse colour (its Lambert albedo) and each light's radiance, set in
 // place on the device (the BVH and everything else stay). Host arrays, 3 floats each; null leaves a set as it is.
-int x2_scene_set_params(x2_scene* s, const float* albedo, const float* radiance) {
+int x2_scene_set_params(x2_scene* s, const float* albedo, const float* roughness, const float* radiance) {
     if (!s) return X2_EINVAL;
     if (int rc = x2_wait(s, 600000, nullptr)) return rc;
     cudaStream_t st = s->ctx->stream;
-    if (albedo) {
+    if (albedo || roughness) {
         std::vector<MaterialRec> mats(s->materialCount);
         CUDA_OR(cudaMemcpyAsync(mats.data(), s->materials, sizeof(MaterialRec) * mats.size(), cudaMemcpyDeviceToHost, st), X2_ECUDA);
         CUDA_OR(cudaStreamSynchronize(st), X2_ECUDA);
-        for (uint32_t m = 0; m < s->materialCount; ++m)
-            for (int k = 0; k < 3; ++k) mats[m].diffuse[k] = albedo[3 * m + k];
+        for (uint32_t m = 0; m < s->materialCount; ++m) {
+            if (albedo)
+                for (int k = 0; k < 3; ++k) mats[m].diffuse[k] = albedo[3 * m + k];
+            if (roughness) mats[m].roughness = roughness[m];
+        }
         CUDA_OR(cudaMemcpyAsync(s->materials, mats.data(), sizeof(MaterialRec) * mats.size(), cudaMemcpyHostToDevice, st), X2_ECUDA);
         CUDA_OR(cudaStreamSynchronize(st), X2_ECUDA);
     }
@@ -1223,9 +1235,11 @@ int x2_scene_set_params(x2_scene* s, const float* albedo, const float* radiance)
 }
 
 // The adjoint of a frame's samples [first, first + count) of every pixel: gradients of a loss with respect to each
-// material's albedo and each light's radiance, given the loss's derivative with respect to the image (device, 3
-// floats a pixel, the image being the film's mean). Device outputs (FP64), added to.
-int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad, double* d_radiance_grad) {
+// material's albedo and roughness and each light's radiance, given the loss's derivative with respect to the image
+// (device, 3 floats a pixel, the image being the film's mean). Device outputs (FP64), added to; a null roughness
+// output skips that set.
+int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad, double* d_roughness_grad,
+               double* d_radiance_grad) {
     if (!s || !s->configured || !d_dloss_dimage || !d_albedo_grad || !d_radiance_grad || count == 0) {
         setError("x2_adjoint: configured scene, device arrays and a sample count");
         return X2_EINVAL;
@@ -1234,9 +1248,9 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
         setError("x2_adjoint: no volumes, max_depth < 128, bsdf_samples = 1");
         return X2_EINVAL;
     }
-    const uint32_t params = 3 * (s->materialCount + s->lightCount);
+    const uint32_t params = 4 * s->materialCount + 3 * s->lightCount;
     if (size_t(params) * sizeof(float) > 96 * 1024) {
-        setError("x2_adjoint: at most %u materials and lights", 96 * 1024 / 12);
+        setError("x2_adjoint: 4 x materials + 3 x lights must be at most %u", 96 * 1024 / 4);
         return X2_EINVAL;
     }
     if (int rc = checkDevice(s->ctx)) return rc;
@@ -1262,9 +1276,10 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     adjointKernel<<<s->ctx->smCount * 8, 128, shared, st>>>(v, d, tiles, count, d_dloss_dimage, grads, s->materialCount, s->lightCount);
     int rc = cudaGetLastError() == cudaSuccess ? X2_OK : X2_ECUDA;
     if (!rc) {
-        // Added to the caller's arrays: albedo then radiance.
+        // Added to the caller's arrays: albedo, roughness, radiance.
         addInto<<<(params + 255) / 256, 256, 0, st>>>(d_albedo_grad, grads, 3 * s->materialCount);
-        addInto<<<(params + 255) / 256, 256, 0, st>>>(d_radiance_grad, grads + 3 * s->materialCount, 3 * s->lightCount);
+        if (d_roughness_grad) addInto<<<(params + 255) / 256, 256, 0, st>>>(d_roughness_grad, grads + 3 * s->materialCount, s->materialCount);
+        addInto<<<(params + 255) / 256, 256, 0, st>>>(d_radiance_grad, grads + 4 * s->materialCount, 3 * s->lightCount);
         rc = x2_synchronize(s->ctx, 600000);
     } else {
         setError("x2_adjoint: launch failed");
@@ -1318,7 +1333,8 @@ int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefron
                           {&x2_wavefront_shape::tri_limit, {1, 2, 4}},
                           {&x2_wavefront_shape::shade_blocks, {0, 3, 4}},
                           {&x2_wavefront_shape::trace_blocks, {0, 9}},
-                          {&x2_wavefront_shape::blocks_per_sm, {8, 16, 32}}};
+                          {&x2_wavefront_shape::blocks_per_sm, {8, 16, 32}},
+                          {&x2_wavefront_shape::lobe_queues, {0, 1}}};
     for (const Knob& k : knobs) {
         x2_wavefront_shape keep = cur;
         for (uint32_t v : k.values) {
@@ -1424,7 +1440,9 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
     int rc = X2_OK;
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = ctx->smCount * int(s0->blocksPerSm);
-    const WaveKernels wk = waveKernelsBatch();
+    bool anyVolumes = false;
+    for (const SceneView& v : views) anyVolumes = anyVolumes || v.config.volume_count != 0;
+    const WaveKernels wk = waveKernelsBatch(anyVolumes);
     std::vector<unsigned long long> items;
     uint32_t iterations = 0;
     if (cudaMalloc(&dViews, sizeof(SceneView) * n) != cudaSuccess || cudaMalloc(&dFilms, sizeof(BatchFilm) * n) != cudaSuccess ||
@@ -1470,6 +1488,8 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
         a.shadowCount = s0->waveCounters + 2;
         a.extendNext = s0->waveCounters + 3;
         a.shadowNext = s0->waveCounters + 4;
+        a.shadeQ = s0->lobeQueues ? s0->shadeQ : nullptr;
+        a.shadeCount = s0->waveCounters + 5;
         a.refill = s0->refill;
         a.triLimit = s0->triLimit;
         a.out = s0->out;
@@ -1492,6 +1512,7 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
             wfResetQueues<<<1, 32, 0, st>>>(a);
             wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
             wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
+            if (a.shadeQ) wfSortShadeBatch<<<gridWork, kWaveBlock, 0, st>>>(a);
             wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
             wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
         }

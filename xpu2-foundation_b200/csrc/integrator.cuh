@@ -137,6 +137,9 @@ __device__ __forceinline__ void cameraPending(const CameraRay& camera, Pending& 
 // then, on a camera ray, the lights the camera sees (async_integrator.h:2095-2106, :2172-2185).
 // With volumes, the volumes the ray passes on its way (async_integrator.h:2107-2118): their light, the throughput
 // through them (pv's T and volume depth change) and, for a camera ray that hits nothing, their opacity as its alpha.
+// kVolumes false compiles the volume code out (the kernels for scenes without volumes: the march's state would
+// otherwise take registers and stack from every surface vertex); a scene with volumes takes the kVolumes form.
+template <bool kVolumes = true>
 __device__ __forceinline__ void afterTrace(const SceneView& s, const Identity& root, Pending& pv, const Hit& hit, V3 cameraPosition,
                                            V3& radiance, float& alpha) {
     if (pv.heldLight != ~0u) {
@@ -144,7 +147,7 @@ __device__ __forceinline__ void afterTrace(const SceneView& s, const Identity& r
         if (kept > 0.0f) radiance = add(radiance, kept < 1.0f ? mul(pv.held, kept) : pv.held);
     }
     V3 volumeAlphaT{1, 1, 1};
-    if (s.config.volume_count) {
+    if (kVolumes && s.config.volume_count) {
         const V3 volumeLight = volumeRadiance(s, root, pv, pv.origin, pv.dir, pv.nearT, hit.geom == ~0u ? pv.farT : hit.t, volumeAlphaT);
         radiance = add(radiance, volumeLight);
     }
@@ -169,12 +172,13 @@ struct ShadowReq {
 // One hit (async_integrator.h:2222-3031 for the admitted materials): shading state, emission, a light sample of
 // every light that can light the hit, the lobe's BSDF sample, and its child. `top` is the pending stack's size after
 // this vertex was popped. The sink takes shadow rays (shadow(req, bsdf)) and the child (push(child) -> bool).
-// Returns false when the hit's shading state cannot be made (SampleStatus::Error).
-template <class Sink>
+// Returns false when the hit's shading state cannot be made (SampleStatus::Error). kVolumes as afterTrace's.
+template <bool kVolumes = true, class Sink>
 __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& root, uint32_t pixel, uint32_t index, const Pending& pv,
                                             const Hit& hit, V3 va, V3 vb, V3 vc, uint32_t top, V3& radiance, float& alpha, Sink& sink) {
     const x2_config& c = s.config;
     const uint32_t policy = c.sampling;
+    const bool volumes = kVolumes && c.volume_count;
     State st;
     if (!hitState(va, vb, vc, hit.u, hit.v, hit.point, pv.dir, st)) return false;
     Bsdf bsdf;
@@ -182,7 +186,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
     shadeMaterial(s.materials[material], st, bsdf);
     if (pv.depth == 0) alpha += 1.0f * (1.0f - (0.0f + 0.0f + 0.0f) / 3.0f);
     radiance = add(radiance, mulv(pv.T, bsdf.emission));
-    sink.vertex(material, bsdf);  // the vertex, its emission added: what comes after passes its lobe
+    sink.vertex(material, bsdf, st.wo);  // the vertex, its emission added: what comes after passes its lobe
     if (bsdf.count == 0) return true;
 
     uint32_t indirectFlags = 0;
@@ -268,7 +272,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
             q.dir = wi;
             q.near = fmaxf(0.0f, 0.0f);
             q.far = fmaxf((lh.distance - 0.0f) * kHitEpsilonEnd, 2.0f * q.near);
-            if (c.volume_count) {
+            if (volumes) {
                 // The volumes on the shadow ray's way (transmittance(), async_integrator.h:2722-2731); it matters only
                 // when nothing occludes the ray, and its stream is its own, so it is taken here.
                 Identity tid = lid;
@@ -352,7 +356,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
             shadowNear = fmaxf(shadowNear, 0.0f);
             shadowFar = fmaxf((lightDistance - 0.0f) * kHitEpsilonEnd, 2.0f * shadowNear);
             held = bounces && thinning >= 1.0f && topNow + kPendingReserve < kMaxPending && lobeMask && (c.shadow_reuse & lobeMask) == lobeMask &&
-                   !c.volume_count && shadowNear == start;
+                   !volumes && shadowNear == start;
             if (held) {
                 sink.held();
             } else {
@@ -363,7 +367,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
                 q.far = shadowFar;
                 q.contribution = direct;
                 q.light = lightIndex;
-                if (c.volume_count) {
+                if (volumes) {
                     Identity tid = bid;
                     tid.branch = childBranch(sampleBranch, 0xfffb, 0);
                     Stream vs(tid, pv.depth, 0);
@@ -425,12 +429,13 @@ struct PlainSink {
         if (visible(s, q.origin, q.dir, q.near, q.far)) radiance = add(radiance, q.contribution);
     }
     __device__ void held() { ++out.held; }
-    __device__ void vertex(uint32_t, const Bsdf&) {}
+    __device__ void vertex(uint32_t, const Bsdf&, V3) {}
     __device__ uint32_t top(uint32_t) const { return size; }
     __device__ void push(const Pending& p) { stack[size++] = p; }
 };
 
 // integratePaths for one sample (pixel, index): the plain megakernel's whole path loop on one thread.
+template <bool kVolumes>
 static __device__ __noinline__ void integrate(const SceneView& s, uint32_t pixel, uint32_t index, SampleOut& out) {
     const x2_config& c = s.config;
     out.rgb[0] = out.rgb[1] = out.rgb[2] = 0.0f;
@@ -454,9 +459,9 @@ static __device__ __noinline__ void integrate(const SceneView& s, uint32_t pixel
         V3 va, vb, vc;
         const Hit hit = trace(s, pv.origin, pv.dir, pv.nearT, pv.farT, va, vb, vc);
         ++out.trace;
-        afterTrace(s, root, pv, hit, cameraPosition, radiance, alpha);
+        afterTrace<kVolumes>(s, root, pv, hit, cameraPosition, radiance, alpha);
         if (hit.geom == ~0u) continue;
-        if (!shadeVertex(s, root, pixel, index, pv, hit, va, vb, vc, top, radiance, alpha, sink)) {
+        if (!shadeVertex<kVolumes>(s, root, pixel, index, pv, hit, va, vb, vc, top, radiance, alpha, sink)) {
             out.status = X2_ERROR;
             return;
         }

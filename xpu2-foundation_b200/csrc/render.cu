@@ -47,7 +47,8 @@ __device__ __forceinline__ void addCounters(Counters* dst, unsigned long long tr
 
 }  // namespace
 
-__global__ void __launch_bounds__(kRenderBlock) renderChunks(RenderArgs a) {
+template <bool kVolumes>
+__device__ __forceinline__ void renderChunksBody(const RenderArgs& a) {
     const unsigned full = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t width = a.scene.config.width, height = a.scene.config.height;
@@ -74,7 +75,7 @@ __global__ void __launch_bounds__(kRenderBlock) renderChunks(RenderArgs a) {
         o.status = X2_SKIP;
         o.rgb[0] = o.rgb[1] = o.rgb[2] = o.alpha = 0.0f;
         if (pixel != ~0u) {
-            integrate(a.scene, pixel, index, o);
+            integrate<kVolumes>(a.scene, pixel, index, o);
             trace += o.trace;
             nee += o.nee;
             bsdf += o.bsdf;
@@ -134,10 +135,13 @@ __global__ void __launch_bounds__(kRenderBlock) renderChunks(RenderArgs a) {
     }
     addCounters(a.counters, trace, nee, bsdf, held, samples, errors);
 }
+__global__ void __launch_bounds__(kRenderBlock) renderChunks(RenderArgs a) { renderChunksBody<false>(a); }
+__global__ void __launch_bounds__(kRenderBlock) renderChunksVolumes(RenderArgs a) { renderChunksBody<true>(a); }
 
 // The per-sample API: integrate() for n (pixel, index) pairs.
-__global__ void __launch_bounds__(kRenderBlock) integratePairs(SceneView s, const uint32_t* __restrict__ pairs, unsigned long long n,
-                                                               double* __restrict__ rgba, uint32_t* __restrict__ status, Counters* counters) {
+template <bool kVolumes>
+__device__ __forceinline__ void integratePairsBody(const SceneView& s, const uint32_t* __restrict__ pairs, unsigned long long n,
+                                                   double* __restrict__ rgba, uint32_t* __restrict__ status, Counters* counters) {
     unsigned long long trace = 0, nee = 0, bsdf = 0, held = 0, samples = 0, errors = 0;
     const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
     const unsigned long long first = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -147,7 +151,7 @@ __global__ void __launch_bounds__(kRenderBlock) integratePairs(SceneView s, cons
         const unsigned long long i = first + r * stride;
         if (i >= n) continue;
         SampleOut o;
-        integrate(s, pairs[2 * i], pairs[2 * i + 1], o);
+        integrate<kVolumes>(s, pairs[2 * i], pairs[2 * i + 1], o);
         rgba[4 * i] = double(o.rgb[0]);
         rgba[4 * i + 1] = double(o.rgb[1]);
         rgba[4 * i + 2] = double(o.rgb[2]);
@@ -161,6 +165,15 @@ __global__ void __launch_bounds__(kRenderBlock) integratePairs(SceneView s, cons
         else errors += o.status == X2_SKIP ? 0 : 1;
     }
     addCounters(counters, trace, nee, bsdf, held, samples, errors);
+}
+__global__ void __launch_bounds__(kRenderBlock) integratePairs(SceneView s, const uint32_t* __restrict__ pairs, unsigned long long n,
+                                                               double* __restrict__ rgba, uint32_t* __restrict__ status, Counters* counters) {
+    integratePairsBody<false>(s, pairs, n, rgba, status, counters);
+}
+__global__ void __launch_bounds__(kRenderBlock) integratePairsVolumes(SceneView s, const uint32_t* __restrict__ pairs, unsigned long long n,
+                                                                      double* __restrict__ rgba, uint32_t* __restrict__ status,
+                                                                      Counters* counters) {
+    integratePairsBody<true>(s, pairs, n, rgba, status, counters);
 }
 
 // Closest hit and occlusion for n rays (8 floats each: origin, direction, near, far).

@@ -322,6 +322,12 @@ struct Bsdf {
     Lobe lobe;
 };
 __device__ __forceinline__ float saturate(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+// The lobe shadeMaterial makes for a material: 1 a GGX lobe, 0 a Lambert lobe, 2 none (the wavefront's per-lobe
+// queues sort paths by it before shading).
+__device__ __forceinline__ uint32_t lobeClass(const MaterialRec& m) {
+    if (m.kind == X2_MAT_GGX && !isBlack(V3{saturate(m.specular[0]), saturate(m.specular[1]), saturate(m.specular[2])})) return 1;
+    return isBlack(V3{m.diffuse[0], m.diffuse[1], m.diffuse[2]}) ? 2 : 0;
+}
 // shadeUsdPreviewSurface with useSpecularWorkflow = 1 (shade_material.h:338-383).
 __device__ __forceinline__ void shadeMaterial(const MaterialRec& m, const State& st, Bsdf& b) {
     b.count = 0;

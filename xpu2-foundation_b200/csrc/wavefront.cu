@@ -7,7 +7,8 @@
 //           claim a new sample for an empty slot (regeneration: a camera ray), and append every slot with a ray to
 //           trace to the extend queue (warp-aggregated atomics);
 //   extend  closest hit of every queued ray (traverse.cuh);
-//   shade   each queued path's vertex (integrator.cuh shadeVertex): its shadow rays go to fixed per-path record slots
+//   sort    the extended paths into per-lobe queues by their hit's material (GGX, Lambert, none or missed);
+//   shade   each queued path's vertex, the queues in that order (integrator.cuh shadeVertex): its shadow rays go to fixed per-path record slots
 //           and, by one warp-aggregated reservation a warp, to the shadow queue; its child becomes the slot's ray;
 //   shadow  any hit of every queued shadow ray, a visibility flag each.
 // Iterations are captured once as a CUDA graph and replayed until every item is done. The per-item output (rgb,
@@ -310,7 +311,7 @@ struct WaveSink {
         else ++nNee;
     }
     __device__ void held() { ++nHeld; }
-    __device__ void vertex(uint32_t, const Bsdf&) {}
+    __device__ void vertex(uint32_t, const Bsdf&, V3) {}
     __device__ uint32_t top(uint32_t t) const { return t; }
     __device__ void push(const Pending& c) {
         child = c;
@@ -318,10 +319,59 @@ struct WaveSink {
     }
 };
 
+// ---- sort: per-lobe shade queues ----
+// Each extended path goes to the queue of the lobe its hit's material makes (shading.cuh lobeClass: 0 Lambert, 1 GGX,
+// 2 none) or, when its ray hit nothing, to queue 2; queue order: GGX (0), Lambert (1), none or missed (2). One
+// warp-aggregated atomic a queue a warp round.
 template <bool kBatch>
+__device__ __forceinline__ void sortBody(const WaveArgs& a) {
+    const WaveState& w = a.w;
+    const uint32_t n = *a.extendCount;
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t queue = 3, p = 0;
+        if (i < n) {
+            p = a.extendQ[i];
+            queue = 2;
+            const uint2 hr = w.hit[p];
+            if (hr.x != ~0u) {
+                const SceneView& s = sceneOf<kBatch>(a, requestOf(w, p));
+                const uint32_t tri = __float_as_uint(__ldg(reinterpret_cast<const float*>(s.bvh.tris + hr.x) + 3));
+                const uint32_t c = lobeClass(s.materials[__ldg(s.meshMaterial + __ldg(s.triMesh + tri))]);
+                queue = c == 1 ? 0u : c == 0 ? 1u : 2u;
+            }
+        }
+#pragma unroll
+        for (uint32_t q = 0; q < 3; ++q) {
+            const unsigned mask = __ballot_sync(full, queue == q);
+            if (!mask) continue;
+            const uint32_t leader = __ffs(mask) - 1;
+            uint32_t at = 0;
+            if (lane == leader) at = atomicAdd(a.shadeCount + q, uint32_t(__popc(mask)));
+            at = __shfl_sync(full, at, leader);
+            if (queue == q) a.shadeQ[size_t(q) * a.paths + at + __popc(mask & ((1u << lane) - 1u))] = p;
+        }
+    }
+}
+__global__ void __launch_bounds__(kWaveBlock) wfSortShade(WaveArgs a) { sortBody<false>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfSortShadeBatch(WaveArgs a) { sortBody<true>(a); }
+
+// The i-th path shade takes: from the per-lobe queues in their order when they are on, else the extend queue's.
+__device__ __forceinline__ uint32_t shadeEntry(const WaveArgs& a, uint32_t i, uint32_t c0, uint32_t c1) {
+    if (!a.shadeQ) return a.extendQ[i];
+    if (i < c0) return a.shadeQ[i];
+    if (i < c0 + c1) return a.shadeQ[a.paths + (i - c0)];
+    return a.shadeQ[2ull * a.paths + (i - c0 - c1)];
+}
+
+template <bool kBatch, bool kVolumes>
 __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
     const WaveState& w = a.w;
     const uint32_t n = *a.extendCount;
+    const uint32_t c0 = a.shadeQ ? a.shadeCount[0] : 0u, c1 = a.shadeQ ? a.shadeCount[1] : 0u;
     unsigned long long nee = 0, bsdf = 0, held = 0;
     // Every lane of a warp runs the same rounds: the shadow queue's reservation is a warp-wide scan.
     const uint32_t stride = gridDim.x * blockDim.x;
@@ -329,7 +379,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
         const uint32_t i = base + threadIdx.x;
         uint32_t records = 0, p = 0;
         if (i < n) {
-            p = a.extendQ[i];
+            p = shadeEntry(a, i, c0, c1);
             Pending pv;
             loadPending(w, p, pv);
             const uint4 m = w.meta[p];
@@ -361,11 +411,11 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
             // The camera's position (a pinhole: every camera ray's origin).
             const V3 cameraPosition = add(mvector(s.camera.camera_to_render, V3{0, 0, 0}),
                                           V3{s.camera.camera_to_render[3][0], s.camera.camera_to_render[3][1], s.camera.camera_to_render[3][2]});
-            afterTrace(s, root, pv, hit, cameraPosition, radiance, alpha);
+            afterTrace<kVolumes>(s, root, pv, hit, cameraPosition, radiance, alpha);
             uint32_t next = kDone;
             if (hit.geom != ~0u) {
                 WaveSink sink{w, p, 0, a.recordsPerPath, false, Pending{}, 0, 0, 0};
-                if (!shadeVertex(s, root, pixel, index, pv, hit, va, vb, vc, 0u, radiance, alpha, sink)) {
+                if (!shadeVertex<kVolumes>(s, root, pixel, index, pv, hit, va, vb, vc, 0u, radiance, alpha, sink)) {
                     next = kError;
                 } else {
                     records = sink.n;
@@ -399,9 +449,12 @@ __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
 }
 
 // The kernels, each in a few occupancy variants (blocks of kWaveBlock threads a SM that the register allocation must
-// allow), chosen at launch (x2_wavefront_tune); batches in the compiler's allocation.
+// allow), chosen at launch (x2_wavefront_tune); batches in the compiler's allocation. Shade comes in a form for
+// scenes without volumes (the volume code compiled out) and one for scenes with them.
 __global__ void __launch_bounds__(kWaveBlock) wfExtend(WaveArgs a) { extendBody<false>(a); }
-__global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) { shadeBody<false>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) { shadeBody<false, false>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShadeVolumes(WaveArgs a) { shadeBody<false, true>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShadeBatchVolumes(WaveArgs a) { shadeBody<true, true>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) { shadowBody<false>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfExtendBatch(WaveArgs a) { extendBody<true>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadowBatch(WaveArgs a) { shadowBody<true>(a); }
@@ -411,28 +464,28 @@ __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfExtendOcc(WaveArgs a
 }
 template <int kMinBlocks, bool kBatch>
 __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadeOcc(WaveArgs a) {
-    shadeBody<kBatch>(a);
+    shadeBody<kBatch, false>(a);
 }
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadowOcc(WaveArgs a) {
     shadowBody<false>(a);
 }
 
-WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks) {
+WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes) {
     WaveKernels k;
     k.logic = wfLogic;
     k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : wfExtend;
     k.shadow = traceBlocks >= 10 ? wfShadowOcc<10> : traceBlocks >= 9 ? wfShadowOcc<9> : wfShadow;
-    k.shade = shadeBlocks >= 4 ? wfShadeOcc<4, false> : shadeBlocks >= 3 ? wfShadeOcc<3, false> : wfShade;
+    k.shade = volumes ? wfShadeVolumes : shadeBlocks >= 4 ? wfShadeOcc<4, false> : shadeBlocks >= 3 ? wfShadeOcc<3, false> : wfShade;
     return k;
 }
 
-WaveKernels waveKernelsBatch() {
+WaveKernels waveKernelsBatch(bool volumes) {
     WaveKernels k;
     k.logic = wfLogicBatch;
     k.extend = wfExtendBatch;
     k.shadow = wfShadowBatch;
-    k.shade = wfShadeOcc<4, true>;
+    k.shade = volumes ? wfShadeBatchVolumes : wfShadeOcc<4, true>;
     return k;
 }
 
@@ -445,6 +498,7 @@ __global__ void wfResetQueues(WaveArgs a) {
         *a.shadowCount = 0;
         *a.extendNext = 0;
         *a.shadowNext = 0;
+        if (a.shadeQ) a.shadeCount[0] = a.shadeCount[1] = a.shadeCount[2] = 0;
     }
 }
 

@@ -43,6 +43,12 @@ struct WaveArgs {
     uint32_t* shadowCount;
     uint32_t* extendNext;  // the extend and shadow kernels' fetch counters over their queues
     uint32_t* shadowNext;
+    // Per-lobe shade queues (null: shade walks the extend queue as it is): after extend, wfSortShade sorts the
+    // extended paths by the lobe their hit's material makes (GGX, Lambert, none or missed) into three queues of
+    // `paths` entries each (shadeQ + k * paths) with counts shadeCount[0..2]; shade walks them in that order, so a
+    // warp's lanes run one lobe's code.
+    uint32_t* shadeQ;
+    uint32_t* shadeCount;
     uint32_t refill;       // a warp fetches new rays once this many of its lanes are idle (1..32)
     uint32_t triLimit;     // triangle tests a lane makes a traversal step
     float4* out;          // per item: rgb, alpha
@@ -68,15 +74,18 @@ cudaError_t uploadSobolWavefront(const uint32_t directions[17][32]);
 
 // The logic, extend, shade and shadow kernels for an occupancy: at least `traceBlocks` / `shadeBlocks` blocks a SM
 // (10, 9 or 0 for the traversals; 4, 3 or 0 for shade; 0 leaves the register allocation to the compiler); and the
-// batch forms, which take each path's scene from WaveArgs::scenes.
+// batch forms, which take each path's scene from WaveArgs::scenes. `volumes`: a scene (or any request) has volumes,
+// which takes the shade kernel with the volume code (in the compiler's allocation).
 struct WaveKernels {
     void (*logic)(WaveArgs);
     void (*extend)(WaveArgs);
     void (*shade)(WaveArgs);
     void (*shadow)(WaveArgs);
 };
-WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks);
-WaveKernels waveKernelsBatch();
+WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes);
+WaveKernels waveKernelsBatch(bool volumes);
+__global__ void wfSortShade(WaveArgs a);
+__global__ void wfSortShadeBatch(WaveArgs a);
 __global__ void wfResetQueues(WaveArgs a);
 __global__ void wfFilmReduce(WaveArgs a, uint32_t chunkCount, double* sums, double* odd, uint32_t* counts);
 __global__ void wfFilmReduceBatch(WaveArgs a, const BatchFilm* films);

@@ -109,8 +109,8 @@ class Request(C.Structure):
 
 
 class WavefrontShape(C.Structure):
-    FIELDS = ("paths", "refill", "blocks_per_sm", "trace_blocks", "shade_blocks", "tri_limit", "batch_window")
-    _fields_ = [(f, C.c_uint32) for f in FIELDS] + [("reserved", C.c_uint32 * 1)]
+    FIELDS = ("paths", "refill", "blocks_per_sm", "trace_blocks", "shade_blocks", "tri_limit", "batch_window", "lobe_queues")
+    _fields_ = [(f, C.c_uint32) for f in FIELDS]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k in self.FIELDS}
@@ -159,7 +159,7 @@ def library():
         "x2_launch_wavefront_static": ([vp, vp, u32, u32, vp, vp, C.POINTER(u64)], i32),
         "x2_render_batch": ([vp, C.POINTER(Request), u32, C.POINTER(Completion)], i32),
         "x2_wavefront_autotune": ([vp, u32, u32, C.POINTER(WavefrontShape), C.POINTER(C.c_float)], i32),
-        "x2_scene_set_params": ([vp, vp, vp], i32), "x2_adjoint": ([vp, u32, u32, vp, vp, vp], i32),
+        "x2_scene_set_params": ([vp, vp, vp, vp], i32), "x2_adjoint": ([vp, u32, u32, vp, vp, vp, vp], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
@@ -400,17 +400,19 @@ class Scene:
         _check(library().x2_wavefront_tune(self._h, C.byref(s)))
         return s.as_dict()
 
-    def set_params(self, albedo=None, radiance=None):
-        """The differentiable parameters (x2_scene_set_params): each material's diffuse colour (n x 3) and each light's
-        radiance (n x 3), or None to leave a set."""
+    def set_params(self, albedo=None, radiance=None, roughness=None):
+        """The differentiable parameters (x2_scene_set_params): each material's diffuse colour (n x 3), each light's
+        radiance (n x 3) and each material's roughness (n), or None to leave a set."""
         a = None if albedo is None else np.ascontiguousarray(albedo, np.float32)
         r = None if radiance is None else np.ascontiguousarray(radiance, np.float32)
-        _check(library().x2_scene_set_params(self._h, _ptr(a), _ptr(r)))
+        g = None if roughness is None else np.ascontiguousarray(roughness, np.float32)
+        _check(library().x2_scene_set_params(self._h, _ptr(a), _ptr(g), _ptr(r)))
 
-    def adjoint(self, first, count, d_dloss_dimage, d_albedo_grad, d_radiance_grad):
-        """x2_adjoint on device pointers (ints): adds dL/dalbedo and dL/dradiance for samples [first, first + count) of
-        every pixel, given dL/dimage (3 floats a pixel)."""
-        _check(library().x2_adjoint(self._h, first, count, C.c_void_p(d_dloss_dimage), C.c_void_p(d_albedo_grad), C.c_void_p(d_radiance_grad)))
+    def adjoint(self, first, count, d_dloss_dimage, d_albedo_grad, d_radiance_grad, d_roughness_grad=None):
+        """x2_adjoint on device pointers (ints): adds dL/dalbedo, dL/dradiance and (when given) dL/droughness for
+        samples [first, first + count) of every pixel, given dL/dimage (3 floats a pixel)."""
+        _check(library().x2_adjoint(self._h, first, count, C.c_void_p(d_dloss_dimage), C.c_void_p(d_albedo_grad),
+                                    C.c_void_p(d_roughness_grad), C.c_void_p(d_radiance_grad)))
 
     def wavefront_autotune(self, tiles=0, spp=None):
         """Time the wavefront launch shapes on `tiles` evenly spaced tiles (0: all) at `spp` samples (default: the
