@@ -267,10 +267,15 @@ int x2_scene_set_params(x2_scene* scene, const float* albedo, const float* rough
  * floats a pixel), adds dL/dalbedo (device, 3 doubles a material), dL/droughness (device, 1 double a material; null:
  * not wanted) and dL/dradiance (device, 3 doubles a light). Each sample's path is replayed from its identity (nothing
  * of a primal pass is stored) and each contribution credited to the light it reached and the Lambert and GGX vertices
- * it passed, the sampling decisions (directions, pdfs, MIS weights, roulette) held fixed. Requires no volumes,
+ * it passed, the sampling decisions (directions, pdfs, MIS weights, roulette) held fixed. The replay runs in the
+ * wavefront form (x2_wavefront_reserve paths in flight, x2_wavefront_tune's shape). Requires no volumes,
  * max_depth < 128, bsdf_samples = 1, 4 x materials + 3 x lights <= 24576. Waits. */
 int x2_adjoint(x2_scene* scene, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad,
                double* d_roughness_grad, double* d_radiance_grad);
+/* x2_adjoint with its replay in the plain megakernel's form (one thread a sample) instead of the wavefront form: the
+ * same estimator and results (up to the FP32 partial sums' order). */
+int x2_adjoint_plain(x2_scene* scene, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad,
+                     double* d_roughness_grad, double* d_radiance_grad);
 /* The last timed wavefront launch's queue sizes: for each iteration, rays extended then shadow rays (2 a
  * iteration, at most max values). */
 int x2_wavefront_queues(x2_scene* scene, uint32_t* sizes, uint32_t max);

@@ -206,3 +206,32 @@ def test_adjoint_matches_fp64_cpu_adjoint(field):
         worst = max(worst, abs(g - c) / bar)
         assert abs(g - c) <= bar, (kind, idx, g, c, m)
     print(f"64 parameters ({illConditioned} ill-conditioned): worst difference {worst:.2f} of its bar")
+
+
+def test_wavefront_adjoint_matches_plain_replay(field):
+    """x2_adjoint (the replay in the wavefront form, credits in the logic and shade kernels) against
+    x2_adjoint_plain (one thread a sample): the same samples and the same estimator, so the same gradients up to the
+    order of the FP32 partial sums."""
+    import torch
+
+    s, scene, albedo, kinds, radiance, roughness = field
+    cfg = s.config
+    spp = 32
+    w = np.random.default_rng(9).random((cfg.width * cfg.height, 3)).astype(np.float32)
+    dev = torch.device("cuda", 0)
+    dl = torch.from_numpy(w).to(dev)
+    scene.set_params(albedo, radiance, roughness)
+    out = {}
+    for plain in (False, True):
+        ga = torch.zeros((len(albedo), 3), dtype=torch.float64, device=dev)
+        gr = torch.zeros((len(radiance), 3), dtype=torch.float64, device=dev)
+        gg = torch.zeros(len(roughness), dtype=torch.float64, device=dev)
+        torch.cuda.synchronize()
+        scene.adjoint(0, spp, dl.data_ptr(), ga.data_ptr(), gr.data_ptr(), gg.data_ptr(), plain=plain)
+        out[plain] = [t.cpu().numpy() for t in (ga, gg, gr)]
+    for k, name in enumerate(("albedo", "roughness", "radiance")):
+        a, b = out[False][k], out[True][k]
+        err = np.linalg.norm(a - b) / np.linalg.norm(b)
+        print(f"{name}: wavefront vs plain relative L2 {err:.2e}")
+        assert err <= 1e-4
+        assert np.array_equal(a == 0, b == 0)

@@ -20,50 +20,14 @@
 // Each vertex's credit is taken once at the path's end from suffix sums (the radiance gathered after the vertex acted),
 // weighted by the loss's derivative for its pixel (dL/dI / samples a pixel). Credits are FP32 sums in the thread and
 // atomics into per-block partials in shared memory, reduced once a block into the FP64 gradients.
-#include "integrator.cuh"
 #include "adjoint.h"
+#include "credits.cuh"
 
 namespace x2 {
 
 // This translation unit's copy of the Sobol direction table (sampler.cuh).
 cudaError_t uploadSobolAdjoint(const uint32_t directions[17][32]) {
     return cudaMemcpyToSymbol(c_sobol, directions, sizeof(uint32_t) * 17 * 32);
-}
-
-// d log f / d(material roughness) of the GGX lobe l (shading.cuh evalGGX) at directions wo, wi; 0 where f is 0 or
-// the roughness is clamped. With a = the lobe roughness max(0.001, r^2) (r the material's roughness, saturated),
-// T = tan^2 of the half vector's angle and t = tan^2 of a direction's angle:
-//   log D  = log(a^2) - 2 log(a^2 + T) + const         -> 2/a - 4a/(a^2 + T)
-//   log G1 = log 2 - log(1 + S), S = sqrt(1 + a^2 t)   -> -a t / (S (1 + S))
-// and da/dr = 2r where r^2 > 0.001 (0 < r < 1). The Schlick Fresnel does not depend on the roughness.
-// Near a mirror (a of 1e-3..1e-2) the two terms of dlog D are hundreds each and a path's credits cancel over samples to
-// a gradient thousands of times smaller, so T must be exact to far better than float's 1 - cos^2 gives: the tangents
-// are taken from |x cross n|^2 / (x . n)^2, in double (a few dozen FP64 operations a vertex).
-__device__ __forceinline__ float ggxLogDerivative(const Lobe& l, float materialRoughness, V3 wo, V3 wi) {
-    const double r = materialRoughness;
-    if (!(r > 0.0 && r < 1.0) || materialRoughness * materialRoughness <= 0.001f) return 0.0f;
-    const double nx = l.frame.z.x, ny = l.frame.z.y, nz = l.frame.z.z;
-    const double ox = wo.x, oy = wo.y, oz = wo.z, ix = wi.x, iy = wi.y, iz = wi.z;
-    const double cosNO = ox * nx + oy * ny + oz * nz, cosNI = ix * nx + iy * ny + iz * nz;
-    if (cosNO <= 0.0 || cosNI <= 0.0) return 0.0f;
-    double mx = ox + ix, my = oy + iy, mz = oz + iz;
-    const double lm = sqrt(mx * mx + my * my + mz * mz);
-    if (!(lm > 0.001)) return 0.0f;
-    mx /= lm;
-    my /= lm;
-    mz /= lm;
-    const double cosThetaM = mx * nx + my * ny + mz * nz;
-    if (cosThetaM <= 0.0 || mx * ix + my * iy + mz * iz <= 0.0) return 0.0f;
-    auto sin2 = [&](double x, double y, double z) {
-        const double cx = y * nz - z * ny, cy = z * nx - x * nz, cz = x * ny - y * nx;
-        return cx * cx + cy * cy + cz * cz;
-    };
-    const double a = l.roughness, a2 = a * a;
-    const double T = sin2(mx, my, mz) / (cosThetaM * cosThetaM);
-    const double to = sin2(ox, oy, oz) / (cosNO * cosNO), ti = sin2(ix, iy, iz) / (cosNI * cosNI);
-    const double so = sqrt(1.0 + a2 * to), si = sqrt(1.0 + a2 * ti);
-    const double dlogf = 2.0 / a - 4.0 * a / (a2 + T) - a * to / (so * (1.0 + so)) - a * ti / (si * (1.0 + si));
-    return float(dlogf * 2.0 * r);
 }
 
 namespace {
@@ -79,15 +43,6 @@ __device__ __forceinline__ uint32_t tilePixelA(uint32_t tile, uint32_t position,
 
 constexpr uint32_t kLightSlots = 32;  // lights whose credits a thread keeps to itself (more: straight to shared memory)
 constexpr uint32_t kGgxVertex = 0x80000000u;  // a vertex record's material index with this bit: a GGX vertex
-
-// Where a block's partial gradients sit in its shared memory: albedo (3 a material), roughness (1 a material),
-// radiance (3 a light).
-struct Layout {
-    uint32_t materials, lights;
-    __device__ uint32_t albedo(uint32_t m) const { return 3 * m; }
-    __device__ uint32_t roughness(uint32_t m) const { return 3 * materials + m; }
-    __device__ uint32_t radiance(uint32_t j) const { return 4 * materials + 3 * j; }
-};
 
 // A thread's credits. Lights: each contribution, weighted by the loss's derivative for its pixel, over its light's
 // radiance, summed in the thread's own array over all its samples, then into the block's partials once. Materials: a

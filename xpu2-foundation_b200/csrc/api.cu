@@ -171,6 +171,13 @@ struct x2_scene {
     bool waveTiming = false;           // time each kernel kind (no graph)
     float waveMs[5] = {0, 0, 0, 0, 0}; // logic, extend, shade, shadow, film reduce
     uint32_t queueLog[2 * 4096] = {};  // timed launches: each iteration's extend and shadow queue sizes
+    // the adjoint's wavefront state (x2_adjoint): vertex records, scales, counts, dL/dI shares, record auxiliaries
+    uint4* avert = nullptr;
+    float4* ascale = nullptr;
+    uint32_t* avcount = nullptr;
+    float4* adelta = nullptr;
+    uint2* aaux = nullptr;
+    uint32_t adjPaths = 0, adjVerts = 0, adjRecords = 0;
 };
 
 namespace {
@@ -638,10 +645,25 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
     return X2_OK;
 }
 
+void freeAdjointWave(x2_scene* s) {
+    cudaFree(s->avert);
+    cudaFree(s->ascale);
+    cudaFree(s->avcount);
+    cudaFree(s->adelta);
+    cudaFree(s->aaux);
+    s->avert = nullptr;
+    s->ascale = nullptr;
+    s->avcount = nullptr;
+    s->adelta = nullptr;
+    s->aaux = nullptr;
+    s->adjPaths = s->adjVerts = s->adjRecords = 0;
+}
+
 int x2_scene_free(x2_scene* s) {
     if (!s) return X2_OK;
     if (s->ctx) cudaSetDevice(s->ctx->device);
     if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
+    freeAdjointWave(s);
     cudaFree(s->bvh.nodes);
     cudaFree(s->bvh.tris);
     cudaFree(s->triMesh);
@@ -1043,6 +1065,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     a.shadowNext = s->waveCounters + 4;
     a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
     a.shadeCount = s->waveCounters + 5;
+    a.adj = AdjointWave{};
     a.refill = s->refill;
     a.triLimit = s->triLimit;
     a.out = s->out;
@@ -1238,8 +1261,9 @@ int x2_scene_set_params(x2_scene* s, const float* albedo, const float* roughness
 // material's albedo and roughness and each light's radiance, given the loss's derivative with respect to the image
 // (device, 3 floats a pixel, the image being the film's mean). Device outputs (FP64), added to; a null roughness
 // output skips that set.
-int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad, double* d_roughness_grad,
-               double* d_radiance_grad) {
+// The replay in the plain megakernel's form (one thread a sample): x2_adjoint's arguments and results.
+int x2_adjoint_plain(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad,
+                     double* d_roughness_grad, double* d_radiance_grad) {
     if (!s || !s->configured || !d_dloss_dimage || !d_albedo_grad || !d_radiance_grad || count == 0) {
         setError("x2_adjoint: configured scene, device arrays and a sample count");
         return X2_EINVAL;
@@ -1285,6 +1309,167 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
         setError("x2_adjoint: launch failed");
     }
     cudaFree(d);
+    cudaFree(grads);
+    return rc;
+}
+
+// The adjoint in the wavefront form: the samples' paths replayed by the wavefront's kernels (logic, extend, per-lobe
+// sort, shade, shadow; the adjoint forms of logic and shade credit as they go), as one graph of iterations replayed
+// until no path is left; the gradient rows then summed into FP64 and added to the caller's arrays.
+int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad, double* d_roughness_grad,
+               double* d_radiance_grad) {
+    if (!s || !s->configured || !d_dloss_dimage || !d_albedo_grad || !d_radiance_grad || count == 0) {
+        setError("x2_adjoint: configured scene, device arrays and a sample count");
+        return X2_EINVAL;
+    }
+    if (s->config.volume_count || s->config.max_depth >= 128 || s->config.bsdf_samples != 1) {
+        setError("x2_adjoint: no volumes, max_depth < 128, bsdf_samples = 1");
+        return X2_EINVAL;
+    }
+    const uint32_t params = 4 * s->materialCount + 3 * s->lightCount;
+    if (size_t(params) * sizeof(float) > 96 * 1024 || s->materialCount >= (1u << 30)) {
+        setError("x2_adjoint: 4 x materials + 3 x lights must be at most %u", 96 * 1024 / 4);
+        return X2_EINVAL;
+    }
+    if (int rc = checkDevice(s->ctx)) return rc;
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    const uint32_t tiles = ((s->config.width + 7) / 8) * ((s->config.height + 7) / 8);
+    const unsigned long long items = (unsigned long long)tiles * 64ull * count;
+    if (items > 0xffffffffull) {
+        setError("x2_adjoint: %llu work items (at most 2^32 - 1)", items);
+        return X2_EINVAL;
+    }
+    uint32_t paths = s->reservePaths ? s->reservePaths : (1u << 20);
+    if (paths > items) paths = uint32_t(items < 1024 ? 1024 : items);
+    const uint32_t records = s->config.light_count * s->config.light_samples + 1;
+    const uint32_t verts = s->config.max_depth + 1;
+    if (int rc = ensureWave(s, paths, records)) return rc;
+    if (int rc = ensureItems(s, items)) return rc;
+    if (s->adjPaths != paths || s->adjVerts != verts || s->adjRecords != records) {
+        freeAdjointWave(s);
+        const size_t V = size_t(paths) * verts;
+        const bool ok = cudaMalloc(&s->avert, sizeof(uint4) * V) == cudaSuccess && cudaMalloc(&s->ascale, sizeof(float4) * V) == cudaSuccess &&
+                        cudaMalloc(&s->avcount, sizeof(uint32_t) * paths) == cudaSuccess &&
+                        cudaMalloc(&s->adelta, sizeof(float4) * paths) == cudaSuccess &&
+                        cudaMalloc(&s->aaux, sizeof(uint2) * size_t(paths) * records) == cudaSuccess;
+        if (!ok) {
+            freeAdjointWave(s);
+            setError("x2_adjoint: device allocation failed for %u paths", paths);
+            return X2_ENOMEM;
+        }
+        s->adjPaths = paths;
+        s->adjVerts = verts;
+        s->adjRecords = records;
+    }
+    Slot& sl = s->slots[0];
+    if (int rc = ensureSlot(sl, tiles)) return rc;
+    constexpr uint32_t kRows = 1024;
+    float* rows = nullptr;
+    double* grads = nullptr;
+    if (cudaMalloc(&rows, sizeof(float) * size_t(kRows) * params) != cudaSuccess || cudaMalloc(&grads, sizeof(double) * params) != cudaSuccess) {
+        cudaFree(rows);
+        setError("x2_adjoint: allocation failed");
+        return X2_ENOMEM;
+    }
+    cudaStream_t st = s->ctx->stream;
+    std::vector<x2_chunk> chunks(tiles);
+    for (uint32_t t = 0; t < tiles; ++t) chunks[t] = x2_chunk{t, first, count, 0};
+    cudaMemcpyAsync(sl.chunks, chunks.data(), sizeof(x2_chunk) * tiles, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(rows, 0, sizeof(float) * size_t(kRows) * params, st);
+    cudaMemsetAsync(grads, 0, sizeof(double) * params, st);
+    cudaMemsetAsync(s->wave.state, 0, sizeof(uint32_t) * paths, st);
+    cudaMemsetAsync(s->wave.ncount, 0, sizeof(uint32_t) * paths, st);
+    cudaMemsetAsync(s->claimed, 0, sizeof(unsigned long long), st);
+    cudaMemsetAsync(s->waveCounters, 0, sizeof(uint32_t) * kWaveCounters, st);
+    cudaMemsetAsync(sl.counters, 0, sizeof(Counters), st);
+    WaveArgs a;
+    a.scene = viewOf(s);
+    a.scene.stats = nullptr;
+    a.w = s->wave;
+    a.paths = paths;
+    a.recordsPerPath = records;
+    a.chunks = sl.chunks;
+    a.itemCount = items;
+    a.samplesPerChunk = count;
+    a.claimed = s->claimed;
+    a.extendQ = s->extendQ;
+    a.extendCount = s->waveCounters;
+    a.lastExtend = s->waveCounters + 1;
+    a.shadowQ = s->shadowQ;
+    a.shadowCount = s->waveCounters + 2;
+    a.extendNext = s->waveCounters + 3;
+    a.shadowNext = s->waveCounters + 4;
+    a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
+    a.shadeCount = s->waveCounters + 5;
+    a.adj = AdjointWave{};
+    a.refill = s->refill;
+    a.triLimit = s->triLimit;
+    a.out = s->out;
+    a.outStatus = s->outStatus;
+    a.counters = sl.counters;
+    a.scenes = nullptr;
+    a.chunkRequest = nullptr;
+    a.chunkItems = nullptr;
+    a.chunkCount = tiles;
+    a.adj = AdjointWave{d_dloss_dimage, rows, kRows, s->materialCount, s->lightCount, verts, s->avert, s->ascale, s->avcount, s->adelta, s->aaux};
+    const size_t shared = sizeof(float) * params;
+    if (shared > 48 * 1024) {
+        cudaFuncSetAttribute(wfLogicAdjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shared));
+        cudaFuncSetAttribute(wfShadeAdjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shared));
+    }
+    // Logic in a grid of a few blocks a SM (each block's partials go to a gradient row once a launch).
+    const int gridLogic = std::min(int((paths + kWaveBlock - 1) / kWaveBlock), s->ctx->smCount * 8);
+    const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
+    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, false);
+    const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
+    constexpr int kIter = 8;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int rc = X2_OK;
+    if (cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        setError("x2_adjoint: stream capture failed");
+        rc = X2_ECUDA;
+    } else {
+        for (int it = 0; it < kIter; ++it) {
+            wfResetQueues<<<1, 32, 0, st>>>(a);
+            wfLogicAdjoint<<<gridLogic, kWaveBlock, shared, st>>>(a);
+            wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
+            if (a.shadeQ) wfSortShade<<<gridWork, kWaveBlock, 0, st>>>(a);
+            wfShadeAdjoint<<<gridWork, kWaveBlock, shared, st>>>(a);
+            wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
+        }
+        wfResetQueues<<<1, 32, 0, st>>>(a);
+        if (cudaStreamEndCapture(st, &graph) != cudaSuccess || cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+            setError("x2_adjoint: graph capture failed");
+            rc = X2_ECUDA;
+        }
+    }
+    uint32_t iterations = 0;
+    while (rc == X2_OK) {
+        if (cudaGraphLaunch(exec, st) != cudaSuccess) {
+            setError("x2_adjoint: graph launch failed");
+            rc = X2_ECUDA;
+            break;
+        }
+        iterations += kIter;
+        cudaMemcpyAsync(s->hostLast, s->waveCounters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        if ((rc = x2_synchronize(s->ctx, 600000)) != X2_OK) break;
+        if (s->hostLast[0] == 0) break;
+        if (iterations > maxIter) {
+            setError("x2_adjoint: the wavefront did not drain after %u iterations", iterations);
+            rc = X2_EDEVICE;
+        }
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (rc == X2_OK) {
+        wfGradRows<<<(params + 255) / 256, 256, 0, st>>>(rows, kRows, params, grads);
+        addInto<<<(params + 255) / 256, 256, 0, st>>>(d_albedo_grad, grads, 3 * s->materialCount);
+        if (d_roughness_grad) addInto<<<(params + 255) / 256, 256, 0, st>>>(d_roughness_grad, grads + 3 * s->materialCount, s->materialCount);
+        addInto<<<(params + 255) / 256, 256, 0, st>>>(d_radiance_grad, grads + 4 * s->materialCount, 3 * s->lightCount);
+        rc = cudaGetLastError() == cudaSuccess ? x2_synchronize(s->ctx, 600000) : X2_ECUDA;
+    }
+    cudaFree(rows);
     cudaFree(grads);
     return rc;
 }
@@ -1490,6 +1675,7 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
         a.shadowNext = s0->waveCounters + 4;
         a.shadeQ = s0->lobeQueues ? s0->shadeQ : nullptr;
         a.shadeCount = s0->waveCounters + 5;
+        a.adj = AdjointWave{};
         a.refill = s0->refill;
         a.triLimit = s0->triLimit;
         a.out = s0->out;

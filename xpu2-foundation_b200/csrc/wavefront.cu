@@ -14,7 +14,7 @@
 // Iterations are captured once as a CUDA graph and replayed until every item is done. The per-item output (rgb,
 // alpha, status) is then summed into the film in sample order by filmReduce, so the film does not depend on the
 // order paths finish in.
-#include "integrator.cuh"
+#include "credits.cuh"
 #include "wavefront.h"
 
 namespace x2 {
@@ -73,6 +73,32 @@ __device__ __forceinline__ void warpAddCounters(Counters* dst, unsigned long lon
         if (samples) atomicAdd(&dst->samples, samples);
         if (errors) atomicAdd(&dst->errors, errors);
     }
+}
+
+// The adjoint's credits into a block's shared partials (x2_adjoint's wavefront form).
+constexpr uint32_t kVertLambert = 0u, kVertGgx = 1u, kVertNone = 3u;  // a vertex record's kind (material bits 30-31)
+
+__device__ __forceinline__ void creditLightTo(float* partial, const Layout& at, const SceneView& s, float4 d, V3 c, uint32_t j) {
+    if (j == ~0u) return;
+    const x2_light& L = s.lights[j];
+    const float w[3] = {d.x * c.x, d.y * c.y, d.z * c.z};
+    for (int k = 0; k < 3; ++k)
+        if (L.radiance[k] != 0.0f && w[k] != 0.0f) atomicAdd(partial + at.radiance(j) + k, w[k] / L.radiance[k]);
+}
+__device__ __forceinline__ void creditRoughnessTo(float* partial, const Layout& at, uint32_t m, float4 d, V3 c, float g) {
+    const float v = (d.x * c.x + d.y * c.y + d.z * c.z) * g;
+    if (v != 0.0f && finitef(v)) atomicAdd(partial + at.roughness(m), v);
+}
+// A block's partials: zeroed at the kernel's start, added to the block's gradient row at its end.
+__device__ __forceinline__ void partialsBegin(float* partial, const Layout& at) {
+    for (uint32_t i = threadIdx.x; i < at.count(); i += blockDim.x) partial[i] = 0.0f;
+    __syncthreads();
+}
+__device__ __forceinline__ void partialsEnd(float* partial, const Layout& at, const AdjointWave& adj) {
+    __syncthreads();
+    float* row = adj.rows + size_t(blockIdx.x % adj.rowCount) * at.count();
+    for (uint32_t i = threadIdx.x; i < at.count(); i += blockDim.x)
+        if (partial[i] != 0.0f) atomicAdd(row + i, partial[i]);
 }
 
 __device__ __forceinline__ uint32_t packDepths(const Pending& p) {
@@ -145,17 +171,20 @@ __device__ __forceinline__ uint32_t chunkOfItem(const WaveArgs& a, unsigned long
 }
 
 // ---- logic ----
-template <bool kBatch>
+template <bool kBatch, bool kAdjoint = false>
 __device__ __forceinline__ void logicBody(const WaveArgs& a) {
     const WaveState& w = a.w;
     unsigned long long samples = 0, errors = 0;
+    extern __shared__ float partial[];  // the adjoint's block partials
+    const Layout at{a.adj.materials, a.adj.lights};
+    if (kAdjoint) partialsBegin(partial, at);
     for (uint32_t base = blockIdx.x * blockDim.x; base < a.paths; base += gridDim.x * blockDim.x) {
         const uint32_t p = base + threadIdx.x;
         uint32_t st = p < a.paths ? w.state[p] : kTrace + 100;  // out of range: no work, no claim
         if (p < a.paths) {
             // The previous vertex's shadow rays, in the order they were made.
             const uint32_t n = w.ncount[p];
-            if (n) {
+            if (n && !kAdjoint) {
                 float4 rad = w.rad[p];
                 const size_t first = size_t(p) * a.recordsPerPath;
                 for (uint32_t k = 0; k < n; ++k)
@@ -167,6 +196,52 @@ __device__ __forceinline__ void logicBody(const WaveArgs& a) {
                     }
                 w.rad[p] = rad;
                 w.ncount[p] = 0;
+            } else if (n && kAdjoint) {
+                // The same, crediting each unoccluded record to its light and, made by a GGX vertex's light sample, to
+                // that vertex's roughness with its own factor; a GGX vertex's suffix then starts after its light
+                // samples (its records come first, its BSDF sample's last).
+                float4 rad = w.rad[p];
+                const size_t first = size_t(p) * a.recordsPerPath;
+                const size_t vj = size_t(p) * a.adj.vertsPerPath + (a.adj.vcount[p] - 1);
+                const uint4 v = a.adj.vert[vj];
+                const bool ggx = (v.x >> 30) == kVertGgx;
+                const float4 d = a.adj.delta[p];
+                float4 afterLights = make_float4(__uint_as_float(v.y), __uint_as_float(v.z), __uint_as_float(v.w), 0.0f);
+                for (uint32_t k = 0; k < n; ++k) {
+                    const uint2 aux = a.adj.aux[first + k];
+                    if (w.svis[first + k]) {
+                        const float4 c = w.scontrib[first + k];
+                        rad.x = rad.x + c.x;
+                        rad.y = rad.y + c.y;
+                        rad.z = rad.z + c.z;
+                        creditLightTo(partial, at, a.scene, d, V3{c.x, c.y, c.z}, aux.x & 0x7fffffffu);
+                        if (ggx && !(aux.x >> 31)) creditRoughnessTo(partial, at, v.x & 0x3fffffffu, d, V3{c.x, c.y, c.z}, __uint_as_float(aux.y));
+                    }
+                    if (!(aux.x >> 31)) afterLights = rad;
+                }
+                if (ggx) a.adj.vert[vj] = make_uint4(v.x, __float_as_uint(afterLights.x), __float_as_uint(afterLights.y), __float_as_uint(afterLights.z));
+                w.rad[p] = rad;
+                w.ncount[p] = 0;
+            }
+            if (kAdjoint && st == kDone) {
+                // The path's end: each vertex credited once with what the path gathered after it acted.
+                const float4 total = w.rad[p], d = a.adj.delta[p];
+                const uint32_t nv = a.adj.vcount[p];
+                for (uint32_t k = 0; k < nv; ++k) {
+                    const size_t vk = size_t(p) * a.adj.vertsPerPath + k;
+                    const uint4 v = a.adj.vert[vk];
+                    const uint32_t kind = v.x >> 30, m = v.x & 0x3fffffffu;
+                    if (kind == kVertNone) continue;
+                    const V3 after{total.x - __uint_as_float(v.y), total.y - __uint_as_float(v.z), total.z - __uint_as_float(v.w)};
+                    const float4 sc = a.adj.scale[vk];
+                    if (kind == kVertGgx) {
+                        creditRoughnessTo(partial, at, m, d, after, sc.x);
+                        continue;
+                    }
+                    if (sc.x != 0.0f && after.x != 0.0f) atomicAdd(partial + at.albedo(m), d.x * after.x * sc.x);
+                    if (sc.y != 0.0f && after.y != 0.0f) atomicAdd(partial + at.albedo(m) + 1, d.y * after.y * sc.y);
+                    if (sc.z != 0.0f && after.z != 0.0f) atomicAdd(partial + at.albedo(m) + 2, d.z * after.z * sc.z);
+                }
             }
             if (st == kDone || st == kError) {
                 const unsigned long long item = w.item[p];
@@ -213,6 +288,12 @@ __device__ __forceinline__ void logicBody(const WaveArgs& a) {
                         cameraPending(camera, p0);
                         storePending(w, p, p0, pixel, index, request);
                         w.rad[p] = make_float4(0, 0, 0, 0);
+                        if (kAdjoint) {
+                            const float inv = 1.0f / float(chunk.count);
+                            a.adj.delta[p] = make_float4(a.adj.dLdI[3ull * pixel] * inv, a.adj.dLdI[3ull * pixel + 1] * inv,
+                                                         a.adj.dLdI[3ull * pixel + 2] * inv, 0.0f);
+                            a.adj.vcount[p] = 0;
+                        }
                         w.item[p] = uint32_t(item);
                         w.state[p] = kTrace;
                         st = kTrace;
@@ -222,14 +303,16 @@ __device__ __forceinline__ void logicBody(const WaveArgs& a) {
         }
         // The extend queue: every slot with a ray to trace.
         const bool trace = st == kTrace;
-        const uint32_t at = warpReserve(a.extendCount, trace ? 1u : 0u);
-        if (trace) a.extendQ[at] = p;
+        const uint32_t slot = warpReserve(a.extendCount, trace ? 1u : 0u);
+        if (trace) a.extendQ[slot] = p;
     }
     warpAddCounters(a.counters, 0, 0, 0, 0, samples, errors);
+    if (kAdjoint) partialsEnd(partial, at, a.adj);
 }
 
 __global__ void __launch_bounds__(kWaveBlock) wfLogic(WaveArgs a) { logicBody<false>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfLogicBatch(WaveArgs a) { logicBody<true>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfLogicAdjoint(WaveArgs a) { logicBody<false, true>(a); }
 
 // ---- extend: closest hits ----
 // Persistent traversal over a queue: each lane walks its ray a node a step; a warp fetches the next rays of the queue
@@ -296,12 +379,25 @@ __device__ __forceinline__ void extendBody(const WaveArgs& a) {
 }
 
 // ---- shade ----
+// The wavefront's sink: shadow rays to the path's record slots, the child to the slot. kAdjoint: also the vertex
+// records the adjoint credits at the path's end and each record's light and own roughness factor.
+template <bool kAdjoint = false>
 struct WaveSink {
     const WaveState& w;
     uint32_t p, n, recordsPerPath;
     bool pushed;
     Pending child;
     unsigned long long nNee, nBsdf, nHeld;
+    // Adjoint only.
+    const AdjointWave* adj;
+    const SceneView* s;
+    const V3* radiance;
+    uint32_t depth;
+    Lobe lobe;
+    V3 wo;
+    float materialRoughness;
+    bool ggx, sampled;
+
     __device__ void shadow(const ShadowReq& q, bool isBsdf) {
         const size_t k = size_t(p) * recordsPerPath + n++;
         w.sray0[k] = make_float4(q.origin.x, q.origin.y, q.origin.z, q.near);
@@ -309,11 +405,40 @@ struct WaveSink {
         w.scontrib[k] = make_float4(q.contribution.x, q.contribution.y, q.contribution.z, 0.0f);
         if (isBsdf) ++nBsdf;
         else ++nNee;
+        if (kAdjoint) {
+            if (isBsdf) bsdfDirection(q.dir);
+            const float g = !isBsdf && ggx ? ggxLogDerivative(lobe, materialRoughness, wo, q.dir) : 0.0f;
+            adj->aux[k] = make_uint2(q.light | (isBsdf ? 0x80000000u : 0u), __float_as_uint(g));
+        }
     }
     __device__ void held() { ++nHeld; }
-    __device__ void vertex(uint32_t, const Bsdf&, V3) {}
+    __device__ void vertex(uint32_t m, const Bsdf& b, V3 out) {
+        if (!kAdjoint) return;
+        const bool lambert = b.count && b.lobe.kind == 0;
+        ggx = b.count && b.lobe.kind == 1;
+        sampled = false;
+        const uint32_t kind = lambert ? kVertLambert : ggx ? kVertGgx : kVertNone;
+        const size_t v = size_t(p) * adj->vertsPerPath + depth;
+        adj->vert[v] = make_uint4(m | (kind << 30), __float_as_uint(radiance->x), __float_as_uint(radiance->y), __float_as_uint(radiance->z));
+        const V3 a = b.lobe.albedo;
+        adj->scale[v] = lambert ? make_float4(a.x != 0.0f ? 1.0f / a.x : 0.0f, a.y != 0.0f ? 1.0f / a.y : 0.0f, a.z != 0.0f ? 1.0f / a.z : 0.0f, 0.0f)
+                                : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        adj->vcount[p] = depth + 1;
+        if (ggx) {
+            lobe = b.lobe;
+            wo = out;
+            materialRoughness = s->materials[m].roughness;
+        }
+    }
+    // The BSDF sample's direction, the first time the vertex hands on something that came through it.
+    __device__ void bsdfDirection(V3 wi) {
+        if (!ggx || sampled) return;
+        sampled = true;
+        adj->scale[size_t(p) * adj->vertsPerPath + depth].x = ggxLogDerivative(lobe, materialRoughness, wo, wi);
+    }
     __device__ uint32_t top(uint32_t t) const { return t; }
     __device__ void push(const Pending& c) {
+        if (kAdjoint) bsdfDirection(c.dir);
         child = c;
         pushed = true;
     }
@@ -367,10 +492,13 @@ __device__ __forceinline__ uint32_t shadeEntry(const WaveArgs& a, uint32_t i, ui
     return a.shadeQ[2ull * a.paths + (i - c0 - c1)];
 }
 
-template <bool kBatch, bool kVolumes>
+template <bool kBatch, bool kVolumes, bool kAdjoint = false>
 __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
     const WaveState& w = a.w;
     const uint32_t n = *a.extendCount;
+    extern __shared__ float partial[];  // the adjoint's block partials
+    const Layout at{a.adj.materials, a.adj.lights};
+    if (kAdjoint) partialsBegin(partial, at);
     const uint32_t c0 = a.shadeQ ? a.shadeCount[0] : 0u, c1 = a.shadeQ ? a.shadeCount[1] : 0u;
     unsigned long long nee = 0, bsdf = 0, held = 0;
     // Every lane of a warp runs the same rounds: the shadow queue's reservation is a warp-wide scan.
@@ -411,10 +539,30 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
             // The camera's position (a pinhole: every camera ray's origin).
             const V3 cameraPosition = add(mvector(s.camera.camera_to_render, V3{0, 0, 0}),
                                           V3{s.camera.camera_to_render[3][0], s.camera.camera_to_render[3][1], s.camera.camera_to_render[3][2]});
+            float4 d{0, 0, 0, 0};
+            if (kAdjoint) {
+                // The held light (bounce-ray reuse), reached unless the ray met something short of it.
+                d = a.adj.delta[p];
+                if (pv.heldLight != ~0u && !(hit.geom != ~0u && hit.t < pv.heldFar)) creditLightTo(partial, at, s, d, pv.held, pv.heldLight);
+            }
+            const V3 prior = radiance;
             afterTrace<kVolumes>(s, root, pv, hit, cameraPosition, radiance, alpha);
+            if (kAdjoint && pv.depth == 0 && s.config.visible_lights) {
+                // The light a camera ray sees (afterTrace added it).
+                const bool missed = hit.geom == ~0u;
+                creditLightTo(partial, at, s, d, sub(radiance, prior),
+                              visibleLightIndex(s, root, missed ? pv.origin : cameraPosition, pv.dir, missed ? 3.4028234663852886e+38f : hit.t));
+            }
             uint32_t next = kDone;
             if (hit.geom != ~0u) {
-                WaveSink sink{w, p, 0, a.recordsPerPath, false, Pending{}, 0, 0, 0};
+                WaveSink<kAdjoint> sink{w, p, 0, a.recordsPerPath, false, Pending{}, 0, 0, 0};
+                if (kAdjoint) {
+                    sink.adj = &a.adj;
+                    sink.s = &s;
+                    sink.radiance = &radiance;
+                    sink.depth = pv.depth;
+                    sink.ggx = sink.sampled = false;
+                }
                 if (!shadeVertex<kVolumes>(s, root, pixel, index, pv, hit, va, vb, vc, 0u, radiance, alpha, sink)) {
                     next = kError;
                 } else {
@@ -434,10 +582,11 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
             const size_t first = size_t(p) * a.recordsPerPath;
             for (uint32_t k = 0; k < records; ++k) w.svis[first + k] = 0;
         }
-        const uint32_t at = warpReserve(a.shadowCount, records);
-        for (uint32_t k = 0; k < records; ++k) a.shadowQ[at + k] = p * a.recordsPerPath + k;
+        const uint32_t slot = warpReserve(a.shadowCount, records);
+        for (uint32_t k = 0; k < records; ++k) a.shadowQ[slot + k] = p * a.recordsPerPath + k;
     }
     warpAddCounters(a.counters, 0, nee, bsdf, held, 0, 0);
+    if (kAdjoint) partialsEnd(partial, at, a.adj);
 }
 
 // ---- shadow: any hits ----
@@ -455,6 +604,16 @@ __global__ void __launch_bounds__(kWaveBlock) wfExtend(WaveArgs a) { extendBody<
 __global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) { shadeBody<false, false>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadeVolumes(WaveArgs a) { shadeBody<false, true>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadeBatchVolumes(WaveArgs a) { shadeBody<true, true>(a); }
+__global__ void __launch_bounds__(kWaveBlock, 4) wfShadeAdjoint(WaveArgs a) { shadeBody<false, false, true>(a); }
+
+// The adjoint's gradient rows summed in FP64 into grads (one thread a gradient).
+__global__ void wfGradRows(const float* rows, uint32_t rowCount, uint32_t params, double* grads) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= params) return;
+    double sum = 0.0;
+    for (uint32_t r = 0; r < rowCount; ++r) sum += double(rows[size_t(r) * params + i]);
+    grads[i] += sum;
+}
 __global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) { shadowBody<false>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfExtendBatch(WaveArgs a) { extendBody<true>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadowBatch(WaveArgs a) { shadowBody<true>(a); }

@@ -28,6 +28,21 @@ struct WaveState {
     uint8_t* svis;     // 1: nothing occludes [near, far]
 };
 
+// The adjoint's wavefront form (x2_adjoint): per path slot the vertices it passed (material, the radiance before the
+// vertex acted, its credit scale), the sample's dL/dI share, and per shadow record its light and own factor; the
+// credits go to per-block shared partials and from there into FP32 gradient rows, summed in FP64 at the end.
+struct AdjointWave {
+    const float* dLdI;   // 3 floats a pixel; null: not an adjoint launch
+    float* rows;         // rowCount x params FP32 partial rows
+    uint32_t rowCount, materials, lights;
+    uint32_t vertsPerPath;  // max_depth + 1
+    uint4* vert;         // slot * vertsPerPath + depth: material | kind bits, radiance before it acted (float bits)
+    float4* scale;       // the same: credit scale (Lambert: 1 / albedo; GGX: dlog f/dr at its BSDF direction in x)
+    uint32_t* vcount;    // a slot's vertices
+    float4* delta;       // a slot's dL/dI share (dL/dI of its pixel over the pixel's samples)
+    uint2* aux;          // per shadow record: light | (BSDF record << 31), own roughness factor (float bits)
+};
+
 struct WaveArgs {
     SceneView scene;
     WaveState w;
@@ -49,6 +64,7 @@ struct WaveArgs {
     // warp's lanes run one lobe's code.
     uint32_t* shadeQ;
     uint32_t* shadeCount;
+    AdjointWave adj;      // adjoint launches only (adj.dLdI null otherwise)
     uint32_t refill;       // a warp fetches new rays once this many of its lanes are idle (1..32)
     uint32_t triLimit;     // triangle tests a lane makes a traversal step
     float4* out;          // per item: rgb, alpha
@@ -86,6 +102,11 @@ WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes
 WaveKernels waveKernelsBatch(bool volumes);
 __global__ void wfSortShade(WaveArgs a);
 __global__ void wfSortShadeBatch(WaveArgs a);
+// The adjoint's logic and shade kernels (dynamic shared memory: the gradient count in floats) and the final sum of the
+// gradient rows into FP64 (added to grads).
+__global__ void wfLogicAdjoint(WaveArgs a);
+__global__ void wfShadeAdjoint(WaveArgs a);
+__global__ void wfGradRows(const float* rows, uint32_t rowCount, uint32_t params, double* grads);
 __global__ void wfResetQueues(WaveArgs a);
 __global__ void wfFilmReduce(WaveArgs a, uint32_t chunkCount, double* sums, double* odd, uint32_t* counts);
 __global__ void wfFilmReduceBatch(WaveArgs a, const BatchFilm* films);

@@ -159,7 +159,7 @@ def library():
         "x2_launch_wavefront_static": ([vp, vp, u32, u32, vp, vp, C.POINTER(u64)], i32),
         "x2_render_batch": ([vp, C.POINTER(Request), u32, C.POINTER(Completion)], i32),
         "x2_wavefront_autotune": ([vp, u32, u32, C.POINTER(WavefrontShape), C.POINTER(C.c_float)], i32),
-        "x2_scene_set_params": ([vp, vp, vp, vp], i32), "x2_adjoint": ([vp, u32, u32, vp, vp, vp, vp], i32),
+        "x2_scene_set_params": ([vp, vp, vp, vp], i32), "x2_adjoint": ([vp, u32, u32, vp, vp, vp, vp], i32), "x2_adjoint_plain": ([vp, u32, u32, vp, vp, vp, vp], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
@@ -408,11 +408,13 @@ class Scene:
         g = None if roughness is None else np.ascontiguousarray(roughness, np.float32)
         _check(library().x2_scene_set_params(self._h, _ptr(a), _ptr(g), _ptr(r)))
 
-    def adjoint(self, first, count, d_dloss_dimage, d_albedo_grad, d_radiance_grad, d_roughness_grad=None):
+    def adjoint(self, first, count, d_dloss_dimage, d_albedo_grad, d_radiance_grad, d_roughness_grad=None, plain=False):
         """x2_adjoint on device pointers (ints): adds dL/dalbedo, dL/dradiance and (when given) dL/droughness for
-        samples [first, first + count) of every pixel, given dL/dimage (3 floats a pixel)."""
-        _check(library().x2_adjoint(self._h, first, count, C.c_void_p(d_dloss_dimage), C.c_void_p(d_albedo_grad),
-                                    C.c_void_p(d_roughness_grad), C.c_void_p(d_radiance_grad)))
+        samples [first, first + count) of every pixel, given dL/dimage (3 floats a pixel). plain: the replay in the
+        plain megakernel's form (x2_adjoint_plain)."""
+        f = library().x2_adjoint_plain if plain else library().x2_adjoint
+        _check(f(self._h, first, count, C.c_void_p(d_dloss_dimage), C.c_void_p(d_albedo_grad), C.c_void_p(d_roughness_grad),
+                 C.c_void_p(d_radiance_grad)))
 
     def wavefront_autotune(self, tiles=0, spp=None):
         """Time the wavefront launch shapes on `tiles` evenly spaced tiles (0: all) at `spp` samples (default: the
