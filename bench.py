@@ -414,14 +414,26 @@ def probe_adjoint(args):
     pixels = cfg.width * cfg.height
     out = {"probe": "adjoint", "triangles": s.desc.triangle_count, "materials": s.desc.material_count, "primal_spp": 32,
            "adjoint_spp": 16}
-    for form in ("wavefront", "plain"):
-        for k in range(2):
+    for form in ("wavefront",) if args.adjoint_only else ("wavefront", "plain"):
+        for k in range(1 if args.adjoint_only else 2):
             scene.frame_begin(32)
             (scene.render_frame_wavefront if form == "wavefront" else scene.render_frame)(0, 32)
             c = scene.wait()
         out[form] = {"ms": c.milliseconds, "msamples_per_s": pixels * 32 / c.milliseconds / 1e3}
     sums, counts = scene.film()
     image = sums[:, :3] / counts[:, None]
+    if args.adjoint_only:
+        # One wavefront adjoint launch, for a profiler.
+        ga = torch.zeros((s.desc.material_count, 3), dtype=torch.float64, device="cuda:0")
+        gr = torch.zeros((s.desc.light_count, 3), dtype=torch.float64, device="cuda:0")
+        gg = torch.zeros(s.desc.material_count, dtype=torch.float64, device="cuda:0")
+        dl = torch.from_numpy(image.astype(np.float32)).to("cuda:0")
+        scene.adjoint(32, 16, dl.data_ptr(), ga.data_ptr(), gr.data_ptr(), gg.data_ptr())
+        torch.cuda.synchronize()
+        print(json.dumps({"probe": "adjoint", "adjoint_only": True, "grad_norms": [float(ga.norm()), float(gr.norm()), float(gg.norm())]}))
+        scene.free()
+        ctx.close()
+        return
     dev = torch.device("cuda", 0)
     dl = torch.from_numpy((2.0 * (image - 0.5 * image)).astype(np.float32)).to(dev)
     ga = torch.zeros((s.desc.material_count, 3), dtype=torch.float64, device=dev)
@@ -509,6 +521,7 @@ def main():
     ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint", "rmse"], help="one bounded launch for a profiler, then exit")
     ap.add_argument("--probe-tiles", type=int, default=592)
     ap.add_argument("--probe-timed", action="store_true", help="wavefront probe without its graph (per-kernel launches)")
+    ap.add_argument("--adjoint-only", action="store_true", help="adjoint probe: one primal frame, then one wavefront adjoint launch")
     ap.add_argument("--shape", default="", help="wavefront launch shape fields, e.g. lobe_queues=0,refill=8 (default: the library's)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
