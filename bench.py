@@ -400,7 +400,8 @@ def probe_volume(args):
 
 
 def probe_adjoint(args):
-    """Config 4 (248,832 triangles, 64 materials, 512x512): the primal frame at 32 spp (wavefront and plain) and the
+    """Config 4 (about 250k triangles: a heightfield under a 1024x1024 albedo texture and 64 icospheres of 64
+    materials; 512x512): the primal frame at 32 spp (wavefront and plain) and the
     adjoint of an L2 image loss at 16 spp (samples 32..47) in both forms (x2_adjoint: wavefront; x2_adjoint_plain:
     one thread a sample), each timed after a warm-up; Msamples/s of each and the adjoint's throughput over the
     primal's."""
@@ -439,16 +440,20 @@ def probe_adjoint(args):
     ga = torch.zeros((s.desc.material_count, 3), dtype=torch.float64, device=dev)
     gr = torch.zeros((s.desc.light_count, 3), dtype=torch.float64, device=dev)
     gg = torch.zeros(s.desc.material_count, dtype=torch.float64, device=dev)
+    tex = s.texture(0)
+    gt = torch.zeros((tex.shape[0] * tex.shape[1], 3), dtype=torch.float64, device=dev)
+    out["texture"] = list(tex.shape)
     for name, plain in (("adjoint", False), ("adjoint_plain", True)):
-        scene.adjoint(32, 16, dl.data_ptr(), ga.data_ptr(), gr.data_ptr(), gg.data_ptr(), plain=plain)
+        scene.adjoint(32, 16, dl.data_ptr(), ga.data_ptr(), gr.data_ptr(), gg.data_ptr(), plain=plain, d_texture_grad=gt.data_ptr())
         torch.cuda.synchronize()
-        ga.zero_(), gr.zero_(), gg.zero_()
+        ga.zero_(), gr.zero_(), gg.zero_(), gt.zero_()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        scene.adjoint(32, 16, dl.data_ptr(), ga.data_ptr(), gr.data_ptr(), gg.data_ptr(), plain=plain)
+        scene.adjoint(32, 16, dl.data_ptr(), ga.data_ptr(), gr.data_ptr(), gg.data_ptr(), plain=plain, d_texture_grad=gt.data_ptr())
         adj_s = time.perf_counter() - t0  # x2_adjoint waits for its launches: host time brackets them
         out[name] = {"ms": adj_s * 1e3, "msamples_per_s": pixels * 16 / adj_s / 1e6,
-                     "grad_norms": {"albedo": float(ga.norm()), "radiance": float(gr.norm()), "roughness": float(gg.norm())}}
+                     "grad_norms": {"albedo": float(ga.norm()), "radiance": float(gr.norm()), "roughness": float(gg.norm()),
+                                    "texels": float(gt.norm())}}
     out["adjoint_over_primal"] = out["adjoint"]["msamples_per_s"] / out["wavefront"]["msamples_per_s"]
     out["adjoint_plain_over_plain"] = out["adjoint_plain"]["msamples_per_s"] / out["plain"]["msamples_per_s"]
     print(json.dumps(out))

@@ -55,7 +55,10 @@ enum { X2_FILTER_BOX = 0 };
  * LAMBERT: diffuseColor = diffuse, specularColor black -> one Lambert lobe (shade_builder.h:689-697).
  * GGX: the Schlick specular path (MatModoUsdSpecular; shade_builder.h:541-556): one GGX lobe whose Fresnel is
  * Schlick with F0 = specular, plus a Lambert lobe under it only when diffuse is not black (not admitted: keep it
- * black). emission is emissiveColor (addEmission). */
+ * black). emission is emissiveColor (addEmission).
+ * diffuse_texture: 0 none; k + 1 binds the scene's texture k to diffuseColor as a UsdUVTexture read at the mesh's
+ * st primvar (a UsdPrimvarReader of the vertices' uvs; shade_mapnodes.h:972-997, :1012-1030): the texel multiplies a
+ * non-black diffuse (MapBinding BindColor, shade_maps.h). */
 enum { X2_MAT_LAMBERT = 0, X2_MAT_GGX = 1 };
 typedef struct x2_material {
     uint32_t kind;
@@ -63,7 +66,17 @@ typedef struct x2_material {
     float specular[3];
     float emission[3];
     float roughness;
+    uint32_t diffuse_texture;
 } x2_material;
+
+/* A texture: one level of fp32 RGB texels, row-major, row 0 the image's top (a lookup at st reads row (1 - t) x
+ * height, texture_core.h lookup), wrap 1 periodic, 0 clamped. UsdUVTexture reads it with no filter footprint
+ * (MoonRay sets the derivatives to zero): level 0 only, bilinear on primary paths and the closest texel on indirect
+ * ones (texture_core.h bilinear, closest; shade_mapnodes.h textureMode). */
+typedef struct x2_texture {
+    uint32_t width, height, wrap, pad;
+    const float* rgb;
+} x2_texture;
 
 /* Lights admitted: lights::Light (light_core.h:59-117) of type Env (constant, whole sphere or hemisphere, no
  * image), Rect (no image, no spread, no clear radius) and Distant (no image: a cone of half-angle acos(cos_theta_max)
@@ -130,6 +143,11 @@ typedef struct x2_scene_desc {
     uint32_t volume_count, grid_count;  /* volume_count <= 32 */
     const x2_volume* volumes;
     const x2_grid* grids;
+    /* Textures and texture coordinates: uvs null (no mesh has st) or 2 floats a vertex (MeshAttributes uvs at
+     * RateVertex, shade_material.h:143-153). */
+    uint32_t texture_count, pad2;
+    const x2_texture* textures;
+    const float* uvs;
 } x2_scene_desc;
 
 /* mixed::Config (gpu_jobs.h:10-44), the fields this engine reads, field for field with the same defaults
@@ -263,19 +281,23 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* requests, uint32_t n, x2_comp
  * material), each material's roughness (a GGX lobe's; 1 float a material) and each light's radiance (3 floats a
  * light); host arrays, null leaves a set as it is. Waits. */
 int x2_scene_set_params(x2_scene* scene, const float* albedo, const float* roughness, const float* radiance);
+/* A texture's texels set in place (host array, the texture's width x height x 3 floats). Waits. */
+int x2_scene_set_texture(x2_scene* scene, uint32_t texture, const float* rgb);
 /* The adjoint of samples [first, first + count) of every pixel (the film's mean image): given dL/dimage (device, 3
- * floats a pixel), adds dL/dalbedo (device, 3 doubles a material), dL/droughness (device, 1 double a material; null:
- * not wanted) and dL/dradiance (device, 3 doubles a light). Each sample's path is replayed from its identity (nothing
+ * floats a pixel), adds dL/dalbedo (device, 3 doubles a material: for a textured material its diffuse multiplier),
+ * dL/droughness (device, 1 double a material; null: not wanted), dL/dradiance (device, 3 doubles a light) and
+ * dL/dtexel (device, 3 doubles a texel over the scene's textures in order; null: not wanted; summed in FP32 before it
+ * is added). Each sample's path is replayed from its identity (nothing
  * of a primal pass is stored) and each contribution credited to the light it reached and the Lambert and GGX vertices
  * it passed, the sampling decisions (directions, pdfs, MIS weights, roulette) held fixed. The replay runs in the
  * wavefront form (x2_wavefront_reserve paths in flight, x2_wavefront_tune's shape). Requires no volumes,
  * max_depth < 128, bsdf_samples = 1, 4 x materials + 3 x lights <= 24576. Waits. */
 int x2_adjoint(x2_scene* scene, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad,
-               double* d_roughness_grad, double* d_radiance_grad);
+               double* d_roughness_grad, double* d_radiance_grad, double* d_texture_grad);
 /* x2_adjoint with its replay in the plain megakernel's form (one thread a sample) instead of the wavefront form: the
  * same estimator and results (up to the FP32 partial sums' order). */
 int x2_adjoint_plain(x2_scene* scene, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad,
-                     double* d_roughness_grad, double* d_radiance_grad);
+                     double* d_roughness_grad, double* d_radiance_grad, double* d_texture_grad);
 /* The last timed wavefront launch's queue sizes: for each iteration, rays extended then shadow rays (2 a
  * iteration, at most max values). */
 int x2_wavefront_queues(x2_scene* scene, uint32_t* sizes, uint32_t max);

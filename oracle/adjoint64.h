@@ -77,13 +77,65 @@ inline Frame frameN(D3 N) {  // Duff et al. 2017 (shade_math.h:138-141)
 inline D3 toWorld(const Frame& f, D3 v) { return f.x * v.x + f.y * v.y + f.z * v.z; }
 
 // The scene as this restatement reads it (the engine's own descriptor records, copied at open).
+struct Texture64 {
+    U32 width, height, wrap;
+    U64 first;  // its first texel among all textures' (for the texel gradients)
+    std::vector<float> rgb;
+};
 struct Scene64 {
     std::vector<x2_material> materials;
     std::vector<U32> meshMaterial;
     std::vector<x2_light> lights;
     x2_camera camera{};
     x2_config config{};
+    std::vector<float> uvs;  // 2 a vertex, or empty
+    std::vector<Texture64> textures;
+    U64 texels = 0;
 };
+
+// UsdUVTexture's zero-footprint lookup (texture_core.h lookup at (s, 1 - t), level 0): bilinear on a primary path,
+// else the closest texel; in double. Its texels (global indices) and weights go to idx / wt (4 each).
+inline int texAddress(long long x, long long n, U32 wrap) {
+    if (wrap) {
+        const long long v = x % n;
+        return int(v < 0 ? v + n : v);
+    }
+    return int(x < 0 ? 0 : x >= n ? n - 1 : x);
+}
+inline bool texLookup(const Texture64& t, double s, double tt, bool primary, D3& out, U64 idx[4], double wt[4]) {
+    double u = s, v = 1.0 - tt;
+    if (!std::isfinite(u) || !std::isfinite(v)) return false;
+    if (std::fabs(u) > 1024) u = t.wrap ? u - std::floor(u) : std::fmin(std::fmax(u, -1.0), 2.0);
+    if (std::fabs(v) > 1024) v = t.wrap ? v - std::floor(v) : std::fmin(std::fmax(v, -1.0), 2.0);
+    double fx = u * t.width - 0.5, fy = v * t.height - 0.5;
+    long long x = (long long)std::floor(fx), y = (long long)std::floor(fy);
+    auto at = [&](long long xx, long long yy) {
+        return U64(texAddress(yy, t.height, t.wrap)) * t.width + U64(texAddress(xx, t.width, t.wrap));
+    };
+    auto texel = [&](U64 i) { return D3{t.rgb[3 * i], t.rgb[3 * i + 1], t.rgb[3 * i + 2]}; };
+    if (primary) {
+        fx -= double(x);
+        fy -= double(y);
+        idx[0] = at(x, y);
+        idx[1] = at(x + 1, y);
+        idx[2] = at(x, y + 1);
+        idx[3] = at(x + 1, y + 1);
+        wt[0] = (1 - fx) * (1 - fy);
+        wt[1] = fx * (1 - fy);
+        wt[2] = (1 - fx) * fy;
+        wt[3] = fx * fy;
+    } else {
+        if (fx - double(x) > 0.5) ++x;
+        if (fy - double(y) > 0.5) ++y;
+        idx[0] = idx[1] = idx[2] = idx[3] = at(x, y);
+        wt[0] = 1;
+        wt[1] = wt[2] = wt[3] = 0;
+    }
+    out = D3{0, 0, 0};
+    for (int k = 0; k < 4; ++k) out = out + texel(idx[k]) * wt[k];
+    for (int k = 0; k < 4; ++k) idx[k] += t.first;
+    return finite(out);
+}
 
 struct Lobe {
     int kind = -1;  // -1 none, 0 Lambert, 1 GGX
@@ -294,6 +346,7 @@ struct Pending {
 struct Grads {
     std::vector<double> albedo, roughness, radiance;
     std::vector<double> albedoMass, roughnessMass, radianceMass;
+    std::vector<double> texture;  // 3 a texel (empty: not wanted)
 };
 
 struct Tracer {
@@ -405,10 +458,14 @@ struct Tracer {
         p0.heldLight = ~0u;
         stack[top++] = p0;
         D3 radiance{0, 0, 0};
-        // The path's vertices by depth: material (~0u none), kind, radiance before it acted, scale.
+        // The path's vertices by depth: material (~0u none), kind, radiance before it acted, scale; a textured
+        // Lambert vertex's texel value, texels and weights.
         U32 vm[128];
         int vk[128];
-        D3 before[128], scale[128];
+        D3 before[128], scale[128], texelAt[128];
+        bool textured[128];
+        U64 texIdx[128][4];
+        double texWt[128][4];
         U32 vertices = 0;
         while (top) {
             Pending pv = stack[--top];
@@ -443,6 +500,27 @@ struct Tracer {
             const x2_material& M = x.materials[mat];
             Lobe lobe;
             const D3 emission = d3(M.emission);
+            // A textured diffuse colour: the lookup at the hit's st (w st1 + u st2 + v st3 of the vertices' uvs).
+            D3 diffuse = d3(M.diffuse), texel{1, 1, 1};
+            U64 tidx[4] = {0, 0, 0, 0};
+            double twt[4] = {0, 0, 0, 0};
+            bool isTextured = false;
+            if (M.diffuse_texture) {
+                const double hu = hit.u, hv = hit.v, w = 1.0 - hu - hv;
+                double uv[6] = {0, 0, 1, 0, 1, 1};
+                if (!x.uvs.empty())
+                    for (int k = 0; k < 3; ++k) {
+                        uv[2 * k] = x.uvs[2 * size_t(s.tris[3 * tri + k])];
+                        uv[2 * k + 1] = x.uvs[2 * size_t(s.tris[3 * tri + k]) + 1];
+                    }
+                const double ss = w * uv[0] + hu * uv[2] + hv * uv[4], tt = w * uv[1] + hu * uv[3] + hv * uv[5];
+                const bool primary = pv.diffuse == 0 && pv.glossy == 0 && pv.mirror == 0;
+                if (!texLookup(x.textures[M.diffuse_texture - 1], ss, tt, primary, texel, tidx, twt)) return radiance;
+                if (!black(diffuse)) {
+                    diffuse = mulv(diffuse, texel);
+                    isTextured = true;
+                }
+            }
             if (!black(emission)) radiance = radiance + mulv(pv.T, emission);
             const double r = std::fmin(std::fmax(double(M.roughness), 0.0), 1.0);
             const D3 spec{std::fmin(std::fmax(double(M.specular[0]), 0.0), 1.0), std::fmin(std::fmax(double(M.specular[1]), 0.0), 1.0),
@@ -459,11 +537,11 @@ struct Tracer {
                 lobe.spec = spec;
                 lobe.alpha = std::fmax(0.001, r * r);
                 lobe.roughness = M.roughness;
-            } else if (!black(d3(M.diffuse))) {
+            } else if (!black(diffuse)) {
                 lobe.kind = 0;
                 lobe.type = kReflection | kDiffuse;
                 lobe.frame = frameN(st.N);
-                lobe.albedo = d3(M.diffuse);
+                lobe.albedo = diffuse;
             }
             const U32 k = pv.depth;
             vertices = k + 1;
@@ -471,6 +549,12 @@ struct Tracer {
             vm[k] = lobe.kind >= 0 ? mat : ~0u;
             vk[k] = lobe.kind;
             scale[k] = D3{0, 0, 0};
+            textured[k] = lobe.kind == 0 && isTextured;
+            texelAt[k] = texel;
+            for (int i = 0; i < 4; ++i) {
+                texIdx[k][i] = tidx[i];
+                texWt[k][i] = twt[i];
+            }
             if (lobe.kind == 0)
                 scale[k] = D3{lobe.albedo.x != 0 ? 1 / lobe.albedo.x : 0, lobe.albedo.y != 0 ? 1 / lobe.albedo.y : 0,
                               lobe.albedo.z != 0 ? 1 / lobe.albedo.z : 0};
@@ -647,9 +731,16 @@ struct Tracer {
             if (vk[k] == 1) {
                 creditRoughness(vm[k], after, scale[k].x);
             } else {
-                creditAlbedo(vm[k], 0, delta.x * after.x * scale[k].x);
-                creditAlbedo(vm[k], 1, delta.y * after.y * scale[k].y);
-                creditAlbedo(vm[k], 2, delta.z * after.z * scale[k].z);
+                // d albedo / d diffuse: the texel (1 untextured); d albedo / d texel: diffuse x the texel's weight.
+                const double w[3] = {delta.x * after.x * scale[k].x, delta.y * after.y * scale[k].y, delta.z * after.z * scale[k].z};
+                const double tv[3] = {texelAt[k].x, texelAt[k].y, texelAt[k].z};
+                const x2_material& M = x.materials[vm[k]];
+                for (int c = 0; c < 3; ++c) {
+                    creditAlbedo(vm[k], c, w[c] * (textured[k] ? tv[c] : 1.0));
+                    if (textured[k] && !g.texture.empty())
+                        for (int i = 0; i < 4; ++i)
+                            if (texWt[k][i] != 0) g.texture[3 * texIdx[k][i] + c] += w[c] * M.diffuse[c] * texWt[k][i];
+                }
             }
         }
         return radiance;

@@ -20,6 +20,7 @@
 #include <cfloat>
 #include <cmath>
 #include <cstdint>
+#include <cstddef>
 #include <cstring>
 #include <memory>
 #include <thread>
@@ -102,6 +103,23 @@ struct Scene {
     std::vector<nanovdb::FloatGrid> floatGrids;
     std::vector<nanovdb::Vec3fGrid> vecGrids;
     std::vector<xi::volume::Grid> grids;
+    // Texture coordinates (2 a vertex; empty: none) and the textures as the reference's images: one level of fp32 RGB
+    // texels (format 0) in 32x32 tile pages, each page's texels row-major at the tile's own width.
+    std::vector<float> uvs;
+    std::vector<xi::tex::Image> images;
+    std::vector<std::vector<const V3*>> pagePointers;
+    std::vector<std::vector<std::vector<V3>>> pages;
+};
+
+// The reference's texture source for its map programs (shadeMaterial's Tex): the scene's images, looked up by
+// texture_core.h's lookup.
+struct OracleTextures {
+    const Scene* s;
+    unsigned lookup(unsigned texture, xi::tex::Binding b, const xi::tex::Footprint& f, V3& out) const {
+        if (texture >= s->images.size()) return xi::tex::Invalid;
+        b.image = &s->images[texture];
+        return xi::tex::lookup(b, f, out);
+    }
 };
 
 // A box's 12 triangles by corner (corner i: hi on x for bit 0, y for bit 1, z for bit 2), each counter-clockwise seen
@@ -249,10 +267,6 @@ bool occluded(const Scene& s, V3 o, V3 d, float tmin, float tmax) {
 }
 
 // ---- the Backend concept (async_integrator.h:52-57), after CpuBackend ----
-struct NoTextures {  // shadeMaterial's texture source: no maps are admitted, so nothing is ever looked up
-    unsigned lookup(unsigned, xi::tex::Binding, const xi::tex::Footprint&, V3&) const { return xi::tex::Invalid; }
-};
-
 struct Counts {
     uint64_t trace = 0, nee = 0, bsdf = 0, held = 0;
 };
@@ -370,7 +384,11 @@ struct OracleBackend {
     bool stateOf(const xi::resume::Hit& h, const xi::surface::Ray& ray, xi::shade::State& st) const {
         const U32 tri = s.meshFirst[h.geom] + h.prim;
         const U32 ia = s.tris[3 * tri], ib = s.tris[3 * tri + 1], ic = s.tris[3 * tri + 2];
-        xi::shade::MeshAttributes attributes;  // no normals, no uvs: the geometric normal and the default st
+        xi::shade::MeshAttributes attributes;  // no normals: the geometric normal; the vertices' uvs when the scene has them
+        if (!s.uvs.empty()) {
+            attributes.uvs = s.uvs.data();
+            attributes.uvRate = xi::shade::RateVertex;
+        }
         if (!xi::shade::hitState(attributes, h.prim, ia, ib, ic, s.vertex(ia), s.vertex(ib), s.vertex(ic), h.u, h.v, h.point,
                                  ray.direction, st))
             return false;
@@ -385,7 +403,7 @@ struct OracleBackend {
     unsigned shade(const xi::resume::Hit& h, const xi::surface::Ray& ray, xi::shade::State& st, xi::shade::Bsdf& bsdf, float& presence) const {
         if (!stateOf(h, ray, st)) return xi::tex::Invalid;
         if (h.geom >= s.records.size()) return xi::tex::Invalid;
-        const NoTextures textures;
+        const OracleTextures textures{&s};
         return xi::shade::shadeMaterial(s.records[h.geom], s.pool.data(), st, textures, bsdf, presence, nullptr, nullptr);
     }
 };
@@ -500,6 +518,91 @@ void* x2ref_open(const x2_scene_desc* d, const x2_config* cfg) {
     s.triGeom.resize(d->triangle_count);
     for (U32 m = 0; m < d->mesh_count; ++m)
         for (U32 t = d->mesh_first[m]; t < d->mesh_first[m + 1]; ++t) s.triGeom[t] = m;
+    // Textures: each a one-level image of 32x32 pages (texture_core.h Mip), and the vertices' uvs.
+    if (d->uvs) s.uvs.assign(d->uvs, d->uvs + 2 * size_t(d->vertex_count));
+    s.images.resize(d->texture_count);
+    s.pagePointers.resize(d->texture_count);
+    s.pages.resize(d->texture_count);
+    for (U32 t = 0; t < d->texture_count; ++t) {
+        const x2_texture& xt = d->textures[t];
+        const U32 T = xi::tex::Tile, nx = (xt.width + T - 1) / T, ny = (xt.height + T - 1) / T;
+        s.pages[t].resize(size_t(nx) * ny);
+        s.pagePointers[t].resize(size_t(nx) * ny);
+        for (U32 ty = 0; ty < ny; ++ty)
+            for (U32 tx = 0; tx < nx; ++tx) {
+                const U32 stride = std::min(T, xt.width - tx * T), rows = std::min(T, xt.height - ty * T);
+                std::vector<V3>& page = s.pages[t][size_t(ty) * nx + tx];
+                page.resize(size_t(stride) * rows);
+                for (U32 y = 0; y < rows; ++y)
+                    for (U32 x = 0; x < stride; ++x) {
+                        const float* v = xt.rgb + 3 * (size_t(ty * T + y) * xt.width + tx * T + x);
+                        page[size_t(y) * stride + x] = V3{v[0], v[1], v[2]};
+                    }
+                s.pagePointers[t][size_t(ty) * nx + tx] = page.data();
+            }
+        xi::tex::Image& img = s.images[t];
+        img.count = 1;
+        img.levels[0].width = xt.width;
+        img.levels[0].height = xt.height;
+        img.levels[0].pages = s.pagePointers[t].data();
+        img.levels[0].tileBase = 0;
+        img.levels[0].format = 0;
+    }
+    // A textured material's map program, once a material: a UsdPrimvarReader of st (mode 2) into register 0, a
+    // UsdUVTexture of the texture at that st (its st bound BindVec2 to register 0) into register 1; the material's
+    // diffuseColor bound BindColor to register 1 (shade_mapnodes.h, shade_maps.h). Returns (program, bindings).
+    auto words = [&](const std::vector<U32>& w) {
+        const U32 at = U32(s.pool.size());
+        for (U32 v : w) {
+            float f;
+            std::memcpy(&f, &v, sizeof(f));
+            s.pool.push_back(f);
+        }
+        return at;
+    };
+    auto floats = [&](const float* f, size_t n) { s.pool.insert(s.pool.end(), f, f + n); };
+    std::vector<std::pair<U32, U32>> programs(d->material_count, {xi::shade::NoMapProgram, 0});
+    for (U32 i = 0; i < d->material_count; ++i) {
+        const x2_material& x = d->materials[i];
+        if (!x.diffuse_texture) continue;
+        namespace sh = xi::shade;
+        const U32 headerFloats = sizeof(sh::MapNodeHeader) / sizeof(float);
+        // The primvar reader.
+        const U32 node0 = U32(s.pool.size());
+        sh::MapNodeHeader h0{};
+        h0.kind = sh::MapUsdPrimvar;
+        h0.reg = 0;
+        h0.paramCount = sizeof(sh::MapUsdPrimvarParams) / sizeof(float);
+        h0.bindingCount = 0;
+        h0.texture = sh::MapNoTexture;
+        floats(reinterpret_cast<const float*>(&h0), headerFloats);
+        sh::MapUsdPrimvarParams q0{};
+        q0.mode = 2.0f;
+        q0.components = 2.0f;
+        floats(reinterpret_cast<const float*>(&q0), h0.paramCount);
+        // The texture.
+        const U32 node1 = U32(s.pool.size());
+        sh::MapNodeHeader h1{};
+        h1.kind = sh::MapUsdUVTexture;
+        h1.reg = 1;
+        h1.paramCount = sizeof(sh::MapUsdUVTextureParams) / sizeof(float);
+        h1.bindingCount = 1;
+        h1.texture = x.diffuse_texture - 1;
+        h1.wrap = d->textures[x.diffuse_texture - 1].wrap;
+        h1.gamma = 0;
+        floats(reinterpret_cast<const float*>(&h1), headerFloats);
+        sh::MapUsdUVTextureParams q1{};
+        q1.output_mode = 0.0f;
+        q1.fallback = sh::Color{1.0f, 1.0f, 1.0f};
+        q1.scale = sh::Color{1.0f, 1.0f, 1.0f};
+        q1.bias = sh::Color{0.0f, 0.0f, 0.0f};
+        floats(reinterpret_cast<const float*>(&q1), h1.paramCount);
+        words({U32(offsetof(sh::MapUsdUVTextureParams, st) / sizeof(float)), U32(sh::BindVec2), 0u});
+        // The program: its nodes in order, then no required attributes.
+        const U32 program = words({2u, node0, node1, 0u});
+        const U32 bindings = words({U32(offsetof(sh::UsdPreviewSurfaceParams, diffuseColor) / sizeof(float)), U32(sh::BindColor), 1u});
+        programs[i] = {program, bindings};
+    }
     // One UsdPreviewSurface record a mesh (its material's parameters in the pool).
     for (U32 m = 0; m < d->mesh_count; ++m) {
         const x2_material& x = d->materials[d->mesh_material[m]];
@@ -523,6 +626,11 @@ void* x2ref_open(const x2_scene_desc* d, const x2_config* cfg) {
         r.count = xi::shade::UsdPreviewSurfaceFloats;
         const float* f = reinterpret_cast<const float*>(&p);
         s.pool.insert(s.pool.end(), f, f + xi::shade::UsdPreviewSurfaceFloats);
+        if (x.diffuse_texture) {
+            r.maps = programs[d->mesh_material[m]].first;
+            r.bindings = programs[d->mesh_material[m]].second;
+            r.bindingCount = 1;
+        }
         s.records.push_back(r);
     }
     for (U32 i = 0; i < d->light_count; ++i) s.lights.push_back(toLight(d->lights[i], i));
@@ -532,6 +640,14 @@ void* x2ref_open(const x2_scene_desc* d, const x2_config* cfg) {
     h->x.lights.assign(d->lights, d->lights + d->light_count);
     h->x.camera = d->camera;
     h->x.config = *cfg;
+    if (d->uvs) h->x.uvs.assign(d->uvs, d->uvs + 2 * size_t(d->vertex_count));
+    for (U32 t = 0; t < d->texture_count; ++t) {
+        const x2_texture& xt = d->textures[t];
+        adj64::Texture64 tx{xt.width, xt.height, xt.wrap, h->x.texels, {}};
+        tx.rgb.assign(xt.rgb, xt.rgb + 3 * size_t(xt.width) * xt.height);
+        h->x.texels += U64(xt.width) * xt.height;
+        h->x.textures.push_back(std::move(tx));
+    }
     // Grids (dense, as the NanoVDB stand-in holds them) and the VdbVolume shaders over them.
     s.gridValues.resize(d->grid_count);
     s.floatGrids.resize(d->grid_count);
@@ -780,7 +896,7 @@ int x2ref_render_tiles_film(void* p, const uint32_t* tiles, uint32_t ntiles, uin
 // magnitudes, in the gradients' order (albedo, roughness, radiance). Requires no volumes and bsdf_samples = 1.
 // Parameters as set with x2ref_set_params (or the scene's own).
 int x2ref_adjoint64(void* p, uint32_t first, uint32_t count, const float* dldi, int threads, double* albedo, double* roughness,
-                    double* radiance, double* image, double* mass) {
+                    double* radiance, double* image, double* mass, double* texture) {
     auto* h = static_cast<Handle*>(p);
     if (!h || !dldi || !albedo || !roughness || !radiance || count == 0) return X2_EINVAL;
     const auto& c = h->x.config;
@@ -797,6 +913,7 @@ int x2ref_adjoint64(void* p, uint32_t first, uint32_t count, const float* dldi, 
         g.albedoMass.assign(3 * M, 0.0);
         g.roughnessMass.assign(M, 0.0);
         g.radianceMass.assign(3 * L, 0.0);
+        if (texture) g.texture.assign(3 * h->x.texels, 0.0);
         for (;;) {
             const U32 px = next.fetch_add(1);
             if (px >= pixels) break;
@@ -820,6 +937,11 @@ int x2ref_adjoint64(void* p, uint32_t first, uint32_t count, const float* dldi, 
     for (U32 i = 0; i < 3 * L; ++i) radiance[i] = 0;
     if (mass)
         for (U32 i = 0; i < 4 * M + 3 * L; ++i) mass[i] = 0;
+    if (texture) {
+        for (U64 i = 0; i < 3 * h->x.texels; ++i) texture[i] = 0;
+        for (const auto& g : per)
+            for (U64 i = 0; i < 3 * h->x.texels; ++i) texture[i] += g.texture[i];
+    }
     for (const auto& g : per) {
         for (U32 i = 0; i < 3 * M; ++i) albedo[i] += g.albedo[i];
         for (U32 i = 0; i < M; ++i) roughness[i] += g.roughness[i];
@@ -829,6 +951,16 @@ int x2ref_adjoint64(void* p, uint32_t first, uint32_t count, const float* dldi, 
         for (U32 i = 0; i < M; ++i) mass[3 * M + i] += g.roughnessMass[i];
         for (U32 i = 0; i < 3 * L; ++i) mass[4 * M + i] += g.radianceMass[i];
     }
+    return X2_OK;
+}
+
+// A texture's texels for the FP64 adjoint (as x2_scene_set_texture sets the engine's); the reference integrator's
+// images are left as they are.
+int x2ref_set_texture(void* p, uint32_t texture, const float* rgb) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h || !rgb || texture >= h->x.textures.size()) return X2_EINVAL;
+    auto& t = h->x.textures[texture];
+    t.rgb.assign(rgb, rgb + 3 * size_t(t.width) * t.height);
     return X2_OK;
 }
 

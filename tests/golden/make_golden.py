@@ -11,6 +11,7 @@ Outputs (small, committed):
   radiance_c0.npz     per-sample Radiance (rgb, alpha) and SampleStatus of seeded (pixel, index) samples of the
   radiance_c108.npz   closed box and of the config-1 scene scaled down by 8, from the reference's integratePaths.
   radiance_c33.npz    the same for the participating medium of config 3, shrunk (a 32^3 grid in the closed box).
+  radiance_c44.npz    the same for the differentiable scene shrunk (config 44: a textured heightfield, UsdUVTexture).
 """
 import json
 import os
@@ -67,4 +68,5 @@ if __name__ == "__main__":
     print("c0", radiance(0, 4096, 11)[1].tolist().count(0), "done of 4096")
     print("c108", radiance(108, 2048, 12)[1].tolist().count(0), "done of 2048")
     print("c33", radiance(33, 2048, 13)[1].tolist().count(0), "done of 2048")
+    print("c44", radiance(44, 4096, 14)[1].tolist().count(0), "done of 4096")
     print("ok")

@@ -170,14 +170,19 @@ def sample_pairs(config, n, seed):
     return pixels, indices
 
 
-def adjoint64(ref, first, count, dldi, threads=None, params=None, masses=False):
+def adjoint64(ref, first, count, dldi, threads=None, params=None, masses=False, texels=0, texture=None):
     """The FP64 CPU adjoint (oracle/adjoint64.h) of samples [first, first + count) of every pixel, given dL/dimage
     (pixels x 3): (albedo grads [materials, 3], roughness grads [materials], radiance grads [lights, 3], image sums
     [pixels, 3]), all FP64, and with `masses` the gradients' credit masses (sums of credit magnitudes) in the same
-    shapes. `params` = (albedo, roughness, radiance) arrays (None entries kept) set first."""
+    shapes. `params` = (albedo, roughness, radiance) arrays (None entries kept) set first; `texture` (an array) sets
+    texture 0's texels first; with `texels` > 0 the texel gradients (texels x 3) come last."""
     lib = ref.lib
     vp = C.c_void_p
-    lib.x2ref_adjoint64.argtypes = [vp, C.c_uint32, C.c_uint32, vp, C.c_int, vp, vp, vp, vp, vp]
+    lib.x2ref_adjoint64.argtypes = [vp, C.c_uint32, C.c_uint32, vp, C.c_int, vp, vp, vp, vp, vp, vp]
+    if texture is not None:
+        t = np.ascontiguousarray(texture, np.float32)
+        lib.x2ref_set_texture.argtypes = [vp, C.c_uint32, vp]
+        assert lib.x2ref_set_texture(ref.h, 0, t.ctypes.data) == 0
     lib.x2ref_adjoint64.restype = C.c_int
     lib.x2ref_set_params.argtypes = [vp, vp, vp, vp]
     lib.x2ref_set_params.restype = C.c_int
@@ -192,10 +197,14 @@ def adjoint64(ref, first, count, dldi, threads=None, params=None, masses=False):
     gr = np.zeros((d[1], 3))
     img = np.zeros((ref.config.width * ref.config.height, 3))
     mass = np.zeros(4 * d[0] + 3 * d[1])
+    tg = np.zeros((texels, 3)) if texels else None
     rc = lib.x2ref_adjoint64(ref.h, first, count, dldi.ctypes.data, threads or os.cpu_count(), ga.ctypes.data, gg.ctypes.data,
-                             gr.ctypes.data, img.ctypes.data, mass.ctypes.data)
+                             gr.ctypes.data, img.ctypes.data, mass.ctypes.data, tg.ctypes.data if texels else None)
     assert rc == 0, rc
+    out = (ga, gg, gr, img)
     if masses:
         M = d[0]
-        return ga, gg, gr, img, (mass[:3 * M].reshape(M, 3), mass[3 * M:4 * M], mass[4 * M:].reshape(-1, 3))
-    return ga, gg, gr, img
+        out = out + ((mass[:3 * M].reshape(M, 3), mass[3 * M:4 * M], mass[4 * M:].reshape(-1, 3)),)
+    if texels:
+        out = out + (tg,)
+    return out

@@ -56,10 +56,13 @@ struct Credits {
     const SceneView& s;
     V3 delta;  // dL/dI of the sample's pixel over its samples
     float* lightSum;  // the thread's light credits (kLightSlots x 3)
-    // The path's vertices by depth: material (~0u: none; kGgxVertex set: GGX), the radiance before it acted, the scale.
+    // The path's vertices by depth: material (~0u: none; kGgxVertex set: GGX), the radiance before it acted, the scale,
+    // a textured Lambert vertex's st and filter.
     uint32_t* material;
     V3* before;
     V3* scale;
+    float4* texc;
+    float* texGrad;
     uint32_t vertices;
 
     __device__ void light(V3 c, uint32_t j) {
@@ -86,10 +89,7 @@ struct Credits {
                 roughness(material[k] & ~kGgxVertex, after, f.x);
                 continue;
             }
-            float* g = partial + at.albedo(material[k]);
-            if (f.x != 0.0f && after.x != 0.0f) atomicAdd(g, delta.x * after.x * f.x);
-            if (f.y != 0.0f && after.y != 0.0f) atomicAdd(g + 1, delta.y * after.y * f.y);
-            if (f.z != 0.0f && after.z != 0.0f) atomicAdd(g + 2, delta.z * after.z * f.z);
+            creditLambert(partial, at, s, material[k], make_float4(delta.x, delta.y, delta.z, 0.0f), after, f, texc + k, texGrad);
         }
     }
 };
@@ -109,7 +109,7 @@ struct AdjointSink {
     float materialRoughness;
     bool ggx, sampled;
 
-    __device__ void vertex(uint32_t m, const Bsdf& b, V3 out) {
+    __device__ void vertex(uint32_t m, const Bsdf& b, V3 out, const TexHit* tex) {
         const bool lambert = b.count && b.lobe.kind == 0;
         ggx = b.count && b.lobe.kind == 1;
         sampled = false;
@@ -118,6 +118,7 @@ struct AdjointSink {
         if (lambert) {
             const V3 a = b.lobe.albedo;
             cr.material[depth] = m;
+            if (tex) cr.texc[depth] = make_float4(tex->s, tex->t, tex->primary ? 1.0f : 0.0f, 0.0f);
             cr.scale[depth] = V3{a.x != 0.0f ? 1.0f / a.x : 0.0f, a.y != 0.0f ? 1.0f / a.y : 0.0f, a.z != 0.0f ? 1.0f / a.z : 0.0f};
         } else if (ggx) {
             cr.material[depth] = m | kGgxVertex;
@@ -156,7 +157,7 @@ struct AdjointSink {
 
 // One sample's replay (the plain megakernel's loop, integrator.cuh's integrate, with the credits).
 __device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, uint32_t index, V3 delta, float* partial, Layout at,
-                                           float* lightSum) {
+                                           float* lightSum, float* texGrad) {
     CameraRay camera;
     if (!cameraRay(s, pixel, index, camera)) return;
     const Identity root{pixel, U64(index), U64(s.config.seed), 0};
@@ -168,7 +169,8 @@ __device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, u
     float alpha = 0.0f;
     uint32_t material[kMaxPathVertices];
     V3 before[kMaxPathVertices], scale[kMaxPathVertices];
-    Credits cr{partial, at, s, delta, lightSum, material, before, scale, 0};
+    float4 texc[kMaxPathVertices];
+    Credits cr{partial, at, s, delta, lightSum, material, before, scale, texc, texGrad, 0};
     while (top) {
         Pending pv = stack[--top];
         if (pv.depth >= kMaxPathVertices) continue;
@@ -195,7 +197,8 @@ __device__ __noinline__ void adjointSample(const SceneView& s, uint32_t pixel, u
 
 // One thread a sample: chunks of 64 x count items (item = chunk * 64 * count + position * count + sample).
 __global__ void __launch_bounds__(128) adjointKernel(SceneView s, const x2_chunk* chunks, uint32_t chunkCount, uint32_t count,
-                                                     const float* dLossdImage, double* gradients, uint32_t materials, uint32_t lights) {
+                                                     const float* dLossdImage, double* gradients, uint32_t materials, uint32_t lights,
+                                                     float* texGrad) {
     extern __shared__ float partial[];
     const Layout at{materials, lights};
     const uint32_t params = 4 * materials + 3 * lights;
@@ -221,7 +224,7 @@ __global__ void __launch_bounds__(128) adjointKernel(SceneView s, const x2_chunk
         const float inv = 1.0f / float(ch.count);
         const V3 delta{dLossdImage[3ull * pixel] * inv, dLossdImage[3ull * pixel + 1] * inv, dLossdImage[3ull * pixel + 2] * inv};
         if (delta.x == 0.0f && delta.y == 0.0f && delta.z == 0.0f) continue;
-        adjointSample(s, pixel, ch.first + sample, delta, partial, at, lightSum);
+        adjointSample(s, pixel, ch.first + sample, delta, partial, at, lightSum, texGrad);
     }
     for (uint32_t j = 0; j < lights && j < kLightSlots; ++j)
         for (int k = 0; k < 3; ++k)

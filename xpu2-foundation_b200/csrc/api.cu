@@ -118,6 +118,10 @@ struct x2_scene {
     uint32_t* meshFirst = nullptr;
     uint32_t* meshMaterial = nullptr;
     MaterialRec* materials = nullptr;
+    TexRec* textures = nullptr;       // the textures (device) and their texels
+    float* texels = nullptr;
+    float* triUV = nullptr;           // scene triangle -> st of its vertices (6 floats), when a material has a texture
+    std::vector<TexRec> hostTextures;
     x2_light* lights = nullptr;
     uint32_t* overflow = nullptr;
     uint32_t lightCount = 0, triangleCount = 0, materialCount = 0;
@@ -177,6 +181,7 @@ struct x2_scene {
     uint32_t* avcount = nullptr;
     float4* adelta = nullptr;
     uint2* aaux = nullptr;
+    float4* atex = nullptr;
     uint32_t adjPaths = 0, adjVerts = 0, adjRecords = 0;
 };
 
@@ -198,6 +203,9 @@ SceneView viewOf(const x2_scene* s) {
     v.grids = s->grids;
     v.volumeTris = s->volumeTris;
     v.gridCount = s->gridCount;
+    v.textures = s->textures;
+    v.texels = s->texels;
+    v.triUV = s->triUV;
     return v;
 }
 
@@ -325,6 +333,10 @@ __global__ void addInto(double* dst, const double* src, uint32_t n) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) dst[i] += src[i];
 }
+__global__ void addFloatInto(double* dst, const float* src, uint64_t n) {
+    const uint64_t i = uint64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] += double(src[i]);
+}
 
 // The scene's device view, stream and device for entry points in other translation units (noalloc.cu).
 int sceneView(x2_scene* s, SceneView* view, cudaStream_t* stream, int* device, int* smCount) {
@@ -449,6 +461,10 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
             setError("material %u: unknown kind %u", i, m.kind);
             return X2_EINVAL;
         }
+        if (m.diffuse_texture > d->texture_count) {
+            setError("material %u: texture %u of %u", i, m.diffuse_texture - 1, d->texture_count);
+            return X2_EINVAL;
+        }
         if (m.kind == X2_MAT_GGX) {
             const bool specBlack = m.specular[0] <= 1e-6f && m.specular[1] <= 1e-6f && m.specular[2] <= 1e-6f;
             const bool diffBlack = m.diffuse[0] <= 1e-6f && m.diffuse[1] <= 1e-6f && m.diffuse[2] <= 1e-6f;
@@ -460,6 +476,13 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
                 setError("material %u: a mirror (roughness 0) is not admitted", i);
                 return X2_EINVAL;
             }
+        }
+    }
+    for (uint32_t i = 0; i < d->texture_count; ++i) {
+        const x2_texture& t = d->textures[i];
+        if (!d->textures || !t.rgb || t.width == 0 || t.height == 0 || t.wrap > 1 || uint64_t(t.width) * t.height > (1ull << 28)) {
+            setError("texture %u: %ux%u texels (at most 2^28), wrap %u (0 or 1)", i, t.width, t.height, t.wrap);
+            return X2_EINVAL;
         }
     }
     for (uint32_t i = 0; i < d->light_count; ++i) {
@@ -541,7 +564,10 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
             mats[i].emission[k] = m.emission[k];
         }
         mats[i].roughness = m.roughness;
+        mats[i].texture = m.diffuse_texture;
     }
+    bool textured = false;
+    for (uint32_t i = 0; i < d->material_count; ++i) textured = textured || d->materials[i].diffuse_texture != 0;
     cudaEvent_t b0, b1;
     cudaEventCreate(&b0);
     cudaEventCreate(&b1);
@@ -574,6 +600,40 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
     if (d->light_count) cudaMemcpyAsync(s->lights, d->lights, sizeof(x2_light) * d->light_count, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(s->overflow, 0, sizeof(uint32_t), st);
     cudaMemsetAsync(s->stats, 0, 2 * sizeof(TraversalStats), st);
+    // Textures: every texture's texels in one array; each triangle's vertices' st (hitState's st1..st3: the vertices'
+    // uvs, or the default (0,0), (1,0), (1,1) of a mesh without them), when a material reads a texture.
+    if (d->texture_count) {
+        uint64_t total = 0;
+        s->hostTextures.resize(d->texture_count);
+        for (uint32_t i = 0; i < d->texture_count; ++i) {
+            s->hostTextures[i] = TexRec{total, d->textures[i].width, d->textures[i].height, d->textures[i].wrap, 0};
+            total += uint64_t(d->textures[i].width) * d->textures[i].height;
+        }
+        if (cudaMalloc(&s->textures, sizeof(TexRec) * d->texture_count) != cudaSuccess ||
+            cudaMalloc(&s->texels, sizeof(float) * 3 * total) != cudaSuccess) {
+            setError("device allocation failed for %llu texels", (unsigned long long)total);
+            return fail(X2_ENOMEM);
+        }
+        cudaMemcpyAsync(s->textures, s->hostTextures.data(), sizeof(TexRec) * d->texture_count, cudaMemcpyHostToDevice, st);
+        for (uint32_t i = 0; i < d->texture_count; ++i)
+            cudaMemcpyAsync(s->texels + 3 * s->hostTextures[i].first, d->textures[i].rgb,
+                            sizeof(float) * 3 * size_t(d->textures[i].width) * d->textures[i].height, cudaMemcpyHostToDevice, st);
+    }
+    if (textured) {
+        std::vector<float> uv(size_t(d->triangle_count) * 6);
+        for (uint32_t t = 0; t < d->triangle_count; ++t)
+            for (int k = 0; k < 3; ++k) {
+                const uint32_t v = d->triangles[3 * t + k];
+                uv[6 * size_t(t) + 2 * k] = d->uvs ? d->uvs[2 * size_t(v)] : (k == 0 ? 0.0f : 1.0f);
+                uv[6 * size_t(t) + 2 * k + 1] = d->uvs ? d->uvs[2 * size_t(v) + 1] : (k == 2 ? 1.0f : 0.0f);
+            }
+        if (cudaMalloc(&s->triUV, sizeof(float) * uv.size()) != cudaSuccess) {
+            setError("device allocation failed for the triangles' st");
+            return fail(X2_ENOMEM);
+        }
+        cudaMemcpyAsync(s->triUV, uv.data(), sizeof(float) * uv.size(), cudaMemcpyHostToDevice, st);
+        CUDA_OR(cudaStreamSynchronize(st), fail(X2_ECUDA));
+    }
     // Volumes: their records, their bounds' twelve triangles each (the oracle's table), their grids' values.
     s->volumeCount = d->volume_count;
     s->gridCount = d->grid_count;
@@ -651,6 +711,8 @@ void freeAdjointWave(x2_scene* s) {
     cudaFree(s->avcount);
     cudaFree(s->adelta);
     cudaFree(s->aaux);
+    cudaFree(s->atex);
+    s->atex = nullptr;
     s->avert = nullptr;
     s->ascale = nullptr;
     s->avcount = nullptr;
@@ -670,6 +732,9 @@ int x2_scene_free(x2_scene* s) {
     cudaFree(s->meshFirst);
     cudaFree(s->meshMaterial);
     cudaFree(s->materials);
+    cudaFree(s->textures);
+    cudaFree(s->texels);
+    cudaFree(s->triUV);
     cudaFree(s->lights);
     cudaFree(s->overflow);
     cudaFree(s->auditWord);
@@ -1257,13 +1322,33 @@ int x2_scene_set_params(x2_scene* s, const float* albedo, const float* roughness
     return X2_OK;
 }
 
+int x2_scene_set_texture(x2_scene* s, uint32_t texture, const float* rgb) {
+    if (!s || !rgb || texture >= s->hostTextures.size()) {
+        setError("x2_scene_set_texture: texture %u of %zu", texture, s ? s->hostTextures.size() : size_t(0));
+        return X2_EINVAL;
+    }
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    const TexRec& t = s->hostTextures[texture];
+    cudaStream_t st = s->ctx->stream;
+    CUDA_OR(cudaMemcpyAsync(s->texels + 3 * t.first, rgb, sizeof(float) * 3 * size_t(t.width) * t.height, cudaMemcpyHostToDevice, st), X2_ECUDA);
+    CUDA_OR(cudaStreamSynchronize(st), X2_ECUDA);
+    return X2_OK;
+}
+
 // The adjoint of a frame's samples [first, first + count) of every pixel: gradients of a loss with respect to each
 // material's albedo and roughness and each light's radiance, given the loss's derivative with respect to the image
 // (device, 3 floats a pixel, the image being the film's mean). Device outputs (FP64), added to; a null roughness
 // output skips that set.
 // The replay in the plain megakernel's form (one thread a sample): x2_adjoint's arguments and results.
+// The texel count of the scene's textures (3 gradients each).
+uint64_t texelCount(const x2_scene* s) {
+    uint64_t n = 0;
+    for (const TexRec& t : s->hostTextures) n += uint64_t(t.width) * t.height;
+    return n;
+}
+
 int x2_adjoint_plain(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad,
-                     double* d_roughness_grad, double* d_radiance_grad) {
+                     double* d_roughness_grad, double* d_radiance_grad, double* d_texture_grad) {
     if (!s || !s->configured || !d_dloss_dimage || !d_albedo_grad || !d_radiance_grad || count == 0) {
         setError("x2_adjoint: configured scene, device arrays and a sample count");
         return X2_EINVAL;
@@ -1285,31 +1370,37 @@ int x2_adjoint_plain(x2_scene* s, uint32_t first, uint32_t count, const float* d
     for (uint32_t t = 0; t < tiles; ++t) chunks[t] = x2_chunk{t, first, count, 0};
     x2_chunk* d = nullptr;
     double* grads = nullptr;
+    float* texGrad = nullptr;
+    const uint64_t texGrads = d_texture_grad ? 3 * texelCount(s) : 0;
     CUDA_OR(cudaMalloc(&d, sizeof(x2_chunk) * tiles), X2_ENOMEM);
-    if (cudaMalloc(&grads, sizeof(double) * params) != cudaSuccess) {
+    if (cudaMalloc(&grads, sizeof(double) * params) != cudaSuccess || (texGrads && cudaMalloc(&texGrad, sizeof(float) * texGrads) != cudaSuccess)) {
         cudaFree(d);
+        cudaFree(grads);
         setError("x2_adjoint: allocation failed");
         return X2_ENOMEM;
     }
+    if (texGrads) cudaMemsetAsync(texGrad, 0, sizeof(float) * texGrads, s->ctx->stream);
     cudaMemcpyAsync(d, chunks.data(), sizeof(x2_chunk) * tiles, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(grads, 0, sizeof(double) * params, st);
     const size_t shared = sizeof(float) * params;
     if (shared > 48 * 1024) cudaFuncSetAttribute(adjointKernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shared));
     SceneView v = viewOf(s);
     v.stats = nullptr;
-    adjointKernel<<<s->ctx->smCount * 8, 128, shared, st>>>(v, d, tiles, count, d_dloss_dimage, grads, s->materialCount, s->lightCount);
+    adjointKernel<<<s->ctx->smCount * 8, 128, shared, st>>>(v, d, tiles, count, d_dloss_dimage, grads, s->materialCount, s->lightCount, texGrad);
     int rc = cudaGetLastError() == cudaSuccess ? X2_OK : X2_ECUDA;
     if (!rc) {
         // Added to the caller's arrays: albedo, roughness, radiance.
         addInto<<<(params + 255) / 256, 256, 0, st>>>(d_albedo_grad, grads, 3 * s->materialCount);
         if (d_roughness_grad) addInto<<<(params + 255) / 256, 256, 0, st>>>(d_roughness_grad, grads + 3 * s->materialCount, s->materialCount);
         addInto<<<(params + 255) / 256, 256, 0, st>>>(d_radiance_grad, grads + 4 * s->materialCount, 3 * s->lightCount);
+        if (texGrads) addFloatInto<<<unsigned((texGrads + 255) / 256), 256, 0, st>>>(d_texture_grad, texGrad, texGrads);
         rc = x2_synchronize(s->ctx, 600000);
     } else {
         setError("x2_adjoint: launch failed");
     }
     cudaFree(d);
     cudaFree(grads);
+    cudaFree(texGrad);
     return rc;
 }
 
@@ -1317,7 +1408,7 @@ int x2_adjoint_plain(x2_scene* s, uint32_t first, uint32_t count, const float* d
 // sort, shade, shadow; the adjoint forms of logic and shade credit as they go), as one graph of iterations replayed
 // until no path is left; the gradient rows then summed into FP64 and added to the caller's arrays.
 int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss_dimage, double* d_albedo_grad, double* d_roughness_grad,
-               double* d_radiance_grad) {
+               double* d_radiance_grad, double* d_texture_grad) {
     if (!s || !s->configured || !d_dloss_dimage || !d_albedo_grad || !d_radiance_grad || count == 0) {
         setError("x2_adjoint: configured scene, device arrays and a sample count");
         return X2_EINVAL;
@@ -1351,7 +1442,8 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
         const bool ok = cudaMalloc(&s->avert, sizeof(uint4) * V) == cudaSuccess && cudaMalloc(&s->ascale, sizeof(float4) * V) == cudaSuccess &&
                         cudaMalloc(&s->avcount, sizeof(uint32_t) * paths) == cudaSuccess &&
                         cudaMalloc(&s->adelta, sizeof(float4) * paths) == cudaSuccess &&
-                        cudaMalloc(&s->aaux, sizeof(uint2) * size_t(paths) * records) == cudaSuccess;
+                        cudaMalloc(&s->aaux, sizeof(uint2) * size_t(paths) * records) == cudaSuccess &&
+                        (!s->triUV || cudaMalloc(&s->atex, sizeof(float4) * V) == cudaSuccess);
         if (!ok) {
             freeAdjointWave(s);
             setError("x2_adjoint: device allocation failed for %u paths", paths);
@@ -1366,8 +1458,12 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     constexpr uint32_t kRows = 1024;
     float* rows = nullptr;
     double* grads = nullptr;
-    if (cudaMalloc(&rows, sizeof(float) * size_t(kRows) * params) != cudaSuccess || cudaMalloc(&grads, sizeof(double) * params) != cudaSuccess) {
+    float* texGrad = nullptr;
+    const uint64_t texGrads = d_texture_grad ? 3 * texelCount(s) : 0;
+    if (cudaMalloc(&rows, sizeof(float) * size_t(kRows) * params) != cudaSuccess || cudaMalloc(&grads, sizeof(double) * params) != cudaSuccess ||
+        (texGrads && cudaMalloc(&texGrad, sizeof(float) * texGrads) != cudaSuccess)) {
         cudaFree(rows);
+        cudaFree(grads);
         setError("x2_adjoint: allocation failed");
         return X2_ENOMEM;
     }
@@ -1377,6 +1473,7 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     cudaMemcpyAsync(sl.chunks, chunks.data(), sizeof(x2_chunk) * tiles, cudaMemcpyHostToDevice, st);
     cudaMemsetAsync(rows, 0, sizeof(float) * size_t(kRows) * params, st);
     cudaMemsetAsync(grads, 0, sizeof(double) * params, st);
+    if (texGrads) cudaMemsetAsync(texGrad, 0, sizeof(float) * texGrads, st);
     cudaMemsetAsync(s->wave.state, 0, sizeof(uint32_t) * paths, st);
     cudaMemsetAsync(s->wave.ncount, 0, sizeof(uint32_t) * paths, st);
     cudaMemsetAsync(s->claimed, 0, sizeof(unsigned long long), st);
@@ -1411,7 +1508,8 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     a.chunkRequest = nullptr;
     a.chunkItems = nullptr;
     a.chunkCount = tiles;
-    a.adj = AdjointWave{d_dloss_dimage, rows, kRows, s->materialCount, s->lightCount, verts, s->avert, s->ascale, s->avcount, s->adelta, s->aaux};
+    a.adj = AdjointWave{d_dloss_dimage, rows, kRows, s->materialCount, s->lightCount, verts, s->avert, s->ascale, s->avcount, s->adelta, s->aaux,
+                        s->atex, texGrad};
     const size_t shared = sizeof(float) * params;
     if (shared > 48 * 1024) {
         cudaFuncSetAttribute(wfLogicAdjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shared));
@@ -1467,10 +1565,12 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
         addInto<<<(params + 255) / 256, 256, 0, st>>>(d_albedo_grad, grads, 3 * s->materialCount);
         if (d_roughness_grad) addInto<<<(params + 255) / 256, 256, 0, st>>>(d_roughness_grad, grads + 3 * s->materialCount, s->materialCount);
         addInto<<<(params + 255) / 256, 256, 0, st>>>(d_radiance_grad, grads + 4 * s->materialCount, 3 * s->lightCount);
+        if (texGrads) addFloatInto<<<unsigned((texGrads + 255) / 256), 256, 0, st>>>(d_texture_grad, texGrad, texGrads);
         rc = cudaGetLastError() == cudaSuccess ? x2_synchronize(s->ctx, 600000) : X2_ECUDA;
     }
     cudaFree(rows);
     cudaFree(grads);
+    cudaFree(texGrad);
     return rc;
 }
 

@@ -51,4 +51,34 @@ __device__ __forceinline__ float ggxLogDerivative(const Lobe& l, float materialR
     return float(dlogf * 2.0 * r);
 }
 
+// A Lambert vertex's credit from what its path gathered after it (`after`), its scale 1 / albedo: to its material's
+// diffuse colour (d albedo / d diffuse = the texel of a textured one, else 1) and, textured, to the texels its lookup
+// read (d albedo / d texel = diffuse x the texel's weight), those as FP32 atomics into texGrad.
+__device__ __forceinline__ void creditLambert(float* partial, const Layout& at, const SceneView& s, uint32_t m, float4 d, V3 after, V3 sc,
+                                              const float4* texc, float* texGrad) {
+    const MaterialRec& mr = s.materials[m];
+    const float w[3] = {d.x * after.x * sc.x, d.y * after.y * sc.y, d.z * after.z * sc.z};
+    V3 texel{1, 1, 1};
+    uint64_t ti[4];
+    float tw[4];
+    bool textured = false;
+    if (mr.texture && texc) {
+        const float4 tc = *texc;
+        TexHit th;
+        th.s = tc.x;
+        th.t = tc.y;
+        th.primary = tc.z != 0.0f ? 1u : 0u;
+        textured = texLookup(s, mr.texture - 1, th, ti, tw);
+        if (textured) texel = th.texel;
+    }
+    const float tv[3] = {texel.x, texel.y, texel.z};
+    for (int c = 0; c < 3; ++c) {
+        if (w[c] == 0.0f) continue;
+        atomicAdd(partial + at.albedo(m) + c, w[c] * tv[c]);
+        if (textured && texGrad)
+            for (int i = 0; i < 4; ++i)
+                if (tw[i] != 0.0f) atomicAdd(texGrad + 3 * ti[i] + c, w[c] * mr.diffuse[c] * tw[i]);
+    }
+}
+
 }  // namespace x2

@@ -183,10 +183,23 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
     if (!hitState(va, vb, vc, hit.u, hit.v, hit.point, pv.dir, st)) return false;
     Bsdf bsdf;
     const uint32_t material = __ldg(s.meshMaterial + hit.geom);
-    shadeMaterial(s.materials[material], st, bsdf);
+    const MaterialRec& mr = s.materials[material];
+    TexHit th;
+    th.primary = 0;
+    if (mr.texture) {
+        // The hit's st (hitState, shade_material.h:142-153: w st1 + u st2 + v st3) and the texture's lookup there; the
+        // path type picks the filter (PathPrimary: no diffuse, glossy or mirror bounce yet, async_integrator.h:2222).
+        const float* uv = s.triUV + 6ull * (__ldg(s.meshFirst + hit.geom) + hit.prim);
+        const float w = 1.0f - hit.u - hit.v;
+        th.s = w * uv[0] + hit.u * uv[2] + hit.v * uv[4];
+        th.t = w * uv[1] + hit.u * uv[3] + hit.v * uv[5];
+        th.primary = pv.diffuse == 0 && pv.glossy == 0 && pv.mirror == 0;
+        if (!texLookup(s, mr.texture - 1, th)) return false;
+    }
+    shadeMaterial(mr, st, bsdf, mr.texture ? th.texel : V3{1, 1, 1});
     if (pv.depth == 0) alpha += 1.0f * (1.0f - (0.0f + 0.0f + 0.0f) / 3.0f);
     radiance = add(radiance, mulv(pv.T, bsdf.emission));
-    sink.vertex(material, bsdf, st.wo);  // the vertex, its emission added: what comes after passes its lobe
+    sink.vertex(material, bsdf, st.wo, mr.texture ? &th : nullptr);  // the vertex, its emission added: what comes after passes its lobe
     if (bsdf.count == 0) return true;
 
     uint32_t indirectFlags = 0;
@@ -429,7 +442,7 @@ struct PlainSink {
         if (visible(s, q.origin, q.dir, q.near, q.far)) radiance = add(radiance, q.contribution);
     }
     __device__ void held() { ++out.held; }
-    __device__ void vertex(uint32_t, const Bsdf&, V3) {}
+    __device__ void vertex(uint32_t, const Bsdf&, V3, const TexHit*) {}
     __device__ uint32_t top(uint32_t) const { return size; }
     __device__ void push(const Pending& p) { stack[size++] = p; }
 };

@@ -66,6 +66,9 @@ struct Holder {
     std::vector<x2_volume> volumes;
     std::vector<x2_grid> grids;
     std::vector<std::vector<float>> gridValues;
+    std::vector<float> uvs;  // 2 a vertex when a mesh has texture coordinates (then every vertex has them)
+    std::vector<x2_texture> textures;
+    std::vector<std::vector<float>> textureValues;
 
     uint32_t vertex(V p) {
         vertices.push_back(p.x);
@@ -111,6 +114,10 @@ struct Holder {
         desc.grid_count = uint32_t(grids.size());
         desc.volumes = volumes.data();
         desc.grids = grids.data();
+        for (size_t t = 0; t < textures.size(); ++t) textures[t].rgb = textureValues[t].data();
+        desc.texture_count = uint32_t(textures.size());
+        desc.textures = textures.data();
+        desc.uvs = uvs.empty() ? nullptr : uvs.data();
     }
 };
 
@@ -332,7 +339,7 @@ x2_material randomMaterial(Rng& r) {
 }
 
 Holder* makeField(uint64_t seed, int tilesPerSide, int spheres, int icoLevel, uint32_t width, uint32_t height, uint32_t spp,
-                  uint32_t depth, x2_config* cfg) {
+                  uint32_t depth, x2_config* cfg, float radiusScale = 1.0f) {
     auto* h = new Holder();
     Rng r(seed);
     const int quadsPerTile = 16, n = tilesPerSide * quadsPerTile;
@@ -363,7 +370,7 @@ Holder* makeField(uint64_t seed, int tilesPerSide, int spheres, int icoLevel, ui
     icosphere(icoLevel, unitVerts, unitFaces);
     for (int s = 0; s < spheres; ++s) {
         const V c{r.uniform(-10.0f, 10.0f), r.uniform(0.0f, 4.0f), r.uniform(-10.0f, 10.0f)};
-        const float radius = float(0.05 * std::exp(r.uniform() * std::log(10.0)));
+        const float radius = radiusScale * float(0.05 * std::exp(r.uniform() * std::log(10.0)));
         h->beginMesh(h->material(randomMaterial(r)));
         const uint32_t b = uint32_t(h->vertices.size() / 3);
         for (const V& v : unitVerts) h->vertex(c + v * radius);
@@ -551,14 +558,45 @@ Holder* makeVolumeBox(uint64_t seed, int n, uint32_t width, uint32_t height, uin
     return h;
 }
 
-// The differentiable scene (config 4): config 1's construction reduced to about 250k triangles (16x16 heightfield
-// tiles, 23 level-4 icospheres) with its meshes sharing a pool of 64 materials (mesh m takes material m mod 64), so
-// each material's parameters are shared by many surfaces; 512x512.
-Holder* makeAdjointField(uint64_t seed, int tiles, int spheres, uint32_t width, uint32_t height, uint32_t spp, uint32_t depth, x2_config* cfg) {
-    Holder* h = makeField(seed, tiles, spheres, 4, width, height, spp, depth, cfg);
-    const uint32_t pool = std::min<uint32_t>(64u, uint32_t(h->materials.size()));
-    h->materials.resize(pool);
-    for (size_t m = 0; m < h->meshMaterial.size(); ++m) h->meshMaterial[m] = uint32_t(m % pool);
+// The differentiable scene (config 4): config 1's construction reduced to about 250k triangles (18x18 heightfield
+// tiles of 16x16 quads, 64 level-3 icospheres), the heightfield's meshes sharing one Lambert material whose diffuse
+// colour is a texture (an fp32 RGB texture of `texels` x `texels` from seeded 4-octave colour fBm in [0.05, 0.9],
+// periodic, over the heightfield's uvs: vertex (i, j) of its (n+1)^2 grid at (i/n, j/n)), the icospheres each one
+// of a pool of `spheres` materials (sphere k takes material k). 512x512. (Config 44, the tests' shrunk copy, makes its
+// icospheres three times larger so that their materials cover enough pixels for finite differences.)
+Holder* makeAdjointField(uint64_t seed, int tiles, int spheres, int icoLevel, uint32_t texels, uint32_t width, uint32_t height, uint32_t spp,
+                         uint32_t depth, x2_config* cfg, float radiusScale = 1.0f) {
+    Holder* h = makeField(seed, tiles, spheres, icoLevel, width, height, spp, depth, cfg, radiusScale);
+    const uint32_t tileMeshes = uint32_t(tiles * tiles);
+    // The icospheres' own materials (each made after its heightfield tiles' by makeField) become the pool.
+    std::vector<x2_material> pool(h->materials.begin() + tileMeshes, h->materials.end());
+    x2_material textured = lambert(1.0f, 1.0f, 1.0f);
+    textured.diffuse_texture = 1;
+    pool.push_back(textured);
+    h->materials = pool;
+    for (size_t m = 0; m < h->meshMaterial.size(); ++m)
+        h->meshMaterial[m] = m < tileMeshes ? uint32_t(pool.size() - 1) : uint32_t(m - tileMeshes);
+    const int n = tiles * 16;
+    h->uvs.assign(h->vertices.size() / 3 * 2, 0.0f);
+    for (int j = 0; j <= n; ++j)
+        for (int i = 0; i <= n; ++i) {
+            const size_t v = size_t(j) * (n + 1) + i;
+            h->uvs[2 * v] = float(i) / float(n);
+            h->uvs[2 * v + 1] = float(j) / float(n);
+        }
+    x2_texture t{};
+    t.width = t.height = texels;
+    t.wrap = 1;
+    std::vector<float> rgb(size_t(texels) * texels * 3);
+    for (uint32_t y = 0; y < texels; ++y)
+        for (uint32_t x = 0; x < texels; ++x)
+            for (int c = 0; c < 3; ++c) {
+                const float u = 8.0f * float(x) / float(texels), v = 8.0f * float(y) / float(texels);
+                const float f = fbm(u, v, 4, uint32_t(seed) + 31u * uint32_t(c + 1));
+                rgb[(size_t(y) * texels + x) * 3 + c] = std::min(0.9f, std::max(0.05f, 0.475f + 0.6f * f));
+            }
+    h->textures.push_back(t);
+    h->textureValues.push_back(std::move(rgb));
     const x2_camera cam = h->desc.camera;
     h->finish();
     h->desc.camera = cam;
@@ -624,9 +662,9 @@ extern "C" int x2_scene_generate(uint32_t config_id, uint64_t seed, x2_scene_des
         } else if (config_id == 11) {
             h = makeField(seed, 32, 2000, 2, 1920, 1080, 64, 12, config);
         } else if (config_id == 4) {
-            h = makeAdjointField(seed, 16, 23, 512, 512, 32, 12, config);
+            h = makeAdjointField(seed, 18, 64, 3, 1024, 512, 512, 32, 12, config);
         } else if (config_id == 44) {
-            h = makeAdjointField(seed, 4, 3, 64, 64, 4, 6, config);
+            h = makeAdjointField(seed, 4, 32, 2, 64, 64, 64, 4, 6, config, 3.0f);
         } else if (config_id == 3) {
             h = makeVolumeBox(seed, 256, 512, 512, 256, 64, config);
         } else if (config_id == 33) {

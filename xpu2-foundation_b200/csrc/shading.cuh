@@ -78,6 +78,12 @@ __device__ __forceinline__ uint32_t lobeRayMask(uint32_t t) {
 struct MaterialRec {
     uint32_t kind;
     float diffuse[3], specular[3], emission[3], roughness;
+    uint32_t texture;  // 0: none; k + 1: texture k bound to the diffuse colour
+};
+// A texture on the device: fp32 RGB texels (3 floats each, row-major, row 0 the top) from `first` texel on.
+struct TexRec {
+    uint64_t first;
+    uint32_t width, height, wrap, pad;
 };
 struct Counters {
     unsigned long long trace, nee, bsdf, held, samples, errors, overflow, pad;
@@ -111,6 +117,9 @@ struct SceneView {
     x2_config config;
     uint32_t* overflow;             // traversal stack overflows
     TraversalStats* stats;          // a counting run's traversal work ([0] closest hits, [1] any hits); null when timed
+    const TexRec* textures;         // the scene's textures and their texels (null without textures)
+    const float* texels;
+    const float* triUV;             // scene triangle -> its vertices' st (6 floats); null: no texture is read
 };
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -322,21 +331,88 @@ struct Bsdf {
     Lobe lobe;
 };
 __device__ __forceinline__ float saturate(float x) { return fminf(fmaxf(x, 0.0f), 1.0f); }
+// ---------------------------------------------------------------------------------------------------------------
+// Textures: UsdUVTexture's lookup (shade_mapnodes.h:972-997) with no filter footprint — texture_core.h lookup at
+// (s, 1 - t): level 0 only; on primary paths the anisotropic filter reduces to one bilinear lookup, on indirect paths
+// (trilinear and one-level modes) to the closest texel (textureMode, shade_mapnodes.h:344-347).
+struct TexHit {
+    float s, t;       // the hit's st (hitState's interpolation of the vertices' uvs)
+    uint32_t primary; // 1: a primary path (bilinear), 0: indirect (closest texel)
+    V3 texel;         // the lookup's value
+};
+__device__ __forceinline__ int texAddress(int x, int n, uint32_t wrap) {
+    if (wrap) {
+        const int v = x % n;
+        return v < 0 ? v + n : v;
+    }
+    return x < 0 ? 0 : x >= n ? n - 1 : x;
+}
+__device__ __forceinline__ V3 texFetch(const SceneView& s, const TexRec& t, int x, int y) {
+    const float* p = s.texels + 3 * (t.first + uint64_t(texAddress(y, int(t.height), t.wrap)) * t.width + uint64_t(texAddress(x, int(t.width), t.wrap)));
+    return V3{__ldg(p), __ldg(p + 1), __ldg(p + 2)};
+}
+// The lookup's texels and weights (up to 4: bilinear x, x+1 over y, y+1; closest: 1), its value in `out`. False where
+// the reference's lookup is Invalid (a non-finite or far coordinate or value).
+__device__ __forceinline__ bool texLookup(const SceneView& s, uint32_t texture, TexHit& h, uint64_t* texels = nullptr, float* weights = nullptr) {
+    const TexRec tr = s.textures[texture];
+    float u = 1.0f * h.s + 0.0f, v = 1.0f - (1.0f * h.t + 0.0f);
+    if (!finitef(u) || !finitef(v)) return false;
+    if (fabsf(u) > 1024) u = tr.wrap ? u - floorf(u) : fminf(fmaxf(u, -1.0f), 2.0f);
+    if (fabsf(v) > 1024) v = tr.wrap ? v - floorf(v) : fminf(fmaxf(v, -1.0f), 2.0f);
+    float fx = u * float(tr.width) - .5f, fy = v * float(tr.height) - .5f;
+    if (!finitef(fx) || !finitef(fy) || fabsf(fx) > 1.e8f || fabsf(fy) > 1.e8f) return false;
+    int x = int(floorf(fx)), y = int(floorf(fy));
+    auto index = [&](int xx, int yy) {
+        return tr.first + uint64_t(texAddress(yy, int(tr.height), tr.wrap)) * tr.width + uint64_t(texAddress(xx, int(tr.width), tr.wrap));
+    };
+    if (h.primary) {
+        fx -= float(x);
+        fy -= float(y);
+        const V3 a = texFetch(s, tr, x, y), b = texFetch(s, tr, x + 1, y), c = texFetch(s, tr, x, y + 1), d = texFetch(s, tr, x + 1, y + 1);
+        h.texel = add(mul(add(mul(a, 1 - fx), mul(b, fx)), 1 - fy), mul(add(mul(c, 1 - fx), mul(d, fx)), fy));
+        if (texels) {
+            texels[0] = index(x, y);
+            texels[1] = index(x + 1, y);
+            texels[2] = index(x, y + 1);
+            texels[3] = index(x + 1, y + 1);
+            weights[0] = (1 - fx) * (1 - fy);
+            weights[1] = fx * (1 - fy);
+            weights[2] = (1 - fx) * fy;
+            weights[3] = fx * fy;
+        }
+    } else {
+        if (fx - float(x) > .5f) ++x;
+        if (fy - float(y) > .5f) ++y;
+        h.texel = texFetch(s, tr, x, y);
+        if (texels) {
+            texels[0] = index(x, y);
+            weights[0] = 1.0f;
+            for (int k = 1; k < 4; ++k) {
+                texels[k] = texels[0];
+                weights[k] = 0.0f;
+            }
+        }
+    }
+    return finite3(h.texel);
+}
+
 // The lobe shadeMaterial makes for a material: 1 a GGX lobe, 0 a Lambert lobe, 2 none (the wavefront's per-lobe
 // queues sort paths by it before shading).
 __device__ __forceinline__ uint32_t lobeClass(const MaterialRec& m) {
     if (m.kind == X2_MAT_GGX && !isBlack(V3{saturate(m.specular[0]), saturate(m.specular[1]), saturate(m.specular[2])})) return 1;
     return isBlack(V3{m.diffuse[0], m.diffuse[1], m.diffuse[2]}) ? 2 : 0;
 }
-// shadeUsdPreviewSurface with useSpecularWorkflow = 1 (shade_material.h:338-383).
-__device__ __forceinline__ void shadeMaterial(const MaterialRec& m, const State& st, Bsdf& b) {
+// shadeUsdPreviewSurface with useSpecularWorkflow = 1 (shade_material.h:338-383); a textured material's diffuse colour
+// times its texel when not black (the map binding's BindColor rule, shade_maps.h applyRule).
+__device__ __forceinline__ void shadeMaterial(const MaterialRec& m, const State& st, Bsdf& b, V3 texel = V3{1, 1, 1}) {
     b.count = 0;
     b.type = 0;
     b.emission = V3{0, 0, 0};
     V3 N;
     if (fabsf(length(st.dPds)) <= kEpsilon) N = st.N;
     else N = normalizeU(localToGlobal(frameNT(st.N, normalizeU(st.dPds)), V3{0, 0, 1}));
-    const V3 albedo{m.diffuse[0], m.diffuse[1], m.diffuse[2]};
+    V3 albedo{m.diffuse[0], m.diffuse[1], m.diffuse[2]};
+    if (m.texture && !isBlack(albedo)) albedo = mulv(albedo, texel);
     const float roughness = saturate(m.roughness);
     const V3 emissive{m.emission[0], m.emission[1], m.emission[2]};
     if (!isBlack(emissive)) b.emission = add(b.emission, emissive);

@@ -238,9 +238,7 @@ __device__ __forceinline__ void logicBody(const WaveArgs& a) {
                         creditRoughnessTo(partial, at, m, d, after, sc.x);
                         continue;
                     }
-                    if (sc.x != 0.0f && after.x != 0.0f) atomicAdd(partial + at.albedo(m), d.x * after.x * sc.x);
-                    if (sc.y != 0.0f && after.y != 0.0f) atomicAdd(partial + at.albedo(m) + 1, d.y * after.y * sc.y);
-                    if (sc.z != 0.0f && after.z != 0.0f) atomicAdd(partial + at.albedo(m) + 2, d.z * after.z * sc.z);
+                    creditLambert(partial, at, a.scene, m, d, after, V3{sc.x, sc.y, sc.z}, a.adj.tex ? &a.adj.tex[vk] : nullptr, a.adj.texGrad);
                 }
             }
             if (st == kDone || st == kError) {
@@ -412,7 +410,7 @@ struct WaveSink {
         }
     }
     __device__ void held() { ++nHeld; }
-    __device__ void vertex(uint32_t m, const Bsdf& b, V3 out) {
+    __device__ void vertex(uint32_t m, const Bsdf& b, V3 out, const TexHit* tex) {
         if (!kAdjoint) return;
         const bool lambert = b.count && b.lobe.kind == 0;
         ggx = b.count && b.lobe.kind == 1;
@@ -424,6 +422,7 @@ struct WaveSink {
         adj->scale[v] = lambert ? make_float4(a.x != 0.0f ? 1.0f / a.x : 0.0f, a.y != 0.0f ? 1.0f / a.y : 0.0f, a.z != 0.0f ? 1.0f / a.z : 0.0f, 0.0f)
                                 : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         adj->vcount[p] = depth + 1;
+        if (lambert && tex && adj->tex) adj->tex[v] = make_float4(tex->s, tex->t, tex->primary ? 1.0f : 0.0f, 0.0f);
         if (ggx) {
             lobe = b.lobe;
             wo = out;

@@ -41,6 +41,8 @@ struct AdjointWave {
     uint32_t* vcount;    // a slot's vertices
     float4* delta;       // a slot's dL/dI share (dL/dI of its pixel over the pixel's samples)
     uint2* aux;          // per shadow record: light | (BSDF record << 31), own roughness factor (float bits)
+    float4* tex;         // per vertex record of a textured Lambert vertex: its st and whether primary (bilinear)
+    float* texGrad;      // FP32 dL/dtexel, 3 a texel over the scene's textures; null: not wanted
 };
 
 struct WaveArgs {

@@ -39,7 +39,11 @@ class Chunk(C.Structure):
 
 class Material(C.Structure):
     _fields_ = [("kind", C.c_uint32), ("diffuse", C.c_float * 3), ("specular", C.c_float * 3), ("emission", C.c_float * 3),
-                ("roughness", C.c_float)]
+                ("roughness", C.c_float), ("diffuse_texture", C.c_uint32)]
+
+
+class Texture(C.Structure):
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("wrap", C.c_uint32), ("pad", C.c_uint32), ("rgb", C.POINTER(C.c_float))]
 
 
 class Light(C.Structure):
@@ -73,7 +77,8 @@ class SceneDesc(C.Structure):
                 ("light_count", C.c_uint32), ("pad", C.c_uint32), ("vertices", C.POINTER(C.c_float)), ("triangles", C.POINTER(C.c_uint32)),
                 ("mesh_first", C.POINTER(C.c_uint32)), ("mesh_material", C.POINTER(C.c_uint32)), ("materials", C.POINTER(Material)),
                 ("lights", C.POINTER(Light)), ("camera", Camera), ("volume_count", C.c_uint32), ("grid_count", C.c_uint32),
-                ("volumes", C.POINTER(Volume)), ("grids", C.POINTER(Grid))]
+                ("volumes", C.POINTER(Volume)), ("grids", C.POINTER(Grid)), ("texture_count", C.c_uint32), ("pad2", C.c_uint32),
+                ("textures", C.POINTER(Texture)), ("uvs", C.POINTER(C.c_float))]
 
 
 _U = C.c_uint32
@@ -159,7 +164,8 @@ def library():
         "x2_launch_wavefront_static": ([vp, vp, u32, u32, vp, vp, C.POINTER(u64)], i32),
         "x2_render_batch": ([vp, C.POINTER(Request), u32, C.POINTER(Completion)], i32),
         "x2_wavefront_autotune": ([vp, u32, u32, C.POINTER(WavefrontShape), C.POINTER(C.c_float)], i32),
-        "x2_scene_set_params": ([vp, vp, vp, vp], i32), "x2_adjoint": ([vp, u32, u32, vp, vp, vp, vp], i32), "x2_adjoint_plain": ([vp, u32, u32, vp, vp, vp, vp], i32),
+        "x2_scene_set_params": ([vp, vp, vp, vp], i32), "x2_adjoint": ([vp, u32, u32, vp, vp, vp, vp, vp], i32), "x2_adjoint_plain": ([vp, u32, u32, vp, vp, vp, vp, vp], i32),
+        "x2_scene_set_texture": ([vp, u32, vp], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
@@ -276,6 +282,11 @@ class SyntheticScene:
             "mesh_first": np.ctypeslib.as_array(d.mesh_first, (d.mesh_count + 1,)).copy(),
             "mesh_material": np.ctypeslib.as_array(d.mesh_material, (d.mesh_count,)).copy(),
         }
+
+    def texture(self, k=0):
+        """Texture k's texels (height x width x 3, float32), a copy."""
+        t = self.desc.textures[k]
+        return np.ctypeslib.as_array(t.rgb, (t.height * t.width * 3,)).reshape(t.height, t.width, 3).copy()
 
     def free(self):
         if self._desc:
@@ -408,13 +419,19 @@ class Scene:
         g = None if roughness is None else np.ascontiguousarray(roughness, np.float32)
         _check(library().x2_scene_set_params(self._h, _ptr(a), _ptr(g), _ptr(r)))
 
-    def adjoint(self, first, count, d_dloss_dimage, d_albedo_grad, d_radiance_grad, d_roughness_grad=None, plain=False):
-        """x2_adjoint on device pointers (ints): adds dL/dalbedo, dL/dradiance and (when given) dL/droughness for
-        samples [first, first + count) of every pixel, given dL/dimage (3 floats a pixel). plain: the replay in the
-        plain megakernel's form (x2_adjoint_plain)."""
+    def set_texture(self, texture, rgb):
+        """x2_scene_set_texture: texture `texture`'s texels (height x width x 3 floats) set in place."""
+        a = np.ascontiguousarray(rgb, np.float32)
+        _check(library().x2_scene_set_texture(self._h, texture, _ptr(a)))
+
+    def adjoint(self, first, count, d_dloss_dimage, d_albedo_grad, d_radiance_grad, d_roughness_grad=None, plain=False,
+                d_texture_grad=None):
+        """x2_adjoint on device pointers (ints): adds dL/dalbedo, dL/dradiance and (when given) dL/droughness and
+        dL/dtexel for samples [first, first + count) of every pixel, given dL/dimage (3 floats a pixel). plain: the
+        replay in the plain megakernel's form (x2_adjoint_plain)."""
         f = library().x2_adjoint_plain if plain else library().x2_adjoint
         _check(f(self._h, first, count, C.c_void_p(d_dloss_dimage), C.c_void_p(d_albedo_grad), C.c_void_p(d_roughness_grad),
-                 C.c_void_p(d_radiance_grad)))
+                 C.c_void_p(d_radiance_grad), C.c_void_p(d_texture_grad)))
 
     def wavefront_autotune(self, tiles=0, spp=None):
         """Time the wavefront launch shapes on `tiles` evenly spaced tiles (0: all) at `spp` samples (default: the
