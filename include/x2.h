@@ -255,6 +255,7 @@ typedef struct x2_wavefront_shape {
     uint32_t lobe_queues;    /* 1: shade takes the extended paths from per-lobe queues (GGX, Lambert, then none or
                                 missed), sorted after extend, so a warp runs one lobe's code; 0: in the extend queue's
                                 order */
+    uint32_t reserved[3];
 } x2_wavefront_shape;
 void x2_wavefront_shape_defaults(x2_wavefront_shape* shape);
 int x2_wavefront_tune(x2_scene* scene, const x2_wavefront_shape* shape);

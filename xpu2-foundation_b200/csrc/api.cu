@@ -814,7 +814,8 @@ int x2_integrate_device(x2_scene* s, const uint32_t* pairs, uint64_t n, double* 
     cudaStream_t st = s->ctx->stream;
     cudaMemsetAsync(sl.counters, 0, sizeof(Counters), st);
     const int blocks = s->ctx->smCount * s->ctx->renderBlocksPerSm;
-    (s->volumeCount ? integratePairsVolumes : integratePairs)<<<blocks, kRenderBlock, 0, st>>>(viewOf(s), pairs, n, rgba, status, sl.counters);
+    (s->volumeCount ? integratePairsVolumes : s->triUV ? integratePairsTextured : integratePairs)<<<blocks, kRenderBlock, 0, st>>>(
+        viewOf(s), pairs, n, rgba, status, sl.counters);
     CUDA_OR(cudaGetLastError(), X2_ECUDA);
     cudaMemcpyAsync(sl.hostCounters, sl.counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
     cudaEventRecord(sl.done, st);
@@ -973,7 +974,7 @@ int x2_launch(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     a.counters = sl->counters;
     const int blocks = s->ctx->smCount * s->ctx->renderBlocksPerSm;
     cudaEventRecord(sl->begin, st);
-    (s->volumeCount ? renderChunksVolumes : renderChunks)<<<blocks, kRenderBlock, 0, st>>>(a);
+    (s->volumeCount ? renderChunksVolumes : s->triUV ? renderChunksTextured : renderChunks)<<<blocks, kRenderBlock, 0, st>>>(a);
     CUDA_OR(cudaGetLastError(), X2_ECUDA);
     cudaEventRecord(sl->end, st);
     cudaMemcpyAsync(sl->hostCounters, sl->counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
@@ -1142,7 +1143,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     a.chunkCount = count;
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
-    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0);
+    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr);
     const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     if (s->waveTiming) {
         // Diagnostic form: no graph; events around every kernel, the iteration's times added once it is done.
@@ -1518,7 +1519,7 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     // Logic in a grid of a few blocks a SM (each block's partials go to a gradient row once a launch).
     const int gridLogic = std::min(int((paths + kWaveBlock - 1) / kWaveBlock), s->ctx->smCount * 8);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
-    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, false);
+    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, false, s->triUV != nullptr);
     const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     constexpr int kIter = 8;
     cudaGraph_t graph = nullptr;
@@ -1725,9 +1726,12 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
     int rc = X2_OK;
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = ctx->smCount * int(s0->blocksPerSm);
-    bool anyVolumes = false;
-    for (const SceneView& v : views) anyVolumes = anyVolumes || v.config.volume_count != 0;
-    const WaveKernels wk = waveKernelsBatch(anyVolumes);
+    bool anyVolumes = false, anyTextures = false;
+    for (const SceneView& v : views) {
+        anyVolumes = anyVolumes || v.config.volume_count != 0;
+        anyTextures = anyTextures || v.triUV != nullptr;
+    }
+    const WaveKernels wk = waveKernelsBatch(anyVolumes, anyTextures);
     std::vector<unsigned long long> items;
     uint32_t iterations = 0;
     if (cudaMalloc(&dViews, sizeof(SceneView) * n) != cudaSuccess || cudaMalloc(&dFilms, sizeof(BatchFilm) * n) != cudaSuccess ||

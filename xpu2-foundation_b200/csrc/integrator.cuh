@@ -172,8 +172,9 @@ struct ShadowReq {
 // One hit (async_integrator.h:2222-3031 for the admitted materials): shading state, emission, a light sample of
 // every light that can light the hit, the lobe's BSDF sample, and its child. `top` is the pending stack's size after
 // this vertex was popped. The sink takes shadow rays (shadow(req, bsdf)) and the child (push(child) -> bool).
-// Returns false when the hit's shading state cannot be made (SampleStatus::Error). kVolumes as afterTrace's.
-template <bool kVolumes = true, class Sink>
+// Returns false when the hit's shading state cannot be made (SampleStatus::Error). kVolumes as afterTrace's; kTextures
+// false compiles the texture lookup out (the kernels for scenes whose materials read no texture).
+template <bool kVolumes = true, bool kTextures = true, class Sink>
 __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& root, uint32_t pixel, uint32_t index, const Pending& pv,
                                             const Hit& hit, V3 va, V3 vb, V3 vc, uint32_t top, V3& radiance, float& alpha, Sink& sink) {
     const x2_config& c = s.config;
@@ -186,7 +187,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
     const MaterialRec& mr = s.materials[material];
     TexHit th;
     th.primary = 0;
-    if (mr.texture) {
+    if (kTextures && mr.texture) {
         // The hit's st (hitState, shade_material.h:142-153: w st1 + u st2 + v st3) and the texture's lookup there; the
         // path type picks the filter (PathPrimary: no diffuse, glossy or mirror bounce yet, async_integrator.h:2222).
         const float* uv = s.triUV + 6ull * (__ldg(s.meshFirst + hit.geom) + hit.prim);
@@ -196,10 +197,10 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
         th.primary = pv.diffuse == 0 && pv.glossy == 0 && pv.mirror == 0;
         if (!texLookup(s, mr.texture - 1, th)) return false;
     }
-    shadeMaterial(mr, st, bsdf, mr.texture ? th.texel : V3{1, 1, 1});
+    shadeMaterial(mr, st, bsdf, kTextures && mr.texture ? th.texel : V3{1, 1, 1});
     if (pv.depth == 0) alpha += 1.0f * (1.0f - (0.0f + 0.0f + 0.0f) / 3.0f);
     radiance = add(radiance, mulv(pv.T, bsdf.emission));
-    sink.vertex(material, bsdf, st.wo, mr.texture ? &th : nullptr);  // the vertex, its emission added: what comes after passes its lobe
+    sink.vertex(material, bsdf, st.wo, kTextures && mr.texture ? &th : nullptr);  // the vertex, its emission added: what comes after passes its lobe
     if (bsdf.count == 0) return true;
 
     uint32_t indirectFlags = 0;
@@ -448,7 +449,7 @@ struct PlainSink {
 };
 
 // integratePaths for one sample (pixel, index): the plain megakernel's whole path loop on one thread.
-template <bool kVolumes>
+template <bool kVolumes, bool kTextures>
 static __device__ __noinline__ void integrate(const SceneView& s, uint32_t pixel, uint32_t index, SampleOut& out) {
     const x2_config& c = s.config;
     out.rgb[0] = out.rgb[1] = out.rgb[2] = 0.0f;
@@ -474,7 +475,7 @@ static __device__ __noinline__ void integrate(const SceneView& s, uint32_t pixel
         ++out.trace;
         afterTrace<kVolumes>(s, root, pv, hit, cameraPosition, radiance, alpha);
         if (hit.geom == ~0u) continue;
-        if (!shadeVertex<kVolumes>(s, root, pixel, index, pv, hit, va, vb, vc, top, radiance, alpha, sink)) {
+        if (!shadeVertex<kVolumes, kTextures>(s, root, pixel, index, pv, hit, va, vb, vc, top, radiance, alpha, sink)) {
             out.status = X2_ERROR;
             return;
         }

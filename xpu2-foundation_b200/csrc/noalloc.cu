@@ -169,7 +169,7 @@ extern "C" int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chu
     cudaMemsetAsync(a.outStatus, X2_SKIP, items, st);
     const int gridLogic = int((kPaths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = smCount * int(kDefaultBlocksPerSm);
-    const WaveKernels wk = waveKernels(kDefaultTraceBlocks, kDefaultShadeBlocks, view.config.volume_count != 0);
+    const WaveKernels wk = waveKernels(kDefaultTraceBlocks, kDefaultShadeBlocks, view.config.volume_count != 0, view.triUV != nullptr);
     const uint64_t maxIter = items * (uint64_t(c.max_depth) + 2) / kPaths + uint64_t(c.max_depth) + 64;
     uint32_t last = 1;
     for (uint64_t it = 0; last; ++it) {

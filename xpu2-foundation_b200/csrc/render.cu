@@ -47,7 +47,7 @@ __device__ __forceinline__ void addCounters(Counters* dst, unsigned long long tr
 
 }  // namespace
 
-template <bool kVolumes>
+template <bool kVolumes, bool kTextures>
 __device__ __forceinline__ void renderChunksBody(const RenderArgs& a) {
     const unsigned full = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u;
@@ -75,7 +75,7 @@ __device__ __forceinline__ void renderChunksBody(const RenderArgs& a) {
         o.status = X2_SKIP;
         o.rgb[0] = o.rgb[1] = o.rgb[2] = o.alpha = 0.0f;
         if (pixel != ~0u) {
-            integrate<kVolumes>(a.scene, pixel, index, o);
+            integrate<kVolumes, kTextures>(a.scene, pixel, index, o);
             trace += o.trace;
             nee += o.nee;
             bsdf += o.bsdf;
@@ -135,11 +135,12 @@ __device__ __forceinline__ void renderChunksBody(const RenderArgs& a) {
     }
     addCounters(a.counters, trace, nee, bsdf, held, samples, errors);
 }
-__global__ void __launch_bounds__(kRenderBlock) renderChunks(RenderArgs a) { renderChunksBody<false>(a); }
-__global__ void __launch_bounds__(kRenderBlock) renderChunksVolumes(RenderArgs a) { renderChunksBody<true>(a); }
+__global__ void __launch_bounds__(kRenderBlock) renderChunks(RenderArgs a) { renderChunksBody<false, false>(a); }
+__global__ void __launch_bounds__(kRenderBlock) renderChunksTextured(RenderArgs a) { renderChunksBody<false, true>(a); }
+__global__ void __launch_bounds__(kRenderBlock) renderChunksVolumes(RenderArgs a) { renderChunksBody<true, true>(a); }
 
 // The per-sample API: integrate() for n (pixel, index) pairs.
-template <bool kVolumes>
+template <bool kVolumes, bool kTextures>
 __device__ __forceinline__ void integratePairsBody(const SceneView& s, const uint32_t* __restrict__ pairs, unsigned long long n,
                                                    double* __restrict__ rgba, uint32_t* __restrict__ status, Counters* counters) {
     unsigned long long trace = 0, nee = 0, bsdf = 0, held = 0, samples = 0, errors = 0;
@@ -151,7 +152,7 @@ __device__ __forceinline__ void integratePairsBody(const SceneView& s, const uin
         const unsigned long long i = first + r * stride;
         if (i >= n) continue;
         SampleOut o;
-        integrate<kVolumes>(s, pairs[2 * i], pairs[2 * i + 1], o);
+        integrate<kVolumes, kTextures>(s, pairs[2 * i], pairs[2 * i + 1], o);
         rgba[4 * i] = double(o.rgb[0]);
         rgba[4 * i + 1] = double(o.rgb[1]);
         rgba[4 * i + 2] = double(o.rgb[2]);
@@ -168,12 +169,17 @@ __device__ __forceinline__ void integratePairsBody(const SceneView& s, const uin
 }
 __global__ void __launch_bounds__(kRenderBlock) integratePairs(SceneView s, const uint32_t* __restrict__ pairs, unsigned long long n,
                                                                double* __restrict__ rgba, uint32_t* __restrict__ status, Counters* counters) {
-    integratePairsBody<false>(s, pairs, n, rgba, status, counters);
+    integratePairsBody<false, false>(s, pairs, n, rgba, status, counters);
+}
+__global__ void __launch_bounds__(kRenderBlock) integratePairsTextured(SceneView s, const uint32_t* __restrict__ pairs, unsigned long long n,
+                                                                       double* __restrict__ rgba, uint32_t* __restrict__ status,
+                                                                       Counters* counters) {
+    integratePairsBody<false, true>(s, pairs, n, rgba, status, counters);
 }
 __global__ void __launch_bounds__(kRenderBlock) integratePairsVolumes(SceneView s, const uint32_t* __restrict__ pairs, unsigned long long n,
                                                                       double* __restrict__ rgba, uint32_t* __restrict__ status,
                                                                       Counters* counters) {
-    integratePairsBody<true>(s, pairs, n, rgba, status, counters);
+    integratePairsBody<true, true>(s, pairs, n, rgba, status, counters);
 }
 
 // Closest hit and occlusion for n rays (8 floats each: origin, direction, near, far).

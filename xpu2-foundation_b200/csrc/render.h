@@ -21,11 +21,14 @@ struct RenderArgs {
 // Fills the Sobol direction table the render kernels read (this device, current context).
 cudaError_t uploadSobol(const uint32_t directions[17][32]);
 
-// The plain megakernel and the per-sample kernel, each in two forms: for scenes without volumes (the volume code
-// compiled out) and with them.
+// The plain megakernel and the per-sample kernel, each in three forms: for scenes without volumes or textures (their
+// code compiled out), with textures, and with volumes (and textures).
 __global__ void renderChunks(RenderArgs a);
+__global__ void renderChunksTextured(RenderArgs a);
 __global__ void renderChunksVolumes(RenderArgs a);
 __global__ void integratePairs(SceneView s, const uint32_t* pairs, unsigned long long n, double* rgba, uint32_t* status, Counters* counters);
+__global__ void integratePairsTextured(SceneView s, const uint32_t* pairs, unsigned long long n, double* rgba, uint32_t* status,
+                                       Counters* counters);
 __global__ void integratePairsVolumes(SceneView s, const uint32_t* pairs, unsigned long long n, double* rgba, uint32_t* status,
                                       Counters* counters);
 __global__ void traceRays(SceneView s, const float* rays, unsigned long long n, uint32_t* tri, float* t, uint32_t* occluded);

@@ -491,7 +491,7 @@ __device__ __forceinline__ uint32_t shadeEntry(const WaveArgs& a, uint32_t i, ui
     return a.shadeQ[2ull * a.paths + (i - c0 - c1)];
 }
 
-template <bool kBatch, bool kVolumes, bool kAdjoint = false>
+template <bool kBatch, bool kVolumes, bool kAdjoint = false, bool kTextures = true>
 __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
     const WaveState& w = a.w;
     const uint32_t n = *a.extendCount;
@@ -562,7 +562,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
                     sink.depth = pv.depth;
                     sink.ggx = sink.sampled = false;
                 }
-                if (!shadeVertex<kVolumes>(s, root, pixel, index, pv, hit, va, vb, vc, 0u, radiance, alpha, sink)) {
+                if (!shadeVertex<kVolumes, kTextures>(s, root, pixel, index, pv, hit, va, vb, vc, 0u, radiance, alpha, sink)) {
                     next = kError;
                 } else {
                     records = sink.n;
@@ -600,9 +600,9 @@ __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
 // allow), chosen at launch (x2_wavefront_tune); batches in the compiler's allocation. Shade comes in a form for
 // scenes without volumes (the volume code compiled out) and one for scenes with them.
 __global__ void __launch_bounds__(kWaveBlock) wfExtend(WaveArgs a) { extendBody<false>(a); }
-__global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) { shadeBody<false, false>(a); }
-__global__ void __launch_bounds__(kWaveBlock) wfShadeVolumes(WaveArgs a) { shadeBody<false, true>(a); }
-__global__ void __launch_bounds__(kWaveBlock) wfShadeBatchVolumes(WaveArgs a) { shadeBody<true, true>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) { shadeBody<false, false, false, false>(a); }
+__global__ void __launch_bounds__(kWaveBlock, 4) wfShadeVolumes(WaveArgs a) { shadeBody<false, true>(a); }
+__global__ void __launch_bounds__(kWaveBlock, 4) wfShadeBatchVolumes(WaveArgs a) { shadeBody<true, true>(a); }
 __global__ void __launch_bounds__(kWaveBlock, 4) wfShadeAdjoint(WaveArgs a) { shadeBody<false, false, true>(a); }
 
 // The adjoint's gradient rows summed in FP64 into grads (one thread a gradient).
@@ -620,30 +620,32 @@ template <int kMinBlocks>
 __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfExtendOcc(WaveArgs a) {
     extendBody<false>(a);
 }
-template <int kMinBlocks, bool kBatch>
+template <int kMinBlocks, bool kBatch, bool kTextures = false>
 __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadeOcc(WaveArgs a) {
-    shadeBody<kBatch, false>(a);
+    shadeBody<kBatch, false, false, kTextures>(a);
 }
 template <int kMinBlocks>
 __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadowOcc(WaveArgs a) {
     shadowBody<false>(a);
 }
 
-WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes) {
+WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures) {
     WaveKernels k;
     k.logic = wfLogic;
     k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : wfExtend;
     k.shadow = traceBlocks >= 10 ? wfShadowOcc<10> : traceBlocks >= 9 ? wfShadowOcc<9> : wfShadow;
-    k.shade = volumes ? wfShadeVolumes : shadeBlocks >= 4 ? wfShadeOcc<4, false> : shadeBlocks >= 3 ? wfShadeOcc<3, false> : wfShade;
+    if (volumes) k.shade = wfShadeVolumes;
+    else if (textures) k.shade = wfShadeOcc<4, false, true>;
+    else k.shade = shadeBlocks >= 4 ? wfShadeOcc<4, false> : shadeBlocks >= 3 ? wfShadeOcc<3, false> : wfShade;
     return k;
 }
 
-WaveKernels waveKernelsBatch(bool volumes) {
+WaveKernels waveKernelsBatch(bool volumes, bool textures) {
     WaveKernels k;
     k.logic = wfLogicBatch;
     k.extend = wfExtendBatch;
     k.shadow = wfShadowBatch;
-    k.shade = volumes ? wfShadeBatchVolumes : wfShadeOcc<4, true>;
+    k.shade = volumes ? wfShadeBatchVolumes : textures ? wfShadeOcc<4, true, true> : wfShadeOcc<4, true>;
     return k;
 }
 

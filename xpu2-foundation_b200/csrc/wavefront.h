@@ -93,15 +93,16 @@ cudaError_t uploadSobolWavefront(const uint32_t directions[17][32]);
 // The logic, extend, shade and shadow kernels for an occupancy: at least `traceBlocks` / `shadeBlocks` blocks a SM
 // (10, 9 or 0 for the traversals; 4, 3 or 0 for shade; 0 leaves the register allocation to the compiler); and the
 // batch forms, which take each path's scene from WaveArgs::scenes. `volumes`: a scene (or any request) has volumes,
-// which takes the shade kernel with the volume code (in the compiler's allocation).
+// which takes the shade kernel with the volume code (4 blocks a SM); `textures`: a material reads a texture, which
+// takes a shade kernel with the lookup.
 struct WaveKernels {
     void (*logic)(WaveArgs);
     void (*extend)(WaveArgs);
     void (*shade)(WaveArgs);
     void (*shadow)(WaveArgs);
 };
-WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes);
-WaveKernels waveKernelsBatch(bool volumes);
+WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures);
+WaveKernels waveKernelsBatch(bool volumes, bool textures);
 __global__ void wfSortShade(WaveArgs a);
 __global__ void wfSortShadeBatch(WaveArgs a);
 // The adjoint's logic and shade kernels (dynamic shared memory: the gradient count in floats) and the final sum of the
