@@ -473,6 +473,41 @@ def probe_rmse(args):
     ctx.close()
 
 
+def probe_adaptive(args):
+    """An adaptive frame of config 0 (the closed box, 256x256; MoonRay's schedule up to 256 samples a pixel, passes from
+    4 samples on adaptive, target error 5e-4): its passes, samples and time; then the image RMSE of its fixture tiles
+    against the converged reference (tests/golden/rmse_c0.npz) beside a uniform frame's of about the same samples."""
+    import rmse_lib
+    import x2
+
+    ctx = x2.Context(0)
+    s = x2.SyntheticScene(0)
+    cfg = s.config
+    scene = x2.Scene(ctx, s.desc, cfg)
+    scene.render_adaptive(4, 256, 5e-4)  # warm-up
+    result = scene.render_adaptive(4, 256, 5e-4)
+    sums, counts = scene.film()
+    f = np.load(os.path.join(ROOT, "tests", "golden", "rmse_c0.npz"))
+    px = rmse_lib.tile_pixels(f["tiles"], cfg.width, cfg.height)
+    live = f["live"]
+    ref = f["ref"].astype(np.float64)
+    img = np.zeros(px.shape + (3,))
+    img[live] = sums[px[live], :3] / counts[px[live], None]
+    mean_spp = result["samples"] / (cfg.width * cfg.height)
+    spp = max(1, int(round(mean_spp)))
+    scene.frame_begin(spp)
+    scene.render_frame_wavefront(0, spp)
+    c = scene.wait()
+    usums, ucounts = scene.film()
+    uimg = np.zeros(px.shape + (3,))
+    uimg[live] = usums[px[live], :3] / ucounts[px[live], None]
+    print(json.dumps({"probe": "adaptive", "config": 0, **result, "mean_spp": mean_spp,
+                      "rmse_adaptive": rmse_lib.rmse(img, ref, live), "uniform_spp": spp,
+                      "rmse_uniform": rmse_lib.rmse(uimg, ref, live), "uniform_ms": c.milliseconds}))
+    scene.free()
+    ctx.close()
+
+
 def probe(args):
     """One bounded launch for profilers (ncu): `--probe-tiles` evenly spaced tiles of config 1 at 64 spp, in one form;
     the wavefront form without its graph (`--probe-timed`) so each kernel launch is visible on its own."""
@@ -486,6 +521,8 @@ def probe(args):
         return probe_adjoint(args)
     if args.probe == "rmse":
         return probe_rmse(args)
+    if args.probe == "adaptive":
+        return probe_adaptive(args)
     ctx = x2.Context(0)
     s = x2.SyntheticScene(1)
     cfg = s.config
@@ -523,7 +560,7 @@ def main():
     ap.add_argument("--impl", default="x2", choices=["x2", "reference"])
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--skip-plain", action="store_true")
-    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint", "rmse"], help="one bounded launch for a profiler, then exit")
+    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint", "rmse", "adaptive"], help="one bounded launch for a profiler, then exit")
     ap.add_argument("--probe-tiles", type=int, default=592)
     ap.add_argument("--probe-timed", action="store_true", help="wavefront probe without its graph (per-kernel launches)")
     ap.add_argument("--adjoint-only", action="store_true", help="adjoint probe: one primal frame, then one wavefront adjoint launch")

@@ -277,6 +277,32 @@ typedef struct x2_request {
  * tiles; x2_film_download / x2_audit read it. Waits. out (or null): samples and errors of the whole batch, its device
  * milliseconds; the ray counters go to the first scene's x2_counters. */
 int x2_render_batch(x2_ctx* ctx, const x2_request* requests, uint32_t n, x2_completion* out);
+/* ---- adaptive sampling (async_render.h's adaptive frame; async_adaptive.h, async_adaptive.cu) ----
+ * A frame whose film also keeps the odd-index sums (GpuLane::begin's adaptive frame, async_gpu.h:1372): as
+ * x2_frame_begin. */
+int x2_frame_begin_adaptive(x2_scene* scene, uint32_t samples_per_chunk);
+/* One step of the reference's GPU pass chain (async_adaptive.cu chainErrors, chainTrees, chainMasks) on the current
+ * adaptive film: each pixel's error (pixelError, async_integrator.h:3109), the overlapping regions' trees
+ * (async_adaptive.h Tree, Regions; target error `target`), and each 8x8 tile's mask of the pixels the next pass of
+ * `size` samples takes (uniform: every pixel in the image, no trees); each active pixel's first sample index and
+ * planned count move on. errors (a float a pixel), masks (a uint64 a tile, bit y * 8 + x) and stop (1: every region
+ * converged, the chain stops) are host arrays, each may be null. Waits. */
+int x2_adaptive_step(x2_scene* scene, float target, uint32_t uniform, uint32_t size, float* errors, uint64_t* masks, uint32_t* stop);
+typedef struct x2_adaptive_result {
+    uint32_t passes, converged;  /* passes rendered; 1 when every region converged before the schedule ran out */
+    uint64_t samples;            /* samples rendered */
+    float milliseconds;          /* host time of the whole frame */
+    uint32_t pad;
+} x2_adaptive_result;
+/* An adaptive frame (the reference's adaptive frame with its GPU chain, async_render.h / async_gpu.h:1929-2090):
+ * MoonRay's pass schedule for max_samples (one sample, then 4, 6, 8, ... more), passes starting below min_samples
+ * uniform, then after each pass the chain's errors, trees and masks; each pass renders its active tiles' masked pixels
+ * in the wavefront form, each pixel from its own next sample index. Ends when every region has converged (target
+ * error), a pass has no active pixel, or the schedule runs out. The film (sums, odd sums, counts) is then read as after
+ * any launch; x2_adaptive_planned gives each pixel's planned count (for x2_audit). Waits. */
+int x2_render_adaptive(x2_scene* scene, uint32_t min_samples, uint32_t max_samples, float target, x2_adaptive_result* result);
+int x2_adaptive_planned(x2_scene* scene, uint32_t* planned);
+
 /* ---- differentiation (no reference counterpart; config 4) ----
  * The differentiable parameters, set in place: each material's diffuse colour (a Lambert lobe's albedo; 3 floats a
  * material), each material's roughness (a GGX lobe's; 1 float a material) and each light's radiance (3 floats a

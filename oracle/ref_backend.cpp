@@ -12,6 +12,7 @@
 // The film and the chunk loop follow renderChunk (async_cpu.h:1584-1667) and the audit async_render.h:992-1048.
 #define XPU2_PATHS_ONLY 1
 #include "async_integrator.h"
+#include "async_adaptive.h"
 
 #include "../include/x2.h"
 
@@ -1022,6 +1023,40 @@ int x2ref_trace_brute(void* p, const float* rays, uint64_t n, uint32_t* tri, flo
         occl[i] = any ? 1u : 0u;
     }
     return X2_OK;
+}
+
+// ---- adaptive sampling (async_integrator.h:3088-3125, async_adaptive.h, async_adaptive_core.h), the reference's own ----
+// Each pixel's error (pixelError) from a film: sums and odd sums (4 doubles a pixel) and counts.
+int x2ref_pixel_errors(const double* sums, const double* odd, const uint32_t* counts, uint64_t pixels, float* errors) {
+    for (uint64_t i = 0; i < pixels; ++i) errors[i] = xi::async::pixelError(sums + 4 * i, odd + 4 * i, counts[i]);
+    return X2_OK;
+}
+// The region trees over a width x height image rebuilt from per-pixel errors (Regions, target error), and each 8x8
+// tile's mask of pixels still to sample (sampleArea, bit y * 8 + x, masked to the image); *done = 1 when every region
+// has converged. masks: one a tile, tiles in row-major order.
+int x2ref_adaptive_masks(uint32_t width, uint32_t height, float target, const float* errors, uint64_t* masks, uint32_t* done) {
+    namespace ad = xi::async::adaptive;
+    ad::Regions regions(int(width), int(height), target);
+    for (size_t r = 0; r < regions.count(); ++r) regions.update(r, errors);
+    const uint32_t tilesX = (width + 7) / 8, tilesY = (height + 7) / 8;
+    for (uint32_t ty = 0; ty < tilesY; ++ty)
+        for (uint32_t tx = 0; tx < tilesX; ++tx) {
+            uint64_t inImage = 0;
+            for (uint32_t p = 0; p < 64; ++p)
+                if (tx * 8 + p % 8 < width && ty * 8 + p / 8 < height) inImage |= uint64_t(1) << p;
+            masks[size_t(ty) * tilesX + tx] = inImage & regions.sampleArea(int(tx * 8), int(ty * 8));
+        }
+    *done = regions.done() ? 1u : 0u;
+    return X2_OK;
+}
+// MoonRay's pass schedule for maxSamples (schedule): passes[2 k], passes[2 k + 1] = start, end; returns the count.
+uint32_t x2ref_adaptive_schedule(uint32_t maxSamples, uint32_t* passes, uint32_t capacity) {
+    const auto s = xi::async::adaptive::schedule(maxSamples);
+    for (size_t k = 0; k < s.size() && k < capacity; ++k) {
+        passes[2 * k] = s[k].start;
+        passes[2 * k + 1] = s[k].end;
+    }
+    return uint32_t(s.size());
 }
 
 // sample::samplingWord (sample_stream.h:127-144), the reference's own.

@@ -208,3 +208,26 @@ def adjoint64(ref, first, count, dldi, threads=None, params=None, masses=False, 
     if texels:
         out = out + (tg,)
     return out
+
+
+def reference_pixel_errors(sums, odd, counts):
+    """The reference's pixelError (async_integrator.h:3109) of every pixel of a film."""
+    lib = C.CDLL(REFERENCE)
+    lib.x2ref_pixel_errors.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_void_p]
+    sums = np.ascontiguousarray(sums, np.float64)
+    odd = np.ascontiguousarray(odd, np.float64)
+    counts = np.ascontiguousarray(counts, np.uint32)
+    out = np.empty(len(counts), np.float32)
+    lib.x2ref_pixel_errors(sums.ctypes.data, odd.ctypes.data, counts.ctypes.data, len(counts), out.ctypes.data)
+    return out
+
+
+def reference_adaptive_masks(width, height, target, errors):
+    """The reference's region trees (async_adaptive.h Regions) over per-pixel errors: (tile masks, all converged)."""
+    lib = C.CDLL(REFERENCE)
+    lib.x2ref_adaptive_masks.argtypes = [C.c_uint32, C.c_uint32, C.c_float, C.c_void_p, C.c_void_p, C.c_void_p]
+    errors = np.ascontiguousarray(errors, np.float32)
+    masks = np.empty(((width + 7) // 8) * ((height + 7) // 8), np.uint64)
+    done = np.zeros(1, np.uint32)
+    lib.x2ref_adaptive_masks(width, height, target, errors.ctypes.data, masks.ctypes.data, done.ctypes.data)
+    return masks, bool(done[0])

@@ -1,0 +1,111 @@
+// The adaptive pass chain on the device (row f2 of the path's scope): between a frame's passes, every pixel's error
+// from the film, the region trees rebuilt from the errors, and the next pass's tile masks with each active pixel's
+// first sample index — the reference's GPU chain (xpu2/interactive/async_adaptive.cu: chainErrors, chainTrees,
+// chainMasks) with the arithmetic of adaptive.cuh, which the host's trees share, so the masks equal the reference's
+// host trees' for the same film.
+#include "adaptive.h"
+
+namespace x2 {
+
+__global__ void adErrors(const double* sums, const double* odd, const uint32_t* counts, float* errors, uint32_t pixels) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= pixels) return;
+    errors[i] = ad::pixelError(sums + 4ull * i, odd + 4ull * i, counts[i]);
+}
+
+// One block a region: the summed-area table of its errors (each row's running sums, then each column's, the sums in
+// the host's order), then its nodes a level at a time, each decided as the host's recursion decides it. A region with a
+// pixel not ready keeps its root alone, unconverged.
+__global__ void adTrees(AdaptiveArgs a) {
+    const uint32_t r = blockIdx.x;
+    const ad::IBox root = a.regions[r];
+    const int w = root.x1 - root.x0, h = root.y1 - root.y0, w1 = w + 1;
+    double* sat = a.sat + a.satOffset[r];
+    ad::Node* nodes = a.nodes + a.nodeOffset[r];
+    __shared__ int notReady, unconverged, count;
+    if (threadIdx.x == 0) {
+        notReady = unconverged = 0;
+        count = 1;
+        nodes[0] = ad::Node{{float(root.x0), float(root.y0), float(root.x1), float(root.y1)}, -1, 0};
+    }
+    __syncthreads();
+    for (int x = threadIdx.x; x <= w; x += blockDim.x) sat[x] = 0.0;
+    for (int y = threadIdx.x; y < h; y += blockDim.x) {
+        const float* e = a.errors + size_t(root.y0 + y) * a.width + root.x0;
+        double* out = sat + size_t(y + 1) * w1;
+        double run = 0.0;
+        out[0] = 0.0;
+        bool missing = false;
+        for (int x = 0; x < w; ++x) {
+            const float v = e[x];
+            missing = missing || v < 0;
+            run += v;
+            out[x + 1] = run;
+        }
+        if (missing) notReady = 1;
+    }
+    __syncthreads();
+    if (notReady) {
+        if (threadIdx.x == 0) a.regionDone[r] = 0;
+        return;
+    }
+    for (int x = threadIdx.x + 1; x <= w; x += blockDim.x)
+        for (int y = 1; y <= h; ++y) sat[size_t(y) * w1 + x] += sat[size_t(y - 1) * w1 + x];
+    __syncthreads();
+    const ad::Sat s{sat, root.x0, root.y0, w1};
+    const int capacity = int(a.nodeCapacity[r]);
+    int begin = 0, end = 1;
+    while (begin < end) {
+        for (int i = begin + int(threadIdx.x); i < end; i += blockDim.x) {
+            ad::FBox left, right;
+            const int fate = ad::decide(s, root, nodes[i].b, a.target, left, right);
+            if (fate == ad::kConverged) {
+                nodes[i].complete = 1;
+            } else if (fate == ad::kSplit) {
+                const int c = atomicAdd(&count, 2);
+                if (c + 2 <= capacity) {
+                    nodes[c] = ad::Node{left, -1, 0};
+                    nodes[c + 1] = ad::Node{right, -1, 0};
+                    nodes[i].children = c;
+                } else {
+                    unconverged = 1;  // past the tree's bound (never, by the bound's construction)
+                }
+            } else {
+                unconverged = 1;
+            }
+        }
+        __syncthreads();
+        begin = end;
+        end = count < capacity ? count : capacity;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) a.regionDone[r] = unconverged ? 0 : 1;
+}
+
+__global__ void adMasks(AdaptiveArgs a, uint32_t uniform, uint32_t size) {
+    if (!uniform) {
+        bool converged = true;
+        for (uint32_t r = 0; r < a.regionCount; ++r) converged = converged && a.regionDone[r] != 0;
+        if (converged) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) *a.stop = 1;
+            return;
+        }
+    }
+    const uint32_t tile = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tile >= a.tiles) return;
+    uint64_t mask = a.inImage[tile];
+    if (!uniform) {
+        const int tx = int(tile % a.tilesX) * 8, ty = int(tile / a.tilesX) * 8;
+        mask &= ad::tileSamples(a.nodes + a.nodeOffset[a.layout.regionOf(tx, ty)], tx, ty);
+    }
+    a.tileMask[tile] = mask;
+    for (uint32_t p = 0; p < 64; ++p)
+        if (mask >> p & 1) {
+            const uint32_t x = (tile % a.tilesX) * 8 + p % 8, y = (tile / a.tilesX) * 8 + p / 8;
+            const uint32_t pixel = y * a.width + x;
+            a.base[pixel] = a.planned[pixel];
+            a.planned[pixel] += size;
+        }
+}
+
+}  // namespace x2

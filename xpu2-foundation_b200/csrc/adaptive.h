@@ -1,0 +1,41 @@
+// The adaptive pass chain's kernels (adaptive.cu; internal to libx2).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "adaptive.cuh"
+
+namespace x2 {
+
+// A frame's adaptive state on the device: the film's pixel errors, the region trees (their bounds, node arrays and
+// summed-area tables), each tile's pixels in the image and its mask for the pass, each pixel's planned sample count
+// and its first sample index in the pass, and the chain's stop word (1: every region converged).
+struct AdaptiveArgs {
+    uint32_t width, height, tilesX, tiles, regionCount;
+    float target;
+    ad::Layout layout;
+    const ad::IBox* regions;
+    const uint32_t* nodeOffset;
+    const uint32_t* nodeCapacity;
+    const unsigned long long* satOffset;
+    double* sat;
+    ad::Node* nodes;
+    uint32_t* regionDone;
+    float* errors;
+    const uint64_t* inImage;
+    uint64_t* tileMask;
+    uint32_t* planned;
+    uint32_t* base;
+    uint32_t* stop;
+};
+
+// Every pixel's error from the film (FP64 sums and odd sums, 4 a pixel; counts).
+__global__ void adErrors(const double* sums, const double* odd, const uint32_t* counts, float* errors, uint32_t pixels);
+// Each region's tree rebuilt from the errors, one block a region (regionDone: 1 converged, 0 not).
+__global__ void adTrees(AdaptiveArgs a);
+// Each tile's mask for a pass of `size` samples a pixel (every pixel in the image in a uniform pass), its pixels'
+// first sample indices and planned counts; a non-uniform pass whose regions have all converged sets the stop word.
+__global__ void adMasks(AdaptiveArgs a, uint32_t uniform, uint32_t size);
+
+}  // namespace x2

@@ -14,6 +14,7 @@
 
 #include "../../include/x2.h"
 #include "engine.h"
+#include "adaptive.h"
 #include "adjoint.h"
 #include "render.h"
 #include "wavefront.h"
@@ -111,6 +112,31 @@ struct x2_ctx {
     int renderBlocksPerSm = 0;
 };
 
+// An adaptive frame's device state (adaptive.h AdaptiveArgs) and its host-side layout.
+struct AdaptiveState {
+    uint32_t width = 0, height = 0, tiles = 0, tilesX = 0, regionCount = 0;
+    float target = 0;
+    x2::ad::Layout layout;
+    x2::ad::IBox* regions = nullptr;
+    uint32_t* nodeOffset = nullptr;
+    uint32_t* nodeCapacity = nullptr;
+    unsigned long long* satOffset = nullptr;
+    double* sat = nullptr;
+    x2::ad::Node* nodes = nullptr;
+    uint32_t* regionDone = nullptr;
+    float* errors = nullptr;
+    uint64_t* inImage = nullptr;
+    uint64_t* tileMask = nullptr;
+    uint32_t* planned = nullptr;
+    uint32_t* base = nullptr;
+    uint32_t* stop = nullptr;
+    uint64_t* chunkMasks = nullptr;  // a pass's active tiles' masks, in its chunks' order
+    ~AdaptiveState() {
+        void* p[] = {regions, nodeOffset, nodeCapacity, satOffset, sat, nodes, regionDone, errors, inImage, tileMask, planned, base, stop, chunkMasks};
+        for (void* q : p) cudaFree(q);
+    }
+};
+
 struct x2_scene {
     x2_ctx* ctx = nullptr;
     DeviceBvh bvh;
@@ -175,6 +201,11 @@ struct x2_scene {
     bool waveTiming = false;           // time each kernel kind (no graph)
     float waveMs[5] = {0, 0, 0, 0, 0}; // logic, extend, shade, shadow, film reduce
     uint32_t queueLog[2 * 4096] = {};  // timed launches: each iteration's extend and shadow queue sizes
+    // an adaptive pass's launch: each chunk's pixel mask and each pixel's first sample index (device; null otherwise)
+    const uint64_t* launchMask = nullptr;
+    const uint32_t* launchBase = nullptr;
+    // the adaptive frame's state (x2_render_adaptive, x2_adaptive_step)
+    AdaptiveState* adaptiveState = nullptr;
     // the adjoint's wavefront state (x2_adjoint): vertex records, scales, counts, dL/dI shares, record auxiliaries
     uint4* avert = nullptr;
     float4* ascale = nullptr;
@@ -726,6 +757,8 @@ int x2_scene_free(x2_scene* s) {
     if (s->ctx) cudaSetDevice(s->ctx->device);
     if (s->ctx) cudaStreamSynchronize(s->ctx->stream);
     freeAdjointWave(s);
+    delete s->adaptiveState;
+    s->adaptiveState = nullptr;
     cudaFree(s->bvh.nodes);
     cudaFree(s->bvh.tris);
     cudaFree(s->triMesh);
@@ -926,6 +959,20 @@ int x2_frame_begin(x2_scene* s, uint32_t samplesPerChunk) {
     cudaMemsetAsync(s->counts, 0, sizeof(uint32_t) * size_t(pixels), st);
     cudaMemsetAsync(s->overflow, 0, sizeof(uint32_t), st);
     s->samplesPerChunk = samplesPerChunk;
+    s->adaptive = false;
+    CUDA_OR(cudaGetLastError(), X2_ECUDA);
+    return X2_OK;
+}
+
+int x2_frame_begin_adaptive(x2_scene* s, uint32_t samplesPerChunk) {
+    if (int rc = x2_frame_begin(s, samplesPerChunk)) return rc;
+    s->adaptive = true;
+    if (s->adaptiveState) {
+        AdaptiveState& a = *s->adaptiveState;
+        cudaMemsetAsync(a.planned, 0, sizeof(uint32_t) * size_t(a.width) * a.height, s->ctx->stream);
+        cudaMemsetAsync(a.base, 0, sizeof(uint32_t) * size_t(a.width) * a.height, s->ctx->stream);
+        cudaMemsetAsync(a.stop, 0, sizeof(uint32_t), s->ctx->stream);
+    }
     CUDA_OR(cudaGetLastError(), X2_ECUDA);
     return X2_OK;
 }
@@ -1132,6 +1179,8 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
     a.shadeCount = s->waveCounters + 5;
     a.adj = AdjointWave{};
+    a.chunkMask = s->launchMask;
+    a.pixelBase = s->launchBase;
     a.refill = s->refill;
     a.triLimit = s->triLimit;
     a.out = s->out;
@@ -1499,7 +1548,6 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     a.shadowNext = s->waveCounters + 4;
     a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
     a.shadeCount = s->waveCounters + 5;
-    a.adj = AdjointWave{};
     a.refill = s->refill;
     a.triLimit = s->triLimit;
     a.out = s->out;
@@ -1511,6 +1559,8 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     a.chunkCount = tiles;
     a.adj = AdjointWave{d_dloss_dimage, rows, kRows, s->materialCount, s->lightCount, verts, s->avert, s->ascale, s->avcount, s->adelta, s->aaux,
                         s->atex, texGrad};
+    a.chunkMask = nullptr;
+    a.pixelBase = nullptr;
     const size_t shared = sizeof(float) * params;
     if (shared > 48 * 1024) {
         cudaFuncSetAttribute(wfLogicAdjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shared));
@@ -1573,6 +1623,223 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     cudaFree(grads);
     cudaFree(texGrad);
     return rc;
+}
+
+// ---- adaptive sampling (row f2): the reference's adaptive frame (async_render.h, async_adaptive.h) on the device ----
+namespace {
+
+// The overlapping regions of a width x height image (the reference's Regions: up to 4 x 4 regions of whole 8-pixel
+// tiles, each widened by an 8-pixel overlap, clamped to the image), their trees' node bounds and table sizes.
+int ensureAdaptive(x2_scene* s, float target) {
+    const uint32_t width = s->config.width, height = s->config.height;
+    AdaptiveState* a = s->adaptiveState;
+    if (a && a->width == width && a->height == height) {
+        a->target = target;
+        return X2_OK;
+    }
+    delete a;
+    a = s->adaptiveState = new AdaptiveState();
+    a->width = width;
+    a->height = height;
+    a->target = target;
+    a->tilesX = (width + 7) / 8;
+    a->tiles = a->tilesX * ((height + 7) / 8);
+    const int tile = 8, overlap = 8, desired = 4, minW = tile + overlap, minH = tile + overlap;
+    auto roundUp = [](int n, int m) { return n % m ? n + m - n % m : n; };
+    const int w = int(width), h = int(height);
+    if (minW >= w || minH >= h) {
+        a->layout.regionW = w;
+        a->layout.regionH = h;
+        a->layout.perDim = 1;
+    } else {
+        a->layout.perDim = std::max(1, std::min(desired, std::min(w / minW, h / minH)));
+        a->layout.regionW = roundUp(1 + (w - 1) / a->layout.perDim, tile);
+        a->layout.regionH = roundUp(1 + (h - 1) / a->layout.perDim, tile);
+    }
+    const int perDim = a->layout.perDim;
+    std::vector<x2::ad::IBox> boxes;
+    std::vector<uint32_t> nodeOffset, nodeCapacity;
+    std::vector<unsigned long long> satOffset;
+    unsigned long long nodes = 0, sat = 0;
+    for (int i = 0; i < perDim * perDim; ++i) {
+        const int rx = i % perDim, ry = i / perDim;
+        x2::ad::IBox b{rx * a->layout.regionW - overlap, ry * a->layout.regionH - overlap, (rx + 1) * a->layout.regionW + overlap,
+                       (ry + 1) * a->layout.regionH + overlap};
+        b = {std::max(b.x0, 0), std::max(b.y0, 0), std::min(b.x1, w), std::min(b.y1, h)};
+        boxes.push_back(b);
+        nodeOffset.push_back(uint32_t(nodes));
+        nodeCapacity.push_back(uint32_t(std::max(1, x2::ad::nodeBound(b))));
+        satOffset.push_back(sat);
+        nodes += nodeCapacity.back();
+        sat += (unsigned long long)(b.x1 - b.x0 + 1) * (unsigned long long)(b.y1 - b.y0 + 1);
+    }
+    a->regionCount = uint32_t(boxes.size());
+    std::vector<uint64_t> inImage(a->tiles);
+    for (uint32_t t = 0; t < a->tiles; ++t) {
+        uint64_t m = 0;
+        const uint32_t tx = (t % a->tilesX) * 8, ty = (t / a->tilesX) * 8;
+        for (uint32_t p = 0; p < 64; ++p)
+            if (tx + p % 8 < width && ty + p / 8 < height) m |= uint64_t(1) << p;
+        inImage[t] = m;
+    }
+    const size_t pixels = size_t(width) * height;
+    const bool ok = cudaMalloc(&a->regions, sizeof(x2::ad::IBox) * boxes.size()) == cudaSuccess &&
+                    cudaMalloc(&a->nodeOffset, sizeof(uint32_t) * boxes.size()) == cudaSuccess &&
+                    cudaMalloc(&a->nodeCapacity, sizeof(uint32_t) * boxes.size()) == cudaSuccess &&
+                    cudaMalloc(&a->satOffset, sizeof(unsigned long long) * boxes.size()) == cudaSuccess &&
+                    cudaMalloc(&a->sat, sizeof(double) * sat) == cudaSuccess && cudaMalloc(&a->nodes, sizeof(x2::ad::Node) * nodes) == cudaSuccess &&
+                    cudaMalloc(&a->regionDone, sizeof(uint32_t) * boxes.size()) == cudaSuccess &&
+                    cudaMalloc(&a->errors, sizeof(float) * pixels) == cudaSuccess && cudaMalloc(&a->inImage, sizeof(uint64_t) * a->tiles) == cudaSuccess &&
+                    cudaMalloc(&a->tileMask, sizeof(uint64_t) * a->tiles) == cudaSuccess &&
+                    cudaMalloc(&a->chunkMasks, sizeof(uint64_t) * a->tiles) == cudaSuccess &&
+                    cudaMalloc(&a->planned, sizeof(uint32_t) * pixels) == cudaSuccess && cudaMalloc(&a->base, sizeof(uint32_t) * pixels) == cudaSuccess &&
+                    cudaMalloc(&a->stop, sizeof(uint32_t)) == cudaSuccess;
+    if (!ok) {
+        delete a;
+        s->adaptiveState = nullptr;
+        setError("device allocation failed for the adaptive frame");
+        return X2_ENOMEM;
+    }
+    cudaStream_t st = s->ctx->stream;
+    cudaMemcpyAsync(a->regions, boxes.data(), sizeof(x2::ad::IBox) * boxes.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(a->nodeOffset, nodeOffset.data(), sizeof(uint32_t) * boxes.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(a->nodeCapacity, nodeCapacity.data(), sizeof(uint32_t) * boxes.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(a->satOffset, satOffset.data(), sizeof(unsigned long long) * boxes.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(a->inImage, inImage.data(), sizeof(uint64_t) * a->tiles, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(a->planned, 0, sizeof(uint32_t) * pixels, st);
+    cudaMemsetAsync(a->base, 0, sizeof(uint32_t) * pixels, st);
+    cudaMemsetAsync(a->stop, 0, sizeof(uint32_t), st);
+    CUDA_OR(cudaStreamSynchronize(st), X2_ECUDA);
+    return X2_OK;
+}
+
+x2::AdaptiveArgs adaptiveArgs(const AdaptiveState& a) {
+    return x2::AdaptiveArgs{a.width, a.height, a.tilesX, a.tiles, a.regionCount, a.target, a.layout, a.regions, a.nodeOffset, a.nodeCapacity,
+                            a.satOffset, a.sat, a.nodes, a.regionDone, a.errors, a.inImage, a.tileMask, a.planned, a.base, a.stop};
+}
+
+// One chain step on the frame's film: errors and trees (not in a uniform pass), then the pass's tile masks.
+int adaptiveChain(x2_scene* s, uint32_t uniform, uint32_t size) {
+    AdaptiveState& a = *s->adaptiveState;
+    cudaStream_t st = s->ctx->stream;
+    const x2::AdaptiveArgs args = adaptiveArgs(a);
+    const uint32_t pixels = a.width * a.height;
+    if (!uniform) {
+        x2::adErrors<<<(pixels + 255) / 256, 256, 0, st>>>(s->sums, s->odd, s->counts, a.errors, pixels);
+        x2::adTrees<<<a.regionCount, 512, 0, st>>>(args);
+    }
+    x2::adMasks<<<(a.tiles + 255) / 256, 256, 0, st>>>(args, uniform, size);
+    CUDA_OR(cudaGetLastError(), X2_ECUDA);
+    return X2_OK;
+}
+
+// MoonRay's pass schedule for maxSamples: one sample, then 4, 6, 8, ... more, the rest last.
+std::vector<std::pair<uint32_t, uint32_t>> adaptiveSchedule(uint32_t maxSamples) {
+    std::vector<std::pair<uint32_t, uint32_t>> passes{{0, 1}};
+    uint32_t current = 1, remaining = maxSamples - 1, size = 4;
+    while (remaining > size && passes.size() < 999) {
+        passes.push_back({current, current + size});
+        remaining -= size;
+        current += size;
+        size += 2;
+    }
+    if (remaining) passes.push_back({current, current + remaining});
+    return passes;
+}
+
+}  // namespace
+
+int x2_adaptive_step(x2_scene* s, float target, uint32_t uniform, uint32_t size, float* errors, uint64_t* masks, uint32_t* stop) {
+    if (!s || !s->configured || !s->filmPixels || !s->adaptive) {
+        setError("x2_adaptive_step: an adaptive frame first (x2_frame_begin_adaptive)");
+        return X2_EINVAL;
+    }
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    if (int rc = ensureAdaptive(s, target)) return rc;
+    if (int rc = adaptiveChain(s, uniform, size)) return rc;
+    AdaptiveState& a = *s->adaptiveState;
+    cudaStream_t st = s->ctx->stream;
+    if (errors) cudaMemcpyAsync(errors, a.errors, sizeof(float) * a.width * a.height, cudaMemcpyDeviceToHost, st);
+    if (masks) cudaMemcpyAsync(masks, a.tileMask, sizeof(uint64_t) * a.tiles, cudaMemcpyDeviceToHost, st);
+    if (stop) cudaMemcpyAsync(stop, a.stop, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    CUDA_OR(cudaStreamSynchronize(st), X2_ECUDA);
+    return X2_OK;
+}
+
+int x2_render_adaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float target, x2_adaptive_result* result) {
+    if (!s || !s->configured || maxSamples == 0 || !(target > 0)) {
+        setError("x2_render_adaptive: a configured scene, at least one sample and a positive target");
+        return X2_EINVAL;
+    }
+    const auto passes = adaptiveSchedule(maxSamples);
+    uint32_t most = 0;
+    for (const auto& p : passes) most = std::max(most, p.second - p.first);
+    if (int rc = x2_frame_begin_adaptive(s, most)) return rc;
+    if (int rc = ensureAdaptive(s, target)) return rc;
+    AdaptiveState& a = *s->adaptiveState;
+    cudaStream_t st = s->ctx->stream;
+    cudaMemsetAsync(a.planned, 0, sizeof(uint32_t) * a.width * a.height, st);
+    cudaMemsetAsync(a.stop, 0, sizeof(uint32_t), st);
+    std::vector<uint64_t> masks(a.tiles);
+    std::vector<x2_chunk> chunks;
+    std::vector<uint64_t> chunkMasks;
+    x2_adaptive_result r{};
+    const auto t0 = std::chrono::steady_clock::now();
+    int rc = X2_OK;
+    for (size_t k = 0; k < passes.size() && rc == X2_OK; ++k) {
+        const uint32_t size = passes[k].second - passes[k].first;
+        const uint32_t uniform = passes[k].first < minSamples ? 1u : 0u;
+        if ((rc = adaptiveChain(s, uniform, size))) break;
+        uint32_t stop = 0;
+        cudaMemcpyAsync(&stop, a.stop, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+        cudaMemcpyAsync(masks.data(), a.tileMask, sizeof(uint64_t) * a.tiles, cudaMemcpyDeviceToHost, st);
+        if (cudaStreamSynchronize(st) != cudaSuccess) {
+            rc = X2_ECUDA;
+            break;
+        }
+        if (stop) {
+            r.converged = 1;
+            break;
+        }
+        chunks.clear();
+        chunkMasks.clear();
+        uint64_t samples = 0;
+        for (uint32_t t = 0; t < a.tiles; ++t)
+            if (masks[t]) {
+                chunks.push_back(x2_chunk{t, 0, size, 0});
+                chunkMasks.push_back(masks[t]);
+                samples += uint64_t(__builtin_popcountll(masks[t])) * size;
+            }
+        if (chunks.empty()) {  // nothing left to sample: the frame ends
+            r.converged = 1;
+            break;
+        }
+        cudaMemcpyAsync(a.chunkMasks, chunkMasks.data(), sizeof(uint64_t) * chunkMasks.size(), cudaMemcpyHostToDevice, st);
+        s->launchMask = a.chunkMasks;
+        s->launchBase = a.base;
+        s->samplesPerChunk = size;
+        rc = x2_launch_wavefront(s, chunks.data(), uint32_t(chunks.size()));
+        s->launchMask = nullptr;
+        s->launchBase = nullptr;
+        s->samplesPerChunk = most;
+        if (rc == X2_OK) rc = x2_wait(s, 600000, nullptr);
+        r.passes++;
+        r.samples += samples;
+    }
+    r.milliseconds = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    if (result) *result = r;
+    return rc;
+}
+
+int x2_adaptive_planned(x2_scene* s, uint32_t* planned) {
+    if (!s || !planned || !s->adaptiveState) {
+        setError("x2_adaptive_planned: no adaptive frame");
+        return X2_EINVAL;
+    }
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    const AdaptiveState& a = *s->adaptiveState;
+    CUDA_OR(cudaMemcpy(planned, a.planned, sizeof(uint32_t) * a.width * a.height, cudaMemcpyDeviceToHost), X2_ECUDA);
+    return X2_OK;
 }
 
 // The launch-shape autotuner: coordinate descent over the shape's knobs (paths in flight, refill, triangle tests a step,
@@ -1780,6 +2047,8 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
         a.shadeQ = s0->lobeQueues ? s0->shadeQ : nullptr;
         a.shadeCount = s0->waveCounters + 5;
         a.adj = AdjointWave{};
+        a.chunkMask = nullptr;
+        a.pixelBase = nullptr;
         a.refill = s0->refill;
         a.triLimit = s0->triLimit;
         a.out = s0->out;

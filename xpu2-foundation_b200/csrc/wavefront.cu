@@ -271,11 +271,12 @@ __device__ __forceinline__ void logicBody(const WaveArgs& a) {
                 const x2_chunk chunk = a.chunks[chunkIndex];
                 const uint32_t request = kBatch ? a.chunkRequest[chunkIndex] : 0u;
                 const SceneView& sv = sceneOf<kBatch>(a, request);
-                const uint32_t pixel = s < chunk.count ? tilePixelW(chunk.tile, position, sv.config.width, sv.config.height) : ~0u;
+                const bool masked = a.chunkMask && !((a.chunkMask[chunkIndex] >> position) & 1ull);
+                const uint32_t pixel = s < chunk.count && !masked ? tilePixelW(chunk.tile, position, sv.config.width, sv.config.height) : ~0u;
                 if (pixel == ~0u) {
                     a.outStatus[item] = uint8_t(X2_SKIP);  // not a sample of this launch
                 } else {
-                    const uint32_t index = chunk.first + s;
+                    const uint32_t index = (a.pixelBase ? a.pixelBase[pixel] : chunk.first) + s;
                     CameraRay camera;
                     if (!cameraRay(sv, pixel, index, camera)) {
                         a.out[item] = make_float4(0, 0, 0, 0);
@@ -675,6 +676,7 @@ __global__ void wfFilmReduce(WaveArgs a, uint32_t chunkCount, double* sums, doub
     double v[4] = {0, 0, 0, 0}, o[4] = {0, 0, 0, 0};
     uint32_t n = 0;
     const unsigned long long first = (unsigned long long)chunkIndex * 64ull * a.samplesPerChunk + (unsigned long long)position * a.samplesPerChunk;
+    const uint32_t indexBase = a.pixelBase ? a.pixelBase[pixel] : chunk.first;
     for (uint32_t s = 0; s < chunk.count; ++s) {
         if (a.outStatus[first + s] != X2_DONE) continue;
         const float4 r = a.out[first + s];
@@ -682,7 +684,7 @@ __global__ void wfFilmReduce(WaveArgs a, uint32_t chunkCount, double* sums, doub
         v[1] += double(r.y);
         v[2] += double(r.z);
         v[3] += double(r.w);
-        if (odd && ((chunk.first + s) & 1u)) {
+        if (odd && ((indexBase + s) & 1u)) {
             o[0] += double(r.x);
             o[1] += double(r.y);
             o[2] += double(r.z);

@@ -67,6 +67,10 @@ struct WaveArgs {
     uint32_t* shadeQ;
     uint32_t* shadeCount;
     AdjointWave adj;      // adjoint launches only (adj.dLdI null otherwise)
+    // Adaptive passes (null otherwise): each chunk's 8x8 mask of the pixels it samples (bit y * 8 + x) and each
+    // pixel's first sample index of the pass (in place of the chunk's first).
+    const uint64_t* chunkMask;
+    const uint32_t* pixelBase;
     uint32_t refill;       // a warp fetches new rays once this many of its lanes are idle (1..32)
     uint32_t triLimit;     // triangle tests a lane makes a traversal step
     float4* out;          // per item: rgb, alpha

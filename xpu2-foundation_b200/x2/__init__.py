@@ -127,6 +127,10 @@ def wavefront_shape_defaults():
     return s
 
 
+class AdaptiveResult(C.Structure):
+    _fields_ = [("passes", C.c_uint32), ("converged", C.c_uint32), ("samples", C.c_uint64), ("milliseconds", C.c_float), ("pad", C.c_uint32)]
+
+
 class Completion(C.Structure):
     _fields_ = [("launch", C.c_uint64), ("samples", C.c_uint64), ("errors", C.c_uint64), ("milliseconds", C.c_float), ("pad", C.c_uint32)]
 
@@ -166,6 +170,8 @@ def library():
         "x2_wavefront_autotune": ([vp, u32, u32, C.POINTER(WavefrontShape), C.POINTER(C.c_float)], i32),
         "x2_scene_set_params": ([vp, vp, vp, vp], i32), "x2_adjoint": ([vp, u32, u32, vp, vp, vp, vp, vp], i32), "x2_adjoint_plain": ([vp, u32, u32, vp, vp, vp, vp, vp], i32),
         "x2_scene_set_texture": ([vp, u32, vp], i32),
+        "x2_frame_begin_adaptive": ([vp, u32], i32), "x2_adaptive_step": ([vp, C.c_float, u32, u32, vp, vp, vp], i32),
+        "x2_render_adaptive": ([vp, u32, u32, C.c_float, C.POINTER(AdaptiveResult)], i32), "x2_adaptive_planned": ([vp, vp], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
@@ -360,6 +366,31 @@ class Scene:
     # -- lane API --
     def frame_begin(self, samples_per_chunk):
         _check(library().x2_frame_begin(self._h, samples_per_chunk))
+
+    def frame_begin_adaptive(self, samples_per_chunk):
+        """x2_frame_begin_adaptive: a frame whose film also keeps the odd-index sums."""
+        _check(library().x2_frame_begin_adaptive(self._h, samples_per_chunk))
+
+    def adaptive_step(self, target, uniform, size):
+        """One adaptive chain step on the current film: (errors [pixels], tile masks [tiles] uint64, stop)."""
+        cfg = self.config
+        errors = np.empty(cfg.width * cfg.height, np.float32)
+        masks = np.empty(((cfg.width + 7) // 8) * ((cfg.height + 7) // 8), np.uint64)
+        stop = C.c_uint32()
+        _check(library().x2_adaptive_step(self._h, target, uniform, size, _ptr(errors), _ptr(masks), C.byref(stop)))
+        return errors, masks, stop.value
+
+    def render_adaptive(self, min_samples, max_samples, target):
+        """x2_render_adaptive: an adaptive frame; returns its AdaptiveResult as a dict."""
+        r = AdaptiveResult()
+        _check(library().x2_render_adaptive(self._h, min_samples, max_samples, target, C.byref(r)))
+        return {"passes": r.passes, "converged": bool(r.converged), "samples": r.samples, "milliseconds": r.milliseconds}
+
+    def adaptive_planned(self):
+        cfg = self.config
+        planned = np.empty(cfg.width * cfg.height, np.uint32)
+        _check(library().x2_adaptive_planned(self._h, _ptr(planned)))
+        return planned
 
     def launch(self, chunks):
         chunks = np.ascontiguousarray(chunks, dtype=CHUNK_DTYPE)
