@@ -298,8 +298,10 @@ typedef struct x2_adaptive_result {
  * MoonRay's pass schedule for max_samples (one sample, then 4, 6, 8, ... more), passes starting below min_samples
  * uniform, then after each pass the chain's errors, trees and masks; each pass renders its active tiles' masked pixels
  * in the wavefront form, each pixel from its own next sample index. Ends when every region has converged (target
- * error), a pass has no active pixel, or the schedule runs out. The film (sums, odd sums, counts) is then read as after
- * any launch; x2_adaptive_planned gives each pixel's planned count (for x2_audit). Waits. */
+ * error), a pass has no active pixel, or the schedule runs out. The whole frame is queued on the device at once (one
+ * graph: the chain, the active tiles' compaction and each pass's launch), so no pass waits on the host. The film (sums,
+ * odd sums, counts) is then read as after any launch; x2_adaptive_planned gives each pixel's planned count (for
+ * x2_audit). Waits. */
 int x2_render_adaptive(x2_scene* scene, uint32_t min_samples, uint32_t max_samples, float target, x2_adaptive_result* result);
 int x2_adaptive_planned(x2_scene* scene, uint32_t* planned);
 

@@ -222,6 +222,16 @@ def reference_pixel_errors(sums, odd, counts):
     return out
 
 
+def reference_adaptive_schedule(max_samples):
+    """The reference's pass schedule (async_adaptive.h schedule): [(start, end)] sample ranges a pixel."""
+    lib = C.CDLL(REFERENCE)
+    lib.x2ref_adaptive_schedule.argtypes = [C.c_uint32, C.c_void_p, C.c_uint32]
+    lib.x2ref_adaptive_schedule.restype = C.c_uint32
+    out = np.zeros(2 * 1024, np.uint32)
+    n = lib.x2ref_adaptive_schedule(max_samples, out.ctypes.data, 1024)
+    return [(int(out[2 * k]), int(out[2 * k + 1])) for k in range(min(n, 1024))]
+
+
 def reference_adaptive_masks(width, height, target, errors):
     """The reference's region trees (async_adaptive.h Regions) over per-pixel errors: (tile masks, all converged)."""
     lib = C.CDLL(REFERENCE)

@@ -65,3 +65,66 @@ def test_adaptive_frame(box):
     sel = (idx & 1) == 1
     np.add.at(odd_want, owner[sel], rgba[sel])
     assert np.allclose(odd[pix], odd_want, rtol=1e-9, atol=1e-12)
+
+
+@needs_reference
+def test_adaptive_frame_replays_reference_frame(box):
+    """The queued frame against the reference's adaptive frame replayed on the host: the reference's schedule, and
+    before each pass past the uniform ones its pixelError of the film so far and its region trees' masks; each active
+    pixel then takes the pass's next samples. Each pass's film is rebuilt from the samples' own radiance (the per-sample
+    API), summed as the device sums it (each pixel's samples of the pass in order, then added to the pixel), so the
+    replay's plan and film equal the device's bit for bit."""
+    s, scene = box
+    cfg = s.config
+    target, min_samples, max_samples = 0.0005, 4, 256
+    result = scene.render_adaptive(min_samples, max_samples, target)
+    planned = scene.adaptive_planned().astype(np.int64)
+    sums, odd, counts = scene.film(odd=True)
+    pixels = cfg.width * cfg.height
+    offsets = np.concatenate([[0], np.cumsum(planned)[:-1]])
+    pix = np.repeat(np.arange(pixels), planned).astype(np.uint32)
+    idx = (np.arange(int(planned.sum())) - np.repeat(offsets, planned)).astype(np.uint32)
+    rgba, status = scene.integrate(pix, idx)
+    assert (status == x2.DONE).all()
+    assert np.array_equal(rgba, rgba.astype(np.float32).astype(np.float64))
+    tiles_x = (cfg.width + 7) // 8
+    film = np.zeros((pixels, 4))
+    film_odd = np.zeros((pixels, 4))
+    film_counts = np.zeros(pixels, np.uint32)
+    plan = np.zeros(pixels, np.int64)
+    converged, passes = False, 0
+    for k, (start, end) in enumerate(oracle_lib.reference_adaptive_schedule(max_samples)):
+        size = end - start
+        if start < min_samples:
+            active = np.arange(pixels)
+        else:
+            errors = oracle_lib.reference_pixel_errors(film, film_odd, film_counts)
+            masks, done = oracle_lib.reference_adaptive_masks(cfg.width, cfg.height, target, errors)
+            if done:
+                converged = True
+                break
+            tiles = np.nonzero(masks)[0]
+            bits = ((masks[tiles, None] >> np.arange(64, dtype=np.uint64)) & np.uint64(1)).astype(bool)
+            t, b = np.nonzero(bits)
+            x = (tiles[t] % tiles_x) * 8 + b % 8
+            y = (tiles[t] // tiles_x) * 8 + b // 8
+            active = np.sort(y * cfg.width + x)
+            if len(active) == 0:
+                converged = True
+                break
+        assert (plan[active] + size <= planned[active]).all(), f"the replay wants more samples than the device planned at pass {k}"
+        first = offsets[active] + plan[active]
+        block = rgba[first[:, None] + np.arange(size)]  # active x size x 4, in sample order
+        film[active] += np.cumsum(block, axis=1)[:, -1]
+        is_odd = ((plan[active, None] + np.arange(size)) & 1).astype(bool)
+        film_odd[active] += np.cumsum(np.where(is_odd[:, :, None], block, 0.0), axis=1)[:, -1]
+        film_counts[active] += size
+        plan[active] += size
+        passes += 1
+    print(result, "replay: passes", passes, "converged", converged)
+    assert np.array_equal(plan, planned), f"{int(np.count_nonzero(plan != planned))} pixels planned differently"
+    assert result["passes"] == passes and bool(result["converged"]) == converged
+    assert np.array_equal(counts, film_counts)
+    assert np.array_equal(sums, film), f"max abs diff {np.abs(sums - film).max()}"
+    assert np.array_equal(odd, film_odd), f"max abs diff {np.abs(odd - film_odd).max()}"
+

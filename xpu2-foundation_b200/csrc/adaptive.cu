@@ -7,16 +7,21 @@
 
 namespace x2 {
 
-__global__ void adErrors(const double* sums, const double* odd, const uint32_t* counts, float* errors, uint32_t pixels) {
+// A queued frame's chain does nothing once the stop word is set.
+__device__ __forceinline__ bool halted(const AdaptiveArgs& a) { return a.queued && *(volatile const uint32_t*)a.stop; }
+
+__global__ void adErrors(AdaptiveArgs a, const double* sums, const double* odd, const uint32_t* counts) {
+    if (halted(a)) return;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= pixels) return;
-    errors[i] = ad::pixelError(sums + 4ull * i, odd + 4ull * i, counts[i]);
+    if (i >= a.width * a.height) return;
+    a.errors[i] = ad::pixelError(sums + 4ull * i, odd + 4ull * i, counts[i]);
 }
 
 // One block a region: the summed-area table of its errors (each row's running sums, then each column's, the sums in
 // the host's order), then its nodes a level at a time, each decided as the host's recursion decides it. A region with a
 // pixel not ready keeps its root alone, unconverged.
 __global__ void adTrees(AdaptiveArgs a) {
+    if (halted(a)) return;
     const uint32_t r = blockIdx.x;
     const ad::IBox root = a.regions[r];
     const int w = root.x1 - root.x0, h = root.y1 - root.y0, w1 = w + 1;
@@ -83,6 +88,7 @@ __global__ void adTrees(AdaptiveArgs a) {
 }
 
 __global__ void adMasks(AdaptiveArgs a, uint32_t uniform, uint32_t size) {
+    if (halted(a)) return;
     if (!uniform) {
         bool converged = true;
         for (uint32_t r = 0; r < a.regionCount; ++r) converged = converged && a.regionDone[r] != 0;
@@ -106,6 +112,50 @@ __global__ void adMasks(AdaptiveArgs a, uint32_t uniform, uint32_t size) {
             a.base[pixel] = a.planned[pixel];
             a.planned[pixel] += size;
         }
+}
+
+__global__ void adCompact(AdaptiveArgs a, uint32_t size) {
+    __shared__ uint32_t scan[kCompactThreads];
+    const uint32_t tid = threadIdx.x;
+    if (halted(a)) {
+        if (tid == 0) *a.live = 0;
+        return;
+    }
+    const uint32_t per = (a.tiles + kCompactThreads - 1) / kCompactThreads, first = tid * per;
+    const uint32_t last = first + per < a.tiles ? first + per : a.tiles;
+    uint32_t mine = 0;
+    unsigned long long pixels = 0;
+    for (uint32_t t = first; t < last; ++t) {
+        const uint64_t m = a.tileMask[t];
+        if (m) {
+            ++mine;
+            pixels += __popcll(m);
+        }
+    }
+    scan[tid] = mine;
+    __syncthreads();
+    for (uint32_t offset = 1; offset < kCompactThreads; offset <<= 1) {
+        const uint32_t v = tid >= offset ? scan[tid - offset] : 0u;
+        __syncthreads();
+        scan[tid] += v;
+        __syncthreads();
+    }
+    uint32_t at = scan[tid] - mine;
+    for (uint32_t t = first; t < last; ++t) {
+        const uint64_t m = a.tileMask[t];
+        if (m) {
+            a.chunks[at] = x2_chunk{t, 0, size, 0};
+            a.chunkMasks[at] = m;
+            ++at;
+        }
+    }
+    if (pixels) atomicAdd(a.samples, pixels * size);
+    if (tid == kCompactThreads - 1) {
+        const uint32_t total = scan[tid];
+        *a.live = total;
+        if (total) ++*a.passes;
+        else *a.stop = 1;
+    }
 }
 
 }  // namespace x2

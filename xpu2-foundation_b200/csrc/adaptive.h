@@ -4,6 +4,7 @@
 
 #include <cstdint>
 
+#include "../../include/x2.h"
 #include "adaptive.cuh"
 
 namespace x2 {
@@ -28,14 +29,27 @@ struct AdaptiveArgs {
     uint32_t* planned;
     uint32_t* base;
     uint32_t* stop;
+    // A frame queued on the device whole (x2_render_adaptive): once the stop word is set its chain steps do nothing
+    // (0: a step the host runs, x2_adaptive_step). Its pass's active tiles as chunks, their masks and their count,
+    // and the frame's tallies: passes launched and samples planned.
+    uint32_t queued;
+    x2_chunk* chunks;
+    uint64_t* chunkMasks;
+    uint32_t* live;
+    uint32_t* passes;
+    unsigned long long* samples;
 };
 
 // Every pixel's error from the film (FP64 sums and odd sums, 4 a pixel; counts).
-__global__ void adErrors(const double* sums, const double* odd, const uint32_t* counts, float* errors, uint32_t pixels);
+__global__ void adErrors(AdaptiveArgs a, const double* sums, const double* odd, const uint32_t* counts);
 // Each region's tree rebuilt from the errors, one block a region (regionDone: 1 converged, 0 not).
 __global__ void adTrees(AdaptiveArgs a);
 // Each tile's mask for a pass of `size` samples a pixel (every pixel in the image in a uniform pass), its pixels'
 // first sample indices and planned counts; a non-uniform pass whose regions have all converged sets the stop word.
 __global__ void adMasks(AdaptiveArgs a, uint32_t uniform, uint32_t size);
+// One block of kCompactThreads: a queued frame's pass's active tiles, in tile order, as chunks of `size` samples with
+// their masks, and their count; a pass with none sets the stop word (nothing can change after it).
+constexpr int kCompactThreads = 1024;
+__global__ void adCompact(AdaptiveArgs a, uint32_t size);
 
 }  // namespace x2

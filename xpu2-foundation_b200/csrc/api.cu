@@ -131,9 +131,18 @@ struct AdaptiveState {
     uint32_t* base = nullptr;
     uint32_t* stop = nullptr;
     uint64_t* chunkMasks = nullptr;  // a pass's active tiles' masks, in its chunks' order
+    // A queued frame's words: [0] the pass's active chunks, [1] passes launched, [2] the pass's drain iterations,
+    // [3] all passes' drain iterations, [4] a drain that hit its bound; its planned samples; their host copies (pinned).
+    uint32_t* words = nullptr;
+    unsigned long long* samples = nullptr;
+    uint32_t* hostWords = nullptr;
+    unsigned long long* hostSamples = nullptr;
     ~AdaptiveState() {
-        void* p[] = {regions, nodeOffset, nodeCapacity, satOffset, sat, nodes, regionDone, errors, inImage, tileMask, planned, base, stop, chunkMasks};
+        void* p[] = {regions, nodeOffset, nodeCapacity, satOffset, sat, nodes, regionDone, errors, inImage, tileMask, planned, base, stop, chunkMasks,
+                     words, samples};
         for (void* q : p) cudaFree(q);
+        if (hostWords) cudaFreeHost(hostWords);
+        if (hostSamples) cudaFreeHost(hostSamples);
     }
 };
 
@@ -181,7 +190,9 @@ struct x2_scene {
     float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};  // the vertices' bounds
     // wavefront
     WaveState wave{};
-    uint32_t wavePaths = 0, waveRecords = 0, reservePaths = 0;
+    uint32_t wavePaths = 0, waveRecords = 0, reservePaths = 0;  // the last launch's paths; records a path
+    uint32_t waveCap = 0;                                          // paths the wave's buffers hold
+    cudaGraphExec_t waveExec = nullptr;  // the last wavefront launch's drain graph, updated in place by the next
     uint32_t* extendQ = nullptr;
     uint32_t* shadowQ = nullptr;
     uint32_t* waveCounters = nullptr;  // kWaveCounters words
@@ -213,7 +224,7 @@ struct x2_scene {
     float4* adelta = nullptr;
     uint2* aaux = nullptr;
     float4* atex = nullptr;
-    uint32_t adjPaths = 0, adjVerts = 0, adjRecords = 0;
+    uint32_t adjPaths = 0, adjVerts = 0, adjRecords = 0;  // paths the adjoint's buffers hold; their vertices, records
 };
 
 namespace {
@@ -311,12 +322,17 @@ void freeWave(x2_scene* s) {
     cudaFree(s->shadowQ);
     cudaFree(s->shadeQ);
     s->extendQ = s->shadowQ = s->shadeQ = nullptr;
-    s->wavePaths = s->waveRecords = 0;
+    s->wavePaths = s->waveRecords = s->waveCap = 0;
 }
 
 // Path slots for `paths` paths with `records` shadow records each.
+// Buffers that already hold at least `paths` paths are kept (a launch indexes them by its own path count), so launches
+// of varying sizes (an adaptive frame's passes) allocate once.
 int ensureWave(x2_scene* s, uint32_t paths, uint32_t records) {
-    if (s->wavePaths == paths && s->waveRecords == records) return X2_OK;
+    if (paths <= s->waveCap && s->waveRecords == records) {
+        s->wavePaths = paths;
+        return X2_OK;
+    }
     freeWave(s);
     WaveState& w = s->wave;
     const size_t P = paths, R = size_t(paths) * records;
@@ -337,7 +353,7 @@ int ensureWave(x2_scene* s, uint32_t paths, uint32_t records) {
         setError("device allocation failed for %u wavefront paths", paths);
         return X2_ENOMEM;
     }
-    s->wavePaths = paths;
+    s->wavePaths = s->waveCap = paths;
     s->waveRecords = records;
     return X2_OK;
 }
@@ -776,6 +792,7 @@ int x2_scene_free(x2_scene* s) {
     cudaFree(s->volumeTris);
     cudaFree(s->grids);
     for (float* g : s->gridValues) cudaFree(g);
+    if (s->waveExec) cudaGraphExecDestroy(s->waveExec);
     freeWave(s);
     cudaFree(s->out);
     cudaFree(s->outStatus);
@@ -1119,6 +1136,44 @@ int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     return X2_OK;
 }
 
+namespace {
+// A single scene's wavefront launch of `count` chunks (sl.chunks) and `items` items over `paths` path slots.
+WaveArgs launchArgs(x2_scene* s, Slot& sl, uint32_t paths, uint32_t records, unsigned long long items, uint32_t count) {
+    WaveArgs a;
+    a.scene = viewOf(s);
+    a.w = s->wave;
+    a.paths = paths;
+    a.recordsPerPath = records;
+    a.chunks = sl.chunks;
+    a.itemCount = items;
+    a.samplesPerChunk = s->samplesPerChunk;
+    a.claimed = s->claimed;
+    a.extendQ = s->extendQ;
+    a.extendCount = s->waveCounters;
+    a.lastExtend = s->waveCounters + 1;
+    a.shadowQ = s->shadowQ;
+    a.shadowCount = s->waveCounters + 2;
+    a.extendNext = s->waveCounters + 3;
+    a.shadowNext = s->waveCounters + 4;
+    a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
+    a.shadeCount = s->waveCounters + 5;
+    a.adj = AdjointWave{};
+    a.chunkMask = s->launchMask;
+    a.pixelBase = s->launchBase;
+    a.liveChunks = nullptr;
+    a.refill = s->refill;
+    a.triLimit = s->triLimit;
+    a.out = s->out;
+    a.outStatus = s->outStatus;
+    a.counters = sl.counters;
+    a.scenes = nullptr;
+    a.chunkRequest = nullptr;
+    a.chunkItems = nullptr;
+    a.chunkCount = count;
+    return a;
+}
+}  // namespace
+
 int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     if (!s || !s->configured || !s->filmPixels || !s->samplesPerChunk) {
         setError("x2_frame_begin first");
@@ -1160,36 +1215,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     cudaMemsetAsync(s->waveCounters, 0, sizeof(uint32_t) * kWaveCounters, st);
     cudaMemsetAsync(sl.counters, 0, sizeof(Counters), st);
     cudaMemsetAsync(s->outStatus, X2_SKIP, items, st);
-    WaveArgs a;
-    a.scene = viewOf(s);
-    a.w = s->wave;
-    a.paths = paths;
-    a.recordsPerPath = records;
-    a.chunks = sl.chunks;
-    a.itemCount = items;
-    a.samplesPerChunk = s->samplesPerChunk;
-    a.claimed = s->claimed;
-    a.extendQ = s->extendQ;
-    a.extendCount = s->waveCounters;
-    a.lastExtend = s->waveCounters + 1;
-    a.shadowQ = s->shadowQ;
-    a.shadowCount = s->waveCounters + 2;
-    a.extendNext = s->waveCounters + 3;
-    a.shadowNext = s->waveCounters + 4;
-    a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
-    a.shadeCount = s->waveCounters + 5;
-    a.adj = AdjointWave{};
-    a.chunkMask = s->launchMask;
-    a.pixelBase = s->launchBase;
-    a.refill = s->refill;
-    a.triLimit = s->triLimit;
-    a.out = s->out;
-    a.outStatus = s->outStatus;
-    a.counters = sl.counters;
-    a.scenes = nullptr;
-    a.chunkRequest = nullptr;
-    a.chunkItems = nullptr;
-    a.chunkCount = count;
+    const WaveArgs a = launchArgs(s, sl, paths, records, items, count);
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
     const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr);
@@ -1269,11 +1295,26 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     }
     wfResetQueues<<<1, 32, 0, st>>>(a);  // the last iteration's extend count, for the host
     CUDA_OR(cudaStreamEndCapture(st, &graph), X2_ECUDA);
-    if (cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess) {
+    // The graph differs from the last launch's in its kernels' arguments at most (same kernels in the same order)
+    // unless the scene's shape changed: update the last executable graph in place, instantiate when that fails.
+    bool updated = false;
+    if (s->waveExec) {
+        cudaGraphExecUpdateResultInfo info;
+        updated = cudaGraphExecUpdate(s->waveExec, graph, &info) == cudaSuccess;
+        if (!updated) {
+            (void)cudaGetLastError();  // the failed update's status, not an error of the launch
+            cudaGraphExecDestroy(s->waveExec);
+            s->waveExec = nullptr;
+        }
+    }
+    if (!updated && cudaGraphInstantiate(&s->waveExec, graph, 0) != cudaSuccess) {
         cudaGraphDestroy(graph);
+        s->waveExec = nullptr;
         setError("graph instantiation failed");
         return X2_ECUDA;
     }
+    cudaGraphDestroy(graph);
+    exec = s->waveExec;
     cudaEventRecord(sl.begin, st);
     uint32_t iterations = 0;
     int rc = X2_OK;
@@ -1293,8 +1334,6 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
             break;
         }
     }
-    cudaGraphExecDestroy(exec);
-    cudaGraphDestroy(graph);
     if (rc) return rc;
     wfFilmReduce<<<int((64ull * count + 255) / 256), 256, 0, st>>>(a, count, s->sums, s->adaptive ? s->odd : nullptr, s->counts);
     CUDA_OR(cudaGetLastError(), X2_ECUDA);
@@ -1486,7 +1525,7 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     const uint32_t verts = s->config.max_depth + 1;
     if (int rc = ensureWave(s, paths, records)) return rc;
     if (int rc = ensureItems(s, items)) return rc;
-    if (s->adjPaths != paths || s->adjVerts != verts || s->adjRecords != records) {
+    if (s->adjPaths < paths || s->adjVerts != verts || s->adjRecords != records) {
         freeAdjointWave(s);
         const size_t V = size_t(paths) * verts;
         const bool ok = cudaMalloc(&s->avert, sizeof(uint4) * V) == cudaSuccess && cudaMalloc(&s->ascale, sizeof(float4) * V) == cudaSuccess &&
@@ -1561,6 +1600,7 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
                         s->atex, texGrad};
     a.chunkMask = nullptr;
     a.pixelBase = nullptr;
+    a.liveChunks = nullptr;
     const size_t shared = sizeof(float) * params;
     if (shared > 48 * 1024) {
         cudaFuncSetAttribute(wfLogicAdjoint, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shared));
@@ -1693,7 +1733,10 @@ int ensureAdaptive(x2_scene* s, float target) {
                     cudaMalloc(&a->tileMask, sizeof(uint64_t) * a->tiles) == cudaSuccess &&
                     cudaMalloc(&a->chunkMasks, sizeof(uint64_t) * a->tiles) == cudaSuccess &&
                     cudaMalloc(&a->planned, sizeof(uint32_t) * pixels) == cudaSuccess && cudaMalloc(&a->base, sizeof(uint32_t) * pixels) == cudaSuccess &&
-                    cudaMalloc(&a->stop, sizeof(uint32_t)) == cudaSuccess;
+                    cudaMalloc(&a->stop, sizeof(uint32_t)) == cudaSuccess && cudaMalloc(&a->words, sizeof(uint32_t) * 8) == cudaSuccess &&
+                    cudaMalloc(&a->samples, sizeof(unsigned long long)) == cudaSuccess &&
+                    cudaMallocHost(&a->hostWords, sizeof(uint32_t) * 8) == cudaSuccess &&
+                    cudaMallocHost(&a->hostSamples, sizeof(unsigned long long)) == cudaSuccess;
     if (!ok) {
         delete a;
         s->adaptiveState = nullptr;
@@ -1713,19 +1756,20 @@ int ensureAdaptive(x2_scene* s, float target) {
     return X2_OK;
 }
 
-x2::AdaptiveArgs adaptiveArgs(const AdaptiveState& a) {
+// The chain's arguments; a queued frame's (chunks: its compacted chunks) or a host-run step's (chunks null).
+x2::AdaptiveArgs adaptiveArgs(const AdaptiveState& a, x2_chunk* chunks = nullptr) {
     return x2::AdaptiveArgs{a.width, a.height, a.tilesX, a.tiles, a.regionCount, a.target, a.layout, a.regions, a.nodeOffset, a.nodeCapacity,
-                            a.satOffset, a.sat, a.nodes, a.regionDone, a.errors, a.inImage, a.tileMask, a.planned, a.base, a.stop};
+                            a.satOffset, a.sat, a.nodes, a.regionDone, a.errors, a.inImage, a.tileMask, a.planned, a.base, a.stop,
+                            chunks ? 1u : 0u, chunks, a.chunkMasks, a.words, a.words + 1, a.samples};
 }
 
 // One chain step on the frame's film: errors and trees (not in a uniform pass), then the pass's tile masks.
-int adaptiveChain(x2_scene* s, uint32_t uniform, uint32_t size) {
+int adaptiveChain(x2_scene* s, const x2::AdaptiveArgs& args, uint32_t uniform, uint32_t size) {
     AdaptiveState& a = *s->adaptiveState;
     cudaStream_t st = s->ctx->stream;
-    const x2::AdaptiveArgs args = adaptiveArgs(a);
     const uint32_t pixels = a.width * a.height;
     if (!uniform) {
-        x2::adErrors<<<(pixels + 255) / 256, 256, 0, st>>>(s->sums, s->odd, s->counts, a.errors, pixels);
+        x2::adErrors<<<(pixels + 255) / 256, 256, 0, st>>>(args, s->sums, s->odd, s->counts);
         x2::adTrees<<<a.regionCount, 512, 0, st>>>(args);
     }
     x2::adMasks<<<(a.tiles + 255) / 256, 256, 0, st>>>(args, uniform, size);
@@ -1756,7 +1800,7 @@ int x2_adaptive_step(x2_scene* s, float target, uint32_t uniform, uint32_t size,
     }
     if (int rc = x2_wait(s, 600000, nullptr)) return rc;
     if (int rc = ensureAdaptive(s, target)) return rc;
-    if (int rc = adaptiveChain(s, uniform, size)) return rc;
+    if (int rc = adaptiveChain(s, adaptiveArgs(*s->adaptiveState), uniform, size)) return rc;
     AdaptiveState& a = *s->adaptiveState;
     cudaStream_t st = s->ctx->stream;
     if (errors) cudaMemcpyAsync(errors, a.errors, sizeof(float) * a.width * a.height, cudaMemcpyDeviceToHost, st);
@@ -1766,69 +1810,159 @@ int x2_adaptive_step(x2_scene* s, float target, uint32_t uniform, uint32_t size,
     return X2_OK;
 }
 
+// The whole frame as one graph, queued at once: for each pass of the schedule the chain, the compaction of its active
+// tiles and the pass's wavefront launch, whose iterations run in a conditional while node until no path is left, then
+// its film reduce. The host waits once, at the frame's end; a pass that finds nothing to do costs a few empty launches.
 int x2_render_adaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float target, x2_adaptive_result* result) {
     if (!s || !s->configured || maxSamples == 0 || !(target > 0)) {
         setError("x2_render_adaptive: a configured scene, at least one sample and a positive target");
         return X2_EINVAL;
     }
+    if (s->config.bsdf_samples != 1) {
+        setError("the wavefront form takes one BSDF sample a lobe (bsdf_samples = 1)");
+        return X2_EINVAL;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
     const auto passes = adaptiveSchedule(maxSamples);
     uint32_t most = 0;
     for (const auto& p : passes) most = std::max(most, p.second - p.first);
     if (int rc = x2_frame_begin_adaptive(s, most)) return rc;
     if (int rc = ensureAdaptive(s, target)) return rc;
-    AdaptiveState& a = *s->adaptiveState;
+    if (int rc = checkDevice(s->ctx)) return rc;
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    AdaptiveState& ad = *s->adaptiveState;
+    const unsigned long long maxItems = (unsigned long long)ad.tiles * 64ull * most;
+    if (maxItems > 0xffffffffull) {
+        setError("x2_render_adaptive: %llu work items in a pass (at most 2^32 - 1)", maxItems);
+        return X2_EINVAL;
+    }
+    Slot& sl = s->slots[0];
+    if (int rc = ensureSlot(sl, ad.tiles)) return rc;
+    uint32_t paths = s->reservePaths ? s->reservePaths : (1u << 20);
+    if (paths > maxItems) paths = uint32_t(maxItems < 1024 ? 1024 : maxItems);
+    const uint32_t records = s->config.light_count * s->config.light_samples + 1;
+    if (int rc = ensureWave(s, paths, records)) return rc;
+    if (int rc = ensureItems(s, maxItems)) return rc;
     cudaStream_t st = s->ctx->stream;
-    cudaMemsetAsync(a.planned, 0, sizeof(uint32_t) * a.width * a.height, st);
-    cudaMemsetAsync(a.stop, 0, sizeof(uint32_t), st);
-    std::vector<uint64_t> masks(a.tiles);
-    std::vector<x2_chunk> chunks;
-    std::vector<uint64_t> chunkMasks;
-    x2_adaptive_result r{};
-    const auto t0 = std::chrono::steady_clock::now();
-    int rc = X2_OK;
-    for (size_t k = 0; k < passes.size() && rc == X2_OK; ++k) {
+    cudaMemsetAsync(ad.planned, 0, sizeof(uint32_t) * ad.width * ad.height, st);
+    cudaMemsetAsync(ad.stop, 0, sizeof(uint32_t), st);
+    cudaMemsetAsync(ad.words, 0, sizeof(uint32_t) * 8, st);
+    cudaMemsetAsync(ad.samples, 0, sizeof(unsigned long long), st);
+    cudaMemsetAsync(sl.counters, 0, sizeof(Counters), st);
+    CUDA_OR(cudaGetLastError(), X2_ECUDA);
+    const x2::AdaptiveArgs chain = adaptiveArgs(ad, sl.chunks);
+    WaveArgs a = launchArgs(s, sl, paths, records, maxItems, ad.tiles);
+    a.chunkMask = ad.chunkMasks;
+    a.pixelBase = ad.base;
+    a.liveChunks = ad.words;
+    const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
+    const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
+    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr);
+    const uint64_t bound = maxItems * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
+    const uint32_t maxIter = uint32_t(std::min<uint64_t>(bound, 0xffffffffu));
+
+    // The graph, built in segments: each captured onto the graph after the last segment's end nodes.
+    cudaGraph_t graph = nullptr;
+    CUDA_OR(cudaGraphCreate(&graph, 0), X2_ECUDA);
+    std::vector<cudaGraphNode_t> tail;
+    cudaError_t err = cudaSuccess;
+    auto check = [&](cudaError_t e) {
+        if (err == cudaSuccess && e != cudaSuccess) err = e;
+        return err == cudaSuccess;
+    };
+    auto beginSegment = [&](cudaGraph_t g, bool chained) {
+        return check(cudaStreamBeginCaptureToGraph(st, g, chained && !tail.empty() ? tail.data() : nullptr, nullptr,
+                                                   chained ? tail.size() : 0, cudaStreamCaptureModeThreadLocal));
+    };
+    auto endSegment = [&](bool chained) {
+        cudaStreamCaptureStatus status;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t n = 0;
+        const cudaError_t info = cudaStreamGetCaptureInfo(st, &status, nullptr, nullptr, &deps, &n);
+        if (info == cudaSuccess && chained) tail.assign(deps, deps + n);
+        cudaGraph_t out = nullptr;
+        check(info);
+        return check(cudaStreamEndCapture(st, &out));
+    };
+    for (size_t k = 0; k < passes.size() && err == cudaSuccess; ++k) {
         const uint32_t size = passes[k].second - passes[k].first;
         const uint32_t uniform = passes[k].first < minSamples ? 1u : 0u;
-        if ((rc = adaptiveChain(s, uniform, size))) break;
-        uint32_t stop = 0;
-        cudaMemcpyAsync(&stop, a.stop, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-        cudaMemcpyAsync(masks.data(), a.tileMask, sizeof(uint64_t) * a.tiles, cudaMemcpyDeviceToHost, st);
-        if (cudaStreamSynchronize(st) != cudaSuccess) {
-            rc = X2_ECUDA;
-            break;
-        }
-        if (stop) {
-            r.converged = 1;
-            break;
-        }
-        chunks.clear();
-        chunkMasks.clear();
-        uint64_t samples = 0;
-        for (uint32_t t = 0; t < a.tiles; ++t)
-            if (masks[t]) {
-                chunks.push_back(x2_chunk{t, 0, size, 0});
-                chunkMasks.push_back(masks[t]);
-                samples += uint64_t(__builtin_popcountll(masks[t])) * size;
-            }
-        if (chunks.empty()) {  // nothing left to sample: the frame ends
-            r.converged = 1;
-            break;
-        }
-        cudaMemcpyAsync(a.chunkMasks, chunkMasks.data(), sizeof(uint64_t) * chunkMasks.size(), cudaMemcpyHostToDevice, st);
-        s->launchMask = a.chunkMasks;
-        s->launchBase = a.base;
-        s->samplesPerChunk = size;
-        rc = x2_launch_wavefront(s, chunks.data(), uint32_t(chunks.size()));
-        s->launchMask = nullptr;
-        s->launchBase = nullptr;
-        s->samplesPerChunk = most;
-        if (rc == X2_OK) rc = x2_wait(s, 600000, nullptr);
-        r.passes++;
-        r.samples += samples;
+        a.samplesPerChunk = size;
+        a.itemCount = (unsigned long long)ad.tiles * 64ull * size;
+        if (!beginSegment(graph, true)) break;
+        adaptiveChain(s, chain, uniform, size);
+        x2::adCompact<<<1, x2::kCompactThreads, 0, st>>>(chain, size);
+        cudaMemsetAsync(s->wave.state, 0, sizeof(uint32_t) * paths, st);
+        cudaMemsetAsync(s->wave.ncount, 0, sizeof(uint32_t) * paths, st);
+        cudaMemsetAsync(s->claimed, 0, sizeof(unsigned long long), st);
+        cudaMemsetAsync(s->waveCounters, 0, sizeof(uint32_t) * kWaveCounters, st);
+        cudaMemsetAsync(s->outStatus, X2_SKIP, a.itemCount, st);
+        cudaMemsetAsync(ad.words + 2, 0, sizeof(uint32_t), st);
+        check(cudaGetLastError());
+        if (!endSegment(true)) break;
+        // The pass's drain: a while node whose body is one iteration and the test that decides the next.
+        cudaGraphConditionalHandle loop;
+        if (!check(cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault))) break;
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = loop;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (!check(cudaGraphAddNode(&node, graph, tail.data(), tail.size(), &cp))) break;
+        tail.assign(1, node);
+        if (!beginSegment(cp.conditional.phGraph_out[0], false)) break;
+        wfResetQueues<<<1, 32, 0, st>>>(a);
+        wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
+        wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
+        if (a.shadeQ) wfSortShade<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wfDrainCheck<<<1, 32, 0, st>>>(a, loop, ad.words + 2, maxIter, ad.words + 4);
+        check(cudaGetLastError());
+        if (!endSegment(false)) break;
+        if (!beginSegment(graph, true)) break;
+        wfFilmReduce<<<int((64ull * ad.tiles + 255) / 256), 256, 0, st>>>(a, ad.tiles, s->sums, s->odd, s->counts);
+        check(cudaGetLastError());
+        endSegment(true);
     }
+    cudaGraphExec_t exec = nullptr;
+    if (err == cudaSuccess) check(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess) {
+        setError("x2_render_adaptive: building the frame's graph: %s", cudaGetErrorString(err));
+        return X2_ECUDA;
+    }
+    cudaEventRecord(sl.begin, st);
+    check(cudaGraphLaunch(exec, st));
+    cudaEventRecord(sl.end, st);
+    cudaMemcpyAsync(sl.hostCounters, sl.counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(ad.hostWords, ad.words, sizeof(uint32_t) * 8, cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(ad.hostSamples, ad.samples, sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(ad.hostWords + 5, ad.stop, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
+    cudaEventRecord(sl.done, st);
+    sl.busy = true;
+    sl.seq = s->nextSeq++;
+    s->lastItems = 0;  // the passes' per-item outputs are not kept
+    int rc = x2_synchronize(s->ctx, 600000);
+    cudaGraphExecDestroy(exec);
+    if (err != cudaSuccess) {
+        setError("x2_render_adaptive: graph launch failed: %s", cudaGetErrorString(err));
+        return X2_ECUDA;
+    }
+    if (rc) return rc;
+    s->waveIterations = ad.hostWords[3];
+    if (ad.hostWords[4]) {
+        setError("x2_render_adaptive: a pass did not drain after %u iterations", maxIter);
+        return X2_EDEVICE;
+    }
+    x2_adaptive_result r{};
+    r.passes = ad.hostWords[1];
+    r.samples = *ad.hostSamples;
+    r.converged = ad.hostWords[5] ? 1u : 0u;
     r.milliseconds = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
     if (result) *result = r;
-    return rc;
+    return X2_OK;
 }
 
 int x2_adaptive_planned(x2_scene* s, uint32_t* planned) {
@@ -2049,6 +2183,7 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
         a.adj = AdjointWave{};
         a.chunkMask = nullptr;
         a.pixelBase = nullptr;
+        a.liveChunks = nullptr;
         a.refill = s0->refill;
         a.triLimit = s0->triLimit;
         a.out = s0->out;

@@ -153,6 +153,7 @@ extern "C" int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chu
     a.adj = AdjointWave{};
     a.chunkMask = nullptr;
     a.pixelBase = nullptr;
+    a.liveChunks = nullptr;
     a.refill = kDefaultRefill;
     a.triLimit = kDefaultTriLimit;
     a.out = reinterpret_cast<float4*>(base + kOut);

@@ -178,6 +178,7 @@ __device__ __forceinline__ void logicBody(const WaveArgs& a) {
     extern __shared__ float partial[];  // the adjoint's block partials
     const Layout at{a.adj.materials, a.adj.lights};
     if (kAdjoint) partialsBegin(partial, at);
+    const unsigned long long itemCount = a.liveChunks ? (unsigned long long)(*a.liveChunks) * 64ull * a.samplesPerChunk : a.itemCount;
     for (uint32_t base = blockIdx.x * blockDim.x; base < a.paths; base += gridDim.x * blockDim.x) {
         const uint32_t p = base + threadIdx.x;
         uint32_t st = p < a.paths ? w.state[p] : kTrace + 100;  // out of range: no work, no claim
@@ -262,7 +263,7 @@ __device__ __forceinline__ void logicBody(const WaveArgs& a) {
         }
         if (wants) {
             const unsigned long long item = first + __popc(want & ((1u << (threadIdx.x & 31u)) - 1u));
-            if (item < a.itemCount) {
+            if (item < itemCount) {
                 unsigned long long chunkFirst;
                 uint32_t perPixel;
                 const uint32_t chunkIndex = chunkOfItem<kBatch>(a, item, chunkFirst, perPixel);
@@ -663,11 +664,22 @@ __global__ void wfResetQueues(WaveArgs a) {
     }
 }
 
+__global__ void wfDrainCheck(WaveArgs a, cudaGraphConditionalHandle loop, uint32_t* iterations, uint32_t maxIterations,
+                             uint32_t* overrun) {
+    if (threadIdx.x != 0) return;
+    const uint32_t n = ++iterations[0];
+    ++iterations[1];
+    const bool more = *a.extendCount != 0;
+    if (more && n >= maxIterations) *overrun = 1;
+    cudaGraphSetConditional(loop, more && n < maxIterations ? 1u : 0u);
+}
+
 // The film: each (chunk, position)'s samples summed in sample order, then added to the pixel (async_gpu.cu:320-364's
 // sums and counts, without the per-sample atomics).
 __global__ void wfFilmReduce(WaveArgs a, uint32_t chunkCount, double* sums, double* odd, uint32_t* counts) {
     const uint32_t width = a.scene.config.width, height = a.scene.config.height;
     const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (a.liveChunks && *a.liveChunks < chunkCount) chunkCount = *a.liveChunks;
     if (i >= 64ull * chunkCount) return;
     const uint32_t chunkIndex = uint32_t(i / 64), position = uint32_t(i % 64);
     const x2_chunk chunk = a.chunks[chunkIndex];

@@ -71,6 +71,9 @@ struct WaveArgs {
     // pixel's first sample index of the pass (in place of the chunk's first).
     const uint64_t* chunkMask;
     const uint32_t* pixelBase;
+    // A launch queued before its chunks are known (an adaptive frame's pass): its chunk count in device memory, read
+    // when the launch runs; its items are that count x 64 x samplesPerChunk (null: itemCount and the count given).
+    const uint32_t* liveChunks;
     uint32_t refill;       // a warp fetches new rays once this many of its lanes are idle (1..32)
     uint32_t triLimit;     // triangle tests a lane makes a traversal step
     float4* out;          // per item: rgb, alpha
@@ -115,6 +118,11 @@ __global__ void wfLogicAdjoint(WaveArgs a);
 __global__ void wfShadeAdjoint(WaveArgs a);
 __global__ void wfGradRows(const float* rows, uint32_t rowCount, uint32_t params, double* grads);
 __global__ void wfResetQueues(WaveArgs a);
+// The drain loop's test, last in the body of a conditional while node: go on while the iteration extended a ray, at
+// most maxIterations times (then *overrun is set and the loop ends). iterations[0] counts this loop's iterations,
+// iterations[1] a running total.
+__global__ void wfDrainCheck(WaveArgs a, cudaGraphConditionalHandle loop, uint32_t* iterations, uint32_t maxIterations,
+                             uint32_t* overrun);
 __global__ void wfFilmReduce(WaveArgs a, uint32_t chunkCount, double* sums, double* odd, uint32_t* counts);
 __global__ void wfFilmReduceBatch(WaveArgs a, const BatchFilm* films);
 
