@@ -508,6 +508,39 @@ def probe_adaptive(args):
     ctx.close()
 
 
+def probe_workgrid(args):
+    """Config 1 (1920x1080, 64 spp) fed from the work grid by the GPU broker: the progressive order (ranges of 1, 1, 2,
+    then 4 samples; GPU-only cells of 64 px, 32 cellular workers) with launches of about one range of the image (32,400
+    chunks) and with the whole frame taken at once, beside the uniform wavefront frame; each film audited. Prints the
+    frame times and Msamples/s."""
+    import x2
+
+    ctx = x2.Context(0)
+    s = x2.SyntheticScene(1)
+    cfg = s.config
+    scene = x2.Scene(ctx, s.desc, cfg)
+    pixels = cfg.width * cfg.height
+    tiles = ((cfg.width + 7) // 8) * ((cfg.height + 7) // 8)
+    out = {"probe": "workgrid", "config": 1, "spp": cfg.spp, "samples": pixels * cfg.spp}
+    scene.frame_begin(cfg.spp)
+    scene.render_frame_wavefront(0, cfg.spp)  # warm-up
+    c = scene.wait()
+    scene.frame_begin(cfg.spp)
+    scene.render_frame_wavefront(0, cfg.spp)
+    c = scene.wait()
+    out["uniform_ms"] = c.milliseconds
+    for name, want in (("per_range", tiles), ("whole", 1 << 22)):
+        grid = x2.WorkGrid(cfg.width, cfg.height, cfg.spp, x2.workgrid_options(mode=x2.WORKGRID_GPU, samples_per_chunk=4))
+        r = scene.render_workgrid(grid, want)
+        scene.audit(np.full(pixels, cfg.spp, np.uint32))
+        out[name] = {"chunks_per_launch": want, "launches": r["launches"], "ms": r["milliseconds"], "gpu_ms": r["gpu_milliseconds"],
+                     "msamples_per_s": r["samples"] / r["milliseconds"] / 1e3}
+        grid.free()
+    print(json.dumps(out))
+    scene.free()
+    ctx.close()
+
+
 def probe(args):
     """One bounded launch for profilers (ncu): `--probe-tiles` evenly spaced tiles of config 1 at 64 spp, in one form;
     the wavefront form without its graph (`--probe-timed`) so each kernel launch is visible on its own."""
@@ -523,6 +556,8 @@ def probe(args):
         return probe_rmse(args)
     if args.probe == "adaptive":
         return probe_adaptive(args)
+    if args.probe == "workgrid":
+        return probe_workgrid(args)
     ctx = x2.Context(0)
     s = x2.SyntheticScene(1)
     cfg = s.config
@@ -560,7 +595,7 @@ def main():
     ap.add_argument("--impl", default="x2", choices=["x2", "reference"])
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--skip-plain", action="store_true")
-    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint", "rmse", "adaptive"], help="one bounded launch for a profiler, then exit")
+    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint", "rmse", "adaptive", "workgrid"], help="one bounded launch for a profiler, then exit")
     ap.add_argument("--probe-tiles", type=int, default=592)
     ap.add_argument("--probe-timed", action="store_true", help="wavefront probe without its graph (per-kernel launches)")
     ap.add_argument("--adjoint-only", action="store_true", help="adjoint probe: one primal frame, then one wavefront adjoint launch")

@@ -305,6 +305,73 @@ typedef struct x2_adaptive_result {
 int x2_render_adaptive(x2_scene* scene, uint32_t min_samples, uint32_t max_samples, float target, x2_adaptive_result* result);
 int x2_adaptive_planned(x2_scene* scene, uint32_t* planned);
 
+/* ---- the work grid: replaces Grid (async_grid.h:96-430) and the GPU feeder's claims (async_render.h:600-605,
+ * 780-797) ----
+ * The image in square cells, each with its queue of unstarted chunks (x2_chunk.cell: the chunk's cell) that any number
+ * of claimants take from, each chunk exactly once. A uniform frame's chunks are made at creation: its sample ranges
+ * (progressive: 1, 1, 2, then samples_per_chunk samples; else samples_per_chunk each) over every tile with pixels in
+ * the viewport, each cell's ordered by range and then tile; a claim reaches no further than its device's frontier (the
+ * least range still unclaimed among the cells the device works), an important cell one range further. Devices:
+ * X2_DEVICE_CPU, X2_DEVICE_GPU. Claims are thread-safe; appends have one writer. */
+enum { X2_DEVICE_CPU = 0, X2_DEVICE_GPU = 1 };
+enum { X2_WORKGRID_CPU = 0, X2_WORKGRID_GPU = 1, X2_WORKGRID_BOTH = 2 }; /* which devices own cells (GridOptions::mode) */
+typedef struct x2_workgrid x2_workgrid;
+typedef struct x2_workgrid_options {
+    uint32_t cell_size;          /* pixels, a multiple of 8 (default 64) */
+    uint32_t samples_per_chunk;  /* sample indices a chunk (default 4) */
+    int32_t mode;                /* X2_WORKGRID_*: both devices own cells in a checkerboard unless owners are given */
+    uint32_t progressive;        /* 1: the progressive order (default); 0: ranges of samples_per_chunk */
+    uint32_t sample_first, sample_count; /* a share of the frame: its sample indices [first, first + count) (count 0: all) */
+    uint32_t gpu_workers;        /* the GPU broker's cellular workers, each a share of a launch (default 32) */
+    uint32_t pad;
+} x2_workgrid_options;
+void x2_workgrid_options_defaults(x2_workgrid_options* options);
+/* A grid for a width x height frame of spp samples. owners: one word a cell (1: the GPU's), used in X2_WORKGRID_BOTH when
+ * owner_count equals the cell count (else the checkerboard, the GPU on even cells). empty: no chunks made (cells filled
+ * by x2_workgrid_append). viewport: min x, min y, max x, max y (half open; null: the image). */
+int x2_workgrid_create(uint32_t width, uint32_t height, uint32_t spp, const x2_workgrid_options* options, const uint32_t* owners,
+                   uint32_t owner_count, uint32_t empty, const int32_t* viewport, x2_workgrid** out);
+void x2_workgrid_free(x2_workgrid* grid);
+int x2_workgrid_info(const x2_workgrid* grid, uint32_t* width, uint32_t* height, uint32_t* spp, x2_workgrid_options* options);
+uint32_t x2_workgrid_cells(const x2_workgrid* grid);
+uint64_t x2_workgrid_total(const x2_workgrid* grid);  /* chunks published */
+/* The frame's sample ranges: (first, count) pairs, up to capacity of them written; returns how many there are. */
+uint32_t x2_workgrid_ranges(const x2_workgrid* grid, uint32_t* ranges, uint32_t capacity);
+int x2_workgrid_cell(const x2_workgrid* grid, uint32_t cell, uint32_t* owner, uint32_t* tiles, uint32_t* published, uint32_t* taken);
+int x2_workgrid_append(x2_workgrid* grid, uint32_t cell, const x2_chunk* chunks, uint32_t n);
+/* Up to n chunks of a cell for a device, none past what its frontier allows; returns how many (0 once closed). */
+uint32_t x2_workgrid_claim(x2_workgrid* grid, uint32_t cell, uint32_t n, x2_chunk* out, uint32_t device);
+uint32_t x2_workgrid_claimable(const x2_workgrid* grid, uint32_t cell, uint32_t device);
+uint32_t x2_workgrid_remaining(const x2_workgrid* grid, uint32_t cell);
+uint32_t x2_workgrid_empty(const x2_workgrid* grid);
+uint32_t x2_workgrid_frontier(const x2_workgrid* grid, uint32_t device);
+/* The cellular rules: the cell a worker of a device in cell `current` (~0u: none) works next, ~0u when it may take
+ * nothing now (Grid::choose); the starting cell of worker w of n (Grid::seed). */
+uint32_t x2_workgrid_choose(const x2_workgrid* grid, uint32_t device, uint32_t current, uint32_t salt);
+uint32_t x2_workgrid_seed(const x2_workgrid* grid, uint32_t device, uint32_t worker, uint32_t workers);
+/* Important parts first: each cell's score (below zero: not known yet); cells above the mean are important. */
+int x2_workgrid_set_scores(x2_workgrid* grid, const float* scores, uint32_t n);
+int x2_workgrid_set_suitability(x2_workgrid* grid, const float* gpu_probability, uint32_t n);
+/* The rights of passage's measurements: the GPU's chunk items a second, one CPU worker's samples a second, the CPU's
+ * workers, a GPU launch's target seconds. */
+int x2_workgrid_set_rates(x2_workgrid* grid, double gpu_items, double cpu_worker, uint32_t cpu_workers, double window);
+int x2_workgrid_rendered(x2_workgrid* grid, uint32_t cell, uint32_t device, uint64_t samples);
+void x2_workgrid_close(x2_workgrid* grid);  /* a drain: nothing is handed out any more */
+/* The GPU broker: its next launch's chunks, up to want, taken by its cellular workers (options.gpu_workers, seeded at
+ * the first call), a share each, from their cells by the cellular rules. Returns how many. */
+uint32_t x2_workgrid_take(x2_workgrid* grid, uint32_t want, x2_chunk* out);
+uint64_t x2_workgrid_stolen(const x2_workgrid* grid);  /* chunks the broker took from cells the CPU owns */
+typedef struct x2_workgrid_result {
+    uint64_t launches, chunks, samples;  /* wavefront launches made, chunks and samples rendered */
+    float milliseconds;                  /* host time of the whole frame */
+    float gpu_milliseconds;              /* the launches' device times, added */
+} x2_workgrid_result;
+/* A frame fed from a grid: the film cleared (x2_frame_begin), then launch after launch of up to chunks_per_launch
+ * chunks (the broker's takes, x2_workgrid_take, until the launch is full or nothing more is handed out), each rendered
+ * in the wavefront form and waited for, until the grid hands out nothing. The grid's size must be the scene's frame.
+ * Waits. */
+int x2_render_workgrid(x2_scene* scene, x2_workgrid* grid, uint32_t chunks_per_launch, x2_workgrid_result* result);
+
 /* ---- differentiation (no reference counterpart; config 4) ----
  * The differentiable parameters, set in place: each material's diffuse colour (a Lambert lobe's albedo; 3 floats a
  * material), each material's roughness (a GGX lobe's; 1 float a material) and each light's radiance (3 floats a

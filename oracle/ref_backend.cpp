@@ -13,6 +13,7 @@
 #define XPU2_PATHS_ONLY 1
 #include "async_integrator.h"
 #include "async_adaptive.h"
+#include "async_grid.h"
 
 #include "../include/x2.h"
 
@@ -1067,6 +1068,71 @@ int x2ref_sample_words(const x2_identity* ids, const uint32_t* dims, uint64_t n,
     }
     return X2_OK;
 }
+
+// ---- the reference's work grid (async_grid.h Grid), driven call by call ----
+void* x2ref_grid_open(uint32_t width, uint32_t height, uint32_t spp, uint32_t cellSize, uint32_t samplesPerChunk, int mode,
+                      int progressive, uint32_t sampleFirst, uint32_t sampleCount, const uint32_t* owners, uint32_t ownerCount,
+                      int empty, const int32_t* viewport) {
+    namespace A = xi::async;
+    A::GridOptions o;
+    o.cellSize = cellSize;
+    o.samplesPerChunk = samplesPerChunk;
+    o.mode = mode;
+    o.progressive = progressive != 0;
+    o.sampleFirst = sampleFirst;
+    o.sampleCount = sampleCount;
+    std::vector<A::Device> own;
+    for (uint32_t i = 0; owners && i < ownerCount; ++i) own.push_back(owners[i] ? A::Device::Gpu : A::Device::Cpu);
+    int view[4];
+    if (viewport)
+        for (int k = 0; k < 4; ++k) view[k] = viewport[k];
+    try {
+        return new A::Grid(width, height, spp, o, owners ? &own : nullptr, empty != 0, viewport ? view : nullptr);
+    } catch (...) {
+        return nullptr;
+    }
+}
+void x2ref_grid_free(void* g) { delete static_cast<xi::async::Grid*>(g); }
+uint32_t x2ref_grid_cells(void* g) { return static_cast<xi::async::Grid*>(g)->cellCount(); }
+uint64_t x2ref_grid_total(void* g) { return static_cast<xi::async::Grid*>(g)->totalChunks(); }
+uint32_t x2ref_grid_ranges(void* g, uint32_t* out, uint32_t capacity) {
+    const auto& r = static_cast<xi::async::Grid*>(g)->ranges();
+    for (size_t k = 0; k < r.size() && k < capacity; ++k) {
+        out[2 * k] = r[k].first;
+        out[2 * k + 1] = r[k].count;
+    }
+    return uint32_t(r.size());
+}
+uint32_t x2ref_grid_owner(void* g, uint32_t cell) { return uint32_t(static_cast<xi::async::Grid*>(g)->owner(cell)); }
+uint32_t x2ref_grid_claim(void* g, uint32_t cell, uint32_t n, x2_chunk* out, uint32_t device) {
+    static_assert(sizeof(xi::async::Chunk) == sizeof(x2_chunk), "chunk layouts");
+    return static_cast<xi::async::Grid*>(g)->claim(cell, n, reinterpret_cast<xi::async::Chunk*>(out), xi::async::Device(device));
+}
+uint32_t x2ref_grid_claimable(void* g, uint32_t cell, uint32_t device) {
+    return static_cast<xi::async::Grid*>(g)->claimable(cell, xi::async::Device(device));
+}
+uint32_t x2ref_grid_remaining(void* g, uint32_t cell) { return static_cast<xi::async::Grid*>(g)->remaining(cell); }
+uint32_t x2ref_grid_empty(void* g) { return static_cast<xi::async::Grid*>(g)->empty() ? 1u : 0u; }
+uint32_t x2ref_grid_frontier(void* g, uint32_t device) { return static_cast<xi::async::Grid*>(g)->frontier(xi::async::Device(device)); }
+uint32_t x2ref_grid_choose(void* g, uint32_t device, uint32_t current, uint32_t salt) {
+    return static_cast<xi::async::Grid*>(g)->choose(xi::async::Device(device), current, salt);
+}
+uint32_t x2ref_grid_seed(void* g, uint32_t device, uint32_t worker, uint32_t workers) {
+    return static_cast<xi::async::Grid*>(g)->seed(xi::async::Device(device), worker, workers);
+}
+void x2ref_grid_set_scores(void* g, const float* scores, uint32_t n) {
+    static_cast<xi::async::Grid*>(g)->setScores(std::vector<float>(scores, scores + n));
+}
+void x2ref_grid_set_suitability(void* g, const float* p, uint32_t n) {
+    static_cast<xi::async::Grid*>(g)->setSuitability(std::vector<float>(p, p + n));
+}
+void x2ref_grid_set_rates(void* g, double gpuItems, double cpuWorker, uint32_t cpuWorkers, double window) {
+    static_cast<xi::async::Grid*>(g)->setRates(gpuItems, cpuWorker, cpuWorkers, window);
+}
+void x2ref_grid_append(void* g, uint32_t cell, const x2_chunk* chunks, uint32_t n) {
+    static_cast<xi::async::Grid*>(g)->append(cell, reinterpret_cast<const xi::async::Chunk*>(chunks), n);
+}
+void x2ref_grid_close(void* g) { static_cast<xi::async::Grid*>(g)->close(); }
 
 // paths::childBranch (async_integrator.h:281-287), the reference's own.
 uint64_t x2ref_child_branch(uint64_t parent, uint32_t a, uint32_t b) { return xi::async::paths::childBranch(parent, a, b); }

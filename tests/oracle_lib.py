@@ -241,3 +241,124 @@ def reference_adaptive_masks(width, height, target, errors):
     done = np.zeros(1, np.uint32)
     lib.x2ref_adaptive_masks(width, height, target, errors.ctypes.data, masks.ctypes.data, done.ctypes.data)
     return masks, bool(done[0])
+
+
+class RefWorkGrid:
+    """The reference's own work grid (async_grid.h Grid, compiled from source into oracle/_ref), call by call, with the
+    same methods as x2.WorkGrid."""
+
+    def __init__(self, width, height, spp, options, owners=None, empty=False, viewport=None):
+        lib = self.lib = C.CDLL(REFERENCE)
+        vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
+        sig = {
+            "x2ref_grid_open": ([u32, u32, u32, u32, u32, C.c_int, C.c_int, u32, u32, vp, u32, C.c_int, vp], vp),
+            "x2ref_grid_free": ([vp], None), "x2ref_grid_cells": ([vp], u32), "x2ref_grid_total": ([vp], u64),
+            "x2ref_grid_ranges": ([vp, vp, u32], u32), "x2ref_grid_owner": ([vp, u32], u32),
+            "x2ref_grid_claim": ([vp, u32, u32, vp, u32], u32), "x2ref_grid_claimable": ([vp, u32, u32], u32),
+            "x2ref_grid_remaining": ([vp, u32], u32), "x2ref_grid_empty": ([vp], u32), "x2ref_grid_frontier": ([vp, u32], u32),
+            "x2ref_grid_choose": ([vp, u32, u32, u32], u32), "x2ref_grid_seed": ([vp, u32, u32, u32], u32),
+            "x2ref_grid_set_scores": ([vp, vp, u32], None), "x2ref_grid_set_suitability": ([vp, vp, u32], None),
+            "x2ref_grid_set_rates": ([vp, C.c_double, C.c_double, u32, C.c_double], None),
+            "x2ref_grid_append": ([vp, u32, vp, u32], None), "x2ref_grid_close": ([vp], None),
+        }
+        for name, (args, res) in sig.items():
+            f = getattr(lib, name)
+            f.argtypes = args
+            f.restype = res
+        own = None if owners is None else np.ascontiguousarray(owners, np.uint32)
+        view = None if viewport is None else np.ascontiguousarray(viewport, np.int32)
+        self._own, self._view = own, view
+        self._h = lib.x2ref_grid_open(width, height, spp, options.cell_size, options.samples_per_chunk, options.mode, options.progressive,
+                                      options.sample_first, options.sample_count, None if own is None else own.ctypes.data,
+                                      0 if own is None else len(own), int(bool(empty)), None if view is None else view.ctypes.data)
+        assert self._h, "the reference grid refused its arguments"
+
+    def free(self):
+        if self._h:
+            self.lib.x2ref_grid_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    @property
+    def cells(self):
+        return self.lib.x2ref_grid_cells(self._h)
+
+    @property
+    def total(self):
+        return self.lib.x2ref_grid_total(self._h)
+
+    def ranges(self):
+        out = np.zeros(2 * 4096, np.uint32)
+        n = self.lib.x2ref_grid_ranges(self._h, out.ctypes.data, 4096)
+        return [(int(out[2 * k]), int(out[2 * k + 1])) for k in range(n)]
+
+    def owner(self, cell):
+        return self.lib.x2ref_grid_owner(self._h, cell)
+
+    def claim(self, cell, n, device):
+        out = np.zeros(max(n, 1), x2.CHUNK_DTYPE)
+        got = self.lib.x2ref_grid_claim(self._h, cell, n, out.ctypes.data, device)
+        return out[:got]
+
+    def claimable(self, cell, device):
+        return self.lib.x2ref_grid_claimable(self._h, cell, device)
+
+    def remaining(self, cell):
+        return self.lib.x2ref_grid_remaining(self._h, cell)
+
+    def empty(self):
+        return bool(self.lib.x2ref_grid_empty(self._h))
+
+    def frontier(self, device):
+        return self.lib.x2ref_grid_frontier(self._h, device)
+
+    def choose(self, device, current, salt):
+        return self.lib.x2ref_grid_choose(self._h, device, current, salt)
+
+    def seed(self, device, worker, workers):
+        return self.lib.x2ref_grid_seed(self._h, device, worker, workers)
+
+    def set_scores(self, scores):
+        scores = np.ascontiguousarray(scores, np.float32)
+        self.lib.x2ref_grid_set_scores(self._h, scores.ctypes.data, len(scores))
+
+    def set_suitability(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        self.lib.x2ref_grid_set_suitability(self._h, p.ctypes.data, len(p))
+
+    def set_rates(self, gpu_items, cpu_worker, cpu_workers, window):
+        self.lib.x2ref_grid_set_rates(self._h, gpu_items, cpu_worker, cpu_workers, window)
+
+    def append(self, cell, chunks):
+        chunks = np.ascontiguousarray(chunks, dtype=x2.CHUNK_DTYPE)
+        self.lib.x2ref_grid_append(self._h, cell, chunks.ctypes.data, len(chunks))
+
+    def close(self):
+        self.lib.x2ref_grid_close(self._h)
+
+    def take(self, want, cells):
+        """The reference feeder's claims for one GPU launch (async_render.h:784-797), restated over this grid: `cells`
+        (the GPU's cellular workers' cells, seeded by the caller with seed()) move as the feeder moves them."""
+        out, got = [], 0
+        share = (want + len(cells) - 1) // len(cells)
+        for w in range(len(cells)):
+            if got >= want:
+                break
+            need, moves = min(share, want - got), 0
+            while need and moves < 8:
+                cell = self.choose(x2.DEVICE_GPU, cells[w], w)
+                if cell == 0xFFFFFFFF:
+                    break
+                cells[w] = cell
+                c = self.claim(cell, need, x2.DEVICE_GPU)
+                out.append(c)
+                got += len(c)
+                need -= len(c)
+                moves += 1
+        return np.concatenate(out) if out else np.zeros(0, x2.CHUNK_DTYPE)
+

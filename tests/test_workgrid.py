@@ -1,0 +1,179 @@
+"""The work grid (x2_workgrid_*, host side) against the reference's own Grid (async_grid.h, compiled from source into
+oracle/_ref), call by call: the same chunks in the same cells and order, the same claims, frontiers, cellular choices
+and starting cells, under the progressive and flat orders, shares of a frame, viewports, owners and scores; the GPU
+broker's launches against the reference feeder's claims restated over the reference grid; and claims from many threads
+taking every chunk exactly once."""
+import threading
+
+import numpy as np
+import pytest
+
+import oracle_lib
+from oracle_lib import RefWorkGrid, x2
+
+needs_reference = pytest.mark.skipif(not oracle_lib.have_reference(), reason="oracle/_ref not built")
+NONE = 0xFFFFFFFF
+
+CASES = [
+    # width, height, spp, options, owners, viewport
+    (256, 256, 64, {}, None, None),
+    (1000, 700, 37, {"cell_size": 32, "samples_per_chunk": 5}, None, None),
+    (517, 263, 16, {"progressive": 0, "samples_per_chunk": 3}, None, None),
+    (640, 480, 64, {"mode": x2.WORKGRID_GPU}, None, None),
+    (640, 480, 9, {"mode": x2.WORKGRID_CPU, "samples_per_chunk": 2}, None, None),
+    (384, 320, 64, {"sample_first": 16, "sample_count": 24}, None, None),
+    (384, 320, 20, {}, "random", None),
+    (300, 200, 12, {"samples_per_chunk": 8}, None, (37, 21, 250, 170)),
+]
+
+
+def _make(case):
+    width, height, spp, opts, owners, view = case
+    options = x2.workgrid_options(**opts)
+    cells = ((width + options.cell_size - 1) // options.cell_size) * ((height + options.cell_size - 1) // options.cell_size)
+    own = np.random.default_rng(width).integers(0, 2, cells).astype(np.uint32) if owners == "random" else None
+    mine = x2.WorkGrid(width, height, spp, options, owners=own, viewport=view)
+    ref = RefWorkGrid(width, height, spp, options, owners=own, viewport=view)
+    return mine, ref
+
+
+@needs_reference
+@pytest.mark.parametrize("case", CASES, ids=[f"{c[0]}x{c[1]}s{c[2]}-{i}" for i, c in enumerate(CASES)])
+def test_grid_layout_matches_reference(case):
+    mine, ref = _make(case)
+    assert mine.cells == ref.cells
+    assert mine.total == ref.total
+    assert mine.ranges() == ref.ranges()
+    for d in (x2.DEVICE_CPU, x2.DEVICE_GPU):
+        assert mine.frontier(d) == ref.frontier(d)
+    for i in range(mine.cells):
+        assert mine.cell(i)["owner"] == ref.owner(i)
+        assert mine.remaining(i) == ref.remaining(i)
+        for d in (x2.DEVICE_CPU, x2.DEVICE_GPU):
+            assert mine.claimable(i, d) == ref.claimable(i, d)
+    # Each cell's claimable chunks in queue order (as far as the frontier lets one claim reach).
+    for i in range(mine.cells):
+        a = mine.claim(i, 1 << 20, x2.DEVICE_GPU)
+        b = ref.claim(i, 1 << 20, x2.DEVICE_GPU)
+        assert np.array_equal(a, b)
+
+
+@needs_reference
+@pytest.mark.parametrize("case", CASES, ids=[f"{c[0]}x{c[1]}s{c[2]}-{i}" for i, c in enumerate(CASES)])
+def test_claims_and_choices_match_reference(case):
+    """A seeded script of claims by both devices' workers moving by the cellular rules, scores set part way, rates
+    set for the rights of passage, then a drain: every answer of both grids equal."""
+    mine, ref = _make(case)
+    rng = np.random.default_rng(case[2] * 7 + case[0])
+    cells = mine.cells
+    workers = {x2.DEVICE_CPU: [mine.seed(x2.DEVICE_CPU, w, 6) for w in range(6)], x2.DEVICE_GPU: [mine.seed(x2.DEVICE_GPU, w, 4) for w in range(4)]}
+    for d, ws in workers.items():
+        assert ws == [ref.seed(d, w, len(ws)) for w in range(len(ws))]
+    steps = 0
+    while steps < 4000:
+        steps += 1
+        if steps == 60:
+            scores = rng.random(cells).astype(np.float32)
+            scores[rng.random(cells) < 0.2] = -1.0
+            mine.set_scores(scores)
+            ref.set_scores(scores)
+        if steps == 120:
+            p = rng.random(cells).astype(np.float32)
+            mine.set_suitability(p)
+            ref.set_suitability(p)
+            mine.set_rates(2e6, 1e4, 6, 0.02)
+            ref.set_rates(2e6, 1e4, 6, 0.02)
+        d = int(rng.integers(0, 2))
+        w = int(rng.integers(0, len(workers[d])))
+        cur = workers[d][w]
+        a = mine.choose(d, cur, w)
+        b = ref.choose(d, cur, w)
+        assert a == b, f"step {steps}: choose({d}, {cur}, {w})"
+        for dd in (x2.DEVICE_CPU, x2.DEVICE_GPU):
+            assert mine.frontier(dd) == ref.frontier(dd)
+        if a == NONE:
+            if mine.empty():
+                assert ref.empty()
+                break
+            continue
+        workers[d][w] = a
+        n = int(rng.integers(1, 9))
+        assert np.array_equal(mine.claim(a, n, d), ref.claim(a, n, d)), f"step {steps}: claim({a}, {n}, {d})"
+    assert mine.empty() == ref.empty()
+    for i in range(cells):
+        assert mine.remaining(i) == ref.remaining(i)
+
+
+@needs_reference
+@pytest.mark.parametrize("want", [1, 7, 64, 1024, 1 << 20])
+def test_broker_launches_match_reference_feeder(want):
+    """The GPU broker's launches (x2_workgrid_take) against the reference feeder's claims over the reference grid, a
+    GPU-only progressive frame drained launch by launch."""
+    options = x2.workgrid_options(mode=x2.WORKGRID_GPU, gpu_workers=32)
+    mine = x2.WorkGrid(720, 480, 24, options)
+    ref = RefWorkGrid(720, 480, 24, options)
+    cells = [ref.seed(x2.DEVICE_GPU, w, 32) for w in range(32)]
+    launches = 0
+    while True:
+        a = mine.take(want)
+        b = ref.take(want, cells)
+        assert np.array_equal(a, b), f"launch {launches}"
+        if not len(a):
+            break
+        launches += 1
+    assert mine.empty() and ref.empty()
+    assert launches >= 1
+
+
+def test_progressive_ranges_and_frontier():
+    g = x2.WorkGrid(128, 128, 20, x2.workgrid_options(mode=x2.WORKGRID_GPU, samples_per_chunk=4))
+    assert g.ranges() == [(0, 1), (1, 1), (2, 2), (4, 4), (8, 4), (12, 4), (16, 4)]
+    flat = x2.WorkGrid(128, 128, 10, x2.workgrid_options(progressive=0, samples_per_chunk=4))
+    assert flat.ranges() == [(0, 4), (4, 4), (8, 2)]
+    share = x2.WorkGrid(128, 128, 64, x2.workgrid_options(sample_first=10, sample_count=7))
+    assert share.ranges() == [(10, 1), (11, 1), (12, 2), (14, 3)]
+    # The frontier holds each cell to the least range still unclaimed anywhere: cell 0 drains range 0 only.
+    tiles = g.cell(0)["tiles"]
+    assert tiles == 64
+    got = g.claim(0, 1000, x2.DEVICE_GPU)
+    assert len(got) == tiles and set(got["first"]) == {0}
+    assert g.frontier(x2.DEVICE_GPU) == 0
+    for i in range(1, g.cells):
+        g.claim(i, 1000, x2.DEVICE_GPU)
+    assert g.frontier(x2.DEVICE_GPU) == 1
+    # A closed grid hands out nothing.
+    g.close()
+    assert g.empty() and len(g.claim(0, 10, x2.DEVICE_GPU)) == 0
+
+
+def test_claims_from_many_threads_take_each_chunk_once():
+    g = x2.WorkGrid(512, 512, 32, x2.workgrid_options(mode=x2.WORKGRID_GPU, progressive=0, samples_per_chunk=2))
+    total = g.total
+    taken = [[] for _ in range(8)]
+
+    def worker(k):
+        rng = np.random.default_rng(k)
+        while not g.empty():
+            cell = int(rng.integers(0, g.cells))
+            c = g.claim(cell, int(rng.integers(1, 17)), x2.DEVICE_GPU)
+            if len(c):
+                taken[k].append(c)
+
+    threads = [threading.Thread(target=worker, args=(k,)) for k in range(8)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    allc = np.concatenate([c for t in taken for c in t])
+    assert len(allc) == total
+    keys = allc["tile"].astype(np.int64) * 1000 + allc["first"]
+    assert len(np.unique(keys)) == total
+
+
+def test_bad_grids_are_refused():
+    with pytest.raises(x2.X2Error):
+        x2.WorkGrid(0, 10, 4)
+    with pytest.raises(x2.X2Error):
+        x2.WorkGrid(64, 64, 4, x2.workgrid_options(cell_size=12))
+    with pytest.raises(x2.X2Error):
+        x2.WorkGrid(64, 64, 4, x2.workgrid_options(mode=3))

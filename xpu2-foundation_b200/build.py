@@ -12,7 +12,7 @@ CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "x2", "libx2.so")
 BUILD = os.path.join(HERE, "_build")
 CU = ["api.cu", "render.cu", "wavefront.cu", "bvh_build.cu", "noalloc.cu", "adjoint.cu", "adaptive.cu"]
-CPP = ["scene_gen.cpp"]
+CPP = ["scene_gen.cpp", "grid.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-fmad=false", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

@@ -1965,6 +1965,62 @@ int x2_render_adaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, fl
     return X2_OK;
 }
 
+// ---- the work grid's GPU broker (row f1): launches fed from a grid (grid.cpp), as the reference's feeder feeds
+// its GPU lane (async_render.h:780-797) ----
+int x2_render_workgrid(x2_scene* s, x2_workgrid* g, uint32_t want, x2_workgrid_result* result) {
+    uint32_t width = 0, height = 0, spp = 0;
+    x2_workgrid_options o;
+    if (!s || !s->configured || !g || !want || x2_workgrid_info(g, &width, &height, &spp, &o) != X2_OK) {
+        setError("x2_render_workgrid: a configured scene, a grid and at least one chunk a launch");
+        return X2_EINVAL;
+    }
+    if (width != s->config.width || height != s->config.height) {
+        setError("x2_render_workgrid: a %ux%u grid for a %ux%u frame", width, height, s->config.width, s->config.height);
+        return X2_EINVAL;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    if (int rc = x2_frame_begin(s, o.samples_per_chunk)) return rc;
+    std::vector<x2_chunk> chunks(want);
+    const uint32_t tilesX = (width + 7) / 8;
+    x2_workgrid_result r{};
+    int rc = X2_OK;
+    for (;;) {
+        // A launch holds up to `want` chunks: the broker's takes until it is full or nothing more is handed out (each
+        // take moves the frontier on as it claims, so one launch may span several ranges).
+        uint32_t got = 0;
+        while (got < want) {
+            const uint32_t n = x2_workgrid_take(g, want - got, chunks.data() + got);
+            if (!n) break;
+            got += n;
+        }
+        if (!got) break;
+        // The launch's items are its chunks x 64 x its largest count (the progressive order's first ranges are short).
+        uint32_t most = 1;
+        uint64_t samples = 0;
+        for (uint32_t i = 0; i < got; ++i) {
+            const x2_chunk& c = chunks[i];
+            most = std::max(most, c.count);
+            const uint32_t x = (c.tile % tilesX) * 8, y = (c.tile / tilesX) * 8;
+            const uint64_t pixels = uint64_t(std::min(8u, width - x)) * std::min(8u, height - y);
+            samples += pixels * c.count;
+            x2_workgrid_rendered(g, c.cell, X2_DEVICE_GPU, pixels * c.count);
+        }
+        s->samplesPerChunk = most;
+        rc = x2_launch_wavefront(s, chunks.data(), got);
+        s->samplesPerChunk = o.samples_per_chunk;
+        x2_completion c{};
+        if (rc == X2_OK) rc = x2_wait(s, 600000, &c);
+        if (rc) break;
+        r.launches++;
+        r.chunks += got;
+        r.samples += samples;
+        r.gpu_milliseconds += c.milliseconds;
+    }
+    r.milliseconds = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    if (result) *result = r;
+    return rc;
+}
+
 int x2_adaptive_planned(x2_scene* s, uint32_t* planned) {
     if (!s || !planned || !s->adaptiveState) {
         setError("x2_adaptive_planned: no adaptive frame");

@@ -131,6 +131,16 @@ class AdaptiveResult(C.Structure):
     _fields_ = [("passes", C.c_uint32), ("converged", C.c_uint32), ("samples", C.c_uint64), ("milliseconds", C.c_float), ("pad", C.c_uint32)]
 
 
+class WorkGridOptions(C.Structure):
+    _fields_ = [("cell_size", C.c_uint32), ("samples_per_chunk", C.c_uint32), ("mode", C.c_int32), ("progressive", C.c_uint32),
+                ("sample_first", C.c_uint32), ("sample_count", C.c_uint32), ("gpu_workers", C.c_uint32), ("pad", C.c_uint32)]
+
+
+class WorkGridResult(C.Structure):
+    _fields_ = [("launches", C.c_uint64), ("chunks", C.c_uint64), ("samples", C.c_uint64), ("milliseconds", C.c_float),
+                ("gpu_milliseconds", C.c_float)]
+
+
 class Completion(C.Structure):
     _fields_ = [("launch", C.c_uint64), ("samples", C.c_uint64), ("errors", C.c_uint64), ("milliseconds", C.c_float), ("pad", C.c_uint32)]
 
@@ -175,6 +185,20 @@ def library():
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
+        "x2_workgrid_options_defaults": ([C.POINTER(WorkGridOptions)], None),
+        "x2_workgrid_create": ([u32, u32, u32, C.POINTER(WorkGridOptions), vp, u32, u32, vp, C.POINTER(vp)], i32),
+        "x2_workgrid_free": ([vp], None), "x2_workgrid_info": ([vp, vp, vp, vp, C.POINTER(WorkGridOptions)], i32),
+        "x2_workgrid_cells": ([vp], u32), "x2_workgrid_total": ([vp], u64), "x2_workgrid_ranges": ([vp, vp, u32], u32),
+        "x2_workgrid_cell": ([vp, u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)], i32),
+        "x2_workgrid_append": ([vp, u32, vp, u32], i32), "x2_workgrid_claim": ([vp, u32, u32, vp, u32], u32),
+        "x2_workgrid_claimable": ([vp, u32, u32], u32), "x2_workgrid_remaining": ([vp, u32], u32), "x2_workgrid_empty": ([vp], u32),
+        "x2_workgrid_frontier": ([vp, u32], u32), "x2_workgrid_choose": ([vp, u32, u32, u32], u32),
+        "x2_workgrid_seed": ([vp, u32, u32, u32], u32), "x2_workgrid_set_scores": ([vp, vp, u32], i32),
+        "x2_workgrid_set_suitability": ([vp, vp, u32], i32),
+        "x2_workgrid_set_rates": ([vp, C.c_double, C.c_double, u32, C.c_double], i32),
+        "x2_workgrid_rendered": ([vp, u32, u32, u64], i32), "x2_workgrid_close": ([vp], None),
+        "x2_workgrid_take": ([vp, u32, vp], u32), "x2_workgrid_stolen": ([vp], u64),
+        "x2_render_workgrid": ([vp, vp, u32, C.POINTER(WorkGridResult)], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -386,6 +410,12 @@ class Scene:
         _check(library().x2_render_adaptive(self._h, min_samples, max_samples, target, C.byref(r)))
         return {"passes": r.passes, "converged": bool(r.converged), "samples": r.samples, "milliseconds": r.milliseconds}
 
+    def render_workgrid(self, grid, chunks_per_launch):
+        """x2_render_workgrid: a frame fed from a work grid by the GPU broker; returns its WorkGridResult as a dict."""
+        r = WorkGridResult()
+        _check(library().x2_render_workgrid(self._h, grid._h, chunks_per_launch, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in WorkGridResult._fields_}
+
     def adaptive_planned(self):
         cfg = self.config
         planned = np.empty(cfg.width * cfg.height, np.uint32)
@@ -536,3 +566,112 @@ def image(sums, counts, width, height):
     """The film's pixel values: (sum over samples) / count, rgba, as the reference's merge does."""
     c = np.maximum(counts, 1).astype(np.float64)[:, None]
     return (sums / c).reshape(height, width, 4)
+
+
+DEVICE_CPU, DEVICE_GPU = 0, 1
+WORKGRID_CPU, WORKGRID_GPU, WORKGRID_BOTH = 0, 1, 2
+
+
+def workgrid_options(**kw):
+    """The work grid's options (x2_workgrid_options_defaults), with the given fields changed."""
+    o = WorkGridOptions()
+    library().x2_workgrid_options_defaults(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+class WorkGrid:
+    """The work grid (x2_workgrid_*): cells of chunk queues, claims, frontiers and the cellular choice; host-side."""
+
+    def __init__(self, width, height, spp, options=None, owners=None, empty=False, viewport=None):
+        self.options = options if options is not None else workgrid_options()
+        own = None if owners is None else np.ascontiguousarray(owners, np.uint32)
+        view = None if viewport is None else np.ascontiguousarray(viewport, np.int32)
+        h = C.c_void_p()
+        _check(library().x2_workgrid_create(width, height, spp, C.byref(self.options), _ptr(own) if own is not None else None,
+                                            0 if own is None else len(own), int(bool(empty)),
+                                            _ptr(view) if view is not None else None, C.byref(h)))
+        self._h = h
+
+    def free(self):
+        if self._h:
+            library().x2_workgrid_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    @property
+    def cells(self):
+        return library().x2_workgrid_cells(self._h)
+
+    @property
+    def total(self):
+        return library().x2_workgrid_total(self._h)
+
+    def ranges(self):
+        n = library().x2_workgrid_ranges(self._h, None, 0)
+        out = np.zeros(2 * max(n, 1), np.uint32)
+        library().x2_workgrid_ranges(self._h, _ptr(out), n)
+        return [(int(out[2 * k]), int(out[2 * k + 1])) for k in range(n)]
+
+    def cell(self, i):
+        v = [C.c_uint32() for _ in range(4)]
+        _check(library().x2_workgrid_cell(self._h, i, *[C.byref(x) for x in v]))
+        return dict(zip(("owner", "tiles", "published", "taken"), (x.value for x in v)))
+
+    def append(self, cell, chunks):
+        chunks = np.ascontiguousarray(chunks, dtype=CHUNK_DTYPE)
+        _check(library().x2_workgrid_append(self._h, cell, _ptr(chunks), len(chunks)))
+
+    def claim(self, cell, n, device):
+        out = np.zeros(max(n, 1), CHUNK_DTYPE)
+        got = library().x2_workgrid_claim(self._h, cell, n, _ptr(out), device)
+        return out[:got]
+
+    def claimable(self, cell, device):
+        return library().x2_workgrid_claimable(self._h, cell, device)
+
+    def remaining(self, cell):
+        return library().x2_workgrid_remaining(self._h, cell)
+
+    def empty(self):
+        return bool(library().x2_workgrid_empty(self._h))
+
+    def frontier(self, device):
+        return library().x2_workgrid_frontier(self._h, device)
+
+    def choose(self, device, current, salt):
+        return library().x2_workgrid_choose(self._h, device, current, salt)
+
+    def seed(self, device, worker, workers):
+        return library().x2_workgrid_seed(self._h, device, worker, workers)
+
+    def set_scores(self, scores):
+        scores = np.ascontiguousarray(scores, np.float32)
+        _check(library().x2_workgrid_set_scores(self._h, _ptr(scores), len(scores)))
+
+    def set_suitability(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        _check(library().x2_workgrid_set_suitability(self._h, _ptr(p), len(p)))
+
+    def set_rates(self, gpu_items, cpu_worker, cpu_workers, window):
+        _check(library().x2_workgrid_set_rates(self._h, gpu_items, cpu_worker, cpu_workers, window))
+
+    def close(self):
+        library().x2_workgrid_close(self._h)
+
+    def take(self, want):
+        """The GPU broker's next launch: up to `want` chunks (x2_workgrid_take)."""
+        out = np.zeros(max(want, 1), CHUNK_DTYPE)
+        got = library().x2_workgrid_take(self._h, want, _ptr(out))
+        return out[:got]
+
+    @property
+    def stolen(self):
+        return library().x2_workgrid_stolen(self._h)
+
