@@ -582,19 +582,26 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
             setError("triangle %llu: vertex index out of range", (unsigned long long)(i / 3));
             return X2_EINVAL;
         }
+    // The vertices' bounds. Coordinates are finite and within 1e14 of the origin: the traversal's slab arithmetic
+    // (traverse.cuh visitNode) scales a node's quantum by 2^23 and must stay finite.
+    float lo[3] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f}, hi[3] = {-3.402823466e38f, -3.402823466e38f, -3.402823466e38f};
+    for (uint64_t i = 0; i < uint64_t(d->triangle_count) * 3; ++i)
+        for (int k = 0; k < 3; ++k) {
+            const float v = d->vertices[3 * size_t(d->triangles[i]) + k];
+            if (!(fabsf(v) <= 1e14f)) {
+                setError("triangle %llu: a vertex coordinate %g is not finite or beyond 1e14", (unsigned long long)(i / 3), double(v));
+                return X2_EINVAL;
+            }
+            lo[k] = v < lo[k] ? v : lo[k];
+            hi[k] = v > hi[k] ? v : hi[k];
+        }
     auto* s = new x2_scene();
     s->ctx = ctx;
     s->camera = d->camera;
     for (int k = 0; k < 3; ++k) {
-        s->lo[k] = 3.402823466e38f;
-        s->hi[k] = -3.402823466e38f;
+        s->lo[k] = lo[k];
+        s->hi[k] = hi[k];
     }
-    for (uint64_t i = 0; i < uint64_t(d->triangle_count) * 3; ++i)
-        for (int k = 0; k < 3; ++k) {
-            const float v = d->vertices[3 * size_t(d->triangles[i]) + k];
-            s->lo[k] = v < s->lo[k] ? v : s->lo[k];
-            s->hi[k] = v > s->hi[k] ? v : s->hi[k];
-        }
     s->lightCount = d->light_count;
     s->triangleCount = d->triangle_count;
     s->materialCount = d->material_count;

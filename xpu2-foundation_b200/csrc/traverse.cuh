@@ -120,18 +120,19 @@ __device__ __forceinline__ float min3f(float a, float b, float c) {
     return r;
 }
 
-// Byte j of w as an exact float: 0x4B0000bb is 2^23 + bb, less 2^23 (a byte permute and an add, no conversion).
-__device__ __forceinline__ float qbyte(uint32_t w, int j) {
-    return __fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | uint32_t(j))), 8388608.0f);
-}
+// Byte j of w with 2^23 added, as an exact float: 0x4B0000bb is 2^23 + bb (one byte permute, no conversion).
+__device__ __forceinline__ float qbyte23(uint32_t w, int j) { return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | uint32_t(j))); }
 
 // One node: the hit mask (bits 24..31 internal children in traversal order, 0..23 leaf triangles), its child and
 // triangle bases and its internal-child mask.
 //
-// Conservative by construction: the quantised child boxes contain the exact ones (the build rounds outward), and the
-// computed slab distance q * s + a = q * 2^e * (1/d) + (p - o) * (1/d) differs from the exact one by at most four
-// roundings of its terms (1/d, p - o, the product, the FMA), under 2^-22 (|a| + 255 |s|); every slab is widened by
-// 2^-21 (|a| + 255 |s|) each way, folded into the constant term.
+// Conservative by construction: the quantised child boxes contain the exact ones (the build rounds outward). The slab
+// distance q * s + a (s = 2^e * (1/d), a = (p - o) * (1/d)) is computed as one FMA of the byte with 2^23 added,
+// (2^23 + q) * s + c with c = (a -+ w) - 2^23 s, which saves the byte's conversion: against q * s + a exactly, it errs
+// by the four roundings of a and s (under 2^-22 (|a| + 255 |s|)), by c's rounding at the magnitude of 2^23 s (at most
+// |s| / 2 + 2^-24 (|a| + w)) and by the FMA's (under 2^-24 (|a| + 257 |s| + w)). Every slab is widened by
+// w = |s| / 2 + 2^-19 (|a| + 256 |s|) each way, which covers them; 2^23 s stays finite for the scene extents the
+// loader admits.
 __device__ __forceinline__ uint32_t visitNode(const Node8* __restrict__ nodes, uint32_t index, const RayQ& r, float tmin, float tmax,
                                               uint32_t& childBase, uint32_t& triBase, uint32_t& imask) {
     const uint4* p = reinterpret_cast<const uint4*>(nodes + index);
@@ -143,9 +144,12 @@ __device__ __forceinline__ uint32_t visitNode(const Node8* __restrict__ nodes, u
     triBase = n1.y;
     const float sx = __uint_as_float(ex << 23) * r.ix, sy = __uint_as_float(ey << 23) * r.iy, sz = __uint_as_float(ez << 23) * r.iz;
     const float ax = (px - r.ox) * r.ix, ay = (py - r.oy) * r.iy, az = (pz - r.oz) * r.iz;
-    const float wx = (fabsf(ax) + 255.0f * fabsf(sx)) * 0x1p-21f, wy = (fabsf(ay) + 255.0f * fabsf(sy)) * 0x1p-21f,
-                wz = (fabsf(az) + 255.0f * fabsf(sz)) * 0x1p-21f;
-    const float axn = ax - wx, axf = ax + wx, ayn = ay - wy, ayf = ay + wy, azn = az - wz, azf = az + wz;
+    const float wx = 0.5f * fabsf(sx) + (fabsf(ax) + 256.0f * fabsf(sx)) * 0x1p-19f,
+                wy = 0.5f * fabsf(sy) + (fabsf(ay) + 256.0f * fabsf(sy)) * 0x1p-19f,
+                wz = 0.5f * fabsf(sz) + (fabsf(az) + 256.0f * fabsf(sz)) * 0x1p-19f;
+    const float axn = __fmaf_rn(-8388608.0f, sx, ax - wx), axf = __fmaf_rn(-8388608.0f, sx, ax + wx);
+    const float ayn = __fmaf_rn(-8388608.0f, sy, ay - wy), ayf = __fmaf_rn(-8388608.0f, sy, ay + wy);
+    const float azn = __fmaf_rn(-8388608.0f, sz, az - wz), azf = __fmaf_rn(-8388608.0f, sz, az + wz);
     // The near and far planes' quantised words for the ray's direction signs, chosen once a node.
     const bool fx = r.ix >= 0.0f, fy = r.iy >= 0.0f, fz = r.iz >= 0.0f;
     const uint32_t nx0 = fx ? n2.x : n3.z, nx1 = fx ? n2.y : n3.w, fx0 = fx ? n3.z : n2.x, fx1 = fx ? n3.w : n2.y;
@@ -159,9 +163,9 @@ __device__ __forceinline__ uint32_t visitNode(const Node8* __restrict__ nodes, u
 #pragma unroll
     for (int s = 0; s < 8; ++s) {
         const int j = s & 3;
-        const float nx = __fmaf_rn(qbyte(s < 4 ? nx0 : nx1, j), sx, axn), fxx = __fmaf_rn(qbyte(s < 4 ? fx0 : fx1, j), sx, axf);
-        const float ny = __fmaf_rn(qbyte(s < 4 ? ny0 : ny1, j), sy, ayn), fyy = __fmaf_rn(qbyte(s < 4 ? fy0 : fy1, j), sy, ayf);
-        const float nz = __fmaf_rn(qbyte(s < 4 ? nz0 : nz1, j), sz, azn), fzz = __fmaf_rn(qbyte(s < 4 ? fz0 : fz1, j), sz, azf);
+        const float nx = __fmaf_rn(qbyte23(s < 4 ? nx0 : nx1, j), sx, axn), fxx = __fmaf_rn(qbyte23(s < 4 ? fx0 : fx1, j), sx, axf);
+        const float ny = __fmaf_rn(qbyte23(s < 4 ? ny0 : ny1, j), sy, ayn), fyy = __fmaf_rn(qbyte23(s < 4 ? fy0 : fy1, j), sy, ayf);
+        const float nz = __fmaf_rn(qbyte23(s < 4 ? nz0 : nz1, j), sz, azn), fzz = __fmaf_rn(qbyte23(s < 4 ? fz0 : fz1, j), sz, azf);
         const float entry = max3f(nx, ny, fmaxf(nz, tmin)), exit = min3f(fxx, fyy, fminf(fzz, tmax));
         const uint32_t meta = ((s < 4 ? m0 : m1) >> (8 * j)) & 0xffu;
         if (entry <= exit) hits |= (meta >> 5) << (meta & 31u);
