@@ -476,7 +476,8 @@ def probe_rmse(args):
 def probe_adaptive(args):
     """An adaptive frame of config 0 (the closed box, 256x256; MoonRay's schedule up to 256 samples a pixel, passes from
     4 samples on adaptive, target error 5e-4): its passes, samples and time; then the image RMSE of its fixture tiles
-    against the converged reference (tests/golden/rmse_c0.npz) beside a uniform frame's of about the same samples."""
+    against the converged reference (tests/golden/rmse_c0.npz) beside a uniform frame's of about the same samples, and
+    the same frame by cellular generations."""
     import rmse_lib
     import x2
 
@@ -501,9 +502,15 @@ def probe_adaptive(args):
     usums, ucounts = scene.film()
     uimg = np.zeros(px.shape + (3,))
     uimg[live] = usums[px[live], :3] / ucounts[px[live], None]
+    scene.render_adaptive(4, 256, 5e-4, cellular=True)  # warm-up
+    cell = scene.render_adaptive(4, 256, 5e-4, cellular=True)
+    csums, ccounts = scene.film()
+    cimg = np.zeros(px.shape + (3,))
+    cimg[live] = csums[px[live], :3] / ccounts[px[live], None]
     print(json.dumps({"probe": "adaptive", "config": 0, **result, "mean_spp": mean_spp,
                       "rmse_adaptive": rmse_lib.rmse(img, ref, live), "uniform_spp": spp,
-                      "rmse_uniform": rmse_lib.rmse(uimg, ref, live), "uniform_ms": c.milliseconds}))
+                      "rmse_uniform": rmse_lib.rmse(uimg, ref, live), "uniform_ms": c.milliseconds,
+                      "cellular": {**cell, "mean_spp": cell["samples"] / (cfg.width * cfg.height), "rmse": rmse_lib.rmse(cimg, ref, live)}}))
     scene.free()
     ctx.close()
 

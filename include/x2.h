@@ -303,6 +303,11 @@ typedef struct x2_adaptive_result {
  * odd sums, counts) is then read as after any launch; x2_adaptive_planned gives each pixel's planned count (for
  * x2_audit). Waits. */
 int x2_render_adaptive(x2_scene* scene, uint32_t min_samples, uint32_t max_samples, float target, x2_adaptive_result* result);
+/* The same frame with cellular generations in place of MoonRay's trees (the reference's preview default,
+ * adaptive::Cellular, async_adaptive.h:147-232): before each adaptive pass the image's 8x8 tiles are a generation of
+ * cells, a tile living by its error over the target and its live neighbours; a live tile samples all its pixels. Ends
+ * when a generation has no live tile or the schedule runs out. Waits. */
+int x2_render_adaptive_cellular(x2_scene* scene, uint32_t min_samples, uint32_t max_samples, float target, x2_adaptive_result* result);
 int x2_adaptive_planned(x2_scene* scene, uint32_t* planned);
 
 /* ---- the work grid: replaces Grid (async_grid.h:96-430) and the GPU feeder's claims (async_render.h:600-605,

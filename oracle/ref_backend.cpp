@@ -1069,6 +1069,18 @@ int x2ref_sample_words(const x2_identity* ids, const uint32_t* dims, uint64_t n,
     return X2_OK;
 }
 
+// ---- the reference's cellular generations (async_adaptive.h Cellular) ----
+void* x2ref_cellular_open(int width, int height, float target, const uint64_t* inImage, uint32_t tiles) {
+    auto* c = new xi::async::adaptive::Cellular(width, height, target);
+    c->deadForever(std::vector<std::uint64_t>(inImage, inImage + tiles));
+    return c;
+}
+void x2ref_cellular_free(void* c) { delete static_cast<xi::async::adaptive::Cellular*>(c); }
+uint64_t x2ref_cellular_update(void* c, const float* errors) { return static_cast<xi::async::adaptive::Cellular*>(c)->update(errors); }
+void x2ref_cellular_alive(void* c, uint8_t* out, uint32_t tiles) {
+    for (uint32_t t = 0; t < tiles; ++t) out[t] = static_cast<xi::async::adaptive::Cellular*>(c)->alive(t) ? 1 : 0;
+}
+
 // ---- the reference's work grid (async_grid.h Grid), driven call by call ----
 void* x2ref_grid_open(uint32_t width, uint32_t height, uint32_t spp, uint32_t cellSize, uint32_t samplesPerChunk, int mode,
                       int progressive, uint32_t sampleFirst, uint32_t sampleCount, const uint32_t* owners, uint32_t ownerCount,

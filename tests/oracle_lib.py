@@ -222,6 +222,38 @@ def reference_pixel_errors(sums, odd, counts):
     return out
 
 
+class RefCellular:
+    """The reference's cellular generations (async_adaptive.h Cellular) over a width x height image's tiles."""
+
+    def __init__(self, width, height, target, in_image):
+        lib = self.lib = C.CDLL(REFERENCE)
+        lib.x2ref_cellular_open.argtypes = [C.c_int, C.c_int, C.c_float, C.c_void_p, C.c_uint32]
+        lib.x2ref_cellular_open.restype = C.c_void_p
+        lib.x2ref_cellular_free.argtypes = [C.c_void_p]
+        lib.x2ref_cellular_update.argtypes = [C.c_void_p, C.c_void_p]
+        lib.x2ref_cellular_update.restype = C.c_uint64
+        lib.x2ref_cellular_alive.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        in_image = np.ascontiguousarray(in_image, np.uint64)
+        self.tiles = len(in_image)
+        self._h = lib.x2ref_cellular_open(width, height, target, in_image.ctypes.data, self.tiles)
+
+    def update(self, errors):
+        """The next generation from per-pixel errors; its live tiles' count."""
+        errors = np.ascontiguousarray(errors, np.float32)
+        return int(self.lib.x2ref_cellular_update(self._h, errors.ctypes.data))
+
+    def alive(self):
+        out = np.zeros(self.tiles, np.uint8)
+        self.lib.x2ref_cellular_alive(self._h, out.ctypes.data, self.tiles)
+        return out
+
+    def __del__(self):
+        try:
+            self.lib.x2ref_cellular_free(self._h)
+        except Exception:
+            pass
+
+
 def reference_adaptive_schedule(max_samples):
     """The reference's pass schedule (async_adaptive.h schedule): [(start, end)] sample ranges a pixel."""
     lib = C.CDLL(REFERENCE)

@@ -67,17 +67,14 @@ def test_adaptive_frame(box):
     assert np.allclose(odd[pix], odd_want, rtol=1e-9, atol=1e-12)
 
 
-@needs_reference
-def test_adaptive_frame_replays_reference_frame(box):
-    """The queued frame against the reference's adaptive frame replayed on the host: the reference's schedule, and
-    before each pass past the uniform ones its pixelError of the film so far and its region trees' masks; each active
-    pixel then takes the pass's next samples. Each pass's film is rebuilt from the samples' own radiance (the per-sample
-    API), summed as the device sums it (each pixel's samples of the pass in order, then added to the pixel), so the
-    replay's plan and film equal the device's bit for bit."""
-    s, scene = box
-    cfg = s.config
-    target, min_samples, max_samples = 0.0005, 4, 256
-    result = scene.render_adaptive(min_samples, max_samples, target)
+def _replay(scene, cfg, target, min_samples, max_samples, cellular):
+    """Renders an adaptive frame and replays the reference's frame on the host against it: the reference's schedule,
+    and before each pass past the uniform ones its pixelError of the film so far and its region trees' masks (cellular:
+    its next generation, a live tile sampling all its pixels); each active pixel then takes the pass's next samples.
+    Each pass's film is rebuilt from the samples' own radiance (the per-sample API), summed as the device sums it (each
+    pixel's samples of the pass in order, then added to the pixel), so the replay's plan and film equal the device's
+    bit for bit."""
+    result = scene.render_adaptive(min_samples, max_samples, target, cellular=cellular)
     planned = scene.adaptive_planned().astype(np.int64)
     sums, odd, counts = scene.film(odd=True)
     pixels = cfg.width * cfg.height
@@ -87,28 +84,47 @@ def test_adaptive_frame_replays_reference_frame(box):
     rgba, status = scene.integrate(pix, idx)
     assert (status == x2.DONE).all()
     assert np.array_equal(rgba, rgba.astype(np.float32).astype(np.float64))
-    tiles_x = (cfg.width + 7) // 8
+    tiles_x, tiles_y = (cfg.width + 7) // 8, (cfg.height + 7) // 8
+    tile_of = (np.arange(pixels) // cfg.width // 8) * tiles_x + (np.arange(pixels) % cfg.width) // 8
+    in_image = np.zeros(tiles_x * tiles_y, np.uint64)
+    for t in range(len(in_image)):
+        x0, y0 = (t % tiles_x) * 8, (t // tiles_x) * 8
+        m = 0
+        for b in range(64):
+            if x0 + b % 8 < cfg.width and y0 + b // 8 < cfg.height:
+                m |= 1 << b
+        in_image[t] = m
+    cells = oracle_lib.RefCellular(cfg.width, cfg.height, target, in_image) if cellular else None
     film = np.zeros((pixels, 4))
     film_odd = np.zeros((pixels, 4))
     film_counts = np.zeros(pixels, np.uint32)
     plan = np.zeros(pixels, np.int64)
-    converged, passes = False, 0
+    converged, passes, generations = False, 0, []
     for k, (start, end) in enumerate(oracle_lib.reference_adaptive_schedule(max_samples)):
         size = end - start
         if start < min_samples:
             active = np.arange(pixels)
         else:
             errors = oracle_lib.reference_pixel_errors(film, film_odd, film_counts)
-            masks, done = oracle_lib.reference_adaptive_masks(cfg.width, cfg.height, target, errors)
-            if done:
-                converged = True
-                break
-            tiles = np.nonzero(masks)[0]
-            bits = ((masks[tiles, None] >> np.arange(64, dtype=np.uint64)) & np.uint64(1)).astype(bool)
-            t, b = np.nonzero(bits)
-            x = (tiles[t] % tiles_x) * 8 + b % 8
-            y = (tiles[t] // tiles_x) * 8 + b // 8
-            active = np.sort(y * cfg.width + x)
+            if cellular:
+                live = cells.update(errors)
+                if live == 0:
+                    converged = True
+                    break
+                alive = cells.alive()
+                generations.append(live)
+                active = np.nonzero(alive[tile_of])[0]
+            else:
+                masks, done = oracle_lib.reference_adaptive_masks(cfg.width, cfg.height, target, errors)
+                if done:
+                    converged = True
+                    break
+                tiles = np.nonzero(masks)[0]
+                bits = ((masks[tiles, None] >> np.arange(64, dtype=np.uint64)) & np.uint64(1)).astype(bool)
+                t, b = np.nonzero(bits)
+                x = (tiles[t] % tiles_x) * 8 + b % 8
+                y = (tiles[t] // tiles_x) * 8 + b // 8
+                active = np.sort(y * cfg.width + x)
             if len(active) == 0:
                 converged = True
                 break
@@ -121,10 +137,26 @@ def test_adaptive_frame_replays_reference_frame(box):
         film_counts[active] += size
         plan[active] += size
         passes += 1
-    print(result, "replay: passes", passes, "converged", converged)
+    print(result, "replay: passes", passes, "converged", converged, "live tiles a generation", generations)
     assert np.array_equal(plan, planned), f"{int(np.count_nonzero(plan != planned))} pixels planned differently"
     assert result["passes"] == passes and bool(result["converged"]) == converged
     assert np.array_equal(counts, film_counts)
     assert np.array_equal(sums, film), f"max abs diff {np.abs(sums - film).max()}"
     assert np.array_equal(odd, film_odd), f"max abs diff {np.abs(odd - film_odd).max()}"
+    return result, generations
 
+
+@needs_reference
+def test_adaptive_frame_replays_reference_frame(box):
+    s, scene = box
+    _replay(scene, s.config, 0.0005, 4, 256, cellular=False)
+
+
+@needs_reference
+@pytest.mark.parametrize("target", [0.002, 0.0005])
+def test_cellular_frame_replays_reference_frame(box, target):
+    """The cellular generations' frame against the reference's Cellular replayed on the host, bit for bit; the
+    generations thin out as tiles converge."""
+    s, scene = box
+    result, generations = _replay(scene, s.config, target, 4, 256, cellular=True)
+    assert len(generations) >= 2 and min(generations) < max(generations)

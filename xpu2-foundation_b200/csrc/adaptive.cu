@@ -91,7 +91,9 @@ __global__ void adMasks(AdaptiveArgs a, uint32_t uniform, uint32_t size) {
     if (halted(a)) return;
     if (!uniform) {
         bool converged = true;
-        for (uint32_t r = 0; r < a.regionCount; ++r) converged = converged && a.regionDone[r] != 0;
+        if (a.alive) converged = *a.liveTiles == 0;
+        else
+            for (uint32_t r = 0; r < a.regionCount; ++r) converged = converged && a.regionDone[r] != 0;
         if (converged) {
             if (blockIdx.x == 0 && threadIdx.x == 0) *a.stop = 1;
             return;
@@ -100,7 +102,9 @@ __global__ void adMasks(AdaptiveArgs a, uint32_t uniform, uint32_t size) {
     const uint32_t tile = blockIdx.x * blockDim.x + threadIdx.x;
     if (tile >= a.tiles) return;
     uint64_t mask = a.inImage[tile];
-    if (!uniform) {
+    if (!uniform && a.alive) {
+        if (!a.alive[tile]) mask = 0;
+    } else if (!uniform) {
         const int tx = int(tile % a.tilesX) * 8, ty = int(tile / a.tilesX) * 8;
         mask &= ad::tileSamples(a.nodes + a.nodeOffset[a.layout.regionOf(tx, ty)], tx, ty);
     }
@@ -112,6 +116,37 @@ __global__ void adMasks(AdaptiveArgs a, uint32_t uniform, uint32_t size) {
             a.base[pixel] = a.planned[pixel];
             a.planned[pixel] += size;
         }
+}
+
+__global__ void adCellular(AdaptiveArgs a, const uint8_t* aliveIn, uint8_t* aliveOut) {
+    if (halted(a)) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= a.tiles) return;
+    const int tilesX = int(a.tilesX), tilesY = int(a.tiles / a.tilesX), tx = int(t) % tilesX, ty = int(t) / tilesX;
+    const int width = int(a.width), height = int(a.height);
+    double sum = 0.0;
+    int n = 0;
+    bool unknown = false;
+    for (int y = ty * 8; y < ad::imin(height, ty * 8 + 8); ++y)
+        for (int x = tx * 8; x < ad::imin(width, tx * 8 + 8); ++x) {
+            const float e = a.errors[size_t(y) * size_t(width) + size_t(x)];
+            if (e < 0) unknown = true;
+            else sum += e;
+            ++n;
+        }
+    const float error = unknown ? -1.0f : ad::nodeError(float(sum), float(n));
+    const float ratio = error < 0 ? 3.4e38f : error / a.target;
+    int k = 0;
+    for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+            const int x = tx + dx, y = ty + dy;
+            if ((dx || dy) && x >= 0 && y >= 0 && x < tilesX && y < tilesY && aliveIn[size_t(y) * tilesX + x]) ++k;
+        }
+    bool next = aliveIn[t] ? (ratio >= 1.0f || (ratio >= kSurvive && k >= kSurviveNeighbours))
+                           : (ratio >= 1.0f || (ratio >= kBirth && k >= kBirthNeighbours));
+    if (!a.inImage[t]) next = false;
+    aliveOut[t] = next ? 1 : 0;
+    if (next) atomicAdd(a.liveTiles, 1u);
 }
 
 __global__ void adCompact(AdaptiveArgs a, uint32_t size) {

@@ -132,14 +132,18 @@ struct AdaptiveState {
     uint32_t* stop = nullptr;
     uint64_t* chunkMasks = nullptr;  // a pass's active tiles' masks, in its chunks' order
     // A queued frame's words: [0] the pass's active chunks, [1] passes launched, [2] the pass's drain iterations,
-    // [3] all passes' drain iterations, [4] a drain that hit its bound; its planned samples; their host copies (pinned).
+    // [3] all passes' drain iterations, [4] a drain that hit its bound, [5] a cellular generation's live tiles; its
+    // planned samples; their host copies (pinned).
     uint32_t* words = nullptr;
     unsigned long long* samples = nullptr;
     uint32_t* hostWords = nullptr;
     unsigned long long* hostSamples = nullptr;
+    // Cellular generations: two generations of live tiles (a byte a tile each), the first every tile in the image.
+    uint8_t* alive = nullptr;
+    std::vector<uint8_t> firstAlive;
     ~AdaptiveState() {
         void* p[] = {regions, nodeOffset, nodeCapacity, satOffset, sat, nodes, regionDone, errors, inImage, tileMask, planned, base, stop, chunkMasks,
-                     words, samples};
+                     words, samples, alive};
         for (void* q : p) cudaFree(q);
         if (hostWords) cudaFreeHost(hostWords);
         if (hostSamples) cudaFreeHost(hostSamples);
@@ -1722,12 +1726,14 @@ int ensureAdaptive(x2_scene* s, float target) {
     }
     a->regionCount = uint32_t(boxes.size());
     std::vector<uint64_t> inImage(a->tiles);
+    a->firstAlive.assign(a->tiles, 0);
     for (uint32_t t = 0; t < a->tiles; ++t) {
         uint64_t m = 0;
         const uint32_t tx = (t % a->tilesX) * 8, ty = (t / a->tilesX) * 8;
         for (uint32_t p = 0; p < 64; ++p)
             if (tx + p % 8 < width && ty + p / 8 < height) m |= uint64_t(1) << p;
         inImage[t] = m;
+        a->firstAlive[t] = m ? 1 : 0;
     }
     const size_t pixels = size_t(width) * height;
     const bool ok = cudaMalloc(&a->regions, sizeof(x2::ad::IBox) * boxes.size()) == cudaSuccess &&
@@ -1743,7 +1749,8 @@ int ensureAdaptive(x2_scene* s, float target) {
                     cudaMalloc(&a->stop, sizeof(uint32_t)) == cudaSuccess && cudaMalloc(&a->words, sizeof(uint32_t) * 8) == cudaSuccess &&
                     cudaMalloc(&a->samples, sizeof(unsigned long long)) == cudaSuccess &&
                     cudaMallocHost(&a->hostWords, sizeof(uint32_t) * 8) == cudaSuccess &&
-                    cudaMallocHost(&a->hostSamples, sizeof(unsigned long long)) == cudaSuccess;
+                    cudaMallocHost(&a->hostSamples, sizeof(unsigned long long)) == cudaSuccess &&
+                    cudaMalloc(&a->alive, 2 * size_t(a->tiles)) == cudaSuccess;
     if (!ok) {
         delete a;
         s->adaptiveState = nullptr;
@@ -1767,7 +1774,7 @@ int ensureAdaptive(x2_scene* s, float target) {
 x2::AdaptiveArgs adaptiveArgs(const AdaptiveState& a, x2_chunk* chunks = nullptr) {
     return x2::AdaptiveArgs{a.width, a.height, a.tilesX, a.tiles, a.regionCount, a.target, a.layout, a.regions, a.nodeOffset, a.nodeCapacity,
                             a.satOffset, a.sat, a.nodes, a.regionDone, a.errors, a.inImage, a.tileMask, a.planned, a.base, a.stop,
-                            chunks ? 1u : 0u, chunks, a.chunkMasks, a.words, a.words + 1, a.samples};
+                            chunks ? 1u : 0u, chunks, a.chunkMasks, a.words, a.words + 1, a.samples, nullptr, a.words + 5};
 }
 
 // One chain step on the frame's film: errors and trees (not in a uniform pass), then the pass's tile masks.
@@ -1820,7 +1827,8 @@ int x2_adaptive_step(x2_scene* s, float target, uint32_t uniform, uint32_t size,
 // The whole frame as one graph, queued at once: for each pass of the schedule the chain, the compaction of its active
 // tiles and the pass's wavefront launch, whose iterations run in a conditional while node until no path is left, then
 // its film reduce. The host waits once, at the frame's end; a pass that finds nothing to do costs a few empty launches.
-int x2_render_adaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float target, x2_adaptive_result* result) {
+namespace {
+int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float target, bool cellular, x2_adaptive_result* result) {
     if (!s || !s->configured || maxSamples == 0 || !(target > 0)) {
         setError("x2_render_adaptive: a configured scene, at least one sample and a positive target");
         return X2_EINVAL;
@@ -1856,8 +1864,10 @@ int x2_render_adaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, fl
     cudaMemsetAsync(ad.words, 0, sizeof(uint32_t) * 8, st);
     cudaMemsetAsync(ad.samples, 0, sizeof(unsigned long long), st);
     cudaMemsetAsync(sl.counters, 0, sizeof(Counters), st);
+    if (cellular) cudaMemcpyAsync(ad.alive, ad.firstAlive.data(), ad.tiles, cudaMemcpyHostToDevice, st);
     CUDA_OR(cudaGetLastError(), X2_ECUDA);
     const x2::AdaptiveArgs chain = adaptiveArgs(ad, sl.chunks);
+    uint32_t generation = 0;
     WaveArgs a = launchArgs(s, sl, paths, records, maxItems, ad.tiles);
     a.chunkMask = ad.chunkMasks;
     a.pixelBase = ad.base;
@@ -1897,7 +1907,23 @@ int x2_render_adaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, fl
         a.samplesPerChunk = size;
         a.itemCount = (unsigned long long)ad.tiles * 64ull * size;
         if (!beginSegment(graph, true)) break;
-        adaptiveChain(s, chain, uniform, size);
+        if (cellular) {
+            // The next generation from the film so far, then the pass's masks from it.
+            x2::AdaptiveArgs pass = chain;
+            if (!uniform) {
+                const uint8_t* aliveIn = ad.alive + size_t(generation % 2) * ad.tiles;
+                uint8_t* aliveOut = ad.alive + size_t((generation + 1) % 2) * ad.tiles;
+                ++generation;
+                const uint32_t pixels = ad.width * ad.height;
+                x2::adErrors<<<(pixels + 255) / 256, 256, 0, st>>>(chain, s->sums, s->odd, s->counts);
+                cudaMemsetAsync(chain.liveTiles, 0, sizeof(uint32_t), st);
+                x2::adCellular<<<(ad.tiles + 255) / 256, 256, 0, st>>>(chain, aliveIn, aliveOut);
+                pass.alive = aliveOut;
+            }
+            x2::adMasks<<<(ad.tiles + 255) / 256, 256, 0, st>>>(pass, uniform, size);
+        } else {
+            adaptiveChain(s, chain, uniform, size);
+        }
         x2::adCompact<<<1, x2::kCompactThreads, 0, st>>>(chain, size);
         cudaMemsetAsync(s->wave.state, 0, sizeof(uint32_t) * paths, st);
         cudaMemsetAsync(s->wave.ncount, 0, sizeof(uint32_t) * paths, st);
@@ -1970,6 +1996,16 @@ int x2_render_adaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, fl
     r.milliseconds = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
     if (result) *result = r;
     return X2_OK;
+}
+
+}  // namespace
+
+int x2_render_adaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float target, x2_adaptive_result* result) {
+    return renderAdaptive(s, minSamples, maxSamples, target, false, result);
+}
+
+int x2_render_adaptive_cellular(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float target, x2_adaptive_result* result) {
+    return renderAdaptive(s, minSamples, maxSamples, target, true, result);
 }
 
 // ---- the work grid's GPU broker (row f1): launches fed from a grid (grid.cpp), as the reference's feeder feeds

@@ -181,7 +181,7 @@ def library():
         "x2_scene_set_params": ([vp, vp, vp, vp], i32), "x2_adjoint": ([vp, u32, u32, vp, vp, vp, vp, vp], i32), "x2_adjoint_plain": ([vp, u32, u32, vp, vp, vp, vp, vp], i32),
         "x2_scene_set_texture": ([vp, u32, vp], i32),
         "x2_frame_begin_adaptive": ([vp, u32], i32), "x2_adaptive_step": ([vp, C.c_float, u32, u32, vp, vp, vp], i32),
-        "x2_render_adaptive": ([vp, u32, u32, C.c_float, C.POINTER(AdaptiveResult)], i32), "x2_adaptive_planned": ([vp, vp], i32),
+        "x2_render_adaptive": ([vp, u32, u32, C.c_float, C.POINTER(AdaptiveResult)], i32), "x2_render_adaptive_cellular": ([vp, u32, u32, C.c_float, C.POINTER(AdaptiveResult)], i32), "x2_adaptive_planned": ([vp, vp], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
@@ -404,10 +404,12 @@ class Scene:
         _check(library().x2_adaptive_step(self._h, target, uniform, size, _ptr(errors), _ptr(masks), C.byref(stop)))
         return errors, masks, stop.value
 
-    def render_adaptive(self, min_samples, max_samples, target):
-        """x2_render_adaptive: an adaptive frame; returns its AdaptiveResult as a dict."""
+    def render_adaptive(self, min_samples, max_samples, target, cellular=False):
+        """x2_render_adaptive (cellular: x2_render_adaptive_cellular): an adaptive frame; returns its AdaptiveResult as
+        a dict."""
         r = AdaptiveResult()
-        _check(library().x2_render_adaptive(self._h, min_samples, max_samples, target, C.byref(r)))
+        f = library().x2_render_adaptive_cellular if cellular else library().x2_render_adaptive
+        _check(f(self._h, min_samples, max_samples, target, C.byref(r)))
         return {"passes": r.passes, "converged": bool(r.converged), "samples": r.samples, "milliseconds": r.milliseconds}
 
     def render_workgrid(self, grid, chunks_per_launch):
