@@ -308,6 +308,13 @@ int x2_render_adaptive(x2_scene* scene, uint32_t min_samples, uint32_t max_sampl
  * cells, a tile living by its error over the target and its live neighbours; a live tile samples all its pixels. Ends
  * when a generation has no live tile or the schedule runs out. Waits. */
 int x2_render_adaptive_cellular(x2_scene* scene, uint32_t min_samples, uint32_t max_samples, float target, x2_adaptive_result* result);
+/* A frame by sampling generations under a budget of samples (cpu::Plan sampleBudget with budgetBySamples): the
+ * cellular generations, each with the target the samples still to spend would bring every tile to (no lower than
+ * floor; 0: none), made on the host between passes as the reference makes them (async_render.h:1318-1410); a pass
+ * whose live tiles want more than is left takes those furthest above the target first. Ends once the budget is spent,
+ * a generation has no live tile or the schedule runs out. Waits. */
+int x2_render_adaptive_budget(x2_scene* scene, uint32_t min_samples, uint32_t max_samples, float floor, uint64_t budget,
+                              x2_adaptive_result* result);
 int x2_adaptive_planned(x2_scene* scene, uint32_t* planned);
 
 /* ---- the work grid: replaces Grid (async_grid.h:96-430) and the GPU feeder's claims (async_render.h:600-605,
@@ -363,7 +370,7 @@ int x2_workgrid_set_rates(x2_workgrid* grid, double gpu_items, double cpu_worker
 int x2_workgrid_rendered(x2_workgrid* grid, uint32_t cell, uint32_t device, uint64_t samples);
 void x2_workgrid_close(x2_workgrid* grid);  /* a drain: nothing is handed out any more */
 /* The GPU broker: its next launch's chunks, up to want, taken by its cellular workers (options.gpu_workers, seeded at
- * the first call), a share each, from their cells by the cellular rules. Returns how many. */
+ * the first call), a share each, from their cells by the cellular rules. Returns how many. One broker thread a grid. */
 uint32_t x2_workgrid_take(x2_workgrid* grid, uint32_t want, x2_chunk* out);
 uint64_t x2_workgrid_stolen(const x2_workgrid* grid);  /* chunks the broker took from cells the CPU owns */
 typedef struct x2_workgrid_result {

@@ -1077,6 +1077,15 @@ void* x2ref_cellular_open(int width, int height, float target, const uint64_t* i
 }
 void x2ref_cellular_free(void* c) { delete static_cast<xi::async::adaptive::Cellular*>(c); }
 uint64_t x2ref_cellular_update(void* c, const float* errors) { return static_cast<xi::async::adaptive::Cellular*>(c)->update(errors); }
+uint64_t x2ref_cellular_update_budget(void* c, const float* errors, const uint32_t* planned, uint64_t pixels, double remaining,
+                                      uint32_t most, float floor) {
+    const std::vector<uint32_t> samples(planned, planned + pixels);
+    const xi::async::adaptive::Budget b{&samples, remaining, most, floor};
+    return static_cast<xi::async::adaptive::Cellular*>(c)->update(errors, &b);
+}
+void x2ref_cellular_ratio(void* c, float* out, uint32_t tiles) {
+    for (uint32_t t = 0; t < tiles; ++t) out[t] = static_cast<xi::async::adaptive::Cellular*>(c)->ratio(t);
+}
 void x2ref_cellular_alive(void* c, uint8_t* out, uint32_t tiles) {
     for (uint32_t t = 0; t < tiles; ++t) out[t] = static_cast<xi::async::adaptive::Cellular*>(c)->alive(t) ? 1 : 0;
 }

@@ -242,6 +242,23 @@ class RefCellular:
         errors = np.ascontiguousarray(errors, np.float32)
         return int(self.lib.x2ref_cellular_update(self._h, errors.ctypes.data))
 
+    def update_budget(self, errors, planned, remaining, most, floor):
+        """The next generation under a budget (Budget: each pixel's planned samples, the samples left, the most a pixel
+        may have, the error floor); its live tiles' count."""
+        f = self.lib.x2ref_cellular_update_budget
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint64, C.c_double, C.c_uint32, C.c_float]
+        f.restype = C.c_uint64
+        errors = np.ascontiguousarray(errors, np.float32)
+        planned = np.ascontiguousarray(planned, np.uint32)
+        return int(f(self._h, errors.ctypes.data, planned.ctypes.data, len(planned), remaining, most, floor))
+
+    def ratio(self):
+        f = self.lib.x2ref_cellular_ratio
+        f.argtypes = [C.c_void_p, C.c_void_p, C.c_uint32]
+        out = np.zeros(self.tiles, np.float32)
+        f(self._h, out.ctypes.data, self.tiles)
+        return out
+
     def alive(self):
         out = np.zeros(self.tiles, np.uint8)
         self.lib.x2ref_cellular_alive(self._h, out.ctypes.data, self.tiles)

@@ -67,14 +67,17 @@ def test_adaptive_frame(box):
     assert np.allclose(odd[pix], odd_want, rtol=1e-9, atol=1e-12)
 
 
-def _replay(scene, cfg, target, min_samples, max_samples, cellular):
+def _replay(scene, cfg, target, min_samples, max_samples, cellular, budget=0):
     """Renders an adaptive frame and replays the reference's frame on the host against it: the reference's schedule,
     and before each pass past the uniform ones its pixelError of the film so far and its region trees' masks (cellular:
     its next generation, a live tile sampling all its pixels); each active pixel then takes the pass's next samples.
     Each pass's film is rebuilt from the samples' own radiance (the per-sample API), summed as the device sums it (each
     pixel's samples of the pass in order, then added to the pixel), so the replay's plan and film equal the device's
     bit for bit."""
-    result = scene.render_adaptive(min_samples, max_samples, target, cellular=cellular)
+    if budget:
+        result = scene.render_adaptive_budget(min_samples, max_samples, target, budget)
+    else:
+        result = scene.render_adaptive(min_samples, max_samples, target, cellular=cellular)
     planned = scene.adaptive_planned().astype(np.int64)
     sums, odd, counts = scene.film(odd=True)
     pixels = cfg.width * cfg.height
@@ -99,20 +102,37 @@ def _replay(scene, cfg, target, min_samples, max_samples, cellular):
     film_odd = np.zeros((pixels, 4))
     film_counts = np.zeros(pixels, np.uint32)
     plan = np.zeros(pixels, np.int64)
-    converged, passes, generations = False, 0, []
+    converged, passes, generations, spent = False, 0, [], 0
     for k, (start, end) in enumerate(oracle_lib.reference_adaptive_schedule(max_samples)):
         size = end - start
         if start < min_samples:
             active = np.arange(pixels)
         else:
+            if budget and spent >= budget:
+                break
             errors = oracle_lib.reference_pixel_errors(film, film_odd, film_counts)
             if cellular:
-                live = cells.update(errors)
+                left = max(0, budget - spent)
+                live = cells.update_budget(errors, plan, left, max_samples, target) if budget else cells.update(errors)
                 if live == 0:
                     converged = True
                     break
                 alive = cells.alive()
                 generations.append(live)
+                if budget:
+                    # The reference's pass under a budget (async_render.h:1376-1395): the live tiles furthest above the
+                    # target first, while each fits in what is left.
+                    ratio = cells.ratio()
+                    cost = np.array([bin(int(m)).count("1") for m in in_image]) * size
+                    live_tiles = [t for t in range(len(in_image)) if in_image[t] and alive[t]]
+                    if sum(cost[t] for t in live_tiles) > left:
+                        kept, taken = np.zeros_like(alive), 0
+                        for t in sorted(live_tiles, key=lambda t: -ratio[t]):
+                            if taken + cost[t] > left:
+                                break
+                            taken += cost[t]
+                            kept[t] = 1
+                        alive = kept
                 active = np.nonzero(alive[tile_of])[0]
             else:
                 masks, done = oracle_lib.reference_adaptive_masks(cfg.width, cfg.height, target, errors)
@@ -136,6 +156,7 @@ def _replay(scene, cfg, target, min_samples, max_samples, cellular):
         film_odd[active] += np.cumsum(np.where(is_odd[:, :, None], block, 0.0), axis=1)[:, -1]
         film_counts[active] += size
         plan[active] += size
+        spent += len(active) * size
         passes += 1
     print(result, "replay: passes", passes, "converged", converged, "live tiles a generation", generations)
     assert np.array_equal(plan, planned), f"{int(np.count_nonzero(plan != planned))} pixels planned differently"
@@ -160,3 +181,15 @@ def test_cellular_frame_replays_reference_frame(box, target):
     s, scene = box
     result, generations = _replay(scene, s.config, target, 4, 256, cellular=True)
     assert len(generations) >= 2 and min(generations) < max(generations)
+
+
+@needs_reference
+@pytest.mark.parametrize("budget", [3_000_000, 9_000_000])
+def test_budget_frame_replays_reference_frame(box, budget):
+    """A frame by sampling generations under a budget of samples against the reference's Cellular with its Budget
+    (and the pass's tile choice under the budget) replayed on the host, bit for bit; it spends about its budget."""
+    s, scene = box
+    result, generations = _replay(scene, s.config, 0.0, 4, 256, cellular=True, budget=budget)
+    assert result["samples"] <= budget + s.config.width * s.config.height * 32
+    assert result["samples"] >= 0.5 * budget
+

@@ -15,6 +15,7 @@
 #include "../../include/x2.h"
 #include "engine.h"
 #include "adaptive.h"
+#include "cellular.h"
 #include "adjoint.h"
 #include "render.h"
 #include "wavefront.h"
@@ -2006,6 +2007,101 @@ int x2_render_adaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, fl
 
 int x2_render_adaptive_cellular(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float target, x2_adaptive_result* result) {
     return renderAdaptive(s, minSamples, maxSamples, target, true, result);
+}
+
+// A frame by sampling generations under a sample budget: the generations made on the host between passes, as the
+// reference makes them (async_render.h Adaptive: rebuild, generate, samplesLeft with budgetBySamples), each pass's
+// errors read back from the device and its masks sent to it.
+int x2_render_adaptive_budget(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float floor, uint64_t budget,
+                              x2_adaptive_result* result) {
+    if (!s || !s->configured || maxSamples == 0 || !(floor >= 0) || budget == 0) {
+        setError("x2_render_adaptive_budget: a configured scene, at least one sample, a floor of 0 or more and a budget");
+        return X2_EINVAL;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    const auto passes = adaptiveSchedule(maxSamples);
+    uint32_t most = 0;
+    for (const auto& p : passes) most = std::max(most, p.second - p.first);
+    if (int rc = x2_frame_begin_adaptive(s, most)) return rc;
+    if (int rc = ensureAdaptive(s, floor > 0 ? floor : 1.0f)) return rc;
+    AdaptiveState& ad = *s->adaptiveState;
+    cudaStream_t st = s->ctx->stream;
+    const uint32_t pixels = ad.width * ad.height;
+    std::vector<uint64_t> inImage(ad.tiles);
+    for (uint32_t t = 0; t < ad.tiles; ++t) {
+        uint64_t m = 0;
+        const uint32_t tx = (t % ad.tilesX) * 8, ty = (t / ad.tilesX) * 8;
+        for (uint32_t p = 0; p < 64; ++p)
+            if (tx + p % 8 < ad.width && ty + p / 8 < ad.height) m |= uint64_t(1) << p;
+        inImage[t] = m;
+    }
+    x2::CellularGenerations cells(int(ad.width), int(ad.height), floor, inImage);
+    std::vector<uint32_t> planned(pixels, 0), base(pixels, 0);
+    std::vector<float> errors(pixels);
+    std::vector<x2_chunk> chunks;
+    std::vector<uint64_t> chunkMasks;
+    const x2::AdaptiveArgs args = adaptiveArgs(ad);
+    double spent = 0;
+    x2_adaptive_result r{};
+    int rc = X2_OK;
+    for (size_t k = 0; k < passes.size() && rc == X2_OK; ++k) {
+        const uint32_t size = passes[k].second - passes[k].first;
+        const bool uniform = passes[k].first < minSamples;
+        std::vector<char> dropped;
+        if (!uniform) {
+            if (spent >= double(budget)) break;  // the budget is spent
+            x2::adErrors<<<(pixels + 255) / 256, 256, 0, st>>>(args, s->sums, s->odd, s->counts);
+            cudaMemcpyAsync(errors.data(), ad.errors, sizeof(float) * pixels, cudaMemcpyDeviceToHost, st);
+            if (cudaStreamSynchronize(st) != cudaSuccess) {
+                rc = X2_ECUDA;
+                break;
+            }
+            const x2::SampleBudget b{&planned, std::max(0.0, double(budget) - spent), maxSamples, floor};
+            if (cells.update(errors.data(), &b) == 0) {
+                r.converged = 1;
+                break;
+            }
+            dropped = x2::dropForBudget(cells, inImage, size, b.remaining);
+        }
+        chunks.clear();
+        chunkMasks.clear();
+        uint64_t samples = 0;
+        for (uint32_t t = 0; t < ad.tiles; ++t) {
+            uint64_t m = inImage[t];
+            if (!uniform && !(cells.alive(t) && (dropped.empty() || !dropped[t]))) m = 0;
+            if (!m) continue;
+            for (uint32_t p = 0; p < 64; ++p)
+                if (m >> p & 1) {
+                    const uint32_t pixel = ((t / ad.tilesX) * 8 + p / 8) * ad.width + (t % ad.tilesX) * 8 + p % 8;
+                    base[pixel] = planned[pixel];
+                    planned[pixel] += size;
+                    samples += size;
+                }
+            chunks.push_back(x2_chunk{t, 0, size, 0});
+            chunkMasks.push_back(m);
+        }
+        if (chunks.empty()) {
+            r.converged = 1;
+            break;
+        }
+        spent += double(samples);
+        cudaMemcpyAsync(ad.chunkMasks, chunkMasks.data(), sizeof(uint64_t) * chunkMasks.size(), cudaMemcpyHostToDevice, st);
+        cudaMemcpyAsync(ad.base, base.data(), sizeof(uint32_t) * pixels, cudaMemcpyHostToDevice, st);
+        s->launchMask = ad.chunkMasks;
+        s->launchBase = ad.base;
+        s->samplesPerChunk = size;
+        rc = x2_launch_wavefront(s, chunks.data(), uint32_t(chunks.size()));
+        s->launchMask = nullptr;
+        s->launchBase = nullptr;
+        s->samplesPerChunk = most;
+        if (rc == X2_OK) rc = x2_wait(s, 600000, nullptr);
+        r.passes++;
+        r.samples += samples;
+    }
+    if (rc == X2_OK && cudaMemcpy(ad.planned, planned.data(), sizeof(uint32_t) * pixels, cudaMemcpyHostToDevice) != cudaSuccess) rc = X2_ECUDA;
+    r.milliseconds = float(std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count());
+    if (result) *result = r;
+    return rc;
 }
 
 // ---- the work grid's GPU broker (row f1): launches fed from a grid (grid.cpp), as the reference's feeder feeds

@@ -181,7 +181,8 @@ def library():
         "x2_scene_set_params": ([vp, vp, vp, vp], i32), "x2_adjoint": ([vp, u32, u32, vp, vp, vp, vp, vp], i32), "x2_adjoint_plain": ([vp, u32, u32, vp, vp, vp, vp, vp], i32),
         "x2_scene_set_texture": ([vp, u32, vp], i32),
         "x2_frame_begin_adaptive": ([vp, u32], i32), "x2_adaptive_step": ([vp, C.c_float, u32, u32, vp, vp, vp], i32),
-        "x2_render_adaptive": ([vp, u32, u32, C.c_float, C.POINTER(AdaptiveResult)], i32), "x2_render_adaptive_cellular": ([vp, u32, u32, C.c_float, C.POINTER(AdaptiveResult)], i32), "x2_adaptive_planned": ([vp, vp], i32),
+        "x2_render_adaptive": ([vp, u32, u32, C.c_float, C.POINTER(AdaptiveResult)], i32), "x2_render_adaptive_cellular": ([vp, u32, u32, C.c_float, C.POINTER(AdaptiveResult)], i32),
+        "x2_render_adaptive_budget": ([vp, u32, u32, C.c_float, u64, C.POINTER(AdaptiveResult)], i32), "x2_adaptive_planned": ([vp, vp], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
@@ -417,6 +418,12 @@ class Scene:
         r = WorkGridResult()
         _check(library().x2_render_workgrid(self._h, grid._h, chunks_per_launch, C.byref(r)))
         return {k: getattr(r, k) for k, _ in WorkGridResult._fields_}
+
+    def render_adaptive_budget(self, min_samples, max_samples, floor, budget):
+        """x2_render_adaptive_budget: a frame by cellular generations under a budget of `budget` samples."""
+        r = AdaptiveResult()
+        _check(library().x2_render_adaptive_budget(self._h, min_samples, max_samples, floor, budget, C.byref(r)))
+        return {"passes": r.passes, "converged": bool(r.converged), "samples": r.samples, "milliseconds": r.milliseconds}
 
     def adaptive_planned(self):
         cfg = self.config
