@@ -76,11 +76,65 @@ def test_volume_wavefront_equals_plain(medium):
 
 def test_volume_configs_refused(ctx, medium):
     s, scene = medium
-    cfg = s.config
-    cfg.max_volume_depth = 2
+    cfg = x2.Config.from_buffer_copy(s.config)
+    cfg.max_volume_depth = 65
     with pytest.raises(x2.X2Error) as e:
         scene.set_config(cfg)
     assert e.value.code == x2.EINVAL
+    scene.set_config(s.config)
+
+
+def _multiple(s, depth):
+    cfg = x2.Config.from_buffer_copy(s.config)
+    cfg.max_volume_depth = depth
+    cfg.volume_illumination_samples = 2
+    return cfg
+
+
+@needs_reference
+@pytest.mark.parametrize("depth", [2, 4])
+def test_multiple_scattering_matches_reference(medium, depth):
+    """The multiple-scattering approximation (max_volume_depth above one: free paths from scatter events, each order's
+    light through its attenuation and contribution factors) against the reference's on the same identities."""
+    s, scene = medium
+    cfg = _multiple(s, depth)
+    scene.set_config(cfg)
+    try:
+        n = cfg.width * cfg.height
+        px = np.arange(n, dtype=np.uint32)
+        idx = np.full(n, 3, np.uint32)
+        rgba, status = scene.integrate(px, idx)
+        rrgba, rstatus = oracle_lib.Reference(s, cfg).integrate(px, idx)
+        single = oracle_lib.Reference(s, s.config).integrate(px, idx)[0]
+    finally:
+        scene.set_config(s.config)
+    assert np.array_equal(status, rstatus)
+    ok = (np.abs(rgba - rrgba) <= RTOL * np.abs(rrgba) + ATOL).all(axis=1)
+    print(f"multiple scattering, depth {depth}: {ok.mean() * 100:.3f}% of {n} samples within {RTOL}; "
+          f"mean {rgba[:, :3].mean():.6f} against single scattering's {single[:, :3].mean():.6f}")
+    assert ok.mean() >= 0.99
+    assert np.allclose(rgba[:, :3].mean(axis=0), rrgba[:, :3].mean(axis=0), rtol=2e-3)
+    assert rrgba[:, :3].mean() > single[:, :3].mean()  # the higher orders add light
+
+
+def test_multiple_scattering_wavefront_equals_plain(medium):
+    s, scene = medium
+    cfg = _multiple(s, 3)
+    scene.set_config(cfg)
+    try:
+        spp = 4
+        scene.frame_begin(spp)
+        scene.render_frame(0, spp)
+        scene.wait()
+        plain, pc = scene.film()
+        scene.frame_begin(spp)
+        scene.render_frame_wavefront(0, spp)
+        scene.wait()
+        wave, wc = scene.film()
+    finally:
+        scene.set_config(s.config)
+    assert np.array_equal(pc, wc)
+    assert np.allclose(plain, wave, rtol=1e-12, atol=1e-12)
 
 
 def test_volume_golden(medium):

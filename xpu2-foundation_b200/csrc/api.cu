@@ -845,9 +845,8 @@ int x2_config_set(x2_scene* s, const x2_config* c) {
         setError("config volume_count %u differs from the scene's %u volumes", c->volume_count, s->volumeCount);
         return X2_EINVAL;
     }
-    if (c->volume_count && (c->max_volume_depth > 1 || c->volume_overlap_mode > kOverlapRnd || c->max_depth > 120)) {
-        setError("volumes: max_volume_depth 0 or 1 (the multiple-scattering approximation is not built), overlap mode 0..2, "
-                 "max_depth <= 120");
+    if (c->volume_count && (c->max_volume_depth > 64 || c->volume_overlap_mode > kOverlapRnd || c->max_depth > 120)) {
+        setError("volumes: max_volume_depth <= 64, overlap mode 0..2, max_depth <= 120");
         return X2_EINVAL;
     }
     s->config = *c;

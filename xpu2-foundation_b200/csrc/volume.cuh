@@ -14,11 +14,14 @@
 //   scattering    integrateVolumeScatteringDirect: per light, equi-angular (bounded lights) and distance samples with
 //                 MIS, each through the light's source term (a light sample, its surface shadow ray, the volumes'
 //                 transmittance on the way by ray marching at the nearest voxel, the Henyey-Greenstein phase);
-//   shadows       transmittance(): the volumes' optical thickness along a surface's shadow ray.
+//   shadows       transmittance(): the volumes' optical thickness along a surface's shadow ray;
+//   multiple      (max_volume_depth > 1) the multiple-scattering approximation: scatter events picked from the
+//                 march's steps, then free paths from each, each order's extinction, contribution and anisotropy
+//                 shrunk by its factor, every light's source term at each event.
 //
 // Not built: homogeneous BaseVolumes and mapped ones (their ramps and map programs), holdouts (cutouts), motion and
-// velocity, emissive regions as light sources, the multiple-scattering approximation (max_volume_depth > 1), light
-// sets and LPEs; x2_scene_load and x2_config_set refuse scenes and configs that would need them.
+// velocity, emissive regions as light sources, light sets and LPEs; x2_scene_load and x2_config_set refuse scenes and
+// configs that would need them.
 #pragma once
 #include "shading.cuh"
 
@@ -560,6 +563,77 @@ static __device__ __noinline__ V3 volumeSourceTerm(const SceneView& s, Stream& s
     return vscaled(vtimes(tr, Li), ph / pdfL * keep);
 }
 
+// Henyey-Greenstein sampling about the reversed outgoing direction (volume_core.h phaseSample): uniform over the
+// sphere when |g| is at most 1e-3.
+__device__ __forceinline__ V3 phaseSample(float g, V3 wo, float u1, float u2) {
+    if (fabsf(g) <= 1e-3f) {
+        const float cosTheta = 1.0f - 2.0f * u1, sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
+        return localSpherical(cosTheta, sinTheta, u2 * kTwoPi);
+    }
+    u1 = fmaxf(u1, kVolumeEpsilon);
+    const float sqrTerm = (1.0f - g * g) / (1.0f - g + 2.0f * g * u1);
+    const float cosTheta = (1.0f + g * g - sqrTerm * sqrTerm) / (2.0f * g);
+    const float sinTheta = sqrtf(fmaxf(0.0f, 1.0f - cosTheta * cosTheta));
+    return localToGlobal(frameN(V3{-wo.x, -wo.y, -wo.z}), localSpherical(cosTheta, sinTheta, kTwoPi * u2));
+}
+
+// approximateVolumeMultipleScattering (async_integrator.h:1058-1150, after Wrenninge 2015), pv's volume depth already
+// one on: for each of the volume illumination samples, a scatter event picked from the march's steps and a distance
+// in it, then free paths from it through the volumes, order after order up to max_volume_depth while the throughput
+// stays above the transmittance threshold; at each event every light's source term with the order's attenuation,
+// added with the order's contribution factor, and the next direction from the phase function with the order's
+// anisotropy. The draws come from one stream a sample, in the reference's order.
+static __device__ __noinline__ void volumeMultipleScatter(const SceneView& s, const Identity& root, const Pending& pv, U64 volumeBranch,
+                                                          const ReplaySteps& lookup, V3 org, V3 dir, V3 T, V3& radiance) {
+    const x2_config& c = s.config;
+    if (!(pv.volumeDepth < c.max_volume_depth && c.volume_illumination_samples > 0)) return;
+    const uint32_t scatterSamples = c.volume_illumination_samples;
+    const float invN = 1.0f / float(scatterSamples);
+    for (uint32_t i = 0; i < scatterSamples; ++i) {
+        Identity mid = root;
+        mid.branch = childBranch(volumeBranch, 0xffff, i);
+        Stream ms(mid, pv.depth, 0);
+        float pdfDensity, utRemapped;
+        const VolumeStep vp = lookup.pick(ms.next(), pdfDensity, utRemapped);
+        float sigmaT = vlum(vp.sigmaT);
+        const float t0 = vp.tStart, t1 = vp.tStart + vp.delta;
+        const float td = sampleDistanceExponential(utRemapped, sigmaT, t0, t1);
+        const float pdfT = pdfDensity * pdfDistanceExponential(td, sigmaT, t0, t1);
+        if (pdfT == 0.0f || !vfinite(pdfT)) continue;
+        const V3 trScatter = vtimes(vp.tr, expNeg(vp.sigmaT, td - t0));
+        V3 scatterPoint = add(org, mul(dir, td));
+        V3 throughput = vscaled(vtimes(vtimes(T, vp.sigmaS), trScatter), 1.0f / pdfT);
+        const float up0 = ms.next(), up1 = ms.next();
+        V3 scatterDir = phaseSample(vp.g, V3{-dir.x, -dir.y, -dir.z}, up0, up1);
+        for (uint32_t depth = pv.volumeDepth; depth < c.max_volume_depth; ++depth) {
+            if (vlum(throughput) < c.volume_transmittance_threshold) break;
+            const float ai = powf(c.volume_attenuation_factor, float(depth)), bi = powf(c.volume_contribution_factor, float(depth)),
+                        ci = powf(c.volume_phase_attenuation_factor, float(depth));
+            const float tFreePath = -logf(1.0f - ms.next()) / sigmaT;
+            Crossing y[kMaxCrossings];
+            uint32_t here;
+            const uint32_t m = volumeIntervals(s, scatterPoint, scatterDir, kVolumeEpsilon, y, here);
+            for (uint32_t j = 0; j < m && y[j].t <= tFreePath; ++j) applyCrossing(here, y[j]);
+            const V3 rayDir = scatterDir;
+            scatterPoint = add(scatterPoint, mul(scatterDir, tFreePath));
+            if (!here) break;
+            const float rnd = c.volume_overlap_mode == kOverlapRnd ? ms.next() : 0.0f;
+            const VolumeCoefficients kk = evalShadersAt(s, here, c.volume_overlap_mode, rnd, scatterPoint, kNoGrid, nullptr, nullptr);
+            const float g = kk.g * ci;
+            sigmaT = vlum(kk.sigmaT);
+            if (vIsZero(sigmaT)) break;
+            throughput = vscaled(vtimes(throughput, kk.sigmaS), 1.0f / sigmaT);
+            for (uint32_t li = 0; li < c.light_count; ++li) {
+                const float usl[3] = {ms.next(), ms.next(), ms.next()};
+                const V3 Ls = volumeSourceTerm(s, ms, s.lights[li], scatterPoint, rayDir, g, usl, ai);
+                radiance = vplus(radiance, vscaled(vtimes(throughput, Ls), invN * bi));
+            }
+            const float uq0 = ms.next(), uq1 = ms.next();
+            scatterDir = phaseSample(g, V3{-rayDir.x, -rayDir.y, -rayDir.z}, uq0, uq1);
+        }
+    }
+}
+
 // What volumeRadiance leaves besides its light: the transmittance the path's throughput takes and the alpha's.
 struct VolumePass {
     V3 transmittance, alphaTransmittance;
@@ -674,6 +748,7 @@ static __device__ __noinline__ V3 volumeRadiance(const SceneView& s, const Ident
             }
         }
         ++pv.volumeDepth;
+        volumeMultipleScatter(s, root, pv, volumeBranch, lookup, org, dir, T, radiance);
     }
     pv.T = vtimes(pv.T, vt);
     return radiance;
