@@ -18,6 +18,16 @@ def box(ctx):
     return s, x2.Scene(ctx, s.desc, s.config)
 
 
+@pytest.fixture(scope="module")
+def ragged(ctx):
+    """The closed box at 250 x 190: partial tiles on the right and bottom edges, regions clamped to the image."""
+    s = x2.SyntheticScene(0)
+    cfg = x2.Config.from_buffer_copy(s.config)
+    cfg.width, cfg.height = 250, 190
+    s.config = cfg
+    return s, x2.Scene(ctx, s.desc, cfg)
+
+
 @needs_reference
 @pytest.mark.parametrize("spp,target", [(5, 0.05), (16, 0.02), (16, 0.002), (37, 0.01)])
 def test_chain_matches_reference_trees(box, spp, target):
@@ -192,4 +202,12 @@ def test_budget_frame_replays_reference_frame(box, budget):
     result, generations = _replay(scene, s.config, 0.0, 4, 256, cellular=True, budget=budget)
     assert result["samples"] <= budget + s.config.width * s.config.height * 32
     assert result["samples"] >= 0.5 * budget
+
+
+@needs_reference
+@pytest.mark.parametrize("cellular", [False, True])
+def test_ragged_frame_replays_reference_frame(ragged, cellular):
+    """Trees and cellular generations on an image whose edge tiles are partial, against the reference replayed."""
+    s, scene = ragged
+    _replay(scene, s.config, 0.001, 4, 128, cellular=cellular)
 
