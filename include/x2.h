@@ -369,6 +369,12 @@ int x2_workgrid_set_suitability(x2_workgrid* grid, const float* gpu_probability,
 int x2_workgrid_set_rates(x2_workgrid* grid, double gpu_items, double cpu_worker, uint32_t cpu_workers, double window);
 int x2_workgrid_rendered(x2_workgrid* grid, uint32_t cell, uint32_t device, uint64_t samples);
 void x2_workgrid_close(x2_workgrid* grid);  /* a drain: nothing is handed out any more */
+/* Important parts first (async_render.h:1581-1611 cellScores, from the preview picture of async_cpu.h:1359-1379):
+ * each cell's score from the scene's film so far, the mean over its sampled pixels of their tones' differences from
+ * their sampled left and upper neighbours (tone: luma / (1 + luma) of the film's mean, 0 unless finite and positive),
+ * -1 for a cell without samples; computed on the device, then set on the grid (x2_workgrid_set_scores). scores: each
+ * cell's score (host array, may be null). The grid's size must be the film's. Waits. */
+int x2_workgrid_score_film(x2_scene* scene, x2_workgrid* grid, float* scores);
 /* The GPU broker: its next launch's chunks, up to want, taken by its cellular workers (options.gpu_workers, seeded at
  * the first call), a share each, from their cells by the cellular rules. Returns how many. One broker thread a grid. */
 uint32_t x2_workgrid_take(x2_workgrid* grid, uint32_t want, x2_chunk* out);

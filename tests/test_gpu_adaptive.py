@@ -211,3 +211,13 @@ def test_ragged_frame_replays_reference_frame(ragged, cellular):
     s, scene = ragged
     _replay(scene, s.config, 0.001, 4, 128, cellular=cellular)
 
+
+
+def test_adaptive_arguments_refused(box):
+    s, scene = box
+    for call in (lambda: scene.render_adaptive(4, 0, 0.001), lambda: scene.render_adaptive(4, 64, 0.0),
+                 lambda: scene.render_adaptive(4, 64, -1.0, cellular=True), lambda: scene.render_adaptive_budget(4, 64, 0.0, 0),
+                 lambda: scene.render_adaptive_budget(4, 64, -1.0, 1000)):
+        with pytest.raises(x2.X2Error) as e:
+            call()
+        assert e.value.code == x2.EINVAL

@@ -58,3 +58,55 @@ def test_mismatched_grid_is_refused(box):
     grid = x2.WorkGrid(s.config.width + 8, s.config.height, 4)
     with pytest.raises(x2.X2Error):
         scene.render_workgrid(grid, 64)
+
+
+def _cell_scores(sums, counts, width, height, cell):
+    """The reference's cellScores (async_render.h:1581-1611) over the preview picture of HostFilm::preview
+    (async_cpu.h:1359-1379: each pixel's sum over its count, as float32), restated in numpy with float32 tones and the
+    cells' FP64 sums taken in the reference's pixel order."""
+    n = counts.astype(np.float64)
+    rgb = np.where(counts[:, None] > 0, (sums[:, :3] / np.maximum(n, 1)[:, None]).astype(np.float32), np.float32(0))
+    lum = (np.float32(0.2126) * rgb[:, 0] + np.float32(0.7152) * rgb[:, 1]) + np.float32(0.0722) * rgb[:, 2]
+    with np.errstate(invalid="ignore", over="ignore"):
+        tone = np.where(np.isfinite(lum) & (lum > 0), lum / (np.float32(1) + lum), np.float32(0)).astype(np.float32)
+    covered = (counts > 0).reshape(height, width)
+    tone = tone.reshape(height, width)
+    d = np.zeros((height, width), np.float64)
+    left = np.zeros_like(covered)
+    left[:, 1:] = covered[:, :-1]
+    up = np.zeros_like(covered)
+    up[1:, :] = covered[:-1, :]
+    dl = np.zeros((height, width), np.float32)
+    dl[:, 1:] = np.abs(tone[:, 1:] - tone[:, :-1])
+    du = np.zeros((height, width), np.float32)
+    du[1:, :] = np.abs(tone[1:, :] - tone[:-1, :])
+    d = np.where(left, dl.astype(np.float64), 0.0)
+    d = d + np.where(up, du.astype(np.float64), 0.0)
+    cx, cy = (width + cell - 1) // cell, (height + cell - 1) // cell
+    scores = np.full(cx * cy, -1.0, np.float32)
+    for c in range(cx * cy):
+        x0, y0 = (c % cx) * cell, (c // cx) * cell
+        block = d[y0:y0 + cell, x0:x0 + cell][covered[y0:y0 + cell, x0:x0 + cell]]
+        if len(block):
+            scores[c] = np.float32(np.cumsum(block)[-1] / len(block))
+    return scores
+
+
+def test_cell_scores_from_the_film(box):
+    """Important parts first: the cells' scores computed on the device from a film where a third of the tiles have
+    samples equal the reference's cellScores restated over the same film, bit for bit."""
+    s, scene = box
+    cfg = s.config
+    tiles = ((cfg.width + 7) // 8) * ((cfg.height + 7) // 8)
+    sel = np.arange(0, tiles, 3, dtype=np.uint32)
+    chunks = np.zeros(len(sel), x2.CHUNK_DTYPE)
+    chunks["tile"], chunks["first"], chunks["count"] = sel, 0, 4
+    scene.frame_begin(4)
+    scene.launch_wavefront(chunks)
+    scene.wait()
+    sums, counts = scene.film()
+    grid = x2.WorkGrid(cfg.width, cfg.height, 16, x2.workgrid_options(cell_size=32))
+    got = scene.score_workgrid(grid)
+    want = _cell_scores(sums, counts, cfg.width, cfg.height, 32)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32)), f"{int(np.count_nonzero(got != want))} cells differ"
+    assert (got > 0).sum() > 0

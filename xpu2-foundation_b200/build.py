@@ -11,7 +11,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "x2", "libx2.so")
 BUILD = os.path.join(HERE, "_build")
-CU = ["api.cu", "render.cu", "wavefront.cu", "bvh_build.cu", "noalloc.cu", "adjoint.cu", "adaptive.cu"]
+CU = ["api.cu", "render.cu", "wavefront.cu", "bvh_build.cu", "noalloc.cu", "adjoint.cu", "adaptive.cu", "scores.cu"]
 CPP = ["scene_gen.cpp", "grid.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -199,7 +199,7 @@ def library():
         "x2_workgrid_set_rates": ([vp, C.c_double, C.c_double, u32, C.c_double], i32),
         "x2_workgrid_rendered": ([vp, u32, u32, u64], i32), "x2_workgrid_close": ([vp], None),
         "x2_workgrid_take": ([vp, u32, vp], u32), "x2_workgrid_stolen": ([vp], u64),
-        "x2_render_workgrid": ([vp, vp, u32, C.POINTER(WorkGridResult)], i32),
+        "x2_render_workgrid": ([vp, vp, u32, C.POINTER(WorkGridResult)], i32), "x2_workgrid_score_film": ([vp, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -424,6 +424,12 @@ class Scene:
         r = AdaptiveResult()
         _check(library().x2_render_adaptive_budget(self._h, min_samples, max_samples, floor, budget, C.byref(r)))
         return {"passes": r.passes, "converged": bool(r.converged), "samples": r.samples, "milliseconds": r.milliseconds}
+
+    def score_workgrid(self, grid):
+        """x2_workgrid_score_film: the grid's cell scores from this scene's film (set on the grid); returns them."""
+        out = np.zeros(grid.cells, np.float32)
+        _check(library().x2_workgrid_score_film(self._h, grid._h, _ptr(out)))
+        return out
 
     def adaptive_planned(self):
         cfg = self.config
