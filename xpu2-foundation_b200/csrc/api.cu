@@ -197,7 +197,6 @@ struct x2_scene {
     WaveState wave{};
     uint32_t wavePaths = 0, waveRecords = 0, reservePaths = 0;  // the last launch's paths; records a path
     uint32_t waveCap = 0;                                          // paths the wave's buffers hold
-    cudaGraphExec_t waveExec = nullptr;  // the last wavefront launch's drain graph, updated in place by the next
     uint32_t* extendQ = nullptr;
     uint32_t* shadowQ = nullptr;
     uint32_t* waveCounters = nullptr;  // kWaveCounters words
@@ -214,6 +213,12 @@ struct x2_scene {
     uint8_t* outStatus = nullptr;
     uint64_t outCap = 0, lastItems = 0;
     uint32_t waveIterations = 0;       // of the last wavefront launch
+    // The asynchronous wavefront launch's drain: [0] its iterations, [1] a running total, [2] its overrun word
+    // (device; 4 words), their host copy (pinned), the launch they belong to (0: none pending) and its bound.
+    uint32_t* drainWords = nullptr;
+    uint32_t* hostDrain = nullptr;
+    uint64_t drainSeq = 0;
+    uint32_t drainBound = 0;
     bool waveTiming = false;           // time each kernel kind (no graph)
     float waveMs[5] = {0, 0, 0, 0, 0}; // logic, extend, shade, shadow, film reduce
     uint32_t queueLog[2 * 4096] = {};  // timed launches: each iteration's extend and shadow queue sizes
@@ -353,6 +358,8 @@ int ensureWave(x2_scene* s, uint32_t paths, uint32_t records) {
     if (ok && !s->waveCounters) ok = cudaMalloc(&s->waveCounters, sizeof(uint32_t) * kWaveCounters) == cudaSuccess;
     if (ok && !s->claimed) ok = cudaMalloc(&s->claimed, sizeof(unsigned long long)) == cudaSuccess;
     if (ok && !s->hostLast) ok = cudaMallocHost(&s->hostLast, sizeof(uint32_t) * 4) == cudaSuccess;
+    if (ok && !s->drainWords) ok = cudaMalloc(&s->drainWords, sizeof(uint32_t) * 4) == cudaSuccess;
+    if (ok && !s->hostDrain) ok = cudaMallocHost(&s->hostDrain, sizeof(uint32_t) * 4) == cudaSuccess;
     if (!ok) {
         freeWave(s);
         setError("device allocation failed for %u wavefront paths", paths);
@@ -804,7 +811,6 @@ int x2_scene_free(x2_scene* s) {
     cudaFree(s->volumeTris);
     cudaFree(s->grids);
     for (float* g : s->gridValues) cudaFree(g);
-    if (s->waveExec) cudaGraphExecDestroy(s->waveExec);
     freeWave(s);
     cudaFree(s->out);
     cudaFree(s->outStatus);
@@ -813,6 +819,8 @@ int x2_scene_free(x2_scene* s) {
     cudaFree(s->waveCounters);
     cudaFree(s->claimed);
     if (s->hostLast) cudaFreeHost(s->hostLast);
+    cudaFree(s->drainWords);
+    if (s->hostDrain) cudaFreeHost(s->hostDrain);
     cudaFree(s->sums);
     cudaFree(s->odd);
     cudaFree(s->counts);
@@ -1071,7 +1079,16 @@ int x2_poll(x2_scene* s, x2_completion* out) {
         setError("launch failed: %s", cudaGetErrorString(q));
         return -X2_ECUDA;
     }
+    const uint64_t seq = oldest->seq;
     retire(s, *oldest, out);
+    if (s->drainSeq && seq == s->drainSeq) {  // an asynchronous wavefront launch: its drain's outcome
+        s->drainSeq = 0;
+        s->waveIterations = s->hostDrain[0];
+        if (s->hostDrain[2]) {
+            setError("wavefront did not drain after %u iterations", s->drainBound);
+            return -X2_EDEVICE;
+        }
+    }
     return 1;
 }
 
@@ -1291,71 +1308,72 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
         s->waveIterations = iterations;
         return X2_OK;
     }
-    // One graph of kIter iterations, replayed until no path is left to trace.
-    constexpr int kIter = 8;
+    // One graph: the launch's iterations in a conditional while node, each iteration's last kernel deciding whether
+    // another follows (at most maxIter; past that it raises the overrun word), then the film reduce. The launch runs
+    // without the host; x2_poll / x2_wait collect it like any launch.
     cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    CUDA_OR(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), X2_ECUDA);
-    for (int it = 0; it < kIter; ++it) {
+    CUDA_OR(cudaGraphCreate(&graph, 0), X2_ECUDA);
+    cudaError_t err = cudaSuccess;
+    auto check = [&](cudaError_t e) {
+        if (err == cudaSuccess && e != cudaSuccess) err = e;
+        return err == cudaSuccess;
+    };
+    cudaGraphConditionalHandle loop;
+    cudaGraphNode_t node = nullptr;
+    cudaGraphNodeParams cp = {};
+    if (check(cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault))) {
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = loop;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        check(cudaGraphAddNode(&node, graph, nullptr, 0, &cp));
+    }
+    const uint32_t bound = uint32_t(std::min<uint64_t>(maxIter, 0xffffffffu));
+    if (err == cudaSuccess && check(cudaStreamBeginCaptureToGraph(st, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                                  cudaStreamCaptureModeThreadLocal))) {
         wfResetQueues<<<1, 32, 0, st>>>(a);
         wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
         wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
         if (a.shadeQ) wfSortShade<<<gridWork, kWaveBlock, 0, st>>>(a);
         wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
         wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
+        wfDrainCheck<<<1, 32, 0, st>>>(a, loop, s->drainWords, bound, s->drainWords + 2);
+        check(cudaGetLastError());
+        cudaGraph_t body = nullptr;
+        check(cudaStreamEndCapture(st, &body));
     }
-    wfResetQueues<<<1, 32, 0, st>>>(a);  // the last iteration's extend count, for the host
-    CUDA_OR(cudaStreamEndCapture(st, &graph), X2_ECUDA);
-    // The graph differs from the last launch's in its kernels' arguments at most (same kernels in the same order)
-    // unless the scene's shape changed: update the last executable graph in place, instantiate when that fails.
-    bool updated = false;
-    if (s->waveExec) {
-        cudaGraphExecUpdateResultInfo info;
-        updated = cudaGraphExecUpdate(s->waveExec, graph, &info) == cudaSuccess;
-        if (!updated) {
-            (void)cudaGetLastError();  // the failed update's status, not an error of the launch
-            cudaGraphExecDestroy(s->waveExec);
-            s->waveExec = nullptr;
-        }
+    if (err == cudaSuccess && check(cudaStreamBeginCaptureToGraph(st, graph, &node, nullptr, 1, cudaStreamCaptureModeThreadLocal))) {
+        wfFilmReduce<<<int((64ull * count + 255) / 256), 256, 0, st>>>(a, count, s->sums, s->adaptive ? s->odd : nullptr, s->counts);
+        check(cudaGetLastError());
+        cudaGraph_t out = nullptr;
+        check(cudaStreamEndCapture(st, &out));
     }
-    if (!updated && cudaGraphInstantiate(&s->waveExec, graph, 0) != cudaSuccess) {
-        cudaGraphDestroy(graph);
-        s->waveExec = nullptr;
-        setError("graph instantiation failed");
+    cudaGraphExec_t exec = nullptr;
+    if (err == cudaSuccess) check(cudaGraphInstantiate(&exec, graph, 0));
+    cudaGraphDestroy(graph);
+    if (err != cudaSuccess) {
+        setError("x2_launch_wavefront: building the launch's graph: %s", cudaGetErrorString(err));
         return X2_ECUDA;
     }
-    cudaGraphDestroy(graph);
-    exec = s->waveExec;
+    cudaMemsetAsync(s->drainWords, 0, sizeof(uint32_t) * 4, st);
     cudaEventRecord(sl.begin, st);
-    uint32_t iterations = 0;
-    int rc = X2_OK;
-    for (;;) {
-        if (cudaGraphLaunch(exec, st) != cudaSuccess) {
-            setError("graph launch failed");
-            rc = X2_ECUDA;
-            break;
-        }
-        iterations += kIter;
-        cudaMemcpyAsync(s->hostLast, s->waveCounters + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
-        if ((rc = x2_synchronize(s->ctx, 600000)) != X2_OK) break;
-        if (s->hostLast[0] == 0) break;
-        if (iterations > maxIter) {
-            setError("wavefront did not drain after %u iterations", iterations);
-            rc = X2_EDEVICE;
-            break;
-        }
+    const cudaError_t launched = cudaGraphLaunch(exec, st);
+    cudaGraphExecDestroy(exec);  // released once the launch completes
+    if (launched != cudaSuccess) {
+        setError("graph launch failed: %s", cudaGetErrorString(launched));
+        return X2_ECUDA;
     }
-    if (rc) return rc;
-    wfFilmReduce<<<int((64ull * count + 255) / 256), 256, 0, st>>>(a, count, s->sums, s->adaptive ? s->odd : nullptr, s->counts);
-    CUDA_OR(cudaGetLastError(), X2_ECUDA);
     cudaEventRecord(sl.end, st);
-    // The extend kernels counted the traced rays; the launch's counters go to the host as x2_launch's do.
+    // The extend kernels counted the traced rays; the launch's counters go to the host as x2_launch's do, with the
+    // drain's iteration count and overrun word.
     cudaMemcpyAsync(sl.hostCounters, sl.counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);
+    cudaMemcpyAsync(s->hostDrain, s->drainWords, sizeof(uint32_t) * 4, cudaMemcpyDeviceToHost, st);
     cudaEventRecord(sl.done, st);
     sl.busy = true;
     sl.seq = s->nextSeq++;
     s->lastItems = items;
-    s->waveIterations = iterations;
+    s->drainSeq = sl.seq;
+    s->drainBound = bound;
     return X2_OK;
 }
 
