@@ -370,8 +370,9 @@ def probe_batch(args):
 def probe_volume(args):
     """Config 3 (the participating medium: a 256^3 grid in the closed box, a rect light and a sun; 512x512, 256 spp,
     depth 64): `--probe-tiles` evenly spaced 8x8 tiles (all 4096 by default when the flag is left at its 592 default
-    is not wanted, pass 4096) at full spp in the wavefront form, then the plain megakernel on the same tiles; the
-    films compared and audited. Prints Msamples/s of each form."""
+    is not wanted, pass 4096) at full spp in the wavefront form (`--probe-timed`: without its graph, each kernel
+    timed), then the plain megakernel on the same tiles; the films compared and audited. Prints Msamples/s of each
+    form."""
     import x2
 
     ctx = x2.Context(0)
@@ -387,10 +388,14 @@ def probe_volume(args):
     films = {}
     for form in ("wavefront", "plain"):
         scene.frame_begin(cfg.spp)
+        if form == "wavefront":
+            scene.wavefront_timing(args.probe_timed)  # --probe-timed: no graph, each kernel's launches visible
         (scene.launch_wavefront if form == "wavefront" else scene.launch)(chunks)
         c = scene.wait()
         films[form] = scene.film()
         out[form] = {"ms": c.milliseconds, "msamples_per_s": n / c.milliseconds / 1e3, "errors": c.errors}
+        if form == "wavefront" and args.probe_timed:
+            out["kernel_ms"] = scene.wavefront_timing(None)
     out["films_close"] = bool(np.allclose(films["wavefront"][0], films["plain"][0], rtol=1e-9, atol=1e-9) and
                               np.array_equal(films["wavefront"][1], films["plain"][1]))
     out["counters"] = scene.counters()
