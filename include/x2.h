@@ -381,6 +381,18 @@ int x2_workgrid_score_film(x2_scene* scene, x2_workgrid* grid, float* scores);
  * the first call), a share each, from their cells by the cellular rules. Returns how many. One broker thread a grid. */
 uint32_t x2_workgrid_take(x2_workgrid* grid, uint32_t want, x2_chunk* out);
 uint64_t x2_workgrid_stolen(const x2_workgrid* grid);  /* chunks the broker took from cells the CPU owns */
+/* Cell ownership across frames (Ownership, async_grid.h:432-480): x2_workgrid_ownership_finished records a finished
+ * frame's grid (each cell's samples by device, x2_workgrid_rendered) and decides the flips for the next frame: a cell
+ * whose other device rendered more than 0.6 of its samples over the last 8 frames changes owner, at most
+ * min(8, max(1, cells / 10)) a frame, the furthest ahead first, none within 16 frames of its last flip, and a flip back
+ * within 32 frames freezes ownership for 64 frames. x2_workgrid_ownership_owners gives the owners for a new grid of
+ * `cells` cells (one word a cell, 1: the GPU's; pass them to x2_workgrid_create) and returns 1, or 0 when it has none
+ * for that size (the checkerboard then). */
+typedef struct x2_workgrid_ownership x2_workgrid_ownership;
+int x2_workgrid_ownership_create(x2_workgrid_ownership** out);
+void x2_workgrid_ownership_free(x2_workgrid_ownership* ownership);
+int x2_workgrid_ownership_finished(x2_workgrid_ownership* ownership, const x2_workgrid* grid);
+uint32_t x2_workgrid_ownership_owners(const x2_workgrid_ownership* ownership, uint32_t cells, uint32_t* owners);
 typedef struct x2_workgrid_result {
     uint64_t launches, chunks, samples;  /* wavefront launches made, chunks and samples rendered */
     float milliseconds;                  /* host time of the whole frame */

@@ -1154,6 +1154,18 @@ void x2ref_grid_append(void* g, uint32_t cell, const x2_chunk* chunks, uint32_t 
     static_cast<xi::async::Grid*>(g)->append(cell, reinterpret_cast<const xi::async::Chunk*>(chunks), n);
 }
 void x2ref_grid_close(void* g) { static_cast<xi::async::Grid*>(g)->close(); }
+void x2ref_grid_rendered(void* g, uint32_t cell, uint32_t device, uint64_t samples) {
+    static_cast<xi::async::Grid*>(g)->rendered(cell, xi::async::Device(device), samples);
+}
+void* x2ref_ownership_open() { return new xi::async::Ownership(); }
+void x2ref_ownership_free(void* o) { delete static_cast<xi::async::Ownership*>(o); }
+void x2ref_ownership_finished(void* o, void* g) { static_cast<xi::async::Ownership*>(o)->finished(*static_cast<xi::async::Grid*>(g)); }
+uint32_t x2ref_ownership_owners(void* o, uint32_t cells, uint32_t* out) {
+    const auto* v = static_cast<xi::async::Ownership*>(o)->owners(cells);
+    if (!v) return 0;
+    for (uint32_t i = 0; i < cells; ++i) out[i] = (*v)[i] == xi::async::Device::Gpu ? 1u : 0u;
+    return 1;
+}
 
 // paths::childBranch (async_integrator.h:281-287), the reference's own.
 uint64_t x2ref_child_branch(uint64_t parent, uint32_t a, uint32_t b) { return xi::async::paths::childBranch(parent, a, b); }

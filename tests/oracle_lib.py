@@ -390,6 +390,11 @@ class RefWorkGrid:
     def close(self):
         self.lib.x2ref_grid_close(self._h)
 
+    def rendered(self, cell, device, samples):
+        f = self.lib.x2ref_grid_rendered
+        f.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64]
+        f(self._h, cell, device, samples)
+
     def take(self, want, cells):
         """The reference feeder's claims for one GPU launch (async_render.h:784-797), restated over this grid: `cells`
         (the GPU's cellular workers' cells, seeded by the caller with seed()) move as the feeder moves them."""
@@ -410,4 +415,30 @@ class RefWorkGrid:
                 need -= len(c)
                 moves += 1
         return np.concatenate(out) if out else np.zeros(0, x2.CHUNK_DTYPE)
+
+
+class RefOwnership:
+    """The reference's cell ownership across frames (async_grid.h Ownership)."""
+
+    def __init__(self):
+        lib = self.lib = C.CDLL(REFERENCE)
+        lib.x2ref_ownership_open.restype = C.c_void_p
+        lib.x2ref_ownership_free.argtypes = [C.c_void_p]
+        lib.x2ref_ownership_finished.argtypes = [C.c_void_p, C.c_void_p]
+        lib.x2ref_ownership_owners.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
+        lib.x2ref_ownership_owners.restype = C.c_uint32
+        self._h = lib.x2ref_ownership_open()
+
+    def finished(self, grid):
+        self.lib.x2ref_ownership_finished(self._h, grid._h)
+
+    def owners(self, cells):
+        out = np.zeros(max(cells, 1), np.uint32)
+        return out[:cells] if self.lib.x2ref_ownership_owners(self._h, cells, out.ctypes.data) else None
+
+    def __del__(self):
+        try:
+            self.lib.x2ref_ownership_free(self._h)
+        except Exception:
+            pass
 

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle_lib
-from oracle_lib import RefWorkGrid, x2
+from oracle_lib import RefOwnership, RefWorkGrid, x2
 
 needs_reference = pytest.mark.skipif(not oracle_lib.have_reference(), reason="oracle/_ref not built")
 NONE = 0xFFFFFFFF
@@ -177,3 +177,44 @@ def test_bad_grids_are_refused():
         x2.WorkGrid(64, 64, 4, x2.workgrid_options(cell_size=12))
     with pytest.raises(x2.X2Error):
         x2.WorkGrid(64, 64, 4, x2.workgrid_options(mode=3))
+
+
+@needs_reference
+@pytest.mark.parametrize("size", [(640, 448), (1920, 1088)])
+def test_ownership_flips_match_reference(size):
+    """Ownership across 200 frames against the reference's Ownership: each frame a grid made with the owners so far,
+    every cell's samples split between the devices around a drifting preference (shifted every 20 frames, so cells
+    flip, cool down and flip back into a freeze), then the frame recorded; the owners agree frame after frame."""
+    width, height = size
+    options = x2.workgrid_options(samples_per_chunk=4)
+    n = ((width + 63) // 64) * ((height + 63) // 64)
+    rng = np.random.default_rng(width + height)
+    mine, ref = x2.Ownership(), RefOwnership()
+    prefer = rng.random(n)
+    flips, previous = 0, None
+    for frame in range(200):
+        own = mine.owners(n)
+        want = ref.owners(n)
+        assert (own is None) == (want is None), f"frame {frame}"
+        if own is not None:
+            assert np.array_equal(own, want), f"frame {frame}: {int(np.count_nonzero(own != want))} owners differ"
+            if previous is not None:
+                flips += int(np.count_nonzero(own != previous))
+            previous = own.copy()
+        g = x2.WorkGrid(width, height, 4, options, owners=own)
+        r = RefWorkGrid(width, height, 4, options, owners=want)
+        if frame % 20 == 19:
+            moved = rng.random(n) < 0.4
+            prefer[moved] = rng.random(int(moved.sum()))
+        totals = rng.integers(0, 5000, n)
+        share = np.clip(prefer + rng.normal(0, 0.05, n), 0, 1)
+        for i in range(n):
+            gpu = int(totals[i] * share[i])
+            for grid in (g, r):
+                grid.rendered(i, x2.DEVICE_GPU, gpu)
+                grid.rendered(i, x2.DEVICE_CPU, int(totals[i]) - gpu)
+        mine.finished(g)
+        ref.finished(r)
+    print(f"{n} cells, {flips} flips over 200 frames")
+    assert flips > 0
+

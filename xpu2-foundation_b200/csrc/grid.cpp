@@ -478,4 +478,70 @@ uint32_t x2_workgrid_take(x2_workgrid* g, uint32_t want, x2_chunk* out) {
 
 uint64_t x2_workgrid_stolen(const x2_workgrid* g) { return g ? g->stolen : 0; }
 
+// Cell ownership across the frames of one grid size (the reference's Ownership, async_grid.h:432-480): each finished
+// frame records every cell's GPU share of its samples in an 8-frame window; from the ninth frame on, a cell whose
+// other device took more than 0.6 of the window's samples flips, at most min(8, max(1, cells / 10)) a frame, the
+// furthest ahead first (ties by cell index), a cell at most once in 16 frames; a cell flipping back within 32 frames
+// freezes every flip for 64 frames instead.
+struct x2_workgrid_ownership {
+    static constexpr uint32_t kWindow = 8;
+    std::vector<uint32_t> owners;
+    std::vector<float> history;
+    std::vector<long long> lastFlip;
+    long long frame = 0, frozenUntil = 0;
+};
+
+int x2_workgrid_ownership_create(x2_workgrid_ownership** out) {
+    if (!out) return X2_EINVAL;
+    *out = new (std::nothrow) x2_workgrid_ownership();
+    return *out ? X2_OK : X2_ENOMEM;
+}
+
+void x2_workgrid_ownership_free(x2_workgrid_ownership* o) { delete o; }
+
+uint32_t x2_workgrid_ownership_owners(const x2_workgrid_ownership* o, uint32_t cells, uint32_t* owners) {
+    if (!o || o->owners.size() != cells || !cells) return 0;
+    if (owners) std::copy(o->owners.begin(), o->owners.end(), owners);
+    return 1;
+}
+
+int x2_workgrid_ownership_finished(x2_workgrid_ownership* o, const x2_workgrid* g) {
+    if (!o || !g) return X2_EINVAL;
+    constexpr uint32_t W = x2_workgrid_ownership::kWindow;
+    const uint32_t n = g->cellCount;
+    if (o->owners.size() != n) {
+        o->owners.resize(n);
+        o->history.assign(size_t(n) * W, 0.0f);
+        o->lastFlip.assign(n, -1000000);
+        for (uint32_t i = 0; i < n; ++i) o->owners[i] = g->cells[i].owner;
+    }
+    for (uint32_t i = 0; i < n; ++i) {
+        const double cpu = double(g->cells[i].samples[0].load()), gpu = double(g->cells[i].samples[1].load());
+        o->history[size_t(i) * W + size_t(o->frame % W)] = cpu + gpu > 0 ? float(gpu / (cpu + gpu)) : 0.5f;
+    }
+    ++o->frame;
+    if (o->frame < o->frozenUntil || o->frame < W) return X2_OK;
+    std::vector<std::pair<float, uint32_t>> flips;  // (the other device's share, cell)
+    for (uint32_t i = 0; i < n; ++i) {
+        if (o->frame - o->lastFlip[i] < 16) continue;
+        float gpuShare = 0;
+        for (uint32_t k = 0; k < W; ++k) gpuShare += o->history[size_t(i) * W + k];
+        gpuShare /= W;
+        const float other = o->owners[i] == X2_DEVICE_CPU ? gpuShare : 1 - gpuShare;
+        if (other > 0.6f) flips.push_back({other, i});
+    }
+    std::stable_sort(flips.begin(), flips.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    const size_t limit = std::min<size_t>(8, std::max<size_t>(1, n / 10));
+    for (size_t k = 0; k < flips.size() && k < limit; ++k) {
+        const uint32_t i = flips[k].second;
+        if (o->frame - o->lastFlip[i] < 32) {
+            o->frozenUntil = o->frame + 64;
+            return X2_OK;
+        }
+        o->owners[i] = o->owners[i] == X2_DEVICE_CPU ? uint32_t(X2_DEVICE_GPU) : uint32_t(X2_DEVICE_CPU);
+        o->lastFlip[i] = o->frame;
+    }
+    return X2_OK;
+}
+
 }  // extern "C"

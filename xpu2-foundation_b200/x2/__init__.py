@@ -199,7 +199,9 @@ def library():
         "x2_workgrid_set_rates": ([vp, C.c_double, C.c_double, u32, C.c_double], i32),
         "x2_workgrid_rendered": ([vp, u32, u32, u64], i32), "x2_workgrid_close": ([vp], None),
         "x2_workgrid_take": ([vp, u32, vp], u32), "x2_workgrid_stolen": ([vp], u64),
-        "x2_render_workgrid": ([vp, vp, u32, C.POINTER(WorkGridResult)], i32), "x2_workgrid_score_film": ([vp, vp, vp], i32),
+        "x2_render_workgrid": ([vp, vp, u32, C.POINTER(WorkGridResult)], i32),
+        "x2_workgrid_ownership_create": ([C.POINTER(vp)], i32), "x2_workgrid_ownership_free": ([vp], None),
+        "x2_workgrid_ownership_finished": ([vp, vp], i32), "x2_workgrid_ownership_owners": ([vp, u32, vp], u32), "x2_workgrid_score_film": ([vp, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -689,4 +691,32 @@ class WorkGrid:
     @property
     def stolen(self):
         return library().x2_workgrid_stolen(self._h)
+
+    def rendered(self, cell, device, samples):
+        _check(library().x2_workgrid_rendered(self._h, cell, device, samples))
+
+
+class Ownership:
+    """Cell ownership across frames (x2_workgrid_ownership_*): flips towards the device that rendered most of a cell."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        _check(library().x2_workgrid_ownership_create(C.byref(h)))
+        self._h = h
+
+    def __del__(self):
+        try:
+            if self._h:
+                library().x2_workgrid_ownership_free(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+    def finished(self, grid):
+        _check(library().x2_workgrid_ownership_finished(self._h, grid._h))
+
+    def owners(self, cells):
+        """The owners for a new grid of `cells` cells (1: the GPU's), or None for the checkerboard."""
+        out = np.zeros(max(cells, 1), np.uint32)
+        return out[:cells] if library().x2_workgrid_ownership_owners(self._h, cells, _ptr(out)) else None
 
