@@ -84,7 +84,7 @@ X2_AD int nodeBound(const IBox& b) {
     return 2 * int(ceilf(mulR(float(w) / kMinNode, float(h) / kMinNode))) - 1;
 }
 // A node's error: its summed pixel error over the square root of its area times a fixed image area (so regions of
-// any image are judged alike).
+// any image are weighed alike).
 X2_AD float nodeError(float error, float area) {
     constexpr float imageArea = ((815.0f - 0.0f) * (1943.0f - -24.0f)) / 4.0f;
     return error / sqrtf(mulR(area, imageArea));
