@@ -218,3 +218,37 @@ def test_ownership_flips_match_reference(size):
     print(f"{n} cells, {flips} flips over 200 frames")
     assert flips > 0
 
+
+
+@needs_reference
+def test_appended_passes_match_reference():
+    """An adaptive frame's grid: cells start empty and the coordinator appends each pass's chunks; claims by both
+    devices' workers against the reference's grid fed the same appends, every answer equal."""
+    options = x2.workgrid_options(cell_size=32)
+    mine = x2.WorkGrid(300, 200, 16, options, empty=True)
+    ref = RefWorkGrid(300, 200, 16, options, empty=True)
+    assert mine.total == ref.total == 0 and mine.ranges() == ref.ranges() == []
+    rng = np.random.default_rng(11)
+    tiles_x = (300 + 7) // 8
+    cells_x = (300 + 31) // 32
+    for p in range(6):
+        for cell in range(mine.cells):
+            cx, cy = cell % cells_x, cell // cells_x
+            tiles = [ty * tiles_x + tx for ty in range(cy * 4, min(25, cy * 4 + 4)) for tx in range(cx * 4, min(tiles_x, cx * 4 + 4))]
+            keep = [t for t in tiles if rng.random() < 0.6]
+            chunks = np.zeros(len(keep), x2.CHUNK_DTYPE)
+            chunks["tile"], chunks["first"], chunks["count"], chunks["cell"] = keep, p << 16, 4, cell
+            mine.append(cell, chunks)
+            ref.append(cell, chunks)
+        assert mine.total == ref.total
+        for _ in range(200):
+            d = int(rng.integers(0, 2))
+            cur = int(rng.integers(0, mine.cells))
+            a, b = mine.choose(d, cur, 3), ref.choose(d, cur, 3)
+            assert a == b
+            if a == NONE:
+                break
+            n = int(rng.integers(1, 12))
+            assert np.array_equal(mine.claim(a, n, d), ref.claim(a, n, d))
+        for i in range(mine.cells):
+            assert mine.remaining(i) == ref.remaining(i)
