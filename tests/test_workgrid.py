@@ -252,3 +252,25 @@ def test_appended_passes_match_reference():
             assert np.array_equal(mine.claim(a, n, d), ref.claim(a, n, d))
         for i in range(mine.cells):
             assert mine.remaining(i) == ref.remaining(i)
+
+
+@pytest.mark.parametrize("world", [1, 2, 3, 8])
+def test_ranks_shares_cover_the_frame_once(world):
+    """Each rank's grid is its share of the frame (x2.lanes.share: sample_first, sample_count): drained, the ranks'
+    chunks together cover every tile's samples [0, spp) exactly once, in the progressive order within each share."""
+    from x2 import lanes
+
+    width, height, spp = 200, 136, 37
+    tiles = ((width + 7) // 8) * ((height + 7) // 8)
+    cover = np.zeros((tiles, spp), np.int32)
+    for rank in range(world):
+        first, count = lanes.share(rank, world, spp)
+        g = x2.WorkGrid(width, height, spp, x2.workgrid_options(mode=x2.WORKGRID_GPU, sample_first=first, sample_count=count))
+        while True:
+            c = g.take(1000)
+            if not len(c):
+                break
+            for t, f, n in zip(c["tile"], c["first"], c["count"]):
+                cover[t, f:f + n] += 1
+        assert g.empty()
+    assert (cover == 1).all()
