@@ -319,57 +319,48 @@ int x2_render_adaptive_budget(x2_scene* scene, uint32_t min_samples, uint32_t ma
                               x2_adaptive_result* result);
 int x2_adaptive_planned(x2_scene* scene, uint32_t* planned);
 
-/* ---- the work grid: replaces Grid (async_grid.h:96-430) and the GPU feeder's claims (async_render.h:600-605,
- * 780-797) ----
- * The image in square cells, each with its queue of unstarted chunks (x2_chunk.cell: the chunk's cell) that any number
- * of claimants take from, each chunk exactly once. A uniform frame's chunks are made at creation: its sample ranges
- * (progressive: 1, 1, 2, then samples_per_chunk samples; else samples_per_chunk each) over every tile with pixels in
- * the viewport, each cell's ordered by range and then tile; a claim reaches no further than its device's frontier (the
- * least range still unclaimed among the cells the device works), an important cell one range further. Devices:
- * X2_DEVICE_CPU, X2_DEVICE_GPU. Claims are thread-safe; appends have one writer. */
-enum { X2_DEVICE_CPU = 0, X2_DEVICE_GPU = 1 };
-enum { X2_WORKGRID_CPU = 0, X2_WORKGRID_GPU = 1, X2_WORKGRID_BOTH = 2 }; /* which devices own cells (GridOptions::mode) */
+/* ---- the work grid: replaces Grid (async_grid.h:96-430) as the GPU lane uses it (GridOptions::mode 1, every cell
+ * the GPU's), and the GPU feeder's claims (async_render.h:600-605, 780-797) ----
+ * The image in square cells, each handing out its chunks (x2_chunk.cell: the chunk's cell) through one cursor, so any
+ * number of claimants take each chunk exactly once. A uniform frame's chunks: its sample ranges (progressive: 1, 1, 2,
+ * then samples_per_chunk samples; else samples_per_chunk each) over every tile with pixels in the viewport, each
+ * cell's ordered by range and then tile; a claim reaches no further than the frontier (the least range still
+ * unclaimed among the cells with work left), an important cell one range further. The CPU lane's side of the
+ * reference's grid (owners, rights of passage, rates, suitability, ownership across frames) has no counterpart: the
+ * product has no CPU lane. Claims are thread-safe; appends have one writer. */
 typedef struct x2_workgrid x2_workgrid;
 typedef struct x2_workgrid_options {
     uint32_t cell_size;          /* pixels, a multiple of 8 (default 64) */
     uint32_t samples_per_chunk;  /* sample indices a chunk (default 4) */
-    int32_t mode;                /* X2_WORKGRID_*: both devices own cells in a checkerboard unless owners are given */
     uint32_t progressive;        /* 1: the progressive order (default); 0: ranges of samples_per_chunk */
     uint32_t sample_first, sample_count; /* a share of the frame: its sample indices [first, first + count) (count 0: all) */
-    uint32_t gpu_workers;        /* the GPU broker's cellular workers, each a share of a launch (default 32) */
-    uint32_t pad;
+    uint32_t workers;            /* the broker's cellular workers, each a share of a launch (default 32) */
 } x2_workgrid_options;
 void x2_workgrid_options_defaults(x2_workgrid_options* options);
-/* A grid for a width x height frame of spp samples. owners: one word a cell (1: the GPU's), used in X2_WORKGRID_BOTH when
- * owner_count equals the cell count (else the checkerboard, the GPU on even cells). empty: no chunks made (cells filled
- * by x2_workgrid_append). viewport: min x, min y, max x, max y (half open; null: the image). */
-int x2_workgrid_create(uint32_t width, uint32_t height, uint32_t spp, const x2_workgrid_options* options, const uint32_t* owners,
-                   uint32_t owner_count, uint32_t empty, const int32_t* viewport, x2_workgrid** out);
+/* A grid for a width x height frame of spp samples. empty: no chunks made (cells filled by x2_workgrid_append).
+ * viewport: min x, min y, max x, max y (half open; null: the image). */
+int x2_workgrid_create(uint32_t width, uint32_t height, uint32_t spp, const x2_workgrid_options* options, uint32_t empty,
+                       const int32_t* viewport, x2_workgrid** out);
 void x2_workgrid_free(x2_workgrid* grid);
 int x2_workgrid_info(const x2_workgrid* grid, uint32_t* width, uint32_t* height, uint32_t* spp, x2_workgrid_options* options);
 uint32_t x2_workgrid_cells(const x2_workgrid* grid);
 uint64_t x2_workgrid_total(const x2_workgrid* grid);  /* chunks published */
 /* The frame's sample ranges: (first, count) pairs, up to capacity of them written; returns how many there are. */
 uint32_t x2_workgrid_ranges(const x2_workgrid* grid, uint32_t* ranges, uint32_t capacity);
-int x2_workgrid_cell(const x2_workgrid* grid, uint32_t cell, uint32_t* owner, uint32_t* tiles, uint32_t* published, uint32_t* taken);
+int x2_workgrid_cell(const x2_workgrid* grid, uint32_t cell, uint32_t* tiles, uint32_t* published, uint32_t* taken);
 int x2_workgrid_append(x2_workgrid* grid, uint32_t cell, const x2_chunk* chunks, uint32_t n);
-/* Up to n chunks of a cell for a device, none past what its frontier allows; returns how many (0 once closed). */
-uint32_t x2_workgrid_claim(x2_workgrid* grid, uint32_t cell, uint32_t n, x2_chunk* out, uint32_t device);
-uint32_t x2_workgrid_claimable(const x2_workgrid* grid, uint32_t cell, uint32_t device);
+/* Up to n chunks of a cell, none past what the frontier allows; returns how many (0 once closed). */
+uint32_t x2_workgrid_claim(x2_workgrid* grid, uint32_t cell, uint32_t n, x2_chunk* out);
+uint32_t x2_workgrid_claimable(const x2_workgrid* grid, uint32_t cell);
 uint32_t x2_workgrid_remaining(const x2_workgrid* grid, uint32_t cell);
 uint32_t x2_workgrid_empty(const x2_workgrid* grid);
-uint32_t x2_workgrid_frontier(const x2_workgrid* grid, uint32_t device);
-/* The cellular rules: the cell a worker of a device in cell `current` (~0u: none) works next, ~0u when it may take
- * nothing now (Grid::choose); the starting cell of worker w of n (Grid::seed). */
-uint32_t x2_workgrid_choose(const x2_workgrid* grid, uint32_t device, uint32_t current, uint32_t salt);
-uint32_t x2_workgrid_seed(const x2_workgrid* grid, uint32_t device, uint32_t worker, uint32_t workers);
+uint32_t x2_workgrid_frontier(const x2_workgrid* grid);
+/* The cellular rules: the cell a worker in cell `current` (~0u: none) works next, ~0u when it may take nothing now
+ * (Grid::choose); the starting cell of worker w of n (Grid::seed). */
+uint32_t x2_workgrid_choose(const x2_workgrid* grid, uint32_t current, uint32_t salt);
+uint32_t x2_workgrid_seed(const x2_workgrid* grid, uint32_t worker, uint32_t workers);
 /* Important parts first: each cell's score (below zero: not known yet); cells above the mean are important. */
 int x2_workgrid_set_scores(x2_workgrid* grid, const float* scores, uint32_t n);
-int x2_workgrid_set_suitability(x2_workgrid* grid, const float* gpu_probability, uint32_t n);
-/* The rights of passage's measurements: the GPU's chunk items a second, one CPU worker's samples a second, the CPU's
- * workers, a GPU launch's target seconds. */
-int x2_workgrid_set_rates(x2_workgrid* grid, double gpu_items, double cpu_worker, uint32_t cpu_workers, double window);
-int x2_workgrid_rendered(x2_workgrid* grid, uint32_t cell, uint32_t device, uint64_t samples);
 void x2_workgrid_close(x2_workgrid* grid);  /* a drain: nothing is handed out any more */
 /* Important parts first (async_render.h:1581-1611 cellScores, from the preview picture of async_cpu.h:1359-1379):
  * each cell's score from the scene's film so far, the mean over its sampled pixels of their tones' differences from
@@ -377,22 +368,9 @@ void x2_workgrid_close(x2_workgrid* grid);  /* a drain: nothing is handed out an
  * -1 for a cell without samples; computed on the device, then set on the grid (x2_workgrid_set_scores). scores: each
  * cell's score (host array, may be null). The grid's size must be the film's. Waits. */
 int x2_workgrid_score_film(x2_scene* scene, x2_workgrid* grid, float* scores);
-/* The GPU broker: its next launch's chunks, up to want, taken by its cellular workers (options.gpu_workers, seeded at
- * the first call), a share each, from their cells by the cellular rules. Returns how many. One broker thread a grid. */
+/* The broker: its next launch's chunks, up to want, taken by its cellular workers (options.workers, seeded at the
+ * first call), a share each, from their cells by the cellular rules. Returns how many. One broker thread a grid. */
 uint32_t x2_workgrid_take(x2_workgrid* grid, uint32_t want, x2_chunk* out);
-uint64_t x2_workgrid_stolen(const x2_workgrid* grid);  /* chunks the broker took from cells the CPU owns */
-/* Cell ownership across frames (Ownership, async_grid.h:432-480): x2_workgrid_ownership_finished records a finished
- * frame's grid (each cell's samples by device, x2_workgrid_rendered) and decides the flips for the next frame: a cell
- * whose other device rendered more than 0.6 of its samples over the last 8 frames changes owner, at most
- * min(8, max(1, cells / 10)) a frame, the furthest ahead first, none within 16 frames of its last flip, and a flip back
- * within 32 frames freezes ownership for 64 frames. x2_workgrid_ownership_owners gives the owners for a new grid of
- * `cells` cells (one word a cell, 1: the GPU's; pass them to x2_workgrid_create) and returns 1, or 0 when it has none
- * for that size (the checkerboard then). */
-typedef struct x2_workgrid_ownership x2_workgrid_ownership;
-int x2_workgrid_ownership_create(x2_workgrid_ownership** out);
-void x2_workgrid_ownership_free(x2_workgrid_ownership* ownership);
-int x2_workgrid_ownership_finished(x2_workgrid_ownership* ownership, const x2_workgrid* grid);
-uint32_t x2_workgrid_ownership_owners(const x2_workgrid_ownership* ownership, uint32_t cells, uint32_t* owners);
 typedef struct x2_workgrid_result {
     uint64_t launches, chunks, samples;  /* wavefront launches made, chunks and samples rendered */
     float milliseconds;                  /* host time of the whole frame */
@@ -435,8 +413,12 @@ int x2_wavefront_queues(x2_scene* scene, uint32_t* sizes, uint32_t max);
  * loading the library holds until exit; the caller passes the chunks (device memory) and the film it adds to
  * (device: 4 doubles and one count a pixel; zero them first). Limits: at most 2^20 work items a call
  * (count x 64 x samples_per_chunk), light_count x light_samples <= 32, bsdf_samples = 1; beyond them X2_EINVAL.
- * The first call on a device looks up the array's address: make it before any stream capture. Calls share the
- * array: calls that overlap on the GPU race. Waits for the launch; *samples_done (or null) gets the samples rendered. */
+ * Each chunk's count should be at most samples_per_chunk; a larger count renders samples_per_chunk samples of its
+ * pixels (the chunks are in device memory and are not read on the host). Every call looks up the array's address
+ * with the scene's device current, and the first call on a device loads the library's module there: make that first
+ * call before any stream capture. Calls share the array: calls that overlap on the GPU race. Waits for the launch,
+ * error returns included; after X2_ETIMEOUT wait for the scene's stream before the next call. *samples_done (or
+ * null) gets the samples rendered. */
 int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chunks, uint32_t count, uint32_t samples_per_chunk,
                                double* d_sums, uint32_t* d_counts, uint64_t* samples_done);
 int x2_film_download(x2_scene* scene, double* sums, double* odd, uint32_t* counts);  /* downloadFilm(); waits */

@@ -16,6 +16,9 @@
 #include "async_grid.h"
 
 #include "../include/x2.h"
+#ifdef X2REF_REPLAY
+#include "replay.h"
+#endif
 
 #include <algorithm>
 #include <atomic>
@@ -295,6 +298,9 @@ struct OracleBackend {
         xi::resume::Hit out;
         float t;
         const U32 tri = closest(s, ray.origin, ray.direction, ray.nearT, ray.farT, t);
+#ifdef X2REF_REPLAY
+        replay::event(1, tri, tri == ~0u ? 0.0f : t, ray.direction.x, ray.direction.y, ray.direction.z);
+#endif
         if (tri == ~0u) return out;
         out.geom = s.triGeom[tri];
         out.prim = tri - s.meshFirst[out.geom];
@@ -305,7 +311,13 @@ struct OracleBackend {
     }
     bool visible(V3 o, V3 d) const { return visible(o, d, INFINITY); }
     bool visible(V3 o, V3 d, float distance) const { return visible(o, d, 0.0f, distance); }
-    bool visible(V3 o, V3 d, float near, float distance) const { return !occluded(s, o, d, near, distance); }
+    bool visible(V3 o, V3 d, float near, float distance) const {
+        const bool v = !occluded(s, o, d, near, distance);
+#ifdef X2REF_REPLAY
+        replay::event(2, v ? 1u : 0u, distance, d.x, d.y, d.z);
+#endif
+        return v;
+    }
     void countRay(U32 kind) const {
         if (kind == xi::async::paths::RayCountNee) ++counts->nee;
         else if (kind == xi::async::paths::RayCountBsdf) ++counts->bsdf;
@@ -743,6 +755,39 @@ int x2ref_integrate(void* p, const uint32_t* pairs, uint64_t n, double* rgba, ui
     return X2_OK;
 }
 
+#ifdef X2REF_REPLAY
+// One sample through the reference integrator on this thread, replaying the given transcendental values (the
+// device's records, x2_diag.h; null or n = 0: libm's own), with the calls it made and the backend's events logged.
+// Returns the number of table misses in *misses; the logs are truncated to their capacities (the full counts in
+// *ncalls and *nevents).
+int x2ref_replay(void* p, uint32_t pixel, uint32_t index, const x2_diag_call* table, uint32_t n, double* rgba, uint32_t* status,
+                 x2_diag_call* calls, uint32_t callCap, uint32_t* ncalls, void* events, uint32_t eventCap, uint32_t* nevents,
+                 uint64_t* misses) {
+    auto* h = static_cast<Handle*>(p);
+    if (!h) return X2_EINVAL;
+    replay::State st;
+    st.useTable = table && n;
+    for (uint32_t i = 0; i < n; ++i) st.table[replay::key(table[i].fn, table[i].a, table[i].b)] = {table[i].r0, table[i].r1};
+    Counts c;
+    OracleBackend backend{h->scene, &c};
+    xi::async::Radiance r;
+    replay::t_state = &st;
+    const auto code = xi::async::integratePaths(h->scene.config, pixel, index, backend, r);
+    replay::t_state = nullptr;
+    rgba[0] = r.rgb[0];
+    rgba[1] = r.rgb[1];
+    rgba[2] = r.rgb[2];
+    rgba[3] = r.alpha;
+    *status = U32(code);
+    *ncalls = uint32_t(st.calls.size());
+    *nevents = uint32_t(st.events.size());
+    std::memcpy(calls, st.calls.data(), sizeof(x2_diag_call) * std::min<size_t>(callCap, st.calls.size()));
+    std::memcpy(events, st.events.data(), sizeof(replay::Event) * std::min<size_t>(eventCap, st.events.size()));
+    *misses = st.misses;
+    return X2_OK;
+}
+#endif
+
 // renderChunk (async_cpu.h:1584-1667): workers claim 8x8 tiles and render their samples [first, first+count)
 // into an FP64 film: sums (4 a pixel), odd-index sums and counts. Ray counts in rays[4] (trace, nee, bsdf, held).
 int x2ref_render(void* p, uint32_t first, uint32_t count, int threads, double* sums, double* odd, uint32_t* counts, uint64_t* rays) {
@@ -1124,7 +1169,6 @@ uint32_t x2ref_grid_ranges(void* g, uint32_t* out, uint32_t capacity) {
     }
     return uint32_t(r.size());
 }
-uint32_t x2ref_grid_owner(void* g, uint32_t cell) { return uint32_t(static_cast<xi::async::Grid*>(g)->owner(cell)); }
 uint32_t x2ref_grid_claim(void* g, uint32_t cell, uint32_t n, x2_chunk* out, uint32_t device) {
     static_assert(sizeof(xi::async::Chunk) == sizeof(x2_chunk), "chunk layouts");
     return static_cast<xi::async::Grid*>(g)->claim(cell, n, reinterpret_cast<xi::async::Chunk*>(out), xi::async::Device(device));
@@ -1144,28 +1188,10 @@ uint32_t x2ref_grid_seed(void* g, uint32_t device, uint32_t worker, uint32_t wor
 void x2ref_grid_set_scores(void* g, const float* scores, uint32_t n) {
     static_cast<xi::async::Grid*>(g)->setScores(std::vector<float>(scores, scores + n));
 }
-void x2ref_grid_set_suitability(void* g, const float* p, uint32_t n) {
-    static_cast<xi::async::Grid*>(g)->setSuitability(std::vector<float>(p, p + n));
-}
-void x2ref_grid_set_rates(void* g, double gpuItems, double cpuWorker, uint32_t cpuWorkers, double window) {
-    static_cast<xi::async::Grid*>(g)->setRates(gpuItems, cpuWorker, cpuWorkers, window);
-}
 void x2ref_grid_append(void* g, uint32_t cell, const x2_chunk* chunks, uint32_t n) {
     static_cast<xi::async::Grid*>(g)->append(cell, reinterpret_cast<const xi::async::Chunk*>(chunks), n);
 }
 void x2ref_grid_close(void* g) { static_cast<xi::async::Grid*>(g)->close(); }
-void x2ref_grid_rendered(void* g, uint32_t cell, uint32_t device, uint64_t samples) {
-    static_cast<xi::async::Grid*>(g)->rendered(cell, xi::async::Device(device), samples);
-}
-void* x2ref_ownership_open() { return new xi::async::Ownership(); }
-void x2ref_ownership_free(void* o) { delete static_cast<xi::async::Ownership*>(o); }
-void x2ref_ownership_finished(void* o, void* g) { static_cast<xi::async::Ownership*>(o)->finished(*static_cast<xi::async::Grid*>(g)); }
-uint32_t x2ref_ownership_owners(void* o, uint32_t cells, uint32_t* out) {
-    const auto* v = static_cast<xi::async::Ownership*>(o)->owners(cells);
-    if (!v) return 0;
-    for (uint32_t i = 0; i < cells; ++i) out[i] = (*v)[i] == xi::async::Device::Gpu ? 1u : 0u;
-    return 1;
-}
 
 // paths::childBranch (async_integrator.h:281-287), the reference's own.
 uint64_t x2ref_child_branch(uint64_t parent, uint32_t a, uint32_t b) { return xi::async::paths::childBranch(parent, a, b); }

@@ -13,6 +13,7 @@ import x2  # noqa: E402
 
 SAMPLER = os.path.join(ROOT, "oracle", "liboracle_sampler.so")
 REFERENCE = os.path.join(ROOT, "oracle", "_ref", "libx2ref.so")
+REPLAY = os.path.join(ROOT, "oracle", "_ref", "libx2ref_replay.so")  # oracle/replay.h
 
 
 def sampler():
@@ -41,15 +42,38 @@ def sampling_words(lib, ids, dims, policy):
     return out
 
 
+# x2_diag_call (include/x2_diag.h) and the replay build's backend event (oracle/replay.h).
+CALL_DTYPE = np.dtype([("fn", np.uint32), ("a", np.float32), ("b", np.float32), ("r0", np.float32), ("r1", np.float32)])
+EVENT_DTYPE = np.dtype([("kind", np.uint32), ("value", np.uint32), ("t", np.float32), ("x", np.float32), ("y", np.float32),
+                        ("z", np.float32)])
+
+
 def have_reference():
     return os.path.exists(REFERENCE)
+
+
+_generator = None
+
+
+def generator():
+    """The reference build's copy of the seeded scene generator (x2_scene_generate, compiled into libx2ref.so), for
+    processes that must not load libx2 (the timed reference arm)."""
+    global _generator
+    if _generator is None:
+        lib = C.CDLL(REFERENCE)
+        lib.x2_scene_generate.argtypes = [C.c_uint32, C.c_uint64, C.POINTER(C.POINTER(x2.SceneDesc)), C.POINTER(x2.Config)]
+        lib.x2_scene_generate.restype = C.c_int
+        lib.x2_scene_desc_free.argtypes = [C.POINTER(x2.SceneDesc)]
+        lib.x2_scene_desc_free.restype = None
+        _generator = lib
+    return _generator
 
 
 class Reference:
     """The reference's integratePaths (async_integrator.h:1986) over a scene, on host threads."""
 
-    def __init__(self, synthetic, config=None):
-        self.lib = lib = C.CDLL(REFERENCE)
+    def __init__(self, synthetic, config=None, path=REFERENCE):
+        self.lib = lib = C.CDLL(path)
         vp, u32, u64, i32 = C.c_void_p, C.c_uint32, C.c_uint64, C.c_int
         lib.x2ref_open.argtypes = [C.POINTER(x2.SceneDesc), C.POINTER(x2.Config)]
         lib.x2ref_open.restype = vp
@@ -124,6 +148,25 @@ class Reference:
         f.restype = C.c_int
         rc = f(self.h, tiles.ctypes.data, len(tiles), first, count, threads or os.cpu_count(), sums.ctypes.data, counts.ctypes.data)
         return rc, sums, counts
+
+    def replay(self, pixel, index, table=None):
+        """One sample through the replay build (Reference(..., path=REPLAY); oracle/replay.h) with the given
+        transcendental values (records as x2_diag_call, or None: libm's own). Returns (rgba, status, calls made, backend
+        events, table misses)."""
+        cap = 1 << 16
+        calls = np.zeros(cap, CALL_DTYPE)
+        events = np.zeros(cap, EVENT_DTYPE)
+        rgba = np.zeros(4)
+        status, nc, ne, misses = C.c_uint32(), C.c_uint32(), C.c_uint32(), C.c_uint64()
+        table = np.ascontiguousarray(table if table is not None else np.zeros(0, CALL_DTYPE), CALL_DTYPE)
+        f = self.lib.x2ref_replay
+        f.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p, C.c_void_p, C.c_uint32,
+                      C.c_void_p, C.c_void_p, C.c_uint32, C.c_void_p, C.c_void_p]
+        f.restype = C.c_int
+        rc = f(self.h, int(pixel), int(index), table.ctypes.data, len(table), rgba.ctypes.data, C.byref(status), calls.ctypes.data, cap,
+               C.byref(nc), events.ctypes.data, cap, C.byref(ne), C.byref(misses))
+        assert rc == 0
+        return rgba, status.value, calls[: min(cap, nc.value)], events[: min(cap, ne.value)], misses.value
 
     def trace(self, rays, brute=False):
         """Closest hit (triangle, t) and occlusion through the oracle's BVH, or by testing every triangle."""
@@ -293,33 +336,34 @@ def reference_adaptive_masks(width, height, target, errors):
 
 
 class RefWorkGrid:
-    """The reference's own work grid (async_grid.h Grid, compiled from source into oracle/_ref), call by call, with the
-    same methods as x2.WorkGrid."""
+    """The reference's own work grid (async_grid.h Grid, compiled from source into oracle/_ref) as the GPU lane uses it
+    (GridOptions::mode 1: every cell the GPU's; every claim and choice the GPU's), call by call, with the same methods
+    as x2.WorkGrid."""
 
-    def __init__(self, width, height, spp, options, owners=None, empty=False, viewport=None):
+    GPU = 1  # Device::Gpu, and GridOptions::mode for a GPU-only grid
+
+    def __init__(self, width, height, spp, options, empty=False, viewport=None):
         lib = self.lib = C.CDLL(REFERENCE)
         vp, u32, u64 = C.c_void_p, C.c_uint32, C.c_uint64
         sig = {
             "x2ref_grid_open": ([u32, u32, u32, u32, u32, C.c_int, C.c_int, u32, u32, vp, u32, C.c_int, vp], vp),
             "x2ref_grid_free": ([vp], None), "x2ref_grid_cells": ([vp], u32), "x2ref_grid_total": ([vp], u64),
-            "x2ref_grid_ranges": ([vp, vp, u32], u32), "x2ref_grid_owner": ([vp, u32], u32),
+            "x2ref_grid_ranges": ([vp, vp, u32], u32),
             "x2ref_grid_claim": ([vp, u32, u32, vp, u32], u32), "x2ref_grid_claimable": ([vp, u32, u32], u32),
             "x2ref_grid_remaining": ([vp, u32], u32), "x2ref_grid_empty": ([vp], u32), "x2ref_grid_frontier": ([vp, u32], u32),
             "x2ref_grid_choose": ([vp, u32, u32, u32], u32), "x2ref_grid_seed": ([vp, u32, u32, u32], u32),
-            "x2ref_grid_set_scores": ([vp, vp, u32], None), "x2ref_grid_set_suitability": ([vp, vp, u32], None),
-            "x2ref_grid_set_rates": ([vp, C.c_double, C.c_double, u32, C.c_double], None),
-            "x2ref_grid_append": ([vp, u32, vp, u32], None), "x2ref_grid_close": ([vp], None),
+            "x2ref_grid_set_scores": ([vp, vp, u32], None), "x2ref_grid_append": ([vp, u32, vp, u32], None),
+            "x2ref_grid_close": ([vp], None),
         }
         for name, (args, res) in sig.items():
             f = getattr(lib, name)
             f.argtypes = args
             f.restype = res
-        own = None if owners is None else np.ascontiguousarray(owners, np.uint32)
         view = None if viewport is None else np.ascontiguousarray(viewport, np.int32)
-        self._own, self._view = own, view
-        self._h = lib.x2ref_grid_open(width, height, spp, options.cell_size, options.samples_per_chunk, options.mode, options.progressive,
-                                      options.sample_first, options.sample_count, None if own is None else own.ctypes.data,
-                                      0 if own is None else len(own), int(bool(empty)), None if view is None else view.ctypes.data)
+        self._view = view
+        self._h = lib.x2ref_grid_open(width, height, spp, options.cell_size, options.samples_per_chunk, self.GPU, options.progressive,
+                                      options.sample_first, options.sample_count, None, 0, int(bool(empty)),
+                                      None if view is None else view.ctypes.data)
         assert self._h, "the reference grid refused its arguments"
 
     def free(self):
@@ -346,16 +390,13 @@ class RefWorkGrid:
         n = self.lib.x2ref_grid_ranges(self._h, out.ctypes.data, 4096)
         return [(int(out[2 * k]), int(out[2 * k + 1])) for k in range(n)]
 
-    def owner(self, cell):
-        return self.lib.x2ref_grid_owner(self._h, cell)
-
-    def claim(self, cell, n, device):
+    def claim(self, cell, n):
         out = np.zeros(max(n, 1), x2.CHUNK_DTYPE)
-        got = self.lib.x2ref_grid_claim(self._h, cell, n, out.ctypes.data, device)
+        got = self.lib.x2ref_grid_claim(self._h, cell, n, out.ctypes.data, self.GPU)
         return out[:got]
 
-    def claimable(self, cell, device):
-        return self.lib.x2ref_grid_claimable(self._h, cell, device)
+    def claimable(self, cell):
+        return self.lib.x2ref_grid_claimable(self._h, cell, self.GPU)
 
     def remaining(self, cell):
         return self.lib.x2ref_grid_remaining(self._h, cell)
@@ -363,25 +404,18 @@ class RefWorkGrid:
     def empty(self):
         return bool(self.lib.x2ref_grid_empty(self._h))
 
-    def frontier(self, device):
-        return self.lib.x2ref_grid_frontier(self._h, device)
+    def frontier(self):
+        return self.lib.x2ref_grid_frontier(self._h, self.GPU)
 
-    def choose(self, device, current, salt):
-        return self.lib.x2ref_grid_choose(self._h, device, current, salt)
+    def choose(self, current, salt):
+        return self.lib.x2ref_grid_choose(self._h, self.GPU, current, salt)
 
-    def seed(self, device, worker, workers):
-        return self.lib.x2ref_grid_seed(self._h, device, worker, workers)
+    def seed(self, worker, workers):
+        return self.lib.x2ref_grid_seed(self._h, self.GPU, worker, workers)
 
     def set_scores(self, scores):
         scores = np.ascontiguousarray(scores, np.float32)
         self.lib.x2ref_grid_set_scores(self._h, scores.ctypes.data, len(scores))
-
-    def set_suitability(self, p):
-        p = np.ascontiguousarray(p, np.float32)
-        self.lib.x2ref_grid_set_suitability(self._h, p.ctypes.data, len(p))
-
-    def set_rates(self, gpu_items, cpu_worker, cpu_workers, window):
-        self.lib.x2ref_grid_set_rates(self._h, gpu_items, cpu_worker, cpu_workers, window)
 
     def append(self, cell, chunks):
         chunks = np.ascontiguousarray(chunks, dtype=x2.CHUNK_DTYPE)
@@ -389,11 +423,6 @@ class RefWorkGrid:
 
     def close(self):
         self.lib.x2ref_grid_close(self._h)
-
-    def rendered(self, cell, device, samples):
-        f = self.lib.x2ref_grid_rendered
-        f.argtypes = [C.c_void_p, C.c_uint32, C.c_uint32, C.c_uint64]
-        f(self._h, cell, device, samples)
 
     def take(self, want, cells):
         """The reference feeder's claims for one GPU launch (async_render.h:784-797), restated over this grid: `cells`
@@ -405,40 +434,15 @@ class RefWorkGrid:
                 break
             need, moves = min(share, want - got), 0
             while need and moves < 8:
-                cell = self.choose(x2.DEVICE_GPU, cells[w], w)
+                cell = self.choose(cells[w], w)
                 if cell == 0xFFFFFFFF:
                     break
                 cells[w] = cell
-                c = self.claim(cell, need, x2.DEVICE_GPU)
+                c = self.claim(cell, need)
                 out.append(c)
                 got += len(c)
                 need -= len(c)
                 moves += 1
         return np.concatenate(out) if out else np.zeros(0, x2.CHUNK_DTYPE)
 
-
-class RefOwnership:
-    """The reference's cell ownership across frames (async_grid.h Ownership)."""
-
-    def __init__(self):
-        lib = self.lib = C.CDLL(REFERENCE)
-        lib.x2ref_ownership_open.restype = C.c_void_p
-        lib.x2ref_ownership_free.argtypes = [C.c_void_p]
-        lib.x2ref_ownership_finished.argtypes = [C.c_void_p, C.c_void_p]
-        lib.x2ref_ownership_owners.argtypes = [C.c_void_p, C.c_uint32, C.c_void_p]
-        lib.x2ref_ownership_owners.restype = C.c_uint32
-        self._h = lib.x2ref_ownership_open()
-
-    def finished(self, grid):
-        self.lib.x2ref_ownership_finished(self._h, grid._h)
-
-    def owners(self, cells):
-        out = np.zeros(max(cells, 1), np.uint32)
-        return out[:cells] if self.lib.x2ref_ownership_owners(self._h, cells, out.ctypes.data) else None
-
-    def __del__(self):
-        try:
-            self.lib.x2ref_ownership_free(self._h)
-        except Exception:
-            pass
 

@@ -27,7 +27,7 @@ def test_progressive_frame_equals_uniform_frame(box, per_launch):
     s, scene = box
     cfg = s.config
     spp = 24
-    grid = x2.WorkGrid(cfg.width, cfg.height, spp, x2.workgrid_options(mode=x2.WORKGRID_GPU, samples_per_chunk=4))
+    grid = x2.WorkGrid(cfg.width, cfg.height, spp, x2.workgrid_options(samples_per_chunk=4))
     r = scene.render_workgrid(grid, per_launch)
     sums, counts = scene.film()
     print(per_launch, r)
@@ -45,7 +45,7 @@ def test_progressive_frame_equals_uniform_frame(box, per_launch):
 def test_share_of_a_frame(box):
     s, scene = box
     cfg = s.config
-    grid = x2.WorkGrid(cfg.width, cfg.height, 64, x2.workgrid_options(mode=x2.WORKGRID_GPU, sample_first=8, sample_count=8))
+    grid = x2.WorkGrid(cfg.width, cfg.height, 64, x2.workgrid_options(sample_first=8, sample_count=8))
     r = scene.render_workgrid(grid, 4096)
     sums, counts = scene.film()
     assert (counts == 8).all() and r["samples"] == cfg.width * cfg.height * 8

@@ -150,6 +150,20 @@ def test_library_exports_every_declared_symbol():
     assert lib.x2_version().startswith(b"x2-b200")
 
 
+def test_diagnostic_library_exports_its_switches():
+    """libx2diag.so (the diagnostic build) loads and exports every function include/x2.h and include/x2_diag.h
+    declare; the product library exports none of x2_diag.h's."""
+    import ctypes
+
+    names = set()
+    for h in ("x2.h", "x2_diag.h"):
+        names |= set(re.findall(r"\b(x2_[a-z0-9_]+)\s*\(", open(os.path.join(oracle_lib.ROOT, "include", h)).read()))
+    diag = ctypes.CDLL(x2.DIAG_LIBRARY)
+    for n in sorted(names):
+        assert hasattr(diag, n), n
+    assert not hasattr(x2.library(), "x2_diag_set")
+
+
 @pytest.fixture(scope="module")
 def adjoint_scene():
     if not oracle_lib.have_reference():

@@ -10,6 +10,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT = os.path.join(HERE, "x2", "libx2.so")
+# The diagnostic build (parity investigation only, never the product): render.cu compiled with -DX2_DIAG (mathfn.cuh:
+# transcendental functions in double on request, and a record of every call), linked with the product's other objects.
+DIAG_OUT = os.path.join(HERE, "x2", "libx2diag.so")
 BUILD = os.path.join(HERE, "_build")
 CU = ["api.cu", "render.cu", "wavefront.cu", "bvh_build.cu", "noalloc.cu", "adjoint.cu", "adaptive.cu", "scores.cu"]
 CPP = ["scene_gen.cpp", "grid.cpp"]
@@ -55,6 +58,13 @@ def build(verbose=False, force=False):
         objs.append(obj)
     if force or _stale(OUT, objs):
         _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", OUT] + objs + ["-lcudart_static"])
+    diag = os.path.join(BUILD, "render_diag.cu.o")
+    src = os.path.join(CSRC, "render.cu")
+    if force or _stale(diag, [src] + headers + [os.path.join(HERE, "..", "include", "x2_diag.h")]):
+        _run([NVCC] + ARCH + FLAGS + ["-DX2_DIAG", "-rdc=false", "-c", src, "-o", diag])
+    diag_objs = [diag if o.endswith(os.sep + "render.cu.o") else o for o in objs]
+    if force or _stale(DIAG_OUT, diag_objs):
+        _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", DIAG_OUT] + diag_objs + ["-lcudart_static"])
     return OUT
 
 

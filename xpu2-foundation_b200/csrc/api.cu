@@ -2159,7 +2159,6 @@ int x2_render_workgrid(x2_scene* s, x2_workgrid* g, uint32_t want, x2_workgrid_r
             const uint32_t x = (c.tile % tilesX) * 8, y = (c.tile / tilesX) * 8;
             const uint64_t pixels = uint64_t(std::min(8u, width - x)) * std::min(8u, height - y);
             samples += pixels * c.count;
-            x2_workgrid_rendered(g, c.cell, X2_DEVICE_GPU, pixels * c.count);
         }
         s->samplesPerChunk = most;
         rc = x2_launch_wavefront(s, chunks.data(), got);

@@ -11,10 +11,14 @@
 // at most kMaxRecords - 1 light samples a vertex (light_count x light_samples), one BSDF sample (bsdf_samples = 1),
 // kPaths paths in flight.
 //
-// Set-up: the first call on a device looks up the array's device address (cudaGetSymbolAddress, with that device
-// current) and keeps it; make that first call before any stream capture. Every call shares the array and keeps the
-// last call's contents; each call clears what must start at zero. Calls that overlap on the GPU (two host threads,
-// two streams, two contexts on one device) race on the array and must not be made.
+// Set-up: every call looks up the array's device address (cudaGetSymbolAddress, with the scene's device current: a
+// lookup, not an allocation), so a context that was destroyed and created again is never handed a stale address.
+// The first call on a device also loads the library's module there: make that first call before any stream capture.
+// Every call shares the array and keeps the last call's contents; each call clears what must start at zero. Calls
+// that overlap on the GPU (two host threads, two streams, two contexts on one device) race on the array and must not
+// be made. A call returns only once its kernels have finished, error returns included, except X2_ETIMEOUT (the
+// stream still busy after the wait's limit): after that, wait for the scene's stream (x2_synchronize) before the
+// next call.
 #include <cuda_runtime.h>
 
 #include <chrono>
@@ -48,7 +52,6 @@ static_assert(kScratchBytes <= 36ull << 20, "the static scratch stays modest (36
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
 std::mutex g_mutex;
-void* g_address[64] = {};  // the array's device address, by device
 
 int waitStream(cudaStream_t st, int timeoutMs) {
     const auto until = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeoutMs);
@@ -101,21 +104,15 @@ extern "C" int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chu
     if (!count) return X2_OK;
     unsigned char* base = nullptr;
     {
+        // The array's address in the current context of the scene's device (sceneView made it current).
         std::lock_guard<std::mutex> lock(g_mutex);
-        if (device < 0 || device >= 64) {
-            setError("device %d out of range", device);
-            return X2_EINVAL;
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
+        if (e != cudaSuccess || !p) {
+            setError("cudaGetSymbolAddress of the static scratch failed on device %d: %s", device, cudaGetErrorString(e));
+            return X2_ECUDA;
         }
-        if (!g_address[device]) {
-            void* p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_scratch);
-            if (e != cudaSuccess || !p) {
-                setError("cudaGetSymbolAddress of the static scratch failed: %s", cudaGetErrorString(e));
-                return X2_ECUDA;
-            }
-            g_address[device] = p;
-        }
-        base = static_cast<unsigned char*>(g_address[device]);
+        base = static_cast<unsigned char*>(p);
     }
     WaveArgs a;
     a.scene = view;
@@ -164,31 +161,45 @@ extern "C" int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chu
     a.chunkItems = nullptr;
     a.chunkCount = count;
     // What must start at zero; the rest is written before it is read.
-    cudaMemsetAsync(a.w.state, 0, 4ull * kPaths, st);
-    cudaMemsetAsync(a.w.ncount, 0, 4ull * kPaths, st);
-    cudaMemsetAsync(queues, 0, 32, st);
-    cudaMemsetAsync(a.claimed, 0, 8, st);
-    cudaMemsetAsync(a.counters, 0, sizeof(Counters), st);
-    cudaMemsetAsync(a.outStatus, X2_SKIP, items, st);
+    const struct {
+        void* p;
+        int v;
+        size_t n;
+    } clears[] = {{a.w.state, 0, 4ull * kPaths}, {a.w.ncount, 0, 4ull * kPaths}, {queues, 0, 32}, {a.claimed, 0, 8},
+                  {a.counters, 0, sizeof(Counters)}, {a.outStatus, X2_SKIP, size_t(items)}};
+    for (const auto& z : clears) {
+        const cudaError_t e = cudaMemsetAsync(z.p, z.v, z.n, st);
+        if (e != cudaSuccess) {
+            setError("clearing the static scratch failed: %s", cudaGetErrorString(e));
+            waitStream(st, 600000);
+            return X2_ECUDA;
+        }
+    }
     const int gridLogic = int((kPaths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = smCount * int(kDefaultBlocksPerSm);
     const WaveKernels wk = waveKernels(kDefaultTraceBlocks, kDefaultShadeBlocks, view.config.volume_count != 0, view.triUV != nullptr);
     const uint64_t maxIter = items * (uint64_t(c.max_depth) + 2) / kPaths + uint64_t(c.max_depth) + 64;
+    // Iterations go in rounds of kRound between reads of the last one's traced-ray count: once an iteration traces
+    // nothing, no path is live and no item is left, and the iterations after it change nothing.
+    constexpr uint64_t kRound = 4;
     uint32_t last = 1;
-    for (uint64_t it = 0; last; ++it) {
+    for (uint64_t it = 0; last; it += kRound) {
         if (it > maxIter) {
             setError("wavefront did not drain after %llu iterations", (unsigned long long)it);
-            return X2_EDEVICE;
+            return X2_EDEVICE;  // the stream is idle here: the last round was waited for
         }
-        wfResetQueues<<<1, 32, 0, st>>>(a);
-        wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
-        wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
-        wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
-        wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
-        wfResetQueues<<<1, 32, 0, st>>>(a);
+        for (uint64_t k = 0; k < kRound; ++k) {
+            wfResetQueues<<<1, 32, 0, st>>>(a);
+            wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
+            wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
+            wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
+            wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
+            wfResetQueues<<<1, 32, 0, st>>>(a);
+        }
         const cudaError_t e = cudaMemcpyAsync(&last, queues + 1, sizeof(uint32_t), cudaMemcpyDeviceToHost, st);
         if (e != cudaSuccess) {
             setError("launch failed: %s", cudaGetErrorString(e));
+            waitStream(st, 600000);
             return X2_ECUDA;
         }
         if (int rc = waitStream(st, 600000)) return rc;

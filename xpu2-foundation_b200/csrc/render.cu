@@ -219,3 +219,21 @@ __global__ void auditCounts(const uint32_t* __restrict__ counts, const uint32_t*
 }
 
 }  // namespace x2
+
+#ifdef X2_DIAG
+// The diagnostic build's switches for this file's kernels (the per-sample API, x2_integrate): mathfn.cuh's mode bits
+// and the call record buffer, set on the current device.
+extern "C" int x2_diag_set(int mode, void* d_calls, uint32_t capacity) {
+    const uint32_t zero = 0;
+    x2::mf::DiagCall* calls = static_cast<x2::mf::DiagCall*>(d_calls);
+    if (cudaMemcpyToSymbol(x2::mf::g_mode, &mode, sizeof(int)) != cudaSuccess ||
+        cudaMemcpyToSymbol(x2::mf::g_calls, &calls, sizeof(calls)) != cudaSuccess ||
+        cudaMemcpyToSymbol(x2::mf::g_cap, &capacity, sizeof(uint32_t)) != cudaSuccess ||
+        cudaMemcpyToSymbol(x2::mf::g_count, &zero, sizeof(uint32_t)) != cudaSuccess)
+        return X2_ECUDA;
+    return X2_OK;
+}
+extern "C" int x2_diag_count(uint32_t* count) {
+    return cudaMemcpyFromSymbol(count, x2::mf::g_count, sizeof(uint32_t)) == cudaSuccess ? X2_OK : X2_ECUDA;
+}
+#endif

@@ -6,13 +6,14 @@
 // The arithmetic follows the reference operation for operation (same association, same float/double types,
 // the same signed-zero behaviour) so that, built without contraction (-fmad=false) like the reference's CPU lane
 // (-ffp-contract=off), a sample's random numbers are bit-exact and its radiance agrees to rounding of the
-// transcendental functions (sincosf on the device, libm on the host). Each function cites what it follows.
+// transcendental functions (CUDA's on the device, libm on the host; mathfn.cuh). Each function cites what it follows.
 #pragma once
 #include <cfloat>
 #include <cstdint>
 
 #include "../../include/x2.h"
 #include "bvh.cuh"
+#include "mathfn.cuh"
 #include "sampler.cuh"
 #include "traverse.cuh"
 
@@ -454,7 +455,7 @@ __device__ __forceinline__ uint32_t surfaceFlags(const Slice& s, V3 wi) {
 }
 __device__ __forceinline__ V3 localSpherical(float cosTheta, float sinTheta, float phi) {
     float s, c;
-    sincosf(phi, &s, &c);
+    mf::sincos(phi, &s, &c);
     return V3{sinTheta * c, sinTheta * s, cosTheta};
 }
 __device__ __forceinline__ V3 schlick(V3 a, float hDotWi) {
@@ -651,7 +652,7 @@ __device__ __forceinline__ bool lightIntersect(const x2_light& l, V3 p, V3 wi, f
 __device__ __forceinline__ bool canIlluminate(const x2_light& l, V3 p, const V3* n) {
     if (l.type == X2_LIGHT_ENV) return true;
     if (l.type == X2_LIGHT_DISTANT) {
-        const float cullThreshold = -cosf(fminf(acosf(fminf(fmaxf(l.cos_theta_max, -1.0f), 1.0f)) + 0.5f * kPi, kPi));
+        const float cullThreshold = -mf::cos(fminf(mf::acos(fminf(fmaxf(l.cos_theta_max, -1.0f), 1.0f)) + 0.5f * kPi, kPi));
         return !(n && dot(*n, ldir(l)) > cullThreshold);
     }
     const float threshold = kEpsilon - 0.0f;

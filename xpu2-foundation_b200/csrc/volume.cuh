@@ -45,7 +45,7 @@ __device__ __forceinline__ V3 vtimes(V3 a, V3 b) { return V3{a.x * b.x, a.y * b.
 __device__ __forceinline__ V3 vscaled(V3 a, float s) { return V3{a.x * s, a.y * s, a.z * s}; }
 __device__ __forceinline__ V3 vplus(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
 __device__ __forceinline__ V3 cmax0(V3 a) { return V3{fmaxf(a.x, 0.0f), fmaxf(a.y, 0.0f), fmaxf(a.z, 0.0f)}; }
-__device__ __forceinline__ V3 expNeg(V3 a, float s) { return V3{expf(-a.x * s), expf(-a.y * s), expf(-a.z * s)}; }
+__device__ __forceinline__ V3 expNeg(V3 a, float s) { return V3{mf::exp(-a.x * s), mf::exp(-a.y * s), mf::exp(-a.z * s)}; }
 __device__ __forceinline__ float vlum(V3 a) { return 0.299f * a.x + 0.587f * a.y + 0.114f * a.z; }
 __device__ __forceinline__ bool vblack(V3 a) { return a.x == 0.0f && a.y == 0.0f && a.z == 0.0f; }
 __device__ __forceinline__ bool vIsZero(float x) { return fabsf(x) < kVolumeEpsilon; }
@@ -283,12 +283,12 @@ __device__ __forceinline__ float phaseEval(float g, V3 wo, V3 wi) {
     return vIsZero(denom) ? 0.0f : kOneOverFourPi * (1 - g * g) / (denom * sqrtf(denom));
 }
 __device__ __forceinline__ float sampleDistanceExponential(float u, float sigma, float a, float b) {
-    return a - logf(1.0f - u * (1.0f - expf(sigma * (a - b)))) / sigma;
+    return a - mf::log(1.0f - u * (1.0f - mf::exp(sigma * (a - b)))) / sigma;
 }
 __device__ __forceinline__ float pdfDistanceExponential(float t, float sigma, float a, float b) {
-    return sigma / (expf((t - a) * sigma) - expf((t - b) * sigma));
+    return sigma / (mf::exp((t - a) * sigma) - mf::exp((t - b) * sigma));
 }
-__device__ __forceinline__ float sampleEquiAngular(float u, float D, float thetaA, float thetaB) { return D * tanf((1 - u) * thetaA + u * thetaB); }
+__device__ __forceinline__ float sampleEquiAngular(float u, float D, float thetaA, float thetaB) { return D * mf::tan((1 - u) * thetaA + u * thetaB); }
 __device__ __forceinline__ float pdfEquiAngular(float t, float D, float thetaA, float thetaB) { return D / ((thetaB - thetaA) * (D * D + t * t)); }
 
 // A light's equi-angular pivot (volume_core.h:630-662) for the admitted lights: a point on a rect.
@@ -517,7 +517,7 @@ static __device__ __noinline__ V3 volumeTransmittance(const SceneView& s, Stream
         if (!regions) return true;
         if (t1 >= kFarLimit) return false;
         const float fs = minFeatureSize(s, regions);
-        const float tauThreshold = c.volume_transmittance_threshold == 0.0f ? 3.402823466e+38f : -logf(c.volume_transmittance_threshold / vlum(tr));
+        const float tauThreshold = c.volume_transmittance_threshold == 0.0f ? 3.402823466e+38f : -mf::log(c.volume_transmittance_threshold / vlum(tr));
         const float u = st.next();
         const float stepSize = fs * c.inv_volume_shadow_quality * fmaxf(float(depth - 1), 1.0f);
         float t = t0 + stepSize * u;
@@ -607,9 +607,9 @@ static __device__ __noinline__ void volumeMultipleScatter(const SceneView& s, co
         V3 scatterDir = phaseSample(vp.g, V3{-dir.x, -dir.y, -dir.z}, up0, up1);
         for (uint32_t depth = pv.volumeDepth; depth < c.max_volume_depth; ++depth) {
             if (vlum(throughput) < c.volume_transmittance_threshold) break;
-            const float ai = powf(c.volume_attenuation_factor, float(depth)), bi = powf(c.volume_contribution_factor, float(depth)),
-                        ci = powf(c.volume_phase_attenuation_factor, float(depth));
-            const float tFreePath = -logf(1.0f - ms.next()) / sigmaT;
+            const float ai = mf::pow(c.volume_attenuation_factor, float(depth)), bi = mf::pow(c.volume_contribution_factor, float(depth)),
+                        ci = mf::pow(c.volume_phase_attenuation_factor, float(depth));
+            const float tFreePath = -mf::log(1.0f - ms.next()) / sigmaT;
             Crossing y[kMaxCrossings];
             uint32_t here;
             const uint32_t m = volumeIntervals(s, scatterPoint, scatterDir, kVolumeEpsilon, y, here);
@@ -706,8 +706,8 @@ static __device__ __noinline__ V3 volumeRadiance(const SceneView& s, const Ident
                             offset = dot(add(pivot, mul(org, -1.0f)), dir);
                             const V3 foot = add(org, mul(dir, offset));
                             D = length(add(pivot, mul(foot, -1.0f)));
-                            thetaA = atan2f(firstStart - offset, D);
-                            thetaB = atan2f(rayEnd - offset, D);
+                            thetaA = mf::atan2(firstStart - offset, D);
+                            thetaB = mf::atan2(rayEnd - offset, D);
                             const float te = sampleEquiAngular(ue, D, thetaA, thetaB);
                             const float pdfTe = pdfEquiAngular(te, D, thetaA, thetaB);
                             if (pdfTe != 0.0f && vfinite(pdfTe)) {

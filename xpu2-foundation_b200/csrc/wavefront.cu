@@ -689,7 +689,10 @@ __global__ void wfFilmReduce(WaveArgs a, uint32_t chunkCount, double* sums, doub
     uint32_t n = 0;
     const unsigned long long first = (unsigned long long)chunkIndex * 64ull * a.samplesPerChunk + (unsigned long long)position * a.samplesPerChunk;
     const uint32_t indexBase = a.pixelBase ? a.pixelBase[pixel] : chunk.first;
-    for (uint32_t s = 0; s < chunk.count; ++s) {
+    // A chunk holds at most samplesPerChunk items a pixel; a larger count (caller input the device-memory entry points
+    // do not check on the host) is clamped as the logic kernel clamps it, so no read leaves the chunk's items.
+    const uint32_t count = min(chunk.count, a.samplesPerChunk);
+    for (uint32_t s = 0; s < count; ++s) {
         if (a.outStatus[first + s] != X2_DONE) continue;
         const float4 r = a.out[first + s];
         v[0] += double(r.x);
@@ -727,7 +730,8 @@ __global__ void wfFilmReduceBatch(WaveArgs a, const BatchFilm* __restrict__ film
     const unsigned long long first = begin + position * perPixel;
     double v[4] = {0, 0, 0, 0}, o[4] = {0, 0, 0, 0};
     uint32_t n = 0;
-    for (uint32_t s = 0; s < chunk.count; ++s) {
+    const uint32_t count = uint32_t(min((unsigned long long)chunk.count, perPixel));
+    for (uint32_t s = 0; s < count; ++s) {
         if (a.outStatus[first + s] != X2_DONE) continue;
         const float4 r = a.out[first + s];
         v[0] += double(r.x);

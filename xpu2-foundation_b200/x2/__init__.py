@@ -15,7 +15,10 @@ import weakref
 import numpy as np
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIBRARY = os.path.join(_HERE, "libx2.so")
+# X2_LIBRARY may name the diagnostic build (libx2diag.so: the product's kernels plus the x2_diag_* switches of
+# include/x2_diag.h) for a parity investigation; the product is libx2.so.
+LIBRARY = os.environ.get("X2_LIBRARY") or os.path.join(_HERE, "libx2.so")
+DIAG_LIBRARY = os.path.join(_HERE, "libx2diag.so")
 
 OK, EINVAL, ECUDA, ENOMEM, ETIMEOUT, EAUDIT, ENODEV, EDEVICE = range(8)
 DONE, MISS, ERROR, SKIP, DEFER = range(5)
@@ -132,8 +135,8 @@ class AdaptiveResult(C.Structure):
 
 
 class WorkGridOptions(C.Structure):
-    _fields_ = [("cell_size", C.c_uint32), ("samples_per_chunk", C.c_uint32), ("mode", C.c_int32), ("progressive", C.c_uint32),
-                ("sample_first", C.c_uint32), ("sample_count", C.c_uint32), ("gpu_workers", C.c_uint32), ("pad", C.c_uint32)]
+    _fields_ = [("cell_size", C.c_uint32), ("samples_per_chunk", C.c_uint32), ("progressive", C.c_uint32),
+                ("sample_first", C.c_uint32), ("sample_count", C.c_uint32), ("workers", C.c_uint32)]
 
 
 class WorkGridResult(C.Structure):
@@ -187,21 +190,16 @@ def library():
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
         "x2_workgrid_options_defaults": ([C.POINTER(WorkGridOptions)], None),
-        "x2_workgrid_create": ([u32, u32, u32, C.POINTER(WorkGridOptions), vp, u32, u32, vp, C.POINTER(vp)], i32),
+        "x2_workgrid_create": ([u32, u32, u32, C.POINTER(WorkGridOptions), u32, vp, C.POINTER(vp)], i32),
         "x2_workgrid_free": ([vp], None), "x2_workgrid_info": ([vp, vp, vp, vp, C.POINTER(WorkGridOptions)], i32),
         "x2_workgrid_cells": ([vp], u32), "x2_workgrid_total": ([vp], u64), "x2_workgrid_ranges": ([vp, vp, u32], u32),
-        "x2_workgrid_cell": ([vp, u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)], i32),
-        "x2_workgrid_append": ([vp, u32, vp, u32], i32), "x2_workgrid_claim": ([vp, u32, u32, vp, u32], u32),
-        "x2_workgrid_claimable": ([vp, u32, u32], u32), "x2_workgrid_remaining": ([vp, u32], u32), "x2_workgrid_empty": ([vp], u32),
-        "x2_workgrid_frontier": ([vp, u32], u32), "x2_workgrid_choose": ([vp, u32, u32, u32], u32),
-        "x2_workgrid_seed": ([vp, u32, u32, u32], u32), "x2_workgrid_set_scores": ([vp, vp, u32], i32),
-        "x2_workgrid_set_suitability": ([vp, vp, u32], i32),
-        "x2_workgrid_set_rates": ([vp, C.c_double, C.c_double, u32, C.c_double], i32),
-        "x2_workgrid_rendered": ([vp, u32, u32, u64], i32), "x2_workgrid_close": ([vp], None),
-        "x2_workgrid_take": ([vp, u32, vp], u32), "x2_workgrid_stolen": ([vp], u64),
-        "x2_render_workgrid": ([vp, vp, u32, C.POINTER(WorkGridResult)], i32),
-        "x2_workgrid_ownership_create": ([C.POINTER(vp)], i32), "x2_workgrid_ownership_free": ([vp], None),
-        "x2_workgrid_ownership_finished": ([vp, vp], i32), "x2_workgrid_ownership_owners": ([vp, u32, vp], u32), "x2_workgrid_score_film": ([vp, vp, vp], i32),
+        "x2_workgrid_cell": ([vp, u32, C.POINTER(u32), C.POINTER(u32), C.POINTER(u32)], i32),
+        "x2_workgrid_append": ([vp, u32, vp, u32], i32), "x2_workgrid_claim": ([vp, u32, u32, vp], u32),
+        "x2_workgrid_claimable": ([vp, u32], u32), "x2_workgrid_remaining": ([vp, u32], u32), "x2_workgrid_empty": ([vp], u32),
+        "x2_workgrid_frontier": ([vp], u32), "x2_workgrid_choose": ([vp, u32, u32], u32),
+        "x2_workgrid_seed": ([vp, u32, u32], u32), "x2_workgrid_set_scores": ([vp, vp, u32], i32),
+        "x2_workgrid_close": ([vp], None), "x2_workgrid_take": ([vp, u32, vp], u32),
+        "x2_render_workgrid": ([vp, vp, u32, C.POINTER(WorkGridResult)], i32), "x2_workgrid_score_film": ([vp, vp, vp], i32),
     }
     for name, (args, res) in sig.items():
         f = getattr(lib, name)
@@ -290,14 +288,20 @@ class SyntheticScene:
     """A seeded synthetic scene made by the library's host generator (x2_scene_generate): its descriptor (owned
     by the library until freed) and the config that goes with it."""
 
-    def __init__(self, config_id, seed=None):
+    def __init__(self, config_id, seed=None, generator=None):
+        """`generator`: another loaded library exporting x2_scene_generate / x2_scene_desc_free with their
+        signatures declared (the oracle's, which compiles the same generator), in place of libx2."""
         self._desc = C.POINTER(SceneDesc)()
         self.config = Config()
         self.config_id = config_id
+        self._gen = generator
         if seed is None:  # a config's generator seed is its index + 1; batched requests (200+, 300+) are config 2's
             seed = 3 if 200 <= config_id < 400 else (config_id % 100) + 1
         self.seed = seed
-        _check(library().x2_scene_generate(config_id, self.seed, C.byref(self._desc), C.byref(self.config)))
+        lib = generator or library()
+        rc = lib.x2_scene_generate(config_id, self.seed, C.byref(self._desc), C.byref(self.config))
+        if rc != OK:
+            raise X2Error(rc, f"x2_scene_generate({config_id}, {self.seed}) failed")
 
     @property
     def desc(self):
@@ -323,7 +327,7 @@ class SyntheticScene:
 
     def free(self):
         if self._desc:
-            library().x2_scene_desc_free(self._desc)
+            (self._gen or library()).x2_scene_desc_free(self._desc)
             self._desc = C.POINTER(SceneDesc)()
 
     def __del__(self):
@@ -585,10 +589,6 @@ def image(sums, counts, width, height):
     return (sums / c).reshape(height, width, 4)
 
 
-DEVICE_CPU, DEVICE_GPU = 0, 1
-WORKGRID_CPU, WORKGRID_GPU, WORKGRID_BOTH = 0, 1, 2
-
-
 def workgrid_options(**kw):
     """The work grid's options (x2_workgrid_options_defaults), with the given fields changed."""
     o = WorkGridOptions()
@@ -599,15 +599,14 @@ def workgrid_options(**kw):
 
 
 class WorkGrid:
-    """The work grid (x2_workgrid_*): cells of chunk queues, claims, frontiers and the cellular choice; host-side."""
+    """The work grid (x2_workgrid_*): cells handing out their chunks through one cursor each, the frontier, the
+    cellular choice and the broker; host-side."""
 
-    def __init__(self, width, height, spp, options=None, owners=None, empty=False, viewport=None):
+    def __init__(self, width, height, spp, options=None, empty=False, viewport=None):
         self.options = options if options is not None else workgrid_options()
-        own = None if owners is None else np.ascontiguousarray(owners, np.uint32)
         view = None if viewport is None else np.ascontiguousarray(viewport, np.int32)
         h = C.c_void_p()
-        _check(library().x2_workgrid_create(width, height, spp, C.byref(self.options), _ptr(own) if own is not None else None,
-                                            0 if own is None else len(own), int(bool(empty)),
+        _check(library().x2_workgrid_create(width, height, spp, C.byref(self.options), int(bool(empty)),
                                             _ptr(view) if view is not None else None, C.byref(h)))
         self._h = h
 
@@ -637,21 +636,21 @@ class WorkGrid:
         return [(int(out[2 * k]), int(out[2 * k + 1])) for k in range(n)]
 
     def cell(self, i):
-        v = [C.c_uint32() for _ in range(4)]
+        v = [C.c_uint32() for _ in range(3)]
         _check(library().x2_workgrid_cell(self._h, i, *[C.byref(x) for x in v]))
-        return dict(zip(("owner", "tiles", "published", "taken"), (x.value for x in v)))
+        return dict(zip(("tiles", "published", "taken"), (x.value for x in v)))
 
     def append(self, cell, chunks):
         chunks = np.ascontiguousarray(chunks, dtype=CHUNK_DTYPE)
         _check(library().x2_workgrid_append(self._h, cell, _ptr(chunks), len(chunks)))
 
-    def claim(self, cell, n, device):
+    def claim(self, cell, n):
         out = np.zeros(max(n, 1), CHUNK_DTYPE)
-        got = library().x2_workgrid_claim(self._h, cell, n, _ptr(out), device)
+        got = library().x2_workgrid_claim(self._h, cell, n, _ptr(out))
         return out[:got]
 
-    def claimable(self, cell, device):
-        return library().x2_workgrid_claimable(self._h, cell, device)
+    def claimable(self, cell):
+        return library().x2_workgrid_claimable(self._h, cell)
 
     def remaining(self, cell):
         return library().x2_workgrid_remaining(self._h, cell)
@@ -659,64 +658,24 @@ class WorkGrid:
     def empty(self):
         return bool(library().x2_workgrid_empty(self._h))
 
-    def frontier(self, device):
-        return library().x2_workgrid_frontier(self._h, device)
+    def frontier(self):
+        return library().x2_workgrid_frontier(self._h)
 
-    def choose(self, device, current, salt):
-        return library().x2_workgrid_choose(self._h, device, current, salt)
+    def choose(self, current, salt):
+        return library().x2_workgrid_choose(self._h, current, salt)
 
-    def seed(self, device, worker, workers):
-        return library().x2_workgrid_seed(self._h, device, worker, workers)
+    def seed(self, worker, workers):
+        return library().x2_workgrid_seed(self._h, worker, workers)
 
     def set_scores(self, scores):
         scores = np.ascontiguousarray(scores, np.float32)
         _check(library().x2_workgrid_set_scores(self._h, _ptr(scores), len(scores)))
 
-    def set_suitability(self, p):
-        p = np.ascontiguousarray(p, np.float32)
-        _check(library().x2_workgrid_set_suitability(self._h, _ptr(p), len(p)))
-
-    def set_rates(self, gpu_items, cpu_worker, cpu_workers, window):
-        _check(library().x2_workgrid_set_rates(self._h, gpu_items, cpu_worker, cpu_workers, window))
-
     def close(self):
         library().x2_workgrid_close(self._h)
 
     def take(self, want):
-        """The GPU broker's next launch: up to `want` chunks (x2_workgrid_take)."""
+        """The broker's next launch: up to `want` chunks (x2_workgrid_take)."""
         out = np.zeros(max(want, 1), CHUNK_DTYPE)
         got = library().x2_workgrid_take(self._h, want, _ptr(out))
         return out[:got]
-
-    @property
-    def stolen(self):
-        return library().x2_workgrid_stolen(self._h)
-
-    def rendered(self, cell, device, samples):
-        _check(library().x2_workgrid_rendered(self._h, cell, device, samples))
-
-
-class Ownership:
-    """Cell ownership across frames (x2_workgrid_ownership_*): flips towards the device that rendered most of a cell."""
-
-    def __init__(self):
-        h = C.c_void_p()
-        _check(library().x2_workgrid_ownership_create(C.byref(h)))
-        self._h = h
-
-    def __del__(self):
-        try:
-            if self._h:
-                library().x2_workgrid_ownership_free(self._h)
-                self._h = None
-        except Exception:
-            pass
-
-    def finished(self, grid):
-        _check(library().x2_workgrid_ownership_finished(self._h, grid._h))
-
-    def owners(self, cells):
-        """The owners for a new grid of `cells` cells (1: the GPU's), or None for the checkerboard."""
-        out = np.zeros(max(cells, 1), np.uint32)
-        return out[:cells] if library().x2_workgrid_ownership_owners(self._h, cells, _ptr(out)) else None
-
