@@ -15,7 +15,7 @@
 #include "../../include/x2.h"
 #include "engine.h"
 #include "adaptive.h"
-#include "cellular.h"
+#include "generations.h"
 #include "adjoint.h"
 #include "render.h"
 #include "wavefront.h"
@@ -117,21 +117,29 @@ struct x2_ctx {
 struct AdaptiveState {
     uint32_t width = 0, height = 0, tiles = 0, tilesX = 0, regionCount = 0;
     float target = 0;
-    x2::ad::Layout layout;
-    x2::ad::IBox* regions = nullptr;
-    uint32_t* nodeOffset = nullptr;
-    uint32_t* nodeCapacity = nullptr;
+    x2::rg::RegionGrid grid;
+    // Per region (device): boxes (4 ints), table offsets, node bounds, node counts, ready / open flags, and the
+    // first row and column index of each region among all regions' rows and columns.
+    int32_t* boxes = nullptr;
     unsigned long long* satOffset = nullptr;
+    uint32_t *bound = nullptr, *nodes = nullptr, *ready = nullptr, *open = nullptr, *rowStart = nullptr, *colStart = nullptr;
+    uint32_t rows = 0, cols = 0;
     double* sat = nullptr;
-    x2::ad::Node* nodes = nullptr;
-    uint32_t* regionDone = nullptr;
+    // The node pool (structure of arrays) and its words: [0] nodes allocated, [1] [2] the level under decision.
+    uint32_t poolCapacity = 0;
+    float *px0 = nullptr, *py0 = nullptr, *px1 = nullptr, *py1 = nullptr;
+    int32_t* pchild = nullptr;
+    uint8_t* pfate = nullptr;
+    uint32_t *pregion = nullptr, *poolWords = nullptr;
     float* errors = nullptr;
     uint64_t* inImage = nullptr;
+    uint64_t* reach = nullptr;
     uint64_t* tileMask = nullptr;
     uint32_t* planned = nullptr;
     uint32_t* base = nullptr;
     uint32_t* stop = nullptr;
     uint64_t* chunkMasks = nullptr;  // a pass's active tiles' masks, in its chunks' order
+    uint32_t* blockTiles = nullptr;  // the compaction's counts, a block of tiles each
     // A queued frame's words: [0] the pass's active chunks, [1] passes launched, [2] the pass's drain iterations,
     // [3] all passes' drain iterations, [4] a drain that hit its bound, [5] a cellular generation's live tiles; its
     // planned samples; their host copies (pinned).
@@ -139,12 +147,14 @@ struct AdaptiveState {
     unsigned long long* samples = nullptr;
     uint32_t* hostWords = nullptr;
     unsigned long long* hostSamples = nullptr;
-    // Cellular generations: two generations of live tiles (a byte a tile each), the first every tile in the image.
+    // Cellular generations: two generations of live tiles (a byte a tile each), the first every tile in the image, and
+    // each tile's error ratio.
     uint8_t* alive = nullptr;
+    float* ratio = nullptr;
     std::vector<uint8_t> firstAlive;
     ~AdaptiveState() {
-        void* p[] = {regions, nodeOffset, nodeCapacity, satOffset, sat, nodes, regionDone, errors, inImage, tileMask, planned, base, stop, chunkMasks,
-                     words, samples, alive};
+        void* p[] = {boxes, satOffset, bound, nodes, ready, open, rowStart, colStart, sat, px0, py0, px1, py1, pchild, pfate, pregion,
+                     poolWords, errors, inImage, reach, tileMask, planned, base, stop, chunkMasks, blockTiles, words, samples, alive, ratio};
         for (void* q : p) cudaFree(q);
         if (hostWords) cudaFreeHost(hostWords);
         if (hostSamples) cudaFreeHost(hostSamples);
@@ -1698,7 +1708,7 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
 namespace {
 
 // The overlapping regions of a width x height image (the reference's Regions: up to 4 x 4 regions of whole 8-pixel
-// tiles, each widened by an 8-pixel overlap, clamped to the image), their trees' node bounds and table sizes.
+// tiles, each widened by an 8-pixel overlap, clamped to the image), their tables, node bounds and the node pool.
 int ensureAdaptive(x2_scene* s, float target) {
     const uint32_t width = s->config.width, height = s->config.height;
     AdaptiveState* a = s->adaptiveState;
@@ -1713,36 +1723,26 @@ int ensureAdaptive(x2_scene* s, float target) {
     a->target = target;
     a->tilesX = (width + 7) / 8;
     a->tiles = a->tilesX * ((height + 7) / 8);
-    const int tile = 8, overlap = 8, desired = 4, minW = tile + overlap, minH = tile + overlap;
-    auto roundUp = [](int n, int m) { return n % m ? n + m - n % m : n; };
-    const int w = int(width), h = int(height);
-    if (minW >= w || minH >= h) {
-        a->layout.regionW = w;
-        a->layout.regionH = h;
-        a->layout.perDim = 1;
-    } else {
-        a->layout.perDim = std::max(1, std::min(desired, std::min(w / minW, h / minH)));
-        a->layout.regionW = roundUp(1 + (w - 1) / a->layout.perDim, tile);
-        a->layout.regionH = roundUp(1 + (h - 1) / a->layout.perDim, tile);
+    a->grid = x2::rg::regionGrid(int(width), int(height));
+    a->regionCount = uint32_t(a->grid.across * a->grid.across);
+    std::vector<int32_t> boxes(4 * a->regionCount);
+    std::vector<uint32_t> bound(a->regionCount), rowStart(a->regionCount), colStart(a->regionCount);
+    std::vector<unsigned long long> satOffset(a->regionCount);
+    unsigned long long sat = 0, pool = 0;
+    for (uint32_t r = 0; r < a->regionCount; ++r) {
+        int* b = boxes.data() + 4 * r;
+        x2::rg::regionBox(a->grid, int(r), int(width), int(height), b);
+        const int w = b[2] - b[0], h = b[3] - b[1];
+        bound[r] = uint32_t(std::max(1, x2::rg::regionNodeBound(w, h)));
+        satOffset[r] = sat;
+        rowStart[r] = a->rows;
+        colStart[r] = a->cols;
+        a->rows += uint32_t(h);
+        a->cols += uint32_t(w);
+        sat += (unsigned long long)(w + 1) * (unsigned long long)(h + 1);
+        pool += bound[r];
     }
-    const int perDim = a->layout.perDim;
-    std::vector<x2::ad::IBox> boxes;
-    std::vector<uint32_t> nodeOffset, nodeCapacity;
-    std::vector<unsigned long long> satOffset;
-    unsigned long long nodes = 0, sat = 0;
-    for (int i = 0; i < perDim * perDim; ++i) {
-        const int rx = i % perDim, ry = i / perDim;
-        x2::ad::IBox b{rx * a->layout.regionW - overlap, ry * a->layout.regionH - overlap, (rx + 1) * a->layout.regionW + overlap,
-                       (ry + 1) * a->layout.regionH + overlap};
-        b = {std::max(b.x0, 0), std::max(b.y0, 0), std::min(b.x1, w), std::min(b.y1, h)};
-        boxes.push_back(b);
-        nodeOffset.push_back(uint32_t(nodes));
-        nodeCapacity.push_back(uint32_t(std::max(1, x2::ad::nodeBound(b))));
-        satOffset.push_back(sat);
-        nodes += nodeCapacity.back();
-        sat += (unsigned long long)(b.x1 - b.x0 + 1) * (unsigned long long)(b.y1 - b.y0 + 1);
-    }
-    a->regionCount = uint32_t(boxes.size());
+    a->poolCapacity = uint32_t(std::min<unsigned long long>(pool, 0x7fffffffull));
     std::vector<uint64_t> inImage(a->tiles);
     a->firstAlive.assign(a->tiles, 0);
     for (uint32_t t = 0; t < a->tiles; ++t) {
@@ -1753,22 +1753,31 @@ int ensureAdaptive(x2_scene* s, float target) {
         inImage[t] = m;
         a->firstAlive[t] = m ? 1 : 0;
     }
-    const size_t pixels = size_t(width) * height;
-    const bool ok = cudaMalloc(&a->regions, sizeof(x2::ad::IBox) * boxes.size()) == cudaSuccess &&
-                    cudaMalloc(&a->nodeOffset, sizeof(uint32_t) * boxes.size()) == cudaSuccess &&
-                    cudaMalloc(&a->nodeCapacity, sizeof(uint32_t) * boxes.size()) == cudaSuccess &&
-                    cudaMalloc(&a->satOffset, sizeof(unsigned long long) * boxes.size()) == cudaSuccess &&
-                    cudaMalloc(&a->sat, sizeof(double) * sat) == cudaSuccess && cudaMalloc(&a->nodes, sizeof(x2::ad::Node) * nodes) == cudaSuccess &&
-                    cudaMalloc(&a->regionDone, sizeof(uint32_t) * boxes.size()) == cudaSuccess &&
-                    cudaMalloc(&a->errors, sizeof(float) * pixels) == cudaSuccess && cudaMalloc(&a->inImage, sizeof(uint64_t) * a->tiles) == cudaSuccess &&
-                    cudaMalloc(&a->tileMask, sizeof(uint64_t) * a->tiles) == cudaSuccess &&
-                    cudaMalloc(&a->chunkMasks, sizeof(uint64_t) * a->tiles) == cudaSuccess &&
-                    cudaMalloc(&a->planned, sizeof(uint32_t) * pixels) == cudaSuccess && cudaMalloc(&a->base, sizeof(uint32_t) * pixels) == cudaSuccess &&
-                    cudaMalloc(&a->stop, sizeof(uint32_t)) == cudaSuccess && cudaMalloc(&a->words, sizeof(uint32_t) * 8) == cudaSuccess &&
-                    cudaMalloc(&a->samples, sizeof(unsigned long long)) == cudaSuccess &&
-                    cudaMallocHost(&a->hostWords, sizeof(uint32_t) * 8) == cudaSuccess &&
-                    cudaMallocHost(&a->hostSamples, sizeof(unsigned long long)) == cudaSuccess &&
-                    cudaMalloc(&a->alive, 2 * size_t(a->tiles)) == cudaSuccess;
+    const size_t pixels = size_t(width) * height, regions = a->regionCount, cap = a->poolCapacity;
+    const size_t blocks = (a->tiles + x2::kCompactBlock - 1) / x2::kCompactBlock;
+    bool ok = true;
+    auto get = [&](auto** p, size_t bytes) { ok = ok && cudaMalloc(reinterpret_cast<void**>(p), bytes) == cudaSuccess; };
+    get(&a->boxes, sizeof(int32_t) * 4 * regions);
+    get(&a->satOffset, sizeof(unsigned long long) * regions);
+    for (uint32_t** p : {&a->bound, &a->nodes, &a->ready, &a->open, &a->rowStart, &a->colStart}) get(p, sizeof(uint32_t) * regions);
+    get(&a->sat, sizeof(double) * sat);
+    for (float** p : {&a->px0, &a->py0, &a->px1, &a->py1}) get(p, sizeof(float) * cap);
+    get(&a->pchild, sizeof(int32_t) * cap);
+    get(&a->pfate, cap);
+    get(&a->pregion, sizeof(uint32_t) * cap);
+    get(&a->poolWords, sizeof(uint32_t) * 4);
+    get(&a->errors, sizeof(float) * pixels);
+    for (uint64_t** p : {&a->inImage, &a->reach, &a->tileMask, &a->chunkMasks}) get(p, sizeof(uint64_t) * a->tiles);
+    get(&a->blockTiles, sizeof(uint32_t) * blocks);
+    get(&a->planned, sizeof(uint32_t) * pixels);
+    get(&a->base, sizeof(uint32_t) * pixels);
+    get(&a->stop, sizeof(uint32_t));
+    get(&a->words, sizeof(uint32_t) * 8);
+    get(&a->samples, sizeof(unsigned long long));
+    get(&a->alive, 2 * size_t(a->tiles));
+    get(&a->ratio, sizeof(float) * a->tiles);
+    ok = ok && cudaMallocHost(&a->hostWords, sizeof(uint32_t) * 8) == cudaSuccess &&
+         cudaMallocHost(&a->hostSamples, sizeof(unsigned long long)) == cudaSuccess;
     if (!ok) {
         delete a;
         s->adaptiveState = nullptr;
@@ -1776,11 +1785,13 @@ int ensureAdaptive(x2_scene* s, float target) {
         return X2_ENOMEM;
     }
     cudaStream_t st = s->ctx->stream;
-    cudaMemcpyAsync(a->regions, boxes.data(), sizeof(x2::ad::IBox) * boxes.size(), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(a->nodeOffset, nodeOffset.data(), sizeof(uint32_t) * boxes.size(), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(a->nodeCapacity, nodeCapacity.data(), sizeof(uint32_t) * boxes.size(), cudaMemcpyHostToDevice, st);
-    cudaMemcpyAsync(a->satOffset, satOffset.data(), sizeof(unsigned long long) * boxes.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(a->boxes, boxes.data(), sizeof(int32_t) * boxes.size(), cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(a->satOffset, satOffset.data(), sizeof(unsigned long long) * regions, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(a->bound, bound.data(), sizeof(uint32_t) * regions, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(a->rowStart, rowStart.data(), sizeof(uint32_t) * regions, cudaMemcpyHostToDevice, st);
+    cudaMemcpyAsync(a->colStart, colStart.data(), sizeof(uint32_t) * regions, cudaMemcpyHostToDevice, st);
     cudaMemcpyAsync(a->inImage, inImage.data(), sizeof(uint64_t) * a->tiles, cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(a->open, 0, sizeof(uint32_t) * regions, st);
     cudaMemsetAsync(a->planned, 0, sizeof(uint32_t) * pixels, st);
     cudaMemsetAsync(a->base, 0, sizeof(uint32_t) * pixels, st);
     cudaMemsetAsync(a->stop, 0, sizeof(uint32_t), st);
@@ -1790,22 +1801,128 @@ int ensureAdaptive(x2_scene* s, float target) {
 
 // The chain's arguments; a queued frame's (chunks: its compacted chunks) or a host-run step's (chunks null).
 x2::AdaptiveArgs adaptiveArgs(const AdaptiveState& a, x2_chunk* chunks = nullptr) {
-    return x2::AdaptiveArgs{a.width, a.height, a.tilesX, a.tiles, a.regionCount, a.target, a.layout, a.regions, a.nodeOffset, a.nodeCapacity,
-                            a.satOffset, a.sat, a.nodes, a.regionDone, a.errors, a.inImage, a.tileMask, a.planned, a.base, a.stop,
-                            chunks ? 1u : 0u, chunks, a.chunkMasks, a.words, a.words + 1, a.samples, nullptr, a.words + 5};
+    x2::AdaptiveArgs g{};
+    g.width = a.width;
+    g.height = a.height;
+    g.tilesX = a.tilesX;
+    g.tiles = a.tiles;
+    g.target = a.target;
+    g.regions = x2::RegionState{a.boxes, a.satOffset, a.bound, a.nodes, a.ready, a.open, a.regionCount, a.rowStart, a.colStart, a.rows, a.cols,
+                                a.grid};
+    g.pool = x2::TreePool{a.px0, a.py0, a.px1, a.py1, a.pchild, a.pfate, a.pregion, a.poolCapacity, a.poolWords, a.poolWords + 1};
+    g.sat = a.sat;
+    g.errors = a.errors;
+    g.inImage = a.inImage;
+    g.reach = a.reach;
+    g.tileMask = a.tileMask;
+    g.planned = a.planned;
+    g.base = a.base;
+    g.stop = a.stop;
+    g.queued = chunks ? 1u : 0u;
+    g.chunks = chunks;
+    g.chunkMasks = a.chunkMasks;
+    g.live = a.words;
+    g.passes = a.words + 1;
+    g.samples = a.samples;
+    g.blockTiles = a.blockTiles;
+    g.alive = nullptr;
+    g.liveTiles = a.words + 5;
+    g.ratio = a.ratio;
+    return g;
 }
 
-// One chain step on the frame's film: errors and trees (not in a uniform pass), then the pass's tile masks.
+// A graph built in segments of captured work on one stream, each after the last segment's end nodes, with
+// conditional while nodes between them.
+struct GraphSegments {
+    cudaStream_t st;
+    cudaGraph_t graph = nullptr;
+    std::vector<cudaGraphNode_t> tail;
+    cudaError_t err = cudaSuccess;
+    bool check(cudaError_t e) {
+        if (err == cudaSuccess && e != cudaSuccess) err = e;
+        return err == cudaSuccess;
+    }
+    bool begin(cudaGraph_t g, bool chained) {
+        return check(cudaStreamBeginCaptureToGraph(st, g, chained && !tail.empty() ? tail.data() : nullptr, nullptr, chained ? tail.size() : 0,
+                                                   cudaStreamCaptureModeThreadLocal));
+    }
+    bool end(bool chained) {
+        cudaStreamCaptureStatus status;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t n = 0;
+        const cudaError_t info = cudaStreamGetCaptureInfo(st, &status, nullptr, nullptr, &deps, &n);
+        if (info == cudaSuccess && chained) tail.assign(deps, deps + n);
+        cudaGraph_t out = nullptr;
+        check(info);
+        return check(cudaStreamEndCapture(st, &out));
+    }
+    // A while node after the tail; returns its body graph (null on failure) and its handle.
+    cudaGraph_t whileNode(cudaGraphConditionalHandle* handle) {
+        if (!check(cudaGraphConditionalHandleCreate(handle, graph, 1, cudaGraphCondAssignDefault))) return nullptr;
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = *handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t node;
+        if (!check(cudaGraphAddNode(&node, graph, tail.data(), tail.size(), &cp))) return nullptr;
+        tail.assign(1, node);
+        return cp.conditional.phGraph_out[0];
+    }
+};
+
+// The region trees of a pass, appended to a graph: the roots and the summed-area tables, then a while node growing
+// every region's trees a level an iteration, then the open leaves' reach over the tiles.
+bool appendTrees(GraphSegments& g, const x2::AdaptiveArgs& args, const AdaptiveState& a, int smCount) {
+    cudaStream_t st = g.st;
+    if (!g.begin(g.graph, true)) return false;
+    x2::treeRoots<<<(a.regionCount + 31) / 32, 32, 0, st>>>(args);
+    x2::tableRows<<<(a.rows + 127) / 128, 128, 0, st>>>(args);
+    x2::tableColumns<<<(a.cols + 127) / 128, 128, 0, st>>>(args);
+    g.check(cudaGetLastError());
+    if (!g.end(true)) return false;
+    cudaGraphConditionalHandle loop;
+    cudaGraph_t body = g.whileNode(&loop);
+    if (!body || !g.begin(body, false)) return false;
+    x2::treeLevel<<<smCount * 4, 256, 0, st>>>(args);
+    x2::treeNextLevel<<<1, 32, 0, st>>>(args, loop);
+    g.check(cudaGetLastError());
+    if (!g.end(false)) return false;
+    if (!g.begin(g.graph, true)) return false;
+    cudaMemsetAsync(a.reach, 0, sizeof(uint64_t) * a.tiles, st);
+    x2::leafReach<<<smCount * 8, 256, 0, st>>>(args);
+    g.check(cudaGetLastError());
+    return g.end(true);
+}
+
+// One chain step on the frame's film, run from the host: errors and trees (not in a uniform pass), then the pass's
+// tile masks; as one small graph, since the trees grow in a while node.
 int adaptiveChain(x2_scene* s, const x2::AdaptiveArgs& args, uint32_t uniform, uint32_t size) {
     AdaptiveState& a = *s->adaptiveState;
-    cudaStream_t st = s->ctx->stream;
+    GraphSegments g;
+    g.st = s->ctx->stream;
+    CUDA_OR(cudaGraphCreate(&g.graph, 0), X2_ECUDA);
     const uint32_t pixels = a.width * a.height;
-    if (!uniform) {
-        x2::adErrors<<<(pixels + 255) / 256, 256, 0, st>>>(args, s->sums, s->odd, s->counts);
-        x2::adTrees<<<a.regionCount, 512, 0, st>>>(args);
+    if (!uniform && g.begin(g.graph, true)) {
+        x2::chainPixelErrors<<<(pixels + 255) / 256, 256, 0, g.st>>>(args, s->sums, s->odd, s->counts);
+        g.check(cudaGetLastError());
+        if (g.end(true)) appendTrees(g, args, a, s->ctx->smCount);
     }
-    x2::adMasks<<<(a.tiles + 255) / 256, 256, 0, st>>>(args, uniform, size);
-    CUDA_OR(cudaGetLastError(), X2_ECUDA);
+    if (g.begin(g.graph, true)) {
+        x2::tileMasks<<<(a.tiles + 255) / 256, 256, 0, g.st>>>(args, uniform, size);
+        g.check(cudaGetLastError());
+        g.end(true);
+    }
+    cudaGraphExec_t exec = nullptr;
+    if (g.err == cudaSuccess) g.check(cudaGraphInstantiate(&exec, g.graph, 0));
+    cudaGraphDestroy(g.graph);
+    if (g.err == cudaSuccess) g.check(cudaGraphLaunch(exec, g.st));
+    if (g.err == cudaSuccess) g.check(cudaStreamSynchronize(g.st));
+    if (exec) cudaGraphExecDestroy(exec);
+    if (g.err != cudaSuccess) {
+        setError("adaptive chain step: %s", cudaGetErrorString(g.err));
+        return X2_ECUDA;
+    }
     return X2_OK;
 }
 
@@ -1897,72 +2014,50 @@ int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float 
     const uint32_t maxIter = uint32_t(std::min<uint64_t>(bound, 0xffffffffu));
 
     // The graph, built in segments: each captured onto the graph after the last segment's end nodes.
-    cudaGraph_t graph = nullptr;
-    CUDA_OR(cudaGraphCreate(&graph, 0), X2_ECUDA);
-    std::vector<cudaGraphNode_t> tail;
-    cudaError_t err = cudaSuccess;
-    auto check = [&](cudaError_t e) {
-        if (err == cudaSuccess && e != cudaSuccess) err = e;
-        return err == cudaSuccess;
-    };
-    auto beginSegment = [&](cudaGraph_t g, bool chained) {
-        return check(cudaStreamBeginCaptureToGraph(st, g, chained && !tail.empty() ? tail.data() : nullptr, nullptr,
-                                                   chained ? tail.size() : 0, cudaStreamCaptureModeThreadLocal));
-    };
-    auto endSegment = [&](bool chained) {
-        cudaStreamCaptureStatus status;
-        const cudaGraphNode_t* deps = nullptr;
-        size_t n = 0;
-        const cudaError_t info = cudaStreamGetCaptureInfo(st, &status, nullptr, nullptr, &deps, &n);
-        if (info == cudaSuccess && chained) tail.assign(deps, deps + n);
-        cudaGraph_t out = nullptr;
-        check(info);
-        return check(cudaStreamEndCapture(st, &out));
-    };
-    for (size_t k = 0; k < passes.size() && err == cudaSuccess; ++k) {
+    GraphSegments g;
+    g.st = st;
+    CUDA_OR(cudaGraphCreate(&g.graph, 0), X2_ECUDA);
+    const uint32_t pixels = ad.width * ad.height;
+    const int compactBlocks = int((ad.tiles + x2::kCompactBlock - 1) / x2::kCompactBlock);
+    for (size_t k = 0; k < passes.size() && g.err == cudaSuccess; ++k) {
         const uint32_t size = passes[k].second - passes[k].first;
         const uint32_t uniform = passes[k].first < minSamples ? 1u : 0u;
         a.samplesPerChunk = size;
         a.itemCount = (unsigned long long)ad.tiles * 64ull * size;
-        if (!beginSegment(graph, true)) break;
-        if (cellular) {
-            // The next generation from the film so far, then the pass's masks from it.
-            x2::AdaptiveArgs pass = chain;
-            if (!uniform) {
+        x2::AdaptiveArgs pass = chain;
+        if (!uniform) {
+            if (!g.begin(g.graph, true)) break;
+            x2::chainPixelErrors<<<(pixels + 255) / 256, 256, 0, st>>>(chain, s->sums, s->odd, s->counts);
+            if (cellular) {
+                // The next generation from the film so far; the pass's masks come from it.
                 const uint8_t* aliveIn = ad.alive + size_t(generation % 2) * ad.tiles;
                 uint8_t* aliveOut = ad.alive + size_t((generation + 1) % 2) * ad.tiles;
                 ++generation;
-                const uint32_t pixels = ad.width * ad.height;
-                x2::adErrors<<<(pixels + 255) / 256, 256, 0, st>>>(chain, s->sums, s->odd, s->counts);
                 cudaMemsetAsync(chain.liveTiles, 0, sizeof(uint32_t), st);
-                x2::adCellular<<<(ad.tiles + 255) / 256, 256, 0, st>>>(chain, aliveIn, aliveOut);
+                x2::tileRatios<<<(ad.tiles + 255) / 256, 256, 0, st>>>(chain);
+                x2::nextGeneration<<<(ad.tiles + 255) / 256, 256, 0, st>>>(chain, aliveIn, aliveOut);
                 pass.alive = aliveOut;
             }
-            x2::adMasks<<<(ad.tiles + 255) / 256, 256, 0, st>>>(pass, uniform, size);
-        } else {
-            adaptiveChain(s, chain, uniform, size);
+            g.check(cudaGetLastError());
+            if (!g.end(true)) break;
+            if (!cellular && !appendTrees(g, chain, ad, s->ctx->smCount)) break;
         }
-        x2::adCompact<<<1, x2::kCompactThreads, 0, st>>>(chain, size);
+        if (!g.begin(g.graph, true)) break;
+        x2::tileMasks<<<(ad.tiles + 255) / 256, 256, 0, st>>>(pass, uniform, size);
+        x2::compactCount<<<compactBlocks, x2::kCompactBlock, 0, st>>>(chain);
+        x2::compactWrite<<<compactBlocks, x2::kCompactBlock, 0, st>>>(chain, size);
         cudaMemsetAsync(s->wave.state, 0, sizeof(uint32_t) * paths, st);
         cudaMemsetAsync(s->wave.ncount, 0, sizeof(uint32_t) * paths, st);
         cudaMemsetAsync(s->claimed, 0, sizeof(unsigned long long), st);
         cudaMemsetAsync(s->waveCounters, 0, sizeof(uint32_t) * kWaveCounters, st);
         cudaMemsetAsync(s->outStatus, X2_SKIP, a.itemCount, st);
         cudaMemsetAsync(ad.words + 2, 0, sizeof(uint32_t), st);
-        check(cudaGetLastError());
-        if (!endSegment(true)) break;
+        g.check(cudaGetLastError());
+        if (!g.end(true)) break;
         // The pass's drain: a while node whose body is one iteration and the test that decides the next.
         cudaGraphConditionalHandle loop;
-        if (!check(cudaGraphConditionalHandleCreate(&loop, graph, 1, cudaGraphCondAssignDefault))) break;
-        cudaGraphNodeParams cp = {};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = loop;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaGraphNode_t node;
-        if (!check(cudaGraphAddNode(&node, graph, tail.data(), tail.size(), &cp))) break;
-        tail.assign(1, node);
-        if (!beginSegment(cp.conditional.phGraph_out[0], false)) break;
+        cudaGraph_t body = g.whileNode(&loop);
+        if (!body || !g.begin(body, false)) break;
         wfResetQueues<<<1, 32, 0, st>>>(a);
         wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
         wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
@@ -1970,13 +2065,19 @@ int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float 
         wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
         wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
         wfDrainCheck<<<1, 32, 0, st>>>(a, loop, ad.words + 2, maxIter, ad.words + 4);
-        check(cudaGetLastError());
-        if (!endSegment(false)) break;
-        if (!beginSegment(graph, true)) break;
+        g.check(cudaGetLastError());
+        if (!g.end(false)) break;
+        if (!g.begin(g.graph, true)) break;
         wfFilmReduce<<<int((64ull * ad.tiles + 255) / 256), 256, 0, st>>>(a, ad.tiles, s->sums, s->odd, s->counts);
-        check(cudaGetLastError());
-        endSegment(true);
+        g.check(cudaGetLastError());
+        g.end(true);
     }
+    cudaError_t err = g.err;
+    auto check = [&](cudaError_t e) {
+        if (err == cudaSuccess && e != cudaSuccess) err = e;
+        return err == cudaSuccess;
+    };
+    cudaGraph_t graph = g.graph;
     cudaGraphExec_t exec = nullptr;
     if (err == cudaSuccess) check(cudaGraphInstantiate(&exec, graph, 0));
     cudaGraphDestroy(graph);
@@ -2052,7 +2153,7 @@ int x2_render_adaptive_budget(x2_scene* s, uint32_t minSamples, uint32_t maxSamp
             if (tx + p % 8 < ad.width && ty + p / 8 < ad.height) m |= uint64_t(1) << p;
         inImage[t] = m;
     }
-    x2::CellularGenerations cells(int(ad.width), int(ad.height), floor, inImage);
+    x2::TileGenerations cells(ad.width, ad.height, floor, inImage);
     std::vector<uint32_t> planned(pixels, 0), base(pixels, 0);
     std::vector<float> errors(pixels);
     std::vector<x2_chunk> chunks;
@@ -2064,28 +2165,28 @@ int x2_render_adaptive_budget(x2_scene* s, uint32_t minSamples, uint32_t maxSamp
     for (size_t k = 0; k < passes.size() && rc == X2_OK; ++k) {
         const uint32_t size = passes[k].second - passes[k].first;
         const bool uniform = passes[k].first < minSamples;
-        std::vector<char> dropped;
+        std::vector<uint8_t> take;
         if (!uniform) {
             if (spent >= double(budget)) break;  // the budget is spent
-            x2::adErrors<<<(pixels + 255) / 256, 256, 0, st>>>(args, s->sums, s->odd, s->counts);
+            x2::chainPixelErrors<<<(pixels + 255) / 256, 256, 0, st>>>(args, s->sums, s->odd, s->counts);
             cudaMemcpyAsync(errors.data(), ad.errors, sizeof(float) * pixels, cudaMemcpyDeviceToHost, st);
             if (cudaStreamSynchronize(st) != cudaSuccess) {
                 rc = X2_ECUDA;
                 break;
             }
-            const x2::SampleBudget b{&planned, std::max(0.0, double(budget) - spent), maxSamples, floor};
-            if (cells.update(errors.data(), &b) == 0) {
+            const double left = std::max(0.0, double(budget) - spent);
+            if (cells.advance(errors.data(), planned, left, maxSamples) == 0) {
                 r.converged = 1;
                 break;
             }
-            dropped = x2::dropForBudget(cells, inImage, size, b.remaining);
+            take = cells.chosen(size, left);
         }
         chunks.clear();
         chunkMasks.clear();
         uint64_t samples = 0;
         for (uint32_t t = 0; t < ad.tiles; ++t) {
             uint64_t m = inImage[t];
-            if (!uniform && !(cells.alive(t) && (dropped.empty() || !dropped[t]))) m = 0;
+            if (!uniform && !take[t]) m = 0;
             if (!m) continue;
             for (uint32_t p = 0; p < 64; ++p)
                 if (m >> p & 1) {
