@@ -425,6 +425,11 @@ int x2_film_download(x2_scene* scene, double* sums, double* odd, uint32_t* count
 int x2_film_device(x2_scene* scene, double** d_sums, double** d_odd, uint32_t** d_counts);
 int x2_audit(x2_scene* scene, const uint32_t* expected, int64_t* bad_pixel);  /* async_render.h:992-1048 */
 int x2_counters_read(x2_scene* scene, x2_counters* out);  /* waits */
+/* Measurement only (no reference counterpart): the device's cache read bandwidth in GB/s, the ceiling of the
+ * traversal kernels' node and triangle fetches. level 2: a buffer of `bytes` (under the L2's size) swept `passes`
+ * times by the whole grid; level 1: each block re-reading its own slice of min(bytes, 96 KiB). Allocates its buffer;
+ * waits. */
+int x2_probe_bandwidth(x2_ctx* ctx, uint32_t level, uint64_t bytes, uint32_t passes, float* gbs);
 int x2_counters_reset(x2_scene* scene);
 /* Counting mode (no reference counterpart; the algorithmic-bytes count of the roofline): launches made while it is
  * on count BVH node visits and triangle tests per ray. It slows them: never time a counting launch. */

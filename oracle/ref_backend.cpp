@@ -1048,26 +1048,34 @@ int x2ref_trace_brute(void* p, const float* rays, uint64_t n, uint32_t* tri, flo
     if (!h) return X2_EINVAL;
     const Scene& s = h->scene;
     const U32 nt = U32(s.tris.size() / 3);
-    for (uint64_t i = 0; i < n; ++i) {
-        const float* r = rays + 8 * i;
-        const V3 o{r[0], r[1], r[2]}, d{r[3], r[4], r[5]};
-        const TriTest sh = shear(d);
-        U32 best = ~0u;
-        float tBest = r[7];
-        bool any = false;
-        for (U32 k = 0; k < nt; ++k) {
-            float th;
-            const V3 a = s.vertex(s.tris[3 * k]), b = s.vertex(s.tris[3 * k + 1]), c = s.vertex(s.tris[3 * k + 2]);
-            if (triHit(sh, o, a, b, c, r[6], r[7], th)) any = true;
-            if (triHit(sh, o, a, b, c, r[6], tBest, th) && (th < tBest || (th == tBest && k < best))) {
-                tBest = th;
-                best = k;
+    std::atomic<uint64_t> next{0};
+    auto work = [&]() {
+        for (uint64_t i; (i = next.fetch_add(1)) < n;) {
+            const float* r = rays + 8 * i;
+            const V3 o{r[0], r[1], r[2]}, d{r[3], r[4], r[5]};
+            const TriTest sh = shear(d);
+            U32 best = ~0u;
+            float tBest = r[7];
+            bool any = false;
+            for (U32 k = 0; k < nt; ++k) {
+                float th;
+                const V3 a = s.vertex(s.tris[3 * k]), b = s.vertex(s.tris[3 * k + 1]), c = s.vertex(s.tris[3 * k + 2]);
+                if (triHit(sh, o, a, b, c, r[6], r[7], th)) any = true;
+                if (triHit(sh, o, a, b, c, r[6], tBest, th) && (th < tBest || (th == tBest && k < best))) {
+                    tBest = th;
+                    best = k;
+                }
             }
+            tri[i] = best;
+            t[i] = best == ~0u ? 0.0f : tBest;
+            occl[i] = any ? 1u : 0u;
         }
-        tri[i] = best;
-        t[i] = best == ~0u ? 0.0f : tBest;
-        occl[i] = any ? 1u : 0u;
-    }
+    };
+    std::vector<std::thread> pool;
+    const unsigned threads = std::max(1u, std::thread::hardware_concurrency());
+    for (unsigned w = 1; w < threads; ++w) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
     return X2_OK;
 }
 

@@ -227,3 +227,30 @@ def test_fp64_adjoint_against_finite_differences(adjoint_scene):
         fd = (loss(albedo, up) - loss(albedo, down)) / (2 * h)
         assert abs(fd - gr[i, 0]) <= 1e-2 * abs(gr[i, 0]) + 2e-3 * np.abs(gr[:, 0]).max(), (i, fd, gr[i, 0])
     oracle_lib.adjoint64(ref, 0, cfg.spp, w, params=(albedo, None, radiance))
+
+
+@pytest.mark.skipif(not oracle_lib.have_reference(), reason="oracle/_ref not built")
+def test_oracle_traversal_matches_brute_force_on_a_field():
+    """The oracle's own BVH against testing every triangle on config 108 (the 1M-triangle field scaled down: 191,488
+    triangles): 10,000 closest-hit rays and 10,000 shadow rays of random origins and directions inside the scene's
+    bounds, the same triangle, t and occlusion. The device traversal is checked against this BVH, so a defect shared by
+    both would have to survive this check too."""
+    r = np.random.default_rng(108)
+    s = x2.SyntheticScene(108)
+    v = np.ctypeslib.as_array(s.desc.vertices, (s.desc.vertex_count, 3))
+    lo, hi = v.min(0), v.max(0)
+    rays = []
+    for shadow in (False, True):
+        o = lo + (hi - lo) * r.random((10000, 3))
+        d = r.normal(size=(10000, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        far = r.random(10000) * np.linalg.norm(hi - lo) if shadow else np.full(10000, 3.4e38)
+        rays.append(np.concatenate([o, d, np.zeros((10000, 1)), far[:, None]], 1).astype(np.float32))
+    rays = np.concatenate(rays)
+    ref = oracle_lib.Reference(s)
+    a = ref.trace(rays)
+    b = ref.trace(rays, brute=True)
+    hits = int((a[0] != 0xFFFFFFFF).sum())
+    assert hits > 5000, hits  # most rays hit something: the check is not vacuous
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)

@@ -14,7 +14,7 @@ OUT = os.path.join(HERE, "x2", "libx2.so")
 # transcendental functions in double on request, and a record of every call), linked with the product's other objects.
 DIAG_OUT = os.path.join(HERE, "x2", "libx2diag.so")
 BUILD = os.path.join(HERE, "_build")
-CU = ["api.cu", "render.cu", "wavefront.cu", "bvh_build.cu", "noalloc.cu", "adjoint.cu", "adaptive.cu", "scores.cu"]
+CU = ["api.cu", "render.cu", "wavefront.cu", "bvh_build.cu", "noalloc.cu", "adjoint.cu", "adaptive.cu", "scores.cu", "probe.cu"]
 CPP = ["scene_gen.cpp", "grid.cpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

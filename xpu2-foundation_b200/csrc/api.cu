@@ -88,7 +88,9 @@ int waitEvent(cudaEvent_t e, int timeoutMs) {
 
 constexpr int kSlots = 2;  // launches in flight, as GpuLane keeps (async_gpu.h:1425)
 constexpr uint32_t kQueueLog = 4096;
-constexpr int kWaveCounters = 8;  // extend count, last extend count, shadow count, extend fetch, shadow fetch
+// extend count, last extend count, shadow count, extend fetch, shadow fetch, 3 shade queue counts, then the shadow
+// queue's record segments (x2::kRecordSegments)
+constexpr int kWaveCounters = 8 + int(x2::kRecordSegments);
 
 struct Slot {
     bool busy = false;
@@ -418,6 +420,17 @@ int sceneView(x2_scene* s, SceneView* view, cudaStream_t* stream, int* device, i
     *stream = s->ctx->stream;
     *device = s->ctx->device;
     *smCount = s->ctx->smCount;
+    return X2_OK;
+}
+// A context's stream and SM count, its device current (probe.cu).
+int contextStream(x2_ctx* ctx, cudaStream_t* stream, int* smCount) {
+    if (!ctx) {
+        setError("null context");
+        return X2_EINVAL;
+    }
+    if (int rc = checkDevice(ctx)) return rc;
+    *stream = ctx->stream;
+    *smCount = ctx->smCount;
     return X2_OK;
 }
 }  // namespace x2
@@ -1191,6 +1204,7 @@ WaveArgs launchArgs(x2_scene* s, Slot& sl, uint32_t paths, uint32_t records, uns
     a.lastExtend = s->waveCounters + 1;
     a.shadowQ = s->shadowQ;
     a.shadowCount = s->waveCounters + 2;
+    a.shadowSlots = a.recordsPerPath <= x2::kRecordSegments ? s->waveCounters + 8 : nullptr;
     a.extendNext = s->waveCounters + 3;
     a.shadowNext = s->waveCounters + 4;
     a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
@@ -1622,6 +1636,7 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     a.lastExtend = s->waveCounters + 1;
     a.shadowQ = s->shadowQ;
     a.shadowCount = s->waveCounters + 2;
+    a.shadowSlots = a.recordsPerPath <= x2::kRecordSegments ? s->waveCounters + 8 : nullptr;
     a.extendNext = s->waveCounters + 3;
     a.shadowNext = s->waveCounters + 4;
     a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
@@ -2488,6 +2503,7 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
         a.lastExtend = s0->waveCounters + 1;
         a.shadowQ = s0->shadowQ;
         a.shadowCount = s0->waveCounters + 2;
+        a.shadowSlots = a.recordsPerPath <= x2::kRecordSegments ? s0->waveCounters + 8 : nullptr;
         a.extendNext = s0->waveCounters + 3;
         a.shadowNext = s0->waveCounters + 4;
         a.shadeQ = s0->lobeQueues ? s0->shadeQ : nullptr;

@@ -11,6 +11,12 @@ namespace x2 {
 // The last failure's text, per host thread (x2_last_error).
 void setError(const char* fmt, ...);
 
+}  // namespace x2
+struct x2_ctx;
+namespace x2 {
+// A context's stream and SM count, with its device made current (api.cu).
+int contextStream(x2_ctx* ctx, cudaStream_t* stream, int* smCount);
+
 struct DeviceBvh {
     Node8* nodes = nullptr;
     TriRec* tris = nullptr;

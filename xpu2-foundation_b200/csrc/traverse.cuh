@@ -241,8 +241,14 @@ static __device__ __noinline__ uint32_t traceClosest(const Bvh8 bvh, const RayQ&
 // A ray traced one node a step, for kernels that keep every lane of a warp busy by handing a lane whose ray is done
 // the next ray of the queue (persistent threads with dynamic ray fetch; Aila and Laine 2009). The steps visit the
 // same nodes and test the same triangles, in the same order, as traceClosest / traceAny, so the results are the same.
+//
+// The stack's first kShortStack entries live in shared memory, entry-major (entry e of thread t at
+// shortStack[e * blockDim.x + t], so a warp's accesses fall in distinct banks); deeper entries, which an 8-wide tree
+// rarely needs, go to the thread's local array.
+constexpr int kShortStack = 8;
 struct Walk {
-    uint2 stack[kStack];
+    uint2 deep[kStack - kShortStack];
+    uint2* shortStack;  // this thread's column: entry e at shortStack[e * blockDim.x]
     int sp;
     uint32_t base, bits, imask;  // the node group being visited: its child base, hit mask, internal-child mask
     uint32_t tbase, tbits;       // triangles of the last node still to test: first leaf-order index, mask
@@ -250,6 +256,20 @@ struct Walk {
     uint32_t best, bestLeaf;     // closest hit: scene triangle (~0u none) and leaf-order index; any hit: 1 if occluded
     uint32_t nodes, tris;        // counting mode
 };
+
+__device__ __forceinline__ void walkPush(Walk& w, uint2 e, uint32_t* overflow) {
+    if (w.sp < kShortStack) w.shortStack[size_t(w.sp) * blockDim.x] = e;
+    else if (w.sp < kStack) w.deep[w.sp - kShortStack] = e;
+    else {
+        atomicAdd(overflow, 1u);
+        return;
+    }
+    ++w.sp;
+}
+__device__ __forceinline__ uint2 walkPop(Walk& w) {
+    --w.sp;
+    return w.sp < kShortStack ? w.shortStack[size_t(w.sp) * blockDim.x] : w.deep[w.sp - kShortStack];
+}
 
 template <bool kAny>
 __device__ __forceinline__ void walkStart(Walk& w, const RayQ& r, float tmin, float tmax) {
@@ -273,7 +293,7 @@ __device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk& w
     if (!w.tbits) {
         if (!(w.bits & 0xff000000u)) {
             if (w.sp == 0) return true;
-            const uint2 e = w.stack[--w.sp];
+            const uint2 e = walkPop(w);
             w.base = e.x;
             w.bits = e.y & 0xff000000u;
             w.imask = (e.y >> 16) & 0xffu;
@@ -282,10 +302,7 @@ __device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk& w
         w.bits &= ~(1u << (24 + b));
         const uint32_t slot = b ^ r.oct7;
         const uint32_t child = w.base + __popc(w.imask & ((1u << slot) - 1u));
-        if (w.bits & 0xff000000u) {
-            if (w.sp < kStack) w.stack[w.sp++] = make_uint2(w.base, w.bits | (w.imask << 16));
-            else atomicAdd(overflow, 1u);
-        }
+        if (w.bits & 0xff000000u) walkPush(w, make_uint2(w.base, w.bits | (w.imask << 16)), overflow);
         uint32_t childBase, imask;
         const uint32_t hits = visitNode(bvh.nodes, child, r, w.tmin - r.eps, w.tmax + r.eps, childBase, w.tbase, imask);
         ++w.nodes;

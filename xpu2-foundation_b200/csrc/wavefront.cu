@@ -318,14 +318,30 @@ __global__ void __launch_bounds__(kWaveBlock) wfLogicAdjoint(WaveArgs a) { logic
 // Persistent traversal over a queue: each lane walks its ray a node a step; a warp fetches the next rays of the queue
 // (one atomic a warp) for its idle lanes once `refill` of them are idle, so lanes whose rays end early are not left
 // waiting for the warp's longest ray. kAny: shadow records (visibility out), else extend rays (closest hit out).
+// A queue in segments (the shadow queue by record): entry i lies in the segment s with start[s] <= i < start[s + 1],
+// at queue[s * stride + i - start[s]]. segments 0: a plain queue.
+struct QueueSegments {
+    const uint32_t* start;  // segments + 1 running totals (shared memory)
+    uint32_t segments, stride;
+    __device__ __forceinline__ uint32_t at(const uint32_t* __restrict__ queue, uint32_t i) const {
+        if (!segments) return queue[i];
+        uint32_t s = 0;
+        while (s + 1 < segments && start[s + 1] <= i) ++s;
+        return queue[size_t(s) * stride + (i - start[s])];
+    }
+};
+
+// shortStacks: the block's kShortStack x kWaveBlock short traversal stacks (shared memory).
 template <bool kAny, bool kStats, bool kBatch>
-__device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, const uint32_t* __restrict__ queue, uint32_t* next) {
+__device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, const uint32_t* __restrict__ queue, uint32_t* next,
+                                                uint2* shortStacks, const QueueSegments seg = QueueSegments{nullptr, 0, 0}) {
     const WaveState& w = a.w;
     Bvh8 bvh = a.scene.bvh;  // a batch: the lane's ray's scene, set at each fetch
     uint32_t* overflow = a.scene.overflow;
     const unsigned full = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u;
     Walk walk;
+    walk.shortStack = shortStacks + threadIdx.x;
     walk.nodes = walk.tris = 0;
     RayQ r;
     uint32_t k = 0, rays = 0;
@@ -341,7 +357,7 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
             if (!live) {
                 const uint32_t i = base + __popc(idle & ((1u << lane) - 1u));
                 if (i < n) {
-                    k = queue[i];
+                    k = seg.at(queue, i);
                     if (kBatch) {
                         const SceneView& sv = a.scenes[requestOf(w, kAny ? k / a.recordsPerPath : k)];
                         bvh = sv.bvh;
@@ -372,9 +388,10 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
 
 template <bool kBatch>
 __device__ __forceinline__ void extendBody(const WaveArgs& a) {
+    __shared__ uint2 shortStacks[kShortStack * kWaveBlock];
     const uint32_t n = *a.extendCount;
-    if (!kBatch && a.scene.stats) persistentTrace<false, true, false>(a, n, a.extendQ, a.extendNext);
-    else persistentTrace<false, false, kBatch>(a, n, a.extendQ, a.extendNext);
+    if (!kBatch && a.scene.stats) persistentTrace<false, true, false>(a, n, a.extendQ, a.extendNext, shortStacks);
+    else persistentTrace<false, false, kBatch>(a, n, a.extendQ, a.extendNext, shortStacks);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters->trace, (unsigned long long)n);
 }
 
@@ -583,8 +600,18 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
             const size_t first = size_t(p) * a.recordsPerPath;
             for (uint32_t k = 0; k < records; ++k) w.svis[first + k] = 0;
         }
-        const uint32_t slot = warpReserve(a.shadowCount, records);
-        for (uint32_t k = 0; k < records; ++k) a.shadowQ[slot + k] = p * a.recordsPerPath + k;
+        if (a.shadowSlots) {
+            // Record k of each lane's path into segment k; the total for the host's statistics.
+            warpReserve(a.shadowCount, records);
+            const uint32_t most = __reduce_max_sync(0xffffffffu, records);
+            for (uint32_t k = 0; k < most; ++k) {
+                const uint32_t slot = warpReserve(a.shadowSlots + k, records > k ? 1u : 0u);
+                if (records > k) a.shadowQ[size_t(k) * a.paths + slot] = p * a.recordsPerPath + k;
+            }
+        } else {
+            const uint32_t slot = warpReserve(a.shadowCount, records);
+            for (uint32_t k = 0; k < records; ++k) a.shadowQ[slot + k] = p * a.recordsPerPath + k;
+        }
     }
     warpAddCounters(a.counters, 0, nee, bsdf, held, 0, 0);
     if (kAdjoint) partialsEnd(partial, at, a.adj);
@@ -593,9 +620,25 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
 // ---- shadow: any hits ----
 template <bool kBatch>
 __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
-    const uint32_t n = *a.shadowCount;
-    if (!kBatch && a.scene.stats) persistentTrace<true, true, false>(a, n, a.shadowQ, a.shadowNext);
-    else persistentTrace<true, false, kBatch>(a, n, a.shadowQ, a.shadowNext);
+    __shared__ uint32_t start[kRecordSegments + 1];
+    QueueSegments seg{start, 0, a.paths};
+    uint32_t n = *a.shadowCount;
+    if (a.shadowSlots) {
+        seg.segments = a.recordsPerPath;
+        if (threadIdx.x == 0) {
+            uint32_t run = 0;
+            for (uint32_t k = 0; k < seg.segments; ++k) {
+                start[k] = run;
+                run += a.shadowSlots[k];
+            }
+            start[seg.segments] = run;
+        }
+        __syncthreads();
+        n = start[seg.segments];
+    }
+    __shared__ uint2 shortStacks[kShortStack * kWaveBlock];
+    if (!kBatch && a.scene.stats) persistentTrace<true, true, false>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
+    else persistentTrace<true, false, kBatch>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
 }
 
 // The kernels, each in a few occupancy variants (blocks of kWaveBlock threads a SM that the register allocation must
@@ -659,6 +702,8 @@ __global__ void wfResetQueues(WaveArgs a) {
         *a.extendCount = 0;
         *a.shadowCount = 0;
         *a.extendNext = 0;
+        if (a.shadowSlots)
+            for (uint32_t k = 0; k < a.recordsPerPath; ++k) a.shadowSlots[k] = 0;
         *a.shadowNext = 0;
         if (a.shadeQ) a.shadeCount[0] = a.shadeCount[1] = a.shadeCount[2] = 0;
     }

@@ -5,6 +5,7 @@
 namespace x2 {
 
 constexpr int kWaveBlock = 128;
+constexpr uint32_t kRecordSegments = 64;
 // Launch-shape defaults (x2_wavefront_tune changes them a scene).
 constexpr uint32_t kDefaultRefill = 8, kDefaultBlocksPerSm = 16, kDefaultTraceBlocks = 0, kDefaultShadeBlocks = 4,
                    kDefaultTriLimit = 1;
@@ -58,6 +59,11 @@ struct WaveArgs {
     uint32_t* lastExtend;
     uint32_t* shadowQ;
     uint32_t* shadowCount;
+    // The shadow queue by record (null: by path, each path's records together): record k of every path that made
+    // one goes to segment k of the queue (shadowQ + k * paths), shadowSlots[k] entries, so a warp traces the k-th
+    // shadow rays of neighbouring paths (mostly toward the same light) instead of one path's rays toward every light.
+    // At most kRecordSegments records a path.
+    uint32_t* shadowSlots;
     uint32_t* extendNext;  // the extend and shadow kernels' fetch counters over their queues
     uint32_t* shadowNext;
     // Per-lobe shade queues (null: shade walks the extend queue as it is): after extend, wfSortShade sorts the

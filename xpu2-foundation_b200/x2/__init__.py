@@ -187,6 +187,7 @@ def library():
         "x2_render_adaptive": ([vp, u32, u32, C.c_float, C.POINTER(AdaptiveResult)], i32), "x2_render_adaptive_cellular": ([vp, u32, u32, C.c_float, C.POINTER(AdaptiveResult)], i32),
         "x2_render_adaptive_budget": ([vp, u32, u32, C.c_float, u64, C.POINTER(AdaptiveResult)], i32), "x2_adaptive_planned": ([vp, vp], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
+        "x2_probe_bandwidth": ([vp, u32, u64, u32, C.POINTER(C.c_float)], i32),
         "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
         "x2_workgrid_options_defaults": ([C.POINTER(WorkGridOptions)], None),
@@ -244,6 +245,12 @@ class Context:
                 s.free()
             library().x2_close(self._h)
             self._h = C.c_void_p()
+
+    def probe_bandwidth(self, level, nbytes, passes):
+        """The device's L2 (level 2) or L1 (level 1) read bandwidth in GB/s (x2_probe_bandwidth)."""
+        g = C.c_float()
+        _check(library().x2_probe_bandwidth(self._h, level, nbytes, passes, C.byref(g)))
+        return g.value
 
     def __enter__(self):
         return self
