@@ -439,6 +439,50 @@ def probe_volume(args):
     ctx.close()
 
 
+def probe_estimators(args):
+    """Config 3 (the 256^3 medium): the reference's decoupled march against delta/ratio tracking over 32^3 majorant
+    grids (x2_config.volume_estimator 1), each rendering the RMSE fixture's tiles (tests/golden/rmse_c3.npz) in the
+    wavefront form: at the configuration's 256 spp, then tracking at the spp that takes the march's time; each image's
+    RMSE against the converged reference (16,384 spp of the march, FP64 film). Then `--probe-tiles` evenly spaced tiles
+    of the frame at 256 spp in each form for throughput."""
+    import rmse_lib
+    import x2
+
+    ctx = x2.Context(0)
+    f = np.load(os.path.join(ROOT, "tests", "golden", "rmse_c3.npz"))
+    tiles, live, ref = f["tiles"], f["live"], f["ref"].astype(np.float64)
+    out = {"probe": "estimators", "config": 3, "fixture_tiles": int(len(tiles)), "fixture_pixels": int(live.sum())}
+    scenes = {}
+    for name, est in (("march", 0), ("tracking", 1)):
+        s = x2.SyntheticScene(3)
+        s.config.volume_estimator = est
+        scenes[name] = (s, x2.Scene(ctx, s.desc, s.config))
+    spp = int(f["spp"])
+    for name, (s, scene) in scenes.items():
+        rmse_lib.render_tiles(scene, tiles, spp, True)  # warm-up
+        img, ms = rmse_lib.render_tiles(scene, tiles, spp, True)
+        out[name] = {"spp": spp, "ms": ms, "rmse": rmse_lib.rmse(img, ref, live), "mean": float(img[live].mean())}
+    out["ref_mean"] = float(ref[live].mean())
+    equal = max(1, int(spp * out["march"]["ms"] / out["tracking"]["ms"]))
+    s, scene = scenes["tracking"]
+    img, ms = rmse_lib.render_tiles(scene, tiles, equal, True)
+    out["tracking_equal_time"] = {"spp": equal, "ms": ms, "rmse": rmse_lib.rmse(img, ref, live)}
+    cfg = scenes["march"][0].config
+    all_tiles = ((cfg.width + 7) // 8) * ((cfg.height + 7) // 8)
+    sel = np.linspace(0, all_tiles - 1, min(all_tiles, args.probe_tiles)).astype(np.uint32)
+    for name, (s, scene) in scenes.items():
+        chunks = np.zeros(len(sel), x2.CHUNK_DTYPE)
+        chunks["tile"], chunks["first"], chunks["count"] = sel, 0, spp
+        scene.frame_begin(spp)
+        scene.launch_wavefront(chunks)
+        c = scene.wait()
+        out[name]["throughput"] = {"tiles": len(sel), "msamples_per_s": len(sel) * 64 * spp / c.milliseconds / 1e3, "ms": c.milliseconds}
+    print(json.dumps(out))
+    for s, scene in scenes.values():
+        scene.free()
+    ctx.close()
+
+
 def probe_adjoint(args):
     """Config 4 (about 250k triangles: a heightfield under a 1024x1024 albedo texture and 64 icospheres of 64
     materials; 512x512): the primal frame at 32 spp (wavefront and plain) and the
@@ -599,6 +643,8 @@ def probe(args):
         return probe_volume(args)
     if args.probe == "adjoint":
         return probe_adjoint(args)
+    if args.probe == "estimators":
+        return probe_estimators(args)
     if args.probe == "rmse":
         return probe_rmse(args)
     if args.probe == "adaptive":
@@ -642,7 +688,7 @@ def main():
     ap.add_argument("--impl", default="x2", choices=["x2", "reference"])
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--skip-plain", action="store_true")
-    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint", "rmse", "adaptive", "workgrid"], help="one bounded launch for a profiler, then exit")
+    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint", "rmse", "adaptive", "workgrid", "estimators"], help="one bounded launch for a profiler, then exit")
     ap.add_argument("--probe-tiles", type=int, default=592)
     ap.add_argument("--probe-timed", action="store_true", help="wavefront probe without its graph (per-kernel launches)")
     ap.add_argument("--adjoint-only", action="store_true", help="adjoint probe: one primal frame, then one wavefront adjoint launch")

@@ -168,7 +168,11 @@ typedef struct x2_config {
     uint32_t volume_count, max_volume_depth, volume_illumination_samples, volume_overlap_mode;
     float volume_transmittance_threshold, volume_attenuation_factor, volume_contribution_factor, volume_phase_attenuation_factor;
     float inv_volume_quality, inv_volume_shadow_quality;
-    uint32_t reserved[8];
+    /* The volume integrals' estimator: 0 the reference's decoupled ray marching (per-sample parity with the
+     * reference); 1 delta and ratio tracking over 32^3 majorant grids (no reference counterpart: the same integrals
+     * sampled otherwise; grey extinction, max_volume_depth 1, overlap modes sum or max). */
+    uint32_t volume_estimator;
+    uint32_t reserved[7];
 } x2_config;
 
 /* Ray counters, the reference's XPU2_PROFILE ray counts (async_gpu_abi.h:16-20): hit rays (trace), shadow rays

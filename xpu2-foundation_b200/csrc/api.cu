@@ -182,6 +182,8 @@ struct x2_scene {
     float* volumeTris = nullptr;
     GridRec* grids = nullptr;
     std::vector<float*> gridValues;
+    std::vector<float*> majorants;  // each volume's majorant grid (device)
+    bool greyVolumes = true;        // every volume's gain has three equal channels (the tracking estimator's condition)
     uint32_t volumeCount = 0, gridCount = 0;
     x2_camera camera{};
     x2_config config{};
@@ -434,6 +436,52 @@ int contextStream(x2_ctx* ctx, cudaStream_t* stream, int* smCount) {
     return X2_OK;
 }
 }  // namespace x2
+
+namespace {
+// A volume's majorant grid: kMajorantCells^3 cells over its bounds, each the largest density any of the lookups can
+// read at a point of the cell (nearest voxel, trilinear or quadratic: the voxels whose index box the cell's corners
+// span, one more each way) times its largest gain channel; *largest the grid's maximum. Corners go to grid space by
+// the volume's affine map and to index space by the grid's, so any affine placement stays conservative.
+std::vector<float> majorantGrid(const x2_volume& v, const x2_grid* grids, uint32_t gridCount, float* largest) {
+    const int n = x2::kMajorantCells;
+    std::vector<float> out(size_t(n) * n * n, 0.0f);
+    *largest = 0.0f;
+    if (v.density_grid >= gridCount || grids[v.density_grid].channels != 1) return out;
+    const x2_grid& g = grids[v.density_grid];
+    const float gain = std::max(0.0f, std::max(v.gain[0], std::max(v.gain[1], v.gain[2])));
+    auto toIndex = [&](double x, double y, double z, double out3[3]) {
+        const float* a = v.world_to_grid;
+        const double gx = a[0] * x + a[1] * y + a[2] * z + a[3], gy = a[4] * x + a[5] * y + a[6] * z + a[7], gz = a[8] * x + a[9] * y + a[10] * z + a[11];
+        const double* m = g.world_to_index;
+        for (int c = 0; c < 3; ++c) out3[c] = gx * m[c] + gy * m[4 + c] + gz * m[8 + c] + m[12 + c];
+    };
+    for (int k = 0; k < n; ++k)
+        for (int j = 0; j < n; ++j)
+            for (int i = 0; i < n; ++i) {
+                double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+                for (int corner = 0; corner < 8; ++corner) {
+                    const int q[3] = {i + (corner & 1), j + (corner >> 1 & 1), k + (corner >> 2 & 1)};
+                    double w[3], ix[3];
+                    for (int a = 0; a < 3; ++a) w[a] = v.bound_lo[a] + (double(v.bound_hi[a]) - v.bound_lo[a]) * q[a] / n;
+                    toIndex(w[0], w[1], w[2], ix);
+                    for (int a = 0; a < 3; ++a) lo[a] = std::min(lo[a], ix[a]), hi[a] = std::max(hi[a], ix[a]);
+                }
+                int from[3], to[3];
+                for (int a = 0; a < 3; ++a) {
+                    from[a] = std::max(int(std::floor(lo[a])) - 1 - g.lo[a], 0);
+                    to[a] = std::min(int(std::ceil(hi[a])) + 1 - g.lo[a], g.dims[a] - 1);
+                }
+                float most = 0.0f;
+                for (int z = from[2]; z <= to[2]; ++z)
+                    for (int y = from[1]; y <= to[1]; ++y)
+                        for (int x = from[0]; x <= to[0]; ++x)
+                            most = std::max(most, g.values[(size_t(z) * g.dims[1] + size_t(y)) * g.dims[0] + size_t(x)]);
+                out[(size_t(k) * n + j) * n + i] = most * gain;
+                *largest = std::max(*largest, most * gain);
+            }
+    return out;
+}
+}  // namespace
 
 extern "C" {
 
@@ -744,6 +792,11 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
             r.densityGrid = x.density_grid;
             r.emissionGrid = x.emission_grid;
             r.interpolation = x.interpolation;
+            r.lo = V3{x.bound_lo[0], x.bound_lo[1], x.bound_lo[2]};
+            r.hi = V3{x.bound_hi[0], x.bound_hi[1], x.bound_hi[2]};
+            r.majorant = nullptr;
+            r.majorantMax = 0.0f;
+            if (!(x.gain[0] == x.gain[1] && x.gain[1] == x.gain[2])) s->greyVolumes = false;
             for (const auto& t : kBox)
                 for (int k = 0; k < 3; ++k)
                     for (int a = 0; a < 3; ++a) tris.push_back((t[k] >> a) & 1 ? x.bound_hi[a] : x.bound_lo[a]);
@@ -764,6 +817,16 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
             r.values = s->gridValues[g];
             for (int a = 0; a < 3; ++a) r.lo[a] = x.lo[a], r.dims[a] = x.dims[a];
             r.channels = x.channels;
+        }
+        // Each volume's majorant grid for the tracking estimator.
+        std::vector<std::vector<float>> majorant(d->volume_count);
+        s->majorants.assign(d->volume_count, nullptr);
+        for (uint32_t v = 0; ok && v < d->volume_count; ++v) {
+            majorant[v] = majorantGrid(d->volumes[v], d->grids, d->grid_count, &recs[v].majorantMax);
+            ok = cudaMalloc(&s->majorants[v], sizeof(float) * majorant[v].size()) == cudaSuccess;
+            if (!ok) break;
+            cudaMemcpyAsync(s->majorants[v], majorant[v].data(), sizeof(float) * majorant[v].size(), cudaMemcpyHostToDevice, st);
+            recs[v].majorant = s->majorants[v];
         }
         if (!ok) {
             setError("device allocation failed for the volumes");
@@ -834,6 +897,7 @@ int x2_scene_free(x2_scene* s) {
     cudaFree(s->volumeTris);
     cudaFree(s->grids);
     for (float* g : s->gridValues) cudaFree(g);
+    for (float* m : s->majorants) cudaFree(m);
     freeWave(s);
     cudaFree(s->out);
     cudaFree(s->outStatus);
@@ -878,6 +942,12 @@ int x2_config_set(x2_scene* s, const x2_config* c) {
     }
     if (c->volume_count && (c->max_volume_depth > 64 || c->volume_overlap_mode > kOverlapRnd || c->max_depth > 120)) {
         setError("volumes: max_volume_depth <= 64, overlap mode 0..2, max_depth <= 120");
+        return X2_EINVAL;
+    }
+    if (c->volume_estimator > 1 ||
+        (c->volume_estimator == 1 && c->volume_count &&
+         (!s->greyVolumes || c->max_volume_depth > 1 || c->volume_overlap_mode == kOverlapRnd))) {
+        setError("volume_estimator: 0 (march) or 1 (tracking: grey extinction, max_volume_depth <= 1, overlap sum or max)");
         return X2_EINVAL;
     }
     s->config = *c;

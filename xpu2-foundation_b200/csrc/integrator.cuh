@@ -34,6 +34,7 @@ struct SampleOut {
 }  // namespace x2
 
 #include "volume.cuh"
+#include "tracking.cuh"
 
 namespace x2 {
 
@@ -148,7 +149,9 @@ __device__ __forceinline__ void afterTrace(const SceneView& s, const Identity& r
     }
     V3 volumeAlphaT{1, 1, 1};
     if (kVolumes && s.config.volume_count) {
-        const V3 volumeLight = volumeRadiance(s, root, pv, pv.origin, pv.dir, pv.nearT, hit.geom == ~0u ? pv.farT : hit.t, volumeAlphaT);
+        const float tEnd = hit.geom == ~0u ? pv.farT : hit.t;
+        const V3 volumeLight = s.config.volume_estimator == 1 ? volumeRadianceTracked(s, root, pv, pv.origin, pv.dir, pv.nearT, tEnd, volumeAlphaT)
+                                                              : volumeRadiance(s, root, pv, pv.origin, pv.dir, pv.nearT, tEnd, volumeAlphaT);
         radiance = add(radiance, volumeLight);
     }
     // A camera ray that hits nothing: the volumes' opacity (none without volumes: 1 - (1+1+1)/3); a hit adds one (its
@@ -292,7 +295,8 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
                 Identity tid = lid;
                 tid.branch = childBranch(lightAddress, si, 0xfffb);
                 Stream vs(tid, pv.depth, 0);
-                t = mulv(t, volumeTransmittance(s, vs, q.origin, wi, q.near, q.far, 1.0f, int(pv.depth) + 1));
+                t = s.config.volume_estimator == 1 ? mul(t, trackedTransmittance(s, vs, q.origin, wi, q.near, q.far))
+                                                   : mulv(t, volumeTransmittance(s, vs, q.origin, wi, q.near, q.far, 1.0f, int(pv.depth) + 1));
             }
             q.contribution = t;
             q.light = i;
@@ -385,7 +389,9 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
                     Identity tid = bid;
                     tid.branch = childBranch(sampleBranch, 0xfffb, 0);
                     Stream vs(tid, pv.depth, 0);
-                    q.contribution = mulv(direct, volumeTransmittance(s, vs, origin, wi, shadowNear, shadowFar, 1.0f, int(pv.depth) + 1));
+                    q.contribution = s.config.volume_estimator == 1
+                                         ? mul(direct, trackedTransmittance(s, vs, origin, wi, shadowNear, shadowFar))
+                                         : mulv(direct, volumeTransmittance(s, vs, origin, wi, shadowNear, shadowFar, 1.0f, int(pv.depth) + 1));
                 }
                 sink.shadow(q, true);
             }

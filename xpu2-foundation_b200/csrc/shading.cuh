@@ -90,11 +90,15 @@ struct Counters {
     unsigned long long trace, nee, bsdf, held, samples, errors, overflow, pad;
 };
 // A volume on the device (x2_volume; volume::Shader's VdbVolume fields, volume_core.h:64-111) and a dense grid.
+constexpr int kMajorantCells = 32;  // a volume's majorant grid: kMajorantCells^3 over its bounds
 struct VolumeRec {
     float worldToGrid[12];
     V3 gain, colorMult, incandescence;
     float g, featureSize, surfaceThreshold;
     uint32_t densityGrid, emissionGrid, interpolation;
+    V3 lo, hi;              // its bounds (world)
+    const float* majorant;  // the largest extinction any lookup can read in each cell (the tracking estimator's)
+    float majorantMax;
 };
 struct GridRec {
     double worldToIndex[16];

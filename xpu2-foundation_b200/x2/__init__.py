@@ -98,7 +98,7 @@ class Config(C.Structure):
                 ("shadow_reuse", _U), ("volume_count", _U), ("max_volume_depth", _U), ("volume_illumination_samples", _U),
                 ("volume_overlap_mode", _U), ("volume_transmittance_threshold", _F), ("volume_attenuation_factor", _F),
                 ("volume_contribution_factor", _F), ("volume_phase_attenuation_factor", _F), ("inv_volume_quality", _F),
-                ("inv_volume_shadow_quality", _F), ("reserved", _U * 8)]
+                ("inv_volume_shadow_quality", _F), ("volume_estimator", _U), ("reserved", _U * 7)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
