@@ -312,6 +312,10 @@ def run(args):
     e2e_s = max_over_ranks(dist, time.perf_counter() - t0, local)
     e2e_value = world * samples_per_frame * args.steps / e2e_s / 1e6
 
+    # Both forms again with the kernels built with contraction (-fmad=true, as the reference's production GPU lane is
+    # built; the parity build above is -fmad=false): one frame each, in a process of its own, at N=1 only.
+    fmad = forms_with("libx2fmad.so") if world == 1 and not args.skip_plain else None
+
     # Multi-GPU: the lanes' films summed over NCCL at frame end, then the audit of the merged counts.
     if dist is not None:
         from x2 import lanes
@@ -352,6 +356,7 @@ def run(args):
                                 for k, c in (("trace", "trace"), ("shadow_nee", "shadow_nee"), ("shadow_bsdf", "shadow_bsdf"), ("held", "held"))},
             "plain_megakernel": plain,
             "wavefront_over_plain": (value / plain["value"]) if plain else None,
+            "fmad_true": fmad,
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": chunk_bytes, "d2h_bytes_per_step": film_bytes},
             "roofline": {"bound": "hbm", "kernel": "wf" + dom.capitalize(), "achieved": achieved, "peak": hbm, "unit": "GB/s",
                          "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
@@ -437,6 +442,37 @@ def probe_volume(args):
     print(json.dumps(out))
     scene.free()
     ctx.close()
+
+
+def probe_forms(args):
+    """One config-1 frame in each form (wavefront, then the plain megakernel), each after a warm-up frame, with the
+    library this process loaded (X2_LIBRARY: the contracted build libx2fmad.so when bench.py asks for it). Prints the
+    Msamples/s of each."""
+    import x2
+
+    ctx = x2.Context(0)
+    s = x2.SyntheticScene(1)
+    cfg = s.config
+    scene = x2.Scene(ctx, s.desc, cfg)
+    n = cfg.width * cfg.height * cfg.spp
+    out = {"probe": "forms", "library": os.path.basename(x2.LIBRARY)}
+    for name, wave in (("wavefront", True), ("plain", False)):
+        frame(scene, cfg, 0, wave)
+        ms = frame(scene, cfg, 0, wave).milliseconds
+        out[name] = {"ms": ms, "msamples_per_s": n / ms / 1e3}
+    print(json.dumps(out))
+    scene.free()
+    ctx.close()
+
+
+def forms_with(library):
+    """probe_forms in a process of its own that loads `library` (the x2 module loads one library a process)."""
+    env = dict(os.environ, X2_LIBRARY=os.path.join(ROOT, "xpu2-foundation_b200", "x2", library))
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--probe", "forms"], capture_output=True, text=True, env=env, timeout=900)
+    for line in r.stdout.splitlines():
+        if line.startswith("{"):
+            return json.loads(line)
+    return {"unavailable": (r.stderr or r.stdout)[-300:]}
 
 
 def probe_estimators(args):
@@ -645,6 +681,8 @@ def probe(args):
         return probe_adjoint(args)
     if args.probe == "estimators":
         return probe_estimators(args)
+    if args.probe == "forms":
+        return probe_forms(args)
     if args.probe == "rmse":
         return probe_rmse(args)
     if args.probe == "adaptive":
@@ -688,7 +726,7 @@ def main():
     ap.add_argument("--impl", default="x2", choices=["x2", "reference"])
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--skip-plain", action="store_true")
-    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint", "rmse", "adaptive", "workgrid", "estimators"], help="one bounded launch for a profiler, then exit")
+    ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint", "rmse", "adaptive", "workgrid", "estimators", "forms"], help="one bounded launch for a profiler, then exit")
     ap.add_argument("--probe-tiles", type=int, default=592)
     ap.add_argument("--probe-timed", action="store_true", help="wavefront probe without its graph (per-kernel launches)")
     ap.add_argument("--adjoint-only", action="store_true", help="adjoint probe: one primal frame, then one wavefront adjoint launch")

@@ -2,8 +2,9 @@
 because the x2 module loads one library a process. Test infrastructure for the parity investigation
 (tests/test_gpu_parity_cause.py).
 
-    python tests/diag_probe.py <scene id> <in.npz: pixels, indices> <out.npz> <mode>
+    python tests/diag_probe.py <scene id> <in.npz: pixels, indices> <out.npz> <mode> [library]
 
+mode 0: every sample as the library computes it (no diagnostic switch; any build).
 mode 1: every sample with the transcendental functions in double rounded to float -> rgba, status.
 mode 2: every sample alone, with CUDA's functions (as the product) and every call recorded -> rgba, status, and the
         records (calls: n x 5 float32 words as x2_diag_call, first: each sample's first record, count: its records).
@@ -17,7 +18,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 sys.path.insert(0, os.path.join(ROOT, "xpu2-foundation_b200"))
-os.environ["X2_LIBRARY"] = os.path.join(ROOT, "xpu2-foundation_b200", "x2", "libx2diag.so")
+# The library: the diagnostic build, or the one a sixth argument names (e.g. libx2fmad.so, the contracted build).
+LIB = sys.argv[5] if len(sys.argv) > 5 else "libx2diag.so"
+os.environ["X2_LIBRARY"] = os.path.join(ROOT, "xpu2-foundation_b200", "x2", LIB)
 
 import x2  # noqa: E402
 
@@ -28,6 +31,8 @@ def main(scene_id, src, dst, mode):
     import torch
 
     lib = x2.library()
+    if mode == 0:
+        return plain(scene_id, src, dst)
     lib.x2_diag_set.argtypes = [C.c_int, C.c_void_p, C.c_uint32]
     lib.x2_diag_set.restype = C.c_int
     lib.x2_diag_count.argtypes = [C.POINTER(C.c_uint32)]
@@ -61,6 +66,19 @@ def main(scene_id, src, dst, mode):
         out.update(rgba=rgba, status=status, calls=np.concatenate(calls) if calls else np.zeros(0, CALL_DTYPE),
                    first=np.array(first, np.int64), count=np.array(count, np.int64))
     np.savez(dst, pixels=pixels, indices=indices, **out)
+    scene.free()
+    s.free()
+    ctx.close()
+
+
+def plain(scene_id, src, dst):
+    f = np.load(src)
+    pixels, indices = f["pixels"].astype(np.uint32), f["indices"].astype(np.uint32)
+    ctx = x2.Context(0)
+    s = x2.SyntheticScene(scene_id)
+    scene = x2.Scene(ctx, s.desc, s.config)
+    rgba, status = scene.integrate(pixels, indices)
+    np.savez(dst, pixels=pixels, indices=indices, rgba=rgba, status=status)
     scene.free()
     s.free()
     ctx.close()

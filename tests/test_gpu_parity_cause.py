@@ -35,11 +35,11 @@ def within(a, b, rtol=RTOL, atol=ATOL):
     return np.abs(a - b) <= rtol * np.abs(b) + atol
 
 
-def diag(scene_id, pixels, indices, mode, tmp_path):
+def diag(scene_id, pixels, indices, mode, tmp_path, library="libx2diag.so"):
     src, dst = str(tmp_path / f"in{mode}.npz"), str(tmp_path / f"out{mode}.npz")
     np.savez(src, pixels=np.asarray(pixels, np.uint32), indices=np.asarray(indices, np.uint32))
-    r = subprocess.run([sys.executable, os.path.join(HERE, "diag_probe.py"), str(scene_id), src, dst, str(mode)], capture_output=True,
-                       text=True, timeout=1200)
+    r = subprocess.run([sys.executable, os.path.join(HERE, "diag_probe.py"), str(scene_id), src, dst, str(mode), library],
+                       capture_output=True, text=True, timeout=1200)
     assert r.returncode == 0, r.stdout + r.stderr
     return np.load(dst)
 
@@ -108,3 +108,21 @@ def test_outliers_replayed_with_device_values(ctx, cid, tmp_path):
                        ("none" if event is None else "the device's path has more events")))
         assert within(got, rgba[i], 1e-5, 1e-7).all(), rows[-1]
     print(f"config {cid}: {len(out)} outliers, each reproduced by the reference with the device's function values\n" + "\n".join(rows))
+
+
+@pytest.mark.parametrize("cid", [108, 0])
+def test_contracted_build_within_tolerance(ctx, cid, tmp_path):
+    """The build with contraction (libx2fmad.so: the render and wavefront kernels with -fmad=true, as the reference's
+    production GPU lane is built) against the reference integrator on the same 60,000 samples: every status equal and
+    the share within 1e-4 reported; contraction moves the triangle test's and shading's roundings, so a few samples
+    take another discrete decision (bar: 99 %)."""
+    s = x2.SyntheticScene(cid)
+    px, idx = oracle_lib.sample_pairs(s.config, 60000, 1000 + cid)
+    ref = oracle_lib.Reference(s)
+    want, wstatus = ref.integrate(px, idx)
+    d = diag(cid, px, idx, 0, tmp_path, library="libx2fmad.so")
+    ok = within(d["rgba"], want).all(1)
+    print(f"config {cid}: contracted build, {ok.mean() * 100:.4f} % of {len(ok)} samples within 1e-4; statuses equal: "
+          f"{bool(np.array_equal(d['status'], wstatus))}")
+    assert (d["status"] == wstatus).mean() >= 0.999
+    assert ok.mean() >= 0.99

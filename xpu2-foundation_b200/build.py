@@ -13,6 +13,10 @@ OUT = os.path.join(HERE, "x2", "libx2.so")
 # The diagnostic build (parity investigation only, never the product): render.cu compiled with -DX2_DIAG (mathfn.cuh:
 # transcendental functions in double on request, and a record of every call), linked with the product's other objects.
 DIAG_OUT = os.path.join(HERE, "x2", "libx2diag.so")
+# The contracted build (a measurement, never the product): the render and wavefront kernels compiled with -fmad=true,
+# as the reference's production GPU lane is built, to report that speed beside the parity build's.
+FMAD_OUT = os.path.join(HERE, "x2", "libx2fmad.so")
+FMAD_CU = ["render.cu", "wavefront.cu"]
 BUILD = os.path.join(HERE, "_build")
 CU = ["api.cu", "render.cu", "wavefront.cu", "bvh_build.cu", "noalloc.cu", "adjoint.cu", "adaptive.cu", "scores.cu", "probe.cu"]
 CPP = ["scene_gen.cpp", "grid.cpp"]
@@ -65,6 +69,19 @@ def build(verbose=False, force=False):
     diag_objs = [diag if o.endswith(os.sep + "render.cu.o") else o for o in objs]
     if force or _stale(DIAG_OUT, diag_objs):
         _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", DIAG_OUT] + diag_objs + ["-lcudart_static"])
+    fmad_objs = []
+    for o in objs:
+        name = os.path.basename(o)[:-2]  # "<file>.cu"
+        if name in FMAD_CU:
+            fo = os.path.join(BUILD, name + ".fmad.o")
+            src = os.path.join(CSRC, name)
+            if force or _stale(fo, [src] + headers):
+                _run([NVCC] + ARCH + [f if f != "-fmad=false" else "-fmad=true" for f in FLAGS] + ["-rdc=false", "-c", src, "-o", fo])
+            fmad_objs.append(fo)
+        else:
+            fmad_objs.append(o)
+    if force or _stale(FMAD_OUT, fmad_objs):
+        _run([NVCC] + ARCH + ["-shared", "-Xcompiler", "-fPIC", "-o", FMAD_OUT] + fmad_objs + ["-lcudart_static"])
     return OUT
 
 
