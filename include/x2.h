@@ -261,7 +261,11 @@ typedef struct x2_wavefront_shape {
     uint32_t lobe_queues;    /* 1: shade takes the extended paths from per-lobe queues (GGX, Lambert, then none or
                                 missed), sorted after extend, so a warp runs one lobe's code; 0: in the extend queue's
                                 order */
-    uint32_t reserved[3];
+    uint32_t shadow_order;   /* 1: the shadow queue by record (record k of every path together, mostly one light's rays
+                                to neighbouring origins); 0: by path (each path's records together) */
+    uint32_t extend_bins;    /* 1: the extend queue binned by the rays' direction octant (a warp's rays share their
+                                children's near-to-far order); 0: in path-slot order */
+    uint32_t reserved[1];
 } x2_wavefront_shape;
 void x2_wavefront_shape_defaults(x2_wavefront_shape* shape);
 int x2_wavefront_tune(x2_scene* scene, const x2_wavefront_shape* shape);

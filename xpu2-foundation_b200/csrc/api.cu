@@ -89,8 +89,8 @@ int waitEvent(cudaEvent_t e, int timeoutMs) {
 constexpr int kSlots = 2;  // launches in flight, as GpuLane keeps (async_gpu.h:1425)
 constexpr uint32_t kQueueLog = 4096;
 // extend count, last extend count, shadow count, extend fetch, shadow fetch, 3 shade queue counts, then the shadow
-// queue's record segments (x2::kRecordSegments)
-constexpr int kWaveCounters = 8 + int(x2::kRecordSegments);
+// queue's record segments (x2::kRecordSegments), then the extend queue's octant bins (x2::kOctants)
+constexpr int kWaveCounters = 8 + int(x2::kRecordSegments) + int(x2::kOctants);
 
 struct Slot {
     bool busy = false;
@@ -219,6 +219,8 @@ struct x2_scene {
     uint32_t traceBlocks = kDefaultTraceBlocks, shadeBlocks = kDefaultShadeBlocks;  // occupancy variants
     uint32_t triLimit = kDefaultTriLimit;  // triangle tests a traversal step
     uint32_t lobeQueues = 1;               // shade from per-lobe queues (wfSortShade)
+    uint32_t shadowOrder = kDefaultShadowOrder;  // the shadow queue by record (1) or by path (0)
+    uint32_t extendBins = kDefaultExtendBins;    // the extend queue binned by octant (1) or in slot order (0)
     uint32_t* shadeQ = nullptr;            // the per-lobe queues: 3 x wavePaths entries
     uint32_t batchWindow = 0;              // x2_render_batch: items a window (0: the default)
     uint32_t* hostLast = nullptr;      // pinned
@@ -367,7 +369,7 @@ int ensureWave(x2_scene* s, uint32_t paths, uint32_t records) {
               cudaMalloc(&w.state, sizeof(uint32_t) * P) == cudaSuccess && cudaMalloc(&w.item, sizeof(uint32_t) * P) == cudaSuccess &&
               cudaMalloc(&w.ncount, sizeof(uint32_t) * P) == cudaSuccess && cudaMalloc(&w.sray0, sizeof(float4) * R) == cudaSuccess &&
               cudaMalloc(&w.sray1, sizeof(float4) * R) == cudaSuccess && cudaMalloc(&w.scontrib, sizeof(float4) * R) == cudaSuccess &&
-              cudaMalloc(&w.svis, R) == cudaSuccess && cudaMalloc(&s->extendQ, sizeof(uint32_t) * P) == cudaSuccess &&
+              cudaMalloc(&w.svis, R) == cudaSuccess && cudaMalloc(&s->extendQ, sizeof(uint32_t) * kOctants * P) == cudaSuccess &&
               cudaMalloc(&s->shadowQ, sizeof(uint32_t) * R) == cudaSuccess && cudaMalloc(&s->shadeQ, sizeof(uint32_t) * 3 * P) == cudaSuccess;
     if (ok && !s->waveCounters) ok = cudaMalloc(&s->waveCounters, sizeof(uint32_t) * kWaveCounters) == cudaSuccess;
     if (ok && !s->claimed) ok = cudaMalloc(&s->claimed, sizeof(unsigned long long)) == cudaSuccess;
@@ -1238,12 +1240,16 @@ void x2_wavefront_shape_defaults(x2_wavefront_shape* shape) {
     shape->shade_blocks = kDefaultShadeBlocks;
     shape->tri_limit = kDefaultTriLimit;
     shape->lobe_queues = 1;
+    shape->shadow_order = kDefaultShadowOrder;
+    shape->extend_bins = kDefaultExtendBins;
 }
 
 int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     if (!s || !shape || shape->refill < 1 || shape->refill > 32 || shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 ||
-        shape->trace_blocks > 32 || shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32 || shape->lobe_queues > 1) {
-        setError("refill is 1..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32, lobe_queues 0 or 1");
+        shape->trace_blocks > 32 || shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32 || shape->lobe_queues > 1 ||
+        shape->shadow_order > 1 || shape->extend_bins > 1) {
+        setError("refill is 1..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32, lobe_queues, "
+                 "shadow_order and extend_bins 0 or 1");
         return X2_EINVAL;
     }
     s->reservePaths = shape->paths;
@@ -1254,6 +1260,8 @@ int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     s->triLimit = shape->tri_limit;
     s->batchWindow = shape->batch_window;
     s->lobeQueues = shape->lobe_queues;
+    s->shadowOrder = shape->shadow_order;
+    s->extendBins = shape->extend_bins;
     return X2_OK;
 }
 
@@ -1274,7 +1282,8 @@ WaveArgs launchArgs(x2_scene* s, Slot& sl, uint32_t paths, uint32_t records, uns
     a.lastExtend = s->waveCounters + 1;
     a.shadowQ = s->shadowQ;
     a.shadowCount = s->waveCounters + 2;
-    a.shadowSlots = a.recordsPerPath <= x2::kRecordSegments ? s->waveCounters + 8 : nullptr;
+    a.shadowSlots = s->shadowOrder && a.recordsPerPath <= x2::kRecordSegments ? s->waveCounters + 8 : nullptr;
+    a.extendSlots = s->extendBins ? s->waveCounters + 8 + x2::kRecordSegments : nullptr;
     a.extendNext = s->waveCounters + 3;
     a.shadowNext = s->waveCounters + 4;
     a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
@@ -1706,7 +1715,8 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     a.lastExtend = s->waveCounters + 1;
     a.shadowQ = s->shadowQ;
     a.shadowCount = s->waveCounters + 2;
-    a.shadowSlots = a.recordsPerPath <= x2::kRecordSegments ? s->waveCounters + 8 : nullptr;
+    a.shadowSlots = s->shadowOrder && a.recordsPerPath <= x2::kRecordSegments ? s->waveCounters + 8 : nullptr;
+    a.extendSlots = s->extendBins ? s->waveCounters + 8 + x2::kRecordSegments : nullptr;
     a.extendNext = s->waveCounters + 3;
     a.shadowNext = s->waveCounters + 4;
     a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
@@ -2418,7 +2428,9 @@ int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefron
                           {&x2_wavefront_shape::shade_blocks, {0, 3, 4}},
                           {&x2_wavefront_shape::trace_blocks, {0, 9}},
                           {&x2_wavefront_shape::blocks_per_sm, {8, 16, 32}},
-                          {&x2_wavefront_shape::lobe_queues, {0, 1}}};
+                          {&x2_wavefront_shape::lobe_queues, {0, 1}},
+                          {&x2_wavefront_shape::shadow_order, {0, 1}},
+                          {&x2_wavefront_shape::extend_bins, {0, 1}}};
     for (const Knob& k : knobs) {
         x2_wavefront_shape keep = cur;
         for (uint32_t v : k.values) {
@@ -2573,7 +2585,8 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
         a.lastExtend = s0->waveCounters + 1;
         a.shadowQ = s0->shadowQ;
         a.shadowCount = s0->waveCounters + 2;
-        a.shadowSlots = a.recordsPerPath <= x2::kRecordSegments ? s0->waveCounters + 8 : nullptr;
+        a.shadowSlots = s0->shadowOrder && a.recordsPerPath <= x2::kRecordSegments ? s0->waveCounters + 8 : nullptr;
+        a.extendSlots = s0->extendBins ? s0->waveCounters + 8 + x2::kRecordSegments : nullptr;
         a.extendNext = s0->waveCounters + 3;
         a.shadowNext = s0->waveCounters + 4;
         a.shadeQ = s0->lobeQueues ? s0->shadeQ : nullptr;

@@ -144,6 +144,7 @@ extern "C" int x2_launch_wavefront_static(x2_scene* scene, const x2_chunk* d_chu
     a.shadowQ = reinterpret_cast<uint32_t*>(base + kShadowQ);
     a.shadowCount = queues + 2;
     a.shadowSlots = nullptr;  // the shadow queue by path
+    a.extendSlots = nullptr;  // the extend queue in slot order
     a.extendNext = queues + 3;
     a.shadowNext = queues + 4;
     a.shadeQ = nullptr;  // shade in the extend queue's order

@@ -301,10 +301,24 @@ __device__ __forceinline__ void logicBody(const WaveArgs& a) {
                 }
             }
         }
-        // The extend queue: every slot with a ray to trace.
+        // The extend queue: every slot with a ray to trace (binned: in the bin of its direction's octant).
         const bool trace = st == kTrace;
         const uint32_t slot = warpReserve(a.extendCount, trace ? 1u : 0u);
-        if (trace) a.extendQ[slot] = p;
+        if (!a.extendSlots) {
+            if (trace) a.extendQ[slot] = p;
+        } else {
+            uint32_t octant = kOctants;
+            if (trace) {
+                const float4 d = w.ray1[p];
+                octant = (signbit(d.x) ? 1u : 0u) | (signbit(d.y) ? 2u : 0u) | (signbit(d.z) ? 4u : 0u);
+            }
+            const unsigned peers = __match_any_sync(full, octant);
+            const uint32_t lane = threadIdx.x & 31u, leader = __ffs(peers) - 1;
+            uint32_t at = 0;
+            if (octant < kOctants && lane == leader) at = atomicAdd(a.extendSlots + octant, uint32_t(__popc(peers)));
+            at = __shfl_sync(peers, at, leader);
+            if (trace) a.extendQ[size_t(octant) * a.paths + at + __popc(peers & ((1u << lane) - 1u))] = p;
+        }
     }
     warpAddCounters(a.counters, 0, 0, 0, 0, samples, errors);
     if (kAdjoint) partialsEnd(partial, at, a.adj);
@@ -389,9 +403,23 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
 template <bool kBatch>
 __device__ __forceinline__ void extendBody(const WaveArgs& a) {
     __shared__ uint2 shortStacks[kShortStack * kWaveBlock];
+    __shared__ uint32_t start[kOctants + 1];
+    QueueSegments seg{start, 0, a.paths};
     const uint32_t n = *a.extendCount;
-    if (!kBatch && a.scene.stats) persistentTrace<false, true, false>(a, n, a.extendQ, a.extendNext, shortStacks);
-    else persistentTrace<false, false, kBatch>(a, n, a.extendQ, a.extendNext, shortStacks);
+    if (a.extendSlots) {
+        seg.segments = kOctants;
+        if (threadIdx.x == 0) {
+            uint32_t run = 0;
+            for (uint32_t o = 0; o < kOctants; ++o) {
+                start[o] = run;
+                run += a.extendSlots[o];
+            }
+            start[kOctants] = run;
+        }
+        __syncthreads();
+    }
+    if (!kBatch && a.scene.stats) persistentTrace<false, true, false>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
+    else persistentTrace<false, false, kBatch>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters->trace, (unsigned long long)n);
 }
 
@@ -462,6 +490,18 @@ struct WaveSink {
     }
 };
 
+// Entry i of the extend queue, its bins read in octant order when it is binned.
+__device__ __forceinline__ uint32_t extendAt(const WaveArgs& a, uint32_t i) {
+    if (!a.extendSlots) return a.extendQ[i];
+    uint32_t o = 0, start = 0;
+    for (; o + 1 < kOctants; ++o) {
+        const uint32_t c = a.extendSlots[o];
+        if (i < start + c) break;
+        start += c;
+    }
+    return a.extendQ[size_t(o) * a.paths + (i - start)];
+}
+
 // ---- sort: per-lobe shade queues ----
 // Each extended path goes to the queue of the lobe its hit's material makes (shading.cuh lobeClass: 0 Lambert, 1 GGX,
 // 2 none) or, when its ray hit nothing, to queue 2; queue order: GGX (0), Lambert (1), none or missed (2). One
@@ -477,7 +517,7 @@ __device__ __forceinline__ void sortBody(const WaveArgs& a) {
         const uint32_t i = base + threadIdx.x;
         uint32_t queue = 3, p = 0;
         if (i < n) {
-            p = a.extendQ[i];
+            p = extendAt(a, i);
             queue = 2;
             const uint2 hr = w.hit[p];
             if (hr.x != ~0u) {
@@ -504,7 +544,7 @@ __global__ void __launch_bounds__(kWaveBlock) wfSortShadeBatch(WaveArgs a) { sor
 
 // The i-th path shade takes: from the per-lobe queues in their order when they are on, else the extend queue's.
 __device__ __forceinline__ uint32_t shadeEntry(const WaveArgs& a, uint32_t i, uint32_t c0, uint32_t c1) {
-    if (!a.shadeQ) return a.extendQ[i];
+    if (!a.shadeQ) return extendAt(a, i);
     if (i < c0) return a.shadeQ[i];
     if (i < c0 + c1) return a.shadeQ[a.paths + (i - c0)];
     return a.shadeQ[2ull * a.paths + (i - c0 - c1)];
@@ -704,6 +744,8 @@ __global__ void wfResetQueues(WaveArgs a) {
         *a.extendNext = 0;
         if (a.shadowSlots)
             for (uint32_t k = 0; k < a.recordsPerPath; ++k) a.shadowSlots[k] = 0;
+        if (a.extendSlots)
+            for (uint32_t o = 0; o < kOctants; ++o) a.extendSlots[o] = 0;
         *a.shadowNext = 0;
         if (a.shadeQ) a.shadeCount[0] = a.shadeCount[1] = a.shadeCount[2] = 0;
     }

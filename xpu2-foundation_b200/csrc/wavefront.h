@@ -8,7 +8,8 @@ constexpr int kWaveBlock = 128;
 constexpr uint32_t kRecordSegments = 64;
 // Launch-shape defaults (x2_wavefront_tune changes them a scene).
 constexpr uint32_t kDefaultRefill = 8, kDefaultBlocksPerSm = 16, kDefaultTraceBlocks = 0, kDefaultShadeBlocks = 4,
-                   kDefaultTriLimit = 1;
+                   kDefaultTriLimit = 1, kDefaultShadowOrder = 1, kDefaultExtendBins = 0;
+constexpr uint32_t kOctants = 8;
 
 // Path slots (structure of arrays, `paths` slots) and shadow-ray records (recordsPerPath a slot).
 struct WaveState {
@@ -56,6 +57,9 @@ struct WaveArgs {
     unsigned long long* claimed;
     uint32_t* extendQ;
     uint32_t* extendCount;
+    // The extend queue binned by direction octant (null: one queue in slot order): the rays of octant o at
+    // extendQ + o * paths, extendSlots[o] of them (extendCount their total).
+    uint32_t* extendSlots;
     uint32_t* lastExtend;
     uint32_t* shadowQ;
     uint32_t* shadowCount;
