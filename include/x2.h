@@ -265,7 +265,7 @@ typedef struct x2_wavefront_shape {
                                 to neighbouring origins); 0: by path (each path's records together) */
     uint32_t extend_bins;    /* 1: the extend queue binned by the rays' direction octant (a warp's rays share their
                                 children's near-to-far order); 0: in path-slot order */
-    uint32_t reserved[1];
+    uint32_t short_stack;    /* 1: the traversal stacks' first 8 entries in shared memory; 0: all in local memory */
 } x2_wavefront_shape;
 void x2_wavefront_shape_defaults(x2_wavefront_shape* shape);
 int x2_wavefront_tune(x2_scene* scene, const x2_wavefront_shape* shape);

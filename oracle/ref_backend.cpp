@@ -123,7 +123,14 @@ struct OracleTextures {
     unsigned lookup(unsigned texture, xi::tex::Binding b, const xi::tex::Footprint& f, V3& out) const {
         if (texture >= s->images.size()) return xi::tex::Invalid;
         b.image = &s->images[texture];
+#ifdef X2REF_REPLAY
+        const unsigned status = xi::tex::lookup(b, f, out);
+        replay::event(3, b.mode, f.u, f.v, out.x, out.y);
+        replay::event(4, status, out.z, 0.0f, 0.0f, 0.0f);
+        return status;
+#else
         return xi::tex::lookup(b, f, out);
+#endif
     }
 };
 

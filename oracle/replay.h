@@ -42,7 +42,8 @@ inline uint32_t bits(float x) {
 inline uint64_t key(uint32_t fn, float a, float b) { return (uint64_t(fn) << 56) ^ (uint64_t(bits(b)) << 24) ^ uint64_t(bits(a)); }
 
 // A backend event: kind 1 a closest hit (value: triangle or ~0u, t), kind 2 a shadow ray's visibility (value 0/1,
-// t: its far distance); x, y, z the ray's direction.
+// t: its far distance); x, y, z the ray's direction. Kind 3 a texture lookup (value: its mode, t and x: its s and t,
+// y and z: the texel's red and green) and kind 4 its rest (value: its status, t: the texel's blue).
 struct Event {
     uint32_t kind, value;
     float t, x, y, z;

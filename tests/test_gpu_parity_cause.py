@@ -106,6 +106,32 @@ def test_outliers_replayed_with_device_values(ctx, cid, tmp_path):
                     + (f"kind {int(e['kind'])} (1 hit, 2 visibility) libm {int(e['value'])} device "
                        f"{int(events[event]['value']) if event < len(events) else 'none'}" if e is not None else
                        ("none" if event is None else "the device's path has more events")))
+        # The rays on both sides in order: the device's recorded closest hits and visibilities against the reference's.
+        dev_events = table[(table["fn"] == 40) | (table["fn"] == 41)]
+        host_events = events[(events["kind"] == 1) | (events["kind"] == 2)]
+        for j in range(min(len(dev_events), len(host_events))):
+            de, he = dev_events[j], host_events[j]
+            dv = int(np.float32(de["a"]).view(np.uint32)) if de["fn"] == 40 else int(de["a"])
+            if (int(de["fn"]) - 39, dv) != (int(he["kind"]), int(he["value"])) or de["r0"] != he["x"] or de["r1"] != he["y"]:
+                rows[-1] += (f"; ray #{j} differs: device {'hit' if de['fn'] == 40 else 'visibility'} {dv} t/far {float(de['b'])!r} "
+                             f"dir ({float(de['r0'])!r}, {float(de['r1'])!r}), reference kind {int(he['kind'])} {int(he['value'])} t/far "
+                             f"{float(he['t'])!r} dir ({float(he['x'])!r}, {float(he['y'])!r})")
+                break
+        else:
+            if len(dev_events) != len(host_events):
+                rows[-1] += f"; {len(dev_events)} rays on the device, {len(host_events)} in the reference"
+        # The texture lookups on both sides in order: the device's recorded (s, t, texel) against the reference's.
+        dl = table[table["fn"] == 20]
+        hl = events[events["kind"] == 3]
+        for j in range(min(len(dl), len(hl))):
+            if (dl[j]["a"], dl[j]["b"], dl[j]["r0"], dl[j]["r1"]) != (hl[j]["t"], hl[j]["x"], hl[j]["y"], hl[j]["z"]):
+                rows[-1] += (f"; texture lookup #{j} differs: device st ({float(dl[j]['a'])!r}, {float(dl[j]['b'])!r}) texel "
+                             f"({float(dl[j]['r0'])!r}, {float(dl[j]['r1'])!r}), reference mode {int(hl[j]['value'])} st "
+                             f"({float(hl[j]['t'])!r}, {float(hl[j]['x'])!r}) texel ({float(hl[j]['y'])!r}, {float(hl[j]['z'])!r})")
+                break
+        else:
+            if len(dl) != len(hl):
+                rows[-1] += f"; {len(dl)} texture lookups on the device, {len(hl)} in the reference"
         assert within(got, rgba[i], 1e-5, 1e-7).all(), rows[-1]
     print(f"config {cid}: {len(out)} outliers, each reproduced by the reference with the device's function values\n" + "\n".join(rows))
 

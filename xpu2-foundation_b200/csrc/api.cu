@@ -221,6 +221,7 @@ struct x2_scene {
     uint32_t lobeQueues = 1;               // shade from per-lobe queues (wfSortShade)
     uint32_t shadowOrder = kDefaultShadowOrder;  // the shadow queue by record (1) or by path (0)
     uint32_t extendBins = kDefaultExtendBins;    // the extend queue binned by octant (1) or in slot order (0)
+    uint32_t shortStack = kDefaultShortStack;    // traversal stacks' top entries in shared memory (1) or local (0)
     uint32_t* shadeQ = nullptr;            // the per-lobe queues: 3 x wavePaths entries
     uint32_t batchWindow = 0;              // x2_render_batch: items a window (0: the default)
     uint32_t* hostLast = nullptr;      // pinned
@@ -1242,14 +1243,15 @@ void x2_wavefront_shape_defaults(x2_wavefront_shape* shape) {
     shape->lobe_queues = 1;
     shape->shadow_order = kDefaultShadowOrder;
     shape->extend_bins = kDefaultExtendBins;
+    shape->short_stack = kDefaultShortStack;
 }
 
 int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     if (!s || !shape || shape->refill < 1 || shape->refill > 32 || shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 ||
         shape->trace_blocks > 32 || shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32 || shape->lobe_queues > 1 ||
-        shape->shadow_order > 1 || shape->extend_bins > 1) {
+        shape->shadow_order > 1 || shape->extend_bins > 1 || shape->short_stack > 1) {
         setError("refill is 1..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32, lobe_queues, "
-                 "shadow_order and extend_bins 0 or 1");
+                 "shadow_order, extend_bins and short_stack 0 or 1");
         return X2_EINVAL;
     }
     s->reservePaths = shape->paths;
@@ -1262,6 +1264,7 @@ int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     s->lobeQueues = shape->lobe_queues;
     s->shadowOrder = shape->shadow_order;
     s->extendBins = shape->extend_bins;
+    s->shortStack = shape->short_stack;
     return X2_OK;
 }
 
@@ -1349,7 +1352,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     const WaveArgs a = launchArgs(s, sl, paths, records, items, count);
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
-    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr);
+    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0);
     const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     if (s->waveTiming) {
         // Diagnostic form: no graph; events around every kernel, the iteration's times added once it is done.
@@ -2104,7 +2107,7 @@ int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float 
     a.liveChunks = ad.words;
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
-    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr);
+    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0);
     const uint64_t bound = maxItems * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     const uint32_t maxIter = uint32_t(std::min<uint64_t>(bound, 0xffffffffu));
 
@@ -2430,7 +2433,8 @@ int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefron
                           {&x2_wavefront_shape::blocks_per_sm, {8, 16, 32}},
                           {&x2_wavefront_shape::lobe_queues, {0, 1}},
                           {&x2_wavefront_shape::shadow_order, {0, 1}},
-                          {&x2_wavefront_shape::extend_bins, {0, 1}}};
+                          {&x2_wavefront_shape::extend_bins, {0, 1}},
+                          {&x2_wavefront_shape::short_stack, {0, 1}}};
     for (const Knob& k : knobs) {
         x2_wavefront_shape keep = cur;
         for (uint32_t v : k.values) {

@@ -446,7 +446,10 @@ struct PlainSink {
     __device__ void shadow(const ShadowReq& q, bool bsdf) {
         if (bsdf) ++out.bsdf;
         else ++out.nee;
-        if (visible(s, q.origin, q.dir, q.near, q.far)) radiance = add(radiance, q.contribution);
+        if (visible(s, q.origin, q.dir, q.near, q.far)) {
+            radiance = add(radiance, q.contribution);
+            X2_DIAG_RECORD(mf::kAdded, bsdf ? 1.0f : 0.0f, q.contribution.x, q.contribution.y, q.contribution.z);
+        }
     }
     __device__ void held() { ++out.held; }
     __device__ void vertex(uint32_t, const Bsdf&, V3, const TexHit*) {}

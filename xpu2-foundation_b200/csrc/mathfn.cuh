@@ -17,6 +17,8 @@ namespace x2 {
 namespace mf {
 
 enum : uint32_t { kSincos = 1, kExp = 2, kLog = 3, kTan = 4, kAtan2 = 5, kPow = 6, kAcos = 7, kCos = 8 };
+// Other values the diagnostic build records beside the functions' calls: a texture lookup's (s, t) and texel.
+enum : uint32_t { kTexLookup = 20, kTexLookupRest = 21, kHit = 40, kVisible = 41, kAdded = 42 };
 
 struct DiagCall {
     uint32_t fn;
@@ -25,6 +27,7 @@ struct DiagCall {
 };
 
 #ifdef X2_DIAG
+#define X2_DIAG_RECORD(fn, a, b, r0, r1) x2::mf::record(fn, a, b, r0, r1)
 static __device__ int g_mode;
 static __device__ DiagCall* g_calls;
 static __device__ uint32_t g_cap;
@@ -38,6 +41,7 @@ __device__ __forceinline__ void record(uint32_t fn, float a, float b, float r0, 
 __device__ __forceinline__ bool wide() { return g_mode & 1; }
 #define X2_MF(fn, a, b, r0, r1) record(fn, a, b, r0, r1)
 #else
+#define X2_DIAG_RECORD(fn, a, b, r0, r1) ((void)0)
 __device__ __forceinline__ constexpr bool wide() { return false; }
 #define X2_MF(fn, a, b, r0, r1) ((void)0)
 #endif

@@ -219,6 +219,7 @@ __device__ __forceinline__ Hit trace(const SceneView& s, V3 o, V3 d, float tmin,
     uint32_t leaf;
     const uint32_t tri = s.stats ? traceClosest<true>(s.bvh, r, tmin, tmax, t, &leaf, s.overflow, s.stats + 0)
                                  : traceClosest<false>(s.bvh, r, tmin, tmax, t, &leaf, s.overflow, nullptr);
+    X2_DIAG_RECORD(mf::kHit, __uint_as_float(tri), tri == ~0u ? 0.0f : t, d.x, d.y);
     if (tri == ~0u) return h;
     const float4* tp = reinterpret_cast<const float4*>(s.bvh.tris + leaf);
     const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
@@ -233,7 +234,9 @@ __device__ __forceinline__ Hit trace(const SceneView& s, V3 o, V3 d, float tmin,
 }
 __device__ __forceinline__ bool visible(const SceneView& s, V3 o, V3 d, float near, float far) {
     const RayQ r = makeRay(s.bvh, o.x, o.y, o.z, d.x, d.y, d.z);
-    return !(s.stats ? traceAny<true>(s.bvh, r, near, far, s.overflow, s.stats + 1) : traceAny<false>(s.bvh, r, near, far, s.overflow, nullptr));
+    const bool v = !(s.stats ? traceAny<true>(s.bvh, r, near, far, s.overflow, s.stats + 1) : traceAny<false>(s.bvh, r, near, far, s.overflow, nullptr));
+    X2_DIAG_RECORD(mf::kVisible, v ? 1.0f : 0.0f, far, d.x, d.y);
+    return v;
 }
 
 // ---------------------------------------------------------------------------------------------------------------
@@ -398,6 +401,8 @@ __device__ __forceinline__ bool texLookup(const SceneView& s, uint32_t texture, 
             }
         }
     }
+    X2_DIAG_RECORD(mf::kTexLookup, h.s, h.t, h.texel.x, h.texel.y);
+    X2_DIAG_RECORD(mf::kTexLookupRest, float(h.primary), 0.0f, h.texel.z, 0.0f);
     return finite3(h.texel);
 }
 

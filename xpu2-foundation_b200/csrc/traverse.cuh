@@ -242,12 +242,13 @@ static __device__ __noinline__ uint32_t traceClosest(const Bvh8 bvh, const RayQ&
 // the next ray of the queue (persistent threads with dynamic ray fetch; Aila and Laine 2009). The steps visit the
 // same nodes and test the same triangles, in the same order, as traceClosest / traceAny, so the results are the same.
 //
-// The stack's first kShortStack entries live in shared memory, entry-major (entry e of thread t at
-// shortStack[e * blockDim.x + t], so a warp's accesses fall in distinct banks); deeper entries, which an 8-wide tree
-// rarely needs, go to the thread's local array.
+// The stack's first kShort entries may live in shared memory, entry-major (entry e of thread t at
+// shortStack[e * blockDim.x + t], so a warp's accesses fall in distinct banks), the deeper ones in the thread's local
+// array; with kShort 0 all of them are local (the shared memory then stays L1's).
 constexpr int kShortStack = 8;
+template <int kShort>
 struct Walk {
-    uint2 deep[kStack - kShortStack];
+    uint2 deep[kStack - kShort];
     uint2* shortStack;  // this thread's column: entry e at shortStack[e * blockDim.x]
     int sp;
     uint32_t base, bits, imask;  // the node group being visited: its child base, hit mask, internal-child mask
@@ -257,22 +258,24 @@ struct Walk {
     uint32_t nodes, tris;        // counting mode
 };
 
-__device__ __forceinline__ void walkPush(Walk& w, uint2 e, uint32_t* overflow) {
-    if (w.sp < kShortStack) w.shortStack[size_t(w.sp) * blockDim.x] = e;
-    else if (w.sp < kStack) w.deep[w.sp - kShortStack] = e;
+template <int kShort>
+__device__ __forceinline__ void walkPush(Walk<kShort>& w, uint2 e, uint32_t* overflow) {
+    if (w.sp < kShort) w.shortStack[size_t(w.sp) * blockDim.x] = e;
+    else if (w.sp < kStack) w.deep[w.sp - kShort] = e;
     else {
         atomicAdd(overflow, 1u);
         return;
     }
     ++w.sp;
 }
-__device__ __forceinline__ uint2 walkPop(Walk& w) {
+template <int kShort>
+__device__ __forceinline__ uint2 walkPop(Walk<kShort>& w) {
     --w.sp;
-    return w.sp < kShortStack ? w.shortStack[size_t(w.sp) * blockDim.x] : w.deep[w.sp - kShortStack];
+    return w.sp < kShort ? w.shortStack[size_t(w.sp) * blockDim.x] : w.deep[w.sp - kShort];
 }
 
-template <bool kAny>
-__device__ __forceinline__ void walkStart(Walk& w, const RayQ& r, float tmin, float tmax) {
+template <bool kAny, int kShort>
+__device__ __forceinline__ void walkStart(Walk<kShort>& w, const RayQ& r, float tmin, float tmax) {
     w.sp = 0;
     w.base = 0;
     w.bits = 0x80000000u;
@@ -288,8 +291,8 @@ __device__ __forceinline__ void walkStart(Walk& w, const RayQ& r, float tmin, fl
 // One step: a node visit (when no triangles are pending) and then at most `triLimit` triangle tests, the rest left
 // for the next steps, so that a lane with a full leaf does not hold its warp for all of them at once. The tests run
 // in the same order whatever the limit. True once the ray is done.
-template <bool kAny>
-__device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk& w, uint32_t* overflow, uint32_t triLimit) {
+template <bool kAny, int kShort>
+__device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk<kShort>& w, uint32_t* overflow, uint32_t triLimit) {
     if (!w.tbits) {
         if (!(w.bits & 0xff000000u)) {
             if (w.sp == 0) return true;

@@ -346,7 +346,7 @@ struct QueueSegments {
 };
 
 // shortStacks: the block's kShortStack x kWaveBlock short traversal stacks (shared memory).
-template <bool kAny, bool kStats, bool kBatch>
+template <bool kAny, bool kStats, bool kBatch, int kShort>
 __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, const uint32_t* __restrict__ queue, uint32_t* next,
                                                 uint2* shortStacks, const QueueSegments seg = QueueSegments{nullptr, 0, 0}) {
     const WaveState& w = a.w;
@@ -354,7 +354,7 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
     uint32_t* overflow = a.scene.overflow;
     const unsigned full = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u;
-    Walk walk;
+    Walk<kShort> walk;
     walk.shortStack = shortStacks + threadIdx.x;
     walk.nodes = walk.tris = 0;
     RayQ r;
@@ -379,14 +379,14 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
                     }
                     const float4 r0 = kAny ? w.sray0[k] : w.ray0[k], r1 = kAny ? w.sray1[k] : w.ray1[k];
                     r = makeRay(bvh, r0.x, r0.y, r0.z, r1.x, r1.y, r1.z);
-                    walkStart<kAny>(walk, r, r0.w, r1.w);
+                    walkStart<kAny, kShort>(walk, r, r0.w, r1.w);
                     live = true;
                     ++rays;
                 }
             }
         }
         if (!__any_sync(full, live)) break;
-        if (live && walkStep<kAny>(bvh, r, walk, overflow, a.triLimit)) {
+        if (live && walkStep<kAny, kShort>(bvh, r, walk, overflow, a.triLimit)) {
             if (kAny) w.svis[k] = walk.best ? 0 : 1;
             else w.hit[k] = make_uint2(walk.best == ~0u ? ~0u : walk.bestLeaf, __float_as_uint(walk.tmax));
             live = false;
@@ -400,9 +400,9 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
     }
 }
 
-template <bool kBatch>
+template <bool kBatch, int kShort = kShortStack>
 __device__ __forceinline__ void extendBody(const WaveArgs& a) {
-    __shared__ uint2 shortStacks[kShortStack * kWaveBlock];
+    __shared__ uint2 shortStacks[kShort > 0 ? kShort * kWaveBlock : 1];
     __shared__ uint32_t start[kOctants + 1];
     QueueSegments seg{start, 0, a.paths};
     const uint32_t n = *a.extendCount;
@@ -418,8 +418,8 @@ __device__ __forceinline__ void extendBody(const WaveArgs& a) {
         }
         __syncthreads();
     }
-    if (!kBatch && a.scene.stats) persistentTrace<false, true, false>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
-    else persistentTrace<false, false, kBatch>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
+    if (!kBatch && a.scene.stats) persistentTrace<false, true, false, kShort>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
+    else persistentTrace<false, false, kBatch, kShort>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters->trace, (unsigned long long)n);
 }
 
@@ -658,7 +658,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
 }
 
 // ---- shadow: any hits ----
-template <bool kBatch>
+template <bool kBatch, int kShort = kShortStack>
 __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
     __shared__ uint32_t start[kRecordSegments + 1];
     QueueSegments seg{start, 0, a.paths};
@@ -676,9 +676,9 @@ __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
         __syncthreads();
         n = start[seg.segments];
     }
-    __shared__ uint2 shortStacks[kShortStack * kWaveBlock];
-    if (!kBatch && a.scene.stats) persistentTrace<true, true, false>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
-    else persistentTrace<true, false, kBatch>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
+    __shared__ uint2 shortStacks[kShort > 0 ? kShort * kWaveBlock : 1];
+    if (!kBatch && a.scene.stats) persistentTrace<true, true, false, kShort>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
+    else persistentTrace<true, false, kBatch, kShort>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
 }
 
 // The kernels, each in a few occupancy variants (blocks of kWaveBlock threads a SM that the register allocation must
@@ -699,6 +699,9 @@ __global__ void wfGradRows(const float* rows, uint32_t rowCount, uint32_t params
     grads[i] += sum;
 }
 __global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) { shadowBody<false>(a); }
+// The traversal kernels with their whole stacks in local memory (wavefront shape short_stack 0).
+__global__ void __launch_bounds__(kWaveBlock) wfExtendLocal(WaveArgs a) { extendBody<false, 0>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShadowLocal(WaveArgs a) { shadowBody<false, 0>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfExtendBatch(WaveArgs a) { extendBody<true>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadowBatch(WaveArgs a) { shadowBody<true>(a); }
 template <int kMinBlocks>
@@ -714,11 +717,11 @@ __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadowOcc(WaveArgs a
     shadowBody<false>(a);
 }
 
-WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures) {
+WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack) {
     WaveKernels k;
     k.logic = wfLogic;
-    k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : wfExtend;
-    k.shadow = traceBlocks >= 10 ? wfShadowOcc<10> : traceBlocks >= 9 ? wfShadowOcc<9> : wfShadow;
+    k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : shortStack ? wfExtend : wfExtendLocal;
+    k.shadow = traceBlocks >= 10 ? wfShadowOcc<10> : traceBlocks >= 9 ? wfShadowOcc<9> : shortStack ? wfShadow : wfShadowLocal;
     if (volumes) k.shade = wfShadeVolumes;
     else if (textures) k.shade = wfShadeOcc<4, false, true>;
     else k.shade = shadeBlocks >= 4 ? wfShadeOcc<4, false> : shadeBlocks >= 3 ? wfShadeOcc<3, false> : wfShade;

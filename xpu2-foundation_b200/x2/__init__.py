@@ -118,8 +118,8 @@ class Request(C.Structure):
 
 class WavefrontShape(C.Structure):
     FIELDS = ("paths", "refill", "blocks_per_sm", "trace_blocks", "shade_blocks", "tri_limit", "batch_window", "lobe_queues",
-              "shadow_order", "extend_bins")
-    _fields_ = [(f, C.c_uint32) for f in FIELDS] + [("reserved", C.c_uint32 * 1)]
+              "shadow_order", "extend_bins", "short_stack")
+    _fields_ = [(f, C.c_uint32) for f in FIELDS]
 
     def as_dict(self):
         return {k: int(getattr(self, k)) for k in self.FIELDS}
