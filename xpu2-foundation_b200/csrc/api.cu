@@ -708,6 +708,9 @@ int x2_scene_load(x2_ctx* ctx, const x2_scene_desc* d, x2_scene** out) {
     }
     bool textured = false;
     for (uint32_t i = 0; i < d->material_count; ++i) textured = textured || d->materials[i].diffuse_texture != 0;
+    // A scene with texture coordinates keeps them on the device even without a texture: they set the hits' partial
+    // derivatives, as the reference binds them for every mesh.
+    textured = textured || d->uvs != nullptr;
     cudaEvent_t b0, b1;
     cudaEventCreate(&b0);
     cudaEventCreate(&b1);

@@ -184,7 +184,10 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
     const uint32_t policy = c.sampling;
     const bool volumes = kVolumes && c.volume_count;
     State st;
-    if (!hitState(va, vb, vc, hit.u, hit.v, hit.point, pv.dir, st)) return false;
+    // A mesh's texture coordinates set its partial derivatives (the reference binds them for every mesh of a scene that
+    // has them); the device keeps them for scenes with textures.
+    const float* stCoords = kTextures && s.triUV ? s.triUV + 6ull * (__ldg(s.meshFirst + hit.geom) + hit.prim) : nullptr;
+    if (!hitState(va, vb, vc, hit.u, hit.v, hit.point, pv.dir, st, stCoords)) return false;
     Bsdf bsdf;
     const uint32_t material = __ldg(s.meshMaterial + hit.geom);
     const MaterialRec& mr = s.materials[material];
@@ -437,11 +440,16 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
 }
 
 // The plain megakernel's sink: shadow rays traced at once, children on the thread's pending stack.
+// The pending stack's top entry lives in registers (topSlot, hasTop) and the rest in `stack`, so a path that never
+// branches (one BSDF sample of one lobe: every admitted wavefront scene) touches no local memory for its pending rays;
+// the order is the stack's, last pushed first popped.
 struct PlainSink {
     const SceneView& s;
     V3& radiance;
     Pending* stack;
     uint32_t& size;
+    Pending& topSlot;
+    bool& hasTop;
     SampleOut& out;
     __device__ void shadow(const ShadowReq& q, bool bsdf) {
         if (bsdf) ++out.bsdf;
@@ -453,8 +461,12 @@ struct PlainSink {
     }
     __device__ void held() { ++out.held; }
     __device__ void vertex(uint32_t, const Bsdf&, V3, const TexHit*) {}
-    __device__ uint32_t top(uint32_t) const { return size; }
-    __device__ void push(const Pending& p) { stack[size++] = p; }
+    __device__ uint32_t top(uint32_t) const { return size + (hasTop ? 1u : 0u); }
+    __device__ void push(const Pending& p) {
+        if (hasTop) stack[size++] = topSlot;
+        topSlot = p;
+        hasTop = true;
+    }
 };
 
 // integratePaths for one sample (pixel, index): the plain megakernel's whole path loop on one thread.
@@ -471,14 +483,23 @@ static __device__ __noinline__ void integrate(const SceneView& s, uint32_t pixel
     }
     const Identity root{pixel, U64(index), U64(c.seed), 0};
     Pending stack[kMaxPending];
-    uint32_t top = 0;
-    cameraPending(camera, stack[top++]);
+    uint32_t size = 0;
+    Pending topSlot;
+    bool hasTop = true;
+    cameraPending(camera, topSlot);
     const V3 cameraPosition = camera.origin;
     V3 radiance{0, 0, 0};
     float alpha = 0.0f;
-    PlainSink sink{s, radiance, stack, top, out};
-    while (top) {
-        Pending pv = stack[--top];
+    PlainSink sink{s, radiance, stack, size, topSlot, hasTop, out};
+    while (hasTop || size) {
+        Pending pv;
+        if (hasTop) {
+            pv = topSlot;
+            hasTop = false;
+        } else {
+            pv = stack[--size];
+        }
+        const uint32_t top = size;  // the pending stack's size after the pop
         V3 va, vb, vc;
         const Hit hit = trace(s, pv.origin, pv.dir, pv.nearT, pv.farT, va, vb, vc);
         ++out.trace;

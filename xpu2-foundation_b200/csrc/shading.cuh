@@ -267,8 +267,11 @@ __device__ __forceinline__ float differenceOfProducts(float a, float b, float c,
     return dop + err;
 }
 // computeTrianglePartials at the default st (0,0), (1,0), (1,1) (shade_material.h:102-116).
-__device__ __forceinline__ bool trianglePartials(V3 x0, V3 x1, V3 x2, V3& dPds) {
-    const float A0 = 1.0f - 0.0f, A1 = 0.0f - 0.0f, A2 = 1.0f - 0.0f, A3 = 1.0f - 0.0f;
+// st: the triangle's three texture coordinates (s, t each), or null for the reference's default (0, 0), (1, 0), (1, 1)
+// of a mesh without them.
+__device__ __forceinline__ bool trianglePartials(V3 x0, V3 x1, V3 x2, const float* st, V3& dPds) {
+    const float A0 = st ? st[2] - st[0] : 1.0f - 0.0f, A1 = st ? st[3] - st[1] : 0.0f - 0.0f;
+    const float A2 = st ? st[4] - st[0] : 1.0f - 0.0f, A3 = st ? st[5] - st[1] : 1.0f - 0.0f;
     const V3 b0 = sub(x1, x0), b1 = sub(x2, x0);
     const float det = differenceOfProducts(A0, A3, A1, A2);
     if (!(fabsf(det) >= 1.17549435e-38f) || !(fabsf(det) <= 3.402823466e38f)) return false;
@@ -284,8 +287,9 @@ struct State {
     V3 P, Ng, N, wo, dPds;
     bool entering;
 };
-// hitState for a mesh without normals or texture coordinates (shade_material.h:121-283).
-__device__ __forceinline__ bool hitState(V3 a, V3 b, V3 c, float u, float v, V3 P, V3 rayDir, State& st) {
+// hitState for a mesh without normals (shade_material.h:121-283); st: its texture coordinates (null: none), which set
+// dPds (and through it the shading frame's rounding, down to the sign of a zero normal component).
+__device__ __forceinline__ bool hitState(V3 a, V3 b, V3 c, float u, float v, V3 P, V3 rayDir, State& st, const float* stCoords = nullptr) {
     (void)u;
     (void)v;
     V3 ng = cross(sub(b, a), sub(c, a));
@@ -301,7 +305,7 @@ __device__ __forceinline__ bool hitState(V3 a, V3 b, V3 c, float u, float v, V3 
     }
     st.Ng = divs(ng, l);
     V3 N = st.Ng;
-    if (!trianglePartials(a, b, c, st.dPds)) st.dPds = frameN(N).x;
+    if (!trianglePartials(a, b, c, stCoords, st.dPds)) st.dPds = frameN(N).x;
     st.P = P;
     st.wo = neg(rayDir);
     st.entering = dot(st.Ng, rayDir) < 0.0f;
