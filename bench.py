@@ -228,6 +228,24 @@ def traffic_from_profile():
         return {}
 
 
+def simt_summary(tc):
+    """Lane use of the persistent traversal kernels from a counting launch, by ray kind: live lanes a warp step, lanes a
+    step that ran the node visit, lanes a triangle-test iteration (each of 32), node visits and triangle tests a ray."""
+    out = {}
+    for kind, name in (("closest", "extend"), ("any", "shadow")):
+        t = tc[kind]
+        l = t["lanes"]
+        if not l["steps"] or not t["rays"]:
+            continue
+        out[name] = {"live_lanes": l["live_lanes"] / l["steps"],
+                     "node_lanes": l["node_lanes"] / max(1, l["node_steps"]),
+                     "tri_lanes": l["tri_lanes"] / max(1, l["tri_steps"]),
+                     "node_steps_per_step": l["node_steps"] / l["steps"],
+                     "tri_iterations_per_step": l["tri_steps"] / l["steps"],
+                     "nodes_per_ray": t["nodes"] / t["rays"], "triangles_per_ray": t["triangles"] / t["rays"]}
+    return out
+
+
 def apply_shape(scene, spec):
     """x2_wavefront_tune with the fields named in `spec` ("k=v,k=v"), the others at their defaults."""
     if spec:
@@ -363,7 +381,7 @@ def run(args):
                          "algorithmic_bytes_per_launch": alg_bytes / launches_per_frame if launches_per_frame else None,
                          "traffic_source": prof.get("source"),
                          "algorithmic_bytes_per_frame": alg_bytes, "kernel_ms_per_frame": dom_ms,
-                         "kernel_ms_by_kind": kms, "traversal": tc,
+                         "kernel_ms_by_kind": kms, "traversal": tc, "simt": simt_summary(tc),
                          "bytes": {"node": NODE_BYTES, "triangle": TRI_BYTES, "extend_ray": EXTEND_RAY_BYTES, "shadow_ray": SHADOW_RAY_BYTES}},
             "cpu_baseline": base if base else {"value": None, "unavailable": why},
             "clocks": clk, "gpu_launches": launches_per_frame * 5 * args.steps,
@@ -699,6 +717,14 @@ def probe(args):
     chunks = np.zeros(len(sel), x2.CHUNK_DTYPE)
     chunks["tile"], chunks["first"], chunks["count"] = sel, 0, cfg.spp
     n = len(sel) * 64 * cfg.spp
+    tc = None
+    if args.probe == "wavefront" and args.probe_count:
+        scene.frame_begin(cfg.spp)
+        scene.count_traversal(True)
+        scene.launch_wavefront(chunks)
+        scene.wait()
+        tc = scene.traversal_counts()
+        scene.count_traversal(False)
     scene.frame_begin(cfg.spp)
     if args.probe == "plain":
         scene.launch(chunks)
@@ -713,6 +739,9 @@ def probe(args):
         out["wavefront"] = scene.wavefront_info()
         if args.probe_timed:
             out["queues"] = scene.wavefront_queues().tolist()  # per iteration: rays extended, shadow rays
+        if tc is not None:
+            out["traversal"] = tc
+            out["simt"] = simt_summary(tc)
     print(json.dumps(out))
     scene.free()
     ctx.close()
@@ -729,6 +758,8 @@ def main():
     ap.add_argument("--probe", choices=["plain", "wavefront", "batch", "volume", "adjoint", "rmse", "adaptive", "workgrid", "estimators", "forms"], help="one bounded launch for a profiler, then exit")
     ap.add_argument("--probe-tiles", type=int, default=592)
     ap.add_argument("--probe-timed", action="store_true", help="wavefront probe without its graph (per-kernel launches)")
+    ap.add_argument("--probe-count", action="store_true", help="wavefront probe: first an untimed counting launch (node visits, "
+                    "triangle tests, traversal lane use)")
     ap.add_argument("--adjoint-only", action="store_true", help="adjoint probe: one primal frame, then one wavefront adjoint launch")
     ap.add_argument("--shape", default="", help="wavefront launch shape fields, e.g. lobe_queues=0,refill=8 (default: the library's)")
     args = ap.parse_args()

@@ -444,6 +444,10 @@ int x2_counters_reset(x2_scene* scene);
 int x2_count_traversal(x2_scene* scene, int on);
 /* Each output is two counts: [0] closest-hit rays, [1] any-hit (shadow) rays. Waits; resets the counts. */
 int x2_traversal_counts(x2_scene* scene, uint64_t* rays, uint64_t* nodes, uint64_t* triangles);
+/* The wavefront traversal kernels' lane use in counting mode, six counts a ray kind ([0..5] closest hit, [6..11] any
+ * hit): warp steps, live lanes summed over them, steps that visited a node, lanes that visited, triangle-test
+ * iterations, lanes that tested. Waits; does not reset (x2_traversal_counts does). */
+int x2_traversal_lanes(x2_scene* scene, uint64_t* lanes);
 
 /* ---- host-side synthetic scenes (test and bench inputs, not the hot path) ----
  * config_id 0: the closed box with two boxes and a rect light; 1: heightfield + icospheres with 16 rect lights

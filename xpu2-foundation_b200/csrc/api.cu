@@ -1355,7 +1355,8 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     const WaveArgs a = launchArgs(s, sl, paths, records, items, count);
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
-    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0);
+    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0,
+                                       a.scene.stats != nullptr);
     const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     if (s->waveTiming) {
         // Diagnostic form: no graph; events around every kernel, the iteration's times added once it is done.
@@ -2110,7 +2111,8 @@ int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float 
     a.liveChunks = ad.words;
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
-    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0);
+    const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0,
+                                       a.scene.stats != nullptr);
     const uint64_t bound = maxItems * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     const uint32_t maxIter = uint32_t(std::min<uint64_t>(bound, 0xffffffffu));
 
@@ -2796,6 +2798,18 @@ int x2_traversal_counts(x2_scene* s, uint64_t* rays, uint64_t* nodes, uint64_t* 
         if (rays) rays[k] = h[k].rays;
         if (nodes) nodes[k] = h[k].nodes;
         if (triangles) triangles[k] = h[k].tris;
+    }
+    return X2_OK;
+}
+
+int x2_traversal_lanes(x2_scene* s, uint64_t* lanes) {
+    if (!s || !lanes) return X2_EINVAL;
+    if (int rc = x2_wait(s, 600000, nullptr)) return rc;
+    TraversalStats h[2]{};
+    CUDA_OR(cudaMemcpy(h, s->stats, sizeof(h), cudaMemcpyDeviceToHost), X2_ECUDA);
+    for (int k = 0; k < 2; ++k) {
+        const unsigned long long v[6] = {h[k].steps, h[k].liveLanes, h[k].nodeSteps, h[k].nodeLanes, h[k].triSteps, h[k].triLanes};
+        for (int j = 0; j < 6; ++j) lanes[6 * k + j] = v[j];
     }
     return X2_OK;
 }

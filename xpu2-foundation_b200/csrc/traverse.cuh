@@ -175,8 +175,11 @@ __device__ __forceinline__ uint32_t visitNode(const Node8* __restrict__ nodes, u
 
 // Traversal work of a counting run (node visits and triangle tests), for the roofline's algorithmic bytes. The
 // timed kernels are instantiated without it.
+// The persistent kernels also count their warps' lane use: warp steps and the live lanes in them, steps that ran the
+// node visit and the lanes that visited, triangle-test iterations and the lanes that tested.
 struct TraversalStats {
     unsigned long long rays, nodes, tris;
+    unsigned long long steps, liveLanes, nodeSteps, nodeLanes, triSteps, triLanes;
 };
 
 // Closest hit on [tmin, tmax]: the scene triangle index (~0u: none), its t and its position in leaf order.
@@ -244,11 +247,12 @@ static __device__ __noinline__ uint32_t traceClosest(const Bvh8 bvh, const RayQ&
 //
 // The stack's first kShort entries may live in shared memory, entry-major (entry e of thread t at
 // shortStack[e * blockDim.x + t], so a warp's accesses fall in distinct banks), the deeper ones in the thread's local
-// array; with kShort 0 all of them are local (the shared memory then stays L1's).
+// array `deep` (kStack - kShort entries); with kShort 0 all of them are local (the shared memory then stays L1's).
+// The local array is the caller's, not a member of Walk: an array indexed at run time keeps its whole aggregate in
+// local memory, and Walk's scalars, updated every step, must stay in registers.
 constexpr int kShortStack = 8;
 template <int kShort>
 struct Walk {
-    uint2 deep[kStack - kShort];
     uint2* shortStack;  // this thread's column: entry e at shortStack[e * blockDim.x]
     int sp;
     uint32_t base, bits, imask;  // the node group being visited: its child base, hit mask, internal-child mask
@@ -259,9 +263,9 @@ struct Walk {
 };
 
 template <int kShort>
-__device__ __forceinline__ void walkPush(Walk<kShort>& w, uint2 e, uint32_t* overflow) {
+__device__ __forceinline__ void walkPush(Walk<kShort>& w, uint2* deep, uint2 e, uint32_t* overflow) {
     if (w.sp < kShort) w.shortStack[size_t(w.sp) * blockDim.x] = e;
-    else if (w.sp < kStack) w.deep[w.sp - kShort] = e;
+    else if (w.sp < kStack) deep[w.sp - kShort] = e;
     else {
         atomicAdd(overflow, 1u);
         return;
@@ -269,9 +273,9 @@ __device__ __forceinline__ void walkPush(Walk<kShort>& w, uint2 e, uint32_t* ove
     ++w.sp;
 }
 template <int kShort>
-__device__ __forceinline__ uint2 walkPop(Walk<kShort>& w) {
+__device__ __forceinline__ uint2 walkPop(Walk<kShort>& w, const uint2* deep) {
     --w.sp;
-    return w.sp < kShort ? w.shortStack[size_t(w.sp) * blockDim.x] : w.deep[w.sp - kShort];
+    return w.sp < kShort ? w.shortStack[size_t(w.sp) * blockDim.x] : deep[w.sp - kShort];
 }
 
 template <bool kAny, int kShort>
@@ -292,11 +296,12 @@ __device__ __forceinline__ void walkStart(Walk<kShort>& w, const RayQ& r, float 
 // for the next steps, so that a lane with a full leaf does not hold its warp for all of them at once. The tests run
 // in the same order whatever the limit. True once the ray is done.
 template <bool kAny, int kShort>
-__device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk<kShort>& w, uint32_t* overflow, uint32_t triLimit) {
+__device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk<kShort>& w, uint2* deep, uint32_t* overflow,
+                                         uint32_t triLimit) {
     if (!w.tbits) {
         if (!(w.bits & 0xff000000u)) {
             if (w.sp == 0) return true;
-            const uint2 e = walkPop(w);
+            const uint2 e = walkPop(w, deep);
             w.base = e.x;
             w.bits = e.y & 0xff000000u;
             w.imask = (e.y >> 16) & 0xffu;
@@ -305,7 +310,7 @@ __device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk<kS
         w.bits &= ~(1u << (24 + b));
         const uint32_t slot = b ^ r.oct7;
         const uint32_t child = w.base + __popc(w.imask & ((1u << slot) - 1u));
-        if (w.bits & 0xff000000u) walkPush(w, make_uint2(w.base, w.bits | (w.imask << 16)), overflow);
+        if (w.bits & 0xff000000u) walkPush(w, deep, make_uint2(w.base, w.bits | (w.imask << 16)), overflow);
         uint32_t childBase, imask;
         const uint32_t hits = visitNode(bvh.nodes, child, r, w.tmin - r.eps, w.tmax + r.eps, childBase, w.tbase, imask);
         ++w.nodes;

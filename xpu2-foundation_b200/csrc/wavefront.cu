@@ -355,10 +355,12 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
     const unsigned full = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u;
     Walk<kShort> walk;
+    uint2 deep[kStack - kShort];
     walk.shortStack = shortStacks + threadIdx.x;
     walk.nodes = walk.tris = 0;
     RayQ r;
     uint32_t k = 0, rays = 0;
+    uint32_t steps = 0, liveLanes = 0, nodeSteps = 0, nodeLanes = 0, triSteps = 0, triLanes = 0;  // kStats, lane 0
     bool live = false, drained = false;
     for (;;) {
         const uint32_t idle = __ballot_sync(full, !live);
@@ -386,10 +388,27 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
             }
         }
         if (!__any_sync(full, live)) break;
-        if (live && walkStep<kAny, kShort>(bvh, r, walk, overflow, a.triLimit)) {
+        uint32_t liveMask = 0, nodeMask = 0, tris0 = walk.tris;
+        if (kStats) {
+            liveMask = __ballot_sync(full, live);
+            nodeMask = __ballot_sync(full, live && !walk.tbits && ((walk.bits & 0xff000000u) || walk.sp));
+        }
+        if (live && walkStep<kAny, kShort>(bvh, r, walk, deep, overflow, a.triLimit)) {
             if (kAny) w.svis[k] = walk.best ? 0 : 1;
             else w.hit[k] = make_uint2(walk.best == ~0u ? ~0u : walk.bestLeaf, __float_as_uint(walk.tmax));
             live = false;
+        }
+        if (kStats) {
+            const uint32_t tested = walk.tris - tris0;
+            const uint32_t most = __reduce_max_sync(full, tested), all = __reduce_add_sync(full, tested);
+            if (lane == 0) {
+                ++steps;
+                liveLanes += __popc(liveMask);
+                nodeSteps += nodeMask != 0;
+                nodeLanes += __popc(nodeMask);
+                triSteps += most;
+                triLanes += all;
+            }
         }
     }
     if (kStats) {
@@ -397,10 +416,18 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
         atomicAdd(&st->rays, (unsigned long long)rays);
         atomicAdd(&st->nodes, (unsigned long long)walk.nodes);
         atomicAdd(&st->tris, (unsigned long long)walk.tris);
+        if (lane == 0) {
+            atomicAdd(&st->steps, (unsigned long long)steps);
+            atomicAdd(&st->liveLanes, (unsigned long long)liveLanes);
+            atomicAdd(&st->nodeSteps, (unsigned long long)nodeSteps);
+            atomicAdd(&st->nodeLanes, (unsigned long long)nodeLanes);
+            atomicAdd(&st->triSteps, (unsigned long long)triSteps);
+            atomicAdd(&st->triLanes, (unsigned long long)triLanes);
+        }
     }
 }
 
-template <bool kBatch, int kShort = kShortStack>
+template <bool kBatch, int kShort = kShortStack, bool kStats = false>
 __device__ __forceinline__ void extendBody(const WaveArgs& a) {
     __shared__ uint2 shortStacks[kShort > 0 ? kShort * kWaveBlock : 1];
     __shared__ uint32_t start[kOctants + 1];
@@ -418,8 +445,7 @@ __device__ __forceinline__ void extendBody(const WaveArgs& a) {
         }
         __syncthreads();
     }
-    if (!kBatch && a.scene.stats) persistentTrace<false, true, false, kShort>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
-    else persistentTrace<false, false, kBatch, kShort>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
+    persistentTrace<false, kStats && !kBatch, kBatch, kShort>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters->trace, (unsigned long long)n);
 }
 
@@ -658,7 +684,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
 }
 
 // ---- shadow: any hits ----
-template <bool kBatch, int kShort = kShortStack>
+template <bool kBatch, int kShort = kShortStack, bool kStats = false>
 __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
     __shared__ uint32_t start[kRecordSegments + 1];
     QueueSegments seg{start, 0, a.paths};
@@ -677,8 +703,7 @@ __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
         n = start[seg.segments];
     }
     __shared__ uint2 shortStacks[kShort > 0 ? kShort * kWaveBlock : 1];
-    if (!kBatch && a.scene.stats) persistentTrace<true, true, false, kShort>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
-    else persistentTrace<true, false, kBatch, kShort>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
+    persistentTrace<true, kStats && !kBatch, kBatch, kShort>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
 }
 
 // The kernels, each in a few occupancy variants (blocks of kWaveBlock threads a SM that the register allocation must
@@ -699,6 +724,10 @@ __global__ void wfGradRows(const float* rows, uint32_t rowCount, uint32_t params
     grads[i] += sum;
 }
 __global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) { shadowBody<false>(a); }
+// Counting mode's traversal kernels (node visits, triangle tests, lane use; x2_count_traversal): kernels of their own,
+// so that the timed ones carry none of the counting's registers.
+__global__ void __launch_bounds__(kWaveBlock) wfExtendCount(WaveArgs a) { extendBody<false, kShortStack, true>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShadowCount(WaveArgs a) { shadowBody<false, kShortStack, true>(a); }
 // The traversal kernels with their whole stacks in local memory (wavefront shape short_stack 0).
 __global__ void __launch_bounds__(kWaveBlock) wfExtendLocal(WaveArgs a) { extendBody<false, 0>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadowLocal(WaveArgs a) { shadowBody<false, 0>(a); }
@@ -717,11 +746,15 @@ __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadowOcc(WaveArgs a
     shadowBody<false>(a);
 }
 
-WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack) {
+WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack, bool counting) {
     WaveKernels k;
     k.logic = wfLogic;
     k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : shortStack ? wfExtend : wfExtendLocal;
     k.shadow = traceBlocks >= 10 ? wfShadowOcc<10> : traceBlocks >= 9 ? wfShadowOcc<9> : shortStack ? wfShadow : wfShadowLocal;
+    if (counting) {
+        k.extend = wfExtendCount;
+        k.shadow = wfShadowCount;
+    }
     if (volumes) k.shade = wfShadeVolumes;
     else if (textures) k.shade = wfShadeOcc<4, false, true>;
     else k.shade = shadeBlocks >= 4 ? wfShadeOcc<4, false> : shadeBlocks >= 3 ? wfShadeOcc<3, false> : wfShade;

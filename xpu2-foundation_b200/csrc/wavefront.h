@@ -8,7 +8,7 @@ constexpr int kWaveBlock = 128;
 constexpr uint32_t kRecordSegments = 64;
 // Launch-shape defaults (x2_wavefront_tune changes them a scene).
 constexpr uint32_t kDefaultRefill = 8, kDefaultBlocksPerSm = 16, kDefaultTraceBlocks = 0, kDefaultShadeBlocks = 4,
-                   kDefaultTriLimit = 1, kDefaultShadowOrder = 1, kDefaultExtendBins = 0, kDefaultShortStack = 1;
+                   kDefaultTriLimit = 1, kDefaultShadowOrder = 0, kDefaultExtendBins = 1, kDefaultShortStack = 1;
 constexpr uint32_t kOctants = 8;
 
 // Path slots (structure of arrays, `paths` slots) and shadow-ray records (recordsPerPath a slot).
@@ -118,7 +118,10 @@ struct WaveKernels {
     void (*shade)(WaveArgs);
     void (*shadow)(WaveArgs);
 };
-WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack = kDefaultShortStack != 0);
+// counting: the traversal kernels that count node visits, triangle tests and lane use (the scene view's stats must
+// be set).
+WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack = kDefaultShortStack != 0,
+                        bool counting = false);
 WaveKernels waveKernelsBatch(bool volumes, bool textures);
 __global__ void wfSortShade(WaveArgs a);
 __global__ void wfSortShadeBatch(WaveArgs a);

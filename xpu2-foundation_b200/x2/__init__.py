@@ -189,7 +189,7 @@ def library():
         "x2_render_adaptive_budget": ([vp, u32, u32, C.c_float, u64, C.POINTER(AdaptiveResult)], i32), "x2_adaptive_planned": ([vp, vp], i32),
         "x2_counters_reset": ([vp], i32), "x2_count_traversal": ([vp, i32], i32),
         "x2_probe_bandwidth": ([vp, u32, u64, u32, C.POINTER(C.c_float)], i32),
-        "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
+        "x2_traversal_counts": ([vp, vp, vp, vp], i32), "x2_traversal_lanes": ([vp, vp], i32), "x2_scene_generate": ([u32, u64, C.POINTER(C.POINTER(SceneDesc)), C.POINTER(Config)], i32),
         "x2_scene_desc_free": ([C.POINTER(SceneDesc)], None),
         "x2_workgrid_options_defaults": ([C.POINTER(WorkGridOptions)], None),
         "x2_workgrid_create": ([u32, u32, u32, C.POINTER(WorkGridOptions), u32, vp, C.POINTER(vp)], i32),
@@ -584,8 +584,12 @@ class Scene:
     def traversal_counts(self):
         """Node visits and triangle tests of the launches made in counting mode, by ray kind."""
         r, n, t = (C.c_uint64 * 2)(), (C.c_uint64 * 2)(), (C.c_uint64 * 2)()
+        lanes = (C.c_uint64 * 12)()
+        _check(library().x2_traversal_lanes(self._h, lanes))
         _check(library().x2_traversal_counts(self._h, r, n, t))
-        return {kind: {"rays": r[k], "nodes": n[k], "triangles": t[k]} for k, kind in enumerate(("closest", "any"))}
+        names = ("steps", "live_lanes", "node_steps", "node_lanes", "tri_steps", "tri_lanes")
+        return {kind: {"rays": r[k], "nodes": n[k], "triangles": t[k], "lanes": {nm: lanes[6 * k + j] for j, nm in enumerate(names)}}
+                for k, kind in enumerate(("closest", "any"))}
 
 
 CHUNK_DTYPE = np.dtype([("tile", "<u4"), ("first", "<u4"), ("count", "<u4"), ("cell", "<u4")])
