@@ -286,6 +286,10 @@ def run(args):
     frame(scene, cfg, first, True)
     kms = scene.wavefront_timing(False)
     scene.reset_counters()
+    # The cache levels' read bandwidth on this GPU, measured here (untimed): the ceilings of the traversal kernels'
+    # node and triangle fetches, which hit L1 and L2 far more than HBM.
+    l1_gbs = ctx.probe_bandwidth(1, 96 << 10, 200)
+    l2_gbs = ctx.probe_bandwidth(2, 32 << 20, 20)
 
     # Device-timed wavefront frames.
     for _ in range(args.warmup):
@@ -340,8 +344,11 @@ def run(args):
 
         lanes.merge_and_audit(sums, counts, world * cfg.spp, device="cuda:%d" % local)
 
-    # Roofline of the dominant wavefront kernel: its algorithmic bytes (BVH nodes and triangles its rays visit, and
-    # its ray records) over its time in the per-kernel timed frame.
+    # Roofline of the dominant wavefront kernel. Its algorithmic bytes (BVH nodes and triangles its rays visit, and
+    # its ray records, counted in the counting frame) over its time in the per-kernel timed frame, against the cache
+    # level that serves them and against HBM; and its instruction issue, the limit it runs against (warp instructions
+    # a ray from the committed ncu capture, times this frame's rays, over the same time, against four issues a cycle
+    # a SM at the clock sampled during the timed frames).
     hbm, peak_kind = peaks()
     per_kernel = {
         "extend": (tc["closest"]["nodes"] * NODE_BYTES + tc["closest"]["triangles"] * TRI_BYTES + tc["closest"]["rays"] * EXTEND_RAY_BYTES,
@@ -358,6 +365,24 @@ def run(args):
     prof = traffic_from_profile().get(dom, {})
     dom_rays = tc["any" if dom == "shadow" else "closest"]["rays"]
     traffic = prof["dram_bytes_per_ray"] * dom_rays / launches_per_frame if "dram_bytes_per_ray" in prof and launches_per_frame else None
+    secs = dom_ms / 1e3 if dom_ms > 0 else float("inf")
+
+    def level(per_ray_key, peak):
+        if per_ray_key not in prof:
+            return None
+        got = prof[per_ray_key] * dom_rays / secs / 1e9
+        return {"measured_bytes_per_ray": prof[per_ray_key], "achieved": got, "peak": peak, "frac": got / peak if peak else None}
+
+    sm_mhz = clk.get("sm_mhz") or 1965.0
+    import torch
+
+    sms = torch.cuda.get_device_properties(local).multi_processor_count
+    issue_peak = 4 * sms * sm_mhz * 1e6 / 1e9  # warp instructions a second (Ginst/s): four schedulers a SM
+    issue = None
+    if "warp_inst_per_ray" in prof:
+        got = prof["warp_inst_per_ray"] * dom_rays / secs / 1e9
+        issue = {"bound": "issue", "unit": "Ginst/s", "achieved": got, "peak": issue_peak, "frac": got / issue_peak,
+                 "warp_inst_per_ray": prof["warp_inst_per_ray"], "lanes_active": prof.get("lanes_active")}
     if rank == 0:
         base, why = cpu_baseline(s) if world == 1 else (None, "rank 0 at N=1 only")
         line = {
@@ -376,8 +401,16 @@ def run(args):
             "wavefront_over_plain": (value / plain["value"]) if plain else None,
             "fmad_true": fmad,
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": chunk_bytes, "d2h_bytes_per_step": film_bytes},
-            "roofline": {"bound": "hbm", "kernel": "wf" + dom.capitalize(), "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                         "frac": achieved / hbm, "traffic": traffic, "peak_kind": peak_kind,
+            "roofline": {"bound": "l1", "kernel": "wf" + dom.capitalize(), "achieved": achieved, "peak": l1_gbs, "unit": "GB/s",
+                         "frac": achieved / l1_gbs, "traffic": traffic,
+                         "peak_kind": "measured in this run (x2_probe_bandwidth level 1: every SM re-reading 96 KB)",
+                         "l2": {"achieved": achieved, "peak": l2_gbs, "frac": achieved / l2_gbs,
+                                "peak_kind": "measured in this run (x2_probe_bandwidth level 2: a 32 MB buffer swept by the grid)",
+                                "read_from_l2": level("l2_read_bytes_per_ray", l2_gbs)},
+                         "hbm": {"achieved": achieved, "peak": hbm, "frac": achieved / hbm, "peak_kind": peak_kind,
+                                 "dram": level("dram_bytes_per_ray", hbm)},
+                         "l1_requests": level("l1_bytes_per_ray", l1_gbs),
+                         "issue": issue,
                          "algorithmic_bytes_per_launch": alg_bytes / launches_per_frame if launches_per_frame else None,
                          "traffic_source": prof.get("source"),
                          "algorithmic_bytes_per_frame": alg_bytes, "kernel_ms_per_frame": dom_ms,

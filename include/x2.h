@@ -238,7 +238,7 @@ int x2_render_frame(x2_scene* scene, uint32_t first, uint32_t count);  /* every 
  * regeneration; the same film. The launch is one CUDA graph whose iterations run in a conditional while node until no
  * path is left (at most a bound from the items, paths and depth; a launch past it completes with X2_EDEVICE at
  * x2_poll / x2_wait), so it returns without waiting, as x2_launch does. One BSDF sample a lobe (bsdf_samples = 1).
- * Paths in flight: x2_wavefront_reserve (default 2^20). x2_items_download reads the last wavefront launch's per-item radiance and
+ * Paths in flight: x2_wavefront_reserve (default 2^21). x2_items_download reads the last wavefront launch's per-item radiance and
  * status (item = chunk * 64 * samples_per_chunk + position * samples_per_chunk + sample). */
 int x2_wavefront_reserve(x2_scene* scene, uint32_t paths);
 int x2_launch_wavefront(x2_scene* scene, const x2_chunk* chunks, uint32_t count);
@@ -250,7 +250,7 @@ int x2_wavefront_info(x2_scene* scene, uint32_t* paths, uint32_t* records, uint3
 int x2_wavefront_timing(x2_scene* scene, int on, float* ms);
 /* Wavefront launch shape (no reference counterpart; the autotuner's knobs). The results do not depend on it. */
 typedef struct x2_wavefront_shape {
-    uint32_t paths;          /* path slots in flight (0: 2^20, fewer when the launch has fewer items) */
+    uint32_t paths;          /* path slots in flight (0: 2^21, fewer when the launch has fewer items) */
     uint32_t refill;         /* 1..32 idle lanes that make a traversal warp fetch the next rays of its queue */
     uint32_t blocks_per_sm;  /* traversal and shade grids: blocks a SM, 1..32 */
     uint32_t trace_blocks;   /* traversal kernels' occupancy variant: blocks a SM their registers allow (0, 9, 10;
@@ -266,11 +266,14 @@ typedef struct x2_wavefront_shape {
     uint32_t extend_bins;    /* 1: the extend queue binned by the rays' direction octant (a warp's rays share their
                                 children's near-to-far order); 0: in path-slot order */
     uint32_t short_stack;    /* 1: the traversal stacks' first 8 entries in shared memory; 0: all in local memory */
+    uint32_t tri_defer;      /* 0: a lane tests a node's triangles at once; 1..32: a warp tests once that many of its lanes
+                                hold triangles, the others visiting nodes meanwhile (needs short_stack 1; trace_blocks 0) */
 } x2_wavefront_shape;
 void x2_wavefront_shape_defaults(x2_wavefront_shape* shape);
 int x2_wavefront_tune(x2_scene* scene, const x2_wavefront_shape* shape);
 /* The autotuner: times wavefront launches of `tiles` evenly spaced tiles (0: all) at `spp` samples, one knob at a time
- * (paths, refill, tri_limit, shade_blocks, trace_blocks, blocks_per_sm, best of two launches a candidate), sets the
+ * (paths, refill, tri_limit, shade_blocks, trace_blocks, blocks_per_sm, lobe_queues, shadow_order, extend_bins,
+ * short_stack, tri_defer; best of two launches a candidate), sets the
  * fastest shape and returns it (best, best_ms may be null). Renders into the scene's film, which it leaves reset (as
  * x2_frame_begin(scene, spp)). Waits. */
 int x2_wavefront_autotune(x2_scene* scene, uint32_t tiles, uint32_t spp, x2_wavefront_shape* best, float* best_ms);

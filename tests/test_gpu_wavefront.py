@@ -115,3 +115,34 @@ def test_autotuned_shape_renders_the_same_film(ctx):
     got, gc = scene.film()
     assert np.array_equal(gc, wc)
     assert np.array_equal(got, want)
+
+
+SHAPES = [{"shadow_order": 1}, {"extend_bins": 0}, {"short_stack": 0}, {"trace_blocks": 9}, {"lobe_queues": 0},
+          {"tri_defer": 1}, {"tri_defer": 12}, {"tri_defer": 32}, {"tri_defer": 8, "tri_limit": 3}, {"paths": 1024}]
+
+
+@pytest.mark.parametrize("shape", SHAPES, ids=lambda d: ",".join(f"{k}={v}" for k, v in d.items()))
+def test_every_launch_shape_renders_the_same_film(ctx, shape):
+    """The launch shape moves work between lanes, queues and steps, never the samples' arithmetic: the film and the
+    counters equal the default shape's bit for bit (config 108: GGX and Lambert, 16 rect lights and an environment)."""
+    s = x2.SyntheticScene(108)
+    cfg = s.config
+    cfg.spp = 4
+    scene = x2.Scene(ctx, s.desc, cfg)
+    scene.frame_begin(4)
+    scene.render_frame_wavefront(0, 4)
+    scene.wait()
+    want, wc = scene.film()
+    base = scene.counters()
+    scene.reset_counters()
+    scene.wavefront_tune(**shape)
+    scene.frame_begin(4)
+    scene.render_frame_wavefront(0, 4)
+    scene.wait()
+    scene.audit()
+    got, gc = scene.film()
+    assert np.array_equal(gc, wc)
+    assert np.array_equal(got, want)
+    after = scene.counters()
+    for k in ("trace", "shadow_nee", "shadow_bsdf", "held", "samples", "errors", "stack_overflows"):
+        assert after[k] == base[k], k

@@ -222,6 +222,7 @@ struct x2_scene {
     uint32_t shadowOrder = kDefaultShadowOrder;  // the shadow queue by record (1) or by path (0)
     uint32_t extendBins = kDefaultExtendBins;    // the extend queue binned by octant (1) or in slot order (0)
     uint32_t shortStack = kDefaultShortStack;    // traversal stacks' top entries in shared memory (1) or local (0)
+    uint32_t triDefer = kDefaultTriDefer;        // postponed triangle tests: lanes holding triangles a test step needs
     uint32_t* shadeQ = nullptr;            // the per-lobe queues: 3 x wavePaths entries
     uint32_t batchWindow = 0;              // x2_render_batch: items a window (0: the default)
     uint32_t* hostLast = nullptr;      // pinned
@@ -1247,14 +1248,16 @@ void x2_wavefront_shape_defaults(x2_wavefront_shape* shape) {
     shape->shadow_order = kDefaultShadowOrder;
     shape->extend_bins = kDefaultExtendBins;
     shape->short_stack = kDefaultShortStack;
+    shape->tri_defer = kDefaultTriDefer;
 }
 
 int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     if (!s || !shape || shape->refill < 1 || shape->refill > 32 || shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 ||
         shape->trace_blocks > 32 || shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32 || shape->lobe_queues > 1 ||
-        shape->shadow_order > 1 || shape->extend_bins > 1 || shape->short_stack > 1) {
+        shape->shadow_order > 1 || shape->extend_bins > 1 || shape->short_stack > 1 || shape->tri_defer > 32 ||
+        (shape->tri_defer && !shape->short_stack)) {
         setError("refill is 1..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32, lobe_queues, "
-                 "shadow_order, extend_bins and short_stack 0 or 1");
+                 "shadow_order, extend_bins and short_stack 0 or 1, tri_defer 0..32 (with short_stack 1)");
         return X2_EINVAL;
     }
     s->reservePaths = shape->paths;
@@ -1268,6 +1271,7 @@ int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     s->shadowOrder = shape->shadow_order;
     s->extendBins = shape->extend_bins;
     s->shortStack = shape->short_stack;
+    s->triDefer = shape->tri_defer;
     return X2_OK;
 }
 
@@ -1300,6 +1304,7 @@ WaveArgs launchArgs(x2_scene* s, Slot& sl, uint32_t paths, uint32_t records, uns
     a.liveChunks = nullptr;
     a.refill = s->refill;
     a.triLimit = s->triLimit;
+    a.triDefer = s->triDefer;
     a.out = s->out;
     a.outStatus = s->outStatus;
     a.counters = sl.counters;
@@ -1339,7 +1344,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
         setError("%llu work items in one wavefront launch (at most 2^32 - 1)", items);
         return X2_EINVAL;
     }
-    uint32_t paths = s->reservePaths ? s->reservePaths : (1u << 20);
+    uint32_t paths = s->reservePaths ? s->reservePaths : kDefaultPaths;
     if (paths > items) paths = uint32_t(items < 1024 ? 1024 : items);
     const uint32_t records = s->config.light_count * s->config.light_samples + 1;
     if (int rc = ensureWave(s, paths, records)) return rc;
@@ -1356,7 +1361,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
     const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0,
-                                       a.scene.stats != nullptr);
+                                       a.scene.stats != nullptr, s->triDefer != 0 && s->traceBlocks < 9);
     const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     if (s->waveTiming) {
         // Diagnostic form: no graph; events around every kernel, the iteration's times added once it is done.
@@ -1658,7 +1663,7 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
         setError("x2_adjoint: %llu work items (at most 2^32 - 1)", items);
         return X2_EINVAL;
     }
-    uint32_t paths = s->reservePaths ? s->reservePaths : (1u << 20);
+    uint32_t paths = s->reservePaths ? s->reservePaths : kDefaultPaths;
     if (paths > items) paths = uint32_t(items < 1024 ? 1024 : items);
     const uint32_t records = s->config.light_count * s->config.light_samples + 1;
     const uint32_t verts = s->config.max_depth + 1;
@@ -1730,6 +1735,7 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     a.shadeCount = s->waveCounters + 5;
     a.refill = s->refill;
     a.triLimit = s->triLimit;
+    a.triDefer = s->triDefer;
     a.out = s->out;
     a.outStatus = s->outStatus;
     a.counters = sl.counters;
@@ -2090,7 +2096,7 @@ int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float 
     }
     Slot& sl = s->slots[0];
     if (int rc = ensureSlot(sl, ad.tiles)) return rc;
-    uint32_t paths = s->reservePaths ? s->reservePaths : (1u << 20);
+    uint32_t paths = s->reservePaths ? s->reservePaths : kDefaultPaths;
     if (paths > maxItems) paths = uint32_t(maxItems < 1024 ? 1024 : maxItems);
     const uint32_t records = s->config.light_count * s->config.light_samples + 1;
     if (int rc = ensureWave(s, paths, records)) return rc;
@@ -2112,7 +2118,7 @@ int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float 
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
     const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0,
-                                       a.scene.stats != nullptr);
+                                       a.scene.stats != nullptr, s->triDefer != 0 && s->traceBlocks < 9);
     const uint64_t bound = maxItems * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     const uint32_t maxIter = uint32_t(std::min<uint64_t>(bound, 0xffffffffu));
 
@@ -2424,7 +2430,7 @@ int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefron
     if (int rc = timeShape(cur, curMs)) return rc;
     const uint64_t items = uint64_t(tiles) * 64ull * spp;
     std::vector<uint32_t> pathOptions;
-    for (uint32_t p = 1u << 18; p <= (1u << 21); p <<= 1)
+    for (uint32_t p = 1u << 18; p <= (1u << 22); p <<= 1)
         if (p <= items) pathOptions.push_back(p);
     struct Knob {
         uint32_t x2_wavefront_shape::*field;
@@ -2439,7 +2445,8 @@ int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefron
                           {&x2_wavefront_shape::lobe_queues, {0, 1}},
                           {&x2_wavefront_shape::shadow_order, {0, 1}},
                           {&x2_wavefront_shape::extend_bins, {0, 1}},
-                          {&x2_wavefront_shape::short_stack, {0, 1}}};
+                          {&x2_wavefront_shape::short_stack, {0, 1}},
+                          {&x2_wavefront_shape::tri_defer, {0, 8, 12, 16}}};
     for (const Knob& k : knobs) {
         x2_wavefront_shape keep = cur;
         for (uint32_t v : k.values) {
@@ -2530,7 +2537,7 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
     }
     x2_scene* s0 = req[0].scene;
     cudaStream_t st = ctx->stream;
-    uint32_t paths = s0->reservePaths ? s0->reservePaths : (1u << 20);
+    uint32_t paths = s0->reservePaths ? s0->reservePaths : kDefaultPaths;
     if (uint64_t(paths) > windowMax) paths = uint32_t(windowMax);
     if (int rc = ensureWave(s0, paths, records)) return rc;
     if (int rc = ensureItems(s0, windowMax)) return rc;

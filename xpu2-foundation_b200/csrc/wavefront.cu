@@ -346,7 +346,7 @@ struct QueueSegments {
 };
 
 // shortStacks: the block's kShortStack x kWaveBlock short traversal stacks (shared memory).
-template <bool kAny, bool kStats, bool kBatch, int kShort>
+template <bool kAny, bool kStats, bool kBatch, int kShort, bool kDefer = false>
 __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, const uint32_t* __restrict__ queue, uint32_t* next,
                                                 uint2* shortStacks, const QueueSegments seg = QueueSegments{nullptr, 0, 0}) {
     const WaveState& w = a.w;
@@ -393,7 +393,10 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
             liveMask = __ballot_sync(full, live);
             nodeMask = __ballot_sync(full, live && !walk.tbits && ((walk.bits & 0xff000000u) || walk.sp));
         }
-        if (live && walkStep<kAny, kShort>(bvh, r, walk, deep, overflow, a.triLimit)) {
+        bool testNow = true;
+        if (kDefer) testNow = __popc(__ballot_sync(full, live && walk.tbits)) >= a.triDefer;
+        if (live && (kDefer ? walkStepDeferred<kAny, kShort>(bvh, r, walk, deep, overflow, a.triLimit, testNow)
+                            : walkStep<kAny, kShort>(bvh, r, walk, deep, overflow, a.triLimit))) {
             if (kAny) w.svis[k] = walk.best ? 0 : 1;
             else w.hit[k] = make_uint2(walk.best == ~0u ? ~0u : walk.bestLeaf, __float_as_uint(walk.tmax));
             live = false;
@@ -427,7 +430,7 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
     }
 }
 
-template <bool kBatch, int kShort = kShortStack, bool kStats = false>
+template <bool kBatch, int kShort = kShortStack, bool kStats = false, bool kDefer = false>
 __device__ __forceinline__ void extendBody(const WaveArgs& a) {
     __shared__ uint2 shortStacks[kShort > 0 ? kShort * kWaveBlock : 1];
     __shared__ uint32_t start[kOctants + 1];
@@ -445,7 +448,7 @@ __device__ __forceinline__ void extendBody(const WaveArgs& a) {
         }
         __syncthreads();
     }
-    persistentTrace<false, kStats && !kBatch, kBatch, kShort>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
+    persistentTrace<false, kStats && !kBatch, kBatch, kShort, kDefer>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters->trace, (unsigned long long)n);
 }
 
@@ -684,7 +687,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
 }
 
 // ---- shadow: any hits ----
-template <bool kBatch, int kShort = kShortStack, bool kStats = false>
+template <bool kBatch, int kShort = kShortStack, bool kStats = false, bool kDefer = false>
 __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
     __shared__ uint32_t start[kRecordSegments + 1];
     QueueSegments seg{start, 0, a.paths};
@@ -703,7 +706,7 @@ __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
         n = start[seg.segments];
     }
     __shared__ uint2 shortStacks[kShort > 0 ? kShort * kWaveBlock : 1];
-    persistentTrace<true, kStats && !kBatch, kBatch, kShort>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
+    persistentTrace<true, kStats && !kBatch, kBatch, kShort, kDefer>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
 }
 
 // The kernels, each in a few occupancy variants (blocks of kWaveBlock threads a SM that the register allocation must
@@ -728,6 +731,12 @@ __global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) { shadowBody<
 // so that the timed ones carry none of the counting's registers.
 __global__ void __launch_bounds__(kWaveBlock) wfExtendCount(WaveArgs a) { extendBody<false, kShortStack, true>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadowCount(WaveArgs a) { shadowBody<false, kShortStack, true>(a); }
+// Postponed triangle tests (wavefront shape tri_defer: the warp tests once that many of its lanes hold triangles), in
+// the timed and the counting form.
+__global__ void __launch_bounds__(kWaveBlock) wfExtendDefer(WaveArgs a) { extendBody<false, kShortStack, false, true>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShadowDefer(WaveArgs a) { shadowBody<false, kShortStack, false, true>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfExtendDeferCount(WaveArgs a) { extendBody<false, kShortStack, true, true>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShadowDeferCount(WaveArgs a) { shadowBody<false, kShortStack, true, true>(a); }
 // The traversal kernels with their whole stacks in local memory (wavefront shape short_stack 0).
 __global__ void __launch_bounds__(kWaveBlock) wfExtendLocal(WaveArgs a) { extendBody<false, 0>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadowLocal(WaveArgs a) { shadowBody<false, 0>(a); }
@@ -746,12 +755,16 @@ __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadowOcc(WaveArgs a
     shadowBody<false>(a);
 }
 
-WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack, bool counting) {
+WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack, bool counting,
+                        bool defer) {
     WaveKernels k;
     k.logic = wfLogic;
     k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : shortStack ? wfExtend : wfExtendLocal;
     k.shadow = traceBlocks >= 10 ? wfShadowOcc<10> : traceBlocks >= 9 ? wfShadowOcc<9> : shortStack ? wfShadow : wfShadowLocal;
-    if (counting) {
+    if (defer) {
+        k.extend = counting ? wfExtendDeferCount : wfExtendDefer;
+        k.shadow = counting ? wfShadowDeferCount : wfShadowDefer;
+    } else if (counting) {
         k.extend = wfExtendCount;
         k.shadow = wfShadowCount;
     }

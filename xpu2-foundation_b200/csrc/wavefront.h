@@ -6,9 +6,12 @@ namespace x2 {
 
 constexpr int kWaveBlock = 128;
 constexpr uint32_t kRecordSegments = 64;
-// Launch-shape defaults (x2_wavefront_tune changes them a scene).
+// Launch-shape defaults (x2_wavefront_tune changes them a scene). Paths in flight: 2^21 (each launch of the traversal
+// kernels then has twice the rays of 2^20 for the same ramp-down at its end: 3 % faster on config 1's 4096 tiles).
+constexpr uint32_t kDefaultPaths = 1u << 21;
 constexpr uint32_t kDefaultRefill = 8, kDefaultBlocksPerSm = 16, kDefaultTraceBlocks = 0, kDefaultShadeBlocks = 4,
-                   kDefaultTriLimit = 1, kDefaultShadowOrder = 0, kDefaultExtendBins = 1, kDefaultShortStack = 1;
+                   kDefaultTriLimit = 1, kDefaultShadowOrder = 0, kDefaultExtendBins = 1, kDefaultShortStack = 1,
+                   kDefaultTriDefer = 0;
 constexpr uint32_t kOctants = 8;
 
 // Path slots (structure of arrays, `paths` slots) and shadow-ray records (recordsPerPath a slot).
@@ -86,6 +89,7 @@ struct WaveArgs {
     const uint32_t* liveChunks;
     uint32_t refill;       // a warp fetches new rays once this many of its lanes are idle (1..32)
     uint32_t triLimit;     // triangle tests a lane makes a traversal step
+    uint32_t triDefer;     // postponed triangle tests: a warp tests once this many lanes hold triangles (0: at once)
     float4* out;          // per item: rgb, alpha
     uint8_t* outStatus;   // per item: SampleStatus (Skip for items that are not samples)
     Counters* counters;
@@ -120,8 +124,9 @@ struct WaveKernels {
 };
 // counting: the traversal kernels that count node visits, triangle tests and lane use (the scene view's stats must
 // be set).
+// defer: the traversal kernels that postpone triangle tests (WaveArgs::triDefer lanes).
 WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack = kDefaultShortStack != 0,
-                        bool counting = false);
+                        bool counting = false, bool defer = false);
 WaveKernels waveKernelsBatch(bool volumes, bool textures);
 __global__ void wfSortShade(WaveArgs a);
 __global__ void wfSortShadeBatch(WaveArgs a);
