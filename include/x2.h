@@ -266,14 +266,14 @@ typedef struct x2_wavefront_shape {
     uint32_t extend_bins;    /* 1: the extend queue binned by the rays' direction octant (a warp's rays share their
                                 children's near-to-far order); 0: in path-slot order */
     uint32_t short_stack;    /* 1: the traversal stacks' first 8 entries in shared memory; 0: all in local memory */
-    uint32_t tri_defer;      /* 0: a lane tests a node's triangles at once; 1..32: a warp tests once that many of its lanes
-                                hold triangles, the others visiting nodes meanwhile (needs short_stack 1; trace_blocks 0) */
+    uint32_t shade_split;    /* 1: shade as one kernel a per-lobe queue (GGX, Lambert, the rest; with lobe_queues 1, surface
+                                scenes), each holding one lobe's code; 0: one shade kernel */
 } x2_wavefront_shape;
 void x2_wavefront_shape_defaults(x2_wavefront_shape* shape);
 int x2_wavefront_tune(x2_scene* scene, const x2_wavefront_shape* shape);
 /* The autotuner: times wavefront launches of `tiles` evenly spaced tiles (0: all) at `spp` samples, one knob at a time
  * (paths, refill, tri_limit, shade_blocks, trace_blocks, blocks_per_sm, lobe_queues, shadow_order, extend_bins,
- * short_stack, tri_defer; best of two launches a candidate), sets the
+ * short_stack, shade_split; best of two launches a candidate), sets the
  * fastest shape and returns it (best, best_ms may be null). Renders into the scene's film, which it leaves reset (as
  * x2_frame_begin(scene, spp)). Waits. */
 int x2_wavefront_autotune(x2_scene* scene, uint32_t tiles, uint32_t spp, x2_wavefront_shape* best, float* best_ms);

@@ -118,7 +118,7 @@ def test_autotuned_shape_renders_the_same_film(ctx):
 
 
 SHAPES = [{"shadow_order": 1}, {"extend_bins": 0}, {"short_stack": 0}, {"trace_blocks": 9}, {"lobe_queues": 0},
-          {"tri_defer": 1}, {"tri_defer": 12}, {"tri_defer": 32}, {"tri_defer": 8, "tri_limit": 3}, {"paths": 1024}]
+          {"shade_split": 0}, {"tri_limit": 3}, {"refill": 1}, {"paths": 1024}, {"shade_blocks": 3}]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=lambda d: ",".join(f"{k}={v}" for k, v in d.items()))

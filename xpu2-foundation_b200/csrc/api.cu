@@ -222,7 +222,7 @@ struct x2_scene {
     uint32_t shadowOrder = kDefaultShadowOrder;  // the shadow queue by record (1) or by path (0)
     uint32_t extendBins = kDefaultExtendBins;    // the extend queue binned by octant (1) or in slot order (0)
     uint32_t shortStack = kDefaultShortStack;    // traversal stacks' top entries in shared memory (1) or local (0)
-    uint32_t triDefer = kDefaultTriDefer;        // postponed triangle tests: lanes holding triangles a test step needs
+    uint32_t shadeSplit = kDefaultShadeSplit;    // shade as one kernel a per-lobe queue (1) or one kernel (0)
     uint32_t* shadeQ = nullptr;            // the per-lobe queues: 3 x wavePaths entries
     uint32_t batchWindow = 0;              // x2_render_batch: items a window (0: the default)
     uint32_t* hostLast = nullptr;      // pinned
@@ -1248,16 +1248,15 @@ void x2_wavefront_shape_defaults(x2_wavefront_shape* shape) {
     shape->shadow_order = kDefaultShadowOrder;
     shape->extend_bins = kDefaultExtendBins;
     shape->short_stack = kDefaultShortStack;
-    shape->tri_defer = kDefaultTriDefer;
+    shape->shade_split = kDefaultShadeSplit;
 }
 
 int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     if (!s || !shape || shape->refill < 1 || shape->refill > 32 || shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 ||
         shape->trace_blocks > 32 || shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32 || shape->lobe_queues > 1 ||
-        shape->shadow_order > 1 || shape->extend_bins > 1 || shape->short_stack > 1 || shape->tri_defer > 32 ||
-        (shape->tri_defer && !shape->short_stack)) {
+        shape->shadow_order > 1 || shape->extend_bins > 1 || shape->short_stack > 1 || shape->shade_split > 1) {
         setError("refill is 1..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32, lobe_queues, "
-                 "shadow_order, extend_bins and short_stack 0 or 1, tri_defer 0..32 (with short_stack 1)");
+                 "shadow_order, extend_bins, short_stack and shade_split 0 or 1");
         return X2_EINVAL;
     }
     s->reservePaths = shape->paths;
@@ -1271,7 +1270,7 @@ int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     s->shadowOrder = shape->shadow_order;
     s->extendBins = shape->extend_bins;
     s->shortStack = shape->short_stack;
-    s->triDefer = shape->tri_defer;
+    s->shadeSplit = shape->shade_split;
     return X2_OK;
 }
 
@@ -1304,7 +1303,6 @@ WaveArgs launchArgs(x2_scene* s, Slot& sl, uint32_t paths, uint32_t records, uns
     a.liveChunks = nullptr;
     a.refill = s->refill;
     a.triLimit = s->triLimit;
-    a.triDefer = s->triDefer;
     a.out = s->out;
     a.outStatus = s->outStatus;
     a.counters = sl.counters;
@@ -1361,7 +1359,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
     const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0,
-                                       a.scene.stats != nullptr, s->triDefer != 0 && s->traceBlocks < 9);
+                                       a.scene.stats != nullptr, s->shadeSplit != 0);
     const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     if (s->waveTiming) {
         // Diagnostic form: no graph; events around every kernel, the iteration's times added once it is done.
@@ -1378,8 +1376,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
             cudaEventRecord(ev[1], st);
             wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
             cudaEventRecord(ev[2], st);
-            if (a.shadeQ) wfSortShade<<<gridWork, kWaveBlock, 0, st>>>(a);
-            wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
+            launchShade(wk, a, gridWork, st);
             cudaEventRecord(ev[3], st);
             wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
             cudaEventRecord(ev[4], st);
@@ -1449,8 +1446,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
         wfResetQueues<<<1, 32, 0, st>>>(a);
         wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
         wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
-        if (a.shadeQ) wfSortShade<<<gridWork, kWaveBlock, 0, st>>>(a);
-        wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
+        launchShade(wk, a, gridWork, st);
         wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
         wfDrainCheck<<<1, 32, 0, st>>>(a, loop, s->drainWords, bound, s->drainWords + 2);
         check(cudaGetLastError());
@@ -1735,7 +1731,6 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
     a.shadeCount = s->waveCounters + 5;
     a.refill = s->refill;
     a.triLimit = s->triLimit;
-    a.triDefer = s->triDefer;
     a.out = s->out;
     a.outStatus = s->outStatus;
     a.counters = sl.counters;
@@ -2118,7 +2113,7 @@ int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float 
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
     const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0,
-                                       a.scene.stats != nullptr, s->triDefer != 0 && s->traceBlocks < 9);
+                                       a.scene.stats != nullptr, s->shadeSplit != 0);
     const uint64_t bound = maxItems * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     const uint32_t maxIter = uint32_t(std::min<uint64_t>(bound, 0xffffffffu));
 
@@ -2170,8 +2165,7 @@ int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float 
         wfResetQueues<<<1, 32, 0, st>>>(a);
         wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
         wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
-        if (a.shadeQ) wfSortShade<<<gridWork, kWaveBlock, 0, st>>>(a);
-        wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
+        launchShade(wk, a, gridWork, st);
         wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
         wfDrainCheck<<<1, 32, 0, st>>>(a, loop, ad.words + 2, maxIter, ad.words + 4);
         g.check(cudaGetLastError());
@@ -2446,7 +2440,7 @@ int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefron
                           {&x2_wavefront_shape::shadow_order, {0, 1}},
                           {&x2_wavefront_shape::extend_bins, {0, 1}},
                           {&x2_wavefront_shape::short_stack, {0, 1}},
-                          {&x2_wavefront_shape::tri_defer, {0, 8, 12, 16}}};
+                          {&x2_wavefront_shape::shade_split, {0, 1}}};
     for (const Knob& k : knobs) {
         x2_wavefront_shape keep = cur;
         for (uint32_t v : k.values) {

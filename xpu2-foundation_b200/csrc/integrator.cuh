@@ -177,7 +177,9 @@ struct ShadowReq {
 // this vertex was popped. The sink takes shadow rays (shadow(req, bsdf)) and the child (push(child) -> bool).
 // Returns false when the hit's shading state cannot be made (SampleStatus::Error). kVolumes as afterTrace's; kTextures
 // false compiles the texture lookup out (the kernels for scenes whose materials read no texture).
-template <bool kVolumes = true, bool kTextures = true, class Sink>
+// kLobe: the lobe kind every vertex of the launch makes (1 Lambert, 2 GGX; 0 any), as the per-lobe shade queues sort
+// them; the kernel then holds one lobe's evaluation and sampling code.
+template <bool kVolumes = true, bool kTextures = true, int kLobe = 0, class Sink>
 __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& root, uint32_t pixel, uint32_t index, const Pending& pv,
                                             const Hit& hit, V3 va, V3 vb, V3 vc, uint32_t top, V3& radiance, float& alpha, Sink& sink) {
     const x2_config& c = s.config;
@@ -269,7 +271,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
             bool any = false;
             if (matchesFlags(lobe.type, flags) && (lobeRayMask(lobe.type) & L.visibility_mask)) {
                 float pdf;
-                const V3 f = lobeEval(lobe, slice, wi, pdf);
+                const V3 f = lobeEvalAs<kLobe>(lobe, slice, wi, pdf);
                 if (!(pdf == 0.0f || isExactlyZero(f))) {
                     V3 tk = mul(mulv(factor, f), powerHeuristic(float(nl) * pdfL, float(nk) * pdf));
                     if (clampHere && c.clamp_value > 0) {
@@ -325,7 +327,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
         }
         V3 wi;
         float pdf;
-        const V3 f = lobeSample(lobe, slice, r1, r2, wi, pdf);
+        const V3 f = lobeSampleAs<kLobe>(lobe, slice, r1, r2, wi, pdf);
         if (pdf == 0.0f || isExactlyZero(f) || !finite3(f) || !finite3(wi)) continue;
         if (!matchesFlags(lobe.type, surfaceFlags(slice, wi))) continue;
         const V3 pt = mul(mulv(pv.T, f), 1.0f / (float(nk) * pdf));

@@ -538,6 +538,22 @@ __device__ __forceinline__ V3 lobeSample(const Lobe& l, const Slice& s, float r1
     return evalGGX(l, s, wi, pdf);
 }
 
+// The same evaluation and sampling in a kernel that knows the lobe's kind (kLobe 1: Lambert, 2: GGX; 0: read from
+// the lobe), so that it holds one lobe's code.
+template <int kLobe>
+__device__ __forceinline__ V3 lobeEvalAs(const Lobe& l, const Slice& s, V3 wi, float& pdf) {
+    if (kLobe == 1) return evalLambert(l, wi, pdf);
+    if (kLobe == 2) return evalGGX(l, s, wi, pdf);
+    return lobeEval(l, s, wi, pdf);
+}
+template <int kLobe>
+__device__ __forceinline__ V3 lobeSampleAs(const Lobe& l, const Slice& s, float r1, float r2, V3& wi, float& pdf) {
+    if (kLobe == 0) return lobeSample(l, s, r1, r2, wi, pdf);
+    Lobe k = l;
+    k.kind = kLobe == 1 ? 0 : 1;
+    return lobeSample(k, s, r1, r2, wi, pdf);
+}
+
 // ---------------------------------------------------------------------------------------------------------------
 // Lights (light_core.h): Rect and constant Env.
 struct LightHit {

@@ -342,98 +342,6 @@ __device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk<kS
     return !w.tbits && !(w.bits & 0xff000000u) && w.sp == 0;
 }
 
-// The entry on top of the stack, left there.
-template <int kShort>
-__device__ __forceinline__ uint2 walkTop(const Walk<kShort>& w, const uint2* deep) {
-    const int t = w.sp - 1;
-    return t < kShort ? w.shortStack[size_t(t) * blockDim.x] : deep[t - kShort];
-}
-
-// A step that postpones triangle tests until enough of the warp holds triangles (Ylitie et al. 2017 postpone the
-// triangles of a node when few threads would test them). The warp decides each step (testNow, the same on every lane):
-// when it tests, a lane holding triangles tests them (triLimit a step) and the others visit a node, testing the new
-// node's triangles in the same step, as walkStep does; when it does not, a holding lane goes on visiting nodes,
-// pushing the triangles of each further node onto the stack as a triangle group (an entry whose top byte is zero:
-// node groups always have an internal child there), and tests only when it has nothing else to do. A popped
-// triangle group becomes the held one. The tests and visits are the same set in another order; a closest hit does not
-// depend on the order (nearest t, then lowest triangle), an any hit even less.
-template <bool kAny, int kShort>
-__device__ __forceinline__ bool walkStepDeferred(const Bvh8& bvh, const RayQ& r, Walk<kShort>& w, uint2* deep, uint32_t* overflow,
-                                                 uint32_t triLimit, bool testNow) {
-    bool test = testNow;
-    if (!(w.tbits && testNow)) {
-        bool visit = true;
-        if (!(w.bits & 0xff000000u)) {
-            if (w.sp == 0) {
-                if (!w.tbits) return true;
-                visit = false;
-                test = true;  // holds triangles and has nothing else to do
-            } else {
-                const uint2 e = walkTop(w, deep);
-                if (!(e.y >> 24)) {  // a postponed triangle group
-                    visit = false;
-                    if (w.tbits) {
-                        test = true;  // one group held at a time: test the held one first
-                    } else {
-                        --w.sp;
-                        w.tbase = e.x;
-                        w.tbits = e.y;
-                    }
-                } else {
-                    --w.sp;
-                    w.base = e.x;
-                    w.bits = e.y & 0xff000000u;
-                    w.imask = (e.y >> 16) & 0xffu;
-                }
-            }
-        }
-        if (visit) {
-            const uint32_t b = __ffs(w.bits >> 24) - 1;
-            w.bits &= ~(1u << (24 + b));
-            const uint32_t slot = b ^ r.oct7;
-            const uint32_t child = w.base + __popc(w.imask & ((1u << slot) - 1u));
-            if (w.bits & 0xff000000u) walkPush(w, deep, make_uint2(w.base, w.bits | (w.imask << 16)), overflow);
-            uint32_t childBase, imask, triBase;
-            const uint32_t hits = visitNode(bvh.nodes, child, r, w.tmin - r.eps, w.tmax + r.eps, childBase, triBase, imask);
-            ++w.nodes;
-            const uint32_t nt = hits & 0x00ffffffu;
-            if (nt) {
-                if (w.tbits) walkPush(w, deep, make_uint2(triBase, nt), overflow);
-                else {
-                    w.tbase = triBase;
-                    w.tbits = nt;
-                }
-            }
-            w.base = childBase;
-            w.bits = hits & 0xff000000u;
-            w.imask = imask;
-        }
-    }
-    if (test) {
-        for (uint32_t n = 0; w.tbits && n < triLimit; ++n) {
-            const uint32_t k = __ffs(w.tbits) - 1;
-            w.tbits &= w.tbits - 1;
-            const float4* tp = reinterpret_cast<const float4*>(bvh.tris + w.tbase + k);
-            const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
-            ++w.tris;
-            float t;
-            if (triTest(r, v0, v1, v2, w.tmin, w.tmax, t)) {
-                if (kAny) {
-                    w.best = 1;
-                    return true;
-                }
-                const uint32_t id = __float_as_uint(v0.w);
-                if (t < w.tmax || (t == w.tmax && id < w.best)) {
-                    w.tmax = t;
-                    w.best = id;
-                    w.bestLeaf = w.tbase + k;
-                }
-            }
-        }
-    }
-    return !w.tbits && !(w.bits & 0xff000000u) && w.sp == 0;
-}
-
 // Any hit on [tmin, tmax].
 template <bool kStats>
 static __device__ __noinline__ bool traceAny(const Bvh8 bvh, const RayQ& r, float tmin, float tmax, uint32_t* overflow, TraversalStats* stats) {

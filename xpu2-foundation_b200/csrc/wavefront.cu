@@ -346,7 +346,7 @@ struct QueueSegments {
 };
 
 // shortStacks: the block's kShortStack x kWaveBlock short traversal stacks (shared memory).
-template <bool kAny, bool kStats, bool kBatch, int kShort, bool kDefer = false>
+template <bool kAny, bool kStats, bool kBatch, int kShort>
 __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, const uint32_t* __restrict__ queue, uint32_t* next,
                                                 uint2* shortStacks, const QueueSegments seg = QueueSegments{nullptr, 0, 0}) {
     const WaveState& w = a.w;
@@ -393,10 +393,7 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
             liveMask = __ballot_sync(full, live);
             nodeMask = __ballot_sync(full, live && !walk.tbits && ((walk.bits & 0xff000000u) || walk.sp));
         }
-        bool testNow = true;
-        if (kDefer) testNow = __popc(__ballot_sync(full, live && walk.tbits)) >= a.triDefer;
-        if (live && (kDefer ? walkStepDeferred<kAny, kShort>(bvh, r, walk, deep, overflow, a.triLimit, testNow)
-                            : walkStep<kAny, kShort>(bvh, r, walk, deep, overflow, a.triLimit))) {
+        if (live && walkStep<kAny, kShort>(bvh, r, walk, deep, overflow, a.triLimit)) {
             if (kAny) w.svis[k] = walk.best ? 0 : 1;
             else w.hit[k] = make_uint2(walk.best == ~0u ? ~0u : walk.bestLeaf, __float_as_uint(walk.tmax));
             live = false;
@@ -430,7 +427,7 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
     }
 }
 
-template <bool kBatch, int kShort = kShortStack, bool kStats = false, bool kDefer = false>
+template <bool kBatch, int kShort = kShortStack, bool kStats = false>
 __device__ __forceinline__ void extendBody(const WaveArgs& a) {
     __shared__ uint2 shortStacks[kShort > 0 ? kShort * kWaveBlock : 1];
     __shared__ uint32_t start[kOctants + 1];
@@ -448,7 +445,7 @@ __device__ __forceinline__ void extendBody(const WaveArgs& a) {
         }
         __syncthreads();
     }
-    persistentTrace<false, kStats && !kBatch, kBatch, kShort, kDefer>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
+    persistentTrace<false, kStats && !kBatch, kBatch, kShort>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters->trace, (unsigned long long)n);
 }
 
@@ -579,10 +576,12 @@ __device__ __forceinline__ uint32_t shadeEntry(const WaveArgs& a, uint32_t i, ui
     return a.shadeQ[2ull * a.paths + (i - c0 - c1)];
 }
 
-template <bool kBatch, bool kVolumes, bool kAdjoint = false, bool kTextures = true>
+// kQueue: -1 every extended path (the per-lobe queues in order when they are on, else the extend queue); 0, 1, 2 one
+// per-lobe queue (GGX, Lambert, the rest), its kernel holding that lobe's code only.
+template <bool kBatch, bool kVolumes, bool kAdjoint = false, bool kTextures = true, int kQueue = -1>
 __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
     const WaveState& w = a.w;
-    const uint32_t n = *a.extendCount;
+    const uint32_t n = kQueue < 0 ? *a.extendCount : a.shadeCount[kQueue];
     extern __shared__ float partial[];  // the adjoint's block partials
     const Layout at{a.adj.materials, a.adj.lights};
     if (kAdjoint) partialsBegin(partial, at);
@@ -594,7 +593,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
         const uint32_t i = base + threadIdx.x;
         uint32_t records = 0, p = 0;
         if (i < n) {
-            p = shadeEntry(a, i, c0, c1);
+            p = kQueue < 0 ? shadeEntry(a, i, c0, c1) : a.shadeQ[size_t(kQueue) * a.paths + i];
             Pending pv;
             loadPending(w, p, pv);
             const uint4 m = w.meta[p];
@@ -650,7 +649,8 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
                     sink.depth = pv.depth;
                     sink.ggx = sink.sampled = false;
                 }
-                if (!shadeVertex<kVolumes, kTextures>(s, root, pixel, index, pv, hit, va, vb, vc, 0u, radiance, alpha, sink)) {
+                if (!shadeVertex<kVolumes, kTextures, kQueue == 0 ? 2 : kQueue == 1 ? 1 : 0>(s, root, pixel, index, pv, hit, va, vb, vc, 0u,
+                                                                                           radiance, alpha, sink)) {
                     next = kError;
                 } else {
                     records = sink.n;
@@ -687,7 +687,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
 }
 
 // ---- shadow: any hits ----
-template <bool kBatch, int kShort = kShortStack, bool kStats = false, bool kDefer = false>
+template <bool kBatch, int kShort = kShortStack, bool kStats = false>
 __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
     __shared__ uint32_t start[kRecordSegments + 1];
     QueueSegments seg{start, 0, a.paths};
@@ -706,7 +706,7 @@ __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
         n = start[seg.segments];
     }
     __shared__ uint2 shortStacks[kShort > 0 ? kShort * kWaveBlock : 1];
-    persistentTrace<true, kStats && !kBatch, kBatch, kShort, kDefer>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
+    persistentTrace<true, kStats && !kBatch, kBatch, kShort>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
 }
 
 // The kernels, each in a few occupancy variants (blocks of kWaveBlock threads a SM that the register allocation must
@@ -731,12 +731,6 @@ __global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) { shadowBody<
 // so that the timed ones carry none of the counting's registers.
 __global__ void __launch_bounds__(kWaveBlock) wfExtendCount(WaveArgs a) { extendBody<false, kShortStack, true>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadowCount(WaveArgs a) { shadowBody<false, kShortStack, true>(a); }
-// Postponed triangle tests (wavefront shape tri_defer: the warp tests once that many of its lanes hold triangles), in
-// the timed and the counting form.
-__global__ void __launch_bounds__(kWaveBlock) wfExtendDefer(WaveArgs a) { extendBody<false, kShortStack, false, true>(a); }
-__global__ void __launch_bounds__(kWaveBlock) wfShadowDefer(WaveArgs a) { shadowBody<false, kShortStack, false, true>(a); }
-__global__ void __launch_bounds__(kWaveBlock) wfExtendDeferCount(WaveArgs a) { extendBody<false, kShortStack, true, true>(a); }
-__global__ void __launch_bounds__(kWaveBlock) wfShadowDeferCount(WaveArgs a) { shadowBody<false, kShortStack, true, true>(a); }
 // The traversal kernels with their whole stacks in local memory (wavefront shape short_stack 0).
 __global__ void __launch_bounds__(kWaveBlock) wfExtendLocal(WaveArgs a) { extendBody<false, 0>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadowLocal(WaveArgs a) { shadowBody<false, 0>(a); }
@@ -754,17 +748,34 @@ template <int kMinBlocks>
 __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadowOcc(WaveArgs a) {
     shadowBody<false>(a);
 }
+// Shade split by lobe (wavefront shape shade_split): one kernel a per-lobe queue, each with one lobe's code.
+template <int kQueue, bool kTextures>
+__global__ void __launch_bounds__(kWaveBlock, 4) wfShadeQueue(WaveArgs a) {
+    shadeBody<false, false, false, kTextures, kQueue>(a);
+}
+
+void launchShade(const WaveKernels& k, const WaveArgs& a, int grid, cudaStream_t st) {
+    if (a.shadeQ) wfSortShade<<<grid, kWaveBlock, 0, st>>>(a);
+    if (a.shadeQ && k.shadeBy[0]) {
+        for (int q = 0; q < 3; ++q) k.shadeBy[q]<<<grid, kWaveBlock, 0, st>>>(a);
+    } else {
+        k.shade<<<grid, kWaveBlock, 0, st>>>(a);
+    }
+}
 
 WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack, bool counting,
-                        bool defer) {
+                        bool shadeSplit) {
     WaveKernels k;
+    k.shadeBy[0] = k.shadeBy[1] = k.shadeBy[2] = nullptr;
+    if (shadeSplit && !volumes) {
+        k.shadeBy[0] = textures ? wfShadeQueue<0, true> : wfShadeQueue<0, false>;
+        k.shadeBy[1] = textures ? wfShadeQueue<1, true> : wfShadeQueue<1, false>;
+        k.shadeBy[2] = textures ? wfShadeQueue<2, true> : wfShadeQueue<2, false>;
+    }
     k.logic = wfLogic;
     k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : shortStack ? wfExtend : wfExtendLocal;
     k.shadow = traceBlocks >= 10 ? wfShadowOcc<10> : traceBlocks >= 9 ? wfShadowOcc<9> : shortStack ? wfShadow : wfShadowLocal;
-    if (defer) {
-        k.extend = counting ? wfExtendDeferCount : wfExtendDefer;
-        k.shadow = counting ? wfShadowDeferCount : wfShadowDefer;
-    } else if (counting) {
+    if (counting) {
         k.extend = wfExtendCount;
         k.shadow = wfShadowCount;
     }
@@ -776,6 +787,7 @@ WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes
 
 WaveKernels waveKernelsBatch(bool volumes, bool textures) {
     WaveKernels k;
+    k.shadeBy[0] = k.shadeBy[1] = k.shadeBy[2] = nullptr;
     k.logic = wfLogicBatch;
     k.extend = wfExtendBatch;
     k.shadow = wfShadowBatch;

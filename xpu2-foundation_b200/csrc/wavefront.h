@@ -11,7 +11,7 @@ constexpr uint32_t kRecordSegments = 64;
 constexpr uint32_t kDefaultPaths = 1u << 21;
 constexpr uint32_t kDefaultRefill = 8, kDefaultBlocksPerSm = 16, kDefaultTraceBlocks = 0, kDefaultShadeBlocks = 4,
                    kDefaultTriLimit = 1, kDefaultShadowOrder = 0, kDefaultExtendBins = 1, kDefaultShortStack = 1,
-                   kDefaultTriDefer = 0;
+                   kDefaultShadeSplit = 1;
 constexpr uint32_t kOctants = 8;
 
 // Path slots (structure of arrays, `paths` slots) and shadow-ray records (recordsPerPath a slot).
@@ -89,7 +89,6 @@ struct WaveArgs {
     const uint32_t* liveChunks;
     uint32_t refill;       // a warp fetches new rays once this many of its lanes are idle (1..32)
     uint32_t triLimit;     // triangle tests a lane makes a traversal step
-    uint32_t triDefer;     // postponed triangle tests: a warp tests once this many lanes hold triangles (0: at once)
     float4* out;          // per item: rgb, alpha
     uint8_t* outStatus;   // per item: SampleStatus (Skip for items that are not samples)
     Counters* counters;
@@ -121,12 +120,15 @@ struct WaveKernels {
     void (*extend)(WaveArgs);
     void (*shade)(WaveArgs);
     void (*shadow)(WaveArgs);
+    void (*shadeBy[3])(WaveArgs);  // shade split by lobe queue (GGX, Lambert, the rest), or null: shade in one kernel
 };
 // counting: the traversal kernels that count node visits, triangle tests and lane use (the scene view's stats must
 // be set).
-// defer: the traversal kernels that postpone triangle tests (WaveArgs::triDefer lanes).
+// shadeSplit: shade as one kernel a per-lobe queue (surface scenes).
 WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack = kDefaultShortStack != 0,
-                        bool counting = false, bool defer = false);
+                        bool counting = false, bool shadeSplit = false);
+// The iteration's shade step: the per-lobe sort (when the queues are on) and the shade kernel or kernels.
+void launchShade(const WaveKernels& k, const WaveArgs& a, int grid, cudaStream_t st);
 WaveKernels waveKernelsBatch(bool volumes, bool textures);
 __global__ void wfSortShade(WaveArgs a);
 __global__ void wfSortShadeBatch(WaveArgs a);
