@@ -228,6 +228,15 @@ def traffic_from_profile():
         return {}
 
 
+def kernels_per_iteration(spec):
+    """Kernels a wavefront iteration launches: queue reset, logic, extend, the per-lobe sort (lobe_queues), shade (three
+    kernels with shade_split, else one), shadow and the drain check."""
+    shape = dict(kv.split("=") for kv in spec.split(",")) if spec else {}
+    lobe = int(shape.get("lobe_queues", 1))
+    split = int(shape.get("shade_split", 1)) and lobe
+    return 5 + lobe + (3 if split else 1)
+
+
 def simt_summary(tc):
     """Lane use of the persistent traversal kernels from a counting launch, by ray kind: live lanes a warp step, lanes a
     step that ran the node visit, lanes a triangle-test iteration (each of 32), node visits and triangle tests a ray."""
@@ -401,23 +410,25 @@ def run(args):
             "wavefront_over_plain": (value / plain["value"]) if plain else None,
             "fmad_true": fmad,
             "e2e": {"value": e2e_value, "unit": "Msamples/s", "h2d_bytes_per_step": chunk_bytes, "d2h_bytes_per_step": film_bytes},
-            "roofline": {"bound": "l1", "kernel": "wf" + dom.capitalize(), "achieved": achieved, "peak": l1_gbs, "unit": "GB/s",
-                         "frac": achieved / l1_gbs, "traffic": traffic,
-                         "peak_kind": "measured in this run (x2_probe_bandwidth level 1: every SM re-reading 96 KB)",
-                         "l2": {"achieved": achieved, "peak": l2_gbs, "frac": achieved / l2_gbs,
-                                "peak_kind": "measured in this run (x2_probe_bandwidth level 2: a 32 MB buffer swept by the grid)",
-                                "read_from_l2": level("l2_read_bytes_per_ray", l2_gbs)},
-                         "hbm": {"achieved": achieved, "peak": hbm, "frac": achieved / hbm, "peak_kind": peak_kind,
-                                 "dram": level("dram_bytes_per_ray", hbm)},
-                         "l1_requests": level("l1_bytes_per_ray", l1_gbs),
+            "roofline": {"bound": "issue", "kernel": "wf" + dom.capitalize(), "unit": "Ginst/s",
+                         "achieved": issue["achieved"] if issue else None, "peak": issue_peak,
+                         "frac": issue["frac"] if issue else None, "traffic": traffic,
+                         "peak_kind": "4 warp instructions a cycle a SM x %d SMs x the SM clock sampled during the timed frames" % sms,
                          "issue": issue,
+                         "algorithmic": {
+                             "unit": "GB/s", "achieved": achieved, "bytes_per_launch": alg_bytes / launches_per_frame if launches_per_frame else None,
+                             "l1": {"peak": l1_gbs, "frac": achieved / l1_gbs, "requested": level("l1_bytes_per_ray", l1_gbs),
+                                    "peak_kind": "measured in this run (x2_probe_bandwidth level 1: every SM re-reading 96 KB)"},
+                             "l2": {"peak": l2_gbs, "frac": achieved / l2_gbs, "read_from_l2": level("l2_read_bytes_per_ray", l2_gbs),
+                                    "peak_kind": "measured in this run (x2_probe_bandwidth level 2: a 32 MB buffer swept by the grid)"},
+                             "hbm": {"peak": hbm, "frac": achieved / hbm, "dram": level("dram_bytes_per_ray", hbm), "peak_kind": peak_kind}},
                          "algorithmic_bytes_per_launch": alg_bytes / launches_per_frame if launches_per_frame else None,
                          "traffic_source": prof.get("source"),
                          "algorithmic_bytes_per_frame": alg_bytes, "kernel_ms_per_frame": dom_ms,
                          "kernel_ms_by_kind": kms, "traversal": tc, "simt": simt_summary(tc),
                          "bytes": {"node": NODE_BYTES, "triangle": TRI_BYTES, "extend_ray": EXTEND_RAY_BYTES, "shadow_ray": SHADOW_RAY_BYTES}},
             "cpu_baseline": base if base else {"value": None, "unavailable": why},
-            "clocks": clk, "gpu_launches": launches_per_frame * 5 * args.steps,
+            "clocks": clk, "gpu_launches": (launches_per_frame * kernels_per_iteration(args.shape) + 1) * args.steps,
             "errors": counters["errors"], "stack_overflows": counters["stack_overflows"],
         }
         print(json.dumps(line))

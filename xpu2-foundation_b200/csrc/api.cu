@@ -2433,7 +2433,7 @@ int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefron
     const Knob knobs[] = {{&x2_wavefront_shape::paths, pathOptions},
                           {&x2_wavefront_shape::refill, {4, 8, 16}},
                           {&x2_wavefront_shape::tri_limit, {1, 2, 4}},
-                          {&x2_wavefront_shape::shade_blocks, {0, 3, 4}},
+                          {&x2_wavefront_shape::shade_blocks, {0, 3, 4, 5}},
                           {&x2_wavefront_shape::trace_blocks, {0, 9}},
                           {&x2_wavefront_shape::blocks_per_sm, {8, 16, 32}},
                           {&x2_wavefront_shape::lobe_queues, {0, 1}},

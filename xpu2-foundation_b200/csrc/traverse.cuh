@@ -295,17 +295,28 @@ __device__ __forceinline__ void walkStart(Walk<kShort>& w, const RayQ& r, float 
 // One step: a node visit (when no triangles are pending) and then at most `triLimit` triangle tests, the rest left
 // for the next steps, so that a lane with a full leaf does not hold its warp for all of them at once. The tests run
 // in the same order whatever the limit. True once the ray is done.
+//
+// `lanes` is the set of the warp's lanes that make this step (all of them call it): they meet at a __syncwarp after
+// the stack pop, so that the lanes that popped and those that went on with their node group visit their nodes
+// together, and again before the triangle tests. The compiler may otherwise give each way its own copy of the code
+// that follows, and the warp then runs it once for each group of lanes.
 template <bool kAny, int kShort>
 __device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk<kShort>& w, uint2* deep, uint32_t* overflow,
-                                         uint32_t triLimit) {
-    if (!w.tbits) {
-        if (!(w.bits & 0xff000000u)) {
-            if (w.sp == 0) return true;
+                                         uint32_t triLimit, unsigned lanes) {
+    bool visit = !w.tbits, done = false;
+    if (visit && !(w.bits & 0xff000000u)) {
+        if (w.sp == 0) {
+            visit = false;
+            done = true;
+        } else {
             const uint2 e = walkPop(w, deep);
             w.base = e.x;
             w.bits = e.y & 0xff000000u;
             w.imask = (e.y >> 16) & 0xffu;
         }
+    }
+    __syncwarp(lanes);
+    if (visit) {
         const uint32_t b = __ffs(w.bits >> 24) - 1;
         w.bits &= ~(1u << (24 + b));
         const uint32_t slot = b ^ r.oct7;
@@ -319,6 +330,7 @@ __device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk<kS
         w.bits = hits & 0xff000000u;
         w.imask = imask;
     }
+    __syncwarp(lanes);  // and the triangle tests together, the lanes that visited and those that held triangles
     for (uint32_t n = 0; w.tbits && n < triLimit; ++n) {
         const uint32_t k = __ffs(w.tbits) - 1;
         w.tbits &= w.tbits - 1;
@@ -339,7 +351,7 @@ __device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk<kS
             }
         }
     }
-    return !w.tbits && !(w.bits & 0xff000000u) && w.sp == 0;
+    return done || (!w.tbits && !(w.bits & 0xff000000u) && w.sp == 0);
 }
 
 // Any hit on [tmin, tmax].

@@ -388,12 +388,10 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
             }
         }
         if (!__any_sync(full, live)) break;
-        uint32_t liveMask = 0, nodeMask = 0, tris0 = walk.tris;
-        if (kStats) {
-            liveMask = __ballot_sync(full, live);
-            nodeMask = __ballot_sync(full, live && !walk.tbits && ((walk.bits & 0xff000000u) || walk.sp));
-        }
-        if (live && walkStep<kAny, kShort>(bvh, r, walk, deep, overflow, a.triLimit)) {
+        const uint32_t liveMask = __ballot_sync(full, live), tris0 = walk.tris;
+        uint32_t nodeMask = 0;
+        if (kStats) nodeMask = __ballot_sync(full, live && !walk.tbits && ((walk.bits & 0xff000000u) || walk.sp));
+        if (live && walkStep<kAny, kShort>(bvh, r, walk, deep, overflow, a.triLimit, liveMask)) {
             if (kAny) w.svis[k] = walk.best ? 0 : 1;
             else w.hit[k] = make_uint2(walk.best == ~0u ? ~0u : walk.bestLeaf, __float_as_uint(walk.tmax));
             live = false;
@@ -749,8 +747,8 @@ __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadowOcc(WaveArgs a
     shadowBody<false>(a);
 }
 // Shade split by lobe (wavefront shape shade_split): one kernel a per-lobe queue, each with one lobe's code.
-template <int kQueue, bool kTextures>
-__global__ void __launch_bounds__(kWaveBlock, 4) wfShadeQueue(WaveArgs a) {
+template <int kQueue, bool kTextures, int kMinBlocks>
+__global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadeQueue(WaveArgs a) {
     shadeBody<false, false, false, kTextures, kQueue>(a);
 }
 
@@ -768,9 +766,11 @@ WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes
     WaveKernels k;
     k.shadeBy[0] = k.shadeBy[1] = k.shadeBy[2] = nullptr;
     if (shadeSplit && !volumes) {
-        k.shadeBy[0] = textures ? wfShadeQueue<0, true> : wfShadeQueue<0, false>;
-        k.shadeBy[1] = textures ? wfShadeQueue<1, true> : wfShadeQueue<1, false>;
-        k.shadeBy[2] = textures ? wfShadeQueue<2, true> : wfShadeQueue<2, false>;
+        // The GGX and Lambert kernels at 4 blocks a SM (128 registers) or, with shade_blocks 5, at 5 (96, more spilled).
+        const bool five = shadeBlocks >= 5;
+        k.shadeBy[0] = textures ? (five ? wfShadeQueue<0, true, 5> : wfShadeQueue<0, true, 4>) : (five ? wfShadeQueue<0, false, 5> : wfShadeQueue<0, false, 4>);
+        k.shadeBy[1] = textures ? (five ? wfShadeQueue<1, true, 5> : wfShadeQueue<1, true, 4>) : (five ? wfShadeQueue<1, false, 5> : wfShadeQueue<1, false, 4>);
+        k.shadeBy[2] = textures ? wfShadeQueue<2, true, 4> : wfShadeQueue<2, false, 4>;
     }
     k.logic = wfLogic;
     k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : shortStack ? wfExtend : wfExtendLocal;
