@@ -5,7 +5,9 @@
  * The transcendental functions of the per-sample kernels (x2_integrate) run either as CUDA's single-precision
  * functions (mode bit 0 clear, as in the product) or in double rounded to float (bit 0 set); with bit 1 set every
  * call (x2_diag_call: function, arguments, results) is appended to a device buffer of `capacity` records, in call
- * order when one sample is integrated a call. Both act on the current device. */
+ * order when one sample is integrated a call. With bit 2 set the volume march's single scattering gives each distance
+ * sample the light point of its pair's equi-angular sample (the pivot of both MIS weights) instead of a point of its
+ * own: not the reference's estimator; a study of its bias. All act on the current device. */
 #ifndef X2_DIAG_H
 #define X2_DIAG_H
 #include <stdint.h>

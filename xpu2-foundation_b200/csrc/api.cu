@@ -442,17 +442,21 @@ int contextStream(x2_ctx* ctx, cudaStream_t* stream, int* smCount) {
 }  // namespace x2
 
 namespace {
-// A volume's majorant grid: kMajorantCells^3 cells over its bounds, each the largest density any of the lookups can
-// read at a point of the cell (nearest voxel, trilinear or quadratic: the voxels whose index box the cell's corners
-// span, one more each way) times its largest gain channel; *largest the grid's maximum. Corners go to grid space by
-// the volume's affine map and to index space by the grid's, so any affine placement stays conservative.
+// A volume's majorant grid: kMajorantCells^3 cells over its bounds, each a bound on the density any of the lookups
+// can read at a point of the cell — the largest of the voxels whose index box the cell's corners span, one more each
+// way, which bounds the nearest voxel and the trilinear lookup, times the quadratic lookup's overshoot when the volume
+// uses it — times its largest gain channel; *largest the grid's maximum. Corners go to grid space by the volume's affine
+// map and to index space by the grid's, so any affine placement stays conservative.
 std::vector<float> majorantGrid(const x2_volume& v, const x2_grid* grids, uint32_t gridCount, float* largest) {
     const int n = x2::kMajorantCells;
     std::vector<float> out(size_t(n) * n * n, 0.0f);
     *largest = 0.0f;
     if (v.density_grid >= gridCount || grids[v.density_grid].channels != 1) return out;
     const x2_grid& g = grids[v.density_grid];
-    const float gain = std::max(0.0f, std::max(v.gain[0], std::max(v.gain[1], v.gain[2])));
+    // The quadratic lookup (interpolation 2) is a Lagrange quadratic through three voxels an axis, which at its
+    // parameter w in [0, 1) reaches up to (1 + w - w^2) <= 1.25 times the largest of them: 1.25^3 over three axes.
+    const float overshoot = v.interpolation == 2 ? 1.953125f : 1.0f;
+    const float gain = overshoot * std::max(0.0f, std::max(v.gain[0], std::max(v.gain[1], v.gain[2])));
     auto toIndex = [&](double x, double y, double z, double out3[3]) {
         const float* a = v.world_to_grid;
         const double gx = a[0] * x + a[1] * y + a[2] * z + a[3], gy = a[4] * x + a[5] * y + a[6] * z + a[7], gz = a[8] * x + a[9] * y + a[10] * z + a[11];

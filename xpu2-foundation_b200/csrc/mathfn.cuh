@@ -6,10 +6,12 @@
 // divide, square root, without contraction) rounds alike on both sides.
 //
 // A diagnostic build (-DX2_DIAG, libx2diag.so; never the product, and only the per-sample kernels of render.cu) adds
-// two switches, set by x2_diag_set: mode bit 0 evaluates each function in double and rounds the result to float (the
+// switches, set by x2_diag_set: mode bit 0 evaluates each function in double and rounds the result to float (the
 // correctly rounded value but for rare double roundings — what a libm within half an ulp returns), and bit 1 records
 // every call of the launch (function, arguments, results) into a caller's device buffer, in call order for a
-// one-sample launch. The records let the host replay a sample through the reference with the device's values.
+// one-sample launch. The records let the host replay a sample through the reference with the device's values. Bit 2
+// (sharedPivot) changes the volume march's single scattering, for the estimator study only: a distance sample's light
+// point is its pair's equi-angular light point, the pivot both MIS weights were computed with.
 #pragma once
 #include <cstdint>
 
@@ -39,10 +41,12 @@ __device__ __forceinline__ void record(uint32_t fn, float a, float b, float r0, 
     if (k < g_cap) g_calls[k] = DiagCall{fn, a, b, r0, r1};
 }
 __device__ __forceinline__ bool wide() { return g_mode & 1; }
+__device__ __forceinline__ bool sharedPivot() { return g_mode & 4; }
 #define X2_MF(fn, a, b, r0, r1) record(fn, a, b, r0, r1)
 #else
 #define X2_DIAG_RECORD(fn, a, b, r0, r1) ((void)0)
 __device__ __forceinline__ constexpr bool wide() { return false; }
+__device__ __forceinline__ constexpr bool sharedPivot() { return false; }
 #define X2_MF(fn, a, b, r0, r1) ((void)0)
 #endif
 

@@ -699,9 +699,12 @@ static __device__ __noinline__ V3 volumeRadiance(const SceneView& s, const Ident
                         sid.branch = childBranch(volumeBranch, 1 + li, ls * scatterCount + ts);
                         Stream ss(sid, pv.depth, 0);
                         float D = 0.0f, thetaA = 0.0f, thetaB = 0.0f, offset = 0.0f;
+                        float uel[3] = {0.0f, 0.0f, 0.0f};
                         if (equiAngular) {
                             const float ue = ss.next();
-                            const float uel[3] = {ss.next(), ss.next(), ss.next()};
+                            uel[0] = ss.next();
+                            uel[1] = ss.next();
+                            uel[2] = ss.next();
                             const V3 pivot = lightPivot(L, uel);
                             offset = dot(add(pivot, mul(org, -1.0f)), dir);
                             const V3 foot = add(org, mul(dir, offset));
@@ -740,7 +743,10 @@ static __device__ __noinline__ V3 volumeRadiance(const SceneView& s, const Ident
                             const float pdfTe = pdfEquiAngular(td - offset, D, thetaA, thetaB);
                             if (vfinite(pdfTe)) mis = powerHeuristic(pdfTd, pdfTe);
                         }
-                        const V3 Ls = volumeSourceTerm(s, ss, L, add(org, mul(dir, td)), dir, vp.g, udl, 1.0f);
+                        // (The diagnostic build's shared-pivot switch gives this sample the equi-angular sample's light
+                        // point, the pivot its MIS weight was computed with; the reference draws a point of its own.)
+                        const V3 Ls = volumeSourceTerm(s, ss, L, add(org, mul(dir, td)), dir, vp.g,
+                                                       equiAngular && mf::sharedPivot() ? uel : udl, 1.0f);
                         direct = vplus(direct, vscaled(vtimes(vtimes(T, vp.sigmaS), vtimes(trScatter, Ls)), invN * mis / pdfTd));
                     }
                 }
