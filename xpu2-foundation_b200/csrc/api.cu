@@ -259,7 +259,8 @@ namespace {
 
 SceneView viewOf(const x2_scene* s) {
     SceneView v;
-    v.bvh = Bvh8{s->bvh.nodes, s->bvh.tris, s->bvh.nodeCount, s->bvh.triCount, {s->lo[0], s->lo[1], s->lo[2]}, {s->hi[0], s->hi[1], s->hi[2]}};
+    v.bvh = Bvh8{s->bvh.nodes, s->bvh.tris, s->bvh.nodeCount, s->bvh.triCount, {s->lo[0], s->lo[1], s->lo[2]}, {s->hi[0], s->hi[1], s->hi[2]},
+                 {s->bvh.rot[0], s->bvh.rot[1], s->bvh.tris}};
     v.triMesh = s->triMesh;
     v.meshFirst = s->meshFirst;
     v.meshMaterial = s->meshMaterial;
@@ -893,6 +894,8 @@ int x2_scene_free(x2_scene* s) {
     s->adaptiveState = nullptr;
     cudaFree(s->bvh.nodes);
     cudaFree(s->bvh.tris);
+    cudaFree(s->bvh.rot[0]);
+    cudaFree(s->bvh.rot[1]);
     cudaFree(s->triMesh);
     cudaFree(s->meshFirst);
     cudaFree(s->meshMaterial);
@@ -970,7 +973,7 @@ int x2_scene_info(x2_scene* s, uint64_t* nodes, uint64_t* bvhBytes, uint64_t* tr
     if (!s) return X2_EINVAL;
     if (nodes) *nodes = s->bvh.nodeCount;
     if (bvhBytes) *bvhBytes = uint64_t(s->bvh.nodeCount) * sizeof(Node8);
-    if (triBytes) *triBytes = uint64_t(s->bvh.triCount) * sizeof(TriRec);
+    if (triBytes) *triBytes = uint64_t(s->bvh.triCount) * sizeof(TriRec) * 3;  // the leaf-order triangles and their two rotations
     if (buildMs) *buildMs = s->buildMs;
     return X2_OK;
 }

@@ -9,6 +9,9 @@
 //                   order from childBase, leaf triangles from triBase), so a node costs five 16-byte loads.
 //   TriRec[tris]    48 B each, three float4: the vertices (fp32, as the scene gives them) with the triangle's
 //                   scene index in v0.w (bit cast), stored in leaf order so a leaf's 1-3 triangles are adjacent.
+//   two more TriRec[tris] copies with each vertex's coordinates rotated to (y, z, x) and (z, x, y): the watertight
+//                   test wants a vertex's coordinates in the order (kx, ky, kz) of its ray's dominant axis kz, and
+//                   a ray reads the copy of its axis (the original serves kz = 2) instead of picking components.
 // The reference delegates traversal to Embree / OptiX RT cores (async_cpu.h:669-720, async_gpu_device.h:
 // 330-355, 521-533); B200 has no RT cores, so this is the engine's own.
 #pragma once
@@ -34,7 +37,8 @@ struct Bvh8 {
     const Node8* nodes;
     const TriRec* tris;
     uint32_t nodeCount, triCount;
-    float lo[3], hi[3];  // the scene's bounds, for each ray's distance tolerance (traverse.cuh, makeRay)
+    float lo[3], hi[3];     // the scene's bounds, for each ray's distance tolerance (traverse.cuh, makeRay)
+    const TriRec* rot[3];   // by dominant axis kz: the triangles rotated to (kx, ky, kz) (rot[2] is tris)
 };
 
 }  // namespace x2

@@ -332,6 +332,22 @@ struct CollapseArgs {
 
 // One wide node from binary node `b`: open the largest-area internal node until eight children; binary subtrees of
 // at most three triangles become leaves; order the slots by direction octant; quantise the child boxes.
+// The leaf-order triangles with each vertex's coordinates rotated: (y, z, x) for rays whose dominant axis is x, and
+// (z, x, y) for y (traverse.cuh triTestRotated); the scene index stays in v0.w.
+__global__ void rotateTriangles(const TriRec* __restrict__ tris, uint32_t n, TriRec* __restrict__ yzx, TriRec* __restrict__ zxy) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const TriRec t = tris[i];
+    const float4 v[3] = {t.v0, t.v1, t.v2};
+    float4 a[3], b[3];
+    for (int k = 0; k < 3; ++k) {
+        a[k] = make_float4(v[k].y, v[k].z, v[k].x, v[k].w);
+        b[k] = make_float4(v[k].z, v[k].x, v[k].y, v[k].w);
+    }
+    yzx[i] = TriRec{a[0], a[1], a[2]};
+    zxy[i] = TriRec{b[0], b[1], b[2]};
+}
+
 __global__ void countLeafTriangles(const TriRec* __restrict__ tris, uint32_t n, unsigned* seen) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -637,6 +653,10 @@ int buildBvh(const float* dVertices, const uint32_t* dTriangles, uint32_t n, cud
         setError("BVH build: %u triangles not in exactly one leaf", host[3]);
         goto fail;
     }
+    CK(cudaMallocAsync(&out->rot[0], sizeof(TriRec) * n, stream));
+    CK(cudaMallocAsync(&out->rot[1], sizeof(TriRec) * n, stream));
+    rotateTriangles<<<grid, kBlock, 0, stream>>>(tris, n, out->rot[0], out->rot[1]);
+    CK(cudaGetLastError());
     out->nodes = nodes;
     out->tris = tris;
     out->nodeCount = host[0];
@@ -664,6 +684,11 @@ fail:
     cudaFreeAsync(temp, stream);
     if (nodes) cudaFreeAsync(nodes, stream);
     if (tris) cudaFreeAsync(tris, stream);
+    if (!out->nodes)
+        for (TriRec*& r : out->rot) {
+            if (r) cudaFreeAsync(r, stream);
+            r = nullptr;
+        }
     cudaStreamSynchronize(stream);
     return out->nodes ? 0 : 1;
 }

@@ -20,6 +20,7 @@ int contextStream(x2_ctx* ctx, cudaStream_t* stream, int* smCount);
 struct DeviceBvh {
     Node8* nodes = nullptr;
     TriRec* tris = nullptr;
+    TriRec* rot[2] = {nullptr, nullptr};  // the triangles rotated to (y, z, x) and (z, x, y)
     uint32_t nodeCount = 0, triCount = 0, levels = 0;
 };
 

@@ -23,9 +23,10 @@ struct RayQ {
     float ox, oy, oz, dx, dy, dz;
     float ix, iy, iz;  // inverse direction for the box test (components below 1e-18 clamped)
     uint32_t oct7;     // XOR pattern that orders a node's slots near to far
-    int kx, ky, kz;    // the shear's axes
+    int kz;            // the shear's axes: kz the dominant one, kx = kz + 1 and ky = kz + 2 (mod 3)
     float Sx, Sy, Sz;
     float okx, oky, okz;  // the origin's components along kx, ky, kz
+    const TriRec* tris;   // the leaf-order triangles rotated to (kx, ky, kz)
     // The triangle test's t carries an absolute error of a few ulps of the distance to the vertices (its sheared
     // products cancel), which a near hit can make large relative to t: boxes are tested against [tmin - eps,
     // tmax + eps], eps = 2^-18 times the ray origin's distance to the farthest corner of the scene's bounds.
@@ -56,17 +57,10 @@ __device__ __forceinline__ RayQ makeRay(const Bvh8& bvh, float ox, float oy, flo
     const uint32_t oct = (signbit(dx) ? 1u : 0u) | (signbit(dy) ? 2u : 0u) | (signbit(dz) ? 4u : 0u);
     r.oct7 = ~oct & 7u;
     const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
-    int kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
-    int kx = kz == 2 ? 0 : kz + 1;
-    int ky = kx == 2 ? 0 : kx + 1;
+    const int kz = ax > ay ? (ax > az ? 0 : 2) : (ay > az ? 1 : 2);
+    const int kx = kz == 2 ? 0 : kz + 1;
+    const int ky = kx == 2 ? 0 : kx + 1;
     const float dzz = pick3(dx, dy, dz, kz);
-    if (dzz < 0.0f) {
-        const int t = kx;
-        kx = ky;
-        ky = t;
-    }
-    r.kx = kx;
-    r.ky = ky;
     r.kz = kz;
     r.Sx = pick3(dx, dy, dz, kx) / dzz;
     r.Sy = pick3(dx, dy, dz, ky) / dzz;
@@ -74,20 +68,20 @@ __device__ __forceinline__ RayQ makeRay(const Bvh8& bvh, float ox, float oy, flo
     r.okx = pick3(ox, oy, oz, kx);
     r.oky = pick3(ox, oy, oz, ky);
     r.okz = pick3(ox, oy, oz, kz);
+    r.tris = kz == 0 ? bvh.rot[0] : kz == 1 ? bvh.rot[1] : bvh.rot[2];  // constant indices: bvh stays in registers
     return r;
 }
 
-// Watertight ray/triangle test; the operations match the oracle's triHit exactly.
-__device__ __forceinline__ bool triTest(const RayQ& r, const float4& a, const float4& b, const float4& c, float tmin, float tmax, float& tOut) {
-    const float Akx = pick3(a.x, a.y, a.z, r.kx) - r.okx;
-    const float Aky = pick3(a.x, a.y, a.z, r.ky) - r.oky;
-    const float Akz = pick3(a.x, a.y, a.z, r.kz) - r.okz;
-    const float Bkx = pick3(b.x, b.y, b.z, r.kx) - r.okx;
-    const float Bky = pick3(b.x, b.y, b.z, r.ky) - r.oky;
-    const float Bkz = pick3(b.x, b.y, b.z, r.kz) - r.okz;
-    const float Ckx = pick3(c.x, c.y, c.z, r.kx) - r.okx;
-    const float Cky = pick3(c.x, c.y, c.z, r.ky) - r.oky;
-    const float Ckz = pick3(c.x, c.y, c.z, r.kz) - r.okz;
+// Watertight ray/triangle test on vertices whose coordinates come in the ray's (kx, ky, kz) order. The oracle's triHit
+// swaps kx and ky when the dominant direction component is negative, to keep the edge functions' signs; here the axes
+// stay in rotation order, which negates U, V, W, their sum and T exactly (a product's operands commute, and a
+// difference's operands exchanged give its exact negation, in float and in the double fallback alike), so the test's
+// outcome (the same-sign test, the zero determinant) and t = T / det are bit for bit the oracle's.
+__device__ __forceinline__ bool triTestRotated(const RayQ& r, const float4& a, const float4& b, const float4& c, float tmin, float tmax,
+                                               float& tOut) {
+    const float Akx = a.x - r.okx, Aky = a.y - r.oky, Akz = a.z - r.okz;
+    const float Bkx = b.x - r.okx, Bky = b.y - r.oky, Bkz = b.z - r.okz;
+    const float Ckx = c.x - r.okx, Cky = c.y - r.oky, Ckz = c.z - r.okz;
     const float Ax = Akx - r.Sx * Akz, Ay = Aky - r.Sy * Akz;
     const float Bx = Bkx - r.Sx * Bkz, By = Bky - r.Sy * Bkz;
     const float Cx = Ckx - r.Sx * Ckz, Cy = Cky - r.Sy * Ckz;
@@ -106,6 +100,12 @@ __device__ __forceinline__ bool triTest(const RayQ& r, const float4& a, const fl
     if (!(t >= tmin && t <= tmax)) return false;
     tOut = t;
     return true;
+}
+// The same test on vertices in scene order (x, y, z): picks each vertex's coordinates in the ray's axis order.
+__device__ __forceinline__ bool triTest(const RayQ& r, const float4& a, const float4& b, const float4& c, float tmin, float tmax, float& tOut) {
+    const int kx = r.kz == 2 ? 0 : r.kz + 1, ky = kx == 2 ? 0 : kx + 1;
+    auto rotate = [&](const float4& v) { return make_float4(pick3(v.x, v.y, v.z, kx), pick3(v.x, v.y, v.z, ky), pick3(v.x, v.y, v.z, r.kz), v.w); };
+    return triTestRotated(r, rotate(a), rotate(b), rotate(c), tmin, tmax, tOut);
 }
 
 // Three-input max / min (one instruction on sm_100; same NaN rule as fmaxf / fminf).
@@ -208,11 +208,11 @@ static __device__ __noinline__ uint32_t traceClosest(const Bvh8 bvh, const RayQ&
             while (tBits) {
                 const uint32_t k = __ffs(tBits) - 1;
                 tBits &= tBits - 1;
-                const float4* tp = reinterpret_cast<const float4*>(bvh.tris + triBase + k);
+                const float4* tp = reinterpret_cast<const float4*>(r.tris + triBase + k);
                 const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
                 if (kStats) ++tris;
                 float t;
-                if (triTest(r, v0, v1, v2, tmin, tBest, t)) {
+                if (triTestRotated(r, v0, v1, v2, tmin, tBest, t)) {
                     const uint32_t id = __float_as_uint(v0.w);
                     if (t < tBest || (t == tBest && id < best)) {
                         tBest = t;
@@ -334,11 +334,11 @@ __device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk<kS
     for (uint32_t n = 0; w.tbits && n < triLimit; ++n) {
         const uint32_t k = __ffs(w.tbits) - 1;
         w.tbits &= w.tbits - 1;
-        const float4* tp = reinterpret_cast<const float4*>(bvh.tris + w.tbase + k);
+        const float4* tp = reinterpret_cast<const float4*>(r.tris + w.tbase + k);
         const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
         ++w.tris;
         float t;
-        if (triTest(r, v0, v1, v2, w.tmin, w.tmax, t)) {
+        if (triTestRotated(r, v0, v1, v2, w.tmin, w.tmax, t)) {
             if (kAny) {
                 w.best = 1;
                 return true;
@@ -379,11 +379,11 @@ static __device__ __noinline__ bool traceAny(const Bvh8 bvh, const RayQ& r, floa
             while (tBits) {
                 const uint32_t k = __ffs(tBits) - 1;
                 tBits &= tBits - 1;
-                const float4* tp = reinterpret_cast<const float4*>(bvh.tris + triBase + k);
+                const float4* tp = reinterpret_cast<const float4*>(r.tris + triBase + k);
                 const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
                 if (kStats) ++tris;
                 float t;
-                if (triTest(r, v0, v1, v2, tmin, tmax, t)) {
+                if (triTestRotated(r, v0, v1, v2, tmin, tmax, t)) {
                     hit = true;
                     goto done;
                 }
