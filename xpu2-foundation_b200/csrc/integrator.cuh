@@ -256,8 +256,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
             const float u = ls.next();
             if (split) {
                 const Identity strat{pixel, U64(index) * nl + si, U64(c.seed), lightAddress};
-                r[0] = draw(strat, CameraDimensions + 2, policy);
-                r[1] = draw(strat, CameraDimensions + 3, policy);
+                drawPair(strat, CameraDimensions + 2, policy, r[0], r[1]);
             }
             V3 wi;
             LightHit lh;
@@ -322,8 +321,7 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
         const float choice = bs.next(), u = bs.next();
         if (split && !mirror) {
             const Identity strat{pixel, U64(index) * nk + i, U64(c.seed), lobeBranch};
-            r1 = draw(strat, CameraDimensions, policy);
-            r2 = draw(strat, CameraDimensions + 1, policy);
+            drawPair(strat, CameraDimensions, policy, r1, r2);
         }
         V3 wi;
         float pdf;

@@ -205,7 +205,14 @@ __global__ void sampleWords(const x2_identity* __restrict__ ids, const uint32_t*
     for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const x2_identity x = ids[i];
         const Identity id{x.pixel, x.index, x.stream, x.branch};
-        out[i] = samplingWord(id, dims[i], policy);
+        const uint32_t d = dims[i];
+        if (d >= 16 && d <= 19) {  // the BSDF and light pairs, as the integrator draws them
+            uint32_t a, b;
+            samplingWordPair(id, d & ~1u, policy, a, b);
+            out[i] = d & 1u ? b : a;
+        } else {
+            out[i] = samplingWord(id, d, policy);
+        }
     }
 }
 

@@ -95,6 +95,35 @@ __device__ __forceinline__ float draw(const Identity& id, U32 dimension, U32 pol
     return unit(samplingWord(id, dimension, policy));
 }
 
+// samplingWord(id, d) and samplingWord(id, d + 1) for the BSDF pair (d = 16) or the light pair (d = 18): the two
+// dimensions share their Philox group (and, where the policy takes Sobol, their seed block and the index's Gray-code
+// bits), so one block and one pass over the bits give both words.
+__device__ __forceinline__ void samplingWordPair(const Identity& id, U32 dimension, U32 policy, U32& a, U32& b) {
+    const bool sobolPair = dimension == 16 ? (policy & 2) != 0 : (policy & 4) != 0;
+    if (!sobolPair) {
+        const Words w = block(id.pixel, id.index, id.stream, id.branch, dimension >> 2);
+        a = pick(w, dimension & 3);
+        b = pick(w, (dimension + 1) & 3);
+        return;
+    }
+    const U32 d = dimension - 14;
+    const Words seeds = block(id.pixel, id.index >> 32, id.stream, id.branch, 0x534f424fu + (d >> 2));
+    U32 gray = U32(id.index) ^ (U32(id.index) >> 1), r0 = 0, r1 = 0;
+    for (U32 bit = 0; gray; ++bit, gray >>= 1)
+        if (gray & 1u) {
+            r0 ^= c_sobol[d][bit];
+            r1 ^= c_sobol[d + 1][bit];
+        }
+    a = owenScramble(r0, pick(seeds, d & 3));
+    b = owenScramble(r1, pick(seeds, (d + 1) & 3));
+}
+__device__ __forceinline__ void drawPair(const Identity& id, U32 dimension, U32 policy, float& a, float& b) {
+    U32 wa, wb;
+    samplingWordPair(id, dimension, policy, wa, wb);
+    a = unit(wa);
+    b = unit(wb);
+}
+
 constexpr U32 CameraDimensions = 16, DimensionsPerBounce = 256;
 
 // A vertex's uniform numbers: dimension 16 + bounce * 256 + offset of its branch's Philox stream, one block per
