@@ -269,12 +269,15 @@ typedef struct x2_wavefront_shape {
     uint32_t short_stack;    /* 1: the traversal stacks' first 8 entries in shared memory; 0: all in local memory */
     uint32_t shade_split;    /* 1: shade as one kernel a per-lobe queue (GGX, Lambert, the rest; with lobe_queues 1, surface
                                 scenes), each holding one lobe's code; 0: one shade kernel */
+    uint32_t light_split;    /* 1, 2 (with shade_split): the GGX and Lambert vertices' light samples in kernels of their
+                                own, after shade, from the vertex's stored inputs, at 6 (1) or 8 (2) blocks a SM; 0: inside
+                                shade */
 } x2_wavefront_shape;
 void x2_wavefront_shape_defaults(x2_wavefront_shape* shape);
 int x2_wavefront_tune(x2_scene* scene, const x2_wavefront_shape* shape);
 /* The autotuner: times wavefront launches of `tiles` evenly spaced tiles (0: all) at `spp` samples, one knob at a time
  * (paths, refill, tri_limit, shade_blocks, trace_blocks, blocks_per_sm, lobe_queues, shadow_order, extend_bins,
- * short_stack, shade_split; best of two launches a candidate), sets the
+ * short_stack, shade_split, light_split; best of two launches a candidate), sets the
  * fastest shape and returns it (best, best_ms may be null). Renders into the scene's film, which it leaves reset (as
  * x2_frame_begin(scene, spp)). Waits. */
 int x2_wavefront_autotune(x2_scene* scene, uint32_t tiles, uint32_t spp, x2_wavefront_shape* best, float* best_ms);

@@ -223,6 +223,7 @@ struct x2_scene {
     uint32_t extendBins = kDefaultExtendBins;    // the extend queue binned by octant (1) or in slot order (0)
     uint32_t shortStack = kDefaultShortStack;    // traversal stacks' top entries in shared memory (1) or local (0)
     uint32_t shadeSplit = kDefaultShadeSplit;    // shade as one kernel a per-lobe queue (1) or one kernel (0)
+    uint32_t lightSplit = kDefaultLightSplit;    // the lobe queues' light samples in kernels of their own (1)
     uint32_t* shadeQ = nullptr;            // the per-lobe queues: 3 x wavePaths entries
     uint32_t batchWindow = 0;              // x2_render_batch: items a window (0: the default)
     uint32_t* hostLast = nullptr;      // pinned
@@ -344,7 +345,8 @@ void retire(x2_scene* s, Slot& sl, x2_completion* out) {
 
 void freeWave(x2_scene* s) {
     WaveState& w = s->wave;
-    void* ptrs[] = {w.ray0, w.ray1, w.T, w.held, w.meta, w.branch, w.rad, w.hit, w.state, w.item, w.ncount, w.sray0, w.sray1, w.scontrib, w.svis};
+    void* ptrs[] = {w.ray0, w.ray1, w.T, w.held, w.meta, w.branch, w.rad, w.hit, w.state, w.item, w.ncount, w.sray0, w.sray1, w.scontrib, w.svis,
+                    w.lightJob, w.lightFlags};
     for (void* p : ptrs) cudaFree(p);
     w = WaveState{};
     cudaFree(s->extendQ);
@@ -373,7 +375,9 @@ int ensureWave(x2_scene* s, uint32_t paths, uint32_t records) {
               cudaMalloc(&w.ncount, sizeof(uint32_t) * P) == cudaSuccess && cudaMalloc(&w.sray0, sizeof(float4) * R) == cudaSuccess &&
               cudaMalloc(&w.sray1, sizeof(float4) * R) == cudaSuccess && cudaMalloc(&w.scontrib, sizeof(float4) * R) == cudaSuccess &&
               cudaMalloc(&w.svis, R) == cudaSuccess && cudaMalloc(&s->extendQ, sizeof(uint32_t) * kOctants * P) == cudaSuccess &&
-              cudaMalloc(&s->shadowQ, sizeof(uint32_t) * R) == cudaSuccess && cudaMalloc(&s->shadeQ, sizeof(uint32_t) * 3 * P) == cudaSuccess;
+              cudaMalloc(&s->shadowQ, sizeof(uint32_t) * R) == cudaSuccess && cudaMalloc(&s->shadeQ, sizeof(uint32_t) * 3 * P) == cudaSuccess &&
+              cudaMalloc(&w.lightJob, sizeof(uint4) * kLightJobWords * P) == cudaSuccess &&
+              cudaMalloc(&w.lightFlags, sizeof(uint32_t) * P) == cudaSuccess;
     if (ok && !s->waveCounters) ok = cudaMalloc(&s->waveCounters, sizeof(uint32_t) * kWaveCounters) == cudaSuccess;
     if (ok && !s->claimed) ok = cudaMalloc(&s->claimed, sizeof(unsigned long long)) == cudaSuccess;
     if (ok && !s->hostLast) ok = cudaMallocHost(&s->hostLast, sizeof(uint32_t) * 4) == cudaSuccess;
@@ -1256,14 +1260,16 @@ void x2_wavefront_shape_defaults(x2_wavefront_shape* shape) {
     shape->extend_bins = kDefaultExtendBins;
     shape->short_stack = kDefaultShortStack;
     shape->shade_split = kDefaultShadeSplit;
+    shape->light_split = kDefaultLightSplit;
 }
 
 int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     if (!s || !shape || shape->refill < 1 || shape->refill > 32 || shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 ||
         shape->trace_blocks > 32 || shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32 || shape->lobe_queues > 1 ||
-        shape->shadow_order > 1 || shape->extend_bins > 1 || shape->short_stack > 1 || shape->shade_split > 1) {
+        shape->shadow_order > 1 || shape->extend_bins > 1 || shape->short_stack > 1 || shape->shade_split > 1 ||
+        shape->light_split > 2) {
         setError("refill is 1..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32, lobe_queues, "
-                 "shadow_order, extend_bins, short_stack and shade_split 0 or 1");
+                 "shadow_order, extend_bins, short_stack and shade_split 0 or 1, light_split 0..2");
         return X2_EINVAL;
     }
     s->reservePaths = shape->paths;
@@ -1278,6 +1284,7 @@ int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     s->extendBins = shape->extend_bins;
     s->shortStack = shape->short_stack;
     s->shadeSplit = shape->shade_split;
+    s->lightSplit = shape->light_split;
     return X2_OK;
 }
 
@@ -1366,7 +1373,8 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
     const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0,
-                                       a.scene.stats != nullptr, s->shadeSplit != 0);
+                                       a.scene.stats != nullptr, s->shadeSplit != 0,
+                                       s->wave.lightJob != nullptr ? s->lightSplit : 0u);
     const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     if (s->waveTiming) {
         // Diagnostic form: no graph; events around every kernel, the iteration's times added once it is done.
@@ -2120,7 +2128,8 @@ int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float 
     const int gridLogic = int((paths + kWaveBlock - 1) / kWaveBlock);
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
     const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0,
-                                       a.scene.stats != nullptr, s->shadeSplit != 0);
+                                       a.scene.stats != nullptr, s->shadeSplit != 0,
+                                       s->wave.lightJob != nullptr ? s->lightSplit : 0u);
     const uint64_t bound = maxItems * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     const uint32_t maxIter = uint32_t(std::min<uint64_t>(bound, 0xffffffffu));
 
@@ -2447,7 +2456,8 @@ int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefron
                           {&x2_wavefront_shape::shadow_order, {0, 1}},
                           {&x2_wavefront_shape::extend_bins, {0, 1}},
                           {&x2_wavefront_shape::short_stack, {0, 1}},
-                          {&x2_wavefront_shape::shade_split, {0, 1}}};
+                          {&x2_wavefront_shape::shade_split, {0, 1}},
+                          {&x2_wavefront_shape::light_split, {0, 1, 2}}};
     for (const Knob& k : knobs) {
         x2_wavefront_shape keep = cur;
         for (uint32_t v : k.values) {

@@ -172,6 +172,99 @@ struct ShadowReq {
     uint32_t light;  // the light it reaches
 };
 
+// What a vertex's light samples read: the shading point and its frame, the path's throughput and identity, the lobe,
+// and the vertex's sampling switches (shadeVertex fills it).
+struct LightJob {
+    V3 P, Ng, wo, T, above, below, cull;
+    Lobe lobe;
+    U64 branch;
+    uint32_t pixel, index, depth, nl, nk;
+    bool hasCull, split, clampHere, rr;
+};
+
+// A vertex's light samples (async_integrator.h:2633-2772): every light of the set that can light the hit, each sample's
+// contribution, MIS-weighted against the lobe, clamped and rouletted, to the sink as a shadow request, in light order.
+// root: the sample's identity (pixel, index, the frame seed, branch 0).
+template <bool kVolumes, int kLobe, class Sink>
+__device__ __forceinline__ void lightSamples(const SceneView& s, const Identity& root, const LightJob& j, Sink& sink) {
+    const x2_config& c = s.config;
+    const uint32_t policy = c.sampling;
+    const bool volumes = kVolumes && c.volume_count;
+    const V3* cullN = j.hasCull ? &j.cull : nullptr;
+    const Slice slice{j.Ng, j.wo};
+    const uint32_t nl = j.nl, nk = j.nk;
+    const uint32_t pixel = j.pixel, index = j.index;
+    const Lobe& lobe = j.lobe;
+    const V3 above = j.above, below = j.below;
+    const U64 lightBranch = childBranch(j.branch, 0xfffe, 0);
+    for (uint32_t i = 0; i < c.light_count; ++i) {
+        const x2_light& L = s.lights[i];
+        if (!canIlluminate(L, j.P, cullN)) continue;
+        const U64 lightAddress = childBranch(lightBranch, i, 0);
+        Identity lid = root;
+        lid.branch = lightAddress;
+        Stream ls(lid, j.depth, 0);
+        for (uint32_t si = 0; si < nl; ++si) {
+            float r[3];
+            r[0] = ls.next();
+            r[1] = ls.next();
+            r[2] = ls.next();
+            const float u = ls.next();
+            if (j.split) {
+                const Identity strat{pixel, U64(index) * nl + si, U64(c.seed), lightAddress};
+                drawPair(strat, CameraDimensions + 2, policy, r[0], r[1]);
+            }
+            V3 wi;
+            LightHit lh;
+            if (!lightSample(L, j.P, cullN, r, wi, lh)) continue;
+            float pdfL;
+            const V3 Li = lightEval(L, wi, lh, pdfL);
+            if (pdfL == 0.0f || isExactlyZero(Li) || !(fabsf(pdfL) < 3.4e38f) || !finite3(Li)) continue;
+            const V3 factor = mul(mulv(j.T, Li), 1.0f / (float(nl) * pdfL * 1.0f));
+            const uint32_t flags = surfaceFlags(slice, wi);
+            V3 t{0, 0, 0};
+            bool any = false;
+            if (matchesFlags(lobe.type, flags) && (lobeRayMask(lobe.type) & L.visibility_mask)) {
+                float pdf;
+                const V3 f = lobeEvalAs<kLobe>(lobe, slice, wi, pdf);
+                if (!(pdf == 0.0f || isExactlyZero(f))) {
+                    V3 tk = mul(mulv(factor, f), powerHeuristic(float(nl) * pdfL, float(nk) * pdf));
+                    if (j.clampHere && c.clamp_value > 0) {
+                        const float mx = fmaxf(tk.x, fmaxf(tk.y, tk.z));
+                        if (mx > c.clamp_value) tk = mul(tk, c.clamp_value / mx);
+                    }
+                    t = add(t, tk);
+                    any = true;
+                }
+            }
+            if (!any) continue;
+            if (j.rr) {
+                float scale;
+                if (!roulette(luminance(t), c.rr_threshold, u, scale)) continue;
+                t = mul(t, scale);
+            }
+            if (!finite3(t) || isExactlyZero(t)) continue;
+            ShadowReq q;
+            q.origin = dot(wi, j.Ng) >= 0.0f ? above : below;
+            q.dir = wi;
+            q.near = fmaxf(0.0f, 0.0f);
+            q.far = fmaxf((lh.distance - 0.0f) * kHitEpsilonEnd, 2.0f * q.near);
+            if (volumes) {
+                // The volumes on the shadow ray's way (transmittance(), async_integrator.h:2722-2731); it matters only
+                // when nothing occludes the ray, and its stream is its own, so it is taken here.
+                Identity tid = lid;
+                tid.branch = childBranch(lightAddress, si, 0xfffb);
+                Stream vs(tid, j.depth, 0);
+                t = s.config.volume_estimator == 1 ? mul(t, trackedTransmittance(s, vs, q.origin, wi, q.near, q.far))
+                                                   : mulv(t, volumeTransmittance(s, vs, q.origin, wi, q.near, q.far, 1.0f, int(j.depth) + 1));
+            }
+            q.contribution = t;
+            q.light = i;
+            sink.shadow(q, false);
+        }
+    }
+}
+
 // One hit (async_integrator.h:2222-3031 for the admitted materials): shading state, emission, a light sample of
 // every light that can light the hit, the lobe's BSDF sample, and its child. `top` is the pending stack's size after
 // this vertex was popped. The sink takes shadow rays (shadow(req, bsdf)) and the child (push(child) -> bool).
@@ -179,7 +272,8 @@ struct ShadowReq {
 // false compiles the texture lookup out (the kernels for scenes whose materials read no texture).
 // kLobe: the lobe kind every vertex of the launch makes (1 Lambert, 2 GGX; 0 any), as the per-lobe shade queues sort
 // them; the kernel then holds one lobe's evaluation and sampling code.
-template <bool kVolumes = true, bool kTextures = true, int kLobe = 0, class Sink>
+// kDeferLights: the light samples are not taken here; the sink gets the vertex's LightJob (sink.lights) instead.
+template <bool kVolumes = true, bool kTextures = true, int kLobe = 0, bool kDeferLights = false, class Sink>
 __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& root, uint32_t pixel, uint32_t index, const Pending& pv,
                                             const Hit& hit, V3 va, V3 vb, V3 vc, uint32_t top, V3& radiance, float& alpha, Sink& sink) {
     const x2_config& c = s.config;
@@ -239,73 +333,30 @@ __device__ __forceinline__ bool shadeVertex(const SceneView& s, const Identity& 
     }();
     const V3 above = hit.origin, below = hit.below;
 
-    // Light samples (async_integrator.h:2633-2772): every light of the set that can light the hit.
-    const U64 lightBranch = childBranch(pv.branch, 0xfffe, 0);
-    for (uint32_t i = 0; i < c.light_count; ++i) {
-        const x2_light& L = s.lights[i];
-        if (!canIlluminate(L, st.P, cullN)) continue;
-        const U64 lightAddress = childBranch(lightBranch, i, 0);
-        Identity lid = root;
-        lid.branch = lightAddress;
-        Stream ls(lid, pv.depth, 0);
-        for (uint32_t si = 0; si < nl; ++si) {
-            float r[3];
-            r[0] = ls.next();
-            r[1] = ls.next();
-            r[2] = ls.next();
-            const float u = ls.next();
-            if (split) {
-                const Identity strat{pixel, U64(index) * nl + si, U64(c.seed), lightAddress};
-                drawPair(strat, CameraDimensions + 2, policy, r[0], r[1]);
-            }
-            V3 wi;
-            LightHit lh;
-            if (!lightSample(L, st.P, cullN, r, wi, lh)) continue;
-            float pdfL;
-            const V3 Li = lightEval(L, wi, lh, pdfL);
-            if (pdfL == 0.0f || isExactlyZero(Li) || !(fabsf(pdfL) < 3.4e38f) || !finite3(Li)) continue;
-            const V3 factor = mul(mulv(pv.T, Li), 1.0f / (float(nl) * pdfL * 1.0f));
-            const uint32_t flags = surfaceFlags(slice, wi);
-            V3 t{0, 0, 0};
-            bool any = false;
-            if (matchesFlags(lobe.type, flags) && (lobeRayMask(lobe.type) & L.visibility_mask)) {
-                float pdf;
-                const V3 f = lobeEvalAs<kLobe>(lobe, slice, wi, pdf);
-                if (!(pdf == 0.0f || isExactlyZero(f))) {
-                    V3 tk = mul(mulv(factor, f), powerHeuristic(float(nl) * pdfL, float(nk) * pdf));
-                    if (clampHere && c.clamp_value > 0) {
-                        const float mx = fmaxf(tk.x, fmaxf(tk.y, tk.z));
-                        if (mx > c.clamp_value) tk = mul(tk, c.clamp_value / mx);
-                    }
-                    t = add(t, tk);
-                    any = true;
-                }
-            }
-            if (!any) continue;
-            if (rr) {
-                float scale;
-                if (!roulette(luminance(t), c.rr_threshold, u, scale)) continue;
-                t = mul(t, scale);
-            }
-            if (!finite3(t) || isExactlyZero(t)) continue;
-            ShadowReq q;
-            q.origin = dot(wi, st.Ng) >= 0.0f ? above : below;
-            q.dir = wi;
-            q.near = fmaxf(0.0f, 0.0f);
-            q.far = fmaxf((lh.distance - 0.0f) * kHitEpsilonEnd, 2.0f * q.near);
-            if (volumes) {
-                // The volumes on the shadow ray's way (transmittance(), async_integrator.h:2722-2731); it matters only
-                // when nothing occludes the ray, and its stream is its own, so it is taken here.
-                Identity tid = lid;
-                tid.branch = childBranch(lightAddress, si, 0xfffb);
-                Stream vs(tid, pv.depth, 0);
-                t = s.config.volume_estimator == 1 ? mul(t, trackedTransmittance(s, vs, q.origin, wi, q.near, q.far))
-                                                   : mulv(t, volumeTransmittance(s, vs, q.origin, wi, q.near, q.far, 1.0f, int(pv.depth) + 1));
-            }
-            q.contribution = t;
-            q.light = i;
-            sink.shadow(q, false);
-        }
+    // Light samples: here, or (kDeferLights) handed to the sink for a kernel of their own, which runs lightSamples on the
+    // same job.
+    {
+        LightJob job;
+        job.P = st.P;
+        job.Ng = st.Ng;
+        job.wo = st.wo;
+        job.T = pv.T;
+        job.above = above;
+        job.below = below;
+        job.cull = cull;
+        job.hasCull = cullN != nullptr;
+        job.lobe = lobe;
+        job.branch = pv.branch;
+        job.pixel = pixel;
+        job.index = index;
+        job.depth = pv.depth;
+        job.nl = nl;
+        job.nk = nk;
+        job.split = split;
+        job.clampHere = clampHere;
+        job.rr = rr;
+        if constexpr (kDeferLights) sink.lights(job);
+        else lightSamples<kVolumes, kLobe>(s, root, job, sink);
     }
 
     // The lobe's BSDF samples (async_integrator.h:2792-3031).

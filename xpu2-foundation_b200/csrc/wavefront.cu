@@ -450,7 +450,63 @@ __device__ __forceinline__ void extendBody(const WaveArgs& a) {
 // ---- shade ----
 // The wavefront's sink: shadow rays to the path's record slots, the child to the slot. kAdjoint: also the vertex
 // records the adjoint credits at the path's end and each record's light and own roughness factor.
-template <bool kAdjoint = false>
+// A vertex's LightJob in the wave state (kLightJobWords uint4 a slot) and back.
+__device__ __forceinline__ void storeLightJob(const WaveState& w, uint32_t p, const LightJob& j) {
+    uint4* q = w.lightJob + size_t(p) * kLightJobWords;
+    auto f = [](float x) { return __float_as_uint(x); };
+    const Lobe& l = j.lobe;
+    const uint32_t flags = (j.hasCull ? 1u : 0u) | (j.split ? 2u : 0u) | (j.clampHere ? 4u : 0u) | (j.rr ? 8u : 0u) | (l.kind << 4);
+    q[0] = make_uint4(f(j.P.x), f(j.P.y), f(j.P.z), f(j.Ng.x));
+    q[1] = make_uint4(f(j.Ng.y), f(j.Ng.z), f(j.wo.x), f(j.wo.y));
+    q[2] = make_uint4(f(j.wo.z), f(j.T.x), f(j.T.y), f(j.T.z));
+    q[3] = make_uint4(f(j.above.x), f(j.above.y), f(j.above.z), f(j.below.x));
+    q[4] = make_uint4(f(j.below.y), f(j.below.z), f(j.cull.x), f(j.cull.y));
+    q[5] = make_uint4(f(j.cull.z), f(l.frame.x.x), f(l.frame.x.y), f(l.frame.x.z));
+    q[6] = make_uint4(f(l.frame.y.x), f(l.frame.y.y), f(l.frame.y.z), f(l.frame.z.x));
+    q[7] = make_uint4(f(l.frame.z.y), f(l.frame.z.z), f(l.albedo.x), f(l.albedo.y));
+    q[8] = make_uint4(f(l.albedo.z), f(l.spec.x), f(l.spec.y), f(l.spec.z));
+    q[9] = make_uint4(f(l.roughness), uint32_t(j.branch), uint32_t(j.branch >> 32), l.type);
+    q[10] = make_uint4(j.pixel, j.index, j.depth | (flags << 16), j.nl | (j.nk << 16));
+}
+__device__ __forceinline__ LightJob loadLightJob(const WaveState& w, uint32_t p) {
+    const uint4* q = w.lightJob + size_t(p) * kLightJobWords;
+    uint4 v[kLightJobWords];
+#pragma unroll
+    for (uint32_t k = 0; k < kLightJobWords; ++k) v[k] = q[k];
+    auto f = [](uint32_t x) { return __uint_as_float(x); };
+    LightJob j;
+    j.P = V3{f(v[0].x), f(v[0].y), f(v[0].z)};
+    j.Ng = V3{f(v[0].w), f(v[1].x), f(v[1].y)};
+    j.wo = V3{f(v[1].z), f(v[1].w), f(v[2].x)};
+    j.T = V3{f(v[2].y), f(v[2].z), f(v[2].w)};
+    j.above = V3{f(v[3].x), f(v[3].y), f(v[3].z)};
+    j.below = V3{f(v[3].w), f(v[4].x), f(v[4].y)};
+    j.cull = V3{f(v[4].z), f(v[4].w), f(v[5].x)};
+    j.lobe.frame.x = V3{f(v[5].y), f(v[5].z), f(v[5].w)};
+    j.lobe.frame.y = V3{f(v[6].x), f(v[6].y), f(v[6].z)};
+    j.lobe.frame.z = V3{f(v[6].w), f(v[7].x), f(v[7].y)};
+    j.lobe.albedo = V3{f(v[7].z), f(v[7].w), f(v[8].x)};
+    j.lobe.spec = V3{f(v[8].y), f(v[8].z), f(v[8].w)};
+    j.lobe.roughness = f(v[9].x);
+    j.branch = U64(v[9].y) | (U64(v[9].z) << 32);
+    j.lobe.type = v[9].w;
+    j.pixel = v[10].x;
+    j.index = v[10].y;
+    j.depth = v[10].z & 0xffffu;
+    const uint32_t flags = v[10].z >> 16;
+    j.hasCull = flags & 1u;
+    j.split = flags & 2u;
+    j.clampHere = flags & 4u;
+    j.rr = flags & 8u;
+    j.lobe.kind = (flags >> 4) & 1u;
+    j.nl = v[10].w & 0xffffu;
+    j.nk = v[10].w >> 16;
+    return j;
+}
+
+// kDefer: the light samples are deferred to the light kernel (sink.lights stores the vertex's job), and the BSDF
+// sample's shadow record waits in the slot's last record, which the light kernel moves after the light records.
+template <bool kAdjoint = false, bool kDefer = false>
 struct WaveSink {
     const WaveState& w;
     uint32_t p, n, recordsPerPath;
@@ -467,8 +523,22 @@ struct WaveSink {
     float materialRoughness;
     bool ggx, sampled;
 
+    bool deferred = false, stashed = false;  // kDefer: a job stored; the BSDF record stashed
+
+    __device__ void lights(const LightJob& j) {
+        if constexpr (kDefer) {
+            storeLightJob(w, p, j);
+            deferred = true;
+        }
+    }
     __device__ void shadow(const ShadowReq& q, bool isBsdf) {
-        const size_t k = size_t(p) * recordsPerPath + n++;
+        size_t k;
+        if (kDefer && isBsdf) {
+            k = size_t(p) * recordsPerPath + recordsPerPath - 1;
+            stashed = true;
+        } else {
+            k = size_t(p) * recordsPerPath + n++;
+        }
         w.sray0[k] = make_float4(q.origin.x, q.origin.y, q.origin.z, q.near);
         w.sray1[k] = make_float4(q.dir.x, q.dir.y, q.dir.z, q.far);
         w.scontrib[k] = make_float4(q.contribution.x, q.contribution.y, q.contribution.z, 0.0f);
@@ -574,9 +644,68 @@ __device__ __forceinline__ uint32_t shadeEntry(const WaveArgs& a, uint32_t i, ui
     return a.shadeQ[2ull * a.paths + (i - c0 - c1)];
 }
 
+// A path's `records` shadow records into the shadow queue (every lane of the warp calls it, each with its own count):
+// by record (record k of each lane's path into segment k) or by path.
+__device__ __forceinline__ void reserveShadows(const WaveArgs& a, uint32_t p, uint32_t records) {
+    if (a.shadowSlots) {
+        warpReserve(a.shadowCount, records);  // the total, for the host's statistics
+        const uint32_t most = __reduce_max_sync(0xffffffffu, records);
+        for (uint32_t k = 0; k < most; ++k) {
+            const uint32_t slot = warpReserve(a.shadowSlots + k, records > k ? 1u : 0u);
+            if (records > k) a.shadowQ[size_t(k) * a.paths + slot] = p * a.recordsPerPath + k;
+        }
+    } else {
+        const uint32_t slot = warpReserve(a.shadowCount, records);
+        for (uint32_t k = 0; k < records; ++k) a.shadowQ[slot + k] = p * a.recordsPerPath + k;
+    }
+}
+
+// The light samples of one per-lobe queue's vertices (kQueue 0 GGX, 1 Lambert), after its deferring shade kernel: each
+// slot's job through lightSamples — the arithmetic the fused shade runs — its records written from the slot's first,
+// then the BSDF sample's stashed record moved after them, the count and the shadow queue as the fused shade leaves
+// them.
+template <int kQueue>
+__device__ __forceinline__ void lightsBody(const WaveArgs& a) {
+    const WaveState& w = a.w;
+    const SceneView& s = a.scene;
+    const uint32_t n = a.shadeCount[kQueue];
+    const uint32_t R = a.recordsPerPath;
+    unsigned long long nee = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        uint32_t records = 0, p = 0;
+        if (i < n) {
+            p = a.shadeQ[size_t(kQueue) * a.paths + i];
+            const uint32_t flags = w.lightFlags[p];
+            WaveSink<false> sink{w, p, 0, R, false, Pending{}, 0, 0, 0};
+            if (flags & 1u) {
+                const LightJob j = loadLightJob(w, p);
+                const Identity root{j.pixel, U64(j.index), U64(s.config.seed), 0};
+                lightSamples<false, kQueue == 0 ? 2 : 1>(s, root, j, sink);
+            }
+            records = sink.n;
+            nee += sink.nNee;
+            const size_t first = size_t(p) * R;
+            if (flags & 2u) {
+                if (records != R - 1) {
+                    w.sray0[first + records] = w.sray0[first + R - 1];
+                    w.sray1[first + records] = w.sray1[first + R - 1];
+                    w.scontrib[first + records] = w.scontrib[first + R - 1];
+                }
+                ++records;
+            }
+            w.ncount[p] = records;
+            for (uint32_t k = 0; k < records; ++k) w.svis[first + k] = 0;
+        }
+        reserveShadows(a, p, records);
+    }
+    warpAddCounters(a.counters, 0, nee, 0, 0, 0, 0);
+}
+
 // kQueue: -1 every extended path (the per-lobe queues in order when they are on, else the extend queue); 0, 1, 2 one
 // per-lobe queue (GGX, Lambert, the rest), its kernel holding that lobe's code only.
-template <bool kBatch, bool kVolumes, bool kAdjoint = false, bool kTextures = true, int kQueue = -1>
+template <bool kBatch, bool kVolumes, bool kAdjoint = false, bool kTextures = true, int kQueue = -1, bool kDefer = false>
 __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
     const WaveState& w = a.w;
     const uint32_t n = kQueue < 0 ? *a.extendCount : a.shadeCount[kQueue];
@@ -589,7 +718,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
     const uint32_t stride = gridDim.x * blockDim.x;
     for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const uint32_t i = base + threadIdx.x;
-        uint32_t records = 0, p = 0;
+        uint32_t records = 0, p = 0, lightFlags = 0;
         if (i < n) {
             p = kQueue < 0 ? shadeEntry(a, i, c0, c1) : a.shadeQ[size_t(kQueue) * a.paths + i];
             Pending pv;
@@ -639,7 +768,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
             }
             uint32_t next = kDone;
             if (hit.geom != ~0u) {
-                WaveSink<kAdjoint> sink{w, p, 0, a.recordsPerPath, false, Pending{}, 0, 0, 0};
+                WaveSink<kAdjoint, kDefer> sink{w, p, 0, a.recordsPerPath, false, Pending{}, 0, 0, 0};
                 if (kAdjoint) {
                     sink.adj = &a.adj;
                     sink.s = &s;
@@ -647,8 +776,10 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
                     sink.depth = pv.depth;
                     sink.ggx = sink.sampled = false;
                 }
-                if (!shadeVertex<kVolumes, kTextures, kQueue == 0 ? 2 : kQueue == 1 ? 1 : 0>(s, root, pixel, index, pv, hit, va, vb, vc, 0u,
-                                                                                           radiance, alpha, sink)) {
+                const bool ok = shadeVertex<kVolumes, kTextures, kQueue == 0 ? 2 : kQueue == 1 ? 1 : 0, kDefer>(
+                    s, root, pixel, index, pv, hit, va, vb, vc, 0u, radiance, alpha, sink);
+                if (kDefer) lightFlags = (sink.deferred ? 1u : 0u) | (sink.stashed ? 2u : 0u);
+                if (!ok) {
                     next = kError;
                 } else {
                     records = sink.n;
@@ -662,23 +793,16 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
                 held += sink.nHeld;
             }
             w.rad[p] = make_float4(radiance.x, radiance.y, radiance.z, alpha);
-            w.ncount[p] = records;
             w.state[p] = next;
-            const size_t first = size_t(p) * a.recordsPerPath;
-            for (uint32_t k = 0; k < records; ++k) w.svis[first + k] = 0;
-        }
-        if (a.shadowSlots) {
-            // Record k of each lane's path into segment k; the total for the host's statistics.
-            warpReserve(a.shadowCount, records);
-            const uint32_t most = __reduce_max_sync(0xffffffffu, records);
-            for (uint32_t k = 0; k < most; ++k) {
-                const uint32_t slot = warpReserve(a.shadowSlots + k, records > k ? 1u : 0u);
-                if (records > k) a.shadowQ[size_t(k) * a.paths + slot] = p * a.recordsPerPath + k;
+            if (kDefer) {
+                w.lightFlags[p] = lightFlags;  // the light kernel makes the slot's records
+            } else {
+                w.ncount[p] = records;
+                const size_t first = size_t(p) * a.recordsPerPath;
+                for (uint32_t k = 0; k < records; ++k) w.svis[first + k] = 0;
             }
-        } else {
-            const uint32_t slot = warpReserve(a.shadowCount, records);
-            for (uint32_t k = 0; k < records; ++k) a.shadowQ[slot + k] = p * a.recordsPerPath + k;
         }
+        if (!kDefer) reserveShadows(a, p, records);
     }
     warpAddCounters(a.counters, 0, nee, bsdf, held, 0, 0);
     if (kAdjoint) partialsEnd(partial, at, a.adj);
@@ -751,26 +875,48 @@ template <int kQueue, bool kTextures, int kMinBlocks>
 __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadeQueue(WaveArgs a) {
     shadeBody<false, false, false, kTextures, kQueue>(a);
 }
+// With the light samples split off (light_split): the GGX and Lambert queues' shade without them, and their light
+// kernels.
+template <int kQueue, bool kTextures>
+__global__ void __launch_bounds__(kWaveBlock, 4) wfShadeDefer(WaveArgs a) {
+    shadeBody<false, false, false, kTextures, kQueue, true>(a);
+}
+template <int kQueue, int kMinBlocks>
+__global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfLightsQueue(WaveArgs a) {
+    lightsBody<kQueue>(a);
+}
 
 void launchShade(const WaveKernels& k, const WaveArgs& a, int grid, cudaStream_t st) {
     if (a.shadeQ) wfSortShade<<<grid, kWaveBlock, 0, st>>>(a);
     if (a.shadeQ && k.shadeBy[0]) {
         for (int q = 0; q < 3; ++q) k.shadeBy[q]<<<grid, kWaveBlock, 0, st>>>(a);
+        if (k.lightsBy[0])
+            for (int q = 0; q < 2; ++q) k.lightsBy[q]<<<grid, kWaveBlock, 0, st>>>(a);
     } else {
         k.shade<<<grid, kWaveBlock, 0, st>>>(a);
     }
 }
 
 WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack, bool counting,
-                        bool shadeSplit) {
+                        bool shadeSplit, uint32_t lightSplit) {
+    const bool lightSplit8 = lightSplit == 2;
     WaveKernels k;
     k.shadeBy[0] = k.shadeBy[1] = k.shadeBy[2] = nullptr;
+    k.lightsBy[0] = k.lightsBy[1] = nullptr;
     if (shadeSplit && !volumes) {
         // The GGX and Lambert kernels at 4 blocks a SM (128 registers) or, with shade_blocks 5, at 5 (96, more spilled).
         const bool five = shadeBlocks >= 5;
         k.shadeBy[0] = textures ? (five ? wfShadeQueue<0, true, 5> : wfShadeQueue<0, true, 4>) : (five ? wfShadeQueue<0, false, 5> : wfShadeQueue<0, false, 4>);
         k.shadeBy[1] = textures ? (five ? wfShadeQueue<1, true, 5> : wfShadeQueue<1, true, 4>) : (five ? wfShadeQueue<1, false, 5> : wfShadeQueue<1, false, 4>);
         k.shadeBy[2] = textures ? wfShadeQueue<2, true, 4> : wfShadeQueue<2, false, 4>;
+        if (lightSplit) {
+            k.shadeBy[0] = textures ? wfShadeDefer<0, true> : wfShadeDefer<0, false>;
+            k.shadeBy[1] = textures ? wfShadeDefer<1, true> : wfShadeDefer<1, false>;
+            // The light kernels at 6 blocks a SM (80 registers; 64 B of the GGX kernel's spilled) or, light_split 2, at 8
+            // (64 registers, more spilled).
+            k.lightsBy[0] = lightSplit8 ? wfLightsQueue<0, 8> : wfLightsQueue<0, 6>;
+            k.lightsBy[1] = lightSplit8 ? wfLightsQueue<1, 8> : wfLightsQueue<1, 6>;
+        }
     }
     k.logic = wfLogic;
     k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : shortStack ? wfExtend : wfExtendLocal;
@@ -788,6 +934,7 @@ WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes
 WaveKernels waveKernelsBatch(bool volumes, bool textures) {
     WaveKernels k;
     k.shadeBy[0] = k.shadeBy[1] = k.shadeBy[2] = nullptr;
+    k.lightsBy[0] = k.lightsBy[1] = nullptr;
     k.logic = wfLogicBatch;
     k.extend = wfExtendBatch;
     k.shadow = wfShadowBatch;

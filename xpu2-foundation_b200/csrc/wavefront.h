@@ -12,7 +12,7 @@ constexpr uint32_t kRecordSegments = 64;
 constexpr uint32_t kDefaultPaths = 1u << 22;
 constexpr uint32_t kDefaultRefill = 8, kDefaultBlocksPerSm = 16, kDefaultTraceBlocks = 0, kDefaultShadeBlocks = 4,
                    kDefaultTriLimit = 1, kDefaultShadowOrder = 0, kDefaultExtendBins = 1, kDefaultShortStack = 1,
-                   kDefaultShadeSplit = 1;
+                   kDefaultShadeSplit = 1, kDefaultLightSplit = 1;
 constexpr uint32_t kOctants = 8;
 
 // Path slots (structure of arrays, `paths` slots) and shadow-ray records (recordsPerPath a slot).
@@ -32,7 +32,12 @@ struct WaveState {
     float4* sray1;     // direction, far
     float4* scontrib;  // contribution when unoccluded
     uint8_t* svis;     // 1: nothing occludes [near, far]
+    // Light samples in a kernel of their own (wavefront shape light_split): each shaded vertex's LightJob (11 uint4),
+    // and a word a slot: bit 0 a job waits, bit 1 the BSDF sample's shadow record waits in the slot's last record.
+    uint4* lightJob;
+    uint32_t* lightFlags;
 };
+constexpr uint32_t kLightJobWords = 11;
 
 // The adjoint's wavefront form (x2_adjoint): per path slot the vertices it passed (material, the radiance before the
 // vertex acted, its credit scale), the sample's dL/dI share, and per shadow record its light and own factor; the
@@ -122,12 +127,15 @@ struct WaveKernels {
     void (*shade)(WaveArgs);
     void (*shadow)(WaveArgs);
     void (*shadeBy[3])(WaveArgs);  // shade split by lobe queue (GGX, Lambert, the rest), or null: shade in one kernel
+    void (*lightsBy[2])(WaveArgs);  // light samples of the GGX and Lambert queues in kernels of their own, or null
 };
 // counting: the traversal kernels that count node visits, triangle tests and lane use (the scene view's stats must
 // be set).
-// shadeSplit: shade as one kernel a per-lobe queue (surface scenes).
+// shadeSplit: shade as one kernel a per-lobe queue (surface scenes); lightSplit (with shadeSplit; 1 or 2, 0 off): the
+// GGX and Lambert queues' light samples in kernels of their own after shade, at 6 (1) or 8 (2) blocks a SM (the wave
+// state's lightJob must be allocated).
 WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack = kDefaultShortStack != 0,
-                        bool counting = false, bool shadeSplit = false);
+                        bool counting = false, bool shadeSplit = false, uint32_t lightSplit = 0);
 // The iteration's shade step: the per-lobe sort (when the queues are on) and the shade kernel or kernels.
 void launchShade(const WaveKernels& k, const WaveArgs& a, int grid, cudaStream_t st);
 WaveKernels waveKernelsBatch(bool volumes, bool textures);
