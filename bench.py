@@ -230,11 +230,12 @@ def traffic_from_profile():
 
 def kernels_per_iteration(spec):
     """Kernels a wavefront iteration launches: queue reset, logic, extend, the per-lobe sort (lobe_queues), shade (three
-    kernels with shade_split, else one), shadow and the drain check."""
+    kernels with shade_split, else one), the two light kernels (light_split), shadow and the drain check."""
     shape = dict(kv.split("=") for kv in spec.split(",")) if spec else {}
     lobe = int(shape.get("lobe_queues", 1))
     split = int(shape.get("shade_split", 1)) and lobe
-    return 5 + lobe + (3 if split else 1)
+    lights = 2 if split and int(shape.get("light_split", 1)) else 0
+    return 5 + lobe + (3 if split else 1) + lights
 
 
 def simt_summary(tc):

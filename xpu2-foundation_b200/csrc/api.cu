@@ -2568,7 +2568,7 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
         anyVolumes = anyVolumes || v.config.volume_count != 0;
         anyTextures = anyTextures || v.triUV != nullptr;
     }
-    const WaveKernels wk = waveKernelsBatch(anyVolumes, anyTextures);
+    const WaveKernels wk = waveKernelsBatch(anyVolumes, anyTextures, s0->shadeSplit != 0);
     std::vector<unsigned long long> items;
     uint32_t iterations = 0;
     if (cudaMalloc(&dViews, sizeof(SceneView) * n) != cudaSuccess || cudaMalloc(&dFilms, sizeof(BatchFilm) * n) != cudaSuccess ||
@@ -2644,8 +2644,7 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
             wfResetQueues<<<1, 32, 0, st>>>(a);
             wk.logic<<<gridLogic, kWaveBlock, 0, st>>>(a);
             wk.extend<<<gridWork, kWaveBlock, 0, st>>>(a);
-            if (a.shadeQ) wfSortShadeBatch<<<gridWork, kWaveBlock, 0, st>>>(a);
-            wk.shade<<<gridWork, kWaveBlock, 0, st>>>(a);
+            launchShade(wk, a, gridWork, st, true);
             wk.shadow<<<gridWork, kWaveBlock, 0, st>>>(a);
         }
         wfResetQueues<<<1, 32, 0, st>>>(a);

@@ -875,6 +875,11 @@ template <int kQueue, bool kTextures, int kMinBlocks>
 __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfShadeQueue(WaveArgs a) {
     shadeBody<false, false, false, kTextures, kQueue>(a);
 }
+// The batch form's shade split by lobe (each path's scene from the request table).
+template <int kQueue, bool kTextures>
+__global__ void __launch_bounds__(kWaveBlock, 4) wfShadeQueueBatch(WaveArgs a) {
+    shadeBody<true, false, false, kTextures, kQueue>(a);
+}
 // With the light samples split off (light_split): the GGX and Lambert queues' shade without them, and their light
 // kernels.
 template <int kQueue, bool kTextures>
@@ -886,8 +891,8 @@ __global__ void __launch_bounds__(kWaveBlock, kMinBlocks) wfLightsQueue(WaveArgs
     lightsBody<kQueue>(a);
 }
 
-void launchShade(const WaveKernels& k, const WaveArgs& a, int grid, cudaStream_t st) {
-    if (a.shadeQ) wfSortShade<<<grid, kWaveBlock, 0, st>>>(a);
+void launchShade(const WaveKernels& k, const WaveArgs& a, int grid, cudaStream_t st, bool batch) {
+    if (a.shadeQ) (batch ? wfSortShadeBatch : wfSortShade)<<<grid, kWaveBlock, 0, st>>>(a);
     if (a.shadeQ && k.shadeBy[0]) {
         for (int q = 0; q < 3; ++q) k.shadeBy[q]<<<grid, kWaveBlock, 0, st>>>(a);
         if (k.lightsBy[0])
@@ -931,10 +936,15 @@ WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes
     return k;
 }
 
-WaveKernels waveKernelsBatch(bool volumes, bool textures) {
+WaveKernels waveKernelsBatch(bool volumes, bool textures, bool shadeSplit) {
     WaveKernels k;
     k.shadeBy[0] = k.shadeBy[1] = k.shadeBy[2] = nullptr;
     k.lightsBy[0] = k.lightsBy[1] = nullptr;
+    if (shadeSplit && !volumes) {
+        k.shadeBy[0] = textures ? wfShadeQueueBatch<0, true> : wfShadeQueueBatch<0, false>;
+        k.shadeBy[1] = textures ? wfShadeQueueBatch<1, true> : wfShadeQueueBatch<1, false>;
+        k.shadeBy[2] = textures ? wfShadeQueueBatch<2, true> : wfShadeQueueBatch<2, false>;
+    }
     k.logic = wfLogicBatch;
     k.extend = wfExtendBatch;
     k.shadow = wfShadowBatch;

@@ -136,9 +136,10 @@ struct WaveKernels {
 // state's lightJob must be allocated).
 WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack = kDefaultShortStack != 0,
                         bool counting = false, bool shadeSplit = false, uint32_t lightSplit = 0);
-// The iteration's shade step: the per-lobe sort (when the queues are on) and the shade kernel or kernels.
-void launchShade(const WaveKernels& k, const WaveArgs& a, int grid, cudaStream_t st);
-WaveKernels waveKernelsBatch(bool volumes, bool textures);
+// The iteration's shade step: the per-lobe sort (when the queues are on) and the shade kernel or kernels (batch: the
+// batch form's sort).
+void launchShade(const WaveKernels& k, const WaveArgs& a, int grid, cudaStream_t st, bool batch = false);
+WaveKernels waveKernelsBatch(bool volumes, bool textures, bool shadeSplit = kDefaultShadeSplit != 0);
 __global__ void wfSortShade(WaveArgs a);
 __global__ void wfSortShadeBatch(WaveArgs a);
 // The adjoint's logic and shade kernels (dynamic shared memory: the gradient count in floats) and the final sum of the
