@@ -348,11 +348,12 @@ def run(args):
     # built; the parity build above is -fmad=false): one frame each, in a process of its own, at N=1 only.
     fmad = forms_with("libx2fmad.so") if world == 1 and not args.skip_plain else None
 
-    # Multi-GPU: the lanes' films summed over NCCL at frame end, then the audit of the merged counts.
+    # Multi-GPU: the lanes' films summed in place on the devices over NCCL at frame end, then the merged counts'
+    # audit on the device.
     if dist is not None:
         from x2 import lanes
 
-        lanes.merge_and_audit(sums, counts, world * cfg.spp, device="cuda:%d" % local)
+        lanes.merge_and_audit_device(scene, world * cfg.spp)
 
     # Roofline of the dominant wavefront kernel. Its algorithmic bytes (BVH nodes and triangles its rays visit, and
     # its ray records, counted in the counting frame) over its time in the per-kernel timed frame, against the cache

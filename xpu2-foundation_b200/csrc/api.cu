@@ -1166,9 +1166,17 @@ int x2_launch(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     a.odd = s->adaptive ? s->odd : nullptr;
     a.counts = s->counts;
     a.counters = sl->counters;
-    const int blocks = s->ctx->smCount * s->ctx->renderBlocksPerSm;
+    // The bounce-at-a-time form for surface scenes (renderSteps); renderChunks for volumes, counting launches and
+    // vertices with more shadow rays than its list holds.
+    void (*kernel)(RenderArgs) = s->volumeCount ? renderChunksVolumes : s->triUV ? renderChunksTextured : renderChunks;
+    if (!s->volumeCount && !a.scene.stats &&
+        uint64_t(s->config.light_count) * s->config.light_samples + s->config.bsdf_samples <= kStepRecords)
+        kernel = s->triUV ? renderStepsTextured<4> : renderSteps<4>;
+    int perSm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, kernel, kRenderBlock, 0);
+    const int blocks = s->ctx->smCount * std::max(perSm, 1);
     cudaEventRecord(sl->begin, st);
-    (s->volumeCount ? renderChunksVolumes : s->triUV ? renderChunksTextured : renderChunks)<<<blocks, kRenderBlock, 0, st>>>(a);
+    kernel<<<blocks, kRenderBlock, 0, st>>>(a);
     CUDA_OR(cudaGetLastError(), X2_ECUDA);
     cudaEventRecord(sl->end, st);
     cudaMemcpyAsync(sl->hostCounters, sl->counters, sizeof(Counters), cudaMemcpyDeviceToHost, st);

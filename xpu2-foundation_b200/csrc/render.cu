@@ -1,10 +1,13 @@
 // The plain megakernel and the small kernels around it.
 //
-// renderChunks: persistent warps claim 32 work items at a time (one atomic a warp); an item is a (chunk, tile
-// position, sample) triple laid out sample-minor, so a warp renders consecutive samples of one or two pixels:
-// its camera rays are coherent and its film update is one segmented warp reduction and one set of FP64 atomics
-// a pixel (warp-aggregated atomics) instead of one a sample. The film is the reference's: FP64 sums (rgb + alpha),
-// FP64 odd-index sums (adaptive frames), U32 counts (async_gpu.cu:320-364).
+// An item of a launch is a (chunk, tile position, sample) triple laid out sample-minor, so consecutive items are
+// consecutive samples of one pixel: a warp's camera rays are coherent and its film update is one set of FP64 atomics a
+// pixel (warp-aggregated atomics) instead of one a sample. The film is the reference's: FP64 sums (rgb + alpha), FP64
+// odd-index sums (adaptive frames), U32 counts (async_gpu.cu:320-364).
+//
+// renderSteps (surface scenes): a bounce at a time, a lane taking the next item as soon as its sample is done, rays
+// walked a node a step across the warp (below). renderChunks (volumes, counting launches): persistent warps claim 32
+// items at a time (one atomic a warp) and each lane runs its sample's whole path (integrate).
 #include "integrator.cuh"
 #include "render.h"
 
@@ -45,14 +48,86 @@ __device__ __forceinline__ void addCounters(Counters* dst, unsigned long long tr
     }
 }
 
+// Work item `item` of a launch (item < itemCount): its pixel and sample index, or pixel ~0u when it is no sample (past
+// its chunk's count, or outside the frame).
+__device__ __forceinline__ void itemSample(const RenderArgs& a, unsigned long long item, uint32_t& pixel, uint32_t& index) {
+    const unsigned long long perChunk = 64ull * a.samplesPerChunk;
+    const unsigned long long chunkIndex = item / perChunk;
+    const uint32_t offset = uint32_t(item - chunkIndex * perChunk);
+    const uint32_t position = offset / a.samplesPerChunk, s = offset % a.samplesPerChunk;
+    const x2_chunk chunk = a.chunks[chunkIndex];
+    pixel = ~0u;
+    index = 0;
+    if (s < chunk.count) {
+        pixel = tilePixel(chunk.tile, position, a.scene.config.width, a.scene.config.height);
+        index = chunk.first + s;
+    }
+}
+
+// The film update of a warp step: the lanes that finished a sample of the same pixel are summed by the lowest of them
+// (its peers' values added in lane order, whichever lanes they are), which then makes one set of FP64 atomics for the
+// pixel. Every lane of the warp calls it; done: the lane finished a sample this step.
+__device__ __forceinline__ void warpFilm(const RenderArgs& a, bool done, uint32_t pixel, uint32_t index, float r, float g, float b,
+                                         float al) {
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t key = done ? pixel : ~0u;
+    const uint32_t peers = __match_any_sync(full, key);
+    const bool leader = done && lane == uint32_t(__ffs(peers) - 1);
+    const bool isOdd = done && (index & 1u) && a.odd;
+    const double v0 = done ? double(r) : 0.0, v1 = done ? double(g) : 0.0, v2 = done ? double(b) : 0.0, v3 = done ? double(al) : 0.0;
+    double s0 = v0, s1 = v1, s2 = v2, s3 = v3;
+    double w0 = isOdd ? v0 : 0.0, w1 = isOdd ? v1 : 0.0, w2 = isOdd ? v2 : 0.0, w3 = isOdd ? v3 : 0.0;
+    const double o0 = w0, o1 = w1, o2 = w2, o3 = w3;
+    const bool anyOdd = __any_sync(full, isOdd);
+    uint32_t rest = leader ? peers & ~(1u << lane) : 0u;
+    const uint32_t cnt = leader ? uint32_t(__popc(peers)) : 0u;
+    while (__any_sync(full, rest != 0)) {
+        const int src = rest ? __ffs(rest) - 1 : int(lane);
+        const double t0 = __shfl_sync(full, v0, src), t1 = __shfl_sync(full, v1, src);
+        const double t2 = __shfl_sync(full, v2, src), t3 = __shfl_sync(full, v3, src);
+        double u0 = 0.0, u1 = 0.0, u2 = 0.0, u3 = 0.0;
+        if (anyOdd) {
+            u0 = __shfl_sync(full, o0, src);
+            u1 = __shfl_sync(full, o1, src);
+            u2 = __shfl_sync(full, o2, src);
+            u3 = __shfl_sync(full, o3, src);
+        }
+        if (rest) {
+            s0 += t0;
+            s1 += t1;
+            s2 += t2;
+            s3 += t3;
+            w0 += u0;
+            w1 += u1;
+            w2 += u2;
+            w3 += u3;
+            rest &= rest - 1;
+        }
+    }
+    if (leader) {
+        double* s = a.sums + 4ull * key;
+        atomicAdd(s, s0);
+        atomicAdd(s + 1, s1);
+        atomicAdd(s + 2, s2);
+        atomicAdd(s + 3, s3);
+        atomicAdd(a.counts + key, cnt);
+        if (a.odd && (w0 != 0.0 || w1 != 0.0 || w2 != 0.0 || w3 != 0.0)) {
+            double* d = a.odd + 4ull * key;
+            atomicAdd(d, w0);
+            atomicAdd(d + 1, w1);
+            atomicAdd(d + 2, w2);
+            atomicAdd(d + 3, w3);
+        }
+    }
+}
+
 }  // namespace
 
 template <bool kVolumes, bool kTextures>
 __device__ __forceinline__ void renderChunksBody(const RenderArgs& a) {
     const unsigned full = 0xffffffffu;
     const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t width = a.scene.config.width, height = a.scene.config.height;
-    const unsigned long long perChunk = 64ull * a.samplesPerChunk;
     unsigned long long trace = 0, nee = 0, bsdf = 0, held = 0, samples = 0, errors = 0;
     for (;;) {
         unsigned long long base = 0;
@@ -61,16 +136,7 @@ __device__ __forceinline__ void renderChunksBody(const RenderArgs& a) {
         if (base >= a.itemCount) break;
         const unsigned long long item = base + lane;
         uint32_t pixel = ~0u, index = 0;
-        if (item < a.itemCount) {
-            const unsigned long long chunkIndex = item / perChunk;
-            const uint32_t offset = uint32_t(item - chunkIndex * perChunk);
-            const uint32_t position = offset / a.samplesPerChunk, s = offset % a.samplesPerChunk;
-            const x2_chunk chunk = a.chunks[chunkIndex];
-            if (s < chunk.count) {
-                pixel = tilePixel(chunk.tile, position, width, height);
-                index = chunk.first + s;
-            }
-        }
+        if (item < a.itemCount) itemSample(a, item, pixel, index);
         SampleOut o;
         o.status = X2_SKIP;
         o.rgb[0] = o.rgb[1] = o.rgb[2] = o.alpha = 0.0f;
@@ -83,61 +149,179 @@ __device__ __forceinline__ void renderChunksBody(const RenderArgs& a) {
             if (o.status == X2_DONE) ++samples;
             else if (o.status != X2_SKIP) ++errors;
         }
-        // Film: one segmented reduction over the warp's lanes that finished a sample of the same pixel.
-        const bool done = pixel != ~0u && o.status == X2_DONE;
-        const uint32_t key = done ? pixel : ~0u;
-        const uint32_t peers = __match_any_sync(full, key);
-        double v0 = done ? double(o.rgb[0]) : 0.0, v1 = done ? double(o.rgb[1]) : 0.0, v2 = done ? double(o.rgb[2]) : 0.0,
-               v3 = done ? double(o.alpha) : 0.0;
-        uint32_t cnt = done ? 1u : 0u;
-        const bool isOdd = done && (index & 1u) && a.odd;
-        double w0 = isOdd ? v0 : 0.0, w1 = isOdd ? v1 : 0.0, w2 = isOdd ? v2 : 0.0, w3 = isOdd ? v3 : 0.0;
-        const bool anyOdd = __any_sync(full, isOdd);
-#pragma unroll
-        for (int off = 1; off < 32; off <<= 1) {
-            const double t0 = __shfl_down_sync(full, v0, off), t1 = __shfl_down_sync(full, v1, off);
-            const double t2 = __shfl_down_sync(full, v2, off), t3 = __shfl_down_sync(full, v3, off);
-            const uint32_t tc = __shfl_down_sync(full, cnt, off);
-            const bool same = lane + off < 32 && ((peers >> (lane + off)) & 1u);
-            if (same) {
-                v0 += t0;
-                v1 += t1;
-                v2 += t2;
-                v3 += t3;
-                cnt += tc;
-            }
-            if (anyOdd) {
-                const double u0 = __shfl_down_sync(full, w0, off), u1 = __shfl_down_sync(full, w1, off);
-                const double u2 = __shfl_down_sync(full, w2, off), u3 = __shfl_down_sync(full, w3, off);
-                if (same) {
-                    w0 += u0;
-                    w1 += u1;
-                    w2 += u2;
-                    w3 += u3;
-                }
-            }
-        }
-        if (done && lane == uint32_t(__ffs(peers) - 1)) {
-            double* s = a.sums + 4ull * key;
-            atomicAdd(s, v0);
-            atomicAdd(s + 1, v1);
-            atomicAdd(s + 2, v2);
-            atomicAdd(s + 3, v3);
-            atomicAdd(a.counts + key, cnt);
-            if (a.odd && (w0 != 0.0 || w1 != 0.0 || w2 != 0.0 || w3 != 0.0)) {
-                double* d = a.odd + 4ull * key;
-                atomicAdd(d, w0);
-                atomicAdd(d + 1, w1);
-                atomicAdd(d + 2, w2);
-                atomicAdd(d + 3, w3);
-            }
-        }
+        warpFilm(a, pixel != ~0u && o.status == X2_DONE, pixel, index, o.rgb[0], o.rgb[1], o.rgb[2], o.alpha);
     }
     addCounters(a.counters, trace, nee, bsdf, held, samples, errors);
 }
 __global__ void __launch_bounds__(kRenderBlock) renderChunks(RenderArgs a) { renderChunksBody<false, false>(a); }
 __global__ void __launch_bounds__(kRenderBlock) renderChunksTextured(RenderArgs a) { renderChunksBody<false, true>(a); }
 __global__ void __launch_bounds__(kRenderBlock) renderChunksVolumes(RenderArgs a) { renderChunksBody<true, true>(a); }
+
+// renderSteps: the plain megakernel for surface scenes, a bounce at a time. A lane holds one sample's path (its pending
+// rays on a local stack, its radiance) and takes the launch's next item as soon as the sample is done, so a warp never
+// waits for its longest path (path regeneration). A warp step is one vertex of every live lane's path: the closest hit
+// of its next pending ray, walked a node a step together with the warp's other rays (walkStep); the vertex shaded
+// (afterTrace, shadeVertex) with its shadow rays written to a list of the lane's own; then the lists walked together,
+// a lane whose ray is done starting its next one at once; then the unoccluded rays' contributions added in the list's
+// order. That is the order in which integrate (one thread a sample, shadow rays traced as they come) adds them, and
+// the steps visit the nodes and test the triangles traceClosest / traceAny do, so a sample's radiance is the same bit
+// for bit. Scenes with volumes, vertices with more than kStepRecords shadow rays and counting launches use renderChunks.
+struct StepSink {
+    ShadowReq* reqs;
+    uint32_t& n;
+    Pending* stack;
+    uint32_t& size;
+    unsigned long long &nee, &bsdf, &heldRays;
+    bool full;  // a shadow ray beyond kStepRecords (the launch checks the scene's bound, so never set)
+    __device__ void shadow(const ShadowReq& q, bool fromBsdf) {
+        if (fromBsdf) ++bsdf;
+        else ++nee;
+        if (n < kStepRecords) reqs[n++] = q;
+        else full = true;
+    }
+    __device__ void held() { ++heldRays; }
+    __device__ void vertex(uint32_t, const Bsdf&, V3, const TexHit*) {}
+    __device__ uint32_t top(uint32_t) const { return size; }
+    __device__ void push(const Pending& p) { stack[size++] = p; }
+};
+
+template <bool kTextures>
+__device__ __forceinline__ void renderStepsBody(const RenderArgs& a) {
+    __shared__ uint2 shortStacks[kShortStack * kRenderBlock];
+    const unsigned full = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const SceneView& s = a.scene;
+    const Bvh8 bvh = s.bvh;
+    uint32_t* overflow = s.overflow;
+    Walk<kShortStack> walk;
+    uint2 deep[kStack - kShortStack];
+    walk.shortStack = shortStacks + threadIdx.x;
+    walk.nodes = walk.tris = 0;
+    Pending stack[kMaxPending];
+    ShadowReq reqs[kStepRecords];
+    uint32_t size = 0, pixel = 0, index = 0;
+    V3 cameraPosition{0, 0, 0}, radiance{0, 0, 0};
+    float alpha = 0.0f;
+    RayQ r;
+    unsigned long long trace = 0, nee = 0, bsdf = 0, held = 0, samples = 0, errors = 0;
+    bool live = false, drained = false;
+    for (;;) {
+        // Idle lanes take the next items (one atomic a warp); an item that is no sample leaves its lane idle.
+        const uint32_t idle = __ballot_sync(full, !live);
+        if (idle && !drained) {
+            const uint32_t leader = __ffs(idle) - 1, want = __popc(idle);
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(a.claimed, (unsigned long long)want);
+            base = __shfl_sync(full, base, leader);
+            drained = base + want >= a.itemCount;
+            if (!live) {
+                const unsigned long long item = base + __popc(idle & ((1u << lane) - 1u));
+                if (item < a.itemCount) {
+                    itemSample(a, item, pixel, index);
+                    if (pixel != ~0u) {
+                        CameraRay camera;
+                        if (cameraRay(s, pixel, index, camera)) {
+                            cameraPending(camera, stack[0]);
+                            size = 1;
+                            cameraPosition = camera.origin;
+                            radiance = V3{0, 0, 0};
+                            alpha = 0.0f;
+                            live = true;
+                        } else {
+                            ++errors;
+                        }
+                    }
+                }
+            }
+        }
+        if (!__any_sync(full, live)) {
+            if (drained) break;
+            continue;
+        }
+        // The closest hit of each live lane's next pending ray, walked a step at a time.
+        bool tracing = live;
+        if (live) {
+            const Pending& next = stack[size - 1];
+            r = makeRay(bvh, next.origin.x, next.origin.y, next.origin.z, next.dir.x, next.dir.y, next.dir.z);
+            walkStart<false, kShortStack>(walk, r, next.nearT, next.farT);
+        }
+        for (;;) {
+            const uint32_t lanes = __ballot_sync(full, tracing);
+            if (!lanes) break;
+            if (tracing && walkStep<false, kShortStack>(bvh, r, walk, deep, overflow, 1u, lanes)) tracing = false;
+        }
+        // The vertex: the hit rebuilt as trace() does, then afterTrace and shadeVertex, the shadow rays to the list.
+        uint32_t n = 0;
+        if (live) {
+            Pending pv = stack[--size];
+            const uint32_t top = size;
+            ++trace;
+            Hit hit;
+            hit.geom = ~0u;
+            hit.prim = 0;
+            hit.t = hit.u = hit.v = 0;
+            hit.normal = hit.origin = hit.below = hit.point = V3{0, 0, 0};
+            V3 va{0, 0, 0}, vb{0, 0, 0}, vc{0, 0, 0};
+            if (walk.best != ~0u) {
+                const float4* tp = reinterpret_cast<const float4*>(bvh.tris + walk.bestLeaf);
+                const float4 A = __ldg(tp), B = __ldg(tp + 1), Cc = __ldg(tp + 2);
+                va = V3{A.x, A.y, A.z};
+                vb = V3{B.x, B.y, B.z};
+                vc = V3{Cc.x, Cc.y, Cc.z};
+                hit.geom = __ldg(s.triMesh + walk.best);
+                hit.prim = walk.best - __ldg(s.meshFirst + hit.geom);
+                hit.t = walk.tmax;
+                if (!geometryHit(hit, pv.origin, pv.dir, va, vb, vc)) hit.normal = V3{0, 0, 0};
+            }
+            const Identity root{pixel, U64(index), U64(s.config.seed), 0};
+            afterTrace<false>(s, root, pv, hit, cameraPosition, radiance, alpha);
+            if (hit.geom != ~0u) {
+                StepSink sink{reqs, n, stack, size, nee, bsdf, held, false};
+                if (!shadeVertex<false, kTextures>(s, root, pixel, index, pv, hit, va, vb, vc, top, radiance, alpha, sink) || sink.full) {
+                    ++errors;
+                    live = false;
+                    n = 0;
+                }
+            }
+        }
+        // The shadow rays: each lane walks its list, starting its next ray as soon as one is done.
+        uint32_t j = 0, vis = 0;
+        tracing = n > 0;
+        if (tracing) {
+            r = makeRay(bvh, reqs[0].origin.x, reqs[0].origin.y, reqs[0].origin.z, reqs[0].dir.x, reqs[0].dir.y, reqs[0].dir.z);
+            walkStart<true, kShortStack>(walk, r, reqs[0].near, reqs[0].far);
+        }
+        for (;;) {
+            const uint32_t lanes = __ballot_sync(full, tracing);
+            if (!lanes) break;
+            if (tracing && walkStep<true, kShortStack>(bvh, r, walk, deep, overflow, 1u, lanes)) {
+                if (!walk.best) vis |= 1u << j;
+                if (++j < n) {
+                    const ShadowReq& q = reqs[j];
+                    r = makeRay(bvh, q.origin.x, q.origin.y, q.origin.z, q.dir.x, q.dir.y, q.dir.z);
+                    walkStart<true, kShortStack>(walk, r, q.near, q.far);
+                } else {
+                    tracing = false;
+                }
+            }
+        }
+        for (uint32_t k = 0; k < n; ++k)
+            if ((vis >> k) & 1u) radiance = add(radiance, reqs[k].contribution);
+        const bool done = live && size == 0;
+        if (__any_sync(full, done)) warpFilm(a, done, pixel, index, radiance.x, radiance.y, radiance.z, alpha);
+        if (done) {
+            ++samples;
+            live = false;
+        }
+    }
+    addCounters(a.counters, trace, nee, bsdf, held, samples, errors);
+}
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kRenderBlock, kMinBlocks) renderSteps(RenderArgs a) { renderStepsBody<false>(a); }
+template <int kMinBlocks>
+__global__ void __launch_bounds__(kRenderBlock, kMinBlocks) renderStepsTextured(RenderArgs a) { renderStepsBody<true>(a); }
+template __global__ void renderSteps<4>(RenderArgs);
+template __global__ void renderStepsTextured<4>(RenderArgs);
 
 // The per-sample API: integrate() for n (pixel, index) pairs.
 template <bool kVolumes, bool kTextures>

@@ -5,6 +5,8 @@
 namespace x2 {
 
 constexpr int kRenderBlock = 128;
+// Shadow rays a vertex may make in the bounce-at-a-time megakernel (light_count x light_samples + bsdf_samples).
+constexpr uint32_t kStepRecords = 24;
 
 struct RenderArgs {
     SceneView scene;
@@ -26,6 +28,12 @@ cudaError_t uploadSobol(const uint32_t directions[17][32]);
 __global__ void renderChunks(RenderArgs a);
 __global__ void renderChunksTextured(RenderArgs a);
 __global__ void renderChunksVolumes(RenderArgs a);
+// The plain megakernel a bounce at a time (surface scenes whose vertices make at most kStepRecords shadow rays), in
+// occupancy variants: kMinBlocks blocks a SM that the register allocation must allow.
+template <int kMinBlocks>
+__global__ void renderSteps(RenderArgs a);
+template <int kMinBlocks>
+__global__ void renderStepsTextured(RenderArgs a);
 __global__ void integratePairs(SceneView s, const uint32_t* pairs, unsigned long long n, double* rgba, uint32_t* status, Counters* counters);
 __global__ void integratePairsTextured(SceneView s, const uint32_t* pairs, unsigned long long n, double* rgba, uint32_t* status,
                                        Counters* counters);

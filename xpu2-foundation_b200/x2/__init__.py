@@ -555,6 +555,26 @@ class Scene:
         _check(library().x2_wait(self._h, timeout_ms, C.byref(c)))
         return c
 
+    def film_tensors(self, odd=False):
+        """The film in place on the device as torch tensors (no copy; x2_film_device): FP64 sums (pixels x 4), the odd
+        sums (or None) and the counts as int32 (the library's uint32 counts, equal while below 2^31). The library writes
+        them on its own stream: call wait() before reading them and synchronise torch's work before the next launch."""
+        import torch
+
+        sums, odd_p, counts = C.c_void_p(), C.c_void_p(), C.c_void_p()
+        _check(library().x2_film_device(self._h, C.byref(sums), C.byref(odd_p), C.byref(counts)))
+        p = self.config.width * self.config.height
+        dev = "cuda:%d" % self.ctx.device
+
+        def view(ptr, shape, typestr):
+            arr = type("DeviceArray", (), {})()
+            arr.__cuda_array_interface__ = {"shape": shape, "typestr": typestr, "data": (ptr.value, False), "version": 3,
+                                            "strides": None}
+            return torch.as_tensor(arr, device=dev)
+
+        out_odd = view(odd_p, (p, 4), "<f8") if odd and odd_p.value else None
+        return view(sums, (p, 4), "<f8"), out_odd, view(counts, (p,), "<i4")
+
     def film(self, odd=False):
         p = self.config.width * self.config.height
         sums = np.empty((p, 4), np.float64)

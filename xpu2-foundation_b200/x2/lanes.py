@@ -72,6 +72,28 @@ def merge_and_audit(sums, counts, spp, odd=None, dst=0, group=None, device=None)
     return merged
 
 
+def merge_device(scene, odd=False, group=None):
+    """Sum the ranks' films in place on their devices: every rank's scene film (sums, counts and, with `odd`, the odd
+    sums) becomes the sum over the group, with no copy through the host. An all-reduce a buffer, NCCL between GPUs (gloo
+    stages through the host in the single-GPU tests). Waits for the scene's launches first and for the reduces after."""
+    import torch
+    import torch.distributed as dist
+
+    scene.wait()
+    sums, odd_t, counts = scene.film_tensors(odd)
+    for b in (sums, counts) + ((odd_t,) if odd_t is not None else ()):
+        dist.all_reduce(b, op=dist.ReduceOp.SUM, group=group)
+    torch.cuda.synchronize(sums.device)
+
+
+def merge_and_audit_device(scene, spp, odd=False, group=None):
+    """`merge_device`, then the merged film's audit on the device (x2_audit): every pixel holds exactly `spp` samples.
+    Raises X2Error(EAUDIT) on the first pixel that does not, on every rank (each holds the merged film)."""
+    merge_device(scene, odd, group)
+    pixels = scene.config.width * scene.config.height
+    scene.audit(np.full(pixels, spp, np.uint32))
+
+
 def resolve(sums, counts):
     """Pixel values: sum / count per channel as float32, black where a pixel holds no samples."""
     c = np.asarray(counts, np.float64)[:, None]
