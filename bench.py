@@ -483,12 +483,13 @@ def probe_volume(args):
     s = x2.SyntheticScene(3)
     cfg = s.config
     scene = x2.Scene(ctx, s.desc, cfg)
+    apply_shape(scene, args.shape)
     tiles = ((cfg.width + 7) // 8) * ((cfg.height + 7) // 8)
     sel = np.linspace(0, tiles - 1, min(tiles, args.probe_tiles)).astype(np.uint32)
     chunks = np.zeros(len(sel), x2.CHUNK_DTYPE)
     chunks["tile"], chunks["first"], chunks["count"] = sel, 0, cfg.spp
     n = len(sel) * 64 * cfg.spp
-    out = {"probe": "volume", "tiles": len(sel), "samples": n, "grid": "256^3", "spp": cfg.spp}
+    out = {"probe": "volume", "tiles": len(sel), "samples": n, "grid": "256^3", "spp": cfg.spp, "shape": args.shape}
     films = {}
     for form in ("wavefront", "plain"):
         scene.frame_begin(cfg.spp)

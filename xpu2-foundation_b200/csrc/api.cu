@@ -1317,7 +1317,9 @@ WaveArgs launchArgs(x2_scene* s, Slot& sl, uint32_t paths, uint32_t records, uns
     a.extendSlots = s->extendBins ? s->waveCounters + 8 + x2::kRecordSegments : nullptr;
     a.extendNext = s->waveCounters + 3;
     a.shadowNext = s->waveCounters + 4;
-    a.shadeQ = s->lobeQueues ? s->shadeQ : nullptr;
+    // Volume scenes are shaded in the extend queue's order: its neighbouring slots hold samples of one pixel, whose
+    // marches are alike; a per-lobe sort (or one by march length) scatters them and the march's lanes diverge more.
+    a.shadeQ = s->lobeQueues && !s->volumeCount ? s->shadeQ : nullptr;
     a.shadeCount = s->waveCounters + 5;
     a.adj = AdjointWave{};
     a.chunkMask = s->launchMask;
