@@ -71,7 +71,11 @@ def measure(ctx, path):
     out["forms_equal"] = bool(np.array_equal(images["wavefront"], images["plain"]))
     d = np.abs(images["wavefront"] - f["cpu"])[live]
     out["max_abs_diff_vs_cpu"] = float(d.max())
-    out["frac_within_1e-4_vs_cpu"] = float(np.mean(d <= 1e-4 * np.abs(f["cpu"][live]) + 1e-6))
+    inside = d <= 1e-4 * np.abs(f["cpu"][live]) + 1e-6
+    out["frac_within_1e-4_vs_cpu"] = float(np.mean(inside))
+    # The pixels (frame indices) with a channel outside 1e-4 of the reference's render of the same samples.
+    frame_pixels = tile_pixels(tiles, s.config.width, s.config.height)[live]
+    out["pixels_outside_1e-4"] = [int(v) for v in frame_pixels[~inside.all(axis=1)]]
     # The converged image's own error (its samples' variance over 16,384): the floor under every RMSE stated here.
     out["ref_mean"] = float(ref[live].mean())
     scene.free()

@@ -135,11 +135,18 @@ def test_radiance_golden(cid, box, field, textured):
     assert ok.all(), f"{len(bad)} of {len(ok)} samples outside {RTOL}: first {bad[:8]}: {rgba[bad[:3]]} vs {g['rgba'][bad[:3]]}"
 
 
+# The samples of the live test outside the per-sample bar, by configuration: config 108's two are each a one-ulp
+# difference of CUDA's sincosf against the host libm's sincos on a sampled angle, amplified continuously with no
+# discrete decision flipped (tests/test_gpu_parity_cause.py: they vanish with the functions rounded from double, and
+# the reference replayed with the device's function values gives the device's radiance bit for bit).
+EXPECTED_OUTSIDE = {0: set(), 108: {(22444, 55), (26184, 27)}, 44: set()}
+
+
 @needs_reference
 @pytest.mark.parametrize("cid", [0, 108, 44])
 def test_radiance_live_reference(cid, box, field, textured):
-    """Many more samples against the live reference build: the fraction within tolerance is reported and must be
-    at least 99.99%; every status and every alpha must agree."""
+    """Many more samples against the live reference build: every sample within tolerance except the listed, explained
+    ones (EXPECTED_OUTSIDE); every status and every alpha must agree."""
     s, scene = _scene(cid, box, field, textured)
     px, idx = oracle_lib.sample_pairs(s.config, 60000, 1000 + cid)
     rgba, status = scene.integrate(px, idx)
@@ -150,9 +157,8 @@ def test_radiance_live_reference(cid, box, field, textured):
     ok = within(rgba, rrgba).all(axis=1)
     rel = (np.abs(rgba - rrgba) / np.maximum(np.abs(rrgba), 1e-6)).max(axis=1)
     print(f"config {cid}: {ok.mean() * 100:.4f}% of {len(ok)} samples within {RTOL}; outside: {np.sort(rel[~ok])[::-1][:8]}")
-    # Config 44's near-mirror GGX spheres (a of 0.003) turn a last-ulp difference of a sampled direction (CUDA's
-    # sincosf against the host's) into a larger difference of the lobe's value than the others' scenes do.
-    assert ok.mean() >= (0.9995 if cid == 44 else 0.9999)
+    outside = {(int(p), int(i)) for p, i in zip(px[~ok], idx[~ok])}
+    assert outside == EXPECTED_OUTSIDE[cid], f"samples outside {RTOL}: {sorted(outside)}"
 
 
 # ---- film and audit ----

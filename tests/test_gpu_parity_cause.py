@@ -152,3 +152,38 @@ def test_contracted_build_within_tolerance(ctx, cid, tmp_path):
           f"{bool(np.array_equal(d['status'], wstatus))}")
     assert (d["status"] == wstatus).mean() >= 0.999
     assert ok.mean() >= 0.99
+
+
+def test_volume_fixture_outlier_pixels(ctx, tmp_path):
+    """Config 3's RMSE fixture (the 256^3 medium, 384 pixels x 256 samples): the pixels whose mean is outside 1e-4 of
+    the reference's render of the same samples; each one's samples against the reference sample by sample; and those
+    outside, with the transcendental functions rounded from double, back within 1e-4."""
+    import rmse_lib
+
+    f = np.load(os.path.join(HERE, "golden", "rmse_c3.npz"))
+    s = x2.SyntheticScene(3)
+    cfg = s.config
+    scene = x2.Scene(ctx, s.desc, cfg)
+    spp = int(f["spp"])
+    live = f["live"]
+    px = rmse_lib.tile_pixels(f["tiles"], cfg.width, cfg.height)[live]
+    cpu = f["cpu"][live]
+    pixels = np.repeat(px, spp).astype(np.uint32)
+    indices = np.tile(np.arange(spp), len(px)).astype(np.uint32)
+    rgba, status = scene.integrate(pixels, indices)
+    assert (status == x2.DONE).all()
+    img = rgba[:, :3].reshape(len(px), spp, 3).sum(axis=1) / spp
+    bad = np.flatnonzero(~within(img, cpu).all(axis=1))
+    ref = oracle_lib.Reference(s)
+    rows = []
+    for b in bad:
+        sel = slice(b * spp, (b + 1) * spp)
+        want, wstatus = ref.integrate(pixels[sel], indices[sel])
+        assert np.array_equal(wstatus, status[sel])
+        out = np.flatnonzero(~within(rgba[sel], want).all(axis=1))
+        d = diag(3, pixels[sel][out], indices[sel][out], 1, tmp_path)
+        fixed = within(d["rgba"], want[out]).all(axis=1)
+        rows.append(f"  pixel {px[b]}: {len(out)} of {spp} samples outside 1e-4 (indices {indices[sel][out].tolist()}), "
+                    f"{int(fixed.sum())} of them within with the functions rounded from double")
+        assert fixed.all(), rows[-1]
+    print(f"config 3 fixture: {len(bad)} of {len(px)} pixels outside 1e-4\n" + "\n".join(rows))

@@ -15,6 +15,10 @@ import rmse_lib
 pytestmark = pytest.mark.gpu
 
 FIXTURES = rmse_lib.fixtures()
+# The pixels of a fixture outside 1e-4 of the reference's render of the same samples, by configuration: config 3's
+# pixel 88342 holds one sample (index 37) outside the per-sample bar, which comes within it with the transcendental
+# functions rounded from double (tests/test_gpu_parity_cause.py, test_volume_fixture_outlier_pixels).
+OUTSIDE = {3: [88342]}
 
 
 @pytest.mark.parametrize("path", FIXTURES, ids=[os.path.basename(p)[:-4] for p in FIXTURES])
@@ -27,4 +31,4 @@ def test_rmse_against_converged_reference(ctx, path):
     # reference's, up to a rare sample whose discrete decision flips on a last-ulp difference (which moves its pixel by
     # that sample's share, so a few pixels of a frame may differ by more than 1e-4).
     assert abs(r["wavefront"]["rmse"] - r["cpu_rmse"]) <= 0.01 * r["cpu_rmse"] + 1e-7
-    assert r["frac_within_1e-4_vs_cpu"] >= 0.995
+    assert r["pixels_outside_1e-4"] == OUTSIDE.get(r["scene"], []), r["pixels_outside_1e-4"]

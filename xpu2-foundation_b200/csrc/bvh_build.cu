@@ -182,7 +182,7 @@ __device__ __forceinline__ void grow(Aabb& a, const Aabb& b) {
 // Reads of nodes other threads wrote go through L2 (__ldcg), after the arrival counter that orders them.
 constexpr int kTreelet = 7;
 constexpr float kCi = 1.2f, kCt = 1.0f;
-constexpr int kRestructurePasses = 2;
+constexpr int kRestructurePasses = 3;
 
 __device__ void optimiseTreelet(uint32_t root, uint32_t n, uint32_t* left, uint32_t* right, uint32_t* parent, Aabb* box, uint32_t* count,
                                 float* cost) {

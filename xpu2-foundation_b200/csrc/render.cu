@@ -199,7 +199,9 @@ __device__ __forceinline__ void renderStepsBody(const RenderArgs& a) {
     walk.nodes = walk.tris = 0;
     Pending stack[kMaxPending];
     ShadowReq reqs[kStepRecords];
-    uint32_t size = 0, pixel = 0, index = 0;
+    uint32_t size = 0, n = 0, pixel = 0, index = 0;
+    uint32_t hitTri = ~0u, hitLeaf = 0;  // the closest hit of the pending stack's top ray, once walked
+    float hitT = 0.0f;
     V3 cameraPosition{0, 0, 0}, radiance{0, 0, 0};
     float alpha = 0.0f;
     RayQ r;
@@ -223,6 +225,7 @@ __device__ __forceinline__ void renderStepsBody(const RenderArgs& a) {
                         if (cameraRay(s, pixel, index, camera)) {
                             cameraPending(camera, stack[0]);
                             size = 1;
+                            n = 0;
                             cameraPosition = camera.origin;
                             radiance = V3{0, 0, 0};
                             alpha = 0.0f;
@@ -238,21 +241,49 @@ __device__ __forceinline__ void renderStepsBody(const RenderArgs& a) {
             if (drained) break;
             continue;
         }
-        // The closest hit of each live lane's next pending ray, walked a step at a time.
-        bool tracing = live;
-        if (live) {
-            const Pending& next = stack[size - 1];
-            r = makeRay(bvh, next.origin.x, next.origin.y, next.origin.z, next.dir.x, next.dir.y, next.dir.z);
-            walkStart<false, kShortStack>(walk, r, next.nearT, next.farT);
+        // Each live lane's rays, walked a step at a time with the warp's others: the last vertex's shadow rays in
+        // order, then the closest hit of the next pending ray; a lane whose ray is done starts its next at once.
+        uint32_t j = 0, vis = 0;
+        bool tracing = live && (n > 0 || size > 0), any = n > 0;
+        if (tracing) {
+            const V3 o = any ? reqs[0].origin : stack[size - 1].origin, d = any ? reqs[0].dir : stack[size - 1].dir;
+            r = makeRay(bvh, o.x, o.y, o.z, d.x, d.y, d.z);
+            if (any) walkStart<true, kShortStack>(walk, r, reqs[0].near, reqs[0].far);
+            else walkStart<false, kShortStack>(walk, r, stack[size - 1].nearT, stack[size - 1].farT);
         }
         for (;;) {
             const uint32_t lanes = __ballot_sync(full, tracing);
             if (!lanes) break;
-            if (tracing && walkStep<false, kShortStack>(bvh, r, walk, deep, overflow, 1u, lanes)) tracing = false;
+            if (tracing && walkStepEither<kShortStack>(bvh, r, walk, deep, overflow, 1u, lanes, any)) {
+                if (any) {
+                    if (!walk.best) vis |= 1u << j;
+                    ++j;
+                } else {
+                    hitTri = walk.best;
+                    hitLeaf = walk.bestLeaf;
+                    hitT = walk.tmax;
+                }
+                tracing = false;
+                if (any && j < n) {
+                    const ShadowReq& q = reqs[j];
+                    r = makeRay(bvh, q.origin.x, q.origin.y, q.origin.z, q.dir.x, q.dir.y, q.dir.z);
+                    walkStart<true, kShortStack>(walk, r, q.near, q.far);
+                    tracing = true;
+                } else if (any && size > 0) {
+                    const Pending& next = stack[size - 1];
+                    r = makeRay(bvh, next.origin.x, next.origin.y, next.origin.z, next.dir.x, next.dir.y, next.dir.z);
+                    walkStart<false, kShortStack>(walk, r, next.nearT, next.farT);
+                    any = false;
+                    tracing = true;
+                }
+            }
         }
-        // The vertex: the hit rebuilt as trace() does, then afterTrace and shadeVertex, the shadow rays to the list.
-        uint32_t n = 0;
-        if (live) {
+        // The shadow rays' contributions in the list's order, then the next vertex: the hit rebuilt as trace() does,
+        // afterTrace and shadeVertex, its shadow rays to the list.
+        for (uint32_t k = 0; k < n; ++k)
+            if ((vis >> k) & 1u) radiance = add(radiance, reqs[k].contribution);
+        n = 0;
+        if (live && size > 0) {
             Pending pv = stack[--size];
             const uint32_t top = size;
             ++trace;
@@ -262,15 +293,15 @@ __device__ __forceinline__ void renderStepsBody(const RenderArgs& a) {
             hit.t = hit.u = hit.v = 0;
             hit.normal = hit.origin = hit.below = hit.point = V3{0, 0, 0};
             V3 va{0, 0, 0}, vb{0, 0, 0}, vc{0, 0, 0};
-            if (walk.best != ~0u) {
-                const float4* tp = reinterpret_cast<const float4*>(bvh.tris + walk.bestLeaf);
+            if (hitTri != ~0u) {
+                const float4* tp = reinterpret_cast<const float4*>(bvh.tris + hitLeaf);
                 const float4 A = __ldg(tp), B = __ldg(tp + 1), Cc = __ldg(tp + 2);
                 va = V3{A.x, A.y, A.z};
                 vb = V3{B.x, B.y, B.z};
                 vc = V3{Cc.x, Cc.y, Cc.z};
-                hit.geom = __ldg(s.triMesh + walk.best);
-                hit.prim = walk.best - __ldg(s.meshFirst + hit.geom);
-                hit.t = walk.tmax;
+                hit.geom = __ldg(s.triMesh + hitTri);
+                hit.prim = hitTri - __ldg(s.meshFirst + hit.geom);
+                hit.t = hitT;
                 if (!geometryHit(hit, pv.origin, pv.dir, va, vb, vc)) hit.normal = V3{0, 0, 0};
             }
             const Identity root{pixel, U64(index), U64(s.config.seed), 0};
@@ -284,30 +315,7 @@ __device__ __forceinline__ void renderStepsBody(const RenderArgs& a) {
                 }
             }
         }
-        // The shadow rays: each lane walks its list, starting its next ray as soon as one is done.
-        uint32_t j = 0, vis = 0;
-        tracing = n > 0;
-        if (tracing) {
-            r = makeRay(bvh, reqs[0].origin.x, reqs[0].origin.y, reqs[0].origin.z, reqs[0].dir.x, reqs[0].dir.y, reqs[0].dir.z);
-            walkStart<true, kShortStack>(walk, r, reqs[0].near, reqs[0].far);
-        }
-        for (;;) {
-            const uint32_t lanes = __ballot_sync(full, tracing);
-            if (!lanes) break;
-            if (tracing && walkStep<true, kShortStack>(bvh, r, walk, deep, overflow, 1u, lanes)) {
-                if (!walk.best) vis |= 1u << j;
-                if (++j < n) {
-                    const ShadowReq& q = reqs[j];
-                    r = makeRay(bvh, q.origin.x, q.origin.y, q.origin.z, q.dir.x, q.dir.y, q.dir.z);
-                    walkStart<true, kShortStack>(walk, r, q.near, q.far);
-                } else {
-                    tracing = false;
-                }
-            }
-        }
-        for (uint32_t k = 0; k < n; ++k)
-            if ((vis >> k) & 1u) radiance = add(radiance, reqs[k].contribution);
-        const bool done = live && size == 0;
+        const bool done = live && size == 0 && n == 0;
         if (__any_sync(full, done)) warpFilm(a, done, pixel, index, radiance.x, radiance.y, radiance.z, alpha);
         if (done) {
             ++samples;
