@@ -272,6 +272,9 @@ typedef struct x2_wavefront_shape {
     uint32_t light_split;    /* 1, 2 (with shade_split): the GGX and Lambert vertices' light samples in kernels of their
                                 own, after shade, from the vertex's stored inputs, at 6 (1) or 8 (2) blocks a SM; 0: inside
                                 shade */
+    uint32_t tri_overlap;    /* 1: a lane holding a leaf's triangles tests one a step and goes on visiting nodes meanwhile
+                                (takes effect with short_stack 1 and trace_blocks below 9); 0: it visits no node until the
+                                leaf is done */
 } x2_wavefront_shape;
 void x2_wavefront_shape_defaults(x2_wavefront_shape* shape);
 int x2_wavefront_tune(x2_scene* scene, const x2_wavefront_shape* shape);

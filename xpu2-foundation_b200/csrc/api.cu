@@ -224,6 +224,7 @@ struct x2_scene {
     uint32_t shortStack = kDefaultShortStack;    // traversal stacks' top entries in shared memory (1) or local (0)
     uint32_t shadeSplit = kDefaultShadeSplit;    // shade as one kernel a per-lobe queue (1) or one kernel (0)
     uint32_t lightSplit = kDefaultLightSplit;    // the lobe queues' light samples in kernels of their own (1)
+    uint32_t triOverlap = kDefaultTriOverlap;    // a lane's node visits and triangle tests overlapped (1)
     uint32_t* shadeQ = nullptr;            // the per-lobe queues: 3 x wavePaths entries
     uint32_t batchWindow = 0;              // x2_render_batch: items a window (0: the default)
     uint32_t* hostLast = nullptr;      // pinned
@@ -1269,15 +1270,16 @@ void x2_wavefront_shape_defaults(x2_wavefront_shape* shape) {
     shape->short_stack = kDefaultShortStack;
     shape->shade_split = kDefaultShadeSplit;
     shape->light_split = kDefaultLightSplit;
+    shape->tri_overlap = kDefaultTriOverlap;
 }
 
 int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     if (!s || !shape || shape->refill < 1 || shape->refill > 32 || shape->blocks_per_sm < 1 || shape->blocks_per_sm > 32 ||
         shape->trace_blocks > 32 || shape->shade_blocks > 32 || shape->tri_limit < 1 || shape->tri_limit > 32 || shape->lobe_queues > 1 ||
         shape->shadow_order > 1 || shape->extend_bins > 1 || shape->short_stack > 1 || shape->shade_split > 1 ||
-        shape->light_split > 2) {
+        shape->light_split > 2 || shape->tri_overlap > 1) {
         setError("refill is 1..32 lanes, blocks_per_sm 1..32, trace_blocks and shade_blocks 0..32, tri_limit 1..32, lobe_queues, "
-                 "shadow_order, extend_bins, short_stack and shade_split 0 or 1, light_split 0..2");
+                 "shadow_order, extend_bins, short_stack and shade_split 0 or 1, light_split 0..2, tri_overlap 0 or 1");
         return X2_EINVAL;
     }
     s->reservePaths = shape->paths;
@@ -1293,6 +1295,7 @@ int x2_wavefront_tune(x2_scene* s, const x2_wavefront_shape* shape) {
     s->shortStack = shape->short_stack;
     s->shadeSplit = shape->shade_split;
     s->lightSplit = shape->light_split;
+    s->triOverlap = shape->tri_overlap;
     return X2_OK;
 }
 
@@ -1384,7 +1387,7 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
     const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0,
                                        a.scene.stats != nullptr, s->shadeSplit != 0,
-                                       s->wave.lightJob != nullptr ? s->lightSplit : 0u);
+                                       s->wave.lightJob != nullptr ? s->lightSplit : 0u, s->triOverlap != 0 && s->shortStack != 0 && s->traceBlocks < 9);
     const uint64_t maxIter = items * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     if (s->waveTiming) {
         // Diagnostic form: no graph; events around every kernel, the iteration's times added once it is done.
@@ -2139,7 +2142,7 @@ int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float 
     const int gridWork = s->ctx->smCount * int(s->blocksPerSm);
     const WaveKernels wk = waveKernels(s->traceBlocks, s->shadeBlocks, s->volumeCount != 0, s->triUV != nullptr, s->shortStack != 0,
                                        a.scene.stats != nullptr, s->shadeSplit != 0,
-                                       s->wave.lightJob != nullptr ? s->lightSplit : 0u);
+                                       s->wave.lightJob != nullptr ? s->lightSplit : 0u, s->triOverlap != 0 && s->shortStack != 0 && s->traceBlocks < 9);
     const uint64_t bound = maxItems * (uint64_t(s->config.max_depth) + 2) / paths + uint64_t(s->config.max_depth) + 64;
     const uint32_t maxIter = uint32_t(std::min<uint64_t>(bound, 0xffffffffu));
 
@@ -2467,7 +2470,8 @@ int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefron
                           {&x2_wavefront_shape::extend_bins, {0, 1}},
                           {&x2_wavefront_shape::short_stack, {0, 1}},
                           {&x2_wavefront_shape::shade_split, {0, 1}},
-                          {&x2_wavefront_shape::light_split, {0, 1, 2}}};
+                          {&x2_wavefront_shape::light_split, {0, 1, 2}},
+                          {&x2_wavefront_shape::tri_overlap, {0, 1}}};
     for (const Knob& k : knobs) {
         x2_wavefront_shape keep = cur;
         for (uint32_t v : k.values) {

@@ -354,6 +354,85 @@ __device__ __forceinline__ bool walkStep(const Bvh8& bvh, const RayQ& r, Walk<kS
     return done || (!w.tbits && !(w.bits & 0xff000000u) && w.sp == 0);
 }
 
+// The entry on top of the stack, left there.
+template <int kShort>
+__device__ __forceinline__ uint2 walkTop(const Walk<kShort>& w, const uint2* deep) {
+    const int t = w.sp - 1;
+    return t < kShort ? w.shortStack[size_t(t) * blockDim.x] : deep[t - kShort];
+}
+
+// walkStep with a lane's node visits and triangle tests overlapped: a lane that holds a leaf's triangles tests one of
+// them and also visits its next node in the same step, instead of visiting no node until the leaf is done. A leaf met
+// while one is held goes onto the stack as a triangle group (an entry whose top byte is zero, where a node group
+// always has an internal child); once the held leaf is done, a triangle group on top of the stack becomes the held
+// one. Every node and triangle walkStep would reach is still reached, in another order (a closest hit's culling sees
+// a larger tmax for a while, so it may visit a few more nodes); a closest hit does not depend on the order (nearest t,
+// then lowest triangle), and an any hit only asks whether one exists.
+template <bool kAny, int kShort>
+__device__ __forceinline__ bool walkStepOverlap(const Bvh8& bvh, const RayQ& r, Walk<kShort>& w, uint2* deep, uint32_t* overflow,
+                                                unsigned lanes) {
+    bool visit = (w.bits & 0xff000000u) != 0;
+    if (!visit && w.sp > 0) {
+        const uint2 e = walkTop(w, deep);
+        if (e.y >> 24) {  // a node group
+            --w.sp;
+            w.base = e.x;
+            w.bits = e.y & 0xff000000u;
+            w.imask = (e.y >> 16) & 0xffu;
+            visit = true;
+        } else if (!w.tbits) {  // a triangle group, taken once the held one is done
+            --w.sp;
+            w.tbase = e.x;
+            w.tbits = e.y;
+        }
+    }
+    __syncwarp(lanes);
+    if (visit) {
+        const uint32_t b = __ffs(w.bits >> 24) - 1;
+        w.bits &= ~(1u << (24 + b));
+        const uint32_t slot = b ^ r.oct7;
+        const uint32_t child = w.base + __popc(w.imask & ((1u << slot) - 1u));
+        if (w.bits & 0xff000000u) walkPush(w, deep, make_uint2(w.base, w.bits | (w.imask << 16)), overflow);
+        uint32_t childBase, imask, triBase;
+        const uint32_t hits = visitNode(bvh.nodes, child, r, w.tmin - r.eps, w.tmax + r.eps, childBase, triBase, imask);
+        ++w.nodes;
+        const uint32_t nt = hits & 0x00ffffffu;
+        if (nt) {
+            if (w.tbits) {
+                walkPush(w, deep, make_uint2(triBase, nt), overflow);
+            } else {
+                w.tbase = triBase;
+                w.tbits = nt;
+            }
+        }
+        w.base = childBase;
+        w.bits = hits & 0xff000000u;
+        w.imask = imask;
+    }
+    __syncwarp(lanes);
+    if (w.tbits) {
+        const uint32_t k = __ffs(w.tbits) - 1;
+        w.tbits &= w.tbits - 1;
+        const float4* tp = reinterpret_cast<const float4*>(r.tris + w.tbase + k);
+        const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
+        ++w.tris;
+        float t;
+        if (triTestRotated(r, v0, v1, v2, w.tmin, w.tmax, t)) {
+            if (kAny) {
+                w.best = 1;
+                return true;
+            }
+            const uint32_t id = __float_as_uint(v0.w);
+            if (t < w.tmax || (t == w.tmax && id < w.best)) {
+                w.tmax = t;
+                w.best = id;
+                w.bestLeaf = w.tbase + k;
+            }
+        }
+    }
+    return !w.tbits && !(w.bits & 0xff000000u) && w.sp == 0;
+}
+
 // walkStep with the ray's kind (any hit or closest hit) a run-time flag, for a kernel whose lanes walk rays of both
 // kinds in the same steps: one copy of the step's code serves them all. The same visits and tests as walkStep<any>.
 // Start a closest-hit ray with walkStart<false> and an any-hit ray with walkStart<true>.

@@ -346,7 +346,7 @@ struct QueueSegments {
 };
 
 // shortStacks: the block's kShortStack x kWaveBlock short traversal stacks (shared memory).
-template <bool kAny, bool kStats, bool kBatch, int kShort>
+template <bool kAny, bool kStats, bool kBatch, int kShort, bool kOverlap = false>
 __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, const uint32_t* __restrict__ queue, uint32_t* next,
                                                 uint2* shortStacks, const QueueSegments seg = QueueSegments{nullptr, 0, 0}) {
     const WaveState& w = a.w;
@@ -388,14 +388,16 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
             }
         }
         if (!__any_sync(full, live)) break;
-        const uint32_t liveMask = __ballot_sync(full, live), tris0 = walk.tris;
+        const uint32_t liveMask = __ballot_sync(full, live), tris0 = walk.tris, nodes0 = walk.nodes;
         uint32_t nodeMask = 0;
-        if (kStats) nodeMask = __ballot_sync(full, live && !walk.tbits && ((walk.bits & 0xff000000u) || walk.sp));
-        if (live && walkStep<kAny, kShort>(bvh, r, walk, deep, overflow, a.triLimit, liveMask)) {
+        if (kStats && !kOverlap) nodeMask = __ballot_sync(full, live && !walk.tbits && ((walk.bits & 0xff000000u) || walk.sp));
+        if (live && (kOverlap ? walkStepOverlap<kAny, kShort>(bvh, r, walk, deep, overflow, liveMask)
+                              : walkStep<kAny, kShort>(bvh, r, walk, deep, overflow, a.triLimit, liveMask))) {
             if (kAny) w.svis[k] = walk.best ? 0 : 1;
             else w.hit[k] = make_uint2(walk.best == ~0u ? ~0u : walk.bestLeaf, __float_as_uint(walk.tmax));
             live = false;
         }
+        if (kStats && kOverlap) nodeMask = __ballot_sync(full, walk.nodes != nodes0);
         if (kStats) {
             const uint32_t tested = walk.tris - tris0;
             const uint32_t most = __reduce_max_sync(full, tested), all = __reduce_add_sync(full, tested);
@@ -425,7 +427,7 @@ __device__ __forceinline__ void persistentTrace(const WaveArgs& a, uint32_t n, c
     }
 }
 
-template <bool kBatch, int kShort = kShortStack, bool kStats = false>
+template <bool kBatch, int kShort = kShortStack, bool kStats = false, bool kOverlap = false>
 __device__ __forceinline__ void extendBody(const WaveArgs& a) {
     __shared__ uint2 shortStacks[kShort > 0 ? kShort * kWaveBlock : 1];
     __shared__ uint32_t start[kOctants + 1];
@@ -443,7 +445,7 @@ __device__ __forceinline__ void extendBody(const WaveArgs& a) {
         }
         __syncthreads();
     }
-    persistentTrace<false, kStats && !kBatch, kBatch, kShort>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
+    persistentTrace<false, kStats && !kBatch, kBatch, kShort, kOverlap>(a, n, a.extendQ, a.extendNext, shortStacks, seg);
     if (blockIdx.x == 0 && threadIdx.x == 0) atomicAdd(&a.counters->trace, (unsigned long long)n);
 }
 
@@ -809,7 +811,7 @@ __device__ __forceinline__ void shadeBody(const WaveArgs& a) {
 }
 
 // ---- shadow: any hits ----
-template <bool kBatch, int kShort = kShortStack, bool kStats = false>
+template <bool kBatch, int kShort = kShortStack, bool kStats = false, bool kOverlap = false>
 __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
     __shared__ uint32_t start[kRecordSegments + 1];
     QueueSegments seg{start, 0, a.paths};
@@ -828,7 +830,7 @@ __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
         n = start[seg.segments];
     }
     __shared__ uint2 shortStacks[kShort > 0 ? kShort * kWaveBlock : 1];
-    persistentTrace<true, kStats && !kBatch, kBatch, kShort>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
+    persistentTrace<true, kStats && !kBatch, kBatch, kShort, kOverlap>(a, n, a.shadowQ, a.shadowNext, shortStacks, seg);
 }
 
 // The kernels, each in a few occupancy variants (blocks of kWaveBlock threads a SM that the register allocation must
@@ -853,6 +855,11 @@ __global__ void __launch_bounds__(kWaveBlock) wfShadow(WaveArgs a) { shadowBody<
 // so that the timed ones carry none of the counting's registers.
 __global__ void __launch_bounds__(kWaveBlock) wfExtendCount(WaveArgs a) { extendBody<false, kShortStack, true>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadowCount(WaveArgs a) { shadowBody<false, kShortStack, true>(a); }
+// Node visits and triangle tests overlapped in a lane's steps (wavefront shape tri_overlap), timed and counting.
+__global__ void __launch_bounds__(kWaveBlock) wfExtendOverlap(WaveArgs a) { extendBody<false, kShortStack, false, true>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShadowOverlap(WaveArgs a) { shadowBody<false, kShortStack, false, true>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfExtendOverlapCount(WaveArgs a) { extendBody<false, kShortStack, true, true>(a); }
+__global__ void __launch_bounds__(kWaveBlock) wfShadowOverlapCount(WaveArgs a) { shadowBody<false, kShortStack, true, true>(a); }
 // The traversal kernels with their whole stacks in local memory (wavefront shape short_stack 0).
 __global__ void __launch_bounds__(kWaveBlock) wfExtendLocal(WaveArgs a) { extendBody<false, 0>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShadowLocal(WaveArgs a) { shadowBody<false, 0>(a); }
@@ -903,7 +910,7 @@ void launchShade(const WaveKernels& k, const WaveArgs& a, int grid, cudaStream_t
 }
 
 WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack, bool counting,
-                        bool shadeSplit, uint32_t lightSplit) {
+                        bool shadeSplit, uint32_t lightSplit, bool overlap) {
     const bool lightSplit8 = lightSplit == 2;
     WaveKernels k;
     k.shadeBy[0] = k.shadeBy[1] = k.shadeBy[2] = nullptr;
@@ -926,7 +933,10 @@ WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes
     k.logic = wfLogic;
     k.extend = traceBlocks >= 10 ? wfExtendOcc<10> : traceBlocks >= 9 ? wfExtendOcc<9> : shortStack ? wfExtend : wfExtendLocal;
     k.shadow = traceBlocks >= 10 ? wfShadowOcc<10> : traceBlocks >= 9 ? wfShadowOcc<9> : shortStack ? wfShadow : wfShadowLocal;
-    if (counting) {
+    if (overlap) {
+        k.extend = counting ? wfExtendOverlapCount : wfExtendOverlap;
+        k.shadow = counting ? wfShadowOverlapCount : wfShadowOverlap;
+    } else if (counting) {
         k.extend = wfExtendCount;
         k.shadow = wfShadowCount;
     }

@@ -12,7 +12,7 @@ constexpr uint32_t kRecordSegments = 64;
 constexpr uint32_t kDefaultPaths = 1u << 22;
 constexpr uint32_t kDefaultRefill = 8, kDefaultBlocksPerSm = 16, kDefaultTraceBlocks = 0, kDefaultShadeBlocks = 4,
                    kDefaultTriLimit = 1, kDefaultShadowOrder = 0, kDefaultExtendBins = 1, kDefaultShortStack = 1,
-                   kDefaultShadeSplit = 1, kDefaultLightSplit = 1;
+                   kDefaultShadeSplit = 1, kDefaultLightSplit = 1, kDefaultTriOverlap = 1;
 constexpr uint32_t kOctants = 8;
 
 // Path slots (structure of arrays, `paths` slots) and shadow-ray records (recordsPerPath a slot).
@@ -134,8 +134,9 @@ struct WaveKernels {
 // shadeSplit: shade as one kernel a per-lobe queue (surface scenes); lightSplit (with shadeSplit; 1 or 2, 0 off): the
 // GGX and Lambert queues' light samples in kernels of their own after shade, at 6 (1) or 8 (2) blocks a SM (the wave
 // state's lightJob must be allocated).
+// overlap: the traversal kernels that overlap a lane's node visits and triangle tests (walkStepOverlap; short stack).
 WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes, bool textures, bool shortStack = kDefaultShortStack != 0,
-                        bool counting = false, bool shadeSplit = false, uint32_t lightSplit = 0);
+                        bool counting = false, bool shadeSplit = false, uint32_t lightSplit = 0, bool overlap = false);
 // The iteration's shade step: the per-lobe sort (when the queues are on) and the shade kernel or kernels (batch: the
 // batch form's sort).
 void launchShade(const WaveKernels& k, const WaveArgs& a, int grid, cudaStream_t st, bool batch = false);

@@ -118,7 +118,7 @@ class Request(C.Structure):
 
 class WavefrontShape(C.Structure):
     FIELDS = ("paths", "refill", "blocks_per_sm", "trace_blocks", "shade_blocks", "tri_limit", "batch_window", "lobe_queues",
-              "shadow_order", "extend_bins", "short_stack", "shade_split", "light_split")
+              "shadow_order", "extend_bins", "short_stack", "shade_split", "light_split", "tri_overlap")
     _fields_ = [(f, C.c_uint32) for f in FIELDS]
 
     def as_dict(self):
