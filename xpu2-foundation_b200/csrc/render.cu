@@ -254,7 +254,7 @@ __device__ __forceinline__ void renderStepsBody(const RenderArgs& a) {
         for (;;) {
             const uint32_t lanes = __ballot_sync(full, tracing);
             if (!lanes) break;
-            if (tracing && walkStepEither<kShortStack>(bvh, r, walk, deep, overflow, 1u, lanes, any)) {
+            if (tracing && walkStepOverlapKind<kShortStack>(bvh, r, walk, deep, overflow, lanes, any)) {
                 if (any) {
                     if (!walk.best) vis |= 1u << j;
                     ++j;

@@ -368,9 +368,13 @@ __device__ __forceinline__ uint2 walkTop(const Walk<kShort>& w, const uint2* dee
 // one. Every node and triangle walkStep would reach is still reached, in another order (a closest hit's culling sees
 // a larger tmax for a while, so it may visit a few more nodes); a closest hit does not depend on the order (nearest t,
 // then lowest triangle), and an any hit only asks whether one exists.
-template <bool kAny, int kShort>
-__device__ __forceinline__ bool walkStepOverlap(const Bvh8& bvh, const RayQ& r, Walk<kShort>& w, uint2* deep, uint32_t* overflow,
-                                                unsigned lanes) {
+//
+// `any` is the ray's kind (any hit, or closest hit); a kernel whose lanes walk rays of both kinds in the same steps
+// passes it at run time, so that one copy of the step's code serves them all (start a closest-hit ray with
+// walkStart<false> and an any-hit ray with walkStart<true>).
+template <int kShort>
+__device__ __forceinline__ bool walkStepOverlapKind(const Bvh8& bvh, const RayQ& r, Walk<kShort>& w, uint2* deep, uint32_t* overflow,
+                                                    unsigned lanes, bool any) {
     bool visit = (w.bits & 0xff000000u) != 0;
     if (!visit && w.sp > 0) {
         const uint2 e = walkTop(w, deep);
@@ -418,7 +422,7 @@ __device__ __forceinline__ bool walkStepOverlap(const Bvh8& bvh, const RayQ& r, 
         ++w.tris;
         float t;
         if (triTestRotated(r, v0, v1, v2, w.tmin, w.tmax, t)) {
-            if (kAny) {
+            if (any) {
                 w.best = 1;
                 return true;
             }
@@ -432,62 +436,10 @@ __device__ __forceinline__ bool walkStepOverlap(const Bvh8& bvh, const RayQ& r, 
     }
     return !w.tbits && !(w.bits & 0xff000000u) && w.sp == 0;
 }
-
-// walkStep with the ray's kind (any hit or closest hit) a run-time flag, for a kernel whose lanes walk rays of both
-// kinds in the same steps: one copy of the step's code serves them all. The same visits and tests as walkStep<any>.
-// Start a closest-hit ray with walkStart<false> and an any-hit ray with walkStart<true>.
-template <int kShort>
-__device__ __forceinline__ bool walkStepEither(const Bvh8& bvh, const RayQ& r, Walk<kShort>& w, uint2* deep, uint32_t* overflow,
-                                               uint32_t triLimit, unsigned lanes, bool any) {
-    bool visit = !w.tbits, done = false;
-    if (visit && !(w.bits & 0xff000000u)) {
-        if (w.sp == 0) {
-            visit = false;
-            done = true;
-        } else {
-            const uint2 e = walkPop(w, deep);
-            w.base = e.x;
-            w.bits = e.y & 0xff000000u;
-            w.imask = (e.y >> 16) & 0xffu;
-        }
-    }
-    __syncwarp(lanes);
-    if (visit) {
-        const uint32_t b = __ffs(w.bits >> 24) - 1;
-        w.bits &= ~(1u << (24 + b));
-        const uint32_t slot = b ^ r.oct7;
-        const uint32_t child = w.base + __popc(w.imask & ((1u << slot) - 1u));
-        if (w.bits & 0xff000000u) walkPush(w, deep, make_uint2(w.base, w.bits | (w.imask << 16)), overflow);
-        uint32_t childBase, imask;
-        const uint32_t hits = visitNode(bvh.nodes, child, r, w.tmin - r.eps, w.tmax + r.eps, childBase, w.tbase, imask);
-        ++w.nodes;
-        w.tbits = hits & 0x00ffffffu;
-        w.base = childBase;
-        w.bits = hits & 0xff000000u;
-        w.imask = imask;
-    }
-    __syncwarp(lanes);
-    for (uint32_t n = 0; w.tbits && n < triLimit; ++n) {
-        const uint32_t k = __ffs(w.tbits) - 1;
-        w.tbits &= w.tbits - 1;
-        const float4* tp = reinterpret_cast<const float4*>(r.tris + w.tbase + k);
-        const float4 v0 = __ldg(tp), v1 = __ldg(tp + 1), v2 = __ldg(tp + 2);
-        ++w.tris;
-        float t;
-        if (triTestRotated(r, v0, v1, v2, w.tmin, w.tmax, t)) {
-            if (any) {
-                w.best = 1;
-                return true;
-            }
-            const uint32_t id = __float_as_uint(v0.w);
-            if (t < w.tmax || (t == w.tmax && id < w.best)) {
-                w.tmax = t;
-                w.best = id;
-                w.bestLeaf = w.tbase + k;
-            }
-        }
-    }
-    return done || (!w.tbits && !(w.bits & 0xff000000u) && w.sp == 0);
+template <bool kAny, int kShort>
+__device__ __forceinline__ bool walkStepOverlap(const Bvh8& bvh, const RayQ& r, Walk<kShort>& w, uint2* deep, uint32_t* overflow,
+                                                unsigned lanes) {
+    return walkStepOverlapKind<kShort>(bvh, r, w, deep, overflow, lanes, kAny);
 }
 
 // Any hit on [tmin, tmax].
