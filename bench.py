@@ -273,6 +273,7 @@ def frame(scene, cfg, first, wavefront):
 
 def run(args):
     dist, rank, world, local = dist_setup(args.gpus)
+    import torch
     import x2
 
     ctx = x2.Context(local)
@@ -331,15 +332,19 @@ def run(args):
         plain = {"value": world * samples_per_frame / (pmax / 1e3) / 1e6, "unit": "Msamples/s", "ms_per_step": pmax,
                  "steps": len(pms), "warmup": 1, "mrays_per_s": world * rays / args.steps / (pmax / 1e3) / 1e6}
 
-    # End to end through the public API: chunks up, render, film down, audit, every step.
+    # End to end through the public API: chunks up, render, film down, audit, every step. The film comes down into
+    # pinned host arrays the caller keeps across frames (Scene.film's `out`).
     film_bytes = cfg.width * cfg.height * (4 * 8 + 4)
     chunk_bytes = tiles * 16
+    pixels = cfg.width * cfg.height
+    film_out = (torch.empty((pixels, 4), dtype=torch.float64, pin_memory=True).numpy(),
+                torch.empty(pixels, dtype=torch.int32, pin_memory=True).numpy().view(np.uint32))
     barrier(dist, local)
     t0 = time.perf_counter()
     for _ in range(args.steps):
         scene.frame_begin(cfg.spp)
         scene.render_frame_wavefront(first, cfg.spp)
-        sums, counts = scene.film()
+        sums, counts = scene.film(out=film_out)
         scene.audit()
     e2e_s = max_over_ranks(dist, time.perf_counter() - t0, local)
     e2e_value = world * samples_per_frame * args.steps / e2e_s / 1e6

@@ -260,8 +260,8 @@ typedef struct x2_wavefront_shape {
     uint32_t tri_limit;      /* triangle tests a lane makes a traversal step, the rest on the next steps (1..32) */
     uint32_t batch_window;   /* x2_render_batch: work items a window (0: 2^27; at least one chunk a window) */
     uint32_t lobe_queues;    /* 1: shade takes the extended paths from per-lobe queues (GGX, Lambert, then none or
-                                missed), sorted after extend, so a warp runs one lobe's code; 0: in the extend queue's
-                                order */
+                                missed), sorted after extend, so a warp runs one lobe's code (surface scenes; volume
+                                scenes are shaded in the extend queue's order either way); 0: in the extend queue's order */
     uint32_t shadow_order;   /* 1: the shadow queue by record (record k of every path together, mostly one light's rays
                                 to neighbouring origins); 0: by path (each path's records together) */
     uint32_t extend_bins;    /* 1: the extend queue binned by the rays' direction octant (a warp's rays share their

@@ -117,7 +117,7 @@ def test_autotuned_shape_renders_the_same_film(ctx):
     assert np.array_equal(got, want)
 
 
-SHAPES = [{"shadow_order": 1}, {"extend_bins": 0}, {"short_stack": 0}, {"trace_blocks": 9}, {"lobe_queues": 0},
+SHAPES = [{"shadow_order": 1}, {"extend_bins": 1}, {"blocks_per_sm": 16}, {"short_stack": 0}, {"trace_blocks": 9}, {"lobe_queues": 0},
           {"shade_split": 0}, {"light_split": 0}, {"tri_limit": 3}, {"refill": 1}, {"paths": 1024}, {"shade_blocks": 3},
           {"shadow_order": 1, "light_split": 1}, {"tri_overlap": 0}, {"tri_overlap": 0, "shadow_order": 1}]
 

@@ -838,7 +838,9 @@ __device__ __forceinline__ void shadowBody(const WaveArgs& a) {
 // scenes without volumes (the volume code compiled out) and one for scenes with them.
 __global__ void __launch_bounds__(kWaveBlock) wfExtend(WaveArgs a) { extendBody<false>(a); }
 __global__ void __launch_bounds__(kWaveBlock) wfShade(WaveArgs a) { shadeBody<false, false, false, false>(a); }
-__global__ void __launch_bounds__(kWaveBlock, 4) wfShadeVolumes(WaveArgs a) { shadeBody<false, true>(a); }
+// Volume scenes' shade (the march inside it), with the texture lookup compiled in (kTextures) or out.
+template <bool kTextures>
+__global__ void __launch_bounds__(kWaveBlock, 4) wfShadeVolumes(WaveArgs a) { shadeBody<false, true, false, kTextures>(a); }
 __global__ void __launch_bounds__(kWaveBlock, 4) wfShadeBatchVolumes(WaveArgs a) { shadeBody<true, true>(a); }
 __global__ void __launch_bounds__(kWaveBlock, 4) wfShadeAdjoint(WaveArgs a) { shadeBody<false, false, true>(a); }
 
@@ -940,7 +942,7 @@ WaveKernels waveKernels(uint32_t traceBlocks, uint32_t shadeBlocks, bool volumes
         k.extend = wfExtendCount;
         k.shadow = wfShadowCount;
     }
-    if (volumes) k.shade = wfShadeVolumes;
+    if (volumes) k.shade = textures ? wfShadeVolumes<true> : wfShadeVolumes<false>;
     else if (textures) k.shade = wfShadeOcc<4, false, true>;
     else k.shade = shadeBlocks >= 4 ? wfShadeOcc<4, false> : shadeBlocks >= 3 ? wfShadeOcc<3, false> : wfShade;
     return k;

@@ -575,11 +575,22 @@ class Scene:
         out_odd = view(odd_p, (p, 4), "<f8") if odd and odd_p.value else None
         return view(sums, (p, 4), "<f8"), out_odd, view(counts, (p,), "<i4")
 
-    def film(self, odd=False):
+    def film(self, odd=False, out=None):
+        """The film on the host (x2_film_download; waits): FP64 sums (pixels x 4), with `odd` the odd-index sums, and
+        the uint32 counts. `out`, a (sums, counts) or (sums, odd, counts) tuple of C-contiguous arrays of those shapes
+        and types, receives them instead of new arrays: arrays kept across frames (pinned ones copy fastest) spare each
+        frame the allocation and first touch of the film's pages."""
         p = self.config.width * self.config.height
-        sums = np.empty((p, 4), np.float64)
-        counts = np.empty(p, np.uint32)
-        o = np.empty((p, 4), np.float64) if odd else None
+        if out is not None:
+            sums, counts = out[0], out[-1]
+            o = out[1] if odd else None
+            for arr, shape, dt in ((sums, (p, 4), np.float64), (counts, (p,), np.uint32), (o, (p, 4), np.float64)):
+                if arr is not None and (arr.shape != shape or arr.dtype != dt or not arr.flags["C_CONTIGUOUS"]):
+                    raise ValueError("film out arrays must be C-contiguous %s of %s" % (shape, np.dtype(dt).name))
+        else:
+            sums = np.empty((p, 4), np.float64)
+            counts = np.empty(p, np.uint32)
+            o = np.empty((p, 4), np.float64) if odd else None
         _check(library().x2_film_download(self._h, _ptr(sums), _ptr(o), _ptr(counts)))
         return (sums, o, counts) if odd else (sums, counts)
 
