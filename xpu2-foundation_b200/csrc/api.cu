@@ -2453,7 +2453,7 @@ int x2_wavefront_autotune(x2_scene* s, uint32_t tiles, uint32_t spp, x2_wavefron
     if (int rc = timeShape(cur, curMs)) return rc;
     const uint64_t items = uint64_t(tiles) * 64ull * spp;
     std::vector<uint32_t> pathOptions;
-    for (uint32_t p = 1u << 18; p <= (1u << 22); p <<= 1)
+    for (uint32_t p = 1u << 18; p <= (1u << 23); p <<= 1)
         if (p <= items) pathOptions.push_back(p);
     struct Knob {
         uint32_t x2_wavefront_shape::*field;

@@ -9,7 +9,7 @@ constexpr uint32_t kRecordSegments = 64;
 // Launch-shape defaults (x2_wavefront_tune changes them a scene). Paths in flight: 2^22 (each launch of the traversal
 // kernels then has four times the rays of 2^20 for the same ramp-down at its end: 145.3 -> 143.0 -> 155.4 ms for
 // 2^21, 2^22, 2^20 on config 1's 4096 tiles).
-constexpr uint32_t kDefaultPaths = 1u << 22;
+constexpr uint32_t kDefaultPaths = 1u << 23;
 constexpr uint32_t kDefaultRefill = 8, kDefaultBlocksPerSm = 32, kDefaultTraceBlocks = 0, kDefaultShadeBlocks = 4,
                    kDefaultTriLimit = 1, kDefaultShadowOrder = 0, kDefaultExtendBins = 0, kDefaultShortStack = 1,
                    kDefaultShadeSplit = 1, kDefaultLightSplit = 1, kDefaultTriOverlap = 1;
