@@ -238,7 +238,7 @@ int x2_render_frame(x2_scene* scene, uint32_t first, uint32_t count);  /* every 
  * regeneration; the same film. The launch is one CUDA graph whose iterations run in a conditional while node until no
  * path is left (at most a bound from the items, paths and depth; a launch past it completes with X2_EDEVICE at
  * x2_poll / x2_wait), so it returns without waiting, as x2_launch does. One BSDF sample a lobe (bsdf_samples = 1).
- * Paths in flight: x2_wavefront_reserve (default 2^23). x2_items_download reads the last wavefront launch's per-item radiance and
+ * Paths in flight: x2_wavefront_reserve (default 2^23, halved while the path state a scene needs would pass 12 GB). x2_items_download reads the last wavefront launch's per-item radiance and
  * status (item = chunk * 64 * samples_per_chunk + position * samples_per_chunk + sample). */
 int x2_wavefront_reserve(x2_scene* scene, uint32_t paths);
 int x2_launch_wavefront(x2_scene* scene, const x2_chunk* chunks, uint32_t count);

@@ -357,6 +357,17 @@ void freeWave(x2_scene* s) {
     s->wavePaths = s->waveRecords = s->waveCap = 0;
 }
 
+// The paths in flight when the caller reserved none: kDefaultPaths, or fewer (a power of two, at least 2^18) when the
+// path state (slot, light job, queues and `records` shadow records a path) would pass kWaveBudgetBytes, as a scene with
+// many lights would.
+constexpr double kWaveBudgetBytes = 12e9;
+static uint32_t defaultPaths(uint32_t records) {
+    const double perPath = 128.0 + 16.0 * kLightJobWords + 4.0 * (kOctants + 3 + 1) + 53.0 * records;
+    uint32_t paths = kDefaultPaths;
+    while (paths > (1u << 18) && double(paths) * perPath > kWaveBudgetBytes) paths >>= 1;
+    return paths;
+}
+
 // Path slots for `paths` paths with `records` shadow records each.
 // Buffers that already hold at least `paths` paths are kept (a launch indexes them by its own path count), so launches
 // of varying sizes (an adaptive frame's passes) allocate once.
@@ -1369,9 +1380,9 @@ int x2_launch_wavefront(x2_scene* s, const x2_chunk* chunks, uint32_t count) {
         setError("%llu work items in one wavefront launch (at most 2^32 - 1)", items);
         return X2_EINVAL;
     }
-    uint32_t paths = s->reservePaths ? s->reservePaths : kDefaultPaths;
-    if (paths > items) paths = uint32_t(items < 1024 ? 1024 : items);
     const uint32_t records = s->config.light_count * s->config.light_samples + 1;
+    uint32_t paths = s->reservePaths ? s->reservePaths : defaultPaths(records);
+    if (paths > items) paths = uint32_t(items < 1024 ? 1024 : items);
     if (int rc = ensureWave(s, paths, records)) return rc;
     if (int rc = ensureItems(s, items)) return rc;
     cudaStream_t st = s->ctx->stream;
@@ -1687,9 +1698,9 @@ int x2_adjoint(x2_scene* s, uint32_t first, uint32_t count, const float* d_dloss
         setError("x2_adjoint: %llu work items (at most 2^32 - 1)", items);
         return X2_EINVAL;
     }
-    uint32_t paths = s->reservePaths ? s->reservePaths : kDefaultPaths;
-    if (paths > items) paths = uint32_t(items < 1024 ? 1024 : items);
     const uint32_t records = s->config.light_count * s->config.light_samples + 1;
+    uint32_t paths = s->reservePaths ? s->reservePaths : defaultPaths(records);
+    if (paths > items) paths = uint32_t(items < 1024 ? 1024 : items);
     const uint32_t verts = s->config.max_depth + 1;
     if (int rc = ensureWave(s, paths, records)) return rc;
     if (int rc = ensureItems(s, items)) return rc;
@@ -2119,9 +2130,9 @@ int renderAdaptive(x2_scene* s, uint32_t minSamples, uint32_t maxSamples, float 
     }
     Slot& sl = s->slots[0];
     if (int rc = ensureSlot(sl, ad.tiles)) return rc;
-    uint32_t paths = s->reservePaths ? s->reservePaths : kDefaultPaths;
-    if (paths > maxItems) paths = uint32_t(maxItems < 1024 ? 1024 : maxItems);
     const uint32_t records = s->config.light_count * s->config.light_samples + 1;
+    uint32_t paths = s->reservePaths ? s->reservePaths : defaultPaths(records);
+    if (paths > maxItems) paths = uint32_t(maxItems < 1024 ? 1024 : maxItems);
     if (int rc = ensureWave(s, paths, records)) return rc;
     if (int rc = ensureItems(s, maxItems)) return rc;
     cudaStream_t st = s->ctx->stream;
@@ -2562,7 +2573,7 @@ int x2_render_batch(x2_ctx* ctx, const x2_request* req, uint32_t n, x2_completio
     }
     x2_scene* s0 = req[0].scene;
     cudaStream_t st = ctx->stream;
-    uint32_t paths = s0->reservePaths ? s0->reservePaths : kDefaultPaths;
+    uint32_t paths = s0->reservePaths ? s0->reservePaths : defaultPaths(records);
     if (uint64_t(paths) > windowMax) paths = uint32_t(windowMax);
     if (int rc = ensureWave(s0, paths, records)) return rc;
     if (int rc = ensureItems(s0, windowMax)) return rc;
