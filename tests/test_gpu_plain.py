@@ -1,7 +1,8 @@
 """GPU tests of the plain megakernel's frame launch (x2_launch): per sample, the film holds exactly the radiance the
 per-sample entry (x2_integrate, one thread a sample) gives for the same identity, and the launch's counters are the
 wavefront form's. Surface scenes whose vertices make at most 24 shadow rays run the bounce-at-a-time kernel
-(renderSteps), the others the one-thread-a-sample kernel (renderChunks); both must meet the same bar."""
+(renderSteps), the others (volume scenes among them) the one-thread-a-sample kernel (renderChunks); both must meet the
+same bar."""
 import numpy as np
 import pytest
 
@@ -30,11 +31,11 @@ def tile_pixels(cfg, tile):
     return out
 
 
-@pytest.mark.parametrize("cid", [0, 108, 44])
+@pytest.mark.parametrize("cid", [0, 108, 44, 33])
 def test_plain_frame_sample_equals_per_sample_entry(ctx, cid):
     """One sample a pixel: the film's FP64 sum is that sample's float radiance, so it must equal x2_integrate's bit
-    for bit (config 0: the closed box; 108: GGX and Lambert under 16 rect lights and an environment, the bounce-at-a-time
-    kernel; 44: the textured heightfield)."""
+    for bit (config 0: the closed box; 108: GGX and Lambert under 16 rect lights and an environment; 44: the textured
+    heightfield; 33: the participating medium in the box, one thread a sample)."""
     s = x2.SyntheticScene(cid)
     cfg = s.config
     scene = x2.Scene(ctx, s.desc, cfg)
@@ -59,7 +60,7 @@ def test_plain_frame_sample_equals_per_sample_entry(ctx, cid):
     scene.free()
 
 
-@pytest.mark.parametrize("cid", [108, 44])
+@pytest.mark.parametrize("cid", [108, 44, 33])
 def test_plain_launch_counts_the_wavefront_rays(ctx, cid):
     """Ragged chunks (1..6 samples a pixel, edge tiles included): the same film as the wavefront form to FP64 summation
     order, the same counts, and the same rays (closest, light-sample and BSDF shadow rays, held lights, samples)."""
